@@ -1,0 +1,56 @@
+/* CPU oracle: a plain-C restatement of the reference's hot path, used only as
+ * a checker by tests/, __graft_entry__.smoke() and bench.py's CPU baseline.
+ * It is never linked or called by the product library.
+ *
+ * Parity pinning: the generated tables are checked in tests against the
+ * SHA-1 hashes embedded in the reference's own table generator
+ * (pentago/base/precompute.cc:169,194,293,617,929,1035-1038), and every
+ * function is checked against the reference engine itself compiled in place
+ * (oracle/_ref) and against the reference's golden vectors
+ * (pentago/mid/benchmark_test.cc:42-58, pentago/high/high_test.cc:41-85,
+ * data/counts-*.npy).
+ *
+ * Data formats are the reference's: a super is 4 little-endian uint64 words
+ * (bit r = i0 + 4 i1 + 16 i2 + 64 i3, quadrant q rotated left i_q times); a
+ * node is [win, notlost] = 8 uint64 (pentago/end/block_store.h:22-43); a
+ * halfsuper is 2 uint64 (pentago/mid/halfsuper.h:4-60).
+ */
+#ifndef PENTAGO_ORACLE_H
+#define PENTAGO_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+int or_init(void);
+const void* or_table(const char* name, int* bytes);
+
+void or_rmax(const uint64_t* in, uint64_t* out, int n);
+void or_super_wins(const uint64_t* sides, uint64_t* out, int n);
+void or_transform_super(const uint16_t* syms, const uint64_t* in, uint64_t* out, int n);
+void or_symmetry_product(const uint16_t* a, const uint16_t* b, uint16_t* out, int n);
+void or_halfsuper_wins(const uint64_t* sides, const uint8_t* parity, uint64_t* out, int n);
+void or_halfsuper_rmax(const uint64_t* in, uint64_t* out, int n);
+
+int or_line_sizes(uint64_t section_sig, int dim, int length, const uint8_t* block_base,
+                  int64_t* input_nodes, int64_t* output_nodes);
+int or_compute_line(uint64_t section_sig, int dim, int length, const uint8_t* block_base,
+                    const uint64_t* input, uint64_t* output, int threads);
+void or_count_block_wins(uint64_t section_sig, const uint8_t* block, const uint64_t* data,
+                         uint64_t* counts3);
+int or_section_shape(uint64_t section_sig, int* shape4);
+uint64_t or_standardize_section(uint64_t section_sig, int* transform);
+int or_descendent_sections(uint64_t root_sig, int slice, uint64_t* sigs, int cap);
+
+int or_midsolve(uint64_t raw, uint64_t* out_raws, int32_t* out_values);
+void or_midsolve_internal(uint64_t raw, uint64_t* out);
+int or_midsolve_workspace_size(int stones);
+
+int64_t or_rans_encode(const uint8_t* symbols, int64_t n, uint8_t* out, int64_t cap);
+int64_t or_rans_decode(const uint8_t* data, int64_t size, uint8_t* symbols, int64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
