@@ -1,0 +1,316 @@
+"""Benchmark: end-engine block compute on one section, pentago's endgame hot path.
+
+Workload ("config 1", batched): the 30-stone section [[4,4],[4,4],[4,3],[3,4]]
+(shape 160x160x318x318, black to move).  One step computes, for B full 8^4
+blocks of that section, the four block lines through each block (one per
+quadrant dimension, each the full line, exactly the reference's unit of work
+schedule_compute_line), on seeded synthetic child superinfo (win subset of
+notlost, ~31% of notlost bits set; pentago_b200/synthetic.py).  Every line
+has its own child input and output buffer, as in the reference.  Inputs and
+outputs together exceed the 126 MB L2, so no flush is needed between steps.
+
+Metric: positions/s = parent nodes computed x 256 rotations / second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--blocks B] [--impl reference]
+
+Under torchrun each rank computes its own B blocks (weak scaling; lines are
+independent, there is no data-path collective).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SECTION = [[4, 4], [4, 4], [4, 3], [3, 4]]
+METRIC = "end-block positions/s (bit-exact)"
+UNIT = "positions/s"
+PROFILE = os.path.join(ROOT, "profiles", "end_line_kernel.md")
+
+
+def block_of(i):
+    """The i-th benchmark block: full 8^4 blocks spread over the section."""
+    return (i % 20, (7 * i + 3) % 20, (11 * i + 5) % 39, (13 * i + 1) % 39)
+
+
+def plan(blocks, rank):
+    """Line descriptors (without buffers) for this rank's blocks."""
+    from pentago_b200 import end
+    sig = end.section_sig(SECTION)
+    lines = []
+    for t in range(blocks):
+        b = block_of(rank * blocks + t)
+        for dim in range(4):
+            bb = tuple(b[i] for i in range(4) if i != dim)
+            line = end.Line(sig, dim, bb)
+            lines.append((line, end.line_info(line), 1000003 * (rank * blocks + t) + dim))
+    return lines
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == 6:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        import statistics
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[2 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_hbm_peak():
+    try:
+        p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the line kernel from the committed ncu summary."""
+    try:
+        for line in open(PROFILE):
+            if line.startswith("traffic_bytes_per_node:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_reference_rate(seconds=12.0, threads=0):
+    """The reference's own CPU engine (oracle/_ref) on the four lines through
+    block (1,1,1,1) of the section, repeated for about `seconds`."""
+    import ctypes
+    import numpy as np
+    from tests.oracle import reference, P
+    from pentago_b200.synthetic import random_nodes
+    from pentago_b200 import end
+    R = reference()
+    if R is None:
+        return None
+    nthreads = R.lib.ref_threads(threads)
+    sig = end.section_sig(SECTION)
+    work = []
+    for dim in range(4):
+        bb = tuple(1 for i in range(4) if i != dim)
+        line = end.Line(sig, dim, bb)
+        info = end.line_info(line)
+        work.append((dim, line.length, (ctypes.c_uint8 * 3)(*bb), random_nodes(dim + 1, info.input_nodes),
+                     np.zeros((info.output_nodes, 8), np.uint64)))
+    nodes = 0
+    t0 = time.perf_counter()
+    while True:
+        for dim, length, bb, inp, out in work:
+            R.compute_line(sig, dim, length, bb, P(inp), P(out), 0)
+            nodes += out.shape[0]
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return {"value": nodes * 256 / el, "unit": UNIT, "cores": nthreads, "kind": "reference",
+            "sample": f"4 block lines through block (1,1,1,1) of section {SECTION}, repeated for {el:.1f} s "
+                      f"({nodes} parent nodes), reference engine oracle/_ref on {nthreads} threads"}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    r = cpu_reference_rate(seconds=max(5.0, 2.0 * args.steps))
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+        return
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "u64 bitsets",
+            "data": "synthetic", "config": {"workload": f"end block lines, section {SECTION}", "host_cpu": True},
+            "cpu_baseline": r, "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                       "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--blocks", type=int, default=16)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from pentago_b200 import capi, end
+    from pentago_b200.synthetic import random_nodes
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+    capi.check(capi.lib().pg_init())
+    stream = torch.cuda.current_stream()
+
+    # Buffers: pinned host copies (for the end-to-end leg) and device copies
+    lines = plan(args.blocks, rank)
+    host_in, host_out, dev_lines = [], [], []
+    in_bytes = out_bytes = 0
+    out_nodes = 0
+    alg_bytes = 0
+    for line, info, seed in lines:
+        hi = torch.from_numpy(random_nodes(seed, info.input_nodes).view(np.int64)).pin_memory()
+        ho = torch.empty((info.output_nodes, 8), dtype=torch.int64).pin_memory()
+        line.input = hi.to(dev, non_blocking=True)
+        line.output = torch.empty((info.output_nodes, 8), dtype=torch.int64, device=dev)
+        host_in.append(hi)
+        host_out.append(ho)
+        in_bytes += hi.numel() * 8
+        out_bytes += ho.numel() * 8
+        out_nodes += info.output_nodes
+        alg_bytes += 64 * (info.input_nodes + info.output_nodes)
+    ls = [l for l, _, _ in lines]
+    torch.cuda.synchronize()
+
+    def step():
+        end.compute_lines(ls, stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Device-resident timing (value + roofline)
+    for _ in range(args.warmup):
+        step()
+    end.check_errors(stream)
+    barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        barrier()
+        t_start = torch.cuda.Event(enable_timing=True)
+        t_stop = torch.cuda.Event(enable_timing=True)
+        t_start.record(stream)
+        for k in range(args.steps):
+            starts[k].record(stream)
+            step()
+            stops[k].record(stream)
+        t_stop.record(stream)
+        barrier()
+    end.check_errors(stream)
+    elapsed_ms = max_over_ranks(t_start.elapsed_time(t_stop))
+    kernel_ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops)) / args.steps
+    units_all = out_nodes * 256 * args.steps * world
+    value = units_all / (elapsed_ms / 1e3)
+
+    # End-to-end through the public API with host buffers
+    def e2e_step():
+        for l, hi in zip(ls, host_in):
+            l.input.copy_(hi, non_blocking=True)
+        end.compute_lines(ls, stream)
+        for l, ho in zip(ls, host_out):
+            ho.copy_(l.output, non_blocking=True)
+        stream.synchronize()
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    barrier()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_stop = torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(2, args.steps // 2)
+    e_start.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e_stop.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e_start.elapsed_time(e_stop))
+    e2e_value = out_nodes * 256 * e2e_steps * world / (e2e_ms / 1e3)
+
+    peak, peak_kind = measured_hbm_peak()
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    traffic_per_node = profiled_traffic()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_rate(seconds=12.0)
+
+    if rank == 0:
+        result = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64 bitsets", "data": "synthetic",
+            "config": {"workload": f"end-engine block compute: 4 full block lines through each of {args.blocks} "
+                                   f"8^4 blocks of the 30-stone section {SECTION} per GPU",
+                       "blocks_per_gpu": args.blocks, "lines_per_gpu": len(ls),
+                       "parent_nodes_per_step_per_gpu": out_nodes,
+                       "bytes_resident_per_gpu": in_bytes + out_bytes,
+                       "l2": "inputs+outputs exceed L2; no flush between steps", "parallelism": f"lines sharded, dp{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (traffic_per_node * out_nodes / 4) if traffic_per_node else None,
+                         "algorithmic_bytes_per_step": alg_bytes, "kernel": "end_line_kernel",
+                         "launches_per_step": 4},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes},
+            "gpu_launches": 4 * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(result))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

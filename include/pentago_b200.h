@@ -1,0 +1,123 @@
+/* pentago_b200: B200-native (sm_100a) kernels for pentago's backward solve.
+ *
+ * C ABI.  All pointers marked "device" are CUDA device pointers on the current
+ * device; `stream` is a cudaStream_t (NULL = legacy default stream).  Every
+ * entry point returns 0 on success or a negative PG_ERR_* code and never
+ * aborts; pg_last_error() describes the last failure on the calling thread.
+ *
+ * Data formats are the reference's own (github.com/girving/pentago):
+ *   - a super is 4 little-endian uint64 words, bit r = i0 + 4 i1 + 16 i2 + 64 i3
+ *     (pentago/base/superscore.h:29-44);
+ *   - an end-engine node is [we-win super, we-win-or-tie super] = 64 bytes
+ *     (pentago/end/block_store.h:22-43);
+ *   - nodes of a section are ordered by rotation-minimal quadrant index in
+ *     8x8x8x8 blocks, each block row-major in its own shape
+ *     (pentago/end/compute.h:21-27, pentago/base/section.h:26-27);
+ *   - a halfsuper is 2 little-endian uint64 (pentago/mid/halfsuper_c.h:9-19).
+ */
+#ifndef PENTAGO_B200_H
+#define PENTAGO_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PG_OK 0
+#define PG_ERR_ARG -1      /* invalid argument (bad section, dimension, size...) */
+#define PG_ERR_CUDA -2     /* a CUDA call failed */
+#define PG_ERR_BOUNDS -3   /* a device-side bounds check failed */
+#define PG_ERR_TIMEOUT -4  /* a bounded device wait ran out */
+#define PG_ERR_FORMAT -5   /* malformed encoded stream */
+#define PG_ERR_CAPACITY -6 /* output buffer too small / budget exceeded */
+
+const char* pg_last_error(void);
+
+/* Build host tables and upload them to the current device.  Called implicitly
+ * by every entry point; exposed so callers can pay the cost up front. */
+int pg_init(void);
+
+/* ---------------------------------------------------------------------------
+ * End engine.
+ *
+ * pg_line_t mirrors the reference's line_t (pentago/end/line.h:15-33) plus the
+ * buffers that line_details_t owns (pentago/end/compute.h:48-108).  The child
+ * line holds input_blocks blocks of the standardized child section
+ * section.child(dimension).standardize<8>() along the child dimension; the
+ * output line holds `length` blocks of `section` along `dimension`.
+ * ------------------------------------------------------------------------- */
+
+#define PG_LINE_STORE 0 /* write the line's result */
+#define PG_LINE_OR 1    /* OR the result into output (accumulate, end/block_store.cc:173-226) */
+
+typedef struct {
+  uint64_t section;        /* section_t::sig() of the parent section */
+  uint8_t dimension;       /* which way the line points (0..3) */
+  uint8_t length;          /* length in blocks */
+  uint8_t block_base[3];   /* block indices in the other three dimensions */
+  uint8_t flags;           /* PG_LINE_STORE or PG_LINE_OR */
+  uint8_t reserved[2];
+  const uint64_t* input;   /* device: child line data (unused for 35-stone sections) */
+  uint64_t* output;        /* device: parent line data */
+  /* Node offset of child block k from `input`: input_block_offsets[k] if that
+   * host array is given, else k * input_block_stride (0 = packed blocks).
+   * The reference's own buffers use block_stride + 1 (end/compute.cc:135-138). */
+  const int64_t* input_block_offsets;
+  const int64_t* output_block_offsets;
+  int64_t input_block_stride;
+  int64_t output_block_stride;
+} pg_line_t;
+
+typedef struct {
+  int64_t input_nodes;     /* nodes in the child line (0 for 35-stone sections) */
+  int64_t output_nodes;    /* nodes in the output line */
+  int32_t input_blocks;    /* child blocks along the line */
+  int32_t block_stride;    /* nodes per full block of the line (end/compute.h:50) */
+  uint64_t child_section;  /* sig of the standardized child section */
+  int32_t child_dimension; /* dimension of the line inside the child section */
+  int32_t input_shape[4];  /* unstandardized (end/compute.cc:27-37) */
+  int32_t output_shape[4];
+} pg_line_info_t;
+
+/* Shapes of a line (line_data_t, pentago/end/compute.cc:24-46). */
+int pg_line_info(const pg_line_t* line, pg_line_info_t* info);
+
+/* Compute block lines: the GPU form of schedule_compute_line
+ * (pentago/end/compute.h:122-123, compute.cc:394-404).  Lines whose outputs
+ * overlap must not be passed in the same call. */
+int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream);
+
+/* Synchronize `stream` and report device-side bounds violations recorded by
+ * the line kernel since the last call (PG_ERR_BOUNDS), clearing them. */
+int pg_end_check(void* stream);
+
+/* Shape of a section along its four quadrants (section_t::shape,
+ * pentago/base/section.cc:38-43). */
+int pg_section_shape(uint64_t section, int32_t* shape4);
+
+/* Standardized section (section_t::standardize<8>, pentago/base/section.cc:88-101). */
+int pg_section_standardize(uint64_t section, uint64_t* standard, int32_t* transform);
+
+/* ---------------------------------------------------------------------------
+ * Unit-level device operations, used by tests to check the superscore
+ * library against the reference (pentago/base/superscore.h, symmetry.h).
+ *   op 0: out[i] = rmax(in[i])                         in: supers
+ *   op 1: out[i] = super_wins(in[i])                   in: sides (1 uint64)
+ *   op 2: out[i] = transform_super(sym[i], in[i])      sym = global << 8 | local
+ * ------------------------------------------------------------------------- */
+int pg_debug_super(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Self-test entry points (CPU only).  They run the kernels' own arithmetic
+ * (the same __host__ __device__ functions) sequentially on the host, so CPU
+ * tests can check it against the oracle without a GPU.  They are not a
+ * fallback: no entry point above ever calls them.
+ * ------------------------------------------------------------------------- */
+int pg_selftest_super_host(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n);
+int pg_selftest_end_lines_host(const pg_line_t* lines, int n);  /* host buffers */
+const void* pg_selftest_table(const char* name, int* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

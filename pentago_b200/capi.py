@@ -1,0 +1,118 @@
+"""ctypes bindings for the C ABI in include/pentago_b200.h.
+
+The shared library is built in-tree by ``python -m pentago_b200.build`` into
+pentago_b200/_lib/libpentago_b200.so.  Loading fails loudly if it is missing:
+there is no CPU fallback behind these entry points.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libpentago_b200.so")
+
+PG_OK = 0
+PG_ERR_ARG = -1
+PG_ERR_CUDA = -2
+PG_ERR_BOUNDS = -3
+PG_ERR_TIMEOUT = -4
+PG_ERR_FORMAT = -5
+PG_ERR_CAPACITY = -6
+
+PG_LINE_STORE = 0
+PG_LINE_OR = 1
+
+
+class PentagoError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"pentago_b200 error {code}: {message}")
+        self.code = code
+
+
+class pg_line_t(ctypes.Structure):
+    _fields_ = [
+        ("section", ctypes.c_uint64),
+        ("dimension", ctypes.c_uint8),
+        ("length", ctypes.c_uint8),
+        ("block_base", ctypes.c_uint8 * 3),
+        ("flags", ctypes.c_uint8),
+        ("reserved", ctypes.c_uint8 * 2),
+        ("input", ctypes.c_void_p),
+        ("output", ctypes.c_void_p),
+        ("input_block_offsets", ctypes.POINTER(ctypes.c_int64)),
+        ("output_block_offsets", ctypes.POINTER(ctypes.c_int64)),
+        ("input_block_stride", ctypes.c_int64),
+        ("output_block_stride", ctypes.c_int64),
+    ]
+
+
+class pg_line_info_t(ctypes.Structure):
+    _fields_ = [
+        ("input_nodes", ctypes.c_int64),
+        ("output_nodes", ctypes.c_int64),
+        ("input_blocks", ctypes.c_int32),
+        ("block_stride", ctypes.c_int32),
+        ("child_section", ctypes.c_uint64),
+        ("child_dimension", ctypes.c_int32),
+        ("input_shape", ctypes.c_int32 * 4),
+        ("output_shape", ctypes.c_int32 * 4),
+    ]
+
+
+# Every exported symbol of include/pentago_b200.h with its ctypes signature.
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_U64 = ctypes.c_uint64
+_I64 = ctypes.c_int64
+SIGNATURES = {
+    "pg_last_error": (ctypes.c_char_p, []),
+    "pg_init": (_I, []),
+    "pg_line_info": (_I, [ctypes.POINTER(pg_line_t), ctypes.POINTER(pg_line_info_t)]),
+    "pg_end_compute_lines": (_I, [ctypes.POINTER(pg_line_t), _I, _P]),
+    "pg_end_check": (_I, [_P]),
+    "pg_section_shape": (_I, [_U64, ctypes.POINTER(ctypes.c_int32)]),
+    "pg_section_standardize": (_I, [_U64, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_int32)]),
+    "pg_debug_super": (_I, [_I, _P, _P, _P, _I, _P]),
+    "pg_selftest_super_host": (_I, [_I, _P, _P, _P, _I]),
+    "pg_selftest_end_lines_host": (_I, [ctypes.POINTER(pg_line_t), _I]),
+    "pg_selftest_table": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.POINTER(_I)]),
+}
+
+_lib = None
+
+
+def lib():
+    """Load the library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m pentago_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(code):
+    """Raise PentagoError for a negative return code."""
+    if code < 0:
+        raise PentagoError(code, lib().pg_last_error().decode(errors="replace"))
+    return code
+
+
+def ptr(x):
+    """Raw address of a torch tensor or numpy array (or None)."""
+    if x is None:
+        return None
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return x.ctypes.data
+
+
+def stream_handle(stream=None):
+    """cudaStream_t of a torch stream (default: the current stream)."""
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)

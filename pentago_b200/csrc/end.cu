@@ -1,0 +1,373 @@
+// End-engine block-line compute on the GPU: the replacement for
+// schedule_compute_line / compute_microline (pentago/end/compute.cc:219-404).
+//
+// One CTA computes one microline (a 1-D run of parent nodes along the line's
+// dimension at one cross-section position).  It works in two phases:
+//
+//  1. child phase: every child node j of the microline is loaded once and
+//     turned into Q_j = T_{b * L_j}(rmax(~child_j)), the child's contribution
+//     already moved into the parent's frame, for both the win and the
+//     not-lost halves.  rmax commutes with every symmetry (rmax(C) = C + R
+//     with R = {+-e_q}, which every conjugation phi_g preserves), so this is
+//     the reference's rmax(transform_super(s, ~child)) with the per-move part
+//     of s factored out.  Q lives in shared memory.
+//  2. parent phase: each parent node ORs, over its empty cells, the
+//     immediate wins of the move plus Q_j translated along the line's own
+//     axis by the move's rotation (the leftmost factor local((ir&3)<<2dim) of
+//     the reference's symmetry, compute.cc:336-338), then applies the
+//     immediate-win masks of compute.cc:353-355.
+//
+// 35-stone sections have no children (compute_microline<true>): the child
+// result is the immediate one, compute.cc:329-333.
+#include "superscore.cuh"
+#include "lines.h"
+#include "runtime.h"
+#include "../../include/pentago_b200.h"
+#include <algorithm>
+#include <vector>
+
+namespace pg {
+
+PG_HD int pow3(int b) {  // 3^b for 0 <= b < 9, the radix-3 weight of quadrant cell b
+  return ((b & 1) ? 3 : 1) * ((b & 2) ? 9 : 1) * ((b & 4) ? 81 : 1) * ((b & 8) ? 6561 : 1);
+}
+
+PG_HD int ladd(int a, int b) {
+  return (((a & 0x33) + (b & 0x33)) & 0x33) + (((a & 0xcc) + (b & 0xcc)) & 0xcc);
+}
+
+// Per-device error word for device-side bounds checks (bit 0: child index
+// out of range).  Read and cleared by pg_end_check.
+__device__ unsigned int d_end_errors;
+
+struct microline_geom {
+  int64_t input_base, last_input_base, output_base, last_output_base;
+  int input_stride, output_stride;
+  uint64_t base_side0, base_side1;
+  int base_l;
+};
+
+PG_HD void row_strides(const int* shape, int* st) {
+  st[3] = 1;
+  st[2] = shape[3];
+  st[1] = shape[3] * shape[2];
+  st[0] = shape[3] * shape[2] * shape[1];
+}
+
+// Index bookkeeping of compute_microline (compute.cc:224-281).
+template<int DIM>
+PG_HD microline_geom microline_setup(const line_dev_t& L, const dev_tables_t& T, int m) {
+  microline_geom G;
+  int fb[4];
+  const int c1 = L.cross[1], c2 = L.cross[2];
+  fb[DIM] = 0;
+#pragma unroll
+  for (int i = 0, k = 0; i < 4; i++) {
+    if (i == DIM) continue;
+    fb[i] = k == 0 ? m / (c1 * c2) : k == 1 ? m / c2 % c1 : m % c2;
+    k++;
+  }
+  // Parent quadrants of the cross-section
+  uint64_t s0 = 0, s1 = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (q == DIM) continue;
+    const int qv = ldg(T.rmin_flat + L.rmin_off[q] + 8 * L.block0[q] + fb[q]);
+    s0 |= uint64_t(ldg(T.unpack + 2 * qv + L.turn)) << (16 * q);
+    s1 |= uint64_t(ldg(T.unpack + 2 * qv + 1 - L.turn)) << (16 * q);
+  }
+  G.base_side0 = s0;
+  G.base_side1 = s1;
+  // Output addressing
+  int obs[4], ost[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) obs[i] = i == DIM ? 8 : L.out_shape[i];
+  row_strides(obs, ost);
+  G.output_stride = ost[DIM];
+  G.output_base = int64_t(ost[0]) * fb[0] + ost[1] * fb[1] + ost[2] * fb[2] + ost[3] * fb[3];
+  // Input addressing, in the standardized child section
+  int ibs[4], ist[4], fcb[4], rcb[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) ibs[i] = obs[L.perm[i]];
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    fcb[i] = fb[L.perm[i]];
+    const int fcn = 8 * L.first_child_block[i] + fcb[i];
+    rcb[i] = fcb[i] ^ int(i != L.child_dim && fcn < L.refl_moves[i]);
+  }
+  row_strides(ibs, ist);
+  G.input_stride = ist[L.child_dim];
+  G.input_base = int64_t(ist[0]) * rcb[0] + ist[1] * rcb[1] + ist[2] * rcb[2] + ist[3] * rcb[3];
+  // Last blocks are shorter along the line
+  obs[DIM] = (L.nparent & 7) ? (L.nparent & 7) : 8;
+  row_strides(obs, ost);
+  G.last_output_base = int64_t(ost[0]) * fb[0] + ost[1] * fb[1] + ost[2] * fb[2] + ost[3] * fb[3];
+  ibs[L.child_dim] = (L.nchild & 7) ? (L.nchild & 7) : 8;
+  row_strides(ibs, ist);
+  G.last_input_base = int64_t(ist[0]) * rcb[0] + ist[1] * rcb[1] + ist[2] * rcb[2] + ist[3] * rcb[3];
+  // Base transform = inverse_transform * (reflection locals of the cross dims)
+  int local = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    if (i != L.child_dim) local += L.xsym[i][fcb[i] & 7];
+  G.base_l = ladd(L.inv_l, local);
+  return G;
+}
+
+// Phase 1: children j = start, start + step, ... -> Q (4 uint4 per child:
+// win half then not-lost half, both already in the parent frame).
+PG_HD void microline_children(const line_dev_t& L, const microline_geom& G, uint4* q, int start, int step) {
+  for (int j = start; j < L.nchild; j += step) {
+    const int jj = j ^ int(j < L.line_moves);
+    const int blk = j >> 3;
+    const int64_t idx = L.in_off[blk] + (blk == L.input_blocks - 1 ? G.last_input_base : G.input_base) +
+                        int64_t(G.input_stride) * (jj & 7);
+    const uint64_t* node = L.input + 8 * idx;
+    const super8 cw = s_load_ldg(node), cn = s_load_ldg(node + 4);
+    const int l = ladd(G.base_l, L.csym[j]);
+    super8 qw = s_translate(s_rmax(s_not(cn)), l);
+    super8 qn = s_translate(s_rmax(s_not(cw)), l);
+    s_phi_runtime(qw, L.g);
+    s_phi_runtime(qn, L.g);
+    q[4 * j + 0] = make_uint4(qw.w[0], qw.w[1], qw.w[2], qw.w[3]);
+    q[4 * j + 1] = make_uint4(qw.w[4], qw.w[5], qw.w[6], qw.w[7]);
+    q[4 * j + 2] = make_uint4(qn.w[0], qn.w[1], qn.w[2], qn.w[3]);
+    q[4 * j + 3] = make_uint4(qn.w[4], qn.w[5], qn.w[6], qn.w[7]);
+  }
+}
+
+// Phase 2: parents i = start, start + step, ...
+template<int DIM>
+PG_HD void microline_parents(const line_dev_t& L, const dev_tables_t& T, const microline_geom& G,
+                             const uint4* qs, int start, int step, unsigned* errors) {
+  const int turn = L.turn;
+  for (int i = start; i < L.nparent; i += step) {
+    const int q = ldg(T.rmin_flat + L.rmin_off[DIM] + i);
+    const uint32_t sq0 = ldg(T.unpack + 2 * q + turn), sq1 = ldg(T.unpack + 2 * q + 1 - turn);
+    const uint64_t side0 = G.base_side0 | uint64_t(sq0) << (16 * DIM);
+    const uint64_t side1 = G.base_side1 | uint64_t(sq1) << (16 * DIM);
+    const super8 wins0 = s_super_wins(T.win_factors, side0);
+    const super8 wins1 = s_super_wins(T.win_factors, side1);
+    super8 wins = s_zero(), not_loss = s_zero();
+    uint32_t moves = 511u & ~(sq0 | sq1);
+    while (moves) {
+      const int b = ctz32(moves);
+      moves &= moves - 1;
+      const super8 nw = s_super_wins(T.win_factors, side0 | uint64_t(1) << (16 * DIM + b));
+      wins = s_or(wins, nw);
+      if (L.slice35) {
+        wins = s_or(wins, s_rmax(s_andnot(nw, wins1)));
+        not_loss = s_or(not_loss, s_rmax(s_or(nw, s_not(wins1))));
+      } else {
+        const int ir = ldg(T.rmin_inv + q + (1 + turn) * pow3(b));
+        const int j = ir >> 2, r = ir & 3;
+        if (j >= L.nchild) { *errors |= 1u; continue; }
+        const uint4 a = qs[4 * j], bq = qs[4 * j + 1], c = qs[4 * j + 2], d = qs[4 * j + 3];
+        const super8 qw = {{a.x, a.y, a.z, a.w, bq.x, bq.y, bq.z, bq.w}};
+        const super8 qn = {{c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w}};
+        wins = s_or(wins, s_translate_axis<DIM>(qw, r));
+        not_loss = s_or(not_loss, s_translate_axis<DIM>(qn, r));
+      }
+    }
+    const super8 immediate = s_or(wins0, wins1);
+    const super8 r0 = s_or(s_andnot(wins, immediate), s_andnot(wins0, wins1));
+    const super8 r1 = s_or(s_andnot(not_loss, immediate), wins0);
+    const int blk = i >> 3;
+    const int64_t oidx = L.out_off[blk] + (blk == L.length - 1 ? G.last_output_base : G.output_base) +
+                         int64_t(G.output_stride) * (i & 7);
+    uint64_t* out = L.output + 8 * oidx;
+    if (L.flags & PG_LINE_OR) {
+      s_store(out, s_or(s_load(out), r0));
+      s_store(out + 4, s_or(s_load(out + 4), r1));
+    } else {
+      s_store(out, r0);
+      s_store(out + 4, r1);
+    }
+  }
+}
+
+template<int DIM>
+__global__ void __launch_bounds__(128)
+end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
+  const line_dev_t& L = lines[blockIdx.y];
+  const int m = blockIdx.x;
+  if (m >= L.cross[0] * L.cross[1] * L.cross[2]) return;
+  extern __shared__ uint4 q_smem[];
+  const microline_geom G = microline_setup<DIM>(L, T, m);
+  if (!L.slice35) {
+    microline_children(L, G, q_smem, threadIdx.x, blockDim.x);
+    __syncthreads();
+  }
+  unsigned errors = 0;
+  microline_parents<DIM>(L, T, G, q_smem, threadIdx.x, blockDim.x, &errors);
+  if (errors) atomicOr(&d_end_errors, errors);
+}
+
+// The same microline code run sequentially on the host, for CPU self-tests of
+// the kernel arithmetic.  Never used by pg_end_compute_lines.
+template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_tables_t& T) {
+  std::vector<uint4> q(4 * std::max(L.nchild, 1));
+  unsigned errors = 0;
+  for (int m = 0; m < L.cross[0] * L.cross[1] * L.cross[2]; m++) {
+    const microline_geom G = microline_setup<DIM>(L, T, m);
+    if (!L.slice35) microline_children(L, G, q.data(), 0, 1);
+    microline_parents<DIM>(L, T, G, q.data(), 0, 1, &errors);
+  }
+  return errors;
+}
+
+static int launch_lines(std::vector<line_dev_t>& plans, int dim, cudaStream_t stream, const dev_tables_t& T) {
+  if (plans.empty()) return PG_OK;
+  int maxchild = 0;
+  for (const auto& p : plans) maxchild = std::max(maxchild, p.nchild);
+  line_dev_t* d = nullptr;
+  const size_t bytes = sizeof(line_dev_t) * plans.size();
+  PG_CUDA(cudaMallocAsync(&d, bytes, stream));
+  PG_CUDA(cudaMemcpyAsync(d, plans.data(), bytes, cudaMemcpyHostToDevice, stream));
+  const dim3 grid(512, unsigned(plans.size()));
+  const size_t smem = size_t(maxchild) * 64;
+  switch (dim) {
+    case 0: end_line_kernel<0><<<grid, 128, smem, stream>>>(d, T); break;
+    case 1: end_line_kernel<1><<<grid, 128, smem, stream>>>(d, T); break;
+    case 2: end_line_kernel<2><<<grid, 128, smem, stream>>>(d, T); break;
+    default: end_line_kernel<3><<<grid, 128, smem, stream>>>(d, T); break;
+  }
+  PG_CUDA(cudaGetLastError());
+  PG_CUDA(cudaFreeAsync(d, stream));
+  return PG_OK;
+}
+
+static line_in_t to_in(const pg_line_t& l) {
+  line_in_t in;
+  in.section = l.section;
+  in.dim = l.dimension;
+  in.length = l.length;
+  for (int i = 0; i < 3; i++) in.block_base[i] = l.block_base[i];
+  in.flags = l.flags;
+  in.input = l.input;
+  in.output = l.output;
+  in.input_offsets = l.input_block_offsets;
+  in.output_offsets = l.output_block_offsets;
+  in.input_stride = l.input_block_stride;
+  in.output_stride = l.output_block_stride;
+  return in;
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+extern "C" int pg_line_info(const pg_line_t* line, pg_line_info_t* info) {
+  if (!line || !info) return fail(PG_ERR_ARG, "null argument");
+  line_shapes_t s;
+  std::string err;
+  if (!line_shapes(to_in(*line), s, err)) return fail(PG_ERR_ARG, err);
+  info->input_nodes = int64_t(s.in_shape[0]) * s.in_shape[1] * s.in_shape[2] * s.in_shape[3];
+  info->output_nodes = int64_t(s.out_shape[0]) * s.out_shape[1] * s.out_shape[2] * s.out_shape[3];
+  info->input_blocks = s.input_blocks;
+  info->block_stride = s.block_stride;
+  info->child_section = s.child_std.sig();
+  info->child_dimension = s.child_dim;
+  for (int i = 0; i < 4; i++) { info->input_shape[i] = s.in_shape[i]; info->output_shape[i] = s.out_shape[i]; }
+  return PG_OK;
+}
+
+extern "C" int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream) {
+  if (n < 0 || (n && !lines)) return fail(PG_ERR_ARG, "bad line array");
+  const dev_tables_t* T = device_tables();
+  if (!T) return PG_ERR_CUDA;
+  std::vector<line_dev_t> plans[4];
+  std::string err;
+  for (int i = 0; i < n; i++) {
+    line_dev_t d;
+    if (!plan_line(to_in(lines[i]), d, err)) return fail(PG_ERR_ARG, "line " + std::to_string(i) + ": " + err);
+    if (!d.output || (!d.slice35 && !d.input)) return fail(PG_ERR_ARG, "null line buffer");
+    plans[d.dim].push_back(d);
+  }
+  for (int dim = 0; dim < 4; dim++) {
+    const int rc = launch_lines(plans[dim], dim, (cudaStream_t)stream, *T);
+    if (rc) return rc;
+  }
+  return PG_OK;
+}
+
+extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
+  const tables_t& H = tables();
+  const dev_tables_t T = {H.rmin_flat, H.rmin_inv, &H.unpack[0][0], &H.win_factors[0][0][0], H.rmin_off,
+                          &H.commute[0][0]};
+  std::string err;
+  unsigned errors = 0;
+  for (int i = 0; i < n; i++) {
+    line_dev_t d;
+    if (!plan_line(to_in(lines[i]), d, err)) return fail(PG_ERR_ARG, err);
+    switch (d.dim) {
+      case 0: errors |= host_line<0>(d, T); break;
+      case 1: errors |= host_line<1>(d, T); break;
+      case 2: errors |= host_line<2>(d, T); break;
+      default: errors |= host_line<3>(d, T); break;
+    }
+  }
+  return errors ? fail(PG_ERR_BOUNDS, "bounds check failed") : PG_OK;
+}
+
+// Synchronize `stream` and report device-side bounds violations since the last check.
+extern "C" int pg_end_check(void* stream) {
+  PG_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  unsigned int e = 0, zero = 0;
+  PG_CUDA(cudaMemcpyFromSymbol(&e, d_end_errors, sizeof e));
+  PG_CUDA(cudaMemcpyToSymbol(d_end_errors, &zero, sizeof zero));
+  return e ? fail(PG_ERR_BOUNDS, "device bounds check failed in the line kernel") : PG_OK;
+}
+
+extern "C" int pg_section_shape(uint64_t section, int32_t* shape4) {
+  const section_t s = section_t::from_sig(section);
+  if (!s.valid()) return fail(PG_ERR_ARG, "invalid section");
+  int sh[4];
+  s.shape(sh);
+  for (int i = 0; i < 4; i++) shape4[i] = sh[i];
+  return PG_OK;
+}
+
+extern "C" int pg_section_standardize(uint64_t section, uint64_t* standard, int32_t* transform) {
+  const section_t s = section_t::from_sig(section);
+  if (!s.valid()) return fail(PG_ERR_ARG, "invalid section");
+  int g = 0;
+  *standard = s.standardize(&g).sig();
+  if (transform) *transform = g;
+  return PG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Unit-level superscore checks
+// ---------------------------------------------------------------------------
+
+namespace pg {
+PG_HD void debug_super_one(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int i, const uint32_t* wf) {
+  super8 r;
+  if (op == 0) r = s_rmax(s_load(in + 4 * i));
+  else if (op == 1) r = s_super_wins(wf, in[i]);
+  else r = s_transform(s_load(in + 4 * i), sym[i] >> 8, sym[i] & 255);
+  s_store(out + 4 * i, r);
+}
+__global__ void debug_super_kernel(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n,
+                                   const uint32_t* wf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) debug_super_one(op, in, sym, out, i, wf);
+}
+}  // namespace pg
+
+extern "C" int pg_selftest_super_host(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n) {
+  if (op < 0 || op > 2 || n < 0) return fail(PG_ERR_ARG, "bad debug op");
+  for (int i = 0; i < n; i++) debug_super_one(op, in, sym, out, i, &tables().win_factors[0][0][0]);
+  return PG_OK;
+}
+
+extern "C" int pg_debug_super(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n, void* stream) {
+  if (op < 0 || op > 2 || n < 0) return fail(PG_ERR_ARG, "bad debug op");
+  const dev_tables_t* T = device_tables();
+  if (!T) return PG_ERR_CUDA;
+  if (!n) return PG_OK;
+  debug_super_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(op, in, sym, out, n, T->win_factors);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}

@@ -1,0 +1,72 @@
+// Host planning for end-engine block lines: section algebra and the per-line
+// descriptor the line kernel reads.  The index conventions restate
+// line_data_t / line_details_t (pentago/end/compute.cc:24-123) and the
+// per-microline setup of compute_microline (compute.cc:219-281).
+#pragma once
+#include <cstdint>
+#include <string>
+#include "tables.h"
+
+namespace pg {
+
+struct section_t {
+  uint8_t c[4][2];  // counts[quadrant][black, white]
+
+  static section_t from_sig(uint64_t sig);
+  uint64_t sig() const;
+  int sum() const;
+  bool valid() const;
+  void shape(int* s) const;
+  section_t transform(int global) const;               // section.cc:78-86
+  section_t standardize(int* transform) const;          // section.cc:88-101
+  section_t child(int q) const;                         // section.cc:51-57
+};
+
+// quadrant_permutation (section.cc:106-114): quadrant i maps to p[i]
+void quadrant_permutation(int global, int* p);
+inline int invert_global(int g) { return g ^ ((~g >> 2 & (g & 1)) << 1); }
+
+constexpr int kMaxBlocks = 64;   // 420 nodes / 8 per block < 64
+constexpr int kMaxLine = 424;    // nodes along a quadrant axis, rounded up
+
+// Everything a CTA needs to compute one microline of a line.  Plain data,
+// copied to the device as is.
+struct line_dev_t {
+  int32_t dim, child_dim, turn, slice35, flags;
+  int32_t g, inv_l;                 // base transform = (g, inv_l + reflection locals)
+  int32_t nparent, nchild, length, input_blocks, line_moves;
+  int32_t odims[3], cross[3];       // the three cross dimensions and their extents
+  int32_t perm[4], refl_moves[4], block0[4], first_child_block[4];
+  int32_t out_shape[4];
+  int32_t rmin_off[4];              // offsets of the parent quadrant lists in rmin_flat
+  const uint64_t* input;
+  uint64_t* output;
+  int64_t in_off[kMaxBlocks], out_off[kMaxBlocks];
+  uint8_t csym[kMaxLine];           // reflection locals along the child dimension
+  uint8_t xsym[4][8];               // reflection locals of the cross dimensions
+};
+
+struct line_in_t {
+  uint64_t section;
+  int dim, length;
+  uint8_t block_base[3];
+  int flags;
+  const uint64_t* input;
+  uint64_t* output;
+  const int64_t* input_offsets;
+  const int64_t* output_offsets;
+  int64_t input_stride, output_stride;
+};
+
+struct line_shapes_t {
+  int in_shape[4], out_shape[4];
+  int block_stride, input_blocks, child_dim, st;
+  section_t child_std;
+};
+
+// Validate and compute shapes; returns false with a message on bad input.
+bool line_shapes(const line_in_t& in, line_shapes_t& out, std::string& error);
+// Fill the device descriptor.
+bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error);
+
+}  // namespace pg

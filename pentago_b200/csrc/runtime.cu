@@ -1,0 +1,75 @@
+// Per-device table upload and error reporting.
+#include "runtime.h"
+#include "tables.h"
+#include "../../include/pentago_b200.h"
+#include <mutex>
+#include <vector>
+
+namespace pg {
+
+static thread_local std::string last_error;
+
+void set_error(const std::string& msg) { last_error = msg; }
+int fail(int code, const std::string& msg) { last_error = msg; return code; }
+int cuda_fail(cudaError_t e, const char* what) {
+  last_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return PG_ERR_CUDA;
+}
+
+static std::mutex dev_mutex;
+static std::vector<dev_tables_t*> per_device;
+
+template<class T> static T* upload(const T* host, size_t count) {
+  T* d = nullptr;
+  if (cudaMalloc(&d, sizeof(T) * count) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(d, host, sizeof(T) * count, cudaMemcpyHostToDevice) != cudaSuccess) return nullptr;
+  return d;
+}
+
+const dev_tables_t* device_tables() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { set_error("no CUDA device"); return nullptr; }
+  std::lock_guard<std::mutex> lock(dev_mutex);
+  if (int(per_device.size()) <= dev) per_device.resize(dev + 1, nullptr);
+  if (per_device[dev]) return per_device[dev];
+  const tables_t& T = tables();
+  auto* t = new dev_tables_t;
+  t->rmin_flat = upload(T.rmin_flat, 19683);
+  t->rmin_inv = upload(T.rmin_inv, 19683);
+  t->unpack = upload(&T.unpack[0][0], 2 * 19683);
+  t->win_factors = upload(&T.win_factors[0][0][0], 4 * 512 * 16);
+  t->rmin_off = upload(T.rmin_off, 56);
+  t->commute = upload(&T.commute[0][0], 8 * 256);
+  if (!t->rmin_flat || !t->rmin_inv || !t->unpack || !t->win_factors || !t->rmin_off || !t->commute) {
+    set_error("table upload failed");
+    delete t;
+    return nullptr;
+  }
+  per_device[dev] = t;
+  return t;
+}
+
+}  // namespace pg
+
+extern "C" const char* pg_last_error(void) { return pg::last_error.c_str(); }
+
+extern "C" int pg_init(void) {
+  pg::tables();
+  return pg::device_tables() ? PG_OK : PG_ERR_CUDA;
+}
+
+// Host copy of a named lookup table, for tests that pin the tables against
+// the SHA-1 hashes of the reference's generator.
+extern "C" const void* pg_selftest_table(const char* name, int* bytes) {
+  const pg::tables_t& T = pg::tables();
+  const std::string n(name);
+#define PG_T(str, x) if (n == str) { *bytes = int(sizeof(x)); return &x; }
+  PG_T("pack_table", T.pack) PG_T("unpack_table", T.unpack) PG_T("rotations", T.rot)
+  PG_T("reflections", T.refl) PG_T("commute_global_local_symmetries", T.commute)
+  PG_T("rotation_minimal_quadrants_offsets", T.rmin_off) PG_T("rotation_minimal_quadrants_inverse", T.rmin_inv)
+  PG_T("rotation_minimal_quadrants_reflect_moved", T.rmin_moved)
+#undef PG_T
+  if (n == "rotation_minimal_quadrants_flat") { *bytes = 2 * T.rmin_count; return T.rmin_flat; }
+  *bytes = 0;
+  return nullptr;
+}

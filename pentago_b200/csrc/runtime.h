@@ -1,0 +1,29 @@
+// Per-device state of the library: uploaded tables and error reporting.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+
+namespace pg {
+
+// Device copies of the lookup tables (global memory, read through __ldg).
+struct dev_tables_t {
+  const uint16_t* rmin_flat;   // 19683 entries
+  const uint16_t* rmin_inv;    // 19683
+  const uint16_t* unpack;      // 19683 x 2
+  const uint32_t* win_factors; // 4 x 512 x 16
+  const uint16_t* rmin_off;    // 56
+  const uint8_t* commute;      // 8 x 256
+};
+
+// Tables on the current device (uploaded on first use).  Returns nullptr and
+// sets the error on failure.
+const dev_tables_t* device_tables();
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+#define PG_CUDA(call) do { const cudaError_t _e = (call); if (_e != cudaSuccess) return ::pg::cuda_fail(_e, #call); } while (0)
+
+}  // namespace pg

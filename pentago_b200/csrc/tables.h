@@ -1,0 +1,36 @@
+// Host-side lookup tables for the pentago hot path, generated from first
+// principles at library load (no generated source is shipped).  The layouts of
+// the tables that define storage order (rotation-minimal quadrant lists and
+// their inverse) follow pentago/base/precompute.cc:967-1043 exactly, because
+// they fix the order of nodes inside every section; the tests pin them with
+// the SHA-1 hashes that generator embeds.
+#pragma once
+#include <cstdint>
+
+namespace pg {
+
+struct tables_t {
+  uint16_t pack[512];             // base-2 quadrant side -> base-3 digits (precompute.cc:158-172)
+  uint16_t unpack[19683][2];      // base-3 quadrant -> (side0, side1)     (precompute.cc:174-197)
+  uint16_t rot[512][2];           // [left, right] rotation of a quadrant (precompute.cc:278-296)
+  uint16_t refl[512];             // reflection about x = y               (precompute.cc:606-620)
+  uint64_t winpat[32];            // five-in-a-row masks                  (precompute.cc:198-253)
+  uint16_t rmin_off[56];          // rotation_minimal_quadrants_offsets
+  uint16_t rmin_flat[19683];      // rotation_minimal_quadrants_flat (first rmin_count used)
+  int rmin_count;
+  uint16_t rmin_inv[19683];       // rotation_minimal_quadrants_inverse: q -> 4*index + rotation
+  uint16_t rmin_moved[55];        // rotation_minimal_quadrants_reflect_moved
+  uint8_t commute[8][256];        // commute_global_local_symmetries: [g][l] = g' l g
+  uint8_t gprod[8][8];            // product of global symmetries
+  // Super-wins pattern factors, one 64-byte entry per (quadrant, 9-bit side),
+  // laid out as described in superscore.cuh (win_factor_entry).
+  uint32_t win_factors[4][512][16];
+};
+
+// Built once on first use; thread safe.
+const tables_t& tables();
+
+// Rotation-minimal list for a (black, white) quadrant count.
+inline int rmin_bucket(int b, int w) { return b * (21 - b) / 2 + w; }
+
+}  // namespace pg

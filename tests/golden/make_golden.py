@@ -1,0 +1,116 @@
+"""Generate the golden fixtures in tests/golden/ from the reference repository.
+
+Run in a container that has the reference sources and the in-place reference
+build (``make -C oracle ref``):
+
+    python tests/golden/make_golden.py /path/to/pentago
+
+Fixtures written:
+  tables_sha1.json   SHA-1 hashes embedded in pentago/base/precompute.cc's check() calls
+  midsolve_18.json   the 18-stone board and its 163 (board, middle, value) results from
+                     pentago/mid/benchmark_test.cc (read from the test source)
+  high_samples.json  the (board, wins[8]) samples of pentago/high/high_test.cc:41-85
+  workspace.json     midsolve workspace sizes of pentago/mid/mid_test.cc:129-134
+  counts_30_35.npz   per-section (sig, black wins, white wins, total) rows from
+                     data/counts-{30..35}.npy
+  lines.json         block lines computed by the reference engine itself (oracle/_ref)
+                     on seeded inputs: the seed and the SHA-1 of the output
+"""
+import ctypes
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+
+# Lines covering: rotation-only and reflected child sections, every dimension,
+# a 35-stone section (no children), duplicate-quadrant sections, short last blocks.
+LINE_CASES = [([[4, 4], [4, 5], [4, 3], [4, 4]], 2, (1, 0, 1)),
+              ([[3, 5], [5, 3], [4, 4], [5, 4]], 1, (0, 1, 0)),
+              ([[4, 5], [4, 4], [5, 4], [4, 3]], 3, (0, 0, 0)),
+              ([[5, 4], [4, 5], [4, 4], [4, 4]], 2, (0, 0, 1)),
+              ([[4, 4], [5, 4], [4, 4], [4, 4]], 0, (1, 2, 2)),
+              ([[5, 4], [4, 5], [4, 4], [4, 4]], 3, (0, 0, 0)),
+              ([[5, 4], [4, 4], [4, 5], [4, 4]], 1, (0, 0, 0)),
+              ([[5, 4], [4, 5], [5, 4], [4, 4]], 3, (0, 0, 0)),
+              ([[4, 4], [4, 4], [4, 3], [3, 4]], 0, (1, 1, 1)),
+              ([[4, 4], [4, 4], [4, 3], [3, 4]], 3, (1, 1, 1))]
+
+
+def numbers(text):
+    return [int(x) for x in re.findall(r"-?\d+", text)]
+
+
+def main(ref_root):
+    src = lambda p: open(os.path.join(ref_root, p)).read()
+    # 1. table hashes
+    pre = src("pentago/base/precompute.cc")
+    hashes = {}
+    for m in re.finditer(r'check(?:<uint64_t>)?\((\w+(?:\.\w+)?), "([0-9a-f]{40})"\)', pre):
+        hashes.setdefault(m.group(1), []).append(m.group(2))
+    json.dump(hashes, open(os.path.join(HERE, "tables_sha1.json"), "w"), indent=1)
+
+    # 2. midsolve golden (benchmark_test.cc)
+    bt = src("pentago/mid/benchmark_test.cc")
+    raw0 = re.search(r"raw0 = \{(.*?)\};", bt, re.S).group(1)
+    raw1 = re.search(r"raw1 = \{(.*?)\};", bt, re.S).group(1)
+    pairs0 = [(b, v) for b, v in re.findall(r"\{(\d+),(-?\d+)\}", raw0)]
+    pairs1 = [(b, v) for b, v in re.findall(r"\{(\d+),(-?\d+)\}", raw1)]
+    root = int(re.search(r"from_board\((\d+), false\);\n\s+const auto results", bt).group(1))
+    json.dump({"root": root,
+               "results": [[int(b), 0, int(v)] for b, v in pairs0] + [[int(b), 1, int(v)] for b, v in pairs1]},
+              open(os.path.join(HERE, "midsolve_18.json"), "w"))
+
+    # 3. high_test samples
+    ht = src("pentago/high/high_test.cc")
+    samples = {}
+    for m in re.finditer(r"TEST\(high, board_(\d+)\) \{\s*const board_t boards\[\] = \{(.*?)\};\s*"
+                         r"const uint64_t wins\[\] = \{(.*?)\};", ht, re.S):
+        samples[m.group(1)] = {"boards": [int(x) for x in re.findall(r"\d+", m.group(2))],
+                               "wins": [int(x) for x in re.findall(r"\d+", m.group(3))]}
+    json.dump(samples, open(os.path.join(HERE, "high_samples.json"), "w"))
+
+    # 4. workspace sizes
+    mt = src("pentago/mid/mid_test.cc")
+    ws = numbers(re.search(r"const int correct\[\] = \{(.*?)\};", mt, re.S).group(1))
+    json.dump({"first_slice": 18, "sizes": ws}, open(os.path.join(HERE, "workspace.json"), "w"))
+
+    # 5. golden section counts
+    counts = {}
+    for s in range(30, 36):
+        counts[f"counts_{s}"] = np.load(os.path.join(ref_root, "data", f"counts-{s}.npy"))
+    np.savez_compressed(os.path.join(HERE, "counts_30_35.npz"), **counts)
+
+    # 6. reference-computed lines: inputs are regenerated from the seed, only
+    #    the SHA-1 of the reference engine's output is stored
+    import hashlib
+    from tests.oracle import reference, P
+    from pentago_b200.end import section_sig, section_shape
+    from pentago_b200.synthetic import random_nodes
+    R = reference()
+    assert R is not None, "build oracle/_ref first (make -C oracle ref)"
+    lines = []
+    for k, (c, dim, bb) in enumerate(LINE_CASES):
+        sig = section_sig(c)
+        length = (section_shape(sig)[dim] + 7) // 8
+        ni, no = ctypes.c_int64(), ctypes.c_int64()
+        bbv = (ctypes.c_uint8 * 3)(*bb)
+        R.line_sizes(sig, dim, length, bbv, ctypes.byref(ni), ctypes.byref(no))
+        seed = 1000 + k
+        inp = random_nodes(seed, max(ni.value, 1))
+        res = np.zeros((no.value, 8), np.uint64)
+        R.compute_line(sig, dim, length, bbv, P(inp), P(res), 0)
+        lines.append({"counts": c, "section": sig, "dimension": dim, "block_base": list(bb), "length": length,
+                      "seed": seed, "input_nodes": ni.value, "output_nodes": no.value,
+                      "output_sha1": hashlib.sha1(res.tobytes()).hexdigest()})
+    json.dump(lines, open(os.path.join(HERE, "lines.json"), "w"), indent=1)
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,87 @@
+"""The C-ABI library: it loads, exports every symbol include/pentago_b200.h
+declares, builds tables identical to the reference generator's, and its kernel
+arithmetic (run on the host) matches the oracle.  No GPU."""
+import ctypes
+import hashlib
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from tests.oracle import P
+from tests.test_oracle import HASHES, TABLES, LINES, sha1, random_supers, random_sides
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "pentago_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pg_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    from pentago_b200 import capi
+    lib = capi.lib()
+    names = header_functions()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in capi.SIGNATURES, f"{n} has no ctypes signature"
+
+
+@pytest.mark.parametrize("name,dtype,key,idx,cast", TABLES)
+def test_product_tables_match_precompute_sha1(name, dtype, key, idx, cast):
+    from pentago_b200 import capi
+    n = ctypes.c_int()
+    p = capi.lib().pg_selftest_table(name.encode(), ctypes.byref(n))
+    t = np.frombuffer((ctypes.c_char * n.value).from_address(p), dtype=dtype).copy()
+    if cast:
+        t = t.astype(np.uint64)
+    assert sha1(t) == HASHES[key][idx]
+
+
+def test_kernel_superscore_on_host_matches_oracle(O):
+    from pentago_b200 import capi
+    L = capi.lib()
+    rng = np.random.default_rng(3)
+    n = 4096
+    x = random_supers(rng, n)
+    a, b = np.zeros_like(x), np.zeros_like(x)
+    capi.check(L.pg_selftest_super_host(0, P(x), None, P(a), n))
+    O.rmax(P(x), P(b), n)
+    assert np.array_equal(a, b)
+    sides = random_sides(rng, n)
+    capi.check(L.pg_selftest_super_host(1, P(sides), None, P(a), n))
+    O.super_wins(P(sides), P(b), n)
+    assert np.array_equal(a, b)
+    syms = (np.arange(n) % 2048).astype(np.uint16)
+    capi.check(L.pg_selftest_super_host(2, P(x), P(syms), P(a), n))
+    O.transform_super(P(syms), P(x), P(b), n)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("case", LINES, ids=lambda c: f"{c['counts']}-{c['dimension']}")
+def test_kernel_line_code_on_host_matches_reference_golden(case):
+    from pentago_b200 import end
+    from pentago_b200.synthetic import random_nodes
+    line = end.Line(case["section"], case["dimension"], case["block_base"])
+    info = end.line_info(line)
+    assert (info.input_nodes, info.output_nodes) == (case["input_nodes"], case["output_nodes"])
+    line.input = random_nodes(case["seed"], max(case["input_nodes"], 1))
+    line.output = np.zeros((case["output_nodes"], 8), np.uint64)
+    end.selftest_lines_host([line])
+    assert sha1(line.output) == case["output_sha1"]
+
+
+def test_line_rejects_bad_input():
+    from pentago_b200 import capi, end
+    full = end.section_sig([[5, 4], [4, 5], [4, 4], [4, 3]])
+    with pytest.raises(capi.PentagoError):
+        end.line_info(end.Line(full, 0, (0, 0, 0), length=5))   # quadrant 0 is full
+    with pytest.raises(capi.PentagoError):
+        end.line_info(end.Line(end.section_sig([[4, 4], [4, 4], [4, 3], [3, 4]]), 0, (0, 0, 0), length=3))
+    with pytest.raises(capi.PentagoError):
+        end.line_info(end.Line(end.section_sig([[1, 4], [4, 4], [4, 3], [3, 4]]), 0, (0, 0, 0), length=1))
