@@ -99,6 +99,43 @@ int pg_section_shape(uint64_t section, int32_t* shape4);
 int pg_section_standardize(uint64_t section, uint64_t* standard, int32_t* transform);
 
 /* ---------------------------------------------------------------------------
+ * Midsolve.
+ *
+ * pg_mid_values_t has the layout of the reference's wasm export
+ * mid_values_t = pile<tuple<raw_t,int>, 1+18+8*18> (pentago/mid/midengine.h:34,
+ * js_test.cc:9-20): an int count, then 163 16-byte (raw, value) records, in
+ * midsolve_traverse order (midengine.cc:127-158).  raw_t is
+ * board | middle << 63 (pentago/high/board.h:76).
+ * ------------------------------------------------------------------------- */
+
+typedef struct {
+  uint64_t raw;
+  int32_t value;  /* 1 win, 0 tie, -1 loss for the player to move at `raw` */
+  int32_t pad;
+} pg_mid_value_t;
+
+typedef struct {
+  int32_t size;
+  int32_t pad;
+  pg_mid_value_t entries[163];
+} pg_mid_values_t;
+
+/* Workspace entries midsolve needs for a board with `stones` stones
+ * (midsolve_workspace_size, pentago/mid/midengine.cc:44-46). */
+int pg_midsolve_workspace_size(int stones);
+
+/* Device scratch bytes pg_midsolve_batch needs for these boards. */
+int pg_midsolve_scratch_bytes(const uint64_t* raws, int n, int64_t* bytes);
+
+/* Solve n boards (host array of raw_t, each with >= 18 stones), writing
+ * device array out[n]: the GPU form of midsolve(board, workspace)
+ * (pentago/mid/midengine.cc:161-169) and of the wasm export midsolve(raw,
+ * results) (:171-178).  scratch: device buffer of pg_midsolve_scratch_bytes,
+ * or NULL to allocate on the stream. */
+int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* scratch,
+                      int64_t scratch_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Unit-level device operations, used by tests to check the superscore
  * library against the reference (pentago/base/superscore.h, symmetry.h).
  *   op 0: out[i] = rmax(in[i])                         in: supers

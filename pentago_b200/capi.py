@@ -58,6 +58,16 @@ class pg_line_info_t(ctypes.Structure):
     ]
 
 
+class pg_mid_value_t(ctypes.Structure):
+    _fields_ = [("raw", ctypes.c_uint64), ("value", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+class pg_mid_values_t(ctypes.Structure):
+    _fields_ = [("size", ctypes.c_int32), ("pad", ctypes.c_int32), ("entries", pg_mid_value_t * 163)]
+
+
+MID_VALUES_BYTES = 8 + 16 * 163
+
 # Every exported symbol of include/pentago_b200.h with its ctypes signature.
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -75,6 +85,9 @@ SIGNATURES = {
     "pg_selftest_super_host": (_I, [_I, _P, _P, _P, _I]),
     "pg_selftest_end_lines_host": (_I, [ctypes.POINTER(pg_line_t), _I]),
     "pg_selftest_table": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.POINTER(_I)]),
+    "pg_midsolve_workspace_size": (_I, [_I]),
+    "pg_midsolve_scratch_bytes": (_I, [_P, _I, ctypes.POINTER(_I64)]),
+    "pg_midsolve_batch": (_I, [_P, _I, _P, _P, _I64, _P]),
 }
 
 _lib = None

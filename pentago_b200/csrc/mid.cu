@@ -1,0 +1,526 @@
+// Midsolve on the GPU: the replacement for midsolve / midsolve_internal
+// (pentago/mid/midengine.cc:93-178).
+//
+// The reference solves every position downstream of a root with >= 18 stones
+// by retrograde analysis over subset-ranked stone placements: two passes
+// ("aggressive" = who wins ties), each sweeping the number of placed stones n
+// from `spots` down to 0, where level n reads level n+1 from a workspace that
+// ping-pongs between the two ends of one buffer (mid/internal.h:29-69,
+// :358-408).
+//
+// Here one CTA owns one board.  It precomputes the per-level tables
+// (midengine.cc:57-76), then runs both passes with a CTA barrier between
+// levels.  Inside a level the (s0, s1p) items are split over the CTA's
+// threads in tiles of s0 rows whose per-row data (make_set0_info,
+// internal.h:174-259) is built cooperatively in shared memory.  Boards with
+// up to 10 empty spots (26 or more stones) keep their whole workspace in
+// shared memory (bottleneck(10) = 8400 halfsupers = 134 KB); larger boards
+// use a global-memory workspace.  The last step, midsolve_traverse
+// (midengine.cc:127-158), also runs on the device and writes the reference's
+// mid_values_t records.
+#include "superscore.cuh"
+#include "runtime.h"
+#include "tables.h"
+#include "../../include/pentago_b200.h"
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+namespace pg {
+
+// combinations[n][k] for n <= 18, k <= 10 (mid/subsets.h:17-21)
+__constant__ uint32_t c_choose[19][11];
+__constant__ uint64_t c_winpat[32];
+
+PG_HD int choose_t(const uint32_t (*C)[11], int n, int k) {
+  if (n < 0 || k < 0 || k > n) return 0;
+  return int(C[n][k < n - k ? k : n - k]);
+}
+
+struct mid_grab { int ny, lo, size; };
+
+struct mid_job_t {
+  uint64_t side[2];
+  uint32_t ply;
+  int32_t spots;
+  uint8_t empty[18];
+  uint8_t pad[6];
+  int32_t sets1p_off[20], wins1_off[20], cs1ps_off[20];
+  mid_grab spaces[20];
+  uint64_t* sets1p;       // global scratch
+  uint4* wins1;           // 2 per entry: after, before
+  uint16_t* cs1ps;
+  uint4* workspace;       // global workspace, or null when it lives in shared memory
+  pg_mid_values_t* out;
+};
+
+struct set0_info {  // make_set0_info (mid/internal.h:174-259); 256 bytes
+  uint4 wins0;
+  uint16_t child_s0s[18];
+  uint16_t offset0[90];
+  uint8_t empty1[18];
+  uint8_t pad[2];
+};
+static_assert(sizeof(set0_info) == 256, "set0_info layout");
+
+// ---------------------------------------------------------------------------
+// Subset ranking (mid/subsets.h:34-105)
+// ---------------------------------------------------------------------------
+
+// The index-th k-subset of [0,n) in large-entry-major order, 5 bits per entry.
+PG_HD uint64_t unrank(const uint32_t (*C)[11], int n, int k, int index) {
+  uint64_t set = 0;
+  for (int i = k - 1; i >= 0; i--) {
+    int j = i, base = 0;
+    for (; j < n; j++) {
+      const int next = base + choose_t(C, j, i);
+      if (index < next) break;
+      base = next;
+    }
+    set |= uint64_t(j) << (5 * i);
+    index -= base;
+  }
+  return set;
+}
+
+PG_HD uint64_t set_side(const uint8_t* empty, int k, uint64_t set) {
+  uint64_t s = 0;
+  for (int i = 0; i < k; i++) s |= uint64_t(1) << empty[set >> (5 * i) & 0x1f];
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Wins of one side: super_wins split by parity (halfsuper_wins, generated by
+// pentago/base/precompute.cc:330-505; here computed from the full super).
+// ---------------------------------------------------------------------------
+
+PG_HD half4 h_wins(const uint32_t* wf, uint64_t side, int parity) {
+  return s_split(s_super_wins(wf, side), parity);
+}
+
+PG_HD bool won(const uint64_t* pats, uint64_t side) {
+  for (int i = 0; i < 32; i++)
+    if ((side & pats[i]) == pats[i]) return true;
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// The per-board CTA kernel
+// ---------------------------------------------------------------------------
+
+constexpr int kMidThreads = 256;
+constexpr int kSmemWorkspaceMax = 8400;  // bottleneck(10), in halfsupers
+
+struct level_t {
+  int n, k0, k1, spots, parity;
+  uint64_t root0, root1;
+  int nsets0, nsets1p;
+};
+
+__device__ __forceinline__ level_t make_level(const mid_job_t& J, int n) {
+  level_t L;
+  L.n = n;
+  L.k0 = n >> 1;
+  L.k1 = n - L.k0;
+  L.spots = J.spots;
+  L.parity = int((n + J.ply) & 1);
+  L.root0 = J.side[(J.spots + n) & 1];
+  L.root1 = J.side[(J.spots + n + 1) & 1];
+  L.nsets0 = choose_t(c_choose, J.spots, L.k0);
+  L.nsets1p = choose_t(c_choose, J.spots - L.k0, L.k1);
+  return L;
+}
+
+// make_set0_info (mid/internal.h:174-259)
+__device__ void build_set0(const mid_job_t& J, const level_t& L, int s0, const uint32_t* wf, set0_info& I0) {
+  const uint64_t set0 = unrank(c_choose, J.spots, L.k0, s0);
+  const uint64_t side0 = L.root0 | set_side(J.empty, L.k0, set0);
+  I0.wins0 = h_to(h_wins(wf, side0, L.parity));
+  const uint64_t free_ = 0x01ff01ff01ff01ffull & ~side0;
+  int next = 0;
+  for (int i = 0; i < J.spots; i++)
+    if (free_ >> J.empty[i] & 1) I0.empty1[next++] = uint8_t(i);
+  for (int i = 0; i < J.spots - L.k0; i++) {
+    const int j = I0.empty1[i] - i;
+    int v = choose_t(c_choose, I0.empty1[i], j + 1);
+    for (int a = 0; a < L.k0; a++) v += choose_t(c_choose, int(set0 >> (5 * a) & 0x1f), a + (a >= j) + 1);
+    I0.child_s0s[i] = uint16_t(v);
+  }
+  for (int a = 0; a < L.k1; a++)
+    for (int q = 0; q < J.spots - L.k0; q++) {
+      int offset = a ? 0 : s0;
+      for (int i = I0.empty1[q] - q; i < L.k0; i++) {
+        const int v = int(set0 >> (5 * i) & 0x1f);
+        if (v > a) offset -= choose_t(c_choose, v - a - 1, i);
+      }
+      I0.offset0[a * (J.spots - L.k0) + q] = uint16_t(offset);
+    }
+}
+
+// inner (mid/internal.h:358-408)
+__device__ __forceinline__ void inner(const mid_job_t& J, const level_t& L, const set0_info& I0, int s1p,
+                                      int aggressive, const uint4* in, uint4* out, int in_ny, int out_ny,
+                                      uint4* results) {
+  const int n = L.n, spots = L.spots, k0 = L.k0, k1 = L.k1;
+  const uint64_t set1p = J.sets1p[J.sets1p_off[n] + s1p];
+  const int turn_aggressive = aggressive ^ (n & 1);
+  uint32_t filled1p = 0;
+  int s1 = 0, s0p = 0;
+  for (int i = 0; i < k1; i++) {
+    const int q = int(set1p >> (5 * i) & 0x1f);
+    filled1p |= 1u << q;
+    s1 += choose_t(c_choose, I0.empty1[q], i + 1);
+    s0p += I0.offset0[i * (spots - k0) + q];
+  }
+  half4 us = (spots == n && !turn_aggressive) ? h_not(h_zero()) : h_zero();
+  const uint16_t* cs = J.cs1ps + J.cs1ps_off[n] + s1p * (spots - k0);
+  uint32_t unmoved = ~filled1p;
+  for (int m = 0; m < spots - n; m++) {
+    const int i = ctz32(unmoved);
+    unmoved &= unmoved - 1;
+    us = h_or(us, h_from(in[int(I0.child_s0s[i]) * in_ny + cs[i]]));
+  }
+  const uint4* w1 = J.wins1 + 2 * (J.wins1_off[n] + s1);
+  const half4 after = h_from(w1[0]), before = h_from(w1[1]);
+  const half4 wins0 = h_from(I0.wins0);
+  const half4 inplay = h_not(h_or(wins0, after));
+  const half4 mask = turn_aggressive ? h_not(after) : h_not(h_zero());
+  us = h_or(h_and(inplay, us), h_and(wins0, mask));
+  if (n <= 1) results[n + s1p] = h_to(us);
+  out[s1 * out_ny + s0p] = h_to(h_or(h_rmax(h_not(us)), before));
+}
+
+// high_board_t helpers for the traversal (high/board.cc)
+__device__ uint64_t board_of(uint64_t s0, uint64_t s1) {
+  uint64_t board = 0;
+  for (int q = 0; q < 4; q++) {
+    uint32_t quad = 0;
+    for (int i = 8; i >= 0; i--) {
+      const int j = 16 * q + i;
+      quad = 3 * quad + uint32_t(s0 >> j & 1) + 2 * uint32_t(s1 >> j & 1);
+    }
+    board |= uint64_t(quad) << (16 * q);
+  }
+  return board;
+}
+
+__device__ void rotate_sides(uint64_t* side, int q, int d) {
+  for (int s = 0; s < 2; s++) {
+    const uint32_t old = uint32_t(side[s] >> (16 * q)) & 0x1ff;
+    uint32_t quad = 0;
+    for (int i = 0; i < 9; i++)
+      if (old >> i & 1) quad |= 1u << (4 - d * (3 * (i % 3) - i / 3 - 2));
+    side[s] ^= uint64_t(old ^ quad) << (16 * q);
+  }
+}
+
+// done_and_value (high/board.cc:20-29)
+__device__ bool done_value(const uint64_t* side, uint32_t ply, int* value) {
+  const bool bw = won(c_winpat, side[0]), ww = won(c_winpat, side[1]);
+  const int turn = int(ply >> 1 & 1);
+  if (bw || ww) { *value = (bw && ww) ? 0 : (bw == !turn ? 1 : -1); return true; }
+  if (ply == 72) { *value = 0; return true; }
+  return false;
+}
+
+__device__ int hbit(const uint4& h, int i) {
+  const uint32_t w = i < 32 ? h.x : i < 64 ? h.y : i < 96 ? h.z : h.w;
+  return int(w >> (i & 31) & 1);
+}
+
+__device__ void append(pg_mid_values_t* out, uint64_t raw, int v) {
+  const int k = out->size++;
+  if (k < 163) { out->entries[k].raw = raw; out->entries[k].value = v; out->entries[k].pad = 0; }
+}
+
+// midsolve_traverse (midengine.cc:127-158), iteratively; supers[i] = (win, notlose)
+__device__ void traverse(const mid_job_t& J, const uint4* supers, pg_mid_values_t* out) {
+  out->size = 0;
+  out->pad = 0;
+  uint64_t side[2] = {J.side[0], J.side[1]};
+  const uint32_t ply = J.ply;
+  auto middle_children = [&](const uint64_t* sd, uint32_t p, const uint4* r) {
+    int best = -1;
+    for (int s = 0; s < 8; s++) {
+      const int q = s >> 1, d = (s & 1) ? -1 : 1;
+      const int idx = ((d & 3) << (2 * q)) >> 1;
+      const int v = hbit(r[0], idx) + hbit(r[1], idx) - 1;
+      uint64_t rs[2] = {sd[0], sd[1]};
+      rotate_sides(rs, q, d);
+      append(out, board_of(rs[0], rs[1]) | uint64_t((p + 1) & 1) << 63, v);
+      best = max(best, -v);
+    }
+    return best;
+  };
+  int value;
+  if (done_value(side, ply, &value)) {
+  } else if (!(ply & 1)) {
+    value = -1;
+    const uint64_t empty = 0x01ff01ff01ff01ffull ^ side[0] ^ side[1];
+    int s = 0;
+    for (int bit = 0; bit < 64; bit++) {
+      if (!(empty >> bit & 1)) continue;
+      s++;
+      uint64_t cs[2] = {side[0], side[1]};
+      cs[(ply >> 1) & 1] |= uint64_t(1) << bit;
+      const uint32_t cply = ply + 1;
+      int cv;
+      if (!done_value(cs, cply, &cv)) cv = middle_children(cs, cply, supers + 2 * s);
+      append(out, board_of(cs[0], cs[1]) | uint64_t(1) << 63, cv);
+      value = max(value, cv);
+    }
+  } else {
+    value = middle_children(side, ply, supers);
+  }
+  append(out, board_of(side[0], side[1]) | uint64_t(ply & 1) << 63, value);
+}
+
+__global__ void __launch_bounds__(kMidThreads)
+mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict__ wf, int smem_workspace) {
+  const mid_job_t& J = jobs[blockIdx.x];
+  extern __shared__ uint4 smem[];
+  set0_info* tiles = reinterpret_cast<set0_info*>(smem);  // kMidThreads entries
+  uint4* ws = smem_workspace ? smem + kMidThreads * sizeof(set0_info) / sizeof(uint4) : J.workspace;
+  __shared__ uint4 raw[2][19];
+  const int spots = J.spots;
+  const int tid = threadIdx.x, nt = blockDim.x;
+
+  // Per-level tables, the same for both passes (midengine.cc:57-76, :101-107)
+  for (int n = spots; n >= 0; n--) {
+    const int k0 = n >> 1, k1 = n - k0;
+    const int ns1p = choose_t(c_choose, spots - k0, k1);
+    for (int i = tid; i < ns1p; i += nt) J.sets1p[J.sets1p_off[n] + i] = unrank(c_choose, spots - k0, k1, i);
+    const int ns1 = choose_t(c_choose, spots, k1);
+    const int parity = int((n + J.ply) & 1);
+    const uint64_t root1 = J.side[(spots + n + 1) & 1];
+    for (int s = tid; s < ns1; s += nt) {
+      const uint64_t side1 = root1 | set_side(J.empty, k1, unrank(c_choose, spots, k1, s));
+      const super8 w = s_super_wins(wf, side1);
+      J.wins1[2 * (J.wins1_off[n] + s)] = h_to(s_split(w, parity));
+      J.wins1[2 * (J.wins1_off[n] + s) + 1] = h_to(s_split(w, !parity));
+    }
+  }
+  __syncthreads();
+  for (int n = spots; n >= 0; n--) {  // make_cs1ps (mid/internal.h:135-150)
+    const int k0 = n >> 1, k1 = n - k0;
+    const int ns1p = choose_t(c_choose, spots - k0, k1);
+    const uint64_t* sp = J.sets1p + J.sets1p_off[n];
+    for (int idx = tid; idx < ns1p * (spots - k0); idx += nt) {
+      const int s1p = idx / (spots - k0), j = idx - s1p * (spots - k0);
+      int c = s1p;
+      for (int a = 0; a < k1; a++) {
+        const int v = int(sp[s1p] >> (5 * a) & 0x1f);
+        if (j < v) c -= choose_t(c_choose, v - 1, a);
+      }
+      J.cs1ps[J.cs1ps_off[n] + idx] = uint16_t(c);
+    }
+  }
+  __syncthreads();
+
+  for (int aggressive = 0; aggressive < 2; aggressive++) {
+    for (int n = spots; n >= 0; n--) {
+      const level_t L = make_level(J, n);
+      const mid_grab gi = J.spaces[n + 1], go = J.spaces[n];
+      const uint4* in = ws + gi.lo;
+      uint4* out = ws + go.lo;
+      for (int base = 0; base < L.nsets0; base += nt) {
+        const int rows = min(nt, L.nsets0 - base);
+        if (tid < rows) build_set0(J, L, base + tid, wf, tiles[tid]);
+        __syncthreads();
+        const int items = rows * L.nsets1p;
+        for (int it = tid; it < items; it += nt) {
+          const int r = it / L.nsets1p, s1p = it - r * L.nsets1p;
+          inner(J, L, tiles[r], s1p, aggressive, in, out, gi.ny, go.ny, raw[aggressive]);
+        }
+        __syncthreads();
+      }
+    }
+  }
+
+  // Interleave (midengine.cc:119-124) and traverse
+  if (tid == 0) {
+    uint4 supers[2 * 19];
+    for (int i = 0; i < 19; i++)
+      for (int j = 0; j < 2; j++) supers[2 * i + j] = raw[j ^ (i == 0)][i];
+    traverse(J, supers, J.out);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+static uint32_t h_choose[19][11];
+
+static int hchoose(int n, int k) {
+  if (n < 0 || k < 0 || k > n) return 0;
+  long r = 1;
+  for (int i = 0; i < k; i++) r = r * (n - i) / (i + 1);
+  return int(r);
+}
+
+int bottleneck(int spots) {  // mid/internal.h:37-47
+  int worst = 0, prev = 1;
+  for (int n = 0; n <= spots; n++) {
+    int next = hchoose(spots, n + 1);
+    if (next) next *= hchoose(n + 1, (n + 1) / 2);
+    worst = std::max(worst, prev + next);
+    prev = next;
+  }
+  return worst;
+}
+
+struct board_plan {
+  mid_job_t job;
+  size_t sets1p, wins1, cs1ps, workspace;  // element counts
+};
+
+static bool decode_board(uint64_t raw, mid_job_t& J, std::string& err) {
+  // high_board_t::from_raw (high/board.h:77, board.cc:95-111)
+  const uint64_t board = raw << 1 >> 1;
+  const int middle = int(raw >> 63);
+  uint64_t s0 = 0, s1 = 0;
+  for (int q = 0; q < 4; q++) {
+    uint32_t quad = uint32_t(board >> (16 * q)) & 0xffff;
+    if (quad >= 19683) { err = "invalid board"; return false; }
+    for (int i = 0; i < 9; i++) {
+      const int s = quad % 3;
+      quad /= 3;
+      s0 |= uint64_t(s == 1) << (16 * q + i);
+      s1 |= uint64_t(s == 2) << (16 * q + i);
+    }
+  }
+  const int stones = __builtin_popcountll(s0 | s1);
+  if (middle && stones == 0) { err = "invalid board"; return false; }
+  J.side[0] = s0;
+  J.side[1] = s1;
+  J.ply = uint32_t(2 * stones - middle);
+  J.spots = 36 - stones;
+  if (J.spots > 18) { err = "midsolve needs at least 18 stones"; return false; }
+  return true;
+}
+
+static bool plan_board(uint64_t raw, board_plan& P, std::string& err) {
+  mid_job_t& J = P.job;
+  memset(&J, 0, sizeof J);
+  if (!decode_board(raw, J, err)) return false;
+  const uint64_t empty = 0x01ff01ff01ff01ffull ^ J.side[0] ^ J.side[1];
+  int next = 0;
+  for (int i = 0; i < 64; i++)
+    if (empty >> i & 1) J.empty[next++] = uint8_t(i);
+  const int spots = J.spots, ws = bottleneck(spots);
+  for (int n = 0; n <= spots; n++) {  // make_info (mid/internal.h:49-69)
+    const int k0 = n >> 1, k1 = n - k0;
+    const int s1 = hchoose(spots, k1), s0p = hchoose(spots - k1, k0), s1p = hchoose(spots - k0, k1);
+    J.sets1p_off[n + 1] = J.sets1p_off[n] + s1p;
+    J.cs1ps_off[n + 1] = J.cs1ps_off[n] + s1p * (spots - k0);
+    J.wins1_off[n + 1] = J.wins1_off[n] + s1;
+    J.spaces[n].ny = s0p;
+    J.spaces[n].lo = (n & 1) ? ws - s1 * s0p : 0;
+    J.spaces[n].size = s1 * s0p;
+  }
+  J.spaces[spots + 1] = mid_grab{0, 0, 0};
+  P.sets1p = J.sets1p_off[spots + 1];
+  P.wins1 = 2 * size_t(J.wins1_off[spots + 1]);
+  P.cs1ps = J.cs1ps_off[spots + 1];
+  P.workspace = ws;
+  return true;
+}
+
+static std::once_flag mid_consts_once;
+static int upload_consts() {
+  static int rc = 0;
+  std::call_once(mid_consts_once, [] {
+    for (int n = 0; n <= 18; n++)
+      for (int k = 0; k <= 10; k++) h_choose[n][k] = uint32_t(hchoose(n, k));
+    const tables_t& T = tables();
+    if (cudaMemcpyToSymbol(c_choose, h_choose, sizeof h_choose) != cudaSuccess ||
+        cudaMemcpyToSymbol(c_winpat, T.winpat, sizeof T.winpat) != cudaSuccess)
+      rc = PG_ERR_CUDA;
+    if (cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) != cudaSuccess)
+      rc = PG_ERR_CUDA;
+  });
+  return rc;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace pg
+
+using namespace pg;
+
+extern "C" int pg_midsolve_workspace_size(int stones) {
+  if (stones < 18 || stones > 36) return fail(PG_ERR_ARG, "stones out of range");
+  return bottleneck(36 - stones);
+}
+
+extern "C" int pg_midsolve_scratch_bytes(const uint64_t* raws, int n, int64_t* bytes) {
+  std::string err;
+  size_t total = 0;
+  for (int i = 0; i < n; i++) {
+    board_plan P;
+    if (!plan_board(raws[i], P, err)) return fail(PG_ERR_ARG, err);
+    total += align256(P.sets1p * 8) + align256(P.wins1 * 16) + align256(P.cs1ps * 2) +
+             (P.workspace > size_t(kSmemWorkspaceMax) ? align256(P.workspace * 16) : 0);
+  }
+  *bytes = int64_t(total);
+  return PG_OK;
+}
+
+// Solve a batch of boards given as raw_t (high/board.h:77).  out: device array
+// of n pg_mid_values_t.  scratch: device buffer of pg_midsolve_scratch_bytes
+// bytes, or null to let the library allocate it on the stream.
+extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* scratch,
+                                 int64_t scratch_bytes, void* stream_) {
+  if (n < 0 || (n && (!raws || !out))) return fail(PG_ERR_ARG, "bad midsolve arguments");
+  if (!n) return PG_OK;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  const dev_tables_t* T = device_tables();
+  if (!T) return PG_ERR_CUDA;
+  if (int rc = upload_consts()) return fail(rc, "midsolve constant upload failed");
+  std::string err;
+  std::vector<board_plan> plans(n);
+  size_t total = 0;
+  for (int i = 0; i < n; i++) {
+    if (!plan_board(raws[i], plans[i], err)) return fail(PG_ERR_ARG, "board " + std::to_string(i) + ": " + err);
+    const auto& P = plans[i];
+    total += align256(P.sets1p * 8) + align256(P.wins1 * 16) + align256(P.cs1ps * 2);
+    if (P.workspace > size_t(kSmemWorkspaceMax)) total += align256(P.workspace * 16);
+  }
+  char* base = (char*)scratch;
+  bool owned = false;
+  if (!base) {
+    PG_CUDA(cudaMallocAsync((void**)&base, std::max<size_t>(total, 256), stream));
+    owned = true;
+  } else if (size_t(scratch_bytes) < total) {
+    return fail(PG_ERR_CAPACITY, "midsolve scratch too small");
+  }
+  size_t off = 0;
+  std::vector<mid_job_t> small, large;
+  for (int i = 0; i < n; i++) {
+    auto& P = plans[i];
+    mid_job_t& J = P.job;
+    J.sets1p = (uint64_t*)(base + off); off += align256(P.sets1p * 8);
+    J.wins1 = (uint4*)(base + off); off += align256(P.wins1 * 16);
+    J.cs1ps = (uint16_t*)(base + off); off += align256(P.cs1ps * 2);
+    if (P.workspace > size_t(kSmemWorkspaceMax)) { J.workspace = (uint4*)(base + off); off += align256(P.workspace * 16); }
+    J.out = out + i;
+    (P.workspace > size_t(kSmemWorkspaceMax) ? large : small).push_back(J);
+  }
+  for (int pass = 0; pass < 2; pass++) {
+    auto& jobs = pass ? large : small;
+    if (jobs.empty()) continue;
+    mid_job_t* d = nullptr;
+    PG_CUDA(cudaMallocAsync(&d, sizeof(mid_job_t) * jobs.size(), stream));
+    PG_CUDA(cudaMemcpyAsync(d, jobs.data(), sizeof(mid_job_t) * jobs.size(), cudaMemcpyHostToDevice, stream));
+    const int smem_ws = pass == 0;
+    const size_t smem = kMidThreads * sizeof(set0_info) + (smem_ws ? kSmemWorkspaceMax * 16 : 0);
+    mid_board_kernel<<<unsigned(jobs.size()), kMidThreads, smem, stream>>>(d, T->win_factors, smem_ws);
+    PG_CUDA(cudaGetLastError());
+    PG_CUDA(cudaFreeAsync(d, stream));
+  }
+  if (owned) PG_CUDA(cudaFreeAsync(base, stream));
+  return PG_OK;
+}

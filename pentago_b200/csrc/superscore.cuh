@@ -353,4 +353,64 @@ PG_HD super8 s_super_wins(const uint32_t* __restrict__ table, uint64_t side) {
   return win_assemble(win_combine(e0, e1, e2, e3));
 }
 
+// ---------------------------------------------------------------------------
+// Halfsupers (pentago/mid/halfsuper.h:4-60): the half of a super with one
+// rotation parity.  h(p)(a,b,c,d) = s(2a + (b+c+d+p)%2, b, c, d), stored at
+// bit a + 2b + 8c + 32d of four 32-bit words; within a word a, b and c sit in
+// bits 0-4 and the word number is d.
+// ---------------------------------------------------------------------------
+
+struct half4 {
+  uint32_t w[4];
+};
+
+PG_HD half4 h_zero() { return half4{{0, 0, 0, 0}}; }
+PG_HD half4 h_not(const half4& a) { return half4{{~a.w[0], ~a.w[1], ~a.w[2], ~a.w[3]}}; }
+PG_HD half4 h_or(const half4& a, const half4& b) {
+  return half4{{a.w[0] | b.w[0], a.w[1] | b.w[1], a.w[2] | b.w[2], a.w[3] | b.w[3]}};
+}
+PG_HD half4 h_and(const half4& a, const half4& b) {
+  return half4{{a.w[0] & b.w[0], a.w[1] & b.w[1], a.w[2] & b.w[2], a.w[3] & b.w[3]}};
+}
+PG_HD half4 h_from(const uint4 v) { return half4{{v.x, v.y, v.z, v.w}}; }
+PG_HD uint4 h_to(const half4& h) { return make_uint4(h.w[0], h.w[1], h.w[2], h.w[3]); }
+
+// rmax on a halfsuper, which flips its parity: an OR over the parity pair
+// (axis 0), and +-1 shifts along b (bits 1-2 of each byte), c (byte within a
+// word) and d (word).
+PG_HD half4 h_rmax(const half4& x) {
+  half4 r;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    const uint32_t v = x.w[i];
+    const uint32_t t = (v | (v >> 1)) & 0x55555555u;
+    const uint32_t a = t | (t << 1);
+    const uint32_t b = ((v >> 2) & 0x3f3f3f3fu) | ((v << 6) & 0xc0c0c0c0u) |
+                       ((v << 2) & 0xfcfcfcfcu) | ((v >> 6) & 0x03030303u);
+    const uint32_t c = funnel_r(v, v, 8) | funnel_r(v, v, 24);
+    r.w[i] = a | b | c;
+  }
+  const uint32_t d0 = x.w[1] | x.w[3], d1 = x.w[0] | x.w[2];
+  r.w[0] |= d0; r.w[2] |= d0;
+  r.w[1] |= d1; r.w[3] |= d1;
+  return r;
+}
+
+// The parity-p half of a super: from nibble j = b + 4c + 16d of s keep bits
+// q and q + 2, q = (b + c + d + p) % 2.
+PG_HD half4 s_split(const super8& s, int p) {
+  half4 h = h_zero();
+#pragma unroll
+  for (int w = 0; w < 8; w++) {
+    const uint32_t M = ((w >> 1) ^ p) & 1 ? 0xf0f00f0fu : 0x0f0ff0f0u;  // nibbles with q = 1
+    uint32_t z = ((s.w[w] & ~M) | ((s.w[w] >> 1) & M)) & 0x55555555u;
+    z = (z | (z >> 1)) & 0x33333333u;
+    z = (z | (z >> 2)) & 0x0f0f0f0fu;
+    z = (z | (z >> 4)) & 0x00ff00ffu;
+    z = (z | (z >> 8)) & 0x0000ffffu;
+    h.w[w >> 1] |= z << (16 * (w & 1));
+  }
+  return h;
+}
+
 }  // namespace pg

@@ -1,0 +1,152 @@
+"""Midsolve: the host-side mirror of the reference's midsolve interface.
+
+``midsolve(raws)`` solves a batch of boards (raw_t = board | middle << 63,
+pentago/high/board.h:76) with at least 18 stones on the GPU and returns, per
+board, the list of (raw, value) pairs of mid_values_t in the order of
+midsolve_traverse (pentago/mid/midengine.cc:127-178).  ``values_device``
+keeps them on the device as an (n, 8 + 16*163)-byte buffer in the reference's
+wasm layout.
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+
+RECORD_BYTES = capi.MID_VALUES_BYTES
+
+
+def workspace_size(stones):
+    """midsolve_workspace_size (pentago/mid/midengine.cc:44-46)."""
+    return capi.check(capi.lib().pg_midsolve_workspace_size(stones))
+
+
+def scratch_bytes(raws):
+    raws = np.ascontiguousarray(raws, dtype=np.uint64)
+    out = ctypes.c_int64()
+    capi.check(capi.lib().pg_midsolve_scratch_bytes(capi.ptr(raws), len(raws), ctypes.byref(out)))
+    return out.value
+
+
+def values_device(raws, out=None, scratch=None, stream=None):
+    """Solve on the device; returns the (n, RECORD_BYTES) uint8 tensor of records."""
+    import torch
+    raws = np.ascontiguousarray(raws, dtype=np.uint64)
+    n = len(raws)
+    if out is None:
+        out = torch.zeros((n, RECORD_BYTES), dtype=torch.uint8, device="cuda")
+    sp = capi.ptr(scratch) if scratch is not None else None
+    sb = scratch.numel() * scratch.element_size() if scratch is not None else 0
+    capi.check(capi.lib().pg_midsolve_batch(capi.ptr(raws), n, out.data_ptr(), sp, sb, capi.stream_handle(stream)))
+    return out
+
+
+def decode(records):
+    """Host (n, RECORD_BYTES) uint8 array -> list of [(raw, value), ...] per board."""
+    records = np.ascontiguousarray(records, dtype=np.uint8)
+    result = []
+    for row in records:
+        size = int(row[:4].view(np.int32)[0])
+        ent = row[8:8 + 16 * 163].view(np.uint64).reshape(163, 2)
+        raws = ent[:size, 0]
+        vals = ent[:size, 1].view(np.int32).reshape(size, 2)[:, 0] if size else np.zeros(0, np.int32)
+        result.append(list(zip(raws.tolist(), vals.tolist())))
+    return result
+
+
+def midsolve(raws, stream=None):
+    """Solve boards on the GPU and return [(raw, value), ...] per board."""
+    out = values_device(raws, stream=stream)
+    return decode(out.cpu().numpy())
+
+
+def random_boards(seed, n, stones, reject_wins=True):
+    """Seeded boards with `stones` stones placed uniformly on the 6x6 board
+    (black has the extra stone when odd), rejecting boards where either side
+    already has five in a row.  Returns raw_t values with middle = 0."""
+    from .synthetic import splitmix64
+    out = []
+    ctr = 0
+    while len(out) < n:
+        r = splitmix64(seed, 36, ctr)
+        ctr += 36
+        order = np.argsort(r, kind="stable")
+        nb = (stones + 1) // 2
+        cells = np.zeros(36, np.int64)
+        cells[order[:nb]] = 1
+        cells[order[nb:stones]] = 2
+        board = board_from_cells(cells)
+        if reject_wins and (won(board, 1) or won(board, 2)):
+            continue
+        out.append(board)
+    return np.array(out, dtype=np.uint64)
+
+
+def board_from_cells(cells):
+    """6x6 table (x-major, value 0 empty / 1 black / 2 white) -> board_t
+    (from_table, pentago/base/board.cc:83-102)."""
+    q = [0] * 4
+    for qx in range(2):
+        for qy in range(2):
+            v = 0
+            for i in range(9):
+                x, y = i // 3, i % 3
+                v += 3 ** i * int(cells[(3 * qx + x) * 6 + 3 * qy + y])
+            q[2 * qx + qy] = v
+    return q[0] | q[1] << 16 | q[2] << 32 | q[3] << 48
+
+
+_WIN_PATTERNS = None
+
+
+def _patterns():
+    global _WIN_PATTERNS
+    if _WIN_PATTERNS is None:
+        pats = []
+
+        def bit(x, y, flip, rot):
+            if flip:
+                x, y = y, x
+            if rot:
+                x, y = 5 - y, x
+            return 1 << (16 * (2 * (x // 3) + y // 3) + 3 * (x % 3) + y % 3)
+        for x in range(2):
+            for y in range(2):
+                pats.append(sum(bit(2 + x + i, 2 + y + i * (-1 if x == y else 1), 0, 0) for i in range(-2, 3)))
+        for flip in (0, 1):
+            for x in range(2):
+                for y in range(6):
+                    pats.append(sum(bit(x + i, y, flip, 0) for i in range(5)))
+        for rot in (0, 1):
+            for x in range(2):
+                pats.append(sum(bit(i + x, i + x, 0, rot) for i in range(5)))
+        _WIN_PATTERNS = pats
+    return _WIN_PATTERNS
+
+
+def side_of(board, color):
+    s = 0
+    for q in range(4):
+        quad = (board >> (16 * q)) & 0xFFFF
+        for i in range(9):
+            if quad % 3 == color:
+                s |= 1 << (16 * q + i)
+            quad //= 3
+    return s
+
+
+def won(board, color):
+    s = side_of(board, color)
+    return any(s & p == p for p in _patterns())
+
+
+def smoke_check(O):
+    """One 26-stone board against the oracle (used by __graft_entry__.smoke)."""
+    raws = random_boards(0, 2, 26)
+    got = midsolve(raws)
+    for raw, g in zip(raws, got):
+        r = np.zeros(200, np.uint64)
+        v = np.zeros(200, np.int32)
+        n = O.midsolve(int(raw), ctypes.c_void_p(r.ctypes.data), ctypes.c_void_p(v.ctypes.data))
+        assert list(zip(r[:n].tolist(), v[:n].tolist())) == g, "midsolve differs from the oracle"
+    print("smoke: midsolve ok", len(got[0]), "values")
