@@ -87,6 +87,14 @@ int pg_line_info(const pg_line_t* line, pg_line_info_t* info);
  * overlap must not be passed in the same call. */
 int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream);
 
+/* Prepared lines: plan once on the host (line_details_t's work,
+ * compute.cc:55-123), run many times.  The plan keeps the lines' buffer
+ * pointers; the buffers must outlive it. */
+typedef struct pg_end_plan_s* pg_end_plan_t;
+int pg_end_plan_create(const pg_line_t* lines, int n, pg_end_plan_t* plan);
+int pg_end_plan_run(pg_end_plan_t plan, void* stream);
+int pg_end_plan_destroy(pg_end_plan_t plan);
+
 /* Synchronize `stream` and report device-side bounds violations recorded by
  * the line kernel since the last call (PG_ERR_BOUNDS), clearing them. */
 int pg_end_check(void* stream);

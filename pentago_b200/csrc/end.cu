@@ -114,126 +114,193 @@ PG_HD microline_geom microline_setup(const line_dev_t& L, const dev_tables_t& T,
   return G;
 }
 
-// Phase 1: children j = start, start + step, ... -> Q (4 uint4 per child:
-// win half then not-lost half, both already in the parent frame).
-PG_HD void microline_children(const line_dev_t& L, const microline_geom& G, uint4* q, int start, int step) {
-  for (int j = start; j < L.nchild; j += step) {
-    const int jj = j ^ int(j < L.line_moves);
-    const int blk = j >> 3;
-    const int64_t idx = L.in_off[blk] + (blk == L.input_blocks - 1 ? G.last_input_base : G.input_base) +
-                        int64_t(G.input_stride) * (jj & 7);
-    const uint64_t* node = L.input + 8 * idx;
-    const super8 cw = s_load_ldg(node), cn = s_load_ldg(node + 4);
-    const int l = ladd(G.base_l, L.csym[j]);
-    super8 qw = s_translate(s_rmax(s_not(cn)), l);
-    super8 qn = s_translate(s_rmax(s_not(cw)), l);
-    s_phi_runtime(qw, L.g);
-    s_phi_runtime(qn, L.g);
-    q[4 * j + 0] = make_uint4(qw.w[0], qw.w[1], qw.w[2], qw.w[3]);
-    q[4 * j + 1] = make_uint4(qw.w[4], qw.w[5], qw.w[6], qw.w[7]);
-    q[4 * j + 2] = make_uint4(qn.w[0], qn.w[1], qn.w[2], qn.w[3]);
-    q[4 * j + 3] = make_uint4(qn.w[4], qn.w[5], qn.w[6], qn.w[7]);
+// Per-microline context: geometry plus, for both sides, the win factor
+// entries of the three quadrants that are fixed along the line and the part
+// of super_wins they determine on their own.
+struct micro_ctx {
+  microline_geom G;
+  uint32_t fixed[2][64];
+  super8 c0[2];
+};
+
+template<int DIM>
+PG_HD void micro_prepare(const line_dev_t& L, const dev_tables_t& T, int m, micro_ctx& c) {
+  c.G = microline_setup<DIM>(L, T, m);
+  for (int side = 0; side < 2; side++) {
+    const uint64_t sd = side ? c.G.base_side1 : c.G.base_side0;
+    for (int q = 0; q < 4; q++) {
+      uint32_t* e = c.fixed[side] + 16 * q;
+      if (q == DIM) {
+        for (int w = 0; w < 16; w++) e[w] = 0;
+        continue;
+      }
+      load_entry(T.win_factors, q, int(sd >> (16 * q) & 511), e);
+    }
+    c.c0[side] = win_const<DIM>(c.fixed[side]);
   }
 }
 
-// Phase 2: parents i = start, start + step, ...
+// Child j of a microline -> Q_j (4 uint4: win half then not-lost half, both
+// already moved into the parent's frame).
+PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, int j) {
+  const int jj = j ^ int(j < L.line_moves);
+  const int blk = j >> 3;
+  const int64_t idx = L.in_off[blk] + (blk == L.input_blocks - 1 ? G.last_input_base : G.input_base) +
+                      int64_t(G.input_stride) * (jj & 7);
+  const uint64_t* node = L.input + 8 * idx;
+  const super8 cw = s_load_ldg(node), cn = s_load_ldg(node + 4);
+  const int l = ladd(G.base_l, L.csym[j]);
+  super8 qw = s_translate(s_rmax(s_not(cn)), l);
+  super8 qn = s_translate(s_rmax(s_not(cw)), l);
+  s_phi_runtime(qw, L.g);
+  s_phi_runtime(qn, L.g);
+  q[4 * j + 0] = make_uint4(qw.w[0], qw.w[1], qw.w[2], qw.w[3]);
+  q[4 * j + 1] = make_uint4(qw.w[4], qw.w[5], qw.w[6], qw.w[7]);
+  q[4 * j + 2] = make_uint4(qn.w[0], qn.w[1], qn.w[2], qn.w[3]);
+  q[4 * j + 3] = make_uint4(qn.w[4], qn.w[5], qn.w[6], qn.w[7]);
+}
+
+// Parent i of a microline (compute.cc:308-356).
 template<int DIM>
-PG_HD void microline_parents(const line_dev_t& L, const dev_tables_t& T, const microline_geom& G,
-                             const uint4* qs, int start, int step, unsigned* errors) {
+PG_HD void parent_node(const line_dev_t& L, const dev_tables_t& T, const micro_ctx& c, const uint4* qs, int i,
+                       unsigned* errors) {
   const int turn = L.turn;
-  for (int i = start; i < L.nparent; i += step) {
-    const int q = ldg(T.rmin_flat + L.rmin_off[DIM] + i);
-    const uint32_t sq0 = ldg(T.unpack + 2 * q + turn), sq1 = ldg(T.unpack + 2 * q + 1 - turn);
-    const uint64_t side0 = G.base_side0 | uint64_t(sq0) << (16 * DIM);
-    const uint64_t side1 = G.base_side1 | uint64_t(sq1) << (16 * DIM);
-    const super8 wins0 = s_super_wins(T.win_factors, side0);
-    const super8 wins1 = s_super_wins(T.win_factors, side1);
-    super8 wins = s_zero(), not_loss = s_zero();
+  const int q = ldg(T.rmin_flat + L.rmin_off[DIM] + i);
+  const uint32_t sq0 = ldg(T.unpack + 2 * q + turn), sq1 = ldg(T.unpack + 2 * q + 1 - turn);
+  uint32_t e[16];
+  load_entry(T.win_factors, DIM, int(sq0), e);
+  const super8 wins0 = win_eval<DIM>(e, c.fixed[0], c.c0[0]);
+  load_entry(T.win_factors, DIM, int(sq1), e);
+  const super8 wins1 = win_eval<DIM>(e, c.fixed[1], c.c0[1]);
+  // Every move wins immediately where super_wins(side0 | move) does: the
+  // union over the empty cells is one evaluation with the union factor.
+  {
+    const int t = ldg(T.pack + sq0) + 2 * ldg(T.pack + sq1);
+    const uint4* p = reinterpret_cast<const uint4*>(T.win_union + (size_t(DIM) * 19683 + t) * 16);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint4 v = ldg(p + k);
+      e[4 * k] = v.x; e[4 * k + 1] = v.y; e[4 * k + 2] = v.z; e[4 * k + 3] = v.w;
+    }
+  }
+  const super8 moved = win_eval<DIM>(e, c.fixed[0], c.c0[0]);
+  super8 wins = moved, not_loss;
+  if (L.slice35) {
+    // The board is full after the move: the child's value is immediate
+    // (compute.cc:329-333); rmax is OR-linear, so the union over moves works.
+    wins = s_or(wins, s_rmax(s_andnot(moved, wins1)));
+    not_loss = s_rmax(s_or(moved, s_not(wins1)));
+  } else {
+    not_loss = s_zero();
     uint32_t moves = 511u & ~(sq0 | sq1);
     while (moves) {
       const int b = ctz32(moves);
       moves &= moves - 1;
-      const super8 nw = s_super_wins(T.win_factors, side0 | uint64_t(1) << (16 * DIM + b));
-      wins = s_or(wins, nw);
-      if (L.slice35) {
-        wins = s_or(wins, s_rmax(s_andnot(nw, wins1)));
-        not_loss = s_or(not_loss, s_rmax(s_or(nw, s_not(wins1))));
-      } else {
-        const int ir = ldg(T.rmin_inv + q + (1 + turn) * pow3(b));
-        const int j = ir >> 2, r = ir & 3;
-        if (j >= L.nchild) { *errors |= 1u; continue; }
-        const uint4 a = qs[4 * j], bq = qs[4 * j + 1], c = qs[4 * j + 2], d = qs[4 * j + 3];
-        const super8 qw = {{a.x, a.y, a.z, a.w, bq.x, bq.y, bq.z, bq.w}};
-        const super8 qn = {{c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w}};
-        wins = s_or(wins, s_translate_axis<DIM>(qw, r));
-        not_loss = s_or(not_loss, s_translate_axis<DIM>(qn, r));
-      }
+      const int ir = ldg(T.rmin_inv + q + (1 + turn) * pow3(b));
+      const int j = ir >> 2, r = ir & 3;
+      if (j >= L.nchild) { *errors |= 1u; continue; }
+      const uint4 a = qs[4 * j], bq = qs[4 * j + 1], cc = qs[4 * j + 2], d = qs[4 * j + 3];
+      const super8 qw = {{a.x, a.y, a.z, a.w, bq.x, bq.y, bq.z, bq.w}};
+      const super8 qn = {{cc.x, cc.y, cc.z, cc.w, d.x, d.y, d.z, d.w}};
+      wins = s_or(wins, s_translate_axis<DIM>(qw, r));
+      not_loss = s_or(not_loss, s_translate_axis<DIM>(qn, r));
     }
-    const super8 immediate = s_or(wins0, wins1);
-    const super8 r0 = s_or(s_andnot(wins, immediate), s_andnot(wins0, wins1));
-    const super8 r1 = s_or(s_andnot(not_loss, immediate), wins0);
-    const int blk = i >> 3;
-    const int64_t oidx = L.out_off[blk] + (blk == L.length - 1 ? G.last_output_base : G.output_base) +
-                         int64_t(G.output_stride) * (i & 7);
-    uint64_t* out = L.output + 8 * oidx;
-    if (L.flags & PG_LINE_OR) {
-      s_store(out, s_or(s_load(out), r0));
-      s_store(out + 4, s_or(s_load(out + 4), r1));
-    } else {
-      s_store(out, r0);
-      s_store(out + 4, r1);
-    }
+  }
+  const super8 immediate = s_or(wins0, wins1);
+  const super8 r0 = s_or(s_andnot(wins, immediate), s_andnot(wins0, wins1));
+  const super8 r1 = s_or(s_andnot(not_loss, immediate), wins0);
+  const int blk = i >> 3;
+  const int64_t oidx = L.out_off[blk] + (blk == L.length - 1 ? c.G.last_output_base : c.G.output_base) +
+                       int64_t(c.G.output_stride) * (i & 7);
+  uint64_t* out = L.output + 8 * oidx;
+  if (L.flags & PG_LINE_OR) {
+    s_store(out, s_or(s_load(out), r0));
+    s_store(out + 4, s_or(s_load(out + 4), r1));
+  } else {
+    s_store(out, r0);
+    s_store(out + 4, r1);
   }
 }
 
+constexpr int kLineThreads = 256;
+constexpr int kMicro = 4;  // microlines per CTA
+
+// One CTA computes kMicro microlines of one line: set-up, all children of
+// those microlines into shared memory, barrier, all parents.
 template<int DIM>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(kLineThreads, 2)
 end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
   const line_dev_t& L = lines[blockIdx.y];
-  const int m = blockIdx.x;
-  if (m >= L.cross[0] * L.cross[1] * L.cross[2]) return;
+  const int nmicro = L.cross[0] * L.cross[1] * L.cross[2];
+  const int m0 = blockIdx.x * kMicro;
+  if (m0 >= nmicro) return;
+  const int M = min(kMicro, nmicro - m0);
+  __shared__ micro_ctx ctx[kMicro];
   extern __shared__ uint4 q_smem[];
-  const microline_geom G = microline_setup<DIM>(L, T, m);
+  const int tid = threadIdx.x, nt = blockDim.x;
+  if (tid < M) micro_prepare<DIM>(L, T, m0 + tid, ctx[tid]);
+  __syncthreads();
+  const int nc = L.nchild, np = L.nparent;
   if (!L.slice35) {
-    microline_children(L, G, q_smem, threadIdx.x, blockDim.x);
+    for (int x = tid; x < M * nc; x += nt) {
+      const int k = x / nc, j = x - k * nc;
+      child_node(L, ctx[k].G, q_smem + 4 * k * nc, j);
+    }
     __syncthreads();
   }
   unsigned errors = 0;
-  microline_parents<DIM>(L, T, G, q_smem, threadIdx.x, blockDim.x, &errors);
+  for (int x = tid; x < M * np; x += nt) {
+    const int k = x / np, i = x - k * np;
+    parent_node<DIM>(L, T, ctx[k], q_smem + 4 * k * nc, i, &errors);
+  }
   if (errors) atomicOr(&d_end_errors, errors);
 }
 
 // The same microline code run sequentially on the host, for CPU self-tests of
-// the kernel arithmetic.  Never used by pg_end_compute_lines.
+// the kernel arithmetic.  Never used by the device entry points.
 template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_tables_t& T) {
   std::vector<uint4> q(4 * std::max(L.nchild, 1));
   unsigned errors = 0;
+  micro_ctx c;
   for (int m = 0; m < L.cross[0] * L.cross[1] * L.cross[2]; m++) {
-    const microline_geom G = microline_setup<DIM>(L, T, m);
-    if (!L.slice35) microline_children(L, G, q.data(), 0, 1);
-    microline_parents<DIM>(L, T, G, q.data(), 0, 1, &errors);
+    micro_prepare<DIM>(L, T, m, c);
+    if (!L.slice35)
+      for (int j = 0; j < L.nchild; j++) child_node(L, c.G, q.data(), j);
+    for (int i = 0; i < L.nparent; i++) parent_node<DIM>(L, T, c, q.data(), i, &errors);
   }
   return errors;
 }
 
-static int launch_lines(std::vector<line_dev_t>& plans, int dim, cudaStream_t stream, const dev_tables_t& T) {
-  if (plans.empty()) return PG_OK;
-  int maxchild = 0;
-  for (const auto& p : plans) maxchild = std::max(maxchild, p.nchild);
-  line_dev_t* d = nullptr;
-  const size_t bytes = sizeof(line_dev_t) * plans.size();
-  PG_CUDA(cudaMallocAsync(&d, bytes, stream));
-  PG_CUDA(cudaMemcpyAsync(d, plans.data(), bytes, cudaMemcpyHostToDevice, stream));
-  const dim3 grid(512, unsigned(plans.size()));
-  const size_t smem = size_t(maxchild) * 64;
+// A set of planned lines, grouped by dimension, with their descriptors on the device.
+struct end_plan {
+  std::vector<line_dev_t> host[4];
+  line_dev_t* dev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int maxchild[4] = {0, 0, 0, 0};
+  bool owned = false;
+};
+
+template<int DIM> static int set_smem_limit() {
+  static int rc = -1;
+  if (rc < 0)
+    rc = cudaFuncSetAttribute(end_line_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
+  return rc;
+}
+
+static int launch_group(const end_plan& P, int dim, cudaStream_t stream, const dev_tables_t& T) {
+  const int n = int(P.host[dim].size());
+  if (!n) return PG_OK;
+  const dim3 grid((512 + kMicro - 1) / kMicro, unsigned(n));
+  const size_t smem = size_t(kMicro) * P.maxchild[dim] * 64;
+  int rc = 0;
   switch (dim) {
-    case 0: end_line_kernel<0><<<grid, 128, smem, stream>>>(d, T); break;
-    case 1: end_line_kernel<1><<<grid, 128, smem, stream>>>(d, T); break;
-    case 2: end_line_kernel<2><<<grid, 128, smem, stream>>>(d, T); break;
-    default: end_line_kernel<3><<<grid, 128, smem, stream>>>(d, T); break;
+    case 0: rc = set_smem_limit<0>(); end_line_kernel<0><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
+    case 1: rc = set_smem_limit<1>(); end_line_kernel<1><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
+    case 2: rc = set_smem_limit<2>(); end_line_kernel<2><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
+    default: rc = set_smem_limit<3>(); end_line_kernel<3><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
   }
+  if (rc) return fail(rc, "cudaFuncSetAttribute failed");
   PG_CUDA(cudaGetLastError());
-  PG_CUDA(cudaFreeAsync(d, stream));
   return PG_OK;
 }
 
@@ -272,29 +339,79 @@ extern "C" int pg_line_info(const pg_line_t* line, pg_line_info_t* info) {
   return PG_OK;
 }
 
-extern "C" int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream) {
-  if (n < 0 || (n && !lines)) return fail(PG_ERR_ARG, "bad line array");
-  const dev_tables_t* T = device_tables();
-  if (!T) return PG_ERR_CUDA;
-  std::vector<line_dev_t> plans[4];
+static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
   std::string err;
   for (int i = 0; i < n; i++) {
     line_dev_t d;
     if (!plan_line(to_in(lines[i]), d, err)) return fail(PG_ERR_ARG, "line " + std::to_string(i) + ": " + err);
     if (!d.output || (!d.slice35 && !d.input)) return fail(PG_ERR_ARG, "null line buffer");
-    plans[d.dim].push_back(d);
+    P.maxchild[d.dim] = std::max(P.maxchild[d.dim], d.nchild);
+    P.host[d.dim].push_back(d);
   }
+  return PG_OK;
+}
+
+extern "C" int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream_) {
+  if (n < 0 || (n && !lines)) return fail(PG_ERR_ARG, "bad line array");
+  const dev_tables_t* T = device_tables();
+  if (!T) return PG_ERR_CUDA;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  end_plan P;
+  if (int rc = plan_lines(lines, n, P)) return rc;
   for (int dim = 0; dim < 4; dim++) {
-    const int rc = launch_lines(plans[dim], dim, (cudaStream_t)stream, *T);
+    if (P.host[dim].empty()) continue;
+    const size_t bytes = sizeof(line_dev_t) * P.host[dim].size();
+    PG_CUDA(cudaMallocAsync(&P.dev[dim], bytes, stream));
+    PG_CUDA(cudaMemcpyAsync(P.dev[dim], P.host[dim].data(), bytes, cudaMemcpyHostToDevice, stream));
+    const int rc = launch_group(P, dim, stream, *T);
+    PG_CUDA(cudaFreeAsync(P.dev[dim], stream));
     if (rc) return rc;
   }
+  return PG_OK;
+}
+
+extern "C" int pg_end_plan_create(const pg_line_t* lines, int n, pg_end_plan_t* plan) {
+  if (!plan || n < 0 || (n && !lines)) return fail(PG_ERR_ARG, "bad plan arguments");
+  if (!device_tables()) return PG_ERR_CUDA;
+  auto* P = new end_plan;
+  if (int rc = plan_lines(lines, n, *P)) { delete P; return rc; }
+  for (int dim = 0; dim < 4; dim++) {
+    if (P->host[dim].empty()) continue;
+    const size_t bytes = sizeof(line_dev_t) * P->host[dim].size();
+    cudaError_t e = cudaMalloc(&P->dev[dim], bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(P->dev[dim], P->host[dim].data(), bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      for (auto* d : P->dev) if (d) cudaFree(d);
+      delete P;
+      return cuda_fail(e, "pg_end_plan_create");
+    }
+  }
+  *plan = reinterpret_cast<pg_end_plan_t>(P);
+  return PG_OK;
+}
+
+extern "C" int pg_end_plan_run(pg_end_plan_t plan, void* stream) {
+  if (!plan) return fail(PG_ERR_ARG, "null plan");
+  const dev_tables_t* T = device_tables();
+  if (!T) return PG_ERR_CUDA;
+  const end_plan& P = *reinterpret_cast<end_plan*>(plan);
+  for (int dim = 0; dim < 4; dim++)
+    if (int rc = launch_group(P, dim, (cudaStream_t)stream, *T)) return rc;
+  return PG_OK;
+}
+
+extern "C" int pg_end_plan_destroy(pg_end_plan_t plan) {
+  if (!plan) return PG_OK;
+  auto* P = reinterpret_cast<end_plan*>(plan);
+  for (auto* d : P->dev) if (d) cudaFree(d);
+  delete P;
   return PG_OK;
 }
 
 extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
   const tables_t& H = tables();
   const dev_tables_t T = {H.rmin_flat, H.rmin_inv, &H.unpack[0][0], &H.win_factors[0][0][0], H.rmin_off,
-                          &H.commute[0][0]};
+                          &H.commute[0][0], H.win_union.data(), H.pack};
   std::string err;
   unsigned errors = 0;
   for (int i = 0; i < n; i++) {

@@ -40,7 +40,10 @@ const dev_tables_t* device_tables() {
   t->win_factors = upload(&T.win_factors[0][0][0], 4 * 512 * 16);
   t->rmin_off = upload(T.rmin_off, 56);
   t->commute = upload(&T.commute[0][0], 8 * 256);
-  if (!t->rmin_flat || !t->rmin_inv || !t->unpack || !t->win_factors || !t->rmin_off || !t->commute) {
+  t->win_union = upload(T.win_union.data(), T.win_union.size());
+  t->pack = upload(T.pack, 512);
+  if (!t->rmin_flat || !t->rmin_inv || !t->unpack || !t->win_factors || !t->rmin_off || !t->commute ||
+      !t->win_union || !t->pack) {
     set_error("table upload failed");
     delete t;
     return nullptr;

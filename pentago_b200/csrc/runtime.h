@@ -14,6 +14,8 @@ struct dev_tables_t {
   const uint32_t* win_factors; // 4 x 512 x 16
   const uint16_t* rmin_off;    // 56
   const uint8_t* commute;      // 8 x 256
+  const uint32_t* win_union;   // 4 x 19683 x 16
+  const uint16_t* pack;        // 512
 };
 
 // Tables on the current device (uploaded on first use).  Returns nullptr and

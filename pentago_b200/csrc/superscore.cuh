@@ -306,33 +306,73 @@ PG_HD win_sets win_combine(const uint32_t* e0, const uint32_t* e1, const uint32_
   return s;
 }
 
-// Broadcast the set matrices into the 256-bit layout and OR them together.
-PG_HD super8 win_assemble(const win_sets& s) {
+// Set bits of win_sets, in the order of the struct.
+enum : int {
+  kP01 = 1, kP02 = 2, kP03 = 4, kP12 = 8, kP13 = 16, kP23 = 32,
+  kT012 = 64, kT013 = 128, kT023 = 256, kT123 = 512, kAllSets = 1023
+};
+// The pattern sets touching quadrant D.
+template<int D> constexpr int sets_with() {
+  return D == 0 ? kP01 | kP02 | kP03 | kT012 | kT013 | kT023
+       : D == 1 ? kP01 | kP12 | kP13 | kT012 | kT013 | kT123
+       : D == 2 ? kP02 | kP12 | kP23 | kT012 | kT023 | kT123
+                : kP03 | kP13 | kP23 | kT013 | kT023 | kT123;
+}
+
+// Only the sets in MASK, from four quadrant entries.
+template<int MASK>
+PG_HD win_sets win_combine_sets(const uint32_t* e0, const uint32_t* e1, const uint32_t* e2, const uint32_t* e3) {
+  win_sets s = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (MASK & kP01) s.p01 = fold16((e0[0] & e1[0]) | (e0[1] & e1[1]) | (e0[2] & e1[2]));
+  if (MASK & kP02) s.p02 = fold16((e0[3] & e2[0]) | (e0[4] & e2[1]) | (e0[5] & e2[2]));
+  if (MASK & kP03) s.p03 = fold16(e0[6] & e3[0]);
+  if (MASK & kP12) s.p12 = fold16(e1[3] & e2[3]);
+  if (MASK & kP13) s.p13 = fold16((e1[4] & e3[1]) | (e1[5] & e3[2]) | (e1[6] & e3[3]));
+  if (MASK & kP23) s.p23 = fold16((e2[4] & e3[4]) | (e2[5] & e3[5]) | (e2[6] & e3[6]));
+  if (MASK & kT012) s.t012 = u64of(e0[7] & e1[7] & e2[7], e0[8] & e1[8] & e2[8]);
+  if (MASK & kT013) s.t013 = u64of(e0[9] & e1[9] & e3[7], e0[10] & e1[10] & e3[8]);
+  if (MASK & kT023) s.t023 = u64of(e0[11] & e2[9] & e3[9], e0[12] & e2[10] & e3[10]);
+  if (MASK & kT123) s.t123 = u64of(e1[11] & e2[11] & e3[11], e1[12] & e2[12] & e3[12]);
+  return s;
+}
+
+// Broadcast the set matrices in MASK into the 256-bit layout and OR them together.
+template<int MASK>
+PG_HD super8 win_assemble_sets(const win_sets& s) {
   super8 r;
-  const uint32_t p01 = s.p01 | (s.p01 << 16);
-  const uint32_t nib02[4] = {s.p02 & 15, s.p02 >> 4 & 15, s.p02 >> 8 & 15, s.p02 >> 12 & 15};
-  const uint32_t p02[2] = {(nib02[0] | nib02[1] << 16) * 0x1111u, (nib02[2] | nib02[3] << 16) * 0x1111u};
-  const uint32_t p12[2] = {spread4(s.p12 & 15) | spread4(s.p12 >> 4 & 15) << 16,
-                           spread4(s.p12 >> 8 & 15) | spread4(s.p12 >> 12 & 15) << 16};
-  const uint32_t t012[2] = {(uint32_t)s.t012, (uint32_t)(s.t012 >> 32)};
+  const uint32_t p01 = (MASK & kP01) ? s.p01 | (s.p01 << 16) : 0;
+  uint32_t p02[2] = {0, 0}, p12[2] = {0, 0}, t012[2] = {0, 0};
+  if (MASK & kP02) {
+    p02[0] = ((s.p02 & 15) | (s.p02 >> 4 & 15) << 16) * 0x1111u;
+    p02[1] = ((s.p02 >> 8 & 15) | (s.p02 >> 12 & 15) << 16) * 0x1111u;
+  }
+  if (MASK & kP12) {
+    p12[0] = spread4(s.p12 & 15) | spread4(s.p12 >> 4 & 15) << 16;
+    p12[1] = spread4(s.p12 >> 8 & 15) | spread4(s.p12 >> 12 & 15) << 16;
+  }
+  if (MASK & kT012) { t012[0] = (uint32_t)s.t012; t012[1] = (uint32_t)(s.t012 >> 32); }
 #pragma unroll
   for (int r3 = 0; r3 < 4; r3++) {
-    const uint32_t p03 = (s.p03 >> (4 * r3) & 15) * 0x11111111u;
-    const uint32_t p13 = spread4(s.p13 >> (4 * r3) & 15) * 0x10001u;
-    const uint32_t t013 = (uint32_t)(s.t013 >> (16 * r3) & 0xffff) * 0x10001u;
+    const uint32_t p03 = (MASK & kP03) ? (s.p03 >> (4 * r3) & 15) * 0x11111111u : 0;
+    const uint32_t p13 = (MASK & kP13) ? spread4(s.p13 >> (4 * r3) & 15) * 0x10001u : 0;
+    const uint32_t t013 = (MASK & kT013) ? (uint32_t)(s.t013 >> (16 * r3) & 0xffff) * 0x10001u : 0;
     const uint32_t m023 = (uint32_t)(s.t023 >> (16 * r3) & 0xffff);
     const uint32_t m123 = (uint32_t)(s.t123 >> (16 * r3) & 0xffff);
 #pragma unroll
     for (int par = 0; par < 2; par++) {
       const int w = 2 * r3 + par;
-      const uint32_t p23 = ((s.p23 >> (2 * w) & 1) ? 0x0000ffffu : 0u) | ((s.p23 >> (2 * w + 1) & 1) ? 0xffff0000u : 0u);
-      const uint32_t t023 = ((m023 >> (8 * par) & 15) | (m023 >> (8 * par + 4) & 15) << 16) * 0x1111u;
-      const uint32_t t123 = spread4(m123 >> (8 * par) & 15) | spread4(m123 >> (8 * par + 4) & 15) << 16;
-      r.w[w] = p01 | p02[par] | p03 | p12[par] | p13 | p23 | t012[par] | t013 | t023 | t123;
+      uint32_t v = p01 | p02[par] | p03 | p12[par] | p13 | t012[par] | t013;
+      if (MASK & kP23)
+        v |= ((s.p23 >> (2 * w) & 1) ? 0x0000ffffu : 0u) | ((s.p23 >> (2 * w + 1) & 1) ? 0xffff0000u : 0u);
+      if (MASK & kT023) v |= ((m023 >> (8 * par) & 15) | (m023 >> (8 * par + 4) & 15) << 16) * 0x1111u;
+      if (MASK & kT123) v |= spread4(m123 >> (8 * par) & 15) | spread4(m123 >> (8 * par + 4) & 15) << 16;
+      r.w[w] = v;
     }
   }
   return r;
 }
+
+PG_HD super8 win_assemble(const win_sets& s) { return win_assemble_sets<kAllSets>(s); }
 
 PG_HD void load_entry(const uint32_t* __restrict__ table, int q, int side_q, uint32_t* e) {
   const uint4* p = reinterpret_cast<const uint4*>(table + ((q * 512 + side_q) << 4));
@@ -341,6 +381,25 @@ PG_HD void load_entry(const uint32_t* __restrict__ table, int q, int side_q, uin
     const uint4 v = ldg(p + i);
     e[4 * i] = v.x; e[4 * i + 1] = v.y; e[4 * i + 2] = v.z; e[4 * i + 3] = v.w;
   }
+}
+
+// super_wins of a side whose quadrants other than D are fixed: `fixed` holds
+// the four quadrant entries (slot D unused) and c0 the part of the answer that
+// comes from pattern sets not touching D.  `ed` is quadrant D's entry.
+template<int D>
+PG_HD super8 win_eval(const uint32_t* ed, const uint32_t* fixed, const super8& c0) {
+  const uint32_t* e0 = D == 0 ? ed : fixed;
+  const uint32_t* e1 = D == 1 ? ed : fixed + 16;
+  const uint32_t* e2 = D == 2 ? ed : fixed + 32;
+  const uint32_t* e3 = D == 3 ? ed : fixed + 48;
+  constexpr int M = sets_with<D>();
+  return s_or(win_assemble_sets<M>(win_combine_sets<M>(e0, e1, e2, e3)), c0);
+}
+// The part of super_wins that does not depend on quadrant D.
+template<int D>
+PG_HD super8 win_const(const uint32_t* fixed) {
+  constexpr int M = kAllSets & ~sets_with<D>();
+  return win_assemble_sets<M>(win_combine_sets<M>(fixed, fixed + 16, fixed + 32, fixed + 48));
 }
 
 // super_wins (pentago/base/superscore.cc:38-96) for a whole side.

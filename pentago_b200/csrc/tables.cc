@@ -219,6 +219,18 @@ void build(tables_t& T) {
   }
 }
 
+void build_union(tables_t& T) {
+  T.win_union.assign(size_t(4) * 19683 * 16, 0);
+  for (int q = 0; q < 4; q++)
+    for (int t = 0; t < 19683; t++) {
+      const int s0 = T.unpack[t][0], s1 = T.unpack[t][1];
+      uint32_t* e = &T.win_union[(size_t(q) * 19683 + t) * 16];
+      for (int m = 0; m < 9; m++)
+        if (!((s0 | s1) >> m & 1))
+          for (int w = 0; w < 16; w++) e[w] |= T.win_factors[q][s0 | 1 << m][w];
+    }
+}
+
 }  // namespace
 
 const tables_t& tables() {
@@ -227,6 +239,7 @@ const tables_t& tables() {
   std::call_once(once, [] {
     t.reset(new tables_t);
     build(*t);
+    build_union(*t);
   });
   return *t;
 }

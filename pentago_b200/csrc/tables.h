@@ -6,6 +6,7 @@
 // the SHA-1 hashes that generator embeds.
 #pragma once
 #include <cstdint>
+#include <vector>
 
 namespace pg {
 
@@ -25,6 +26,11 @@ struct tables_t {
   // Super-wins pattern factors, one 64-byte entry per (quadrant, 9-bit side),
   // laid out as described in superscore.cuh (win_factor_entry).
   uint32_t win_factors[4][512][16];
+  // OR of win_factors[q][s0 | m] over the empty cells m of a quadrant whose
+  // stones are s0 (mover) and s1, indexed by pack[s0] + 2 pack[s1]: the factor
+  // of "the mover places one more stone in q", so that the union over all
+  // such moves of super_wins costs one evaluation (4 x 19683 x 16 words).
+  std::vector<uint32_t> win_union;
 };
 
 // Built once on first use; thread safe.

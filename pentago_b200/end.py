@@ -127,6 +127,31 @@ def compute_lines(lines: Sequence[Line], stream=None):
     capi.check(capi.lib().pg_end_compute_lines(arr, len(lines), capi.stream_handle(stream)))
 
 
+class Plan:
+    """Lines planned once (the host work of line_details_t) and run many
+    times; the lines' buffers must stay alive while the plan is used."""
+
+    def __init__(self, lines: Sequence[Line]):
+        self._arr = _array(lines)
+        self._lines = list(lines)
+        self._h = ctypes.c_void_p()
+        capi.check(capi.lib().pg_end_plan_create(self._arr, len(lines), ctypes.byref(self._h)))
+
+    def run(self, stream=None):
+        capi.check(capi.lib().pg_end_plan_run(self._h, capi.stream_handle(stream)))
+
+    def close(self):
+        if self._h:
+            capi.lib().pg_end_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def check_errors(stream=None):
     """Synchronize and raise if a device-side bounds check fired."""
     capi.check(capi.lib().pg_end_check(capi.stream_handle(stream)))

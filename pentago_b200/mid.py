@@ -41,16 +41,17 @@ def values_device(raws, out=None, scratch=None, stream=None):
     return out
 
 
+_RECORD = np.dtype([("raw", "<u8"), ("value", "<i4"), ("pad", "<i4")])
+
+
 def decode(records):
     """Host (n, RECORD_BYTES) uint8 array -> list of [(raw, value), ...] per board."""
     records = np.ascontiguousarray(records, dtype=np.uint8)
     result = []
     for row in records:
-        size = int(row[:4].view(np.int32)[0])
-        ent = row[8:8 + 16 * 163].view(np.uint64).reshape(163, 2)
-        raws = ent[:size, 0]
-        vals = ent[:size, 1].view(np.int32).reshape(size, 2)[:, 0] if size else np.zeros(0, np.int32)
-        result.append(list(zip(raws.tolist(), vals.tolist())))
+        size = int(np.frombuffer(row[:4].tobytes(), np.int32)[0])
+        ent = np.frombuffer(row[8:8 + 16 * 163].tobytes(), _RECORD)[:size]
+        result.append(list(zip(ent["raw"].tolist(), ent["value"].tolist())))
     return result
 
 

@@ -118,3 +118,26 @@ def test_single_block_config1_matches_oracle(cuda, O):
     end.check_errors()
     assert np.array_equal(got, want)
     assert got.any()
+
+
+def test_prepared_plan_runs_repeatedly(cuda):
+    """pg_end_plan_create / run / destroy: the same lines run twice give the golden output."""
+    import torch
+    from pentago_b200 import end
+    from pentago_b200.synthetic import random_nodes
+    lines, want = [], []
+    for case in LINES[:5]:
+        line = end.Line(case["section"], case["dimension"], case["block_base"])
+        info = end.line_info(line)
+        line.input = to_dev(random_nodes(case["seed"], max(info.input_nodes, 1)))
+        line.output = torch.zeros((info.output_nodes, 8), dtype=torch.int64, device=cuda)
+        lines.append(line)
+        want.append(case["output_sha1"])
+    plan = end.Plan(lines)
+    for _ in range(2):
+        for l in lines:
+            l.output.zero_()
+        plan.run()
+        end.check_errors()
+        assert [sha1(to_host(l.output)) for l in lines] == want
+    plan.close()
