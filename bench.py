@@ -38,7 +38,7 @@ def block_of(i):
     return (i % 20, (7 * i + 3) % 20, (11 * i + 5) % 39, (13 * i + 1) % 39)
 
 
-def plan(blocks, rank):
+def plan_lines(blocks, rank):
     """Line descriptors (without buffers) for this rank's blocks."""
     from pentago_b200 import end
     sig = end.section_sig(SECTION)
@@ -196,7 +196,7 @@ def main():
     stream = torch.cuda.current_stream()
 
     # Buffers: pinned host copies (for the end-to-end leg) and device copies
-    lines = plan(args.blocks, rank)
+    lines = plan_lines(args.blocks, rank)
     host_in, host_out, dev_lines = [], [], []
     in_bytes = out_bytes = 0
     out_nodes = 0

@@ -99,6 +99,30 @@ int pg_end_plan_destroy(pg_end_plan_t plan);
  * the line kernel since the last call (PG_ERR_BOUNDS), clearing them. */
 int pg_end_check(void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Slice sweeps.  A slice tensor holds the sections of one slice (standardized,
+ * sorted by sig) back to back, each in the block-major node order above.
+ * ------------------------------------------------------------------------- */
+
+/* offsets[i] = node offset of section i in the slice tensor; offsets[n] = total nodes. */
+int pg_slice_layout(const uint64_t* sigs, int n, int64_t* offsets);
+
+/* Standardized sections that `root` depends on at `slice`, sorted by sig
+ * (descendent_sections, pentago/end/sections.cc:18-49).  Returns the count and
+ * writes at most cap of them. */
+int pg_descendent_sections(uint64_t root, int slice, uint64_t* sigs, int cap);
+
+/* Compute every block line of every section of a slice: parent_slice (device)
+ * receives the OR over the line dimensions (compute_lines + accumulate over a
+ * slice).  child_slice is the slice above (ignored for slice 35). */
+int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t* parent_slice,
+                       const uint64_t* child_sigs, int nc, const uint64_t* child_slice, void* stream);
+
+/* Per-section (we-win, we-win-or-tie, total) counts over distinct positions
+ * into device counts3[3 n] (count_block_wins, pentago/end/block_store.cc:330-352,
+ * summed per section as in mpi/io.cc:553-594 before the black/white swap). */
+int pg_section_counts(const uint64_t* sigs, int n, const uint64_t* slice, uint64_t* counts3, void* stream);
+
 /* Shape of a section along its four quadrants (section_t::shape,
  * pentago/base/section.cc:38-43). */
 int pg_section_shape(uint64_t section, int32_t* shape4);
@@ -149,6 +173,8 @@ int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* s
  *   op 0: out[i] = rmax(in[i])                         in: supers
  *   op 1: out[i] = super_wins(in[i])                   in: sides (1 uint64)
  *   op 2: out[i] = transform_super(sym[i], in[i])      sym = global << 8 | local
+ *   op 3: out[i] = halfsuper_wins(in[i], sym[i] & 1)   in: sides; out: halfsupers
+ *   op 4: out[i] = rmax(in[i])                         in, out: halfsupers
  * ------------------------------------------------------------------------- */
 int pg_debug_super(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n, void* stream);
 
@@ -161,6 +187,8 @@ int pg_debug_super(int op, const uint64_t* in, const uint16_t* sym, uint64_t* ou
 int pg_selftest_super_host(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n);
 int pg_selftest_end_lines_host(const pg_line_t* lines, int n);  /* host buffers */
 const void* pg_selftest_table(const char* name, int* bytes);
+/* host out[n]; supers (optional, host): 19 x (win, notlose) halfsupers per board */
+int pg_selftest_midsolve_host(const uint64_t* raws, int n, pg_mid_values_t* out, uint64_t* supers);
 
 #ifdef __cplusplus
 }

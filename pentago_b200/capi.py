@@ -88,7 +88,12 @@ SIGNATURES = {
     "pg_selftest_super_host": (_I, [_I, _P, _P, _P, _I]),
     "pg_selftest_end_lines_host": (_I, [ctypes.POINTER(pg_line_t), _I]),
     "pg_selftest_table": (ctypes.c_void_p, [ctypes.c_char_p, ctypes.POINTER(_I)]),
+    "pg_slice_layout": (_I, [_P, _I, _P]),
+    "pg_descendent_sections": (_I, [_U64, _I, _P, _I]),
+    "pg_end_sweep_slice": (_I, [_P, _I, _P, _P, _I, _P, _P]),
+    "pg_section_counts": (_I, [_P, _I, _P, _P, _P]),
     "pg_midsolve_workspace_size": (_I, [_I]),
+    "pg_selftest_midsolve_host": (_I, [_P, _I, _P, _P]),
     "pg_midsolve_scratch_bytes": (_I, [_P, _I, ctypes.POINTER(_I64)]),
     "pg_midsolve_batch": (_I, [_P, _I, _P, _P, _I64, _P]),
 }

@@ -24,6 +24,8 @@
 #include "runtime.h"
 #include "../../include/pentago_b200.h"
 #include <algorithm>
+#include <cstring>
+#include <mutex>
 #include <vector>
 
 namespace pg {
@@ -461,6 +463,12 @@ extern "C" int pg_section_standardize(uint64_t section, uint64_t* standard, int3
 namespace pg {
 PG_HD void debug_super_one(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int i, const uint32_t* wf) {
   super8 r;
+  if (op == 3 || op == 4) {  // halfsupers: 3 = halfsuper_wins(side, parity = sym), 4 = rmax
+    const half4 h = op == 3 ? s_split(s_super_wins(wf, in[i]), sym[i] & 1)
+                            : h_rmax(h_from(reinterpret_cast<const uint4*>(in)[i]));
+    reinterpret_cast<uint4*>(out)[i] = h_to(h);
+    return;
+  }
   if (op == 0) r = s_rmax(s_load(in + 4 * i));
   else if (op == 1) r = s_super_wins(wf, in[i]);
   else r = s_transform(s_load(in + 4 * i), sym[i] >> 8, sym[i] & 255);
@@ -474,17 +482,435 @@ __global__ void debug_super_kernel(int op, const uint64_t* in, const uint16_t* s
 }  // namespace pg
 
 extern "C" int pg_selftest_super_host(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n) {
-  if (op < 0 || op > 2 || n < 0) return fail(PG_ERR_ARG, "bad debug op");
+  if (op < 0 || op > 4 || n < 0) return fail(PG_ERR_ARG, "bad debug op");
   for (int i = 0; i < n; i++) debug_super_one(op, in, sym, out, i, &tables().win_factors[0][0][0]);
   return PG_OK;
 }
 
 extern "C" int pg_debug_super(int op, const uint64_t* in, const uint16_t* sym, uint64_t* out, int n, void* stream) {
-  if (op < 0 || op > 2 || n < 0) return fail(PG_ERR_ARG, "bad debug op");
+  if (op < 0 || op > 4 || n < 0) return fail(PG_ERR_ARG, "bad debug op");
   const dev_tables_t* T = device_tables();
   if (!T) return PG_ERR_CUDA;
   if (!n) return PG_OK;
   debug_super_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(op, in, sym, out, n, T->win_factors);
   PG_CUDA(cudaGetLastError());
   return PG_OK;
+}
+
+// ===========================================================================
+// Slice sweeps: every block line of every section of a slice, reading the
+// child slice and writing the parent slice in place (the work of
+// compute_lines + accumulate over a whole slice, mpi/flow.cc and
+// end/block_store.cc:173-226, on one GPU).
+//
+// A slice is one tensor: its sections (standardized, sorted by sig) back to
+// back, each section's blocks in row-major block order, each block row-major
+// in its own shape.  Block offsets are arithmetic (blocks before b in row-major
+// order hold sum_i prod_{j<i} s_j(b_j) * 8 b_i * prod_{j>i} S_j nodes, with S
+// the section shape and s_j(k) = min(8, S_j - 8k)), so no offset tables exist.
+//
+// Lines of one (section, dimension) pair form a family that shares one
+// prototype descriptor; a CTA fills in its line's block-dependent fields in
+// shared memory and then runs the same microline code as pg_end_compute_lines.
+// ===========================================================================
+
+namespace pg {
+
+struct alignas(16) family_t {
+  line_dev_t proto;           // everything but the per-line fields
+  int32_t pshape[4], cshape[4], bcount[4];
+  int64_t parent_base, child_base;
+  int32_t first_line, nlines;
+  uint8_t xsym_full[4][kMaxLine];  // reflection local of every child rmin index (cross dims)
+};
+
+PG_HD int64_t block_offset(const int32_t* S, const int* b) {
+  int64_t off = 0, before = 1;
+  for (int i = 0; i < 4; i++) {
+    int64_t after = 1;
+    for (int j = i + 1; j < 4; j++) after *= S[j];
+    off += before * 8 * b[i] * after;
+    before *= std::min(8, S[i] - 8 * b[i]);
+  }
+  return off;
+}
+
+// Fill the per-line fields of a family member (line t of the family).
+PG_HD void family_line(const family_t& F, int t, line_dev_t& L) {
+  const int dim = F.proto.dim;
+  int od[3], k = 0;
+  for (int i = 0; i < 4; i++) if (i != dim) od[k++] = i;
+  // block_base in row-major order over the other three block counts
+  int b[4];
+  b[od[2]] = t % F.bcount[od[2]];
+  b[od[1]] = t / F.bcount[od[2]] % F.bcount[od[1]];
+  b[od[0]] = t / (F.bcount[od[2]] * F.bcount[od[1]]);
+  b[dim] = 0;
+  for (int i = 0; i < 4; i++) {
+    L.block0[i] = b[i];
+    L.out_shape[i] = i == dim ? F.pshape[i] : std::min(8, F.pshape[i] - 8 * b[i]);
+  }
+  for (int j = 0; j < 3; j++) L.cross[j] = L.out_shape[od[j]];
+  for (int i = 0; i < 4; i++) L.first_child_block[i] = b[L.perm[i]];
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 8; j++) {
+      const int idx = 8 * L.first_child_block[i] + j;
+      L.xsym[i][j] = i == L.child_dim || idx >= kMaxLine ? 0 : F.xsym_full[i][idx];
+    }
+}
+
+PG_HD void family_offsets(const family_t& F, line_dev_t& L, int start, int step) {
+  int b[4];
+  for (int k = start; k < L.length + L.input_blocks; k += step) {
+    if (k < L.length) {
+      for (int i = 0; i < 4; i++) b[i] = L.block0[i];
+      b[L.dim] = k;
+      L.out_off[k] = F.parent_base + block_offset(F.pshape, b);
+    } else {
+      const int kk = k - L.length;
+      for (int i = 0; i < 4; i++) b[i] = L.first_child_block[i];
+      b[L.child_dim] = kk;
+      L.in_off[kk] = F.child_base + block_offset(F.cshape, b);
+    }
+  }
+}
+
+template<int DIM>
+__global__ void __launch_bounds__(kLineThreads, 2)
+sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_tables_t T) {
+  __shared__ __align__(16) line_dev_t L;
+  __shared__ micro_ctx ctx[kMicro];
+  __shared__ int s_fam;
+  extern __shared__ uint4 q_smem[];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int line = line0 + blockIdx.x;
+  if (tid == 0) {
+    int lo = 0, hi = nfams - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (fams[mid].first_line <= line) lo = mid; else hi = mid - 1;
+    }
+    s_fam = lo;
+  }
+  __syncthreads();
+  const family_t& F = fams[s_fam];
+  // copy the prototype (as 16-byte words) and fill in this line
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(&F.proto);
+    uint4* dst = reinterpret_cast<uint4*>(&L);
+    for (int i = tid; i < int(sizeof(line_dev_t) / 16); i += nt) dst[i] = src[i];
+  }
+  __syncthreads();
+  if (tid == 0) family_line(F, line - F.first_line, L);
+  __syncthreads();
+  family_offsets(F, L, tid, nt);
+  __syncthreads();
+  const int nmicro = L.cross[0] * L.cross[1] * L.cross[2];
+  const int m0 = blockIdx.y * kMicro;
+  if (m0 >= nmicro) return;
+  const int M = min(kMicro, nmicro - m0);
+  if (tid < M) micro_prepare<DIM>(L, T, m0 + tid, ctx[tid]);
+  __syncthreads();
+  const int nc = L.nchild, np = L.nparent;
+  if (!L.slice35) {
+    for (int x = tid; x < M * nc; x += nt) {
+      const int k = x / nc, j = x - k * nc;
+      child_node(L, ctx[k].G, q_smem + 4 * k * nc, j);
+    }
+    __syncthreads();
+  }
+  unsigned errors = 0;
+  for (int x = tid; x < M * np; x += nt) {
+    const int k = x / np, i = x - k * np;
+    parent_node<DIM>(L, T, ctx[k], q_smem + 4 * k * nc, i, &errors);
+  }
+  if (errors) atomicOr(&d_end_errors, errors);
+}
+
+static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");
+static_assert(sizeof(family_t) % 16 == 0, "family_t array keeps proto 16-byte aligned");
+
+template<int DIM> static int sweep_smem_limit() {
+  static int rc = -1;
+  if (rc < 0)
+    rc = cudaFuncSetAttribute(sweep_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
+  return rc;
+}
+
+// Per-section (we-win, we-win-or-tie, total) counts over distinct positions
+// (count_block_wins, end/block_store.cc:330-352, with popcounts_over_stabilizers,
+// base/count.cc:235-261).  One CTA per block.
+struct count_section_t {
+  int32_t shape[4], bcount[4], rmin_off[4];
+  int64_t base;        // node offset in the slice tensor
+  int64_t first_block;  // prefix over sections
+};
+
+__global__ void __launch_bounds__(256)
+count_kernel(const count_section_t* __restrict__ secs, int nsecs, const uint64_t* __restrict__ slice,
+             unsigned long long* __restrict__ counts, const uint16_t* __restrict__ rmin_flat,
+             const uint8_t* __restrict__ stab) {
+  __shared__ int s_sec;
+  __shared__ unsigned long long red[3][8];
+  const int64_t blk = blockIdx.x;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nsecs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (secs[mid].first_block <= blk) lo = mid; else hi = mid - 1;
+    }
+    s_sec = lo;
+  }
+  __syncthreads();
+  const count_section_t& S = secs[s_sec];
+  int64_t t = blk - S.first_block;
+  int b[4], bs[4];
+  for (int i = 3; i >= 0; i--) { b[i] = int(t % S.bcount[i]); t /= S.bcount[i]; }
+  for (int i = 0; i < 4; i++) bs[i] = min(8, S.shape[i] - 8 * b[i]);
+  const int nodes = bs[0] * bs[1] * bs[2] * bs[3];
+  const uint64_t* data = slice + 8 * (S.base + block_offset(S.shape, b));
+  unsigned long long c0 = 0, c1 = 0, c2 = 0;
+  for (int n = threadIdx.x; n < nodes; n += blockDim.x) {
+    int r = n, idx[4];
+    for (int i = 3; i >= 0; i--) { idx[i] = r % bs[i]; r /= bs[i]; }
+    int shift = 0;
+    for (int q = 0; q < 4; q++) shift += stab[rmin_flat[S.rmin_off[q] + 8 * b[q] + idx[q]]];
+    const uint4* p = reinterpret_cast<const uint4*>(data + 8 * int64_t(n));
+    const uint4 w0 = p[0], w1 = p[1], n0 = p[2], n1 = p[3];
+    const int pw = __popc(w0.x) + __popc(w0.y) + __popc(w0.z) + __popc(w0.w) + __popc(w1.x) + __popc(w1.y) +
+                   __popc(w1.z) + __popc(w1.w);
+    const int pn = __popc(n0.x) + __popc(n0.y) + __popc(n0.z) + __popc(n0.w) + __popc(n1.x) + __popc(n1.y) +
+                   __popc(n1.z) + __popc(n1.w);
+    c0 += pw >> shift;
+    c1 += pn >> shift;
+    c2 += 256 >> shift;
+  }
+  for (int o = 16; o; o >>= 1) {
+    c0 += __shfl_xor_sync(0xffffffffu, c0, o);
+    c1 += __shfl_xor_sync(0xffffffffu, c1, o);
+    c2 += __shfl_xor_sync(0xffffffffu, c2, o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { red[0][warp] = c0; red[1][warp] = c1; red[2][warp] = c2; }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    unsigned long long s = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); w++) s += red[threadIdx.x][w];
+    atomicAdd(counts + 3 * s_sec + threadIdx.x, s);
+  }
+}
+
+static int64_t section_nodes(const section_t& s) {
+  int sh[4];
+  s.shape(sh);
+  return int64_t(sh[0]) * sh[1] * sh[2] * sh[3];
+}
+
+// Build the family descriptor for (section, dim).
+static bool make_family(const section_t& sec, int dim, int64_t parent_base, const uint64_t* child_sigs, int nchild_secs,
+                        const int64_t* child_offsets, uint64_t* parent_slice, const uint64_t* child_slice, int flags,
+                        family_t& F, std::string& err) {
+  memset(&F, 0, sizeof F);
+  line_in_t in;
+  memset(&in, 0, sizeof in);
+  in.section = sec.sig();
+  in.dim = dim;
+  int shape[4];
+  sec.shape(shape);
+  in.length = (shape[dim] + 7) / 8;
+  in.flags = flags;
+  in.output = parent_slice;
+  in.input = child_slice;
+  line_shapes_t s;
+  if (!line_shapes(in, s, err)) return false;
+  // child section base
+  F.child_base = 0;
+  if (sec.sum() < 35) {
+    const uint64_t csig = s.child_std.sig();
+    const uint64_t* it = std::lower_bound(child_sigs, child_sigs + nchild_secs, csig);
+    if (it == child_sigs + nchild_secs || *it != csig) { err = "child section missing from the child slice"; return false; }
+    F.child_base = child_offsets[it - child_sigs];
+    s.child_std.shape(F.cshape);
+  }
+  // prototype: plan the line through block 0 and keep only family-wide fields
+  if (!plan_line(in, F.proto, err)) return false;
+  for (int i = 0; i < 4; i++) {
+    F.pshape[i] = shape[i];
+    F.bcount[i] = (shape[i] + 7) / 8;
+  }
+  F.parent_base = parent_base;
+  F.nlines = 1;
+  for (int i = 0; i < 4; i++) if (i != dim) F.nlines *= F.bcount[i];
+  // reflection locals for every child rmin index of the cross dims
+  if (s.st & 4) {
+    const auto& T = tables();
+    int perm[4];
+    quadrant_permutation(invert_global(s.st), perm);
+    for (int i = 0; i < 4; i++) {
+      if (i == s.child_dim) continue;
+      const int k = rmin_bucket(s.child_std.c[i][0], s.child_std.c[i][1]);
+      const int n = T.rmin_off[k + 1] - T.rmin_off[k];
+      for (int j = 0; j < n && j < kMaxLine; j++) {
+        const uint16_t q = T.rmin_flat[T.rmin_off[k] + j];
+        const int rq = T.pack[T.refl[T.unpack[q][0]]] + 2 * T.pack[T.refl[T.unpack[q][1]]];
+        F.xsym_full[i][j] = uint8_t((T.rmin_inv[rq] & 3) << (2 * i));
+      }
+    }
+  }
+  return true;
+}
+
+}  // namespace pg
+
+extern "C" int pg_slice_layout(const uint64_t* sigs, int n, int64_t* offsets) {
+  if (n < 0 || (n && (!sigs || !offsets))) return fail(PG_ERR_ARG, "bad slice layout arguments");
+  int64_t off = 0;
+  for (int i = 0; i < n; i++) {
+    const section_t s = section_t::from_sig(sigs[i]);
+    if (!s.valid()) return fail(PG_ERR_ARG, "invalid section");
+    if (i && sigs[i] <= sigs[i - 1]) return fail(PG_ERR_ARG, "sections must be sorted by sig");
+    offsets[i] = off;
+    off += section_nodes(s);
+  }
+  offsets[n] = off;
+  return PG_OK;
+}
+
+extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t* parent_slice,
+                                  const uint64_t* child_sigs, int nc, const uint64_t* child_slice, void* stream_) {
+  if (np < 0 || nc < 0 || (np && (!parent_sigs || !parent_slice))) return fail(PG_ERR_ARG, "bad sweep arguments");
+  const dev_tables_t* T = device_tables();
+  if (!T) return PG_ERR_CUDA;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  std::vector<int64_t> poff(np + 1), coff(nc + 1);
+  if (int rc = pg_slice_layout(parent_sigs, np, poff.data())) return rc;
+  if (int rc = pg_slice_layout(child_sigs, nc, coff.data())) return rc;
+  std::string err;
+  for (int dim = 0; dim < 4; dim++) {
+    std::vector<family_t> fams;
+    int total = 0, maxchild = 0;
+    for (int i = 0; i < np; i++) {
+      const section_t sec = section_t::from_sig(parent_sigs[i]);
+      if (sec.c[dim][0] + sec.c[dim][1] >= 9) continue;
+      int first = 0;
+      while (sec.c[first][0] + sec.c[first][1] >= 9) first++;
+      fams.emplace_back();
+      family_t& F = fams.back();
+      if (!make_family(sec, dim, poff[i], child_sigs, nc, coff.data(), parent_slice, child_slice,
+                       dim == first ? PG_LINE_STORE : PG_LINE_OR, F, err))
+        return fail(PG_ERR_ARG, "section " + std::to_string(i) + ": " + err);
+      F.first_line = total;
+      total += F.nlines;
+      maxchild = std::max(maxchild, F.proto.nchild);
+    }
+    if (fams.empty()) continue;
+    family_t* d = nullptr;
+    PG_CUDA(cudaMallocAsync(&d, sizeof(family_t) * fams.size(), stream));
+    PG_CUDA(cudaMemcpyAsync(d, fams.data(), sizeof(family_t) * fams.size(), cudaMemcpyHostToDevice, stream));
+    const size_t smem = size_t(kMicro) * maxchild * 64;
+    for (int line0 = 0; line0 < total; line0 += 1 << 30) {
+      const dim3 grid(unsigned(std::min(total - line0, 1 << 30)), (512 + kMicro - 1) / kMicro);
+      int rc = 0;
+      switch (dim) {
+#define PG_SWEEP(D) case D: \
+        rc = sweep_smem_limit<D>(); \
+        sweep_kernel<D><<<grid, kLineThreads, smem, stream>>>(d, int(fams.size()), line0, *T); break;
+        PG_SWEEP(0) PG_SWEEP(1) PG_SWEEP(2) PG_SWEEP(3)
+#undef PG_SWEEP
+      }
+      if (rc) return fail(rc, "cudaFuncSetAttribute failed");
+      PG_CUDA(cudaGetLastError());
+    }
+    PG_CUDA(cudaFreeAsync(d, stream));
+  }
+  return PG_OK;
+}
+
+namespace pg {
+static const uint8_t* stab_table() {
+  static std::mutex m;
+  static std::vector<uint8_t*> per_device;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(m);
+  if (int(per_device.size()) <= dev) per_device.resize(dev + 1, nullptr);
+  if (!per_device[dev]) {
+    const auto& T = tables();
+    std::vector<uint8_t> h(19683);
+    for (int q = 0; q < 19683; q++) {  // log_count_local_stabilizers (base/count.cc:226-236)
+      const uint16_t s0 = T.unpack[q][0], s1 = T.unpack[q][1];
+      const uint16_t r0 = T.rot[s0][0], r1 = T.rot[s1][0];
+      h[q] = (s0 == r0 && s1 == r1) ? 2 : (s0 == T.rot[r0][0] && s1 == T.rot[r1][0]) ? 1 : 0;
+    }
+    uint8_t* d = nullptr;
+    if (cudaMalloc(&d, 19683) != cudaSuccess || cudaMemcpy(d, h.data(), 19683, cudaMemcpyHostToDevice) != cudaSuccess)
+      return nullptr;
+    per_device[dev] = d;
+  }
+  return per_device[dev];
+}
+}  // namespace pg
+
+extern "C" int pg_section_counts(const uint64_t* sigs, int n, const uint64_t* slice, uint64_t* counts3, void* stream_) {
+  if (n < 0 || (n && (!sigs || !slice || !counts3))) return fail(PG_ERR_ARG, "bad count arguments");
+  const dev_tables_t* T = device_tables();
+  const uint8_t* stab = stab_table();
+  if (!T || !stab) return PG_ERR_CUDA;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  std::vector<int64_t> off(n + 1);
+  if (int rc = pg_slice_layout(sigs, n, off.data())) return rc;
+  std::vector<count_section_t> secs(n);
+  int64_t blocks = 0;
+  for (int i = 0; i < n; i++) {
+    const section_t s = section_t::from_sig(sigs[i]);
+    count_section_t& c = secs[i];
+    s.shape(c.shape);
+    int64_t nb = 1;
+    for (int q = 0; q < 4; q++) {
+      c.bcount[q] = (c.shape[q] + 7) / 8;
+      c.rmin_off[q] = tables().rmin_off[rmin_bucket(s.c[q][0], s.c[q][1])];
+      nb *= c.bcount[q];
+    }
+    c.base = off[i];
+    c.first_block = blocks;
+    blocks += nb;
+  }
+  if (!n) return PG_OK;
+  PG_CUDA(cudaMemsetAsync(counts3, 0, sizeof(uint64_t) * 3 * n, stream));
+  count_section_t* d = nullptr;
+  PG_CUDA(cudaMallocAsync(&d, sizeof(count_section_t) * n, stream));
+  PG_CUDA(cudaMemcpyAsync(d, secs.data(), sizeof(count_section_t) * n, cudaMemcpyHostToDevice, stream));
+  for (int64_t b0 = 0; b0 < blocks; b0 += int64_t(1) << 30) {
+    // grid.x covers at most 2^30 blocks per launch; the kernel reads blockIdx.x only,
+    // so sweeps with more blocks are split by section instead.
+    if (blocks > (int64_t(1) << 30)) return fail(PG_ERR_ARG, "too many blocks in one count call");
+    count_kernel<<<unsigned(blocks), 256, 0, stream>>>(d, n, slice, (unsigned long long*)counts3, T->rmin_flat, stab);
+    PG_CUDA(cudaGetLastError());
+  }
+  PG_CUDA(cudaFreeAsync(d, stream));
+  return PG_OK;
+}
+
+// descendent_sections (end/sections.cc:18-49): the standardized sections that
+// root depends on at `slice`, sorted by sig.  Returns the count (writes at
+// most cap).
+extern "C" int pg_descendent_sections(uint64_t root, int slice, uint64_t* sigs, int cap) {
+  const section_t r = section_t::from_sig(root);
+  if (!r.valid() || slice < r.sum() || slice > 35) return fail(PG_ERR_ARG, "bad root or slice");
+  std::vector<uint64_t> seen, out, stack{root};
+  while (!stack.empty()) {
+    const section_t s = section_t::from_sig(stack.back()).standardize(nullptr);
+    stack.pop_back();
+    const uint64_t sig = s.sig();
+    if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
+    seen.push_back(sig);
+    if (s.sum() == slice) out.push_back(sig);
+    if (s.sum() < slice)
+      for (int q = 0; q < 4; q++)
+        if (s.c[q][0] + s.c[q][1] < 9) stack.push_back(s.child(q).sig());
+  }
+  std::sort(out.begin(), out.end());
+  for (int i = 0; i < int(out.size()) && i < cap; i++) sigs[i] = out[i];
+  return int(out.size());
 }

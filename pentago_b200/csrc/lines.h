@@ -31,7 +31,7 @@ constexpr int kMaxLine = 424;    // nodes along a quadrant axis, rounded up
 
 // Everything a CTA needs to compute one microline of a line.  Plain data,
 // copied to the device as is.
-struct line_dev_t {
+struct alignas(16) line_dev_t {
   int32_t dim, child_dim, turn, slice35, flags;
   int32_t g, inv_l;                 // base transform = (g, inv_l + reflection locals)
   int32_t nparent, nchild, length, input_blocks, line_moves;

@@ -29,9 +29,13 @@
 
 namespace pg {
 
-// combinations[n][k] for n <= 18, k <= 10 (mid/subsets.h:17-21)
-__constant__ uint32_t c_choose[19][11];
-__constant__ uint64_t c_winpat[32];
+// Tables the midsolve code reads: combinations[n][k] for n <= 18, k <= 10
+// (mid/subsets.h:17-21), the 32 five-in-a-row masks, and the win factors.
+struct mid_tables {
+  const uint32_t (*choose)[11];
+  const uint64_t* winpat;
+  const uint32_t* wf;
+};
 
 PG_HD int choose_t(const uint32_t (*C)[11], int n, int k) {
   if (n < 0 || k < 0 || k > n) return 0;
@@ -53,6 +57,8 @@ struct mid_job_t {
   uint16_t* cs1ps;
   uint4* workspace;       // global workspace, or null when it lives in shared memory
   pg_mid_values_t* out;
+  int32_t ws_size;        // workspace entries, for bounds checks
+  int32_t pad2;
 };
 
 struct set0_info {  // make_set0_info (mid/internal.h:174-259); 256 bytes
@@ -118,7 +124,7 @@ struct level_t {
   int nsets0, nsets1p;
 };
 
-__device__ __forceinline__ level_t make_level(const mid_job_t& J, int n) {
+PG_HD level_t make_level(const mid_job_t& J, const mid_tables& MT, int n) {
   level_t L;
   L.n = n;
   L.k0 = n >> 1;
@@ -127,24 +133,24 @@ __device__ __forceinline__ level_t make_level(const mid_job_t& J, int n) {
   L.parity = int((n + J.ply) & 1);
   L.root0 = J.side[(J.spots + n) & 1];
   L.root1 = J.side[(J.spots + n + 1) & 1];
-  L.nsets0 = choose_t(c_choose, J.spots, L.k0);
-  L.nsets1p = choose_t(c_choose, J.spots - L.k0, L.k1);
+  L.nsets0 = choose_t(MT.choose, J.spots, L.k0);
+  L.nsets1p = choose_t(MT.choose, J.spots - L.k0, L.k1);
   return L;
 }
 
 // make_set0_info (mid/internal.h:174-259)
-__device__ void build_set0(const mid_job_t& J, const level_t& L, int s0, const uint32_t* wf, set0_info& I0) {
-  const uint64_t set0 = unrank(c_choose, J.spots, L.k0, s0);
+PG_HD void build_set0(const mid_job_t& J, const mid_tables& MT, const level_t& L, int s0, set0_info& I0) {
+  const uint64_t set0 = unrank(MT.choose, J.spots, L.k0, s0);
   const uint64_t side0 = L.root0 | set_side(J.empty, L.k0, set0);
-  I0.wins0 = h_to(h_wins(wf, side0, L.parity));
+  I0.wins0 = h_to(h_wins(MT.wf, side0, L.parity));
   const uint64_t free_ = 0x01ff01ff01ff01ffull & ~side0;
   int next = 0;
   for (int i = 0; i < J.spots; i++)
     if (free_ >> J.empty[i] & 1) I0.empty1[next++] = uint8_t(i);
   for (int i = 0; i < J.spots - L.k0; i++) {
     const int j = I0.empty1[i] - i;
-    int v = choose_t(c_choose, I0.empty1[i], j + 1);
-    for (int a = 0; a < L.k0; a++) v += choose_t(c_choose, int(set0 >> (5 * a) & 0x1f), a + (a >= j) + 1);
+    int v = choose_t(MT.choose, I0.empty1[i], j + 1);
+    for (int a = 0; a < L.k0; a++) v += choose_t(MT.choose, int(set0 >> (5 * a) & 0x1f), a + (a >= j) + 1);
     I0.child_s0s[i] = uint16_t(v);
   }
   for (int a = 0; a < L.k1; a++)
@@ -152,26 +158,29 @@ __device__ void build_set0(const mid_job_t& J, const level_t& L, int s0, const u
       int offset = a ? 0 : s0;
       for (int i = I0.empty1[q] - q; i < L.k0; i++) {
         const int v = int(set0 >> (5 * i) & 0x1f);
-        if (v > a) offset -= choose_t(c_choose, v - a - 1, i);
+        if (v > a) offset -= choose_t(MT.choose, v - a - 1, i);
       }
       I0.offset0[a * (J.spots - L.k0) + q] = uint16_t(offset);
     }
 }
 
 // inner (mid/internal.h:358-408)
-__device__ __forceinline__ void inner(const mid_job_t& J, const level_t& L, const set0_info& I0, int s1p,
-                                      int aggressive, const uint4* in, uint4* out, int in_ny, int out_ny,
-                                      uint4* results) {
+// Returns false (and does nothing) if an index would leave the workspace.
+PG_HD bool inner(const mid_job_t& J, const mid_tables& MT, const level_t& L, const set0_info& I0, int s1p,
+                 int aggressive, const uint4* in, uint4* out, int in_ny, int out_ny, int in_size, int out_size,
+                 uint4* results) {
   const int n = L.n, spots = L.spots, k0 = L.k0, k1 = L.k1;
   const uint64_t set1p = J.sets1p[J.sets1p_off[n] + s1p];
   const int turn_aggressive = aggressive ^ (n & 1);
+  // Index arithmetic is mod 2^16 as in the reference: offset0 holds wrapped
+  // negative offsets (mid/internal.h:372-381).
   uint32_t filled1p = 0;
-  int s1 = 0, s0p = 0;
+  uint16_t s1 = 0, s0p = 0;
   for (int i = 0; i < k1; i++) {
     const int q = int(set1p >> (5 * i) & 0x1f);
     filled1p |= 1u << q;
-    s1 += choose_t(c_choose, I0.empty1[q], i + 1);
-    s0p += I0.offset0[i * (spots - k0) + q];
+    s1 = uint16_t(s1 + choose_t(MT.choose, I0.empty1[q], i + 1));
+    s0p = uint16_t(s0p + I0.offset0[i * (spots - k0) + q]);
   }
   half4 us = (spots == n && !turn_aggressive) ? h_not(h_zero()) : h_zero();
   const uint16_t* cs = J.cs1ps + J.cs1ps_off[n] + s1p * (spots - k0);
@@ -179,7 +188,9 @@ __device__ __forceinline__ void inner(const mid_job_t& J, const level_t& L, cons
   for (int m = 0; m < spots - n; m++) {
     const int i = ctz32(unmoved);
     unmoved &= unmoved - 1;
-    us = h_or(us, h_from(in[int(I0.child_s0s[i]) * in_ny + cs[i]]));
+    const int idx = int(I0.child_s0s[i]) * in_ny + cs[i];
+    if (unsigned(idx) >= unsigned(in_size)) return false;
+    us = h_or(us, h_from(in[idx]));
   }
   const uint4* w1 = J.wins1 + 2 * (J.wins1_off[n] + s1);
   const half4 after = h_from(w1[0]), before = h_from(w1[1]);
@@ -187,12 +198,15 @@ __device__ __forceinline__ void inner(const mid_job_t& J, const level_t& L, cons
   const half4 inplay = h_not(h_or(wins0, after));
   const half4 mask = turn_aggressive ? h_not(after) : h_not(h_zero());
   us = h_or(h_and(inplay, us), h_and(wins0, mask));
+  const int o = int(s1) * out_ny + s0p;
+  if (unsigned(o) >= unsigned(out_size) || (n <= 1 && n + s1p >= 19)) return false;
   if (n <= 1) results[n + s1p] = h_to(us);
-  out[s1 * out_ny + s0p] = h_to(h_or(h_rmax(h_not(us)), before));
+  out[o] = h_to(h_or(h_rmax(h_not(us)), before));
+  return true;
 }
 
 // high_board_t helpers for the traversal (high/board.cc)
-__device__ uint64_t board_of(uint64_t s0, uint64_t s1) {
+PG_HD uint64_t board_of(uint64_t s0, uint64_t s1) {
   uint64_t board = 0;
   for (int q = 0; q < 4; q++) {
     uint32_t quad = 0;
@@ -205,7 +219,7 @@ __device__ uint64_t board_of(uint64_t s0, uint64_t s1) {
   return board;
 }
 
-__device__ void rotate_sides(uint64_t* side, int q, int d) {
+PG_HD void rotate_sides(uint64_t* side, int q, int d) {
   for (int s = 0; s < 2; s++) {
     const uint32_t old = uint32_t(side[s] >> (16 * q)) & 0x1ff;
     uint32_t quad = 0;
@@ -216,26 +230,26 @@ __device__ void rotate_sides(uint64_t* side, int q, int d) {
 }
 
 // done_and_value (high/board.cc:20-29)
-__device__ bool done_value(const uint64_t* side, uint32_t ply, int* value) {
-  const bool bw = won(c_winpat, side[0]), ww = won(c_winpat, side[1]);
+PG_HD bool done_value(const mid_tables& MT, const uint64_t* side, uint32_t ply, int* value) {
+  const bool bw = won(MT.winpat, side[0]), ww = won(MT.winpat, side[1]);
   const int turn = int(ply >> 1 & 1);
   if (bw || ww) { *value = (bw && ww) ? 0 : (bw == !turn ? 1 : -1); return true; }
   if (ply == 72) { *value = 0; return true; }
   return false;
 }
 
-__device__ int hbit(const uint4& h, int i) {
+PG_HD int hbit(const uint4& h, int i) {
   const uint32_t w = i < 32 ? h.x : i < 64 ? h.y : i < 96 ? h.z : h.w;
   return int(w >> (i & 31) & 1);
 }
 
-__device__ void append(pg_mid_values_t* out, uint64_t raw, int v) {
+PG_HD void append(pg_mid_values_t* out, uint64_t raw, int v) {
   const int k = out->size++;
   if (k < 163) { out->entries[k].raw = raw; out->entries[k].value = v; out->entries[k].pad = 0; }
 }
 
 // midsolve_traverse (midengine.cc:127-158), iteratively; supers[i] = (win, notlose)
-__device__ void traverse(const mid_job_t& J, const uint4* supers, pg_mid_values_t* out) {
+PG_HD void traverse(const mid_job_t& J, const mid_tables& MT, const uint4* supers, pg_mid_values_t* out) {
   out->size = 0;
   out->pad = 0;
   uint64_t side[2] = {J.side[0], J.side[1]};
@@ -249,12 +263,12 @@ __device__ void traverse(const mid_job_t& J, const uint4* supers, pg_mid_values_
       uint64_t rs[2] = {sd[0], sd[1]};
       rotate_sides(rs, q, d);
       append(out, board_of(rs[0], rs[1]) | uint64_t((p + 1) & 1) << 63, v);
-      best = max(best, -v);
+      best = best > -v ? best : -v;
     }
     return best;
   };
   int value;
-  if (done_value(side, ply, &value)) {
+  if (done_value(MT, side, ply, &value)) {
   } else if (!(ply & 1)) {
     value = -1;
     const uint64_t empty = 0x01ff01ff01ff01ffull ^ side[0] ^ side[1];
@@ -266,15 +280,95 @@ __device__ void traverse(const mid_job_t& J, const uint4* supers, pg_mid_values_
       cs[(ply >> 1) & 1] |= uint64_t(1) << bit;
       const uint32_t cply = ply + 1;
       int cv;
-      if (!done_value(cs, cply, &cv)) cv = middle_children(cs, cply, supers + 2 * s);
+      if (!done_value(MT, cs, cply, &cv)) cv = middle_children(cs, cply, supers + 2 * s);
       append(out, board_of(cs[0], cs[1]) | uint64_t(1) << 63, cv);
-      value = max(value, cv);
+      value = value > cv ? value : cv;
     }
   } else {
     value = middle_children(side, ply, supers);
   }
   append(out, board_of(side[0], side[1]) | uint64_t(ply & 1) << 63, value);
 }
+
+// The whole solve of one board by nt cooperating threads (tid = 0..nt-1).
+// `barrier` separates phases; run with nt = 1 and a no-op barrier it is the
+// same computation done sequentially (used by the CPU self-test).
+template<class Barrier>
+PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* tiles, uint4* ws,
+                          uint4 (*raw)[19], int* fault, int tid, int nt, Barrier barrier, uint4* dump = nullptr) {
+  const int spots = J.spots;
+  // Per-level tables, the same for both passes (midengine.cc:57-76, :101-107)
+  for (int n = spots; n >= 0; n--) {
+    const int k0 = n >> 1, k1 = n - k0;
+    const int ns1p = choose_t(MT.choose, spots - k0, k1);
+    for (int i = tid; i < ns1p; i += nt) J.sets1p[J.sets1p_off[n] + i] = unrank(MT.choose, spots - k0, k1, i);
+    const int ns1 = choose_t(MT.choose, spots, k1);
+    const int parity = int((n + J.ply) & 1);
+    const uint64_t root1 = J.side[(spots + n + 1) & 1];
+    for (int s = tid; s < ns1; s += nt) {
+      const uint64_t side1 = root1 | set_side(J.empty, k1, unrank(MT.choose, spots, k1, s));
+      const super8 w = s_super_wins(MT.wf, side1);
+      J.wins1[2 * (J.wins1_off[n] + s)] = h_to(s_split(w, parity));
+      J.wins1[2 * (J.wins1_off[n] + s) + 1] = h_to(s_split(w, !parity));
+    }
+  }
+  barrier();
+  for (int n = spots; n >= 0; n--) {  // make_cs1ps (mid/internal.h:135-150)
+    const int k0 = n >> 1, k1 = n - k0;
+    const int ns1p = choose_t(MT.choose, spots - k0, k1);
+    const uint64_t* sp = J.sets1p + J.sets1p_off[n];
+    for (int idx = tid; idx < ns1p * (spots - k0); idx += nt) {
+      const int s1p = idx / (spots - k0), j = idx - s1p * (spots - k0);
+      int c = s1p;
+      for (int a = 0; a < k1; a++) {
+        const int v = int(sp[s1p] >> (5 * a) & 0x1f);
+        if (j < v) c -= choose_t(MT.choose, v - 1, a);
+      }
+      J.cs1ps[J.cs1ps_off[n] + idx] = uint16_t(c);
+    }
+  }
+  barrier();
+
+  for (int aggressive = 0; aggressive < 2; aggressive++) {
+    for (int n = spots; n >= 0; n--) {
+      const level_t L = make_level(J, MT, n);
+      const mid_grab gi = J.spaces[n + 1], go = J.spaces[n];
+      const uint4* in = ws + gi.lo;
+      uint4* out = ws + go.lo;
+      for (int base = 0; base < L.nsets0; base += kMidThreads) {
+        const int rows = L.nsets0 - base < kMidThreads ? L.nsets0 - base : kMidThreads;
+        for (int r = tid; r < rows; r += nt) build_set0(J, MT, L, base + r, tiles[r]);
+        barrier();
+        const int items = rows * L.nsets1p;
+        for (int it = tid; it < items; it += nt) {
+          const int r = it / L.nsets1p, s1p = it - r * L.nsets1p;
+          if (!inner(J, MT, L, tiles[r], s1p, aggressive, in, out, gi.ny, go.ny, J.ws_size - gi.lo,
+                     J.ws_size - go.lo, raw[aggressive]))
+            *fault = 1;
+        }
+        barrier();
+      }
+    }
+  }
+
+  // Interleave (midengine.cc:119-124) and traverse; a failed bounds check
+  // marks the record with size -1 instead.
+  barrier();
+  if (tid == 0 && *fault) { J.out->size = -1; J.out->pad = 0; }
+  if (tid == 0 && !*fault) {
+    uint4 supers[2 * 19];
+    for (int i = 0; i < 19; i++)
+      for (int j = 0; j < 2; j++) supers[2 * i + j] = raw[j ^ (i == 0)][i];
+    if (dump)
+      for (int i = 0; i < 38; i++) dump[i] = supers[i];
+    traverse(J, MT, supers, J.out);
+  }
+}
+
+__constant__ uint32_t c_choose[19][11];
+__constant__ uint64_t c_winpat[32];
+
+struct sync_threads { __device__ void operator()() const { __syncthreads(); } };
 
 __global__ void __launch_bounds__(kMidThreads)
 mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict__ wf, int smem_workspace) {
@@ -283,68 +377,11 @@ mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict_
   set0_info* tiles = reinterpret_cast<set0_info*>(smem);  // kMidThreads entries
   uint4* ws = smem_workspace ? smem + kMidThreads * sizeof(set0_info) / sizeof(uint4) : J.workspace;
   __shared__ uint4 raw[2][19];
-  const int spots = J.spots;
-  const int tid = threadIdx.x, nt = blockDim.x;
-
-  // Per-level tables, the same for both passes (midengine.cc:57-76, :101-107)
-  for (int n = spots; n >= 0; n--) {
-    const int k0 = n >> 1, k1 = n - k0;
-    const int ns1p = choose_t(c_choose, spots - k0, k1);
-    for (int i = tid; i < ns1p; i += nt) J.sets1p[J.sets1p_off[n] + i] = unrank(c_choose, spots - k0, k1, i);
-    const int ns1 = choose_t(c_choose, spots, k1);
-    const int parity = int((n + J.ply) & 1);
-    const uint64_t root1 = J.side[(spots + n + 1) & 1];
-    for (int s = tid; s < ns1; s += nt) {
-      const uint64_t side1 = root1 | set_side(J.empty, k1, unrank(c_choose, spots, k1, s));
-      const super8 w = s_super_wins(wf, side1);
-      J.wins1[2 * (J.wins1_off[n] + s)] = h_to(s_split(w, parity));
-      J.wins1[2 * (J.wins1_off[n] + s) + 1] = h_to(s_split(w, !parity));
-    }
-  }
+  __shared__ int fault;
+  if (threadIdx.x == 0) fault = 0;
   __syncthreads();
-  for (int n = spots; n >= 0; n--) {  // make_cs1ps (mid/internal.h:135-150)
-    const int k0 = n >> 1, k1 = n - k0;
-    const int ns1p = choose_t(c_choose, spots - k0, k1);
-    const uint64_t* sp = J.sets1p + J.sets1p_off[n];
-    for (int idx = tid; idx < ns1p * (spots - k0); idx += nt) {
-      const int s1p = idx / (spots - k0), j = idx - s1p * (spots - k0);
-      int c = s1p;
-      for (int a = 0; a < k1; a++) {
-        const int v = int(sp[s1p] >> (5 * a) & 0x1f);
-        if (j < v) c -= choose_t(c_choose, v - 1, a);
-      }
-      J.cs1ps[J.cs1ps_off[n] + idx] = uint16_t(c);
-    }
-  }
-  __syncthreads();
-
-  for (int aggressive = 0; aggressive < 2; aggressive++) {
-    for (int n = spots; n >= 0; n--) {
-      const level_t L = make_level(J, n);
-      const mid_grab gi = J.spaces[n + 1], go = J.spaces[n];
-      const uint4* in = ws + gi.lo;
-      uint4* out = ws + go.lo;
-      for (int base = 0; base < L.nsets0; base += nt) {
-        const int rows = min(nt, L.nsets0 - base);
-        if (tid < rows) build_set0(J, L, base + tid, wf, tiles[tid]);
-        __syncthreads();
-        const int items = rows * L.nsets1p;
-        for (int it = tid; it < items; it += nt) {
-          const int r = it / L.nsets1p, s1p = it - r * L.nsets1p;
-          inner(J, L, tiles[r], s1p, aggressive, in, out, gi.ny, go.ny, raw[aggressive]);
-        }
-        __syncthreads();
-      }
-    }
-  }
-
-  // Interleave (midengine.cc:119-124) and traverse
-  if (tid == 0) {
-    uint4 supers[2 * 19];
-    for (int i = 0; i < 19; i++)
-      for (int j = 0; j < 2; j++) supers[2 * i + j] = raw[j ^ (i == 0)][i];
-    traverse(J, supers, J.out);
-  }
+  const mid_tables MT = {c_choose, c_winpat, wf};
+  mid_board_body(J, MT, tiles, ws, raw, &fault, threadIdx.x, blockDim.x, sync_threads());
 }
 
 // ---------------------------------------------------------------------------
@@ -425,6 +462,7 @@ static bool plan_board(uint64_t raw, board_plan& P, std::string& err) {
   P.wins1 = 2 * size_t(J.wins1_off[spots + 1]);
   P.cs1ps = J.cs1ps_off[spots + 1];
   P.workspace = ws;
+  J.ws_size = ws;
   return true;
 }
 
@@ -522,5 +560,36 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     PG_CUDA(cudaFreeAsync(d, stream));
   }
   if (owned) PG_CUDA(cudaFreeAsync(base, stream));
+  return PG_OK;
+}
+
+// The kernel's own solve, run single-threaded on the host (CPU self-test of
+// the midsolve arithmetic and indexing).  out: host array of n records.
+extern "C" int pg_selftest_midsolve_host(const uint64_t* raws, int n, pg_mid_values_t* out, uint64_t* supers) {
+  for (int k = 0; k <= 18; k++)
+    for (int j = 0; j <= 10; j++) h_choose[k][j] = uint32_t(hchoose(k, j));
+  const tables_t& T = tables();
+  const mid_tables MT = {h_choose, T.winpat, &T.win_factors[0][0][0]};
+  std::string err;
+  std::vector<set0_info> tiles(kMidThreads);
+  uint4 raw[2][19];
+  for (int i = 0; i < n; i++) {
+    board_plan P;
+    if (!plan_board(raws[i], P, err)) return fail(PG_ERR_ARG, err);
+    std::vector<uint64_t> sets1p(P.sets1p + 1);
+    std::vector<uint4> wins1(P.wins1 + 1), ws(P.workspace + 1);
+    std::vector<uint16_t> cs1ps(P.cs1ps + 1);
+    mid_job_t J = P.job;
+    J.sets1p = sets1p.data();
+    J.wins1 = wins1.data();
+    J.cs1ps = cs1ps.data();
+    J.workspace = ws.data();
+    J.out = out + i;
+    memset(raw, 0, sizeof raw);
+    int fault = 0;
+    J.ws_size = int(P.workspace);
+    mid_board_body(J, MT, tiles.data(), ws.data(), raw, &fault, 0, 1, [] {},
+                   supers ? reinterpret_cast<uint4*>(supers + 76 * size_t(i)) : nullptr);
+  }
   return PG_OK;
 }

@@ -50,9 +50,21 @@ def decode(records):
     result = []
     for row in records:
         size = int(np.frombuffer(row[:4].tobytes(), np.int32)[0])
+        if size < 0:
+            raise capi.PentagoError(capi.PG_ERR_BOUNDS, "midsolve workspace bounds check failed")
         ent = np.frombuffer(row[8:8 + 16 * 163].tobytes(), _RECORD)[:size]
         result.append(list(zip(ent["raw"].tolist(), ent["value"].tolist())))
     return result
+
+
+def selftest_host(raws, supers=False):
+    """Run the kernel's own solve single-threaded on the CPU (self-test of the
+    kernel arithmetic only).  Returns decoded values (and raw halfsupers)."""
+    raws = np.ascontiguousarray(raws, dtype=np.uint64)
+    out = np.zeros((len(raws), RECORD_BYTES), np.uint8)
+    sup = np.zeros((len(raws), 76), np.uint64) if supers else None
+    capi.check(capi.lib().pg_selftest_midsolve_host(capi.ptr(raws), len(raws), capi.ptr(out), capi.ptr(sup)))
+    return (decode(out), sup) if supers else decode(out)
 
 
 def midsolve(raws, stream=None):
