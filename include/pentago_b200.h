@@ -168,6 +168,33 @@ int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* s
                       int64_t scratch_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Static rANS coder for ternary win/tie/loss symbols, byte-identical to the
+ * reference's serialized format version 2 (arithmetic_encode / _decode /
+ * _serialize, pentago/shard/arithmetic.cc:366-495).  Many independent streams
+ * per call; all arrays are device arrays.
+ * ------------------------------------------------------------------------- */
+
+/* Bytes a stream of n symbols may need. */
+int64_t pg_rans_bound(int64_t n);
+
+/* Stream s encodes symbols[offsets[s] .. offsets[s+1]) (values 0..2) into
+ * out + out_offsets[s] (room for pg_rans_bound) and stores its size. */
+int pg_rans_encode_batch(const uint8_t* symbols, const int64_t* offsets, int nstreams, uint8_t* out,
+                         const int64_t* out_offsets, int64_t* sizes, void* stream);
+
+/* Decode stream s (in + in_offsets[s], in_sizes[s] bytes) into symbols +
+ * sym_offsets[s] (room for sym_caps[s]); status[s] = symbols decoded, or
+ * PG_ERR_FORMAT for a malformed stream, PG_ERR_CAPACITY if it does not fit. */
+int pg_rans_decode_batch(const uint8_t* in, const int64_t* in_offsets, const int64_t* in_sizes, int nstreams,
+                         uint8_t* symbols, const int64_t* sym_offsets, const int64_t* sym_caps, int64_t* status,
+                         void* stream);
+
+/* Ternary symbols of n solved nodes, 256 per node (rotation-major within the
+ * node): black wins + 2 white wins, the on-disk convention of
+ * pentago/shard/shard.cc:448-449.  turn = 1 when white is to move. */
+int pg_node_symbols(const uint64_t* nodes, int64_t n, int turn, uint8_t* symbols, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Unit-level device operations, used by tests to check the superscore
  * library against the reference (pentago/base/superscore.h, symmetry.h).
  *   op 0: out[i] = rmax(in[i])                         in: supers

@@ -1093,6 +1093,7 @@ int64_t or_rans_decode(const u8* data, int64_t size, u8* sym, int64_t cap) {  /*
   for (int l = 0; l < LANES; l++) sum += len[l];
   if (sum != (u64)(size - 60)) return -2;
   const u64 n = counts[0] + counts[1] + counts[2];
+  if (counts[0] > n || counts[1] > n || counts[2] > n || n > ~(u64)0 / 0x3fff) return -2;
   if ((int64_t)n > cap) return -1;
   const freq_t t = make_freq(counts);
   const u8 *ptr[LANES], *end[LANES];

@@ -92,6 +92,10 @@ SIGNATURES = {
     "pg_descendent_sections": (_I, [_U64, _I, _P, _I]),
     "pg_end_sweep_slice": (_I, [_P, _I, _P, _P, _I, _P, _P]),
     "pg_section_counts": (_I, [_P, _I, _P, _P, _P]),
+    "pg_rans_bound": (_I64, [_I64]),
+    "pg_rans_encode_batch": (_I, [_P, _P, _I, _P, _P, _P, _P]),
+    "pg_rans_decode_batch": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P]),
+    "pg_node_symbols": (_I, [_P, _I64, _I, _P, _P]),
     "pg_midsolve_workspace_size": (_I, [_I]),
     "pg_selftest_midsolve_host": (_I, [_P, _I, _P, _P]),
     "pg_midsolve_scratch_bytes": (_I, [_P, _I, ctypes.POINTER(_I64)]),

@@ -1,0 +1,221 @@
+// Static-table rANS over ternary win/tie/loss symbols, byte-identical to the
+// reference's format version 2 (pentago/shard/arithmetic.cc:20-23, 48-77,
+// 366-495): 8 interleaved 32-bit rANS lanes (symbol i on lane i % 8), 14-bit
+// frequency total, byte renormalization at 2^23, each lane's bytes stored in
+// decode order, header = version(4) | counts(3 x 8) | stream lengths(8 x 4).
+//
+// A stream has only 8 sequential chains, so the GPU encodes many streams at
+// once: one 8-thread group per stream (four streams per warp).  A stream's
+// lanes first count its symbols together (the frequency table comes from the
+// counts, make_freq), then each lane encodes its symbols backward into its
+// own slot of the output, and the lanes are finally packed behind the header.
+#include "runtime.h"
+#include "../../include/pentago_b200.h"
+#include <cstdint>
+
+namespace pg {
+
+constexpr uint32_t kRansTotalBits = 14;
+constexpr uint32_t kRansTotal = 1u << kRansTotalBits;
+constexpr uint32_t kRansLower = 1u << 23;
+constexpr int kLanes = 8;
+constexpr int kHeader = 4 + 24 + 32;
+
+struct rans_freq {
+  uint32_t freq[3], cum[3], xmax[3];
+};
+
+// make_freq (arithmetic.cc:48-77), in the same integer arithmetic.
+__host__ __device__ inline rans_freq make_freq(const uint64_t* counts) {
+  rans_freq t;
+  const uint64_t sum = counts[0] + counts[1] + counts[2];
+  uint32_t f[3];
+  if (sum) {
+    for (int i = 0; i < 3; i++) f[i] = uint32_t(counts[i] * kRansTotal / sum);
+    for (int i = 0; i < 3; i++) if (!f[i]) f[i] = 1;
+    const int32_t adjust = int32_t(kRansTotal) - int32_t(f[0] + f[1] + f[2]);
+    int largest = 0;
+    if (f[1] > f[largest]) largest = 1;
+    if (f[2] > f[largest]) largest = 2;
+    f[largest] = uint32_t(int32_t(f[largest]) + adjust);
+  } else {
+    f[0] = f[1] = f[2] = kRansTotal / 3;
+    f[0] += kRansTotal - 3 * (kRansTotal / 3);
+  }
+  const uint32_t xm = (kRansLower >> kRansTotalBits) << 8;
+  for (int i = 0; i < 3; i++) { t.freq[i] = f[i]; t.xmax[i] = xm * f[i]; }
+  t.cum[0] = 0;
+  t.cum[1] = f[0];
+  t.cum[2] = f[0] + f[1];
+  return t;
+}
+
+// Worst-case lane slot (the reference's per-lane buffer, arithmetic.cc:377).
+__host__ __device__ inline int64_t lane_capacity(int64_t n) { return n / kLanes * 2 + 64; }
+__host__ __device__ inline int64_t stream_bound(int64_t n) { return kHeader + kLanes * lane_capacity(n); }
+
+__device__ inline void put_u32(uint8_t* p, uint32_t v) { for (int i = 0; i < 4; i++) p[i] = uint8_t(v >> (8 * i)); }
+__device__ inline void put_u64(uint8_t* p, uint64_t v) { for (int i = 0; i < 8; i++) p[i] = uint8_t(v >> (8 * i)); }
+__device__ inline uint32_t get_u32(const uint8_t* p) {
+  return uint32_t(p[0]) | uint32_t(p[1]) << 8 | uint32_t(p[2]) << 16 | uint32_t(p[3]) << 24;
+}
+__device__ inline uint64_t get_u64(const uint8_t* p) { return uint64_t(get_u32(p)) | uint64_t(get_u32(p + 4)) << 32; }
+
+// One 8-thread group per stream.  out_offsets[s] has room for stream_bound(n_s).
+__global__ void __launch_bounds__(256)
+rans_encode_kernel(const uint8_t* __restrict__ symbols, const int64_t* __restrict__ offsets, int nstreams,
+                   uint8_t* __restrict__ out, const int64_t* __restrict__ out_offsets, int64_t* __restrict__ sizes) {
+  const int group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int lane = threadIdx.x & 7;
+  const unsigned gmask = 0xffu << (threadIdx.x & 24);
+  if (group >= nstreams) return;
+  const int64_t begin = offsets[group], n = offsets[group + 1] - begin;
+  const uint8_t* sym = symbols + begin;
+  // Count symbols
+  uint64_t c[3] = {0, 0, 0};
+  for (int64_t i = lane; i < n; i += kLanes) {
+    const uint8_t s = sym[i];
+    c[0] += s == 0;
+    c[1] += s == 1;
+    c[2] += s == 2;
+  }
+  for (int o = 4; o; o >>= 1)
+    for (int k = 0; k < 3; k++) c[k] += __shfl_xor_sync(gmask, c[k], o, 8);
+  const rans_freq t = make_freq(c);
+  // Encode this lane backward into its slot
+  uint8_t* base = out + out_offsets[group];
+  const int64_t cap = lane_capacity(n);
+  uint8_t* slot_end = base + kHeader + (lane + 1) * cap;
+  uint8_t* cur = slot_end;
+  uint32_t state = kRansLower;
+  int bad = 0;
+  for (int64_t i = (n - 1) - (((n - 1) - lane) & 7); i >= lane && i < n; i -= kLanes) {
+    int s = sym[i];
+    if (s > 2) { bad = 1; s = 0; }
+    while (state >= t.xmax[s]) { *--cur = uint8_t(state & 0xff); state >>= 8; }
+    state = ((state / t.freq[s]) << kRansTotalBits) + (state % t.freq[s]) + t.cum[s];
+  }
+  for (int j = 0; j < 4; j++) *--cur = uint8_t(state >> (8 * j));
+  const uint32_t len = uint32_t(slot_end - cur);
+  bad = __any_sync(gmask, bad);
+  // Lengths of all lanes, and this lane's destination behind the header
+  uint32_t lens[kLanes];
+  for (int l = 0; l < kLanes; l++) lens[l] = __shfl_sync(gmask, len, l, 8);
+  int64_t dst = kHeader;
+  for (int l = 0; l < lane; l++) dst += lens[l];
+  // Pack lanes in order: lane l's bytes move left, never past a lane not yet moved
+  for (int l = 0; l < kLanes; l++) {
+    __syncwarp(gmask);
+    if (l == lane) {
+      uint8_t* d = base + dst;
+      for (uint32_t k = 0; k < len; k++) d[k] = cur[k];
+    }
+  }
+  __syncwarp(gmask);
+  if (lane == 0) {
+    put_u32(base, 2);
+    for (int k = 0; k < 3; k++) put_u64(base + 4 + 8 * k, c[k]);
+    int64_t total = kHeader;
+    for (int l = 0; l < kLanes; l++) { put_u32(base + 28 + 4 * l, lens[l]); total += lens[l]; }
+    sizes[group] = bad ? PG_ERR_ARG : total;
+  }
+}
+
+// status[s]: number of symbols decoded, or PG_ERR_FORMAT / PG_ERR_CAPACITY.
+__global__ void __launch_bounds__(256)
+rans_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ in_offsets,
+                   const int64_t* __restrict__ in_sizes, int nstreams, uint8_t* __restrict__ symbols,
+                   const int64_t* __restrict__ sym_offsets, const int64_t* __restrict__ sym_caps,
+                   int64_t* __restrict__ status) {
+  const int group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+  const int lane = threadIdx.x & 7;
+  if (group >= nstreams) return;
+  const uint8_t* base = in + in_offsets[group];
+  const int64_t size = in_sizes[group];
+  // Header checks as arithmetic_deserialize / arithmetic_decode (arithmetic.cc:403-495)
+  if (size < kHeader || get_u32(base) != 2) { if (lane == 0) status[group] = PG_ERR_FORMAT; return; }
+  uint64_t c[3];
+  for (int k = 0; k < 3; k++) c[k] = get_u64(base + 4 + 8 * k);
+  const uint64_t n = c[0] + c[1] + c[2];
+  if (c[0] > n || c[1] > n || c[2] > n || n > ~uint64_t(0) / 0x3fff) {
+    if (lane == 0) status[group] = PG_ERR_FORMAT;
+    return;
+  }
+  uint64_t total = 0, start = 0;
+  uint32_t lens[kLanes];
+  for (int l = 0; l < kLanes; l++) {
+    lens[l] = get_u32(base + 28 + 4 * l);
+    if (l < lane) start += lens[l];
+    total += lens[l];
+  }
+  if (total != uint64_t(size - kHeader)) { if (lane == 0) status[group] = PG_ERR_FORMAT; return; }
+  if (int64_t(n) > sym_caps[group]) { if (lane == 0) status[group] = PG_ERR_CAPACITY; return; }
+  const rans_freq t = make_freq(c);
+  const uint8_t* p = base + kHeader + start;
+  const uint8_t* end = p + lens[lane];
+  uint32_t state = 0;
+  for (int j = 0; j < 4 && p < end; j++) state = (state << 8) | *p++;
+  uint8_t* out = symbols + sym_offsets[group];
+  for (uint64_t i = lane; i < n; i += kLanes) {
+    const uint32_t slot = state & (kRansTotal - 1);
+    const int s = slot < t.cum[1] ? 0 : slot < t.cum[2] ? 1 : 2;
+    state = t.freq[s] * (state >> kRansTotalBits) + slot - t.cum[s];
+    while (state < kRansLower && p < end) state = (state << 8) | *p++;
+    out[i] = uint8_t(s);
+  }
+  if (lane == 0) status[group] = int64_t(n);
+}
+
+// Ternary symbols of solved nodes in the on-disk convention
+// (shard/shard.cc:448-449 after end/check.cc:154-156, 197-200): for rotation r
+// of node k, symbol = black wins + 2 white wins.  Nodes are [we-win,
+// we-win-or-tie] for the player to move; `turn` = 1 when white moves.
+__global__ void node_symbols_kernel(const uint64_t* __restrict__ nodes, int64_t n, int turn,
+                                    uint8_t* __restrict__ symbols) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;  // one thread per 64 symbols
+  if (i >= n * 4) return;
+  const int64_t k = i >> 2;
+  const int w = int(i & 3);
+  const uint64_t win = nodes[8 * k + w], notlost = nodes[8 * k + 4 + w];
+  const uint64_t black = turn ? ~notlost : win, white = turn ? win : ~notlost;
+  uint8_t* out = symbols + 64 * i;
+  for (int b = 0; b < 64; b++) out[b] = uint8_t((black >> b & 1) + 2 * (white >> b & 1));
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+extern "C" int64_t pg_rans_bound(int64_t n) { return n < 0 ? PG_ERR_ARG : stream_bound(n); }
+
+extern "C" int pg_rans_encode_batch(const uint8_t* symbols, const int64_t* offsets, int nstreams, uint8_t* out,
+                                    const int64_t* out_offsets, int64_t* sizes, void* stream) {
+  if (nstreams < 0) return fail(PG_ERR_ARG, "bad stream count");
+  if (!nstreams) return PG_OK;
+  const int threads = 256, groups_per_block = threads / kLanes;
+  rans_encode_kernel<<<(nstreams + groups_per_block - 1) / groups_per_block, threads, 0, (cudaStream_t)stream>>>(
+      symbols, offsets, nstreams, out, out_offsets, sizes);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}
+
+extern "C" int pg_rans_decode_batch(const uint8_t* in, const int64_t* in_offsets, const int64_t* in_sizes,
+                                    int nstreams, uint8_t* symbols, const int64_t* sym_offsets,
+                                    const int64_t* sym_caps, int64_t* status, void* stream) {
+  if (nstreams < 0) return fail(PG_ERR_ARG, "bad stream count");
+  if (!nstreams) return PG_OK;
+  const int threads = 256, groups_per_block = threads / kLanes;
+  rans_decode_kernel<<<(nstreams + groups_per_block - 1) / groups_per_block, threads, 0, (cudaStream_t)stream>>>(
+      in, in_offsets, in_sizes, nstreams, symbols, sym_offsets, sym_caps, status);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}
+
+extern "C" int pg_node_symbols(const uint64_t* nodes, int64_t n, int turn, uint8_t* symbols, void* stream) {
+  if (n < 0) return fail(PG_ERR_ARG, "bad node count");
+  if (!n) return PG_OK;
+  const int64_t threads = 4 * n;
+  node_symbols_kernel<<<unsigned((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(nodes, n, turn & 1, symbols);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}
