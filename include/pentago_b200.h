@@ -168,6 +168,21 @@ int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* s
                       int64_t scratch_bytes, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Midsolve server: continuous batching on a persistent kernel (one worker CTA
+ * per SM).  Requests are admitted while others run, as long as the request
+ * ring has a free entry and the device scratch budget has room for the
+ * board's tables and workspace; otherwise submit returns PG_ERR_CAPACITY and
+ * the caller polls and retries.  Workers leave after ~2 s without work and
+ * are relaunched by the next submit.
+ * ------------------------------------------------------------------------- */
+
+typedef struct pg_server_s* pg_server_t;
+int pg_serve_open(int64_t budget_bytes, pg_server_t* server);
+int64_t pg_serve_submit(pg_server_t server, uint64_t raw);          /* ticket >= 0 */
+int pg_serve_poll(pg_server_t server, int64_t ticket, pg_mid_values_t* result); /* 1 done, 0 pending */
+int pg_serve_close(pg_server_t server);
+
+/* ---------------------------------------------------------------------------
  * Static rANS coder for ternary win/tie/loss symbols, byte-identical to the
  * reference's serialized format version 2 (arithmetic_encode / _decode /
  * _serialize, pentago/shard/arithmetic.cc:366-495).  Many independent streams

@@ -18,357 +18,13 @@
 // use a global-memory workspace.  The last step, midsolve_traverse
 // (midengine.cc:127-158), also runs on the device and writes the reference's
 // mid_values_t records.
-#include "superscore.cuh"
+#include "mid_body.cuh"
 #include "runtime.h"
-#include "tables.h"
-#include "../../include/pentago_b200.h"
 #include <algorithm>
-#include <cstring>
 #include <mutex>
 #include <vector>
 
 namespace pg {
-
-// Tables the midsolve code reads: combinations[n][k] for n <= 18, k <= 10
-// (mid/subsets.h:17-21), the 32 five-in-a-row masks, and the win factors.
-struct mid_tables {
-  const uint32_t (*choose)[11];
-  const uint64_t* winpat;
-  const uint32_t* wf;
-};
-
-PG_HD int choose_t(const uint32_t (*C)[11], int n, int k) {
-  if (n < 0 || k < 0 || k > n) return 0;
-  return int(C[n][k < n - k ? k : n - k]);
-}
-
-struct mid_grab { int ny, lo, size; };
-
-struct mid_job_t {
-  uint64_t side[2];
-  uint32_t ply;
-  int32_t spots;
-  uint8_t empty[18];
-  uint8_t pad[6];
-  int32_t sets1p_off[20], wins1_off[20], cs1ps_off[20];
-  mid_grab spaces[20];
-  uint64_t* sets1p;       // global scratch
-  uint4* wins1;           // 2 per entry: after, before
-  uint16_t* cs1ps;
-  uint4* workspace;       // global workspace, or null when it lives in shared memory
-  pg_mid_values_t* out;
-  int32_t ws_size;        // workspace entries, for bounds checks
-  int32_t pad2;
-};
-
-struct set0_info {  // make_set0_info (mid/internal.h:174-259); 256 bytes
-  uint4 wins0;
-  uint16_t child_s0s[18];
-  uint16_t offset0[90];
-  uint8_t empty1[18];
-  uint8_t pad[2];
-};
-static_assert(sizeof(set0_info) == 256, "set0_info layout");
-
-// ---------------------------------------------------------------------------
-// Subset ranking (mid/subsets.h:34-105)
-// ---------------------------------------------------------------------------
-
-// The index-th k-subset of [0,n) in large-entry-major order, 5 bits per entry.
-PG_HD uint64_t unrank(const uint32_t (*C)[11], int n, int k, int index) {
-  uint64_t set = 0;
-  for (int i = k - 1; i >= 0; i--) {
-    int j = i, base = 0;
-    for (; j < n; j++) {
-      const int next = base + choose_t(C, j, i);
-      if (index < next) break;
-      base = next;
-    }
-    set |= uint64_t(j) << (5 * i);
-    index -= base;
-  }
-  return set;
-}
-
-PG_HD uint64_t set_side(const uint8_t* empty, int k, uint64_t set) {
-  uint64_t s = 0;
-  for (int i = 0; i < k; i++) s |= uint64_t(1) << empty[set >> (5 * i) & 0x1f];
-  return s;
-}
-
-// ---------------------------------------------------------------------------
-// Wins of one side: super_wins split by parity (halfsuper_wins, generated by
-// pentago/base/precompute.cc:330-505; here computed from the full super).
-// ---------------------------------------------------------------------------
-
-PG_HD half4 h_wins(const uint32_t* wf, uint64_t side, int parity) {
-  return s_split(s_super_wins(wf, side), parity);
-}
-
-PG_HD bool won(const uint64_t* pats, uint64_t side) {
-  for (int i = 0; i < 32; i++)
-    if ((side & pats[i]) == pats[i]) return true;
-  return false;
-}
-
-// ---------------------------------------------------------------------------
-// The per-board CTA kernel
-// ---------------------------------------------------------------------------
-
-constexpr int kMidThreads = 256;
-constexpr int kSmemWorkspaceMax = 8400;  // bottleneck(10), in halfsupers
-
-struct level_t {
-  int n, k0, k1, spots, parity;
-  uint64_t root0, root1;
-  int nsets0, nsets1p;
-};
-
-PG_HD level_t make_level(const mid_job_t& J, const mid_tables& MT, int n) {
-  level_t L;
-  L.n = n;
-  L.k0 = n >> 1;
-  L.k1 = n - L.k0;
-  L.spots = J.spots;
-  L.parity = int((n + J.ply) & 1);
-  L.root0 = J.side[(J.spots + n) & 1];
-  L.root1 = J.side[(J.spots + n + 1) & 1];
-  L.nsets0 = choose_t(MT.choose, J.spots, L.k0);
-  L.nsets1p = choose_t(MT.choose, J.spots - L.k0, L.k1);
-  return L;
-}
-
-// make_set0_info (mid/internal.h:174-259)
-PG_HD void build_set0(const mid_job_t& J, const mid_tables& MT, const level_t& L, int s0, set0_info& I0) {
-  const uint64_t set0 = unrank(MT.choose, J.spots, L.k0, s0);
-  const uint64_t side0 = L.root0 | set_side(J.empty, L.k0, set0);
-  I0.wins0 = h_to(h_wins(MT.wf, side0, L.parity));
-  const uint64_t free_ = 0x01ff01ff01ff01ffull & ~side0;
-  int next = 0;
-  for (int i = 0; i < J.spots; i++)
-    if (free_ >> J.empty[i] & 1) I0.empty1[next++] = uint8_t(i);
-  for (int i = 0; i < J.spots - L.k0; i++) {
-    const int j = I0.empty1[i] - i;
-    int v = choose_t(MT.choose, I0.empty1[i], j + 1);
-    for (int a = 0; a < L.k0; a++) v += choose_t(MT.choose, int(set0 >> (5 * a) & 0x1f), a + (a >= j) + 1);
-    I0.child_s0s[i] = uint16_t(v);
-  }
-  for (int a = 0; a < L.k1; a++)
-    for (int q = 0; q < J.spots - L.k0; q++) {
-      int offset = a ? 0 : s0;
-      for (int i = I0.empty1[q] - q; i < L.k0; i++) {
-        const int v = int(set0 >> (5 * i) & 0x1f);
-        if (v > a) offset -= choose_t(MT.choose, v - a - 1, i);
-      }
-      I0.offset0[a * (J.spots - L.k0) + q] = uint16_t(offset);
-    }
-}
-
-// inner (mid/internal.h:358-408)
-// Returns false (and does nothing) if an index would leave the workspace.
-PG_HD bool inner(const mid_job_t& J, const mid_tables& MT, const level_t& L, const set0_info& I0, int s1p,
-                 int aggressive, const uint4* in, uint4* out, int in_ny, int out_ny, int in_size, int out_size,
-                 uint4* results) {
-  const int n = L.n, spots = L.spots, k0 = L.k0, k1 = L.k1;
-  const uint64_t set1p = J.sets1p[J.sets1p_off[n] + s1p];
-  const int turn_aggressive = aggressive ^ (n & 1);
-  // Index arithmetic is mod 2^16 as in the reference: offset0 holds wrapped
-  // negative offsets (mid/internal.h:372-381).
-  uint32_t filled1p = 0;
-  uint16_t s1 = 0, s0p = 0;
-  for (int i = 0; i < k1; i++) {
-    const int q = int(set1p >> (5 * i) & 0x1f);
-    filled1p |= 1u << q;
-    s1 = uint16_t(s1 + choose_t(MT.choose, I0.empty1[q], i + 1));
-    s0p = uint16_t(s0p + I0.offset0[i * (spots - k0) + q]);
-  }
-  half4 us = (spots == n && !turn_aggressive) ? h_not(h_zero()) : h_zero();
-  const uint16_t* cs = J.cs1ps + J.cs1ps_off[n] + s1p * (spots - k0);
-  uint32_t unmoved = ~filled1p;
-  for (int m = 0; m < spots - n; m++) {
-    const int i = ctz32(unmoved);
-    unmoved &= unmoved - 1;
-    const int idx = int(I0.child_s0s[i]) * in_ny + cs[i];
-    if (unsigned(idx) >= unsigned(in_size)) return false;
-    us = h_or(us, h_from(in[idx]));
-  }
-  const uint4* w1 = J.wins1 + 2 * (J.wins1_off[n] + s1);
-  const half4 after = h_from(w1[0]), before = h_from(w1[1]);
-  const half4 wins0 = h_from(I0.wins0);
-  const half4 inplay = h_not(h_or(wins0, after));
-  const half4 mask = turn_aggressive ? h_not(after) : h_not(h_zero());
-  us = h_or(h_and(inplay, us), h_and(wins0, mask));
-  const int o = int(s1) * out_ny + s0p;
-  if (unsigned(o) >= unsigned(out_size) || (n <= 1 && n + s1p >= 19)) return false;
-  if (n <= 1) results[n + s1p] = h_to(us);
-  out[o] = h_to(h_or(h_rmax(h_not(us)), before));
-  return true;
-}
-
-// high_board_t helpers for the traversal (high/board.cc)
-PG_HD uint64_t board_of(uint64_t s0, uint64_t s1) {
-  uint64_t board = 0;
-  for (int q = 0; q < 4; q++) {
-    uint32_t quad = 0;
-    for (int i = 8; i >= 0; i--) {
-      const int j = 16 * q + i;
-      quad = 3 * quad + uint32_t(s0 >> j & 1) + 2 * uint32_t(s1 >> j & 1);
-    }
-    board |= uint64_t(quad) << (16 * q);
-  }
-  return board;
-}
-
-PG_HD void rotate_sides(uint64_t* side, int q, int d) {
-  for (int s = 0; s < 2; s++) {
-    const uint32_t old = uint32_t(side[s] >> (16 * q)) & 0x1ff;
-    uint32_t quad = 0;
-    for (int i = 0; i < 9; i++)
-      if (old >> i & 1) quad |= 1u << (4 - d * (3 * (i % 3) - i / 3 - 2));
-    side[s] ^= uint64_t(old ^ quad) << (16 * q);
-  }
-}
-
-// done_and_value (high/board.cc:20-29)
-PG_HD bool done_value(const mid_tables& MT, const uint64_t* side, uint32_t ply, int* value) {
-  const bool bw = won(MT.winpat, side[0]), ww = won(MT.winpat, side[1]);
-  const int turn = int(ply >> 1 & 1);
-  if (bw || ww) { *value = (bw && ww) ? 0 : (bw == !turn ? 1 : -1); return true; }
-  if (ply == 72) { *value = 0; return true; }
-  return false;
-}
-
-PG_HD int hbit(const uint4& h, int i) {
-  const uint32_t w = i < 32 ? h.x : i < 64 ? h.y : i < 96 ? h.z : h.w;
-  return int(w >> (i & 31) & 1);
-}
-
-PG_HD void append(pg_mid_values_t* out, uint64_t raw, int v) {
-  const int k = out->size++;
-  if (k < 163) { out->entries[k].raw = raw; out->entries[k].value = v; out->entries[k].pad = 0; }
-}
-
-// midsolve_traverse (midengine.cc:127-158), iteratively; supers[i] = (win, notlose)
-PG_HD void traverse(const mid_job_t& J, const mid_tables& MT, const uint4* supers, pg_mid_values_t* out) {
-  out->size = 0;
-  out->pad = 0;
-  uint64_t side[2] = {J.side[0], J.side[1]};
-  const uint32_t ply = J.ply;
-  auto middle_children = [&](const uint64_t* sd, uint32_t p, const uint4* r) {
-    int best = -1;
-    for (int s = 0; s < 8; s++) {
-      const int q = s >> 1, d = (s & 1) ? -1 : 1;
-      const int idx = ((d & 3) << (2 * q)) >> 1;
-      const int v = hbit(r[0], idx) + hbit(r[1], idx) - 1;
-      uint64_t rs[2] = {sd[0], sd[1]};
-      rotate_sides(rs, q, d);
-      append(out, board_of(rs[0], rs[1]) | uint64_t((p + 1) & 1) << 63, v);
-      best = best > -v ? best : -v;
-    }
-    return best;
-  };
-  int value;
-  if (done_value(MT, side, ply, &value)) {
-  } else if (!(ply & 1)) {
-    value = -1;
-    const uint64_t empty = 0x01ff01ff01ff01ffull ^ side[0] ^ side[1];
-    int s = 0;
-    for (int bit = 0; bit < 64; bit++) {
-      if (!(empty >> bit & 1)) continue;
-      s++;
-      uint64_t cs[2] = {side[0], side[1]};
-      cs[(ply >> 1) & 1] |= uint64_t(1) << bit;
-      const uint32_t cply = ply + 1;
-      int cv;
-      if (!done_value(MT, cs, cply, &cv)) cv = middle_children(cs, cply, supers + 2 * s);
-      append(out, board_of(cs[0], cs[1]) | uint64_t(1) << 63, cv);
-      value = value > cv ? value : cv;
-    }
-  } else {
-    value = middle_children(side, ply, supers);
-  }
-  append(out, board_of(side[0], side[1]) | uint64_t(ply & 1) << 63, value);
-}
-
-// The whole solve of one board by nt cooperating threads (tid = 0..nt-1).
-// `barrier` separates phases; run with nt = 1 and a no-op barrier it is the
-// same computation done sequentially (used by the CPU self-test).
-template<class Barrier>
-PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* tiles, uint4* ws,
-                          uint4 (*raw)[19], int* fault, int tid, int nt, Barrier barrier, uint4* dump = nullptr) {
-  const int spots = J.spots;
-  // Per-level tables, the same for both passes (midengine.cc:57-76, :101-107)
-  for (int n = spots; n >= 0; n--) {
-    const int k0 = n >> 1, k1 = n - k0;
-    const int ns1p = choose_t(MT.choose, spots - k0, k1);
-    for (int i = tid; i < ns1p; i += nt) J.sets1p[J.sets1p_off[n] + i] = unrank(MT.choose, spots - k0, k1, i);
-    const int ns1 = choose_t(MT.choose, spots, k1);
-    const int parity = int((n + J.ply) & 1);
-    const uint64_t root1 = J.side[(spots + n + 1) & 1];
-    for (int s = tid; s < ns1; s += nt) {
-      const uint64_t side1 = root1 | set_side(J.empty, k1, unrank(MT.choose, spots, k1, s));
-      const super8 w = s_super_wins(MT.wf, side1);
-      J.wins1[2 * (J.wins1_off[n] + s)] = h_to(s_split(w, parity));
-      J.wins1[2 * (J.wins1_off[n] + s) + 1] = h_to(s_split(w, !parity));
-    }
-  }
-  barrier();
-  for (int n = spots; n >= 0; n--) {  // make_cs1ps (mid/internal.h:135-150)
-    const int k0 = n >> 1, k1 = n - k0;
-    const int ns1p = choose_t(MT.choose, spots - k0, k1);
-    const uint64_t* sp = J.sets1p + J.sets1p_off[n];
-    for (int idx = tid; idx < ns1p * (spots - k0); idx += nt) {
-      const int s1p = idx / (spots - k0), j = idx - s1p * (spots - k0);
-      int c = s1p;
-      for (int a = 0; a < k1; a++) {
-        const int v = int(sp[s1p] >> (5 * a) & 0x1f);
-        if (j < v) c -= choose_t(MT.choose, v - 1, a);
-      }
-      J.cs1ps[J.cs1ps_off[n] + idx] = uint16_t(c);
-    }
-  }
-  barrier();
-
-  for (int aggressive = 0; aggressive < 2; aggressive++) {
-    for (int n = spots; n >= 0; n--) {
-      const level_t L = make_level(J, MT, n);
-      const mid_grab gi = J.spaces[n + 1], go = J.spaces[n];
-      const uint4* in = ws + gi.lo;
-      uint4* out = ws + go.lo;
-      for (int base = 0; base < L.nsets0; base += kMidThreads) {
-        const int rows = L.nsets0 - base < kMidThreads ? L.nsets0 - base : kMidThreads;
-        for (int r = tid; r < rows; r += nt) build_set0(J, MT, L, base + r, tiles[r]);
-        barrier();
-        const int items = rows * L.nsets1p;
-        for (int it = tid; it < items; it += nt) {
-          const int r = it / L.nsets1p, s1p = it - r * L.nsets1p;
-          if (!inner(J, MT, L, tiles[r], s1p, aggressive, in, out, gi.ny, go.ny, J.ws_size - gi.lo,
-                     J.ws_size - go.lo, raw[aggressive]))
-            *fault = 1;
-        }
-        barrier();
-      }
-    }
-  }
-
-  // Interleave (midengine.cc:119-124) and traverse; a failed bounds check
-  // marks the record with size -1 instead.
-  barrier();
-  if (tid == 0 && *fault) { J.out->size = -1; J.out->pad = 0; }
-  if (tid == 0 && !*fault) {
-    uint4 supers[2 * 19];
-    for (int i = 0; i < 19; i++)
-      for (int j = 0; j < 2; j++) supers[2 * i + j] = raw[j ^ (i == 0)][i];
-    if (dump)
-      for (int i = 0; i < 38; i++) dump[i] = supers[i];
-    traverse(J, MT, supers, J.out);
-  }
-}
-
-__constant__ uint32_t c_choose[19][11];
-__constant__ uint64_t c_winpat[32];
-
-struct sync_threads { __device__ void operator()() const { __syncthreads(); } };
 
 __global__ void __launch_bounds__(kMidThreads)
 mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict__ wf, int smem_workspace) {
@@ -390,7 +46,7 @@ mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict_
 
 static uint32_t h_choose[19][11];
 
-static int hchoose(int n, int k) {
+int hchoose(int n, int k) {
   if (n < 0 || k < 0 || k > n) return 0;
   long r = 1;
   for (int i = 0; i < k; i++) r = r * (n - i) / (i + 1);
@@ -407,11 +63,6 @@ int bottleneck(int spots) {  // mid/internal.h:37-47
   }
   return worst;
 }
-
-struct board_plan {
-  mid_job_t job;
-  size_t sets1p, wins1, cs1ps, workspace;  // element counts
-};
 
 static bool decode_board(uint64_t raw, mid_job_t& J, std::string& err) {
   // high_board_t::from_raw (high/board.h:77, board.cc:95-111)
@@ -438,7 +89,7 @@ static bool decode_board(uint64_t raw, mid_job_t& J, std::string& err) {
   return true;
 }
 
-static bool plan_board(uint64_t raw, board_plan& P, std::string& err) {
+bool plan_board(uint64_t raw, board_plan& P, std::string& err) {
   mid_job_t& J = P.job;
   memset(&J, 0, sizeof J);
   if (!decode_board(raw, J, err)) return false;
@@ -466,24 +117,31 @@ static bool plan_board(uint64_t raw, board_plan& P, std::string& err) {
   return true;
 }
 
-static std::once_flag mid_consts_once;
 static int upload_consts() {
-  static int rc = 0;
-  std::call_once(mid_consts_once, [] {
-    for (int n = 0; n <= 18; n++)
-      for (int k = 0; k <= 10; k++) h_choose[n][k] = uint32_t(hchoose(n, k));
-    const tables_t& T = tables();
-    if (cudaMemcpyToSymbol(c_choose, h_choose, sizeof h_choose) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_winpat, T.winpat, sizeof T.winpat) != cudaSuccess)
-      rc = PG_ERR_CUDA;
-    if (cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) != cudaSuccess)
-      rc = PG_ERR_CUDA;
-  });
-  return rc;
+  if (int rc = mid_prepare_device()) return rc;
+  static int attr = -1;
+  if (attr < 0)
+    attr = cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) == cudaSuccess
+               ? 0 : PG_ERR_CUDA;
+  return attr;
 }
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+size_t scratch_bytes_of(const board_plan& P) {
+  return align256(P.sets1p * 8) + align256(P.wins1 * 16) + align256(P.cs1ps * 2) +
+         (P.workspace > size_t(kSmemWorkspaceMax) ? align256(P.workspace * 16) : 0);
+}
+
+void carve_scratch(board_plan& P, char* base) {
+  mid_job_t& J = P.job;
+  size_t off = 0;
+  J.sets1p = (uint64_t*)(base + off); off += align256(P.sets1p * 8);
+  J.wins1 = (uint4*)(base + off); off += align256(P.wins1 * 16);
+  J.cs1ps = (uint16_t*)(base + off); off += align256(P.cs1ps * 2);
+  J.workspace = P.workspace > size_t(kSmemWorkspaceMax) ? (uint4*)(base + off) : nullptr;
+}
 
 }  // namespace pg
 
@@ -500,8 +158,7 @@ extern "C" int pg_midsolve_scratch_bytes(const uint64_t* raws, int n, int64_t* b
   for (int i = 0; i < n; i++) {
     board_plan P;
     if (!plan_board(raws[i], P, err)) return fail(PG_ERR_ARG, err);
-    total += align256(P.sets1p * 8) + align256(P.wins1 * 16) + align256(P.cs1ps * 2) +
-             (P.workspace > size_t(kSmemWorkspaceMax) ? align256(P.workspace * 16) : 0);
+    total += scratch_bytes_of(P);
   }
   *bytes = int64_t(total);
   return PG_OK;
@@ -523,9 +180,7 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
   size_t total = 0;
   for (int i = 0; i < n; i++) {
     if (!plan_board(raws[i], plans[i], err)) return fail(PG_ERR_ARG, "board " + std::to_string(i) + ": " + err);
-    const auto& P = plans[i];
-    total += align256(P.sets1p * 8) + align256(P.wins1 * 16) + align256(P.cs1ps * 2);
-    if (P.workspace > size_t(kSmemWorkspaceMax)) total += align256(P.workspace * 16);
+    total += scratch_bytes_of(plans[i]);
   }
   char* base = (char*)scratch;
   bool owned = false;
@@ -539,11 +194,9 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
   std::vector<mid_job_t> small, large;
   for (int i = 0; i < n; i++) {
     auto& P = plans[i];
+    carve_scratch(P, base + off);
+    off += scratch_bytes_of(P);
     mid_job_t& J = P.job;
-    J.sets1p = (uint64_t*)(base + off); off += align256(P.sets1p * 8);
-    J.wins1 = (uint4*)(base + off); off += align256(P.wins1 * 16);
-    J.cs1ps = (uint16_t*)(base + off); off += align256(P.cs1ps * 2);
-    if (P.workspace > size_t(kSmemWorkspaceMax)) { J.workspace = (uint4*)(base + off); off += align256(P.workspace * 16); }
     J.out = out + i;
     (P.workspace > size_t(kSmemWorkspaceMax) ? large : small).push_back(J);
   }

@@ -1,0 +1,234 @@
+// Continuous-batching midsolve server.
+//
+// A persistent kernel keeps one worker CTA per SM.  Requests live in a ring in
+// host-mapped memory: the host writes a planned board (mid_job_t with its
+// scratch carved out of a device arena) and then publishes it by raising the
+// ring's tail.  Workers claim ring entries with an atomic on a device counter,
+// solve the board with the midsolve body (mid.cu), write the result records
+// straight into host-mapped memory and raise the entry's done flag.  New
+// requests are admitted by the host whenever the ring has a free entry and the
+// arena has room for the board's scratch (its HBM budget), so work that
+// arrives while others are on the GPU joins them as soon as resources free up.
+//
+// Every wait is bounded: an idle worker polls with nanosleep back-off and
+// leaves after a fixed number of polls (status kIdleExit), so a host that
+// stops talking cannot hold the GPU; the host relaunches workers on the next
+// submit.
+#include "mid_body.cuh"
+#include "runtime.h"
+#include "../../include/pentago_b200.h"
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <vector>
+
+namespace pg {
+
+constexpr int kRing = 1024;
+constexpr unsigned long long kIdlePolls = 2000000ull;  // ~2 s of 1 us sleeps
+enum : int { kRunning = 1, kIdleExit = 2, kClosed = 3, kFault = 4 };
+
+struct serve_entry {          // host-mapped
+  mid_job_t job;              // planned board; job.out points into the result area
+  volatile int32_t done;      // 0 pending, 1 solved, -1 bounds failure
+  int32_t pad[3];
+};
+
+struct serve_ctl {            // host-mapped
+  volatile unsigned long long tail;   // entries published by the host
+  volatile int32_t close;             // host asks workers to leave
+  volatile int32_t status;            // kRunning / kIdleExit / kClosed
+};
+
+__global__ void __launch_bounds__(kMidThreads, 1)
+serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, const uint32_t* __restrict__ wf) {
+  extern __shared__ uint4 smem[];
+  set0_info* tiles = reinterpret_cast<set0_info*>(smem);
+  uint4* smem_ws = smem + kMidThreads * sizeof(set0_info) / sizeof(uint4);
+  __shared__ uint4 raw[2][19];
+  __shared__ int fault;
+  __shared__ long long claimed;
+  const mid_tables MT = {c_choose, c_winpat, wf};
+  for (;;) {
+    if (threadIdx.x == 0) {
+      claimed = -1;
+      unsigned long long polls = 0;
+      for (;;) {
+        const unsigned long long h = atomicAdd(head, 0ull);
+        const unsigned long long t = ctl->tail;
+        if (h < t) {
+          if (atomicCAS(head, h, h + 1) == h) { claimed = (long long)h; __threadfence_system(); break; }
+          continue;
+        }
+        if (ctl->close) { ctl->status = kClosed; break; }
+        if (++polls > kIdlePolls) { ctl->status = kIdleExit; break; }
+        __nanosleep(1000);
+      }
+      fault = 0;
+    }
+    __syncthreads();
+    if (claimed < 0) return;
+    serve_entry& E = ring[claimed % kRing];
+    __threadfence_system();
+    mid_job_t J = E.job;
+    uint4* ws = J.workspace ? J.workspace : smem_ws;
+    mid_board_body(J, MT, tiles, ws, raw, &fault, int(threadIdx.x), int(blockDim.x), sync_threads());
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence_system();
+      E.done = fault ? -1 : 1;
+    }
+    __syncthreads();
+  }
+}
+
+// Host side: first-fit arena over one device allocation
+struct arena {
+  char* base = nullptr;
+  size_t size = 0;
+  std::map<size_t, size_t> free_;  // offset -> length
+  void init(char* b, size_t n) { base = b; size = n; free_.clear(); free_[0] = n; }
+  bool alloc(size_t n, size_t& off) {
+    n = (n + 255) & ~size_t(255);
+    for (auto it = free_.begin(); it != free_.end(); ++it)
+      if (it->second >= n) {
+        off = it->first;
+        const size_t rest = it->second - n;
+        free_.erase(it);
+        if (rest) free_[off + n] = rest;
+        return true;
+      }
+    return false;
+  }
+  void release(size_t off, size_t n) {
+    n = (n + 255) & ~size_t(255);
+    auto it = free_.emplace(off, n).first;
+    auto next = std::next(it);
+    if (next != free_.end() && it->first + it->second == next->first) { it->second += next->second; free_.erase(next); }
+    if (it != free_.begin()) {
+      auto prev = std::prev(it);
+      if (prev->first + prev->second == it->first) { prev->second += it->second; free_.erase(it); }
+    }
+  }
+};
+
+struct server {
+  std::mutex m;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  serve_entry* ring = nullptr;        // mapped
+  serve_ctl* ctl = nullptr;           // mapped
+  pg_mid_values_t* results = nullptr; // mapped, one per ring entry
+  unsigned long long* head = nullptr; // device claim counter
+  arena A;
+  unsigned long long next = 0;        // next ticket
+  struct inflight { size_t off, bytes; bool live; };
+  std::vector<inflight> slots;        // per ring entry
+  bool launched = false;
+  int workers = 0;
+};
+
+static int launch_workers(server& S) {
+  const dev_tables_t* T = device_tables();
+  if (!T) return PG_ERR_CUDA;
+  S.ctl->close = 0;
+  S.ctl->status = kRunning;
+  const size_t smem = kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16;
+  serve_kernel<<<S.workers, kMidThreads, smem, S.stream>>>(S.ring, S.ctl, S.head, T->win_factors);
+  PG_CUDA(cudaGetLastError());
+  S.launched = true;
+  return PG_OK;
+}
+
+}  // namespace pg
+
+using namespace pg;
+
+extern "C" int pg_serve_open(int64_t budget_bytes, pg_server_t* out) {
+  if (!out || budget_bytes <= 0) return fail(PG_ERR_ARG, "bad server arguments");
+  if (int rc = mid_prepare_device()) return rc;
+  auto* S = new server;
+  PG_CUDA(cudaGetDevice(&S->device));
+  int sms = 0;
+  PG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device));
+  S->workers = sms;
+  PG_CUDA(cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)));
+  PG_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
+  PG_CUDA(cudaHostAlloc((void**)&S->ring, sizeof(serve_entry) * kRing, cudaHostAllocMapped));
+  PG_CUDA(cudaHostAlloc((void**)&S->ctl, sizeof(serve_ctl), cudaHostAllocMapped));
+  PG_CUDA(cudaHostAlloc((void**)&S->results, sizeof(pg_mid_values_t) * kRing, cudaHostAllocMapped));
+  memset((void*)S->ring, 0, sizeof(serve_entry) * kRing);
+  memset((void*)S->ctl, 0, sizeof(serve_ctl));
+  char* base = nullptr;
+  PG_CUDA(cudaMalloc(&base, size_t(budget_bytes)));
+  S->A.init(base, size_t(budget_bytes));
+  S->slots.assign(kRing, server::inflight{0, 0, false});
+  PG_CUDA(cudaMalloc(&S->head, sizeof(unsigned long long)));
+  PG_CUDA(cudaMemset(S->head, 0, sizeof(unsigned long long)));
+  *out = reinterpret_cast<pg_server_t>(S);
+  return PG_OK;
+}
+
+// Returns a ticket >= 0, or PG_ERR_CAPACITY when the ring or the budget is full
+// right now (the caller retries after polling).
+extern "C" int64_t pg_serve_submit(pg_server_t h, uint64_t raw) {
+  if (!h) return fail(PG_ERR_ARG, "null server");
+  server& S = *reinterpret_cast<server*>(h);
+  std::lock_guard<std::mutex> lock(S.m);
+  std::string err;
+  board_plan P;
+  if (!plan_board(raw, P, err)) return fail(PG_ERR_ARG, err);
+  const unsigned long long ticket = S.next;
+  const int slot = int(ticket % kRing);
+  if (S.slots[slot].live) return fail(PG_ERR_CAPACITY, "request ring full");
+  const size_t bytes = scratch_bytes_of(P);
+  size_t off = 0;
+  if (!S.A.alloc(bytes, off)) return fail(PG_ERR_CAPACITY, "scratch budget exhausted");
+  carve_scratch(P, S.A.base + off);
+  P.job.out = S.results + slot;
+  serve_entry& E = S.ring[slot];
+  E.done = 0;
+  E.job = P.job;
+  S.slots[slot] = server::inflight{off, bytes, true};
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  S.next = ticket + 1;
+  S.ctl->tail = ticket + 1;
+  if (!S.launched || S.ctl->status != kRunning) {
+    if (S.launched) cudaStreamSynchronize(S.stream);  // workers left after idling
+    if (int rc = launch_workers(S)) return rc;
+  }
+  return int64_t(ticket);
+}
+
+// 1 and the result when ticket is solved, 0 while pending, < 0 on failure.
+extern "C" int pg_serve_poll(pg_server_t h, int64_t ticket, pg_mid_values_t* result) {
+  if (!h || ticket < 0) return fail(PG_ERR_ARG, "bad poll arguments");
+  server& S = *reinterpret_cast<server*>(h);
+  std::lock_guard<std::mutex> lock(S.m);
+  const int slot = int(ticket % kRing);
+  if (!S.slots[slot].live || (unsigned long long)ticket >= S.next) return fail(PG_ERR_ARG, "unknown ticket");
+  const int done = S.ring[slot].done;
+  if (!done) return 0;
+  std::atomic_thread_fence(std::memory_order_acquire);
+  if (result) memcpy(result, (const void*)(S.results + slot), sizeof(pg_mid_values_t));
+  S.A.release(S.slots[slot].off, S.slots[slot].bytes);
+  S.slots[slot].live = false;
+  return done > 0 ? 1 : fail(PG_ERR_BOUNDS, "midsolve bounds check failed");
+}
+
+extern "C" int pg_serve_close(pg_server_t h) {
+  if (!h) return PG_OK;
+  server* S = reinterpret_cast<server*>(h);
+  S->ctl->close = 1;
+  std::atomic_thread_fence(std::memory_order_seq_cst);
+  cudaError_t e = cudaStreamSynchronize(S->stream);
+  cudaFree(S->A.base);
+  cudaFree(S->head);
+  cudaFreeHost((void*)S->ring);
+  cudaFreeHost((void*)S->ctl);
+  cudaFreeHost(S->results);
+  cudaStreamDestroy(S->stream);
+  delete S;
+  return e == cudaSuccess ? PG_OK : cuda_fail(e, "pg_serve_close");
+}

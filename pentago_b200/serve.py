@@ -1,0 +1,146 @@
+"""Continuous-batching midsolve server (the C ABI's pg_serve_*), and the
+serving benchmark:
+
+    python -m pentago_b200.serve [--requests 600] [--rate 400] [--budget-gb 20]
+
+Requests are seeded boards with stone counts uniform in 18..30 (black to move
+when even, white when odd), arriving as a Poisson stream.  It reports p50/p99
+latency (arrival to result) and boards/s, next to the same boards solved one
+request at a time with pg_midsolve_batch.
+"""
+import argparse
+import ctypes
+import json
+import time
+
+import numpy as np
+
+from . import capi, mid
+
+
+class Server:
+    def __init__(self, budget_bytes=8 << 30):
+        self._h = ctypes.c_void_p()
+        capi.check(capi.lib().pg_serve_open(int(budget_bytes), ctypes.byref(self._h)))
+        self._rec = capi.pg_mid_values_t()
+
+    def submit(self, raw):
+        """Ticket, or None when the ring or the scratch budget is full right now."""
+        t = capi.lib().pg_serve_submit(self._h, ctypes.c_uint64(int(raw)))
+        if t == capi.PG_ERR_CAPACITY:
+            return None
+        return capi.check(t)
+
+    def poll(self, ticket):
+        """[(raw, value), ...] when solved, else None."""
+        r = capi.check(capi.lib().pg_serve_poll(self._h, ticket, ctypes.byref(self._rec)))
+        if r == 0:
+            return None
+        rec = self._rec
+        return [(rec.entries[i].raw, rec.entries[i].value) for i in range(rec.size)]
+
+    def close(self):
+        if self._h:
+            capi.check(capi.lib().pg_serve_close(self._h))
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def request_boards(seed, n, lo=18, hi=30):
+    """n seeded boards with stone counts uniform in [lo, hi]."""
+    from .synthetic import splitmix64
+    stones = lo + (splitmix64(seed, n) % np.uint64(hi - lo + 1)).astype(np.int64)
+    out = []
+    for i, s in enumerate(stones):
+        out.append(int(mid.random_boards(seed * 1000003 + i, 1, int(s))[0]))
+    return np.array(out, np.uint64), stones
+
+
+def run_stream(server, raws, arrivals, timeout=600.0):
+    """Submit raws[i] at time arrivals[i] (seconds from start); returns results
+    and latencies."""
+    n = len(raws)
+    results = [None] * n
+    latency = np.zeros(n)
+    pending = {}      # ticket -> index
+    waiting = []      # indices that arrived but were not admitted yet
+    nxt = 0
+    t0 = time.perf_counter()
+    while (nxt < n or pending or waiting) and time.perf_counter() - t0 < timeout:
+        now = time.perf_counter() - t0
+        while nxt < n and arrivals[nxt] <= now:
+            waiting.append(nxt)
+            nxt += 1
+        while waiting:
+            t = server.submit(raws[waiting[0]])
+            if t is None:
+                break
+            pending[t] = waiting.pop(0)
+        for t in list(pending):
+            r = server.poll(t)
+            if r is not None:
+                i = pending.pop(t)
+                results[i] = r
+                latency[i] = time.perf_counter() - t0 - arrivals[i]
+        if not pending and not waiting and nxt < n:
+            time.sleep(max(0.0, min(arrivals[nxt] - (time.perf_counter() - t0), 0.001)))
+    return results, latency, time.perf_counter() - t0
+
+
+def one_at_a_time(raws):
+    """Baseline: each board alone through pg_midsolve_batch, in sequence."""
+    import torch
+    out = torch.zeros((1, mid.RECORD_BYTES), dtype=torch.uint8, device="cuda")
+    lat = np.zeros(len(raws))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = []
+    for i, r in enumerate(raws):
+        t = time.perf_counter()
+        mid.values_device(np.array([r], np.uint64), out=out)
+        res.append(mid.decode(out.cpu().numpy())[0])
+        lat[i] = time.perf_counter() - t
+    return res, lat, time.perf_counter() - t0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--requests", type=int, default=600)
+    ap.add_argument("--rate", type=float, default=400.0, help="Poisson arrival rate (requests/s)")
+    ap.add_argument("--budget-gb", type=float, default=40.0)
+    ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--baseline", type=int, default=200, help="requests for the one-at-a-time baseline")
+    args = ap.parse_args()
+    import torch
+    capi.check(capi.lib().pg_init())
+    raws, stones = request_boards(args.seed, args.requests)
+    rng = np.random.default_rng(args.seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, args.requests))
+    # warm-up: one board of each size class
+    with Server(int(args.budget_gb * (1 << 30))) as S:
+        w, _, _ = run_stream(S, raws[:8], np.zeros(8))
+        res, lat, wall = run_stream(S, raws, arrivals)
+    done = [r is not None for r in res]
+    base_res, base_lat, base_wall = one_at_a_time(raws[:args.baseline])
+    same = all(a == b for a, b in zip(res[:args.baseline], base_res))
+    print(json.dumps({
+        "metric": "midsolve serving latency and throughput", "requests": args.requests,
+        "stones": "uniform 18..30", "rate_per_s": args.rate, "completed": int(sum(done)),
+        "p50_ms": float(np.percentile(lat[done], 50) * 1e3), "p99_ms": float(np.percentile(lat[done], 99) * 1e3),
+        "boards_per_s": float(sum(done) / wall), "wall_s": wall,
+        "baseline_one_at_a_time": {"requests": args.baseline, "boards_per_s": float(args.baseline / base_wall),
+                                   "p50_ms": float(np.percentile(base_lat, 50) * 1e3),
+                                   "p99_ms": float(np.percentile(base_lat, 99) * 1e3)},
+        "results_identical_alone_and_in_mix": bool(same),
+        "p99_by_stones_ms": {int(s): float(np.percentile(lat[(stones == s) & np.array(done)], 99) * 1e3)
+                             for s in sorted(set(stones.tolist())) if ((stones == s) & np.array(done)).any()},
+    }))
+
+
+if __name__ == "__main__":
+    main()

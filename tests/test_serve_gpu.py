@@ -1,0 +1,42 @@
+"""The continuous-batching server: results identical alone and in the mix,
+admission under a small scratch budget, and clean close."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_results_same_alone_and_in_mix(cuda):
+    from pentago_b200 import mid, serve
+    raws, stones = serve.request_boards(11, 40, lo=22, hi=30)
+    alone = [mid.midsolve(np.array([r], np.uint64))[0] for r in raws]
+    arrivals = np.linspace(0, 0.05, len(raws))
+    with serve.Server(2 << 30) as S:
+        res, lat, wall = serve.run_stream(S, raws, arrivals, timeout=120)
+    assert all(r is not None for r in res)
+    for a, b in zip(alone, res):
+        assert a == b
+
+
+def test_admission_respects_budget(cuda):
+    """A budget that fits only a few 22-stone boards at once still serves all of them."""
+    from pentago_b200 import mid, serve
+    raws = mid.random_boards(5, 12, 22)
+    need = mid.scratch_bytes(raws[:1])
+    with serve.Server(3 * need + 4096) as S:
+        first = [S.submit(r) for r in raws]
+        assert any(t is None for t in first), "budget should refuse some boards"
+        res, lat, wall = serve.run_stream(S, raws, np.zeros(len(raws)), timeout=120)
+    assert all(r is not None for r in res)
+    for r, got in zip(raws, res):
+        assert got == mid.midsolve(np.array([r], np.uint64))[0]
+
+
+def test_server_matches_oracle_small_boards(cuda, O):
+    from pentago_b200 import mid, serve
+    from tests.test_mid_gpu import oracle_values
+    raws = mid.random_boards(8, 16, 27)
+    with serve.Server(1 << 30) as S:
+        res, _, _ = serve.run_stream(S, raws, np.zeros(len(raws)), timeout=60)
+    for r, got in zip(raws, res):
+        assert got == oracle_values(O, r)
