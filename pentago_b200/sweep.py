@@ -64,6 +64,7 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None):
     results = {}
     for slice_ in range(35, min_slice - 1, -1):
         sigs = descendent_sections(root, slice_)
+        torch.cuda.synchronize()
         off = slice_layout(sigs)
         parent = torch.empty((int(off[-1]), 8), dtype=torch.int64, device="cuda")
         t0 = torch.cuda.Event(enable_timing=True)
@@ -81,6 +82,7 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None):
             timings[slice_] = {"ms": t0.elapsed_time(t1), "sections": len(sigs), "nodes": int(off[-1]),
                                "child_nodes": int(child.shape[0]) if child is not None else 0}
         del child
+        torch.cuda.empty_cache()  # the slice above is gone; its HBM must be reusable at 180 GB scale
         child, child_sigs = parent, sigs
     if keep_last:
         return results, child, child_sigs
