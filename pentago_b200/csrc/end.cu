@@ -41,6 +41,7 @@ PG_HD int ladd(int a, int b) {
 // Per-device error word for device-side bounds checks (bit 0: child index
 // out of range).  Read and cleared by pg_end_check.
 __device__ unsigned int d_end_errors;
+__device__ void record_errors(unsigned e) { atomicOr(&d_end_errors, e); }
 
 struct microline_geom {
   int64_t input_base, last_input_base, output_base, last_output_base;
@@ -142,6 +143,25 @@ PG_HD void micro_prepare(const line_dev_t& L, const dev_tables_t& T, int m, micr
   }
 }
 
+constexpr int kMaxPat = 126;  // C(9,4): most stone patterns of one count in a quadrant
+
+// super_wins for the side with stone pattern r (of the line quadrant's stone
+// count for that side) and this microline's fixed quadrants; stored as two uint4.
+template<int DIM>
+PG_HD void micro_pattern(const line_dev_t& L, const dev_tables_t& T, const micro_ctx& c, int side, int r, uint4* out) {
+  const int mask = ldg(T.pop_masks + L.pat_off[side] + r);
+  uint32_t e[16];
+  load_entry(T.win_factors, DIM, mask, e);
+  const super8 w = win_eval<DIM>(e, c.fixed[side], c.c0[side]);
+  out[0] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
+  out[1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
+}
+
+PG_HD super8 super_from(const uint4* p) {
+  const uint4 a = p[0], b = p[1];
+  return super8{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
+}
+
 // Child j of a microline -> Q_j (4 uint4: win half then not-lost half, both
 // already moved into the parent's frame).
 PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, int j) {
@@ -164,16 +184,15 @@ PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, in
 
 // Parent i of a microline (compute.cc:308-356).
 template<int DIM>
-PG_HD void parent_node(const line_dev_t& L, const dev_tables_t& T, const micro_ctx& c, const uint4* qs, int i,
-                       unsigned* errors) {
+PG_HD void parent_node(const line_dev_t& L, const dev_tables_t& T, const micro_ctx& c, const uint4* qs,
+                       const uint4* pats, int i, unsigned* errors) {
   const int turn = L.turn;
   const int q = ldg(T.rmin_flat + L.rmin_off[DIM] + i);
   const uint32_t sq0 = ldg(T.unpack + 2 * q + turn), sq1 = ldg(T.unpack + 2 * q + 1 - turn);
+  // super_wins of both sides, looked up by stone pattern (micro_pattern)
+  const super8 wins0 = super_from(pats + 2 * ldg(T.rank9 + sq0));
+  const super8 wins1 = super_from(pats + 2 * (kMaxPat + ldg(T.rank9 + sq1)));
   uint32_t e[16];
-  load_entry(T.win_factors, DIM, int(sq0), e);
-  const super8 wins0 = win_eval<DIM>(e, c.fixed[0], c.c0[0]);
-  load_entry(T.win_factors, DIM, int(sq1), e);
-  const super8 wins1 = win_eval<DIM>(e, c.fixed[1], c.c0[1]);
   // Every move wins immediately where super_wins(side0 | move) does: the
   // union over the empty cells is one evaluation with the union factor.
   {
@@ -227,6 +246,33 @@ PG_HD void parent_node(const line_dev_t& L, const dev_tables_t& T, const micro_c
 constexpr int kLineThreads = 256;
 constexpr int kMicro = 4;  // microlines per CTA
 
+__device__ void record_errors(unsigned e);
+
+// Phases 2-3 of a CTA's microlines: win patterns and children, barrier, parents.
+template<int DIM>
+__device__ __forceinline__ void microline_work(const line_dev_t& L, const dev_tables_t& T, const micro_ctx* ctx,
+                                               uint4 (*pat)[2 * kMaxPat * 2], uint4* q_smem, int M, int tid, int nt) {
+  const int nc = L.nchild, np = L.nparent;
+  const int p0 = L.npat[0], pp = p0 + L.npat[1];
+  for (int x = tid; x < M * pp; x += nt) {
+    const int k = x / pp, r = x - k * pp, side = r >= p0;
+    const int rr = side ? r - p0 : r;
+    micro_pattern<DIM>(L, T, ctx[k], side, rr, pat[k] + 2 * (side * kMaxPat + rr));
+  }
+  if (!L.slice35)
+    for (int x = tid; x < M * nc; x += nt) {
+      const int k = x / nc, j = x - k * nc;
+      child_node(L, ctx[k].G, q_smem + 4 * k * nc, j);
+    }
+  __syncthreads();
+  unsigned errors = 0;
+  for (int x = tid; x < M * np; x += nt) {
+    const int k = x / np, i = x - k * np;
+    parent_node<DIM>(L, T, ctx[k], q_smem + 4 * k * nc, pat[k], i, &errors);
+  }
+  if (errors) record_errors(errors);
+}
+
 // One CTA computes kMicro microlines of one line: set-up, all children of
 // those microlines into shared memory, barrier, all parents.
 template<int DIM>
@@ -238,37 +284,27 @@ end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
   if (m0 >= nmicro) return;
   const int M = min(kMicro, nmicro - m0);
   __shared__ micro_ctx ctx[kMicro];
+  __shared__ uint4 pat_smem[kMicro][2 * kMaxPat * 2];
   extern __shared__ uint4 q_smem[];
   const int tid = threadIdx.x, nt = blockDim.x;
   if (tid < M) micro_prepare<DIM>(L, T, m0 + tid, ctx[tid]);
   __syncthreads();
-  const int nc = L.nchild, np = L.nparent;
-  if (!L.slice35) {
-    for (int x = tid; x < M * nc; x += nt) {
-      const int k = x / nc, j = x - k * nc;
-      child_node(L, ctx[k].G, q_smem + 4 * k * nc, j);
-    }
-    __syncthreads();
-  }
-  unsigned errors = 0;
-  for (int x = tid; x < M * np; x += nt) {
-    const int k = x / np, i = x - k * np;
-    parent_node<DIM>(L, T, ctx[k], q_smem + 4 * k * nc, i, &errors);
-  }
-  if (errors) atomicOr(&d_end_errors, errors);
+  microline_work<DIM>(L, T, ctx, pat_smem, q_smem, M, tid, nt);
 }
 
 // The same microline code run sequentially on the host, for CPU self-tests of
 // the kernel arithmetic.  Never used by the device entry points.
 template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_tables_t& T) {
-  std::vector<uint4> q(4 * std::max(L.nchild, 1));
+  std::vector<uint4> q(4 * std::max(L.nchild, 1)), pat(2 * kMaxPat * 2);
   unsigned errors = 0;
   micro_ctx c;
   for (int m = 0; m < L.cross[0] * L.cross[1] * L.cross[2]; m++) {
     micro_prepare<DIM>(L, T, m, c);
+    for (int side = 0; side < 2; side++)
+      for (int r = 0; r < L.npat[side]; r++) micro_pattern<DIM>(L, T, c, side, r, &pat[2 * (side * kMaxPat + r)]);
     if (!L.slice35)
       for (int j = 0; j < L.nchild; j++) child_node(L, c.G, q.data(), j);
-    for (int i = 0; i < L.nparent; i++) parent_node<DIM>(L, T, c, q.data(), i, &errors);
+    for (int i = 0; i < L.nparent; i++) parent_node<DIM>(L, T, c, q.data(), pat.data(), i, &errors);
   }
   return errors;
 }
@@ -413,7 +449,7 @@ extern "C" int pg_end_plan_destroy(pg_end_plan_t plan) {
 extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
   const tables_t& H = tables();
   const dev_tables_t T = {H.rmin_flat, H.rmin_inv, &H.unpack[0][0], &H.win_factors[0][0][0], H.rmin_off,
-                          &H.commute[0][0], H.win_union.data(), H.pack};
+                          &H.commute[0][0], H.win_union.data(), H.pack, H.pop_masks, H.rank9};
   std::string err;
   unsigned errors = 0;
   for (int i = 0; i < n; i++) {
@@ -580,6 +616,7 @@ __global__ void __launch_bounds__(kLineThreads, 2)
 sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_tables_t T) {
   __shared__ __align__(16) line_dev_t L;
   __shared__ micro_ctx ctx[kMicro];
+  __shared__ uint4 pat_smem[kMicro][2 * kMaxPat * 2];
   __shared__ int s_fam;
   extern __shared__ uint4 q_smem[];
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -611,20 +648,7 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   const int M = min(kMicro, nmicro - m0);
   if (tid < M) micro_prepare<DIM>(L, T, m0 + tid, ctx[tid]);
   __syncthreads();
-  const int nc = L.nchild, np = L.nparent;
-  if (!L.slice35) {
-    for (int x = tid; x < M * nc; x += nt) {
-      const int k = x / nc, j = x - k * nc;
-      child_node(L, ctx[k].G, q_smem + 4 * k * nc, j);
-    }
-    __syncthreads();
-  }
-  unsigned errors = 0;
-  for (int x = tid; x < M * np; x += nt) {
-    const int k = x / np, i = x - k * np;
-    parent_node<DIM>(L, T, ctx[k], q_smem + 4 * k * nc, i, &errors);
-  }
-  if (errors) atomicOr(&d_end_errors, errors);
+  microline_work<DIM>(L, T, ctx, pat_smem, q_smem, M, tid, nt);
 }
 
 static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");

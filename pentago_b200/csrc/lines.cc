@@ -159,6 +159,11 @@ bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error) {
     }
   }
   d.line_moves = d.refl_moves[d.child_dim];
+  for (int side = 0; side < 2; side++) {  // stones of mover (side 0) and opponent in the line quadrant
+    const int k = sec.c[dim][side ? 1 - d.turn : d.turn];
+    d.pat_off[side] = T.pop_off[k];
+    d.npat[side] = T.pop_off[k + 1] - T.pop_off[k];
+  }
   d.input = in.input;
   d.output = in.output;
   if (s.input_blocks > kMaxBlocks || in.length > kMaxBlocks || d.nchild > kMaxLine) {

@@ -39,6 +39,7 @@ struct alignas(16) line_dev_t {
   int32_t perm[4], refl_moves[4], block0[4], first_child_block[4];
   int32_t out_shape[4];
   int32_t rmin_off[4];              // offsets of the parent quadrant lists in rmin_flat
+  int32_t pat_off[2], npat[2];      // stone patterns of the line quadrant: mover, opponent
   const uint64_t* input;
   uint64_t* output;
   int64_t in_off[kMaxBlocks], out_off[kMaxBlocks];

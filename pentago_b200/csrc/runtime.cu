@@ -42,8 +42,10 @@ const dev_tables_t* device_tables() {
   t->commute = upload(&T.commute[0][0], 8 * 256);
   t->win_union = upload(T.win_union.data(), T.win_union.size());
   t->pack = upload(T.pack, 512);
+  t->pop_masks = upload(T.pop_masks, 512);
+  t->rank9 = upload(T.rank9, 512);
   if (!t->rmin_flat || !t->rmin_inv || !t->unpack || !t->win_factors || !t->rmin_off || !t->commute ||
-      !t->win_union || !t->pack) {
+      !t->win_union || !t->pack || !t->pop_masks || !t->rank9) {
     set_error("table upload failed");
     delete t;
     return nullptr;

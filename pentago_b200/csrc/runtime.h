@@ -16,6 +16,8 @@ struct dev_tables_t {
   const uint8_t* commute;      // 8 x 256
   const uint32_t* win_union;   // 4 x 19683 x 16
   const uint16_t* pack;        // 512
+  const uint16_t* pop_masks;   // 512, grouped by popcount
+  const uint8_t* rank9;        // 512
 };
 
 // Tables on the current device (uploaded on first use).  Returns nullptr and

@@ -219,6 +219,17 @@ void build(tables_t& T) {
   }
 }
 
+void build_pop(tables_t& T) {
+  int next = 0;
+  for (int k = 0; k <= 9; k++) {
+    T.pop_off[k] = uint16_t(next);
+    int r = 0;
+    for (int m = 0; m < 512; m++)
+      if (__builtin_popcount(m) == k) { T.pop_masks[next++] = uint16_t(m); T.rank9[m] = uint8_t(r++); }
+  }
+  T.pop_off[10] = uint16_t(next);
+}
+
 void build_union(tables_t& T) {
   T.win_union.assign(size_t(4) * 19683 * 16, 0);
   for (int q = 0; q < 4; q++)
@@ -240,6 +251,7 @@ const tables_t& tables() {
     t.reset(new tables_t);
     build(*t);
     build_union(*t);
+    build_pop(*t);
   });
   return *t;
 }

@@ -31,6 +31,11 @@ struct tables_t {
   // of "the mover places one more stone in q", so that the union over all
   // such moves of super_wins costs one evaluation (4 x 19683 x 16 words).
   std::vector<uint32_t> win_union;
+  // 9-bit quadrant sides grouped by stone count: pop_masks[pop_off[k] + r] is
+  // the r-th mask with k stones (increasing order) and rank9[mask] = r.
+  uint16_t pop_off[11];
+  uint16_t pop_masks[512];
+  uint8_t rank9[512];
 };
 
 // Built once on first use; thread safe.
