@@ -283,8 +283,11 @@ def main():
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
     traffic_per_node = profiled_traffic()
     cpu = None
+    midsolve = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(seconds=12.0)
+        from pentago_b200 import mid
+        midsolve = mid.bench_config0()
 
     if rank == 0:
         result = {
@@ -305,6 +308,7 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes},
             "gpu_launches": 4 * args.steps,
+            "midsolve_config0": midsolve,
             "clocks": clocks.summary(),
         }
         print(json.dumps(result))

@@ -153,6 +153,65 @@ def won(board, color):
     return any(s & p == p for p in _patterns())
 
 
+def positions(raw):
+    """Positions a midsolve of this board evaluates: both passes over every
+    level, 128 rotations (one parity) per (s0, s1p) item (mid/midengine.cc:78-107)."""
+    from math import comb
+    stones = bin(side_of(int(raw) & ((1 << 63) - 1), 1) | side_of(int(raw) & ((1 << 63) - 1), 2)).count("1")
+    spots = 36 - stones
+    items = sum(comb(spots, n >> 1) * comb(spots - (n >> 1), n - (n >> 1)) for n in range(spots + 1))
+    return 2 * 128 * items
+
+
+def bench_config0(steps=20, warmup=3, cpu_seconds=8.0, cpu_threads=None):
+    """Config 0: 64 seeded 26-stone boards (13 black, 13 white, no five).
+    GPU time per batch from CUDA events; the reference engine (oracle/_ref)
+    on the host cores, one board per thread, as the CPU baseline."""
+    import os
+    import time
+    import torch
+    raws = random_boards(0, 64, 26)
+    pos = sum(positions(r) for r in raws)
+    out = torch.zeros((len(raws), RECORD_BYTES), dtype=torch.uint8, device="cuda")
+    scratch = torch.empty(scratch_bytes(raws), dtype=torch.uint8, device="cuda")
+    for _ in range(warmup):
+        values_device(raws, out=out, scratch=scratch)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        values_device(raws, out=out, scratch=scratch)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    result = {"workload": "64 seeded 26-stone boards (13 black, 13 white, no five), full midsolve",
+              "positions_per_batch": pos, "ms_per_batch": ms, "value": pos / (ms / 1e3),
+              "boards_per_s": len(raws) / (ms / 1e3), "unit": "positions/s"}
+    try:
+        from tests.oracle import reference, P
+        R = reference()
+    except ImportError:
+        R = None
+    if R is not None:
+        from concurrent.futures import ThreadPoolExecutor
+        threads = cpu_threads or os.cpu_count() or 1
+
+        def solve(raw):
+            rr, vv = np.zeros(200, np.uint64), np.zeros(200, np.int32)
+            R.midsolve(int(raw), P(rr), P(vv))
+        boards = 0
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(threads) as ex:
+            while time.perf_counter() - t0 < cpu_seconds:
+                list(ex.map(solve, raws))
+                boards += len(raws)
+        el = time.perf_counter() - t0
+        result["cpu_baseline"] = {"value": boards / len(raws) * pos / el, "unit": "positions/s",
+                                  "boards_per_s": boards / el, "cores": threads, "kind": "reference",
+                                  "sample": f"the same 64 boards, repeated for {el:.1f} s, one board per thread"}
+    return result
+
+
 def smoke_check(O):
     """One 26-stone board against the oracle (used by __graft_entry__.smoke)."""
     raws = random_boards(0, 2, 26)
