@@ -167,6 +167,33 @@ int pg_midsolve_scratch_bytes(const uint64_t* raws, int n, int64_t* bytes);
 int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* scratch,
                       int64_t scratch_bytes, void* stream);
 
+/* Midsolve that allocates nothing (no counterpart in the reference).
+ *
+ * For callers that cannot allocate device memory when they need a solve: code
+ * running while a stream is captured into a CUDA graph, code whose framework
+ * owns the device's memory pool, latency-critical loops that must not wait for
+ * or fail in an allocation.  It gives the same results as pg_midsolve_batch
+ * but uses only fixed device arrays that are part of the library image:
+ * PG_NOALLOC_SCRATCH_BYTES of scratch (held on every GPU that loads the
+ * library until the process exits) plus a fixed copy of the win-pattern
+ * table.  The caller passes the inputs (host array of raw_t) and the outputs
+ * (device array of n records), as for pg_midsolve_batch.
+ *
+ * Limits and rules:
+ *   - the boards' job descriptors, per-level tables and (for boards with more
+ *     than 10 empty spots) workspaces must fit in PG_NOALLOC_SCRATCH_BYTES
+ *     together; otherwise the call returns PG_ERR_CAPACITY and does nothing.
+ *     About 64 boards of 26+ stones, or one board of 22 stones, fit;
+ *   - the first call on a device sets that device up (it resolves the arrays'
+ *     device addresses and fills the pattern table; no allocation).  Make that
+ *     first call, with the device current, before any stream capture;
+ *   - all calls share the one scratch array, which keeps the last call's
+ *     contents; nothing in it needs to start at zero (every entry is written
+ *     before it is read).  Calls whose kernels overlap on the GPU (for example
+ *     on two streams without ordering) race on it and must not be made. */
+#define PG_NOALLOC_SCRATCH_BYTES (16 << 20)
+int pg_midsolve_batch_noalloc(const uint64_t* raws, int n, pg_mid_values_t* out, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Midsolve server: continuous batching on a persistent kernel (one worker CTA
  * per SM).  Requests are admitted while others run, as long as the request

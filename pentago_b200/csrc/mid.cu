@@ -246,3 +246,108 @@ extern "C" int pg_selftest_midsolve_host(const uint64_t* raws, int n, pg_mid_val
   }
   return PG_OK;
 }
+
+// ===========================================================================
+// Midsolve without allocation.
+//
+// Some callers cannot allocate device memory at the moment they want a
+// solve: code running while a CUDA stream is being captured into a graph
+// (where cudaMalloc is not allowed), code inside a framework whose memory pool
+// owns the whole device, or a real-time loop that must not pay for, or fail
+// in, an allocation.  pg_midsolve_batch_noalloc serves them with the same
+// kernel as pg_midsolve_batch, but every byte of device scratch it uses (the
+// boards' job descriptors, their per-level tables and, for boards with more
+// than 10 empty spots, their workspace) lives in one fixed array that is part
+// of the library image, plus a fixed copy of the win-pattern table.
+// ===========================================================================
+
+namespace pg {
+
+// Fixed scratch: 16 MiB per device, held by every GPU that loads the library
+// until the process exits.  That fits, for example, 64 boards of 26 or more
+// stones (about 70 KB each) or one board of 22 stones (about 15 MB).
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char noalloc_scratch[kNoAllocScratchBytes];
+static __device__ __align__(256) uint32_t noalloc_win_factors[4 * 512 * 16];
+
+struct noalloc_device {
+  unsigned char* scratch = nullptr;   // device address of noalloc_scratch
+  uint32_t* win_factors = nullptr;    // device address of noalloc_win_factors
+};
+static noalloc_device noalloc_state[64];  // per device ordinal
+
+// Per-device set-up on the first call with that device current: resolve the
+// device addresses of the two arrays (in host code their names are only
+// host-side stand-ins) and fill the win-pattern table.  Nothing here
+// allocates device memory.
+static int noalloc_setup(int dev) {
+  noalloc_device& D = noalloc_state[dev];
+  if (D.scratch) return PG_OK;
+  void* s = nullptr;
+  void* w = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&s, noalloc_scratch);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc_scratch)");
+  e = cudaGetSymbolAddress(&w, noalloc_win_factors);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(noalloc_win_factors)");
+  const tables_t& T = tables();
+  e = cudaMemcpyToSymbol(noalloc_win_factors, &T.win_factors[0][0][0], sizeof(noalloc_win_factors));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyToSymbol(noalloc_win_factors)");
+  if (int rc = upload_consts()) return fail(rc, "midsolve constant upload failed");
+  D.win_factors = static_cast<uint32_t*>(w);
+  D.scratch = static_cast<unsigned char*>(s);
+  return PG_OK;
+}
+
+}  // namespace pg
+
+// Same results as pg_midsolve_batch; see include/pentago_b200.h for the
+// contract (fixed scratch, first-call set-up, calls that overlap race).
+extern "C" int pg_midsolve_batch_noalloc(const uint64_t* raws, int n, pg_mid_values_t* out, void* stream_) {
+  if (n < 0 || (n && (!raws || !out))) return fail(PG_ERR_ARG, "bad midsolve arguments");
+  if (!n) return PG_OK;
+  int dev = 0;
+  PG_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(PG_ERR_ARG, "device ordinal out of range");
+  if (int rc = noalloc_setup(dev)) return rc;
+  const noalloc_device& D = noalloc_state[dev];
+  cudaStream_t stream = (cudaStream_t)stream_;
+  std::string err;
+  // Layout inside the fixed array: job descriptors of the shared-memory
+  // boards, then of the global-workspace boards, then every board's tables.
+  int nsmall = 0, nlarge = 0;
+  size_t tables_bytes = 0;
+  for (int i = 0; i < n; i++) {
+    board_plan P;
+    if (!plan_board(raws[i], P, err)) return fail(PG_ERR_ARG, "board " + std::to_string(i) + ": " + err);
+    (P.workspace > size_t(kSmemWorkspaceMax) ? nlarge : nsmall)++;
+    tables_bytes += scratch_bytes_of(P);
+  }
+  const size_t jobs_bytes = align256(sizeof(mid_job_t) * nsmall) + align256(sizeof(mid_job_t) * nlarge);
+  if (jobs_bytes + tables_bytes > kNoAllocScratchBytes)
+    return fail(PG_ERR_CAPACITY, "boards need " + std::to_string(jobs_bytes + tables_bytes) +
+                                     " bytes of scratch; pg_midsolve_batch_noalloc has " +
+                                     std::to_string(kNoAllocScratchBytes));
+  unsigned char* small_dev = D.scratch;
+  unsigned char* large_dev = D.scratch + align256(sizeof(mid_job_t) * nsmall);
+  size_t off = jobs_bytes;
+  std::vector<mid_job_t> small, large;
+  for (int i = 0; i < n; i++) {
+    board_plan P;
+    plan_board(raws[i], P, err);
+    carve_scratch(P, reinterpret_cast<char*>(D.scratch) + off);
+    off += scratch_bytes_of(P);
+    P.job.out = out + i;
+    (P.workspace > size_t(kSmemWorkspaceMax) ? large : small).push_back(P.job);
+  }
+  for (int pass = 0; pass < 2; pass++) {
+    const auto& jobs = pass ? large : small;
+    if (jobs.empty()) continue;
+    mid_job_t* d = reinterpret_cast<mid_job_t*>(pass ? large_dev : small_dev);
+    PG_CUDA(cudaMemcpyAsync(d, jobs.data(), sizeof(mid_job_t) * jobs.size(), cudaMemcpyHostToDevice, stream));
+    const int smem_ws = pass == 0;
+    const size_t smem = kMidThreads * sizeof(set0_info) + (smem_ws ? kSmemWorkspaceMax * 16 : 0);
+    mid_board_kernel<<<unsigned(jobs.size()), kMidThreads, smem, stream>>>(d, D.win_factors, smem_ws);
+    PG_CUDA(cudaGetLastError());
+  }
+  return PG_OK;
+}
