@@ -186,17 +186,20 @@ PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, in
 template<int DIM>
 PG_HD void parent_node(const line_dev_t& L, const dev_tables_t& T, const micro_ctx& c, const uint4* qs,
                        const uint4* pats, int i, unsigned* errors) {
-  const int turn = L.turn;
-  const int q = ldg(T.rmin_flat + L.rmin_off[DIM] + i);
-  const uint32_t sq0 = ldg(T.unpack + 2 * q + turn), sq1 = ldg(T.unpack + 2 * q + 1 - turn);
+  // One 32-byte record per parent (parent_records): union index, pattern
+  // ranks, and the child index and rotation (4 j + r) of every move.
+  const uint4* rp = reinterpret_cast<const uint4*>(L.recs + i);
+  const uint4 h = ldg(rp), mw = ldg(rp + 1);
+  const uint32_t mvw[6] = {h.z, h.w, mw.x, mw.y, mw.z, mw.w};
+  const int nmoves = int(h.y & 0xff);
   // super_wins of both sides, looked up by stone pattern (micro_pattern)
-  const super8 wins0 = super_from(pats + 2 * ldg(T.rank9 + sq0));
-  const super8 wins1 = super_from(pats + 2 * (kMaxPat + ldg(T.rank9 + sq1)));
+  const super8 wins0 = super_from(pats + 2 * int(h.x >> 16 & 0xff));
+  const super8 wins1 = super_from(pats + 2 * (kMaxPat + int(h.x >> 24)));
   uint32_t e[16];
   // Every move wins immediately where super_wins(side0 | move) does: the
   // union over the empty cells is one evaluation with the union factor.
   {
-    const int t = ldg(T.pack + sq0) + 2 * ldg(T.pack + sq1);
+    const int t = int(h.x & 0xffff);
     const uint4* p = reinterpret_cast<const uint4*>(T.win_union + (size_t(DIM) * 19683 + t) * 16);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -213,11 +216,10 @@ PG_HD void parent_node(const line_dev_t& L, const dev_tables_t& T, const micro_c
     not_loss = s_rmax(s_or(moved, s_not(wins1)));
   } else {
     not_loss = s_zero();
-    uint32_t moves = 511u & ~(sq0 | sq1);
-    while (moves) {
-      const int b = ctz32(moves);
-      moves &= moves - 1;
-      const int ir = ldg(T.rmin_inv + q + (1 + turn) * pow3(b));
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      if (k >= nmoves) break;
+      const int ir = int(mvw[k >> 1] >> (16 * (k & 1)) & 0xffff);
       const int j = ir >> 2, r = ir & 3;
       if (j >= L.nchild) { *errors |= 1u; continue; }
       const uint4 a = qs[4 * j], bq = qs[4 * j + 1], cc = qs[4 * j + 2], d = qs[4 * j + 3];
@@ -314,7 +316,10 @@ struct end_plan {
   std::vector<line_dev_t> host[4];
   line_dev_t* dev[4] = {nullptr, nullptr, nullptr, nullptr};
   int maxchild[4] = {0, 0, 0, 0};
-  bool owned = false;
+  // parent records of every (section, dimension) used, back to back
+  std::vector<parent_rec> recs;
+  std::vector<size_t> rec_off[4];       // per planned line: offset into recs
+  parent_rec* recs_dev = nullptr;
 };
 
 template<int DIM> static int set_smem_limit() {
@@ -379,14 +384,33 @@ extern "C" int pg_line_info(const pg_line_t* line, pg_line_info_t* info) {
 
 static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
   std::string err;
+  std::vector<std::pair<uint64_t, size_t>> seen;  // (section << 2 | dim) -> offset into P.recs
+  std::vector<parent_rec> tmp;
   for (int i = 0; i < n; i++) {
     line_dev_t d;
     if (!plan_line(to_in(lines[i]), d, err)) return fail(PG_ERR_ARG, "line " + std::to_string(i) + ": " + err);
     if (!d.output || (!d.slice35 && !d.input)) return fail(PG_ERR_ARG, "null line buffer");
+    const uint64_t key = lines[i].section << 2 | lines[i].dimension;
+    size_t off = SIZE_MAX;
+    for (const auto& kv : seen) if (kv.first == key) off = kv.second;
+    if (off == SIZE_MAX) {
+      parent_records(lines[i].section, lines[i].dimension, tmp);
+      off = P.recs.size();
+      P.recs.insert(P.recs.end(), tmp.begin(), tmp.end());
+      seen.emplace_back(key, off);
+    }
     P.maxchild[d.dim] = std::max(P.maxchild[d.dim], d.nchild);
     P.host[d.dim].push_back(d);
+    P.rec_off[d.dim].push_back(off);
   }
   return PG_OK;
+}
+
+// Point every planned line at its records, given their device copy.
+static void bind_records(end_plan& P, parent_rec* recs_dev) {
+  P.recs_dev = recs_dev;
+  for (int dim = 0; dim < 4; dim++)
+    for (size_t k = 0; k < P.host[dim].size(); k++) P.host[dim][k].recs = recs_dev + P.rec_off[dim][k];
 }
 
 extern "C" int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream_) {
@@ -396,16 +420,22 @@ extern "C" int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream_
   cudaStream_t stream = (cudaStream_t)stream_;
   end_plan P;
   if (int rc = plan_lines(lines, n, P)) return rc;
-  for (int dim = 0; dim < 4; dim++) {
+  if (P.recs.empty()) return PG_OK;
+  parent_rec* recs = nullptr;
+  PG_CUDA(cudaMallocAsync(&recs, sizeof(parent_rec) * P.recs.size(), stream));
+  PG_CUDA(cudaMemcpyAsync(recs, P.recs.data(), sizeof(parent_rec) * P.recs.size(), cudaMemcpyHostToDevice, stream));
+  bind_records(P, recs);
+  int rc = PG_OK;
+  for (int dim = 0; dim < 4 && !rc; dim++) {
     if (P.host[dim].empty()) continue;
     const size_t bytes = sizeof(line_dev_t) * P.host[dim].size();
     PG_CUDA(cudaMallocAsync(&P.dev[dim], bytes, stream));
     PG_CUDA(cudaMemcpyAsync(P.dev[dim], P.host[dim].data(), bytes, cudaMemcpyHostToDevice, stream));
-    const int rc = launch_group(P, dim, stream, *T);
+    rc = launch_group(P, dim, stream, *T);
     PG_CUDA(cudaFreeAsync(P.dev[dim], stream));
-    if (rc) return rc;
   }
-  return PG_OK;
+  PG_CUDA(cudaFreeAsync(recs, stream));
+  return rc;
 }
 
 extern "C" int pg_end_plan_create(const pg_line_t* lines, int n, pg_end_plan_t* plan) {
@@ -413,6 +443,13 @@ extern "C" int pg_end_plan_create(const pg_line_t* lines, int n, pg_end_plan_t* 
   if (!device_tables()) return PG_ERR_CUDA;
   auto* P = new end_plan;
   if (int rc = plan_lines(lines, n, *P)) { delete P; return rc; }
+  if (!P->recs.empty()) {
+    parent_rec* recs = nullptr;
+    cudaError_t e = cudaMalloc(&recs, sizeof(parent_rec) * P->recs.size());
+    if (e == cudaSuccess) e = cudaMemcpy(recs, P->recs.data(), sizeof(parent_rec) * P->recs.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { if (recs) cudaFree(recs); delete P; return cuda_fail(e, "pg_end_plan_create"); }
+    bind_records(*P, recs);
+  }
   for (int dim = 0; dim < 4; dim++) {
     if (P->host[dim].empty()) continue;
     const size_t bytes = sizeof(line_dev_t) * P->host[dim].size();
@@ -420,6 +457,7 @@ extern "C" int pg_end_plan_create(const pg_line_t* lines, int n, pg_end_plan_t* 
     if (e == cudaSuccess) e = cudaMemcpy(P->dev[dim], P->host[dim].data(), bytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
       for (auto* d : P->dev) if (d) cudaFree(d);
+      if (P->recs_dev) cudaFree(P->recs_dev);
       delete P;
       return cuda_fail(e, "pg_end_plan_create");
     }
@@ -442,6 +480,7 @@ extern "C" int pg_end_plan_destroy(pg_end_plan_t plan) {
   if (!plan) return PG_OK;
   auto* P = reinterpret_cast<end_plan*>(plan);
   for (auto* d : P->dev) if (d) cudaFree(d);
+  if (P->recs_dev) cudaFree(P->recs_dev);
   delete P;
   return PG_OK;
 }
@@ -452,9 +491,12 @@ extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
                           &H.commute[0][0], H.win_union.data(), H.pack, H.pop_masks, H.rank9};
   std::string err;
   unsigned errors = 0;
+  std::vector<parent_rec> recs;
   for (int i = 0; i < n; i++) {
     line_dev_t d;
     if (!plan_line(to_in(lines[i]), d, err)) return fail(PG_ERR_ARG, err);
+    parent_records(lines[i].section, lines[i].dimension, recs);
+    d.recs = recs.data();
     switch (d.dim) {
       case 0: errors |= host_line<0>(d, T); break;
       case 1: errors |= host_line<1>(d, T); break;
@@ -811,8 +853,11 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
   if (int rc = pg_slice_layout(parent_sigs, np, poff.data())) return rc;
   if (int rc = pg_slice_layout(child_sigs, nc, coff.data())) return rc;
   std::string err;
+  std::vector<parent_rec> tmp;
   for (int dim = 0; dim < 4; dim++) {
     std::vector<family_t> fams;
+    std::vector<parent_rec> recs;
+    std::vector<size_t> rec_off;
     int total = 0, maxchild = 0;
     for (int i = 0; i < np; i++) {
       const section_t sec = section_t::from_sig(parent_sigs[i]);
@@ -827,8 +872,15 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
       F.first_line = total;
       total += F.nlines;
       maxchild = std::max(maxchild, F.proto.nchild);
+      parent_records(sec.sig(), dim, tmp);
+      rec_off.push_back(recs.size());
+      recs.insert(recs.end(), tmp.begin(), tmp.end());
     }
     if (fams.empty()) continue;
+    parent_rec* recs_dev = nullptr;
+    PG_CUDA(cudaMallocAsync(&recs_dev, sizeof(parent_rec) * recs.size(), stream));
+    PG_CUDA(cudaMemcpyAsync(recs_dev, recs.data(), sizeof(parent_rec) * recs.size(), cudaMemcpyHostToDevice, stream));
+    for (size_t f = 0; f < fams.size(); f++) fams[f].proto.recs = recs_dev + rec_off[f];
     family_t* d = nullptr;
     PG_CUDA(cudaMallocAsync(&d, sizeof(family_t) * fams.size(), stream));
     PG_CUDA(cudaMemcpyAsync(d, fams.data(), sizeof(family_t) * fams.size(), cudaMemcpyHostToDevice, stream));
@@ -847,6 +899,7 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
       PG_CUDA(cudaGetLastError());
     }
     PG_CUDA(cudaFreeAsync(d, stream));
+    PG_CUDA(cudaFreeAsync(recs_dev, stream));
   }
   return PG_OK;
 }

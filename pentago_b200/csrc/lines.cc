@@ -177,4 +177,25 @@ bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error) {
   return true;
 }
 
+void parent_records(uint64_t section, int dim, std::vector<parent_rec>& recs) {
+  const auto& T = tables();
+  const section_t sec = section_t::from_sig(section);
+  const int turn = sec.sum() & 1;
+  const int k = rmin_bucket(sec.c[dim][0], sec.c[dim][1]);
+  const int n = T.rmin_off[k + 1] - T.rmin_off[k];
+  recs.assign(n, parent_rec{});
+  for (int i = 0; i < n; i++) {
+    const uint16_t q = T.rmin_flat[T.rmin_off[k] + i];
+    const uint16_t s0 = T.unpack[q][turn], s1 = T.unpack[q][1 - turn];
+    parent_rec& r = recs[i];
+    r.t = uint16_t(T.pack[s0] + 2 * T.pack[s1]);
+    r.r0 = T.rank9[s0];
+    r.r1 = T.rank9[s1];
+    int m = 0;
+    for (int b = 0, p3 = 1; b < 9; b++, p3 *= 3)
+      if (!((s0 | s1) >> b & 1)) r.mv[m++] = T.rmin_inv[q + (1 + turn) * p3];
+    r.nmoves = uint8_t(m);
+  }
+}
+
 }  // namespace pg

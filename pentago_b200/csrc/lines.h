@@ -5,6 +5,7 @@
 #pragma once
 #include <cstdint>
 #include <string>
+#include <vector>
 #include "tables.h"
 
 namespace pg {
@@ -29,6 +30,17 @@ inline int invert_global(int g) { return g ^ ((~g >> 2 & (g & 1)) << 1); }
 constexpr int kMaxBlocks = 64;   // 420 nodes / 8 per block < 64
 constexpr int kMaxLine = 424;    // nodes along a quadrant axis, rounded up
 
+// Per-parent facts that depend only on the parent's quadrant along the line
+// (the same for every microline of every line of one section and
+// dimension), so the kernel reads them in one coalesced 32-byte load.
+struct alignas(16) parent_rec {
+  uint16_t t;          // pack[mover stones] + 2 pack[opponent stones]: index of the one-move union factor
+  uint8_t r0, r1;      // ranks of the mover's / opponent's stone patterns (rank9)
+  uint8_t nmoves, pad[3];
+  uint16_t mv[12];     // per empty cell, increasing: rotation_minimal_quadrants_inverse of the child quadrant (4 j + r)
+};
+static_assert(sizeof(parent_rec) == 32, "parent_rec layout");
+
 // Everything a CTA needs to compute one microline of a line.  Plain data,
 // copied to the device as is.
 struct alignas(16) line_dev_t {
@@ -42,6 +54,8 @@ struct alignas(16) line_dev_t {
   int32_t pat_off[2], npat[2];      // stone patterns of the line quadrant: mover, opponent
   const uint64_t* input;
   uint64_t* output;
+  const parent_rec* recs;           // nparent records for this (section, dimension)
+  const void* pad_ptr;
   int64_t in_off[kMaxBlocks], out_off[kMaxBlocks];
   uint8_t csym[kMaxLine];           // reflection locals along the child dimension
   uint8_t xsym[4][8];               // reflection locals of the cross dimensions
@@ -67,7 +81,10 @@ struct line_shapes_t {
 
 // Validate and compute shapes; returns false with a message on bad input.
 bool line_shapes(const line_in_t& in, line_shapes_t& out, std::string& error);
-// Fill the device descriptor.
+// Fill the device descriptor (recs is left null; see parent_records).
 bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error);
+
+// The parent records of a (section, dimension): nparent entries.
+void parent_records(uint64_t section, int dim, std::vector<parent_rec>& recs);
 
 }  // namespace pg
