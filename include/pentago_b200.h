@@ -237,6 +237,63 @@ int pg_rans_decode_batch(const uint8_t* in, const int64_t* in_offsets, const int
 int pg_node_symbols(const uint64_t* nodes, int64_t n, int turn, uint8_t* symbols, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Learned-model rANS for solved blocks: stream format version 3.  No
+ * reference counterpart; it replaces the per-block static table of format 2
+ * (arithmetic_encode, pentago/shard/arithmetic.cc:366-401) by a 3-layer MLP
+ * (hidden 64, bf16 weights, fp32 arithmetic) that predicts each symbol from
+ * the node's board, the rotation and the already coded neighbouring
+ * rotations.  Streams are blocks of a section; symbols are pg_node_symbols'
+ * (256 per node, nodes in the block's C order).  The encoder keeps whichever
+ * of format 3 and format 2 is smaller, and the decoder reads both.
+ * ------------------------------------------------------------------------- */
+
+typedef struct pg_block_ref_t {
+  uint64_t section;   /* section signature (counts as in pg_line_t.section) */
+  int32_t block[4];   /* block coordinates, 8 positions per block per quadrant */
+} pg_block_ref_t;
+
+/* Bytes of a serialized model: "PGLM", version 1, parameter count, bf16 parameters. */
+int64_t pg_learned_model_bytes(void);
+
+/* Bytes a stream of a block with `nodes` nodes may need (either format). */
+int64_t pg_rans_learned_bound(int64_t nodes);
+
+/* Encode stream s: the symbols[offsets[s] .. offsets[s+1]) of block blocks[s]
+ * (256 per node) into out + out_offsets[s] (room for pg_rans_learned_bound),
+ * sizes[s] = its bytes or PG_ERR_ARG.  `model` and `blocks` are host arrays;
+ * symbols, offsets, out, out_offsets and sizes are device arrays. */
+int pg_rans_learned_encode(const uint8_t* model, const pg_block_ref_t* blocks, int nstreams, const uint8_t* symbols,
+                           const int64_t* offsets, uint8_t* out, const int64_t* out_offsets, int64_t* sizes,
+                           void* stream);
+
+/* Decode stream s (either format) into symbols + sym_offsets[s] (room for
+ * sym_caps[s]); status[s] = symbols decoded, PG_ERR_FORMAT (malformed, or
+ * coded with another model or for another block) or PG_ERR_CAPACITY. */
+int pg_rans_learned_decode(const uint8_t* model, const pg_block_ref_t* blocks, int nstreams, const uint8_t* in,
+                           const int64_t* in_offsets, const int64_t* in_sizes, uint8_t* symbols,
+                           const int64_t* sym_offsets, const int64_t* sym_caps, int64_t* status, void* stream);
+
+/* The coder's integer frequencies (3 per sample) for samples (stream << 24 |
+ * node << 8 | rotation), with the contexts taken from `symbols`. */
+int pg_learned_freqs(const uint8_t* model, const pg_block_ref_t* blocks, int nstreams, const uint8_t* symbols,
+                     const int64_t* offsets, const int64_t* samples, int64_t n, uint32_t* freqs, void* stream);
+
+/* Training.  params/m/v/grad are device fp32 arrays of the model's parameter
+ * count (pg_learned_model_bytes() - 12) / 2.  Samples are drawn from
+ * candidates (stream << 16 | node) by a seeded hash of (seed, step, index). */
+int pg_learned_samples(const int64_t* candidates, int64_t ncand, uint64_t seed, int64_t step, int64_t batch,
+                       int64_t* samples, void* stream);
+/* Gradient of the summed cross entropy of the samples with the parameters
+ * rounded to bf16 (loss: device float, sum in bits; may be NULL). */
+int pg_learned_grad(const float* params, const pg_block_ref_t* blocks, int nstreams, const uint8_t* symbols,
+                    const int64_t* offsets, const int64_t* samples, int64_t n, float* grad, float* loss, void* stream);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on grad * scale; step counts from 1. */
+int pg_learned_adam(float* params, float* m, float* v, const float* grad, int64_t step, float lr, float scale,
+                    void* stream);
+/* Serialize host fp32 parameters into a model (host, pg_learned_model_bytes). */
+int pg_learned_export(const float* params, uint8_t* model);
+
+/* ---------------------------------------------------------------------------
  * Unit-level device operations, used by tests to check the superscore
  * library against the reference (pentago/base/superscore.h, symmetry.h).
  *   op 0: out[i] = rmax(in[i])                         in: supers

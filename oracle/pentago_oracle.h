@@ -50,6 +50,18 @@ int or_midsolve_workspace_size(int stones);
 int64_t or_rans_encode(const uint8_t* symbols, int64_t n, uint8_t* out, int64_t cap);
 int64_t or_rans_decode(const uint8_t* data, int64_t size, uint8_t* symbols, int64_t cap);
 
+/* Learned coder, stream format version 3 (learned_oracle.c).  One block per
+ * call: section signature and block coordinates; symbols 256 per node. */
+int64_t or_lm_nodes(uint64_t section, const int* block);
+int or_lm_freqs(const uint8_t* model, uint64_t section, const int* block, const uint8_t* symbols,
+                const int64_t* samples, int64_t n, uint32_t* freqs);
+int64_t or_lm_encode(const uint8_t* model, uint64_t section, const int* block, const uint8_t* symbols,
+                     uint8_t* out, int64_t cap);
+int64_t or_lm_decode(const uint8_t* model, uint64_t section, const int* block, const uint8_t* in, int64_t size,
+                     uint8_t* symbols, int64_t cap);
+double or_lm_grad(const float* params, uint64_t section, const int* block, const uint8_t* symbols,
+                  const int64_t* samples, int64_t n, double* grad);
+
 #ifdef __cplusplus
 }
 #endif

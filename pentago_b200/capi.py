@@ -58,6 +58,10 @@ class pg_line_info_t(ctypes.Structure):
     ]
 
 
+class pg_block_ref_t(ctypes.Structure):
+    _fields_ = [("section", ctypes.c_uint64), ("block", ctypes.c_int32 * 4)]
+
+
 class pg_mid_value_t(ctypes.Structure):
     _fields_ = [("raw", ctypes.c_uint64), ("value", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
@@ -100,6 +104,15 @@ SIGNATURES = {
     "pg_rans_encode_batch": (_I, [_P, _P, _I, _P, _P, _P, _P]),
     "pg_rans_decode_batch": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "pg_node_symbols": (_I, [_P, _I64, _I, _P, _P]),
+    "pg_learned_model_bytes": (_I64, []),
+    "pg_rans_learned_bound": (_I64, [_I64]),
+    "pg_rans_learned_encode": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _P]),
+    "pg_rans_learned_decode": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    "pg_learned_freqs": (_I, [_P, _P, _I, _P, _P, _P, _I64, _P, _P]),
+    "pg_learned_samples": (_I, [_P, _I64, ctypes.c_uint64, _I64, _I64, _P, _P]),
+    "pg_learned_grad": (_I, [_P, _P, _I, _P, _P, _P, _I64, _P, _P, _P]),
+    "pg_learned_adam": (_I, [_P, _P, _P, _P, _I64, ctypes.c_float, ctypes.c_float, _P]),
+    "pg_learned_export": (_I, [_P, _P]),
     "pg_midsolve_workspace_size": (_I, [_I]),
     "pg_selftest_midsolve_host": (_I, [_P, _I, _P, _P]),
     "pg_midsolve_scratch_bytes": (_I, [_P, _I, ctypes.POINTER(_I64)]),

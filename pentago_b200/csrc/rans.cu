@@ -64,12 +64,18 @@ __device__ inline uint64_t get_u64(const uint8_t* p) { return uint64_t(get_u32(p
 // One 8-thread group per stream.  out_offsets[s] has room for stream_bound(n_s).
 __global__ void __launch_bounds__(256)
 rans_encode_kernel(const uint8_t* __restrict__ symbols, const int64_t* __restrict__ offsets, int nstreams,
-                   uint8_t* __restrict__ out, const int64_t* __restrict__ out_offsets, int64_t* __restrict__ sizes) {
+                   uint8_t* __restrict__ out, const int64_t* __restrict__ out_offsets, int64_t* __restrict__ sizes,
+                   const int64_t* __restrict__ expect) {
   const int group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const int lane = threadIdx.x & 7;
   const unsigned gmask = 0xffu << (threadIdx.x & 24);
   if (group >= nstreams) return;
   const int64_t begin = offsets[group], n = offsets[group + 1] - begin;
+  // With `expect`, a stream of another length has no room reserved: refuse it
+  if (expect && n != expect[group]) {
+    if (lane == 0) sizes[group] = PG_ERR_ARG;
+    return;
+  }
   const uint8_t* sym = symbols + begin;
   // Count symbols
   uint64_t c[3] = {0, 0, 0};
@@ -126,12 +132,14 @@ __global__ void __launch_bounds__(256)
 rans_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ in_offsets,
                    const int64_t* __restrict__ in_sizes, int nstreams, uint8_t* __restrict__ symbols,
                    const int64_t* __restrict__ sym_offsets, const int64_t* __restrict__ sym_caps,
-                   int64_t* __restrict__ status) {
+                   int64_t* __restrict__ status, int only_v2) {
   const int group = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
   const int lane = threadIdx.x & 7;
   if (group >= nstreams) return;
   const uint8_t* base = in + in_offsets[group];
   const int64_t size = in_sizes[group];
+  // Streams of another version are left to the learned decoder when asked
+  if (only_v2 && size >= 4 && get_u32(base) != 2) return;
   // Header checks as arithmetic_deserialize / arithmetic_decode (arithmetic.cc:403-495)
   if (size < kHeader || get_u32(base) != 2) { if (lane == 0) status[group] = PG_ERR_FORMAT; return; }
   uint64_t c[3];
@@ -166,6 +174,27 @@ rans_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ i
   if (lane == 0) status[group] = int64_t(n);
 }
 
+int64_t rans_stream_bound(int64_t n) { return stream_bound(n); }
+
+int launch_rans_encode(const uint8_t* symbols, const int64_t* offsets, int nstreams, uint8_t* out,
+                       const int64_t* out_offsets, int64_t* sizes, const int64_t* expect, cudaStream_t stream) {
+  const int threads = 256, groups_per_block = threads / kLanes;
+  rans_encode_kernel<<<(nstreams + groups_per_block - 1) / groups_per_block, threads, 0, stream>>>(
+      symbols, offsets, nstreams, out, out_offsets, sizes, expect);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}
+
+int launch_rans_decode(const uint8_t* in, const int64_t* in_offsets, const int64_t* in_sizes, int nstreams,
+                       uint8_t* symbols, const int64_t* sym_offsets, const int64_t* sym_caps, int64_t* status,
+                       int only_v2, cudaStream_t stream) {
+  const int threads = 256, groups_per_block = threads / kLanes;
+  rans_decode_kernel<<<(nstreams + groups_per_block - 1) / groups_per_block, threads, 0, stream>>>(
+      in, in_offsets, in_sizes, nstreams, symbols, sym_offsets, sym_caps, status, only_v2);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}
+
 // Ternary symbols of solved nodes in the on-disk convention
 // (shard/shard.cc:448-449 after end/check.cc:154-156, 197-200): for rotation r
 // of node k, symbol = black wins + 2 white wins.  Nodes are [we-win,
@@ -192,11 +221,7 @@ extern "C" int pg_rans_encode_batch(const uint8_t* symbols, const int64_t* offse
                                     const int64_t* out_offsets, int64_t* sizes, void* stream) {
   if (nstreams < 0) return fail(PG_ERR_ARG, "bad stream count");
   if (!nstreams) return PG_OK;
-  const int threads = 256, groups_per_block = threads / kLanes;
-  rans_encode_kernel<<<(nstreams + groups_per_block - 1) / groups_per_block, threads, 0, (cudaStream_t)stream>>>(
-      symbols, offsets, nstreams, out, out_offsets, sizes);
-  PG_CUDA(cudaGetLastError());
-  return PG_OK;
+  return launch_rans_encode(symbols, offsets, nstreams, out, out_offsets, sizes, nullptr, (cudaStream_t)stream);
 }
 
 extern "C" int pg_rans_decode_batch(const uint8_t* in, const int64_t* in_offsets, const int64_t* in_sizes,
@@ -204,11 +229,8 @@ extern "C" int pg_rans_decode_batch(const uint8_t* in, const int64_t* in_offsets
                                     const int64_t* sym_caps, int64_t* status, void* stream) {
   if (nstreams < 0) return fail(PG_ERR_ARG, "bad stream count");
   if (!nstreams) return PG_OK;
-  const int threads = 256, groups_per_block = threads / kLanes;
-  rans_decode_kernel<<<(nstreams + groups_per_block - 1) / groups_per_block, threads, 0, (cudaStream_t)stream>>>(
-      in, in_offsets, in_sizes, nstreams, symbols, sym_offsets, sym_caps, status);
-  PG_CUDA(cudaGetLastError());
-  return PG_OK;
+  return launch_rans_decode(in, in_offsets, in_sizes, nstreams, symbols, sym_offsets, sym_caps, status, 0,
+                            (cudaStream_t)stream);
 }
 
 extern "C" int pg_node_symbols(const uint64_t* nodes, int64_t n, int turn, uint8_t* symbols, void* stream) {

@@ -36,6 +36,11 @@ SIGS = {
     "midsolve_workspace_size": (_i, [_i]),
     "rans_encode": (_i64, [_p, _i64, _p, _i64]),
     "rans_decode": (_i64, [_p, _i64, _p, _i64]),
+    "lm_nodes": (_i64, [_u64, _p]),
+    "lm_freqs": (_i, [_p, _u64, _p, _p, _p, _i64, _p]),
+    "lm_encode": (_i64, [_p, _u64, _p, _p, _p, _i64]),
+    "lm_decode": (_i64, [_p, _u64, _p, _p, _i64, _p, _i64]),
+    "lm_grad": (ctypes.c_double, [_p, _u64, _p, _p, _p, _i64, _p]),
 }
 
 
@@ -76,8 +81,7 @@ def build_oracle():
 def oracle():
     global _oracle
     if _oracle is None:
-        if not os.path.exists(ORACLE_LIB):
-            build_oracle()
+        build_oracle()  # make rebuilds it only when a source changed
         _oracle = Checker(ORACLE_LIB, "or_")
     return _oracle
 
