@@ -117,44 +117,93 @@ PG_HD microline_geom microline_setup(const line_dev_t& L, const dev_tables_t& T,
   return G;
 }
 
-// Per-microline context: geometry plus, for both sides, the win factor
-// entries of the three quadrants that are fixed along the line and the part
-// of super_wins they determine on their own.
+// Per-microline context: geometry and, for both sides, the part of
+// super_wins that comes from win patterns not touching the line quadrant.
 struct micro_ctx {
   microline_geom G;
-  uint32_t fixed[2][64];
   super8 c0[2];
 };
 
+// c0 of one side: the sets of win patterns that miss quadrant DIM.
 template<int DIM>
-PG_HD void micro_prepare(const line_dev_t& L, const dev_tables_t& T, int m, micro_ctx& c) {
-  c.G = microline_setup<DIM>(L, T, m);
-  for (int side = 0; side < 2; side++) {
-    const uint64_t sd = side ? c.G.base_side1 : c.G.base_side0;
-    for (int q = 0; q < 4; q++) {
-      uint32_t* e = c.fixed[side] + 16 * q;
-      if (q == DIM) {
-        for (int w = 0; w < 16; w++) e[w] = 0;
-        continue;
-      }
-      load_entry(T.win_factors, q, int(sd >> (16 * q) & 511), e);
-    }
-    c.c0[side] = win_const<DIM>(c.fixed[side]);
+PG_HD super8 micro_const(const dev_tables_t& T, uint64_t sd) {
+  uint32_t fixed[64];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    if (q == DIM) continue;
+    load_entry(T.win_factors, q, int(sd >> (16 * q) & 511), fixed + 16 * q);
   }
+  return win_const<DIM>(fixed);
 }
 
 constexpr int kMaxPat = 126;  // C(9,4): most stone patterns of one count in a quadrant
+constexpr int kTerms = 17;    // win patterns touching one quadrant
+constexpr int kTab = 160;     // subset tables: terms 0-5 (64), 6-11 (64), 12-16 (32)
 
-// super_wins for the side with stone pattern r (of the line quadrant's stone
-// count for that side) and this microline's fixed quadrants; stored as two uint4.
+// super_wins with the line quadrant DIM varying and the other three fixed,
+// as subset tables.  Each win pattern touching DIM ("term" t) wins at the
+// rotations where DIM's coverage bit r_DIM and the fixed quadrants' product
+// f_t(other rotations) are both set, so for each r_DIM the answer is the OR
+// of f_t over the terms that quadrant DIM covers at r_DIM (term_sub), read
+// from three tables of ORs over subsets of terms.  The f_t live in the frame
+// where axes DIM and 3 are swapped, so that one r_DIM is two whole words.
+
+// 4-bit coverage c of the quadrant on frame axis a, broadcast over the other
+// two axes of a 64-bit slice (bit i0 + 4 i1 + 16 i2).
+PG_HD uint64_t axis_broadcast(int a, uint32_t c) {
+  if (a == 0) return uint64_t(c) * 0x1111111111111111ull;
+  if (a == 1) return uint64_t(spread4(c)) * 0x0001000100010001ull;
+  uint64_t f = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) f |= uint64_t(c >> k & 1) * (uint64_t(0xffff) << (16 * k));
+  return f;
+}
+
+// f_t for term t of quadrant DIM and one side's fixed quadrants sd.
 template<int DIM>
-PG_HD void micro_pattern(const line_dev_t& L, const dev_tables_t& T, const micro_ctx& c, int side, int r, uint4* out) {
+PG_HD uint64_t term_fixed(const dev_tables_t& T, int t, uint64_t sd) {
+  const int p = ldg(T.term_pat + kTerms * DIM + t);
+  uint64_t f = ~uint64_t(0);
+#pragma unroll
+  for (int k = 0; k < 2; k++) {
+    const int q = ldg(T.term_other + 2 * (kTerms * DIM + t) + k);
+    if (q > 3) break;
+    const uint32_t c = ldg(T.cov + (4 * p + q) * 512 + int(sd >> (16 * q) & 511));
+    f &= axis_broadcast(q == 3 ? DIM : q, c);
+  }
+  return f;
+}
+
+// Entry e of the subset tables from the 17 f_t.
+PG_HD uint2 table_entry(const uint2* f, int e) {
+  const int c = e < 64 ? 0 : e < 128 ? 1 : 2, s = e - 64 * c;
+  uint32_t lo = 0, hi = 0;
+#pragma unroll
+  for (int b = 0; b < 6; b++)
+    if (s >> b & 1) { lo |= f[6 * c + b].x; hi |= f[6 * c + b].y; }
+  return make_uint2(lo, hi);
+}
+
+// super_wins from the tables and the covered terms per rotation of DIM.
+template<int DIM>
+PG_HD super8 table_eval(const uint2* tab, const uint4 sub, const super8& c0) {
+  super8 r;
+  const uint32_t S[4] = {sub.x, sub.y, sub.z, sub.w};
+#pragma unroll
+  for (int d = 0; d < 4; d++) {
+    const uint2 a = tab[S[d] & 63], b = tab[64 + (S[d] >> 6 & 63)], c = tab[128 + (S[d] >> 12 & 31)];
+    r.w[2 * d] = a.x | b.x | c.x;
+    r.w[2 * d + 1] = a.y | b.y | c.y;
+  }
+  if constexpr (DIM != 3) s_swap_axes<DIM, 3>(r);
+  return s_or(r, c0);
+}
+
+// Covered terms of stone pattern r of a side of the line quadrant.
+template<int DIM>
+PG_HD uint4 pattern_terms(const line_dev_t& L, const dev_tables_t& T, int side, int r) {
   const int mask = ldg(T.pop_masks + L.pat_off[side] + r);
-  uint32_t e[16];
-  load_entry(T.win_factors, DIM, mask, e);
-  const super8 w = win_eval<DIM>(e, c.fixed[side], c.c0[side]);
-  out[0] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
-  out[1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
+  return ldg(reinterpret_cast<const uint4*>(T.term_sub) + DIM * 512 + mask);
 }
 
 PG_HD super8 super_from(const uint4* p) {
@@ -184,30 +233,22 @@ PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, in
 
 // Parent i of a microline (compute.cc:308-356).
 template<int DIM>
-PG_HD void parent_node(const line_dev_t& L, const dev_tables_t& T, const micro_ctx& c, const uint4* qs,
+PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab0, const uint4* qs,
                        const uint4* pats, int i, unsigned* errors) {
-  // One 32-byte record per parent (parent_records): union index, pattern
-  // ranks, and the child index and rotation (4 j + r) of every move.
+  // One 48-byte record per parent (parent_records): the terms covered after
+  // some move, pattern ranks, and the child index and rotation (4 j + r) of
+  // every move.
   const uint4* rp = reinterpret_cast<const uint4*>(L.recs + i);
-  const uint4 h = ldg(rp), mw = ldg(rp + 1);
-  const uint32_t mvw[6] = {h.z, h.w, mw.x, mw.y, mw.z, mw.w};
-  const int nmoves = int(h.y & 0xff);
-  // super_wins of both sides, looked up by stone pattern (micro_pattern)
-  const super8 wins0 = super_from(pats + 2 * int(h.x >> 16 & 0xff));
-  const super8 wins1 = super_from(pats + 2 * (kMaxPat + int(h.x >> 24)));
-  uint32_t e[16];
-  // Every move wins immediately where super_wins(side0 | move) does: the
-  // union over the empty cells is one evaluation with the union factor.
-  {
-    const int t = int(h.x & 0xffff);
-    const uint4* p = reinterpret_cast<const uint4*>(T.win_union + (size_t(DIM) * 19683 + t) * 16);
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      const uint4 v = ldg(p + k);
-      e[4 * k] = v.x; e[4 * k + 1] = v.y; e[4 * k + 2] = v.z; e[4 * k + 3] = v.w;
-    }
-  }
-  const super8 moved = win_eval<DIM>(e, c.fixed[0], c.c0[0]);
+  const uint4 usub = ldg(rp), h = ldg(rp + 1), mw = ldg(rp + 2);
+  const uint32_t mvw[5] = {h.y, h.z, h.w, mw.x, mw.y};
+  const int nmoves = int(h.x >> 16 & 0xff);
+  // super_wins of both sides, looked up by stone pattern
+  const super8 wins0 = super_from(pats + 2 * int(h.x & 0xff));
+  const super8 wins1 = super_from(pats + 2 * (kMaxPat + int(h.x >> 8 & 0xff)));
+  // Every move wins immediately where super_wins(side0 | move) does; the
+  // union over the empty cells is one table evaluation of the union of the
+  // covered terms.
+  const super8 moved = table_eval<DIM>(tab0, usub, c.c0[0]);
   super8 wins = moved, not_loss;
   if (L.slice35) {
     // The board is full after the move: the child's value is immediate
@@ -250,33 +291,68 @@ constexpr int kMicro = 4;  // microlines per CTA
 
 __device__ void record_errors(unsigned e);
 
-// Phases 2-3 of a CTA's microlines: win patterns and children, barrier, parents.
+// Shared memory of a CTA besides the covered-terms list and the children.
+struct cta_smem {
+  micro_ctx ctx[kMicro];
+  uint2 fterm[kMicro][2][kTerms];              // f_t per microline and side
+  uint2 tab[kMicro][2][kTab];                  // subset tables per microline and side
+  uint4 pat[kMicro][2 * kMaxPat * 2];          // super_wins per microline and stone pattern
+};
+constexpr int kSubBytes = 2 * kMaxPat * 16;    // covered terms of every stone pattern (dynamic smem head)
+
+// A CTA's microlines m0 .. m0 + M - 1: set-up (geometry, c0, covered terms),
+// term factors, subset tables, then super_wins of every stone pattern and
+// all children into shared memory, barrier, all parents.
 template<int DIM>
-__device__ __forceinline__ void microline_work(const line_dev_t& L, const dev_tables_t& T, const micro_ctx* ctx,
-                                               uint4 (*pat)[2 * kMaxPat * 2], uint4* q_smem, int M, int tid, int nt) {
+__device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_tables_t& T, cta_smem& S,
+                                               uint4* psub, uint4* q_smem, int m0, int M, int tid, int nt) {
   const int nc = L.nchild, np = L.nparent;
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
+  if (tid < 2 * M) {
+    const int k = tid >> 1, side = tid & 1;
+    const microline_geom G = microline_setup<DIM>(L, T, m0 + k);
+    if (!side) S.ctx[k].G = G;
+    S.ctx[k].c0[side] = micro_const<DIM>(T, side ? G.base_side1 : G.base_side0);
+  }
+  for (int x = tid; x < pp; x += nt) {
+    const int side = x >= p0, rr = side ? x - p0 : x;
+    psub[side * kMaxPat + rr] = pattern_terms<DIM>(L, T, side, rr);
+  }
+  __syncthreads();
+  for (int x = tid; x < M * 2 * kTerms; x += nt) {
+    const int k = x / (2 * kTerms), r = x - k * 2 * kTerms, side = r >= kTerms, t = side ? r - kTerms : r;
+    const microline_geom& G = S.ctx[k].G;
+    const uint64_t f = term_fixed<DIM>(T, t, side ? G.base_side1 : G.base_side0);
+    S.fterm[k][side][t] = make_uint2(uint32_t(f), uint32_t(f >> 32));
+  }
+  __syncthreads();
+  for (int x = tid; x < M * 2 * kTab; x += nt) {
+    const int k = x / (2 * kTab), r = x - k * 2 * kTab, side = r >= kTab, e = side ? r - kTab : r;
+    S.tab[k][side][e] = table_entry(S.fterm[k][side], e);
+  }
+  __syncthreads();
   for (int x = tid; x < M * pp; x += nt) {
-    const int k = x / pp, r = x - k * pp, side = r >= p0;
-    const int rr = side ? r - p0 : r;
-    micro_pattern<DIM>(L, T, ctx[k], side, rr, pat[k] + 2 * (side * kMaxPat + rr));
+    const int k = x / pp, r = x - k * pp, side = r >= p0, rr = side ? r - p0 : r;
+    const super8 w = table_eval<DIM>(S.tab[k][side], psub[side * kMaxPat + rr], S.ctx[k].c0[side]);
+    uint4* out = S.pat[k] + 2 * (side * kMaxPat + rr);
+    out[0] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
+    out[1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
   }
   if (!L.slice35)
     for (int x = tid; x < M * nc; x += nt) {
       const int k = x / nc, j = x - k * nc;
-      child_node(L, ctx[k].G, q_smem + 4 * k * nc, j);
+      child_node(L, S.ctx[k].G, q_smem + 4 * k * nc, j);
     }
   __syncthreads();
   unsigned errors = 0;
   for (int x = tid; x < M * np; x += nt) {
     const int k = x / np, i = x - k * np;
-    parent_node<DIM>(L, T, ctx[k], q_smem + 4 * k * nc, pat[k], i, &errors);
+    parent_node<DIM>(L, S.ctx[k], S.tab[k][0], q_smem + 4 * k * nc, S.pat[k], i, &errors);
   }
   if (errors) record_errors(errors);
 }
 
-// One CTA computes kMicro microlines of one line: set-up, all children of
-// those microlines into shared memory, barrier, all parents.
+// One CTA computes kMicro microlines of one line.
 template<int DIM>
 __global__ void __launch_bounds__(kLineThreads, 2)
 end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
@@ -285,13 +361,9 @@ end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
   const int m0 = blockIdx.x * kMicro;
   if (m0 >= nmicro) return;
   const int M = min(kMicro, nmicro - m0);
-  __shared__ micro_ctx ctx[kMicro];
-  __shared__ uint4 pat_smem[kMicro][2 * kMaxPat * 2];
-  extern __shared__ uint4 q_smem[];
-  const int tid = threadIdx.x, nt = blockDim.x;
-  if (tid < M) micro_prepare<DIM>(L, T, m0 + tid, ctx[tid]);
-  __syncthreads();
-  microline_work<DIM>(L, T, ctx, pat_smem, q_smem, M, tid, nt);
+  __shared__ cta_smem S;
+  extern __shared__ uint4 dyn_smem[];
+  cta_microlines<DIM>(L, T, S, dyn_smem, dyn_smem + kSubBytes / 16, m0, M, threadIdx.x, blockDim.x);
 }
 
 // The same microline code run sequentially on the host, for CPU self-tests of
@@ -300,13 +372,26 @@ template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_table
   std::vector<uint4> q(4 * std::max(L.nchild, 1)), pat(2 * kMaxPat * 2);
   unsigned errors = 0;
   micro_ctx c;
+  uint2 fterm[2][kTerms], tab[2][kTab];
   for (int m = 0; m < L.cross[0] * L.cross[1] * L.cross[2]; m++) {
-    micro_prepare<DIM>(L, T, m, c);
-    for (int side = 0; side < 2; side++)
-      for (int r = 0; r < L.npat[side]; r++) micro_pattern<DIM>(L, T, c, side, r, &pat[2 * (side * kMaxPat + r)]);
+    c.G = microline_setup<DIM>(L, T, m);
+    for (int side = 0; side < 2; side++) {
+      const uint64_t sd = side ? c.G.base_side1 : c.G.base_side0;
+      c.c0[side] = micro_const<DIM>(T, sd);
+      for (int t = 0; t < kTerms; t++) {
+        const uint64_t f = term_fixed<DIM>(T, t, sd);
+        fterm[side][t] = make_uint2(uint32_t(f), uint32_t(f >> 32));
+      }
+      for (int e = 0; e < kTab; e++) tab[side][e] = table_entry(fterm[side], e);
+      for (int r = 0; r < L.npat[side]; r++) {
+        const super8 w = table_eval<DIM>(tab[side], pattern_terms<DIM>(L, T, side, r), c.c0[side]);
+        pat[2 * (side * kMaxPat + r)] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
+        pat[2 * (side * kMaxPat + r) + 1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
+      }
+    }
     if (!L.slice35)
       for (int j = 0; j < L.nchild; j++) child_node(L, c.G, q.data(), j);
-    for (int i = 0; i < L.nparent; i++) parent_node<DIM>(L, T, c, q.data(), pat.data(), i, &errors);
+    for (int i = 0; i < L.nparent; i++) parent_node<DIM>(L, c, tab[0], q.data(), pat.data(), i, &errors);
   }
   return errors;
 }
@@ -326,7 +411,7 @@ template<int DIM> static int set_smem_limit() {
   static int rc = -1;
   if (rc < 0)
     rc = cudaFuncSetAttribute(end_line_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
+                              kSubBytes + kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
   return rc;
 }
 
@@ -334,7 +419,7 @@ static int launch_group(const end_plan& P, int dim, cudaStream_t stream, const d
   const int n = int(P.host[dim].size());
   if (!n) return PG_OK;
   const dim3 grid((512 + kMicro - 1) / kMicro, unsigned(n));
-  const size_t smem = size_t(kMicro) * P.maxchild[dim] * 64;
+  const size_t smem = kSubBytes + size_t(kMicro) * P.maxchild[dim] * 64;
   int rc = 0;
   switch (dim) {
     case 0: rc = set_smem_limit<0>(); end_line_kernel<0><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
@@ -488,7 +573,8 @@ extern "C" int pg_end_plan_destroy(pg_end_plan_t plan) {
 extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
   const tables_t& H = tables();
   const dev_tables_t T = {H.rmin_flat, H.rmin_inv, &H.unpack[0][0], &H.win_factors[0][0][0], H.rmin_off,
-                          &H.commute[0][0], H.win_union.data(), H.pack, H.pop_masks, H.rank9};
+                          &H.commute[0][0], H.win_union.data(), H.pack, H.pop_masks, H.rank9,
+                          &H.term_pat[0][0], &H.term_other[0][0][0], &H.term_sub[0][0][0], &H.cov[0][0][0]};
   std::string err;
   unsigned errors = 0;
   std::vector<parent_rec> recs;
@@ -657,10 +743,9 @@ template<int DIM>
 __global__ void __launch_bounds__(kLineThreads, 2)
 sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_tables_t T) {
   __shared__ __align__(16) line_dev_t L;
-  __shared__ micro_ctx ctx[kMicro];
-  __shared__ uint4 pat_smem[kMicro][2 * kMaxPat * 2];
+  __shared__ cta_smem S;
   __shared__ int s_fam;
-  extern __shared__ uint4 q_smem[];
+  extern __shared__ uint4 dyn_smem[];
   const int tid = threadIdx.x, nt = blockDim.x;
   const int line = line0 + blockIdx.x;
   if (tid == 0) {
@@ -688,9 +773,7 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   const int m0 = blockIdx.y * kMicro;
   if (m0 >= nmicro) return;
   const int M = min(kMicro, nmicro - m0);
-  if (tid < M) micro_prepare<DIM>(L, T, m0 + tid, ctx[tid]);
-  __syncthreads();
-  microline_work<DIM>(L, T, ctx, pat_smem, q_smem, M, tid, nt);
+  cta_microlines<DIM>(L, T, S, dyn_smem, dyn_smem + kSubBytes / 16, m0, M, tid, nt);
 }
 
 static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");
@@ -700,7 +783,7 @@ template<int DIM> static int sweep_smem_limit() {
   static int rc = -1;
   if (rc < 0)
     rc = cudaFuncSetAttribute(sweep_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
+                              kSubBytes + kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
   return rc;
 }
 
@@ -884,7 +967,7 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
     family_t* d = nullptr;
     PG_CUDA(cudaMallocAsync(&d, sizeof(family_t) * fams.size(), stream));
     PG_CUDA(cudaMemcpyAsync(d, fams.data(), sizeof(family_t) * fams.size(), cudaMemcpyHostToDevice, stream));
-    const size_t smem = size_t(kMicro) * maxchild * 64;
+    const size_t smem = kSubBytes + size_t(kMicro) * maxchild * 64;
     for (int line0 = 0; line0 < total; line0 += 1 << 30) {
       const dim3 grid(unsigned(std::min(total - line0, 1 << 30)), (512 + kMicro - 1) / kMicro);
       int rc = 0;

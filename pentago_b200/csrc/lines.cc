@@ -188,12 +188,14 @@ void parent_records(uint64_t section, int dim, std::vector<parent_rec>& recs) {
     const uint16_t q = T.rmin_flat[T.rmin_off[k] + i];
     const uint16_t s0 = T.unpack[q][turn], s1 = T.unpack[q][1 - turn];
     parent_rec& r = recs[i];
-    r.t = uint16_t(T.pack[s0] + 2 * T.pack[s1]);
     r.r0 = T.rank9[s0];
     r.r1 = T.rank9[s1];
     int m = 0;
     for (int b = 0, p3 = 1; b < 9; b++, p3 *= 3)
-      if (!((s0 | s1) >> b & 1)) r.mv[m++] = T.rmin_inv[q + (1 + turn) * p3];
+      if (!((s0 | s1) >> b & 1)) {
+        r.mv[m++] = T.rmin_inv[q + (1 + turn) * p3];
+        for (int k = 0; k < 4; k++) r.usub[k] |= T.term_sub[dim][s0 | 1 << b][k];
+      }
     r.nmoves = uint8_t(m);
   }
 }

@@ -32,14 +32,15 @@ constexpr int kMaxLine = 424;    // nodes along a quadrant axis, rounded up
 
 // Per-parent facts that depend only on the parent's quadrant along the line
 // (the same for every microline of every line of one section and
-// dimension), so the kernel reads them in one coalesced 32-byte load.
+// dimension), so the kernel reads them in three coalesced 16-byte loads.
 struct alignas(16) parent_rec {
-  uint16_t t;          // pack[mover stones] + 2 pack[opponent stones]: index of the one-move union factor
+  uint32_t usub[4];    // win terms (term_sub) the mover covers after a stone on some empty cell, per rotation
   uint8_t r0, r1;      // ranks of the mover's / opponent's stone patterns (rank9)
-  uint8_t nmoves, pad[3];
-  uint16_t mv[12];     // per empty cell, increasing: rotation_minimal_quadrants_inverse of the child quadrant (4 j + r)
+  uint8_t nmoves, pad;
+  uint16_t mv[14];     // per empty cell, increasing: rotation_minimal_quadrants_inverse of the child quadrant
+                       // (4 j + r); at most 9 used
 };
-static_assert(sizeof(parent_rec) == 32, "parent_rec layout");
+static_assert(sizeof(parent_rec) == 48, "parent_rec layout");
 
 // Everything a CTA needs to compute one microline of a line.  Plain data,
 // copied to the device as is.

@@ -44,8 +44,13 @@ const dev_tables_t* device_tables() {
   t->pack = upload(T.pack, 512);
   t->pop_masks = upload(T.pop_masks, 512);
   t->rank9 = upload(T.rank9, 512);
+  t->term_pat = upload(&T.term_pat[0][0], 4 * 17);
+  t->term_other = upload(&T.term_other[0][0][0], 4 * 17 * 2);
+  t->term_sub = upload(&T.term_sub[0][0][0], 4 * 512 * 4);
+  t->cov = upload(&T.cov[0][0][0], 32 * 4 * 512);
   if (!t->rmin_flat || !t->rmin_inv || !t->unpack || !t->win_factors || !t->rmin_off || !t->commute ||
-      !t->win_union || !t->pack || !t->pop_masks || !t->rank9) {
+      !t->win_union || !t->pack || !t->pop_masks || !t->rank9 || !t->term_pat || !t->term_other || !t->term_sub ||
+      !t->cov) {
     set_error("table upload failed");
     delete t;
     return nullptr;

@@ -18,6 +18,10 @@ struct dev_tables_t {
   const uint16_t* pack;        // 512
   const uint16_t* pop_masks;   // 512, grouped by popcount
   const uint8_t* rank9;        // 512
+  const uint8_t* term_pat;     // 4 x 17
+  const uint8_t* term_other;   // 4 x 17 x 2
+  const uint32_t* term_sub;    // 4 x 512 x 4
+  const uint8_t* cov;          // 32 x 4 x 512
 };
 
 // Tables on the current device (uploaded on first use).  Returns nullptr and

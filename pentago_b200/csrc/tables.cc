@@ -216,6 +216,28 @@ void build(tables_t& T) {
           w += 2;
         }
       }
+    // Terms per quadrant
+    for (int p = 0; p < 32; p++)
+      for (int q = 0; q < 4; q++)
+        for (int v = 0; v < 512; v++) T.cov[p][q][v] = uint8_t(coverage(p, q, v));
+    memset(T.term_sub, 0, sizeof T.term_sub);
+    for (int d = 0; d < 4; d++) {
+      int t = 0;
+      for (int p = 0; p < 32; p++) {
+        if (!(T.winpat[p] >> (16 * d) & 0x1ff)) continue;
+        if (t >= 17) throw std::logic_error("win pattern terms");
+        T.term_pat[d][t] = uint8_t(p);
+        int k = 0;
+        T.term_other[d][t][0] = T.term_other[d][t][1] = 0xff;
+        for (int q = 0; q < 4; q++)
+          if (q != d && (T.winpat[p] >> (16 * q) & 0x1ff)) T.term_other[d][t][k++] = uint8_t(q);
+        for (int v = 0; v < 512; v++)
+          for (int r = 0; r < 4; r++)
+            if (T.cov[p][d][v] >> r & 1) T.term_sub[d][v][r] |= 1u << t;
+        t++;
+      }
+      if (t != 17) throw std::logic_error("win pattern terms");
+    }
   }
 }
 

@@ -31,6 +31,15 @@ struct tables_t {
   // of "the mover places one more stone in q", so that the union over all
   // such moves of super_wins costs one evaluation (4 x 19683 x 16 words).
   std::vector<uint32_t> win_union;
+  // super_wins as 17 terms per quadrant D: the win patterns that touch D,
+  // each with the one or two other quadrants it touches (0xff: none).
+  // term_sub[D][v][r] has bit t set when side v of quadrant D, rotated left r
+  // times, covers term t's cells in D; cov[p][q][v] bit r likewise for
+  // pattern p in quadrant q.
+  uint8_t term_pat[4][17];
+  uint8_t term_other[4][17][2];
+  uint32_t term_sub[4][512][4];
+  uint8_t cov[32][4][512];
   // 9-bit quadrant sides grouped by stone count: pop_masks[pop_off[k] + r] is
   // the r-th mask with k stones (increasing order) and rank9[mask] = r.
   uint16_t pop_off[11];
