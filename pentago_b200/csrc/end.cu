@@ -117,24 +117,10 @@ PG_HD microline_geom microline_setup(const line_dev_t& L, const dev_tables_t& T,
   return G;
 }
 
-// Per-microline context: geometry and, for both sides, the part of
-// super_wins that comes from win patterns not touching the line quadrant.
+// Per-microline context: the geometry (the win tables live beside it).
 struct micro_ctx {
   microline_geom G;
-  super8 c0[2];
 };
-
-// c0 of one side: the sets of win patterns that miss quadrant DIM.
-template<int DIM>
-PG_HD super8 micro_const(const dev_tables_t& T, uint64_t sd) {
-  uint32_t fixed[64];
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    if (q == DIM) continue;
-    load_entry(T.win_factors, q, int(sd >> (16 * q) & 511), fixed + 16 * q);
-  }
-  return win_const<DIM>(fixed);
-}
 
 constexpr int kMaxPat = 126;  // C(9,4): most stone patterns of one count in a quadrant
 constexpr int kTerms = 17;    // win patterns touching one quadrant
@@ -174,10 +160,27 @@ PG_HD uint64_t term_fixed(const dev_tables_t& T, int t, uint64_t sd) {
   return f;
 }
 
-// Entry e of the subset tables from the 17 f_t.
-PG_HD uint2 table_entry(const uint2* f, int e) {
+// Product factor of win pattern u among the 15 that miss quadrant DIM (it
+// wins at every rotation of DIM), in the same frame.
+template<int DIM>
+PG_HD uint64_t miss_fixed(const dev_tables_t& T, int u, uint64_t sd) {
+  const int p = ldg(T.miss_pat + 15 * DIM + u);
+  uint64_t f = ~uint64_t(0);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int q = ldg(T.miss_quad + 3 * (15 * DIM + u) + k);
+    if (q > 3) break;
+    const uint32_t c = ldg(T.cov + (4 * p + q) * 512 + int(sd >> (16 * q) & 511));
+    f &= axis_broadcast(q == 3 ? DIM : q, c);
+  }
+  return f;
+}
+
+// Entry e of the subset tables from the 17 f_t; the first table also carries
+// c0, the OR of the patterns that miss DIM, so every evaluation includes it.
+PG_HD uint2 table_entry(const uint2* f, uint64_t c0, int e) {
   const int c = e < 64 ? 0 : e < 128 ? 1 : 2, s = e - 64 * c;
-  uint32_t lo = 0, hi = 0;
+  uint32_t lo = c ? 0u : uint32_t(c0), hi = c ? 0u : uint32_t(c0 >> 32);
 #pragma unroll
   for (int b = 0; b < 6; b++)
     if (s >> b & 1) { lo |= f[6 * c + b].x; hi |= f[6 * c + b].y; }
@@ -186,7 +189,7 @@ PG_HD uint2 table_entry(const uint2* f, int e) {
 
 // super_wins from the tables and the covered terms per rotation of DIM.
 template<int DIM>
-PG_HD super8 table_eval(const uint2* tab, const uint4 sub, const super8& c0) {
+PG_HD super8 table_eval(const uint2* tab, const uint4 sub) {
   super8 r;
   const uint32_t S[4] = {sub.x, sub.y, sub.z, sub.w};
 #pragma unroll
@@ -196,7 +199,7 @@ PG_HD super8 table_eval(const uint2* tab, const uint4 sub, const super8& c0) {
     r.w[2 * d + 1] = a.y | b.y | c.y;
   }
   if constexpr (DIM != 3) s_swap_axes<DIM, 3>(r);
-  return s_or(r, c0);
+  return r;
 }
 
 // Covered terms of stone pattern r of a side of the line quadrant.
@@ -234,11 +237,10 @@ PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, in
 // Parent i of a microline (compute.cc:308-356).
 template<int DIM>
 PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab0, const uint4* qs,
-                       const uint4* pats, int i, unsigned* errors) {
-  // One 48-byte record per parent (parent_records): the terms covered after
+                       const uint4* pats, const uint4* rp, int i, unsigned* errors) {
+  // The parent's 48-byte record (parent_records): the terms covered after
   // some move, pattern ranks, and the child index and rotation (4 j + r) of
   // every move.
-  const uint4* rp = reinterpret_cast<const uint4*>(L.recs + i);
   const uint4 usub = ldg(rp), h = ldg(rp + 1), mw = ldg(rp + 2);
   const uint32_t mvw[5] = {h.y, h.z, h.w, mw.x, mw.y};
   const int nmoves = int(h.x >> 16 & 0xff);
@@ -248,7 +250,7 @@ PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab
   // Every move wins immediately where super_wins(side0 | move) does; the
   // union over the empty cells is one table evaluation of the union of the
   // covered terms.
-  const super8 moved = table_eval<DIM>(tab0, usub, c.c0[0]);
+  const super8 moved = table_eval<DIM>(tab0, usub);
   super8 wins = moved, not_loss;
   if (L.slice35) {
     // The board is full after the move: the child's value is immediate
@@ -294,46 +296,54 @@ __device__ void record_errors(unsigned e);
 // Shared memory of a CTA besides the covered-terms list and the children.
 struct cta_smem {
   micro_ctx ctx[kMicro];
-  uint2 fterm[kMicro][2][kTerms];              // f_t per microline and side
   uint2 tab[kMicro][2][kTab];                  // subset tables per microline and side
   uint4 pat[kMicro][2 * kMaxPat * 2];          // super_wins per microline and stone pattern
 };
 constexpr int kSubBytes = 2 * kMaxPat * 16;    // covered terms of every stone pattern (dynamic smem head)
 
-// A CTA's microlines m0 .. m0 + M - 1: set-up (geometry, c0, covered terms),
-// term factors, subset tables, then super_wins of every stone pattern and
-// all children into shared memory, barrier, all parents.
+// A CTA's microlines m0 .. m0 + M - 1.  Set-up: warp 2 k + side builds
+// microline k's geometry and that side's subset tables (lane t < 17: term t;
+// lanes 17-31: the patterns that miss the line quadrant, ORed into c0) while
+// the other threads stage the covered terms of every stone pattern; barrier;
+// super_wins of every stone pattern and all children into shared memory;
+// barrier; all parents.
 template<int DIM>
 __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_tables_t& T, cta_smem& S,
-                                               uint4* psub, uint4* q_smem, int m0, int M, int tid, int nt) {
+                                               uint4* dyn, int m0, int M, int tid, int nt) {
   const int nc = L.nchild, np = L.nparent;
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
-  if (tid < 2 * M) {
-    const int k = tid >> 1, side = tid & 1;
+  uint4* psub = dyn;
+  uint4* q_smem = dyn + kSubBytes / 16;
+  const int warp = tid >> 5, lane = tid & 31;
+  if (warp < 2 * M) {
+    const int k = warp >> 1, side = warp & 1;
     const microline_geom G = microline_setup<DIM>(L, T, m0 + k);
-    if (!side) S.ctx[k].G = G;
-    S.ctx[k].c0[side] = micro_const<DIM>(T, side ? G.base_side1 : G.base_side0);
+    const uint64_t sd = side ? G.base_side1 : G.base_side0;
+    if (!side && !lane) S.ctx[k].G = G;
+    const uint64_t f = lane < kTerms ? term_fixed<DIM>(T, lane, sd) : miss_fixed<DIM>(T, lane - kTerms, sd);
+    uint64_t c0 = lane < kTerms ? 0 : f;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) c0 |= __shfl_xor_sync(0xffffffffu, c0, o);
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const int e = lane + 32 * j, c = j < 2 ? 0 : j < 4 ? 1 : 2, sub = e - 64 * c;
+      uint64_t v = c ? 0 : c0;
+#pragma unroll
+      for (int b = 0; b < 6; b++) {
+        const uint64_t fb = __shfl_sync(0xffffffffu, f, 6 * c + b);
+        if (sub >> b & 1 && 6 * c + b < kTerms) v |= fb;
+      }
+      S.tab[k][side][e] = make_uint2(uint32_t(v), uint32_t(v >> 32));
+    }
   }
   for (int x = tid; x < pp; x += nt) {
     const int side = x >= p0, rr = side ? x - p0 : x;
     psub[side * kMaxPat + rr] = pattern_terms<DIM>(L, T, side, rr);
   }
   __syncthreads();
-  for (int x = tid; x < M * 2 * kTerms; x += nt) {
-    const int k = x / (2 * kTerms), r = x - k * 2 * kTerms, side = r >= kTerms, t = side ? r - kTerms : r;
-    const microline_geom& G = S.ctx[k].G;
-    const uint64_t f = term_fixed<DIM>(T, t, side ? G.base_side1 : G.base_side0);
-    S.fterm[k][side][t] = make_uint2(uint32_t(f), uint32_t(f >> 32));
-  }
-  __syncthreads();
-  for (int x = tid; x < M * 2 * kTab; x += nt) {
-    const int k = x / (2 * kTab), r = x - k * 2 * kTab, side = r >= kTab, e = side ? r - kTab : r;
-    S.tab[k][side][e] = table_entry(S.fterm[k][side], e);
-  }
-  __syncthreads();
   for (int x = tid; x < M * pp; x += nt) {
     const int k = x / pp, r = x - k * pp, side = r >= p0, rr = side ? r - p0 : r;
-    const super8 w = table_eval<DIM>(S.tab[k][side], psub[side * kMaxPat + rr], S.ctx[k].c0[side]);
+    const super8 w = table_eval<DIM>(S.tab[k][side], psub[side * kMaxPat + rr]);
     uint4* out = S.pat[k] + 2 * (side * kMaxPat + rr);
     out[0] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
     out[1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
@@ -347,14 +357,15 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
   unsigned errors = 0;
   for (int x = tid; x < M * np; x += nt) {
     const int k = x / np, i = x - k * np;
-    parent_node<DIM>(L, S.ctx[k], S.tab[k][0], q_smem + 4 * k * nc, S.pat[k], i, &errors);
+    parent_node<DIM>(L, S.ctx[k], S.tab[k][0], q_smem + 4 * k * nc, S.pat[k],
+                     reinterpret_cast<const uint4*>(L.recs + i), i, &errors);
   }
   if (errors) record_errors(errors);
 }
 
 // One CTA computes kMicro microlines of one line.
 template<int DIM>
-__global__ void __launch_bounds__(kLineThreads, 2)
+__global__ void __launch_bounds__(kLineThreads, 3)
 end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
   const line_dev_t& L = lines[blockIdx.y];
   const int nmicro = L.cross[0] * L.cross[1] * L.cross[2];
@@ -363,7 +374,7 @@ end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
   const int M = min(kMicro, nmicro - m0);
   __shared__ cta_smem S;
   extern __shared__ uint4 dyn_smem[];
-  cta_microlines<DIM>(L, T, S, dyn_smem, dyn_smem + kSubBytes / 16, m0, M, threadIdx.x, blockDim.x);
+  cta_microlines<DIM>(L, T, S, dyn_smem, m0, M, threadIdx.x, blockDim.x);
 }
 
 // The same microline code run sequentially on the host, for CPU self-tests of
@@ -372,26 +383,28 @@ template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_table
   std::vector<uint4> q(4 * std::max(L.nchild, 1)), pat(2 * kMaxPat * 2);
   unsigned errors = 0;
   micro_ctx c;
-  uint2 fterm[2][kTerms], tab[2][kTab];
+  uint2 fterm[kTerms], tab[2][kTab];
   for (int m = 0; m < L.cross[0] * L.cross[1] * L.cross[2]; m++) {
     c.G = microline_setup<DIM>(L, T, m);
     for (int side = 0; side < 2; side++) {
       const uint64_t sd = side ? c.G.base_side1 : c.G.base_side0;
-      c.c0[side] = micro_const<DIM>(T, sd);
+      uint64_t c0 = 0;
+      for (int u = 0; u < 15; u++) c0 |= miss_fixed<DIM>(T, u, sd);
       for (int t = 0; t < kTerms; t++) {
         const uint64_t f = term_fixed<DIM>(T, t, sd);
-        fterm[side][t] = make_uint2(uint32_t(f), uint32_t(f >> 32));
+        fterm[t] = make_uint2(uint32_t(f), uint32_t(f >> 32));
       }
-      for (int e = 0; e < kTab; e++) tab[side][e] = table_entry(fterm[side], e);
+      for (int e = 0; e < kTab; e++) tab[side][e] = table_entry(fterm, c0, e);
       for (int r = 0; r < L.npat[side]; r++) {
-        const super8 w = table_eval<DIM>(tab[side], pattern_terms<DIM>(L, T, side, r), c.c0[side]);
+        const super8 w = table_eval<DIM>(tab[side], pattern_terms<DIM>(L, T, side, r));
         pat[2 * (side * kMaxPat + r)] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
         pat[2 * (side * kMaxPat + r) + 1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
       }
     }
     if (!L.slice35)
       for (int j = 0; j < L.nchild; j++) child_node(L, c.G, q.data(), j);
-    for (int i = 0; i < L.nparent; i++) parent_node<DIM>(L, c, tab[0], q.data(), pat.data(), i, &errors);
+    for (int i = 0; i < L.nparent; i++)
+      parent_node<DIM>(L, c, tab[0], q.data(), pat.data(), reinterpret_cast<const uint4*>(L.recs + i), i, &errors);
   }
   return errors;
 }
@@ -574,7 +587,8 @@ extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
   const tables_t& H = tables();
   const dev_tables_t T = {H.rmin_flat, H.rmin_inv, &H.unpack[0][0], &H.win_factors[0][0][0], H.rmin_off,
                           &H.commute[0][0], H.win_union.data(), H.pack, H.pop_masks, H.rank9,
-                          &H.term_pat[0][0], &H.term_other[0][0][0], &H.term_sub[0][0][0], &H.cov[0][0][0]};
+                          &H.term_pat[0][0], &H.term_other[0][0][0], &H.term_sub[0][0][0], &H.cov[0][0][0],
+                          &H.miss_pat[0][0], &H.miss_quad[0][0][0]};
   std::string err;
   unsigned errors = 0;
   std::vector<parent_rec> recs;
@@ -740,7 +754,7 @@ PG_HD void family_offsets(const family_t& F, line_dev_t& L, int start, int step)
 }
 
 template<int DIM>
-__global__ void __launch_bounds__(kLineThreads, 2)
+__global__ void __launch_bounds__(kLineThreads, 3)
 sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_tables_t T) {
   __shared__ __align__(16) line_dev_t L;
   __shared__ cta_smem S;
@@ -773,7 +787,7 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   const int m0 = blockIdx.y * kMicro;
   if (m0 >= nmicro) return;
   const int M = min(kMicro, nmicro - m0);
-  cta_microlines<DIM>(L, T, S, dyn_smem, dyn_smem + kSubBytes / 16, m0, M, tid, nt);
+  cta_microlines<DIM>(L, T, S, dyn_smem, m0, M, tid, nt);
 }
 
 static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");

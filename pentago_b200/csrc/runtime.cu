@@ -48,9 +48,11 @@ const dev_tables_t* device_tables() {
   t->term_other = upload(&T.term_other[0][0][0], 4 * 17 * 2);
   t->term_sub = upload(&T.term_sub[0][0][0], 4 * 512 * 4);
   t->cov = upload(&T.cov[0][0][0], 32 * 4 * 512);
+  t->miss_pat = upload(&T.miss_pat[0][0], 4 * 15);
+  t->miss_quad = upload(&T.miss_quad[0][0][0], 4 * 15 * 3);
   if (!t->rmin_flat || !t->rmin_inv || !t->unpack || !t->win_factors || !t->rmin_off || !t->commute ||
       !t->win_union || !t->pack || !t->pop_masks || !t->rank9 || !t->term_pat || !t->term_other || !t->term_sub ||
-      !t->cov) {
+      !t->cov || !t->miss_pat || !t->miss_quad) {
     set_error("table upload failed");
     delete t;
     return nullptr;

@@ -22,6 +22,8 @@ struct dev_tables_t {
   const uint8_t* term_other;   // 4 x 17 x 2
   const uint32_t* term_sub;    // 4 x 512 x 4
   const uint8_t* cov;          // 32 x 4 x 512
+  const uint8_t* miss_pat;     // 4 x 15
+  const uint8_t* miss_quad;    // 4 x 15 x 3
 };
 
 // Tables on the current device (uploaded on first use).  Returns nullptr and

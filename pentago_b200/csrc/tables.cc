@@ -237,6 +237,18 @@ void build(tables_t& T) {
         t++;
       }
       if (t != 17) throw std::logic_error("win pattern terms");
+      int u = 0;
+      for (int p = 0; p < 32; p++) {
+        if (T.winpat[p] >> (16 * d) & 0x1ff) continue;
+        if (u >= 15) throw std::logic_error("win patterns missing a quadrant");
+        T.miss_pat[d][u] = uint8_t(p);
+        int k = 0;
+        for (int j = 0; j < 3; j++) T.miss_quad[d][u][j] = 0xff;
+        for (int q = 0; q < 4; q++)
+          if (T.winpat[p] >> (16 * q) & 0x1ff) T.miss_quad[d][u][k++] = uint8_t(q);
+        u++;
+      }
+      if (u != 15) throw std::logic_error("win patterns missing a quadrant");
     }
   }
 }

@@ -38,6 +38,10 @@ struct tables_t {
   // pattern p in quadrant q.
   uint8_t term_pat[4][17];
   uint8_t term_other[4][17][2];
+  // The 15 win patterns that miss quadrant D, with the quadrants they touch
+  // (0xff pads to three).
+  uint8_t miss_pat[4][15];
+  uint8_t miss_quad[4][15][3];
   uint32_t term_sub[4][512][4];
   uint8_t cov[32][4][512];
   // 9-bit quadrant sides grouped by stone count: pop_masks[pop_off[k] + r] is
