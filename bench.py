@@ -173,6 +173,7 @@ def main():
     ap.add_argument("--blocks", type=int, default=16)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-coder measurement")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -284,10 +285,16 @@ def main():
     traffic_per_node = profiled_traffic()
     cpu = None
     midsolve = None
+    learned = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(seconds=12.0)
         from pentago_b200 import mid
         midsolve = mid.bench_config0()
+    if rank == 0 and world == 1 and not args.no_learned:
+        # Config 3 on a sample: 4096 of the root slice's blocks, after the full sweep and training
+        torch.cuda.empty_cache()
+        from pentago_b200 import learned as learned_mod
+        learned = learned_mod.run_config3(max_blocks=4096, cpu_seconds=0.0 if args.no_cpu_baseline else 5.0)
 
     if rank == 0:
         result = {
@@ -309,6 +316,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes},
             "gpu_launches": 4 * args.steps,
             "midsolve_config0": midsolve,
+            "learned_rans_config3": learned,
             "clocks": clocks.summary(),
         }
         print(json.dumps(result))

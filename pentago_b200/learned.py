@@ -225,49 +225,46 @@ def static_sizes(symbols, offsets, stream=None):
     return sizes
 
 
-def main():
+def run_config3(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.01, steps=1500, batch=32768,
+                chunk_blocks=4096, max_blocks=0, seed=1, cpu_seconds=0.0):
+    """Config 3: solve the root's sections down to its own slice, train on a
+    seeded fraction of the root slice's blocks, code max_blocks blocks (0:
+    all) both ways and check the round trip.  With cpu_seconds > 0 the
+    reference's static coder (oracle/_ref) is timed on the host cores on a
+    sample of the same blocks, as the CPU baseline."""
     import torch
     from . import sweep
     from .end import section_sig
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--root", default="4,4,4,5,4,3,3,3")
-    ap.add_argument("--train-fraction", type=float, default=0.01)
-    ap.add_argument("--steps", type=int, default=1500)
-    ap.add_argument("--batch", type=int, default=32768)
-    ap.add_argument("--chunk-blocks", type=int, default=4096)
-    ap.add_argument("--max-blocks", type=int, default=0, help="code only the first N blocks (0: all)")
-    ap.add_argument("--seed", type=int, default=1)
-    args = ap.parse_args()
-    c = [int(x) for x in args.root.split(",")]
-    root = section_sig([[c[0], c[1]], [c[2], c[3]], [c[4], c[5]], [c[6], c[7]]])
-    capi.check(capi.lib().pg_init())
-    slice_ = sum(c)
+    root = section_sig([list(c) for c in root_counts])
+    slice_ = sum(sum(c) for c in root_counts)
     t0 = time.perf_counter()
     _, slice_t, sigs = sweep.sweep(root, keep_last=True)
+    torch.cuda.synchronize()
     t_sweep = time.perf_counter() - t0
     layout = sweep.slice_layout(sigs)
     refs, node_off, nodes = slice_blocks(sigs, layout)
-    nblocks = len(nodes) if not args.max_blocks else min(args.max_blocks, len(nodes))
+    nblocks = len(nodes) if not max_blocks else min(max_blocks, len(nodes))
     turn = slice_ & 1
-    # Training set: a seeded subset of the blocks
-    rng = np.random.default_rng(args.seed)
-    ntrain = max(1, int(round(args.train_fraction * len(nodes))))
+    rng = np.random.default_rng(seed)
+    ntrain = max(1, int(round(train_fraction * len(nodes))))
     tb = np.sort(rng.choice(len(nodes), ntrain, replace=False))
     trefs = subset(refs, tb)
     tsym, toff = block_symbols(slice_t, node_off[tb], nodes[tb], turn)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    tr = Trainer(trefs, tsym, toff, nodes[tb], seed=args.seed)
-    hist = tr.run(args.steps, args.batch, log_every=max(1, args.steps // 10))
+    tr = Trainer(trefs, tsym, toff, nodes[tb], seed=seed)
+    hist = tr.run(steps, batch, log_every=max(1, steps // 10))
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     model = tr.model()
-    del tsym
-    # Code every block, chunk by chunk
+    del tsym, tr
+    # Code the blocks spread evenly over the slice, chunk by chunk
+    pick = np.unique(np.linspace(0, len(nodes) - 1, nblocks).astype(np.int64))
     tot = {"learned": 0, "static": 0, "symbols": 0, "enc_ms": 0.0, "dec_ms": 0.0, "static_streams": 0}
     lossless = True
-    for c0 in range(0, nblocks, args.chunk_blocks):
-        idx = np.arange(c0, min(nblocks, c0 + args.chunk_blocks))
+    cpu_sample = None
+    for c0 in range(0, len(pick), chunk_blocks):
+        idx = pick[c0:c0 + chunk_blocks]
         crefs = subset(refs, idx)
         sym, off = block_symbols(slice_t, node_off[idx], nodes[idx], turn)
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
@@ -288,10 +285,18 @@ def main():
         tot["symbols"] += int(sym.numel())
         tot["static_streams"] += int((dsz_h == ssz.cpu().numpy()).sum())
         lossless &= bool(torch.equal(dec, sym)) and bool((status.cpu().numpy() == nodes[idx] * 256).all())
+        if cpu_sample is None and cpu_seconds > 0:
+            k = min(64, len(idx))
+            o = off.cpu().numpy()
+            cpu_sample = sym[:int(o[k])].cpu().numpy(), o[:k + 1]
         del sym, data, dec
+    del slice_t
+    torch.cuda.empty_cache()
     bits = lambda b: 8.0 * b / tot["symbols"]
-    print(json.dumps({
-        "root": args.root, "slice": slice_, "blocks": int(nblocks), "positions": tot["symbols"],
+    out = {
+        "workload": f"all blocks of slice {slice_} below root {[list(c) for c in root_counts]} "
+                    f"({'all' if len(pick) == len(nodes) else len(pick)} of {len(nodes)} blocks coded)",
+        "blocks": int(len(pick)), "positions": tot["symbols"],
         "static_bits_per_position": bits(tot["static"]), "learned_bits_per_position": bits(tot["learned"]),
         "learned_over_static": tot["learned"] / tot["static"], "model_bytes": len(model),
         "blocks_kept_static": tot["static_streams"], "lossless": lossless,
@@ -299,8 +304,58 @@ def main():
         "decode_GBps_of_nodes": tot["symbols"] / 4 / (tot["dec_ms"] / 1e3) / 1e9,
         "encode_Msym_per_s": tot["symbols"] / (tot["enc_ms"] / 1e3) / 1e6,
         "decode_Msym_per_s": tot["symbols"] / (tot["dec_ms"] / 1e3) / 1e6,
-        "train_blocks": int(ntrain), "train_steps": args.steps, "train_batch": args.batch, "train_s": t_train,
-        "train_loss_bits": hist, "sweep_s": t_sweep}))
+        "train_blocks": int(ntrain), "train_steps": steps, "train_batch": batch, "train_s": t_train,
+        "train_loss_bits": hist, "sweep_s": t_sweep}
+    if cpu_sample is not None:
+        out["cpu_static_coder"] = _cpu_static_rate(*cpu_sample, seconds=cpu_seconds)
+    return out
+
+
+def _cpu_static_rate(symbols, offsets, seconds):
+    """The reference's format-2 encoder (oracle/_ref) on the host cores, one block per thread."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    try:
+        from tests.oracle import reference, P
+        R = reference()
+    except ImportError:
+        R = None
+    if R is None:
+        return None
+    blocks = [np.ascontiguousarray(symbols[offsets[i]:offsets[i + 1]]) for i in range(len(offsets) - 1)]
+    threads = os.cpu_count() or 1
+
+    def enc(b):
+        out = np.zeros(b.size // 2 + 4096, np.uint8)
+        return R.rans_encode(P(b), b.size, P(out), out.size)
+    done = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        while time.perf_counter() - t0 < seconds:
+            list(ex.map(enc, blocks))
+            done += sum(b.size for b in blocks)
+    dt = time.perf_counter() - t0
+    return {"encode_Msym_per_s": done / dt / 1e6, "cores": threads, "kind": "reference",
+            "sample": f"{len(blocks)} blocks' symbols, format-2 encode repeated for {dt:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--root", default="4,4,4,5,4,3,3,3")
+    ap.add_argument("--train-fraction", type=float, default=0.01)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--batch", type=int, default=32768)
+    ap.add_argument("--chunk-blocks", type=int, default=4096)
+    ap.add_argument("--max-blocks", type=int, default=0, help="code only N blocks spread over the slice (0: all)")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=0.0)
+    args = ap.parse_args()
+    c = [int(x) for x in args.root.split(",")]
+    capi.check(capi.lib().pg_init())
+    res = run_config3(((c[0], c[1]), (c[2], c[3]), (c[4], c[5]), (c[6], c[7])), args.train_fraction, args.steps,
+                      args.batch, args.chunk_blocks, args.max_blocks, args.seed, args.cpu_seconds)
+    res["root"] = args.root
+    print(json.dumps(res))
 
 
 if __name__ == "__main__":
