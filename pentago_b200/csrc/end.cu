@@ -214,15 +214,19 @@ PG_HD super8 super_from(const uint4* p) {
   return super8{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
 }
 
-// Child j of a microline -> Q_j (4 uint4: win half then not-lost half, both
-// already moved into the parent's frame).
-PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, int j) {
+// Address of child j of a microline in the line's input.
+PG_HD const uint64_t* child_addr(const line_dev_t& L, const microline_geom& G, int j) {
   const int jj = j ^ int(j < L.line_moves);
   const int blk = j >> 3;
   const int64_t idx = L.in_off[blk] + (blk == L.input_blocks - 1 ? G.last_input_base : G.input_base) +
                       int64_t(G.input_stride) * (jj & 7);
-  const uint64_t* node = L.input + 8 * idx;
-  const super8 cw = s_load_ldg(node), cn = s_load_ldg(node + 4);
+  return L.input + 8 * idx;
+}
+
+// Child j (its node: cw = win, cn = not lost) -> Q_j, 4 uint4: win half then
+// not-lost half, both already moved into the parent's frame.
+PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, int j, const super8& cw,
+                      const super8& cn) {
   const int l = ladd(G.base_l, L.csym[j]);
   super8 qw = s_translate(s_rmax(s_not(cn)), l);
   super8 qn = s_translate(s_rmax(s_not(cw)), l);
@@ -237,11 +241,10 @@ PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, in
 // Parent i of a microline (compute.cc:308-356).
 template<int DIM>
 PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab0, const uint4* qs,
-                       const uint4* pats, const uint4* rp, int i, unsigned* errors) {
+                       const uint4* pats, const uint4 usub, const uint4 h, const uint4 mw, int i, unsigned* errors) {
   // The parent's 48-byte record (parent_records): the terms covered after
-  // some move, pattern ranks, and the child index and rotation (4 j + r) of
-  // every move.
-  const uint4 usub = ldg(rp), h = ldg(rp + 1), mw = ldg(rp + 2);
+  // some move (usub), pattern ranks, and the child index and rotation (4 j +
+  // r) of every move.
   const uint32_t mvw[5] = {h.y, h.z, h.w, mw.x, mw.y};
   const int nmoves = int(h.x >> 16 & 0xff);
   // super_wins of both sides, looked up by stone pattern
@@ -348,17 +351,39 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
     out[0] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
     out[1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
   }
-  if (!L.slice35)
+  if (!L.slice35 && tid < M * nc) {
+    // Each thread's next child is loaded while it transforms the current one.
+    const uint64_t* a = child_addr(L, S.ctx[tid / nc].G, tid % nc);
+    super8 cw = s_load_ldg(a), cn = s_load_ldg(a + 4);
     for (int x = tid; x < M * nc; x += nt) {
       const int k = x / nc, j = x - k * nc;
-      child_node(L, S.ctx[k].G, q_smem + 4 * k * nc, j);
+      const super8 w = cw, n = cn;
+      if (x + nt < M * nc) {
+        const int xn = x + nt;
+        const uint64_t* b = child_addr(L, S.ctx[xn / nc].G, xn % nc);
+        cw = s_load_ldg(b);
+        cn = s_load_ldg(b + 4);
+      }
+      child_node(L, S.ctx[k].G, q_smem + 4 * k * nc, j, w, n);
     }
+  }
   __syncthreads();
   unsigned errors = 0;
+  // Each thread's next record is loaded while it computes the current parent.
+  const uint4* recs = reinterpret_cast<const uint4*>(L.recs);
+  uint4 r0 = make_uint4(0, 0, 0, 0), r1 = r0, r2 = r0;
+  if (tid < M * np) {
+    const int i = tid % np;
+    r0 = ldg(recs + 3 * i); r1 = ldg(recs + 3 * i + 1); r2 = ldg(recs + 3 * i + 2);
+  }
   for (int x = tid; x < M * np; x += nt) {
     const int k = x / np, i = x - k * np;
-    parent_node<DIM>(L, S.ctx[k], S.tab[k][0], q_smem + 4 * k * nc, S.pat[k],
-                     reinterpret_cast<const uint4*>(L.recs + i), i, &errors);
+    const uint4 a = r0, b = r1, c = r2;
+    if (x + nt < M * np) {
+      const int in = (x + nt) % np;
+      r0 = ldg(recs + 3 * in); r1 = ldg(recs + 3 * in + 1); r2 = ldg(recs + 3 * in + 2);
+    }
+    parent_node<DIM>(L, S.ctx[k], S.tab[k][0], q_smem + 4 * k * nc, S.pat[k], a, b, c, i, &errors);
   }
   if (errors) record_errors(errors);
 }
@@ -367,13 +392,21 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
 template<int DIM>
 __global__ void __launch_bounds__(kLineThreads, 3)
 end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
-  const line_dev_t& L = lines[blockIdx.y];
-  const int nmicro = L.cross[0] * L.cross[1] * L.cross[2];
+  const line_dev_t& G = lines[blockIdx.y];
+  const int nmicro = G.cross[0] * G.cross[1] * G.cross[2];
   const int m0 = blockIdx.x * kMicro;
   if (m0 >= nmicro) return;
   const int M = min(kMicro, nmicro - m0);
+  // The descriptor is read throughout; shared memory keeps those reads short.
+  __shared__ __align__(16) line_dev_t L;
   __shared__ cta_smem S;
   extern __shared__ uint4 dyn_smem[];
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(&G);
+    uint4* dst = reinterpret_cast<uint4*>(&L);
+    for (int i = threadIdx.x; i < int(sizeof(line_dev_t) / 16); i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
   cta_microlines<DIM>(L, T, S, dyn_smem, m0, M, threadIdx.x, blockDim.x);
 }
 
@@ -402,9 +435,14 @@ template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_table
       }
     }
     if (!L.slice35)
-      for (int j = 0; j < L.nchild; j++) child_node(L, c.G, q.data(), j);
-    for (int i = 0; i < L.nparent; i++)
-      parent_node<DIM>(L, c, tab[0], q.data(), pat.data(), reinterpret_cast<const uint4*>(L.recs + i), i, &errors);
+      for (int j = 0; j < L.nchild; j++) {
+        const uint64_t* a = child_addr(L, c.G, j);
+        child_node(L, c.G, q.data(), j, s_load_ldg(a), s_load_ldg(a + 4));
+      }
+    for (int i = 0; i < L.nparent; i++) {
+      const uint4* rp = reinterpret_cast<const uint4*>(L.recs + i);
+      parent_node<DIM>(L, c, tab[0], q.data(), pat.data(), rp[0], rp[1], rp[2], i, &errors);
+    }
   }
   return errors;
 }
