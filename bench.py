@@ -106,10 +106,11 @@ def measured_hbm_peak():
 
 
 def profiled_traffic():
-    """DRAM bytes per launch of the line kernel from the committed ncu summary."""
+    """DRAM bytes (read + write) per parent node of the line kernel, measured by
+    ncu on this workload at full size and committed in the profile summary."""
     try:
         for line in open(PROFILE):
-            if line.startswith("traffic_bytes_per_node:"):
+            if line.startswith("dram_bytes_per_parent_node:"):
                 return float(line.split(":")[1])
     except OSError:
         pass
@@ -310,6 +311,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (traffic_per_node * out_nodes / 4) if traffic_per_node else None,
+                         "traffic_note": "dram read + write per launch (mean of the 4 dims), ncu at full size",
                          "algorithmic_bytes_per_step": alg_bytes, "kernel": "end_line_kernel",
                          "launches_per_step": 4},
             "cpu_baseline": cpu,

@@ -315,6 +315,9 @@ int pg_selftest_end_lines_host(const pg_line_t* lines, int n);  /* host buffers 
 const void* pg_selftest_table(const char* name, int* bytes);
 /* host out[n]; supers (optional, host): 19 x (win, notlose) halfsupers per board */
 int pg_selftest_midsolve_host(const uint64_t* raws, int n, pg_mid_values_t* out, uint64_t* supers);
+/* The same solve split into `groups` cooperating groups (one host thread
+ * each, a shared barrier between levels), as the multi-CTA kernel splits it. */
+int pg_selftest_midsolve_groups_host(const uint64_t* raws, int n, int groups, pg_mid_values_t* out);
 
 #ifdef __cplusplus
 }

@@ -21,7 +21,9 @@
 #include "mid_body.cuh"
 #include "runtime.h"
 #include <algorithm>
+#include <condition_variable>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 namespace pg {
@@ -37,7 +39,57 @@ mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict_
   if (threadIdx.x == 0) fault = 0;
   __syncthreads();
   const mid_tables MT = {c_choose, c_winpat, wf};
-  mid_board_body(J, MT, tiles, ws, raw, &fault, threadIdx.x, blockDim.x, sync_threads());
+  mid_board_body(J, MT, tiles, ws, raw, &fault, threadIdx.x, blockDim.x, 0, 1, sync_threads(), sync_threads());
+}
+
+// Barrier over the CTAs that solve one board together.  They are co-resident
+// (cooperative launch); the wait is bounded, and a timeout marks the board
+// as failed and turns every later barrier of that board into a no-op, so the
+// kernel always finishes.
+constexpr unsigned kBarrierPolls = 1u << 26;  // about 6 s of 64 ns sleeps
+
+struct board_barrier {
+  unsigned* count;  // arrivals in the current generation
+  unsigned* gen;    // generation number
+  int ncta;
+  int* fault;
+  __device__ void operator()() const {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      volatile unsigned* vg = gen;
+      volatile int* vf = fault;
+      const unsigned g = *vg;
+      __threadfence();
+      if (atomicAdd(count, 1u) == unsigned(ncta) - 1) {
+        atomicExch(count, 0u);
+        __threadfence();
+        atomicAdd(gen, 1u);
+      } else {
+        for (unsigned i = 0; *vg == g && !*vf; i++) {
+          if (i > kBarrierPolls) { atomicExch(fault, 1); break; }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+  }
+};
+
+// A few large boards: ncta CTAs per board (blockIdx.x / ncta), each taking a
+// contiguous share of every level.  bar: 2 words per board; raw: 38 uint4 per
+// board; faults: one per board; all zero at launch.
+__global__ void __launch_bounds__(kMidThreads)
+mid_board_grid_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict__ wf, int ncta, unsigned* bar,
+                      uint4* rawg, int* faults) {
+  const int board = blockIdx.x / ncta, cta = blockIdx.x % ncta;
+  const mid_job_t& J = jobs[board];
+  extern __shared__ uint4 smem[];
+  set0_info* tiles = reinterpret_cast<set0_info*>(smem);
+  const mid_tables MT = {c_choose, c_winpat, wf};
+  const board_barrier gb{bar + 2 * board, bar + 2 * board + 1, ncta, faults + board};
+  mid_board_body(J, MT, tiles, J.workspace, reinterpret_cast<uint4(*)[19]>(rawg + 38 * board), faults + board,
+                 int(threadIdx.x), int(blockDim.x), cta, ncta, sync_threads(), gb);
 }
 
 // ---------------------------------------------------------------------------
@@ -122,12 +174,43 @@ static int upload_consts() {
   static int attr = -1;
   if (attr < 0)
     attr = cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) == cudaSuccess
+                                int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) == cudaSuccess &&
+                   cudaFuncSetAttribute(mid_board_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        int(kMidThreads * sizeof(set0_info))) == cudaSuccess
                ? 0 : PG_ERR_CUDA;
   return attr;
 }
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// CTAs per board for the grid kernel: the co-resident CTAs of the device
+// shared evenly by the boards; 1 means one CTA per board (the batch kernel).
+static int grid_ctas_per_board(int boards, size_t smem) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mid_board_grid_kernel, kMidThreads, smem) != cudaSuccess)
+    return 1;
+  return std::max(1, sms * per_sm / std::max(boards, 1));
+}
+
+static int launch_grid_boards(const mid_job_t* jobs, int boards, int ncta, size_t smem, const uint32_t* wf,
+                              cudaStream_t stream) {
+  // Per board: barrier words, the n <= 1 results of both passes, a fault flag
+  const size_t bar_bytes = sizeof(unsigned) * 2 * boards, raw_bytes = sizeof(uint4) * 38 * boards;
+  char* aux = nullptr;
+  const size_t aux_bytes = align256(bar_bytes) + align256(raw_bytes) + align256(sizeof(int) * boards);
+  PG_CUDA(cudaMallocAsync((void**)&aux, aux_bytes, stream));
+  PG_CUDA(cudaMemsetAsync(aux, 0, aux_bytes, stream));
+  unsigned* bar = (unsigned*)aux;
+  uint4* rawg = (uint4*)(aux + align256(bar_bytes));
+  int* faults = (int*)(aux + align256(bar_bytes) + align256(raw_bytes));
+  void* args[] = {(void*)&jobs, (void*)&wf, (void*)&ncta, (void*)&bar, (void*)&rawg, (void*)&faults};
+  PG_CUDA(cudaLaunchCooperativeKernel((void*)mid_board_grid_kernel, dim3(unsigned(boards * ncta)), dim3(kMidThreads),
+                                      args, smem, stream));
+  PG_CUDA(cudaFreeAsync(aux, stream));
+  return PG_OK;
+}
 
 size_t scratch_bytes_of(const board_plan& P) {
   return align256(P.sets1p * 8) + align256(P.wins1 * 16) + align256(P.cs1ps * 2) +
@@ -208,8 +291,13 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     PG_CUDA(cudaMemcpyAsync(d, jobs.data(), sizeof(mid_job_t) * jobs.size(), cudaMemcpyHostToDevice, stream));
     const int smem_ws = pass == 0;
     const size_t smem = kMidThreads * sizeof(set0_info) + (smem_ws ? kSmemWorkspaceMax * 16 : 0);
-    mid_board_kernel<<<unsigned(jobs.size()), kMidThreads, smem, stream>>>(d, T->win_factors, smem_ws);
-    PG_CUDA(cudaGetLastError());
+    const int ncta = smem_ws ? 1 : grid_ctas_per_board(int(jobs.size()), smem);
+    if (ncta <= 1) {
+      mid_board_kernel<<<unsigned(jobs.size()), kMidThreads, smem, stream>>>(d, T->win_factors, smem_ws);
+      PG_CUDA(cudaGetLastError());
+    } else {
+      if (int rc = launch_grid_boards(d, int(jobs.size()), ncta, smem, T->win_factors, stream)) return rc;
+    }
     PG_CUDA(cudaFreeAsync(d, stream));
   }
   if (owned) PG_CUDA(cudaFreeAsync(base, stream));
@@ -241,8 +329,64 @@ extern "C" int pg_selftest_midsolve_host(const uint64_t* raws, int n, pg_mid_val
     memset(raw, 0, sizeof raw);
     int fault = 0;
     J.ws_size = int(P.workspace);
-    mid_board_body(J, MT, tiles.data(), ws.data(), raw, &fault, 0, 1, [] {},
+    mid_board_body(J, MT, tiles.data(), ws.data(), raw, &fault, 0, 1, 0, 1, [] {}, [] {},
                    supers ? reinterpret_cast<uint4*>(supers + 76 * size_t(i)) : nullptr);
+  }
+  return PG_OK;
+}
+
+namespace {
+struct host_barrier {
+  std::mutex m;
+  std::condition_variable cv;
+  int n, count = 0;
+  unsigned gen = 0;
+  explicit host_barrier(int n_) : n(n_) {}
+  void wait() {
+    std::unique_lock<std::mutex> lock(m);
+    const unsigned g = gen;
+    if (++count == n) {
+      count = 0;
+      gen++;
+      cv.notify_all();
+    } else {
+      cv.wait(lock, [&] { return gen != g; });
+    }
+  }
+};
+}  // namespace
+
+extern "C" int pg_selftest_midsolve_groups_host(const uint64_t* raws, int n, int groups, pg_mid_values_t* out) {
+  if (n < 0 || groups < 1 || groups > 64) return fail(PG_ERR_ARG, "bad arguments");
+  for (int k = 0; k <= 18; k++)
+    for (int j = 0; j <= 10; j++) h_choose[k][j] = uint32_t(hchoose(k, j));
+  const tables_t& T = tables();
+  const mid_tables MT = {h_choose, T.winpat, &T.win_factors[0][0][0]};
+  std::string err;
+  for (int i = 0; i < n; i++) {
+    board_plan P;
+    if (!plan_board(raws[i], P, err)) return fail(PG_ERR_ARG, err);
+    std::vector<uint64_t> sets1p(P.sets1p + 1);
+    std::vector<uint4> wins1(P.wins1 + 1), ws(P.workspace + 1);
+    std::vector<uint16_t> cs1ps(P.cs1ps + 1);
+    mid_job_t J = P.job;
+    J.sets1p = sets1p.data();
+    J.wins1 = wins1.data();
+    J.cs1ps = cs1ps.data();
+    J.workspace = ws.data();
+    J.out = out + i;
+    J.ws_size = int(P.workspace);
+    uint4 raw[2][19];
+    memset(raw, 0, sizeof raw);
+    int fault = 0;
+    host_barrier hb(groups);
+    std::vector<std::vector<set0_info>> tiles(groups, std::vector<set0_info>(kMidThreads));
+    std::vector<std::thread> threads;
+    for (int g = 0; g < groups; g++)
+      threads.emplace_back([&, g] {
+        mid_board_body(J, MT, tiles[g].data(), ws.data(), raw, &fault, 0, 1, g, groups, [] {}, [&] { hb.wait(); });
+      });
+    for (auto& t : threads) t.join();
   }
   return PG_OK;
 }

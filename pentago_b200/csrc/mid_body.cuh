@@ -270,34 +270,41 @@ PG_HD void traverse(const mid_job_t& J, const mid_tables& MT, const uint4* super
   append(out, board_of(side[0], side[1]) | uint64_t(ply & 1) << 63, value);
 }
 
-// The whole solve of one board by nt cooperating threads (tid = 0..nt-1).
-// `barrier` separates phases; run with nt = 1 and a no-op barrier it is the
-// same computation done sequentially (used by the CPU self-test).
-template<class Barrier>
+// The whole solve of one board by ncta groups of nt cooperating threads
+// (thread tid of group cta).  `barrier` synchronizes one group, `gbarrier`
+// all groups (with one group it is the same barrier).  Inside a level the
+// (s0, s1p) items are split into one contiguous range per group, and each
+// group builds the set0 rows of its own range; a level's output is read by
+// the next level only after the all-group barrier.  Run with one group of one
+// thread and no-op barriers it is the same computation done sequentially
+// (used by the CPU self-test).  `raw` and `fault` are shared by the groups.
+template<class Barrier, class GridBarrier>
 PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* tiles, uint4* ws,
-                          uint4 (*raw)[19], int* fault, int tid, int nt, Barrier barrier, uint4* dump = nullptr) {
+                          uint4 (*raw)[19], int* fault, int tid, int nt, int cta, int ncta, Barrier barrier,
+                          GridBarrier gbarrier, uint4* dump = nullptr) {
   const int spots = J.spots;
+  const int gtid = cta * nt + tid, gnt = ncta * nt;
   // Per-level tables, the same for both passes (midengine.cc:57-76, :101-107)
   for (int n = spots; n >= 0; n--) {
     const int k0 = n >> 1, k1 = n - k0;
     const int ns1p = choose_t(MT.choose, spots - k0, k1);
-    for (int i = tid; i < ns1p; i += nt) J.sets1p[J.sets1p_off[n] + i] = unrank(MT.choose, spots - k0, k1, i);
+    for (int i = gtid; i < ns1p; i += gnt) J.sets1p[J.sets1p_off[n] + i] = unrank(MT.choose, spots - k0, k1, i);
     const int ns1 = choose_t(MT.choose, spots, k1);
     const int parity = int((n + J.ply) & 1);
     const uint64_t root1 = J.side[(spots + n + 1) & 1];
-    for (int s = tid; s < ns1; s += nt) {
+    for (int s = gtid; s < ns1; s += gnt) {
       const uint64_t side1 = root1 | set_side(J.empty, k1, unrank(MT.choose, spots, k1, s));
       const super8 w = s_super_wins(MT.wf, side1);
       J.wins1[2 * (J.wins1_off[n] + s)] = h_to(s_split(w, parity));
       J.wins1[2 * (J.wins1_off[n] + s) + 1] = h_to(s_split(w, !parity));
     }
   }
-  barrier();
+  gbarrier();
   for (int n = spots; n >= 0; n--) {  // make_cs1ps (mid/internal.h:135-150)
     const int k0 = n >> 1, k1 = n - k0;
     const int ns1p = choose_t(MT.choose, spots - k0, k1);
     const uint64_t* sp = J.sets1p + J.sets1p_off[n];
-    for (int idx = tid; idx < ns1p * (spots - k0); idx += nt) {
+    for (int idx = gtid; idx < ns1p * (spots - k0); idx += gnt) {
       const int s1p = idx / (spots - k0), j = idx - s1p * (spots - k0);
       int c = s1p;
       for (int a = 0; a < k1; a++) {
@@ -307,7 +314,7 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
       J.cs1ps[J.cs1ps_off[n] + idx] = uint16_t(c);
     }
   }
-  barrier();
+  gbarrier();
 
   for (int aggressive = 0; aggressive < 2; aggressive++) {
     for (int n = spots; n >= 0; n--) {
@@ -315,27 +322,33 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
       const mid_grab gi = J.spaces[n + 1], go = J.spaces[n];
       const uint4* in = ws + gi.lo;
       uint4* out = ws + go.lo;
-      for (int base = 0; base < L.nsets0; base += kMidThreads) {
-        const int rows = L.nsets0 - base < kMidThreads ? L.nsets0 - base : kMidThreads;
+      // This group's items [i0, i1) and the set0 rows they touch
+      const int64_t total = int64_t(L.nsets0) * L.nsets1p;
+      const int64_t i0 = total * cta / ncta, i1 = total * (cta + 1) / ncta;
+      const int r0 = L.nsets1p ? int(i0 / L.nsets1p) : 0;
+      const int r1 = L.nsets1p && i1 > i0 ? int((i1 - 1) / L.nsets1p) + 1 : r0;
+      for (int base = r0; base < r1; base += kMidThreads) {
+        const int rows = r1 - base < kMidThreads ? r1 - base : kMidThreads;
         for (int r = tid; r < rows; r += nt) build_set0(J, MT, L, base + r, tiles[r]);
         barrier();
-        const int items = rows * L.nsets1p;
-        for (int it = tid; it < items; it += nt) {
-          const int r = it / L.nsets1p, s1p = it - r * L.nsets1p;
-          if (!inner(J, MT, L, tiles[r], s1p, aggressive, in, out, gi.ny, go.ny, J.ws_size - gi.lo,
+        const int64_t a = i0 > int64_t(base) * L.nsets1p ? i0 : int64_t(base) * L.nsets1p;
+        const int64_t b = i1 < int64_t(base + rows) * L.nsets1p ? i1 : int64_t(base + rows) * L.nsets1p;
+        for (int64_t it = a + tid; it < b; it += nt) {
+          const int row = int(it / L.nsets1p), s1p = int(it - int64_t(row) * L.nsets1p);
+          if (!inner(J, MT, L, tiles[row - base], s1p, aggressive, in, out, gi.ny, go.ny, J.ws_size - gi.lo,
                      J.ws_size - go.lo, raw[aggressive]))
             *fault = 1;
         }
         barrier();
       }
+      gbarrier();
     }
   }
 
   // Interleave (midengine.cc:119-124) and traverse; a failed bounds check
   // marks the record with size -1 instead.
-  barrier();
-  if (tid == 0 && *fault) { J.out->size = -1; J.out->pad = 0; }
-  if (tid == 0 && !*fault) {
+  if (gtid == 0 && *fault) { J.out->size = -1; J.out->pad = 0; }
+  if (gtid == 0 && !*fault) {
     uint4 supers[2 * 19];
     for (int i = 0; i < 19; i++)
       for (int j = 0; j < 2; j++) supers[2 * i + j] = raw[j ^ (i == 0)][i];

@@ -72,7 +72,8 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, const 
     __threadfence_system();
     mid_job_t J = E.job;
     uint4* ws = J.workspace ? J.workspace : smem_ws;
-    mid_board_body(J, MT, tiles, ws, raw, &fault, int(threadIdx.x), int(blockDim.x), sync_threads());
+    mid_board_body(J, MT, tiles, ws, raw, &fault, int(threadIdx.x), int(blockDim.x), 0, 1, sync_threads(),
+                   sync_threads());
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence_system();

@@ -67,6 +67,15 @@ def selftest_host(raws, supers=False):
     return (decode(out), sup) if supers else decode(out)
 
 
+def selftest_groups_host(raws, groups):
+    """The kernel's solve split into `groups` cooperating host threads (the
+    multi-CTA partition of every level).  Returns decoded values."""
+    raws = np.ascontiguousarray(raws, dtype=np.uint64)
+    out = np.zeros((len(raws), RECORD_BYTES), np.uint8)
+    capi.check(capi.lib().pg_selftest_midsolve_groups_host(capi.ptr(raws), len(raws), groups, capi.ptr(out)))
+    return decode(out)
+
+
 def midsolve(raws, stream=None):
     """Solve boards on the GPU and return [(raw, value), ...] per board."""
     out = values_device(raws, stream=stream)
