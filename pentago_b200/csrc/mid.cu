@@ -42,40 +42,6 @@ mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict_
   mid_board_body(J, MT, tiles, ws, raw, &fault, threadIdx.x, blockDim.x, 0, 1, sync_threads(), sync_threads());
 }
 
-// Barrier over the CTAs that solve one board together.  They are co-resident
-// (cooperative launch); the wait is bounded, and a timeout marks the board
-// as failed and turns every later barrier of that board into a no-op, so the
-// kernel always finishes.
-constexpr unsigned kBarrierPolls = 1u << 26;  // about 6 s of 64 ns sleeps
-
-struct board_barrier {
-  unsigned* count;  // arrivals in the current generation
-  unsigned* gen;    // generation number
-  int ncta;
-  int* fault;
-  __device__ void operator()() const {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      volatile unsigned* vg = gen;
-      volatile int* vf = fault;
-      const unsigned g = *vg;
-      __threadfence();
-      if (atomicAdd(count, 1u) == unsigned(ncta) - 1) {
-        atomicExch(count, 0u);
-        __threadfence();
-        atomicAdd(gen, 1u);
-      } else {
-        for (unsigned i = 0; *vg == g && !*vf; i++) {
-          if (i > kBarrierPolls) { atomicExch(fault, 1); break; }
-          __nanosleep(64);
-        }
-      }
-      __threadfence();
-    }
-    __syncthreads();
-  }
-};
-
 // A few large boards: ncta CTAs per board (blockIdx.x / ncta), each taking a
 // contiguous share of every level.  bar: 2 words per board; raw: 38 uint4 per
 // board; faults: one per board; all zero at launch.

@@ -365,6 +365,41 @@ static __constant__ uint64_t c_winpat[32];
 
 struct sync_threads { __device__ void operator()() const { __syncthreads(); } };
 
+// Barrier over the CTAs that solve one board together.  They are co-resident
+// (a cooperative launch, or workers of the persistent server); the wait is bounded, and a timeout marks the board
+// as failed and turns every later barrier of that board into a no-op, so the
+// kernel always finishes.
+constexpr unsigned kBarrierPolls = 1u << 28;  // about 20 s of 64 ns sleeps
+
+struct board_barrier {
+  unsigned* count;  // arrivals in the current generation
+  unsigned* gen;    // generation number
+  int ncta;
+  int* fault;
+  __device__ void operator()() const {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      volatile unsigned* vg = gen;
+      volatile int* vf = fault;
+      const unsigned g = *vg;
+      __threadfence();
+      if (atomicAdd(count, 1u) == unsigned(ncta) - 1) {
+        atomicExch(count, 0u);
+        __threadfence();
+        atomicAdd(gen, 1u);
+      } else {
+        for (unsigned i = 0; *vg == g && !*vf; i++) {
+          if (i > kBarrierPolls) { atomicExch(fault, 1); break; }
+          __nanosleep(64);
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+  }
+};
+
+
 // ---------------------------------------------------------------------------
 // Host helpers (mid.cu)
 // ---------------------------------------------------------------------------

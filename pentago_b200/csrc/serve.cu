@@ -17,6 +17,7 @@
 #include "mid_body.cuh"
 #include "runtime.h"
 #include "../../include/pentago_b200.h"
+#include <algorithm>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -30,9 +31,28 @@ enum : int { kRunning = 1, kIdleExit = 2, kClosed = 3, kFault = 4 };
 
 struct serve_entry {          // host-mapped
   mid_job_t job;              // planned board; job.out points into the result area
-  volatile int32_t done;      // 0 pending, 1 solved, -1 bounds failure
-  int32_t pad[3];
+  volatile int32_t done;      // 0 pending, 1 solved, -1 bounds failure (first entry of a request only)
+  int32_t gang;               // workers solving this request together (consecutive entries)
+  int32_t rank;               // this entry's worker within the gang
+  int32_t first;              // ring slot of the request's first entry
 };
+
+// Device state of a request solved by a gang of workers, per ring slot of
+// its first entry: barrier words, the n <= 1 results of both passes, the
+// fault flag.  Zero when idle; the gang leaves it zero again.
+struct gang_aux {
+  unsigned count, gen;
+  int fault, pad;
+  uint4 raw[2][19];
+};
+
+// Workers per request: boards with many empty spots are split over several
+// workers so that they finish in tens of milliseconds instead of seconds.
+static int gang_size(int spots, int workers) {
+  const int g = spots >= 18 ? 64 : spots == 17 ? 32 : spots == 16 ? 16 : spots == 15 ? 8 : spots == 14 ? 4
+              : spots == 13 ? 2 : 1;
+  return std::max(1, std::min(g, workers / 2));
+}
 
 struct serve_ctl {            // host-mapped
   volatile unsigned long long tail;   // entries published by the host
@@ -41,7 +61,8 @@ struct serve_ctl {            // host-mapped
 };
 
 __global__ void __launch_bounds__(kMidThreads, 1)
-serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, const uint32_t* __restrict__ wf) {
+serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_aux* aux,
+             const uint32_t* __restrict__ wf) {
   extern __shared__ uint4 smem[];
   set0_info* tiles = reinterpret_cast<set0_info*>(smem);
   uint4* smem_ws = smem + kMidThreads * sizeof(set0_info) / sizeof(uint4);
@@ -71,13 +92,29 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, const 
     serve_entry& E = ring[claimed % kRing];
     __threadfence_system();
     mid_job_t J = E.job;
-    uint4* ws = J.workspace ? J.workspace : smem_ws;
-    mid_board_body(J, MT, tiles, ws, raw, &fault, int(threadIdx.x), int(blockDim.x), 0, 1, sync_threads(),
-                   sync_threads());
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence_system();
-      E.done = fault ? -1 : 1;
+    const int gang = E.gang, rank = E.rank, first = E.first;
+    if (gang <= 1) {
+      uint4* ws = J.workspace ? J.workspace : smem_ws;
+      mid_board_body(J, MT, tiles, ws, raw, &fault, int(threadIdx.x), int(blockDim.x), 0, 1, sync_threads(),
+                     sync_threads());
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence_system();
+        E.done = fault ? -1 : 1;
+      }
+    } else {
+      // One share of a request split over `gang` workers; the entries of the
+      // gang are consecutive, so earlier requests never wait on later ones.
+      gang_aux& X = aux[first];
+      const board_barrier gb{&X.count, &X.gen, gang, &X.fault};
+      mid_board_body(J, MT, tiles, J.workspace, X.raw, &X.fault, int(threadIdx.x), int(blockDim.x), rank, gang,
+                     sync_threads(), gb);
+      __syncthreads();
+      if (rank == 0 && threadIdx.x == 0) {
+        const int f = atomicExch(&X.fault, 0);
+        __threadfence_system();
+        ring[first].done = f ? -1 : 1;
+      }
     }
     __syncthreads();
   }
@@ -121,9 +158,10 @@ struct server {
   serve_ctl* ctl = nullptr;           // mapped
   pg_mid_values_t* results = nullptr; // mapped, one per ring entry
   unsigned long long* head = nullptr; // device claim counter
+  gang_aux* aux = nullptr;            // device, one per ring slot
   arena A;
-  unsigned long long next = 0;        // next ticket
-  struct inflight { size_t off, bytes; bool live; };
+  unsigned long long next = 0;        // next ticket (ring entry)
+  struct inflight { size_t off, bytes; int gang; bool live; };
   std::vector<inflight> slots;        // per ring entry
   bool launched = false;
   int workers = 0;
@@ -135,7 +173,7 @@ static int launch_workers(server& S) {
   S.ctl->close = 0;
   S.ctl->status = kRunning;
   const size_t smem = kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16;
-  serve_kernel<<<S.workers, kMidThreads, smem, S.stream>>>(S.ring, S.ctl, S.head, T->win_factors);
+  serve_kernel<<<S.workers, kMidThreads, smem, S.stream>>>(S.ring, S.ctl, S.head, S.aux, T->win_factors);
   PG_CUDA(cudaGetLastError());
   S.launched = true;
   return PG_OK;
@@ -164,9 +202,11 @@ extern "C" int pg_serve_open(int64_t budget_bytes, pg_server_t* out) {
   char* base = nullptr;
   PG_CUDA(cudaMalloc(&base, size_t(budget_bytes)));
   S->A.init(base, size_t(budget_bytes));
-  S->slots.assign(kRing, server::inflight{0, 0, false});
+  S->slots.assign(kRing, server::inflight{0, 0, 1, false});
   PG_CUDA(cudaMalloc(&S->head, sizeof(unsigned long long)));
   PG_CUDA(cudaMemset(S->head, 0, sizeof(unsigned long long)));
+  PG_CUDA(cudaMalloc(&S->aux, sizeof(gang_aux) * kRing));
+  PG_CUDA(cudaMemset(S->aux, 0, sizeof(gang_aux) * kRing));
   *out = reinterpret_cast<pg_server_t>(S);
   return PG_OK;
 }
@@ -182,19 +222,27 @@ extern "C" int64_t pg_serve_submit(pg_server_t h, uint64_t raw) {
   if (!plan_board(raw, P, err)) return fail(PG_ERR_ARG, err);
   const unsigned long long ticket = S.next;
   const int slot = int(ticket % kRing);
-  if (S.slots[slot].live) return fail(PG_ERR_CAPACITY, "request ring full");
+  // Boards that keep their workspace in shared memory are one worker's job
+  const int gang = P.workspace > size_t(kSmemWorkspaceMax) ? gang_size(P.job.spots, S.workers) : 1;
+  for (int g = 0; g < gang; g++)
+    if (S.slots[(slot + g) % kRing].live) return fail(PG_ERR_CAPACITY, "request ring full");
   const size_t bytes = scratch_bytes_of(P);
   size_t off = 0;
   if (!S.A.alloc(bytes, off)) return fail(PG_ERR_CAPACITY, "scratch budget exhausted");
   carve_scratch(P, S.A.base + off);
   P.job.out = S.results + slot;
-  serve_entry& E = S.ring[slot];
-  E.done = 0;
-  E.job = P.job;
-  S.slots[slot] = server::inflight{off, bytes, true};
+  for (int g = 0; g < gang; g++) {
+    serve_entry& E = S.ring[(slot + g) % kRing];
+    E.done = 0;
+    E.job = P.job;
+    E.gang = gang;
+    E.rank = g;
+    E.first = slot;
+    S.slots[(slot + g) % kRing] = server::inflight{off, bytes, gang, true};
+  }
   std::atomic_thread_fence(std::memory_order_seq_cst);
-  S.next = ticket + 1;
-  S.ctl->tail = ticket + 1;
+  S.next = ticket + gang;
+  S.ctl->tail = ticket + gang;
   if (!S.launched || S.ctl->status != kRunning) {
     if (S.launched) cudaStreamSynchronize(S.stream);  // workers left after idling
     if (int rc = launch_workers(S)) return rc;
@@ -214,7 +262,8 @@ extern "C" int pg_serve_poll(pg_server_t h, int64_t ticket, pg_mid_values_t* res
   std::atomic_thread_fence(std::memory_order_acquire);
   if (result) memcpy(result, (const void*)(S.results + slot), sizeof(pg_mid_values_t));
   S.A.release(S.slots[slot].off, S.slots[slot].bytes);
-  S.slots[slot].live = false;
+  const int gang = S.slots[slot].gang;
+  for (int g = 0; g < gang; g++) S.slots[(slot + g) % kRing].live = false;
   return done > 0 ? 1 : fail(PG_ERR_BOUNDS, "midsolve bounds check failed");
 }
 
@@ -226,6 +275,7 @@ extern "C" int pg_serve_close(pg_server_t h) {
   cudaError_t e = cudaStreamSynchronize(S->stream);
   cudaFree(S->A.base);
   cudaFree(S->head);
+  cudaFree(S->aux);
   cudaFreeHost((void*)S->ring);
   cudaFreeHost((void*)S->ctl);
   cudaFreeHost(S->results);
