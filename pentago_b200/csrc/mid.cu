@@ -45,7 +45,7 @@ mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict_
 // A few large boards: ncta CTAs per board (blockIdx.x / ncta), each taking a
 // contiguous share of every level.  bar: 2 words per board; raw: 38 uint4 per
 // board; faults: one per board; all zero at launch.
-__global__ void __launch_bounds__(kMidThreads)
+__global__ void __launch_bounds__(kMidThreads, 3)
 mid_board_grid_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict__ wf, int ncta, unsigned* bar,
                       uint4* rawg, int* faults) {
   const int board = blockIdx.x / ncta, cta = blockIdx.x % ncta;
@@ -178,18 +178,18 @@ static int launch_grid_boards(const mid_job_t* jobs, int boards, int ncta, size_
   return PG_OK;
 }
 
-size_t scratch_bytes_of(const board_plan& P) {
+size_t scratch_bytes_of(const board_plan& P, bool global_ws) {
   return align256(P.sets1p * 8) + align256(P.wins1 * 16) + align256(P.cs1ps * 2) +
-         (P.workspace > size_t(kSmemWorkspaceMax) ? align256(P.workspace * 16) : 0);
+         (global_ws || P.workspace > size_t(kSmemWorkspaceMax) ? align256(P.workspace * 16) : 0);
 }
 
-void carve_scratch(board_plan& P, char* base) {
+void carve_scratch(board_plan& P, char* base, bool global_ws) {
   mid_job_t& J = P.job;
   size_t off = 0;
   J.sets1p = (uint64_t*)(base + off); off += align256(P.sets1p * 8);
   J.wins1 = (uint4*)(base + off); off += align256(P.wins1 * 16);
   J.cs1ps = (uint16_t*)(base + off); off += align256(P.cs1ps * 2);
-  J.workspace = P.workspace > size_t(kSmemWorkspaceMax) ? (uint4*)(base + off) : nullptr;
+  J.workspace = global_ws || P.workspace > size_t(kSmemWorkspaceMax) ? (uint4*)(base + off) : nullptr;
 }
 
 }  // namespace pg

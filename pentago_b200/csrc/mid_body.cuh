@@ -412,8 +412,11 @@ struct board_plan {
 int bottleneck(int spots);
 int hchoose(int n, int k);
 bool plan_board(uint64_t raw, board_plan& P, std::string& err);
-size_t scratch_bytes_of(const board_plan& P);  // device scratch the board needs
-void carve_scratch(board_plan& P, char* base);  // point the job's tables into base
+// Device scratch the board needs, and pointing the job's tables into it.  The
+// workspace is in global scratch when it does not fit shared memory, or
+// always with global_ws.
+size_t scratch_bytes_of(const board_plan& P, bool global_ws = false);
+void carve_scratch(board_plan& P, char* base, bool global_ws = false);
 
 // Upload this translation unit's constant tables (once per device).
 static int mid_prepare_device() {

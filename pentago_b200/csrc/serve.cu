@@ -47,10 +47,12 @@ struct gang_aux {
 };
 
 // Workers per request: boards with many empty spots are split over several
-// workers so that they finish in tens of milliseconds instead of seconds.
+// workers so that they finish in tens of milliseconds instead of seconds
+// (shares of the worker pool: 18 empty spots get 3/8 of it, each spot fewer
+// halves that, down to one worker).
 static int gang_size(int spots, int workers) {
-  const int g = spots >= 18 ? 64 : spots == 17 ? 32 : spots == 16 ? 16 : spots == 15 ? 8 : spots == 14 ? 4
-              : spots == 13 ? 2 : 1;
+  if (spots < 12) return 1;
+  const int g = int((int64_t(workers) * 3 / 8) >> (18 - std::min(spots, 18)));
   return std::max(1, std::min(g, workers / 2));
 }
 
@@ -60,12 +62,11 @@ struct serve_ctl {            // host-mapped
   volatile int32_t status;            // kRunning / kIdleExit / kClosed
 };
 
-__global__ void __launch_bounds__(kMidThreads, 1)
+__global__ void __launch_bounds__(kMidThreads, 2)
 serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_aux* aux,
              const uint32_t* __restrict__ wf) {
   extern __shared__ uint4 smem[];
   set0_info* tiles = reinterpret_cast<set0_info*>(smem);
-  uint4* smem_ws = smem + kMidThreads * sizeof(set0_info) / sizeof(uint4);
   __shared__ uint4 raw[2][19];
   __shared__ int fault;
   __shared__ long long claimed;
@@ -94,9 +95,8 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_a
     mid_job_t J = E.job;
     const int gang = E.gang, rank = E.rank, first = E.first;
     if (gang <= 1) {
-      uint4* ws = J.workspace ? J.workspace : smem_ws;
-      mid_board_body(J, MT, tiles, ws, raw, &fault, int(threadIdx.x), int(blockDim.x), 0, 1, sync_threads(),
-                     sync_threads());
+      mid_board_body(J, MT, tiles, J.workspace, raw, &fault, int(threadIdx.x), int(blockDim.x), 0, 1,
+                     sync_threads(), sync_threads());
       __syncthreads();
       if (threadIdx.x == 0) {
         __threadfence_system();
@@ -172,7 +172,7 @@ static int launch_workers(server& S) {
   if (!T) return PG_ERR_CUDA;
   S.ctl->close = 0;
   S.ctl->status = kRunning;
-  const size_t smem = kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16;
+  const size_t smem = kMidThreads * sizeof(set0_info);
   serve_kernel<<<S.workers, kMidThreads, smem, S.stream>>>(S.ring, S.ctl, S.head, S.aux, T->win_factors);
   PG_CUDA(cudaGetLastError());
   S.launched = true;
@@ -188,11 +188,15 @@ extern "C" int pg_serve_open(int64_t budget_bytes, pg_server_t* out) {
   if (int rc = mid_prepare_device()) return rc;
   auto* S = new server;
   PG_CUDA(cudaGetDevice(&S->device));
-  int sms = 0;
+  // Every worker's workspace is in the arena, so a worker needs only its set0
+  // tiles in shared memory and several workers share an SM.
+  int sms = 0, per_sm = 0;
   PG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, S->device));
-  S->workers = sms;
   PG_CUDA(cudaFuncSetAttribute(serve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)));
+                               int(kMidThreads * sizeof(set0_info))));
+  PG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, serve_kernel, kMidThreads,
+                                                        kMidThreads * sizeof(set0_info)));
+  S->workers = sms * std::max(1, per_sm);
   PG_CUDA(cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking));
   PG_CUDA(cudaHostAlloc((void**)&S->ring, sizeof(serve_entry) * kRing, cudaHostAllocMapped));
   PG_CUDA(cudaHostAlloc((void**)&S->ctl, sizeof(serve_ctl), cudaHostAllocMapped));
@@ -222,14 +226,13 @@ extern "C" int64_t pg_serve_submit(pg_server_t h, uint64_t raw) {
   if (!plan_board(raw, P, err)) return fail(PG_ERR_ARG, err);
   const unsigned long long ticket = S.next;
   const int slot = int(ticket % kRing);
-  // Boards that keep their workspace in shared memory are one worker's job
-  const int gang = P.workspace > size_t(kSmemWorkspaceMax) ? gang_size(P.job.spots, S.workers) : 1;
+  const int gang = gang_size(P.job.spots, S.workers);
   for (int g = 0; g < gang; g++)
     if (S.slots[(slot + g) % kRing].live) return fail(PG_ERR_CAPACITY, "request ring full");
-  const size_t bytes = scratch_bytes_of(P);
+  const size_t bytes = scratch_bytes_of(P, true);
   size_t off = 0;
   if (!S.A.alloc(bytes, off)) return fail(PG_ERR_CAPACITY, "scratch budget exhausted");
-  carve_scratch(P, S.A.base + off);
+  carve_scratch(P, S.A.base + off, true);
   P.job.out = S.results + slot;
   for (int g = 0; g < gang; g++) {
     serve_entry& E = S.ring[(slot + g) % kRing];
