@@ -69,7 +69,8 @@ def trained():
 def oracle_stream(O, model, ref, sym):
     blk = np.array(list(ref.block), np.int32)
     out = np.zeros(200 + 512 * (sym.size // 256), np.uint8)
-    n = O.lm_encode(P(np.frombuffer(model, np.uint8)), ref.section, P(blk), P(sym), P(out), out.size)
+    mbytes = np.frombuffer(model, np.uint8)
+    n = O.lm_encode(P(mbytes), ref.section, P(blk), P(sym), P(out), out.size)
     assert n > 0
     st = np.zeros(sym.size // 4 + 1000, np.uint8)
     m = O.rans_encode(P(sym), sym.size, P(st), st.size)
@@ -93,8 +94,10 @@ def test_freqs_match_oracle(cuda, O):
             want = np.zeros((k, 3), np.uint32)
             blk = np.array(list(refs[s].block), np.int32)
             local = np.ascontiguousarray(samples & 0xffffff)
-            assert O.lm_freqs(P(np.frombuffer(model, np.uint8)), refs[s].section, P(blk),
-                              P(np.ascontiguousarray(host[off[s]:off[s + 1]])), P(local), k, P(want)) == 0
+            # (arrays handed to the oracle by address are kept in variables while it runs)
+            mbytes = np.frombuffer(model, np.uint8)
+            block_sym = np.ascontiguousarray(host[off[s]:off[s + 1]])
+            assert O.lm_freqs(P(mbytes), refs[s].section, P(blk), P(block_sym), P(local), k, P(want)) == 0
             assert np.array_equal(got.astype(np.uint32), want)
 
 
@@ -125,7 +128,8 @@ def test_gradient_matches_oracle(cuda, O):
     g = g.cpu().numpy().astype(np.float64)
     want = np.zeros(learned.N_PARAMS)
     blk = np.array(list(refs[0].block), np.int32)
-    wl = O.lm_grad(P(params), refs[0].section, P(blk), P(sym.cpu().numpy()), P(local), k, P(want))
+    host = sym.cpu().numpy()
+    wl = O.lm_grad(P(params), refs[0].section, P(blk), P(host), P(local), k, P(want))
     assert abs(float(loss.item()) - wl) <= 1e-4 * abs(wl)
     scale = np.abs(want).max()
     assert np.abs(g - want).max() <= 2e-4 * scale
