@@ -117,9 +117,10 @@ def profiled_traffic():
     return None
 
 
-def cpu_reference_rate(seconds=12.0, threads=0):
+def cpu_reference_rate(seconds=12.0, threads=0, passes=None, warmup=0):
     """The reference's own CPU engine (oracle/_ref) on the four lines through
-    block (1,1,1,1) of the section, repeated for about `seconds`."""
+    block (1,1,1,1) of the section, repeated for about `seconds` (or exactly
+    `passes` times after `warmup` untimed passes)."""
     import ctypes
     import numpy as np
     from tests.oracle import reference, P
@@ -137,30 +138,45 @@ def cpu_reference_rate(seconds=12.0, threads=0):
         info = end.line_info(line)
         work.append((dim, line.length, (ctypes.c_uint8 * 3)(*bb), random_nodes(dim + 1, info.input_nodes),
                      np.zeros((info.output_nodes, 8), np.uint64)))
-    nodes = 0
-    t0 = time.perf_counter()
-    while True:
+    def one_pass():
+        n = 0
         for dim, length, bb, inp, out in work:
             R.compute_line(sig, dim, length, bb, P(inp), P(out), 0)
-            nodes += out.shape[0]
+            n += out.shape[0]
+        return n
+    for _ in range(warmup):
+        one_pass()
+    nodes = done = 0
+    t0 = time.perf_counter()
+    while True:
+        nodes += one_pass()
+        done += 1
         el = time.perf_counter() - t0
-        if el >= seconds:
+        if (passes is not None and done >= passes) or (passes is None and el >= seconds):
             break
-    return {"value": nodes * 256 / el, "unit": UNIT, "cores": nthreads, "kind": "reference",
-            "sample": f"4 block lines through block (1,1,1,1) of section {SECTION}, repeated for {el:.1f} s "
+    return {"value": nodes * 256 / el, "unit": UNIT, "cores": nthreads, "kind": "reference", "passes": done,
+            "ms_per_pass": 1e3 * el / done,
+            "sample": f"4 block lines through block (1,1,1,1) of section {SECTION}, {done} passes in {el:.1f} s "
                       f"({nodes} parent nodes), reference engine oracle/_ref on {nthreads} threads"}
 
 
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    r = cpu_reference_rate(seconds=max(5.0, 2.0 * args.steps))
+    # One step = one pass of the reference engine over the four lines through
+    # one block of the section (about 12 ms on 16 cores), so K steps stay short.
+    r = cpu_reference_rate(passes=max(1, args.steps), warmup=args.warmup)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
         return
     line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "impl": "reference", "dtype": "u64 bitsets",
-            "data": "synthetic", "config": {"workload": f"end block lines, section {SECTION}", "host_cpu": True},
+            "warmup": args.warmup, "ms_per_step": r["ms_per_pass"], "higher_is_better": True,
+            "impl": "reference", "dtype": "u64 bitsets",
+            "data": "synthetic",
+            "config": {"workload": f"end-engine block compute: 4 full block lines through each of {args.blocks} "
+                                   f"8^4 blocks of the 30-stone section {SECTION} per GPU",
+                       "reference_step": "the 4 lines through one block per step (the rate is per position)",
+                       "host_cpu": True},
             "cpu_baseline": r, "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                        "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
