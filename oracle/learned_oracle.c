@@ -5,11 +5,12 @@
  * format's own specification independently of the GPU code, so that a stream
  * written on the GPU decodes here and the bytes written here equal the GPU's:
  *
+ *   coding order of a node: 128 steps, step s codes rotation s then s + 128;
  *   features of symbol r of node i of a block (120 binary inputs):
  *     18 q + 2 c + colour    stone of colour (0 black, 1 white) on cell c of quadrant q
  *     72 + 4 q + i_q         rotation r = i0 + 4 i1 + 16 i2 + 64 i3
  *     88 + 4 n + v           neighbour n = 2 q + e (quadrant q turned +1 for e = 0,
- *                            +3 for e = 1): its symbol if it precedes r, else v = 3
+ *                            +3 for e = 1): its symbol if its step is earlier, else v = 3
  *   network: W1 (120 x 64), b1, W2 (64 x 64), b2, W3 (64 x 3), b3 as bf16;
  *     a1 = (node + (RA + RB)) + ((P0 + P1) + (P2 + P3)) with node = b1 + stone rows
  *     ascending, RA = row(72 + i0) + row(76 + i1), RB = row(80 + i2) + row(84 + i3),
@@ -19,7 +20,8 @@
  *     degree 7, f_c = 1 + trunc(e_c / (e0 + e1 + e2) * 32765), remainder to the
  *     first largest
  *   stream: version 3 | FNV-1a-64 of the model | nodes | words | 32 lane states |
- *     16-bit words; node i on lane i % 32; encoder steps (round, r) backward,
+ *     16-bit words; node i on lane i % 32; the encoder runs the decoder's
+ *     sequence (round, step, rotation s then s + 128) backward, and
  *     renormalizing lanes append x & 0xffff in lane order when x >= f << 17.
  */
 #include <math.h>
@@ -104,7 +106,7 @@ static int neighbour(int r, int n) {
 
 static int context(const uint8_t* sym, int r, int nb) {
   const int a = neighbour(r, nb);
-  return a < r ? (sym[a] & 3) : 3;
+  return (a & 127) < (r & 127) ? (sym[a] & 3) : 3;
 }
 
 typedef struct { float p[NP]; } model;
@@ -219,8 +221,9 @@ int64_t or_lm_encode(const uint8_t* model_bytes, uint64_t section, const int* bl
   for (int64_t round = rounds - 1; round >= 0; round--) {
     for (int l = 0; l < 32; l++)
       if (32 * round + l < n) node_sum(m, &g, 32 * round + l, node[l]);
-    for (int r = 255; r >= 0; r--)
+    for (int t = 255; t >= 0; t--)
       for (int l = 0; l < 32; l++) {
+        const int r = (t >> 1) + 128 * (t & 1);  /* decoder sequence t: step t / 2, half t % 2 */
         const int64_t i = 32 * round + l;
         if (i >= n) continue;
         const uint8_t* sym = symbols + 256 * i;
@@ -273,7 +276,8 @@ int64_t or_lm_decode(const uint8_t* model_bytes, uint64_t section, const int* bl
   for (int64_t round = 0; round < rounds; round++) {
     for (int l = 0; l < 32; l++)
       if (32 * round + l < n) node_sum(m, &g, 32 * round + l, node[l]);
-    for (int r = 0; r < 256; r++) {
+    for (int t = 0; t < 256; t++) {
+      const int r = (t >> 1) + 128 * (t & 1);
       int need[32], k = 0;
       for (int l = 0; l < 32; l++) {
         const int64_t i = 32 * round + l;

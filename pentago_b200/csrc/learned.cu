@@ -116,11 +116,75 @@ __device__ __forceinline__ void lm_logits(const lm_tables& S, const float* node,
   }
 }
 
+// Logits of the two symbols of step s (rotations s and s + 128) of one node,
+// whose node sums are node[k * 32] (the lane's column of its warp's block).
+// Each logit follows the order of learned.cuh exactly; the pair shares the
+// node sums, the RA lookup and the W2 rows.
+__device__ __forceinline__ void lm_logits2(const lm_tables& S, const float* node, int s, const int* uA,
+                                           const int* uB, float* zA, float* zB) {
+  const int ua = s & 15, ubA = s >> 4, ubB = ubA + 8;
+  float a2A[kLmHidden], a2B[kLmHidden];
+#pragma unroll
+  for (int j = 0; j < kLmHidden; j++) { a2A[j] = S.b2[j]; a2B[j] = S.b2[j]; }
+#pragma unroll 4
+  for (int k = 0; k < kLmHidden; k++) {
+    const float nk = node[32 * k], ra = S.ra[k][ua];
+    const float ctxA = f_add(f_add(S.pt[0][k][uA[0]], S.pt[1][k][uA[1]]), f_add(S.pt[2][k][uA[2]], S.pt[3][k][uA[3]]));
+    const float ctxB = f_add(f_add(S.pt[0][k][uB[0]], S.pt[1][k][uB[1]]), f_add(S.pt[2][k][uB[2]], S.pt[3][k][uB[3]]));
+    const float hA = relu(f_add(f_add(nk, f_add(ra, S.rb[k][ubA])), ctxA));
+    const float hB = relu(f_add(f_add(nk, f_add(ra, S.rb[k][ubB])), ctxB));
+    const float4* w = reinterpret_cast<const float4*>(S.w2[k]);
+#pragma unroll
+    for (int j4 = 0; j4 < kLmHidden / 4; j4++) {
+      const float4 v = w[j4];
+      a2A[4 * j4 + 0] = f_fma(v.x, hA, a2A[4 * j4 + 0]);
+      a2A[4 * j4 + 1] = f_fma(v.y, hA, a2A[4 * j4 + 1]);
+      a2A[4 * j4 + 2] = f_fma(v.z, hA, a2A[4 * j4 + 2]);
+      a2A[4 * j4 + 3] = f_fma(v.w, hA, a2A[4 * j4 + 3]);
+      a2B[4 * j4 + 0] = f_fma(v.x, hB, a2B[4 * j4 + 0]);
+      a2B[4 * j4 + 1] = f_fma(v.y, hB, a2B[4 * j4 + 1]);
+      a2B[4 * j4 + 2] = f_fma(v.z, hB, a2B[4 * j4 + 2]);
+      a2B[4 * j4 + 3] = f_fma(v.w, hB, a2B[4 * j4 + 3]);
+    }
+  }
+  zA[0] = zB[0] = S.b3[0];
+  zA[1] = zB[1] = S.b3[1];
+  zA[2] = zB[2] = S.b3[2];
+#pragma unroll
+  for (int j = 0; j < kLmHidden; j++) {
+    const float4 v = *reinterpret_cast<const float4*>(S.w3[j]);
+    const float hA = relu(a2A[j]), hB = relu(a2B[j]);
+    zA[0] = f_fma(v.x, hA, zA[0]);
+    zA[1] = f_fma(v.y, hA, zA[1]);
+    zA[2] = f_fma(v.z, hA, zA[2]);
+    zB[0] = f_fma(v.x, hB, zB[0]);
+    zB[1] = f_fma(v.y, hB, zB[1]);
+    zB[2] = f_fma(v.z, hB, zB[2]);
+  }
+}
+
+// node[k * 32] = b1[k] + stone rows ascending, for this lane's node.
+__device__ __forceinline__ void lm_node_store(const lm_tables& S, const uint8_t* feats, int nf, float* node) {
+#pragma unroll
+  for (int kc = 0; kc < kLmHidden; kc += 16) {
+    float acc[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) acc[i] = S.b1[kc + i];
+    for (int f = 0; f < nf; f++) {
+      const float* row = S.w1s + feats[f] * kW1Pad + kc;
+#pragma unroll
+      for (int i = 0; i < 16; i++) acc[i] = f_add(acc[i], row[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 16; i++) node[32 * (kc + i)] = acc[i];
+  }
+}
+
 __device__ __forceinline__ void lm_context_clamped(const uint8_t* sym, int r, int* u) {
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int a = lm_neighbour(r, 2 * q), b = lm_neighbour(r, 2 * q + 1);
-    const int va = a < r ? (sym[a] & 3) : 3, vb = b < r ? (sym[b] & 3) : 3;
+    const int va = lm_before(a, r) ? (sym[a] & 3) : 3, vb = lm_before(b, r) ? (sym[b] & 3) : 3;
     u[q] = va + 4 * vb;
   }
 }
@@ -138,6 +202,44 @@ __device__ __forceinline__ uint32_t get32(const uint8_t* p) {
   return uint32_t(p[0]) | uint32_t(p[1]) << 8 | uint32_t(p[2]) << 16 | uint32_t(p[3]) << 24;
 }
 
+// Dynamic shared memory of the coding kernels: the tables, then each warp's
+// node sums (64 x 32 floats, one column per lane).
+constexpr size_t kLmNodeFloats = kLmHidden * 32;
+constexpr size_t kLmCodeSmem = sizeof(lm_tables) + sizeof(float) * kLmNodeFloats * kLmWarps;
+
+// Append one 16-bit word per renormalizing lane, in lane order (encoder).
+__device__ __forceinline__ void lm_put_state(uint32_t& x, const lm_freq_t& F, int v, bool active, uint8_t* words,
+                                             uint32_t& len, unsigned below) {
+  const bool emit = active && x >= (F.f[v] << 17);
+  const unsigned mask = __ballot_sync(0xffffffffu, emit);
+  if (emit) {
+    put16(words + 2 * (len + __popc(mask & below)), uint16_t(x));
+    x >>= 16;
+  }
+  len += __popc(mask);
+  if (active) x = ((x / F.f[v]) << kLmProbBits) + x % F.f[v] + F.cum[v];
+}
+
+// Decode one symbol per active lane and take this step's words (decoder).
+__device__ __forceinline__ int lm_get_symbol(uint32_t& x, const lm_freq_t& F, bool active, const uint8_t* words,
+                                             int64_t& ptr, unsigned above, int& bad) {
+  int v = 0;
+  if (active) {
+    const uint32_t slot = x & (kLmProbTotal - 1);
+    v = slot < F.cum[1] ? 0 : slot < F.cum[2] ? 1 : 2;
+    x = F.f[v] * (x >> kLmProbBits) + slot - F.cum[v];
+  }
+  const bool need = active && x < kLmLower;
+  const unsigned mask = __ballot_sync(0xffffffffu, need);
+  const int64_t at = ptr - 1 - __popc(mask & above);
+  if (need) {
+    if (at >= 0) x = (x << 16) | get16(words + 2 * at);
+    else bad = 1;
+  }
+  ptr -= __popc(mask);
+  return v;
+}
+
 // One warp per stream (grid-stride over streams).  sizes[s] = stream bytes, or
 // PG_ERR_ARG for a symbol above 2 or a symbol count that does not match.
 __global__ void __launch_bounds__(kLmThreads)
@@ -148,9 +250,10 @@ lm_encode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
   lm_tables& S = *reinterpret_cast<lm_tables*>(lm_smem_raw);
   lm_build_tables(S, P, threadIdx.x, blockDim.x);
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* node = reinterpret_cast<float*>(lm_smem_raw + sizeof(lm_tables)) + kLmNodeFloats * warp + lane;
   const unsigned below = (1u << lane) - 1;
-  for (int s = blockIdx.x * kLmWarps + (threadIdx.x >> 5); s < nstreams; s += gridDim.x * kLmWarps) {
+  for (int s = blockIdx.x * kLmWarps + warp; s < nstreams; s += gridDim.x * kLmWarps) {
     const lm_block_t B = blocks[s];
     const int64_t n = B.nodes;
     uint8_t* base = out + out_offsets[s];
@@ -167,31 +270,29 @@ lm_encode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
     for (int64_t round = rounds - 1; round >= 0; round--) {
       const int64_t i = 32 * round + lane;
       const bool active = i < n;
-      float node[kLmHidden];
       uint8_t feats[36];
       const int nf = active ? lm_load_node(B, i, T, feats) : 0;
-      lm_node_sum(S, feats, nf, node);
+      lm_node_store(S, feats, nf, node);
       const uint8_t* sym = sym0 + 256 * (active ? i : 0);
-      for (int r = 255; r >= 0; r--) {
-        lm_freq_t F = {};
-        int v = 0;
+      for (int st = 127; st >= 0; st--) {
+        lm_freq_t FA = {}, FB = {};
+        int vA = 0, vB = 0;
         if (active) {
-          int u[4];
-          lm_context_clamped(sym, r, u);
-          float z[3];
-          lm_logits(S, node, r, u, z);
-          F = lm_freqs(z);
-          v = sym[r];
-          if (v > 2) { bad = 1; v = 0; }
+          int uA[4], uB[4];
+          lm_context_clamped(sym, st, uA);
+          lm_context_clamped(sym, st + 128, uB);
+          float zA[3], zB[3];
+          lm_logits2(S, node, st, uA, uB, zA, zB);
+          FA = lm_freqs(zA);
+          FB = lm_freqs(zB);
+          vA = sym[st];
+          vB = sym[st + 128];
+          if (vA > 2) { bad = 1; vA = 0; }
+          if (vB > 2) { bad = 1; vB = 0; }
         }
-        const bool emit = active && x >= (F.f[v] << 17);
-        const unsigned mask = __ballot_sync(0xffffffffu, emit);
-        if (emit) {
-          put16(words + 2 * (len + __popc(mask & below)), uint16_t(x));
-          x >>= 16;
-        }
-        len += __popc(mask);
-        if (active) x = ((x / F.f[v]) << kLmProbBits) + x % F.f[v] + F.cum[v];
+        // the decoder takes s then s + 128, so the encoder puts s + 128 first
+        lm_put_state(x, FB, vB, active, words, len, below);
+        lm_put_state(x, FA, vA, active, words, len, below);
       }
     }
     put32(base + 20 + 4 * lane, x);
@@ -220,9 +321,10 @@ lm_decode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
   lm_tables& S = *reinterpret_cast<lm_tables*>(lm_smem_raw);
   lm_build_tables(S, P, threadIdx.x, blockDim.x);
   __syncthreads();
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float* node = reinterpret_cast<float*>(lm_smem_raw + sizeof(lm_tables)) + kLmNodeFloats * warp + lane;
   const unsigned above = lane == 31 ? 0u : ~0u << (lane + 1);
-  for (int s = blockIdx.x * kLmWarps + (threadIdx.x >> 5); s < nstreams; s += gridDim.x * kLmWarps) {
+  for (int s = blockIdx.x * kLmWarps + warp; s < nstreams; s += gridDim.x * kLmWarps) {
     const lm_block_t B = blocks[s];
     const int64_t n = B.nodes;
     const uint8_t* base = in + in_offsets[s];
@@ -250,31 +352,27 @@ lm_decode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
     for (int64_t round = 0; round < rounds; round++) {
       const int64_t i = 32 * round + lane;
       const bool active = i < n;
-      float node[kLmHidden];
       uint8_t feats[36];
       const int nf = active ? lm_load_node(B, i, T, feats) : 0;
-      lm_node_sum(S, feats, nf, node);
+      lm_node_store(S, feats, nf, node);
       uint8_t* sym = out0 + 256 * (active ? i : 0);
-      for (int r = 0; r < 256; r++) {
+      for (int st = 0; st < 128; st++) {
+        lm_freq_t FA = {}, FB = {};
         if (active) {
-          int u[4];
-          lm_context_clamped(sym, r, u);
-          float z[3];
-          lm_logits(S, node, r, u, z);
-          const lm_freq_t F = lm_freqs(z);
-          const uint32_t slot = x & (kLmProbTotal - 1);
-          const int v = slot < F.cum[1] ? 0 : slot < F.cum[2] ? 1 : 2;
-          x = F.f[v] * (x >> kLmProbBits) + slot - F.cum[v];
-          sym[r] = uint8_t(v);
+          int uA[4], uB[4];
+          lm_context_clamped(sym, st, uA);
+          lm_context_clamped(sym, st + 128, uB);
+          float zA[3], zB[3];
+          lm_logits2(S, node, st, uA, uB, zA, zB);
+          FA = lm_freqs(zA);
+          FB = lm_freqs(zB);
         }
-        const bool need = active && x < kLmLower;
-        const unsigned mask = __ballot_sync(0xffffffffu, need);
-        const int64_t at = ptr - 1 - __popc(mask & above);
-        if (need) {
-          if (at >= 0) x = (x << 16) | get16(words + 2 * at);
-          else bad = 1;
+        const int vA = lm_get_symbol(x, FA, active, words, ptr, above, bad);
+        const int vB = lm_get_symbol(x, FB, active, words, ptr, above, bad);
+        if (active) {
+          sym[st] = uint8_t(vA);
+          sym[st + 128] = uint8_t(vB);
         }
-        ptr -= __popc(mask);
       }
     }
     // A well-formed stream ends with every word read and every lane back at
@@ -395,7 +493,7 @@ lm_grad_kernel(const float* __restrict__ params, const lm_block_t* __restrict__ 
           for (int q = 0; q < 4; q++) G.feats[tid][nf++] = uint8_t(kLmRot + 4 * q + ((r >> (2 * q)) & 3));
           for (int nb = 0; nb < 8; nb++) {
             const int a = lm_neighbour(r, nb);
-            G.feats[tid][nf++] = uint8_t(kLmCtx + 4 * nb + (a < r ? (sym[a] & 3) : 3));
+            G.feats[tid][nf++] = uint8_t(kLmCtx + 4 * nb + (lm_before(a, r) ? (sym[a] & 3) : 3));
           }
         }
       }
@@ -664,8 +762,8 @@ extern "C" int pg_rans_learned_encode(const uint8_t* model, const pg_block_ref_t
   lm_launch L;
   std::vector<lm_block_t> hb;
   if (int rc = lm_prepare(model, blocks, nstreams, st, L, &hb)) return rc;
-  if (int rc = lm_smem_opt_in(lm_encode_kernel, sizeof(lm_tables))) return rc;
-  lm_encode_kernel<<<lm_grid(nstreams), kLmThreads, sizeof(lm_tables), st>>>(L.params, L.hash, L.blocks, nstreams,
+  if (int rc = lm_smem_opt_in(lm_encode_kernel, kLmCodeSmem)) return rc;
+  lm_encode_kernel<<<lm_grid(nstreams), kLmThreads, kLmCodeSmem, st>>>(L.params, L.hash, L.blocks, nstreams,
                                                                               symbols, offsets, out, out_offsets,
                                                                               sizes, *T);
   PG_CUDA(cudaGetLastError());
@@ -707,8 +805,8 @@ extern "C" int pg_rans_learned_decode(const uint8_t* model, const pg_block_ref_t
   if (int rc = lm_prepare(model, blocks, nstreams, st, L)) return rc;
   if (int rc = launch_rans_decode(in, in_offsets, in_sizes, nstreams, symbols, sym_offsets, sym_caps, status, 1, st))
     return rc;
-  if (int rc = lm_smem_opt_in(lm_decode_kernel, sizeof(lm_tables))) return rc;
-  lm_decode_kernel<<<lm_grid(nstreams), kLmThreads, sizeof(lm_tables), st>>>(L.params, L.hash, L.blocks, nstreams, in,
+  if (int rc = lm_smem_opt_in(lm_decode_kernel, kLmCodeSmem)) return rc;
+  lm_decode_kernel<<<lm_grid(nstreams), kLmThreads, kLmCodeSmem, st>>>(L.params, L.hash, L.blocks, nstreams, in,
                                                                               in_offsets, in_sizes, symbols,
                                                                               sym_offsets, sym_caps, status, *T);
   PG_CUDA(cudaGetLastError());

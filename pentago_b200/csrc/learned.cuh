@@ -4,15 +4,16 @@
 //
 // Symbols are the on-disk ternaries of a block, 256 per node in rotation order
 // r = i0 + 4 i1 + 16 i2 + 64 i3 (shard/shard.cc:448-449).  A node's symbols are
-// coded in that order, and the probability of symbol r comes from a 3-layer
-// MLP (hidden 64, bf16 weights, fp32 arithmetic) over 120 binary features:
+// coded in 128 steps; step s codes rotations s and s + 128 (i3 two apart, so
+// never neighbours).  The probability of symbol r comes from a 3-layer MLP
+// (hidden 64, bf16 weights, fp32 arithmetic) over 120 binary features:
 //
 //   0..71    stones of the node's board: 18 q + 2 c + colour (colour 0 black,
 //            1 white) for cell c of quadrant q;
 //   72..87   rotation: 72 + 4 q + i_q;
 //   88..119  the 8 neighbouring rotations (i_q + 1 and i_q + 3 in quadrant q,
 //            neighbour n = 2 q + (0 | 1)): 88 + 4 n + v, v = that rotation's
-//            symbol if it precedes r, else 3.
+//            symbol if it was coded in an earlier step, else 3.
 //
 // Encoder and decoder must derive identical integer frequencies, so every
 // float operation on the coding path is a separately rounded IEEE operation
@@ -56,7 +57,9 @@ constexpr uint32_t kLmProbBits = 15, kLmProbTotal = 1u << kLmProbBits;
 constexpr uint32_t kLmLower = 1u << 16;
 constexpr int kLmLanes = 32;
 constexpr uint32_t kLmVersion = 3;
-// Stream: version u32 | model hash u64 | nodes u32 | words u32 | 32 lane states u32 | words u16
+// Stream: version u32 | model hash u64 | nodes u32 | words u32 | 32 lane states u32 | words u16.
+// Node i is coded by lane i % 32; a lane codes its nodes in order, each node
+// step by step (rotation s, then s + 128).
 constexpr int kLmStreamHeader = 20 + 4 * kLmLanes;
 
 PG_HD float f_add(float a, float b) {
@@ -200,11 +203,14 @@ PG_HD int lm_node_features(const uint16_t* qid, const uint16_t* unpack, uint8_t*
   return n;
 }
 
+// Rotation a was coded in an earlier step than rotation r.
+PG_HD bool lm_before(int a, int r) { return (a & 127) < (r & 127); }
+
 // Context of symbol r: per quadrant axis q, u_q = v_{2q} + 4 v_{2q+1}.
 PG_HD void lm_context(const uint8_t* sym, int r, int* u) {
   for (int q = 0; q < 4; q++) {
     const int a = lm_neighbour(r, 2 * q), b = lm_neighbour(r, 2 * q + 1);
-    const int va = a < r ? sym[a] : 3, vb = b < r ? sym[b] : 3;
+    const int va = lm_before(a, r) ? sym[a] : 3, vb = lm_before(b, r) ? sym[b] : 3;
     u[q] = va + 4 * vb;
   }
 }
