@@ -38,13 +38,29 @@ def block_of(i):
     return (i % 20, (7 * i + 3) % 20, (11 * i + 5) % 39, (13 * i + 1) % 39)
 
 
+def rank_blocks(blocks, rank):
+    """The blocks rank `rank` computes: its own `blocks` consecutive benchmark
+    blocks, disjoint from every other rank's (weak scaling, no exchange)."""
+    return [block_of(rank * blocks + t) for t in range(blocks)]
+
+
+def max_over_ranks(x, world, device):
+    """The slowest rank's time (all ranks take part)."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def plan_lines(blocks, rank):
     """Line descriptors (without buffers) for this rank's blocks."""
     from pentago_b200 import end
     sig = end.section_sig(SECTION)
     lines = []
-    for t in range(blocks):
-        b = block_of(rank * blocks + t)
+    for t, b in enumerate(rank_blocks(blocks, rank)):
         for dim in range(4):
             bb = tuple(b[i] for i in range(4) if i != dim)
             line = end.Line(sig, dim, bb)
@@ -243,12 +259,8 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def slowest(x):
+        return max_over_ranks(x, world, dev)
 
     # Device-resident timing (value + roofline)
     for _ in range(args.warmup):
@@ -269,7 +281,7 @@ def main():
         t_stop.record(stream)
         barrier()
     end.check_errors(stream)
-    elapsed_ms = max_over_ranks(t_start.elapsed_time(t_stop))
+    elapsed_ms = slowest(t_start.elapsed_time(t_stop))
     kernel_ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops)) / args.steps
     units_all = out_nodes * 256 * args.steps * world
     value = units_all / (elapsed_ms / 1e3)
@@ -294,7 +306,7 @@ def main():
         e2e_step()
     e_stop.record(stream)
     barrier()
-    e2e_ms = max_over_ranks(e_start.elapsed_time(e_stop))
+    e2e_ms = slowest(e_start.elapsed_time(e_stop))
     e2e_value = out_nodes * 256 * e2e_steps * world / (e2e_ms / 1e3)
 
     peak, peak_kind = measured_hbm_peak()
