@@ -97,7 +97,10 @@ def main():
     args = ap.parse_args()
     c = [int(x) for x in args.root.split(",")]
     root = section_sig([[c[0], c[1]], [c[2], c[3]], [c[4], c[5]], [c[6], c[7]]])
+    import torch
     capi.check(capi.lib().pg_init())
+    torch.zeros(1, device="cuda")  # torch's own CUDA set-up, outside the timed sweep
+    torch.cuda.synchronize()
     timings = {}
     t = time.perf_counter()
     res = sweep(root, args.min_slice, timings=timings)
