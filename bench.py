@@ -176,6 +176,116 @@ def cpu_reference_rate(seconds=12.0, threads=0, passes=None, warmup=0):
                       f"({nodes} parent nodes), reference engine oracle/_ref on {nthreads} threads"}
 
 
+CONFIG2_ROOT = [[4, 4], [4, 5], [4, 3], [3, 3]]
+
+
+def cpu_midsolve_rate(raws, positions, seconds=8.0):
+    """The reference's midsolve (oracle/_ref) on the host cores, one board per thread."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    from tests.oracle import reference, P
+    R = reference()
+    if R is None:
+        return None
+    threads = os.cpu_count() or 1
+
+    def solve(raw):
+        rr, vv = np.zeros(200, np.uint64), np.zeros(200, np.int32)
+        R.midsolve(int(raw), P(rr), P(vv))
+    boards = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        while time.perf_counter() - t0 < seconds:
+            list(ex.map(solve, raws))
+            boards += len(raws)
+    el = time.perf_counter() - t0
+    return {"value": boards / len(raws) * positions / el, "unit": "positions/s", "boards_per_s": boards / el,
+            "cores": threads, "kind": "reference",
+            "sample": f"the same {len(raws)} boards, repeated for {el:.1f} s, one board per thread"}
+
+
+def cpu_static_coder_rate(symbols, offsets, seconds=5.0):
+    """The reference's format-2 encoder (oracle/_ref) on the host cores, one block per thread."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+    from tests.oracle import reference, P
+    R = reference()
+    if R is None:
+        return None
+    blocks = [np.ascontiguousarray(symbols[offsets[i]:offsets[i + 1]]) for i in range(len(offsets) - 1)]
+    threads = os.cpu_count() or 1
+
+    def enc(b):
+        out = np.zeros(b.size // 2 + 4096, np.uint8)
+        return R.rans_encode(P(b), b.size, P(out), out.size)
+    done = 0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(threads) as ex:
+        while time.perf_counter() - t0 < seconds:
+            list(ex.map(enc, blocks))
+            done += sum(b.size for b in blocks)
+    el = time.perf_counter() - t0
+    return {"encode_Msym_per_s": done / el / 1e6, "cores": threads, "kind": "reference",
+            "sample": f"{len(blocks)} blocks' symbols, format-2 encode repeated for {el:.1f} s"}
+
+
+def sweep_summary(timings, wall_s):
+    """Config 2 from the per-slice timings of the sweep (slices 35 -> 30)."""
+    ms = sum(v["ms"] for v in timings.values())
+    nbytes = sum(64 * (v["nodes"] + v["child_nodes"]) for v in timings.values())
+    sections = sum(v["sections"] for v in timings.values())
+    return {"workload": f"all sections below root {CONFIG2_ROOT}, slices 35 -> 30, in HBM",
+            "sections": sections, "nodes": sum(v["nodes"] for v in timings.values()), "kernel_ms": ms,
+            "wall_s": wall_s, "sections_per_s": sections / (ms / 1e3),
+            "algorithmic_GBps": nbytes / (ms / 1e3) / 1e9}
+
+
+def cpu_sweep_estimate(root_counts, timings, seconds_per_slice=1.5):
+    """The reference engine's time for the same sweep, estimated on the host
+    cores: per slice, the four block lines through the first block of the
+    slice's largest section are timed on all threads (parent nodes per second),
+    and every section's nodes times its non-full dimensions are charged at
+    that rate (the slices do not fit host memory, 141.7 GB at the peak)."""
+    import ctypes
+    import numpy as np
+    from tests.oracle import reference, P
+    from pentago_b200 import end, sweep
+    from pentago_b200.synthetic import random_nodes
+    R = reference()
+    if R is None:
+        return None
+    nthreads = R.lib.ref_threads(0)
+    root = end.section_sig(root_counts)
+    total_s, per_slice = 0.0, {}
+    for slice_ in sorted(timings):
+        sigs = [int(x) for x in sweep.descendent_sections(root, slice_)]
+        work = 0
+        for sig in sigs:
+            counts = [[(sig >> (16 * q + 8 * k)) & 255 for k in range(2)] for q in range(4)]
+            dims = [d for d in range(4) if sum(counts[d]) < 9]
+            work += int(np.prod(end.section_shape(sig))) * len(dims)
+        big = max(sigs, key=lambda s: int(np.prod(end.section_shape(s))))
+        counts = [[(big >> (16 * q + 8 * k)) & 255 for k in range(2)] for q in range(4)]
+        lines = []
+        for dim in (d for d in range(4) if sum(counts[d]) < 9):
+            line = end.Line(big, dim, (0, 0, 0))
+            info = end.line_info(line)
+            lines.append((dim, line.length, random_nodes(dim + 1, max(info.input_nodes, 1)),
+                          np.zeros((info.output_nodes, 8), np.uint64)))
+        nodes = 0
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < seconds_per_slice:
+            for dim, length, inp, out in lines:
+                R.compute_line(big, dim, length, (ctypes.c_uint8 * 3)(0, 0, 0), P(inp), P(out), 0)
+                nodes += out.shape[0]
+        rate = nodes / (time.perf_counter() - t0)
+        per_slice[str(slice_)] = {"line_nodes": work, "nodes_per_s": rate}
+        total_s += work / rate
+    return {"estimated_s": total_s, "cores": nthreads, "kind": "reference", "per_slice": per_slice,
+            "sample": "per slice, the block lines through the first block of its largest section on "
+                      f"{nthreads} threads, {seconds_per_slice} s each, charged for every line of the sweep"}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -315,15 +425,26 @@ def main():
     cpu = None
     midsolve = None
     learned = None
+    sweep2 = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(seconds=12.0)
+    if rank == 0 and world == 1:
         from pentago_b200 import mid
-        midsolve = mid.bench_config0()
+        midsolve, raws0 = mid.bench_config0()
+        if not args.no_cpu_baseline:
+            midsolve["cpu_baseline"] = cpu_midsolve_rate(raws0, midsolve["positions_per_batch"], seconds=8.0)
     if rank == 0 and world == 1 and not args.no_learned:
-        # Config 3 on a sample: 4096 of the root slice's blocks, after the full sweep and training
+        # Config 2 (the full sweep of the root) and config 3 on a sample of
+        # 4096 of the root slice's blocks, after training
         torch.cuda.empty_cache()
         from pentago_b200 import learned as learned_mod
-        learned = learned_mod.run_config3(max_blocks=4096, cpu_seconds=0.0 if args.no_cpu_baseline else 5.0)
+        timings = {}
+        learned, sample = learned_mod.run_config3(max_blocks=4096, sample_blocks=64, sweep_timings=timings)
+        sweep2 = sweep_summary(timings, learned["sweep_s"])
+        if not args.no_cpu_baseline:
+            learned["cpu_static_coder"] = cpu_static_coder_rate(*sample, seconds=5.0)
+            sweep2["cpu_baseline"] = cpu_sweep_estimate(CONFIG2_ROOT, timings, seconds_per_slice=1.5)
+            sweep2["kernel_speedup_vs_cpu_estimate"] = sweep2["cpu_baseline"]["estimated_s"] / (sweep2["kernel_ms"] / 1e3)
 
     if rank == 0:
         result = {
@@ -346,6 +467,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes},
             "gpu_launches": 4 * args.steps,
             "midsolve_config0": midsolve,
+            "sweep_config2": sweep2,
             "learned_rans_config3": learned,
             "clocks": clocks.summary(),
         }

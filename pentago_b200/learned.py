@@ -226,19 +226,19 @@ def static_sizes(symbols, offsets, stream=None):
 
 
 def run_config3(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.01, steps=1500, batch=32768,
-                chunk_blocks=4096, max_blocks=0, seed=1, cpu_seconds=0.0):
+                chunk_blocks=4096, max_blocks=0, seed=1, sample_blocks=0, sweep_timings=None):
     """Config 3: solve the root's sections down to its own slice, train on a
     seeded fraction of the root slice's blocks, code max_blocks blocks (0:
-    all) both ways and check the round trip.  With cpu_seconds > 0 the
-    reference's static coder (oracle/_ref) is timed on the host cores on a
-    sample of the same blocks, as the CPU baseline."""
+    all) both ways and check the round trip.  With sample_blocks > 0 the
+    symbols of that many coded blocks are also returned on the host (for a
+    CPU comparison); sweep_timings receives the sweep's per-slice timings."""
     import torch
     from . import sweep
     from .end import section_sig
     root = section_sig([list(c) for c in root_counts])
     slice_ = sum(sum(c) for c in root_counts)
     t0 = time.perf_counter()
-    _, slice_t, sigs = sweep.sweep(root, keep_last=True)
+    _, slice_t, sigs = sweep.sweep(root, keep_last=True, timings=sweep_timings)
     torch.cuda.synchronize()
     t_sweep = time.perf_counter() - t0
     layout = sweep.slice_layout(sigs)
@@ -285,8 +285,8 @@ def run_config3(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.0
         tot["symbols"] += int(sym.numel())
         tot["static_streams"] += int((dsz_h == ssz.cpu().numpy()).sum())
         lossless &= bool(torch.equal(dec, sym)) and bool((status.cpu().numpy() == nodes[idx] * 256).all())
-        if cpu_sample is None and cpu_seconds > 0:
-            k = min(64, len(idx))
+        if cpu_sample is None and sample_blocks > 0:
+            k = min(sample_blocks, len(idx))
             o = off.cpu().numpy()
             cpu_sample = sym[:int(o[k])].cpu().numpy(), o[:k + 1]
         del sym, data, dec
@@ -306,37 +306,9 @@ def run_config3(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.0
         "decode_Msym_per_s": tot["symbols"] / (tot["dec_ms"] / 1e3) / 1e6,
         "train_blocks": int(ntrain), "train_steps": steps, "train_batch": batch, "train_s": t_train,
         "train_loss_bits": hist, "sweep_s": t_sweep}
-    if cpu_sample is not None:
-        out["cpu_static_coder"] = _cpu_static_rate(*cpu_sample, seconds=cpu_seconds)
+    if sample_blocks > 0:
+        return out, cpu_sample
     return out
-
-
-def _cpu_static_rate(symbols, offsets, seconds):
-    """The reference's format-2 encoder (oracle/_ref) on the host cores, one block per thread."""
-    import os
-    from concurrent.futures import ThreadPoolExecutor
-    try:
-        from tests.oracle import reference, P
-        R = reference()
-    except ImportError:
-        R = None
-    if R is None:
-        return None
-    blocks = [np.ascontiguousarray(symbols[offsets[i]:offsets[i + 1]]) for i in range(len(offsets) - 1)]
-    threads = os.cpu_count() or 1
-
-    def enc(b):
-        out = np.zeros(b.size // 2 + 4096, np.uint8)
-        return R.rans_encode(P(b), b.size, P(out), out.size)
-    done = 0
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(threads) as ex:
-        while time.perf_counter() - t0 < seconds:
-            list(ex.map(enc, blocks))
-            done += sum(b.size for b in blocks)
-    dt = time.perf_counter() - t0
-    return {"encode_Msym_per_s": done / dt / 1e6, "cores": threads, "kind": "reference",
-            "sample": f"{len(blocks)} blocks' symbols, format-2 encode repeated for {dt:.1f} s"}
 
 
 def main():
@@ -348,12 +320,11 @@ def main():
     ap.add_argument("--chunk-blocks", type=int, default=4096)
     ap.add_argument("--max-blocks", type=int, default=0, help="code only N blocks spread over the slice (0: all)")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--cpu-seconds", type=float, default=0.0)
     args = ap.parse_args()
     c = [int(x) for x in args.root.split(",")]
     capi.check(capi.lib().pg_init())
     res = run_config3(((c[0], c[1]), (c[2], c[3]), (c[4], c[5]), (c[6], c[7])), args.train_fraction, args.steps,
-                      args.batch, args.chunk_blocks, args.max_blocks, args.seed, args.cpu_seconds)
+                      args.batch, args.chunk_blocks, args.max_blocks, args.seed)
     res["root"] = args.root
     print(json.dumps(res))
 
