@@ -20,7 +20,6 @@
 // mid_values_t records.
 #include "mid_body.cuh"
 #include "runtime.h"
-#include <cooperative_groups.h>
 #include <algorithm>
 #include <condition_variable>
 #include <mutex>
@@ -40,78 +39,7 @@ mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict_
   if (threadIdx.x == 0) fault = 0;
   __syncthreads();
   const mid_tables MT = {c_choose, c_winpat, wf};
-  mid_board_body(J, MT, tiles, ws_flat{ws}, raw, &fault, threadIdx.x, blockDim.x, 0, 1, sync_threads(),
-                 sync_threads());
-}
-
-namespace cg = cooperative_groups;
-
-struct cluster_sync { __device__ void operator()() const { cg::this_cluster().sync(); } };
-
-// Boards whose workspace fits shared memory, each split over the C CTAs of a
-// thread-block cluster: every CTA holds a chunk of the workspace (reached by
-// the others through distributed shared memory), builds its own set0 rows and
-// takes 1/C of every level; the cluster barrier separates levels.  The
-// n <= 1 results and the fault flag live in CTA 0.
-template<int C>
-__global__ void __launch_bounds__(kMidThreads)
-mid_board_cluster_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict__ wf) {
-  constexpr int chunk = (kSmemWorkspaceMax + C - 1) / C;
-  cg::cluster_group cluster = cg::this_cluster();
-  const int rank = int(cluster.block_rank());
-  const mid_job_t& J = jobs[blockIdx.x / C];
-  extern __shared__ uint4 smem[];
-  set0_info* tiles = reinterpret_cast<set0_info*>(smem);
-  uint4* mine = smem + kMidThreads * sizeof(set0_info) / sizeof(uint4);
-  __shared__ uint4 raw[2][19];
-  __shared__ int fault;
-  if (threadIdx.x == 0) fault = 0;
-  cluster.sync();  // every CTA of the cluster runs and has initialised its flag
-  ws_split W;
-  for (int r = 0; r < kClusterMax; r++) W.part[r] = cluster.map_shared_rank(mine, r < C ? r : 0);
-  W.chunk = chunk;
-  const mid_tables MT = {c_choose, c_winpat, wf};
-  mid_board_body(J, MT, tiles, W, cluster.map_shared_rank(raw, 0), cluster.map_shared_rank(&fault, 0),
-                 int(threadIdx.x), int(blockDim.x), rank, C, sync_threads(), cluster_sync());
-  cluster.sync();  // no CTA leaves while another may still use its shared memory
-}
-
-template<int C> static size_t cluster_smem() {
-  return kMidThreads * sizeof(set0_info) + size_t((kSmemWorkspaceMax + C - 1) / C) * 16;
-}
-
-template<int C> static int launch_cluster_boards(const mid_job_t* jobs, int boards, const uint32_t* wf,
-                                                 cudaStream_t stream) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(unsigned(boards * C));
-  cfg.blockDim = dim3(kMidThreads);
-  cfg.dynamicSmemBytes = cluster_smem<C>();
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = C;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  PG_CUDA(cudaLaunchKernelEx(&cfg, mid_board_cluster_kernel<C>, jobs, wf));
-  return PG_OK;
-}
-
-// CTAs per board for a batch of small boards: clusters of 4 or 2 when the
-// batch leaves SMs idle with one CTA per board, else 1.
-static int small_board_split(int boards) {
-  int dev = 0, sms = 0, per4 = 0, per2 = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per4, mid_board_cluster_kernel<4>, kMidThreads,
-                                                    cluster_smem<4>()) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, mid_board_cluster_kernel<2>, kMidThreads,
-                                                    cluster_smem<2>()) != cudaSuccess)
-    return 1;
-  if (4 * boards <= sms * per4) return 4;
-  if (2 * boards <= sms * per2) return 2;
-  return 1;
+  mid_board_body(J, MT, tiles, ws, raw, &fault, threadIdx.x, blockDim.x, 0, 1, sync_threads(), sync_threads());
 }
 
 // A few large boards: ncta CTAs per board (blockIdx.x / ncta), each taking a
@@ -126,8 +54,7 @@ mid_board_grid_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __rest
   set0_info* tiles = reinterpret_cast<set0_info*>(smem);
   const mid_tables MT = {c_choose, c_winpat, wf};
   const board_barrier gb{bar + 2 * board, bar + 2 * board + 1, ncta, faults + board};
-  mid_board_body(J, MT, tiles, ws_flat{J.workspace}, reinterpret_cast<uint4(*)[19]>(rawg + 38 * board),
-                 faults + board,
+  mid_board_body(J, MT, tiles, J.workspace, reinterpret_cast<uint4(*)[19]>(rawg + 38 * board), faults + board,
                  int(threadIdx.x), int(blockDim.x), cta, ncta, sync_threads(), gb);
 }
 
@@ -215,11 +142,7 @@ static int upload_consts() {
     attr = cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) == cudaSuccess &&
                    cudaFuncSetAttribute(mid_board_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(kMidThreads * sizeof(set0_info))) == cudaSuccess &&
-                   cudaFuncSetAttribute(mid_board_cluster_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(cluster_smem<2>())) == cudaSuccess &&
-                   cudaFuncSetAttribute(mid_board_cluster_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(cluster_smem<4>())) == cudaSuccess
+                                        int(kMidThreads * sizeof(set0_info))) == cudaSuccess
                ? 0 : PG_ERR_CUDA;
   return attr;
 }
@@ -335,12 +258,7 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     const int smem_ws = pass == 0;
     const size_t smem = kMidThreads * sizeof(set0_info) + (smem_ws ? kSmemWorkspaceMax * 16 : 0);
     const int ncta = smem_ws ? 1 : grid_ctas_per_board(int(jobs.size()), smem);
-    const int split = smem_ws ? small_board_split(int(jobs.size())) : 1;
-    if (split == 4) {
-      if (int rc = launch_cluster_boards<4>(d, int(jobs.size()), T->win_factors, stream)) return rc;
-    } else if (split == 2) {
-      if (int rc = launch_cluster_boards<2>(d, int(jobs.size()), T->win_factors, stream)) return rc;
-    } else if (ncta <= 1) {
+    if (ncta <= 1) {
       mid_board_kernel<<<unsigned(jobs.size()), kMidThreads, smem, stream>>>(d, T->win_factors, smem_ws);
       PG_CUDA(cudaGetLastError());
     } else {
@@ -377,7 +295,7 @@ extern "C" int pg_selftest_midsolve_host(const uint64_t* raws, int n, pg_mid_val
     memset(raw, 0, sizeof raw);
     int fault = 0;
     J.ws_size = int(P.workspace);
-    mid_board_body(J, MT, tiles.data(), ws_flat{ws.data()}, raw, &fault, 0, 1, 0, 1, [] {}, [] {},
+    mid_board_body(J, MT, tiles.data(), ws.data(), raw, &fault, 0, 1, 0, 1, [] {}, [] {},
                    supers ? reinterpret_cast<uint4*>(supers + 76 * size_t(i)) : nullptr);
   }
   return PG_OK;
@@ -429,21 +347,10 @@ extern "C" int pg_selftest_midsolve_groups_host(const uint64_t* raws, int n, int
     int fault = 0;
     host_barrier hb(groups);
     std::vector<std::vector<set0_info>> tiles(groups, std::vector<set0_info>(kMidThreads));
-    // Up to kClusterMax groups also split the workspace in chunks, one per
-    // group, as the cluster kernel does with its CTAs' shared memories.
-    const int chunk = int((P.workspace + groups - 1) / groups);
-    std::vector<std::vector<uint4>> parts(groups, std::vector<uint4>(chunk + 1));
-    ws_split W;
-    for (int r = 0; r < kClusterMax; r++) W.part[r] = parts[r < groups ? r : 0].data();
-    W.chunk = chunk;
     std::vector<std::thread> threads;
     for (int g = 0; g < groups; g++)
       threads.emplace_back([&, g] {
-        if (groups <= kClusterMax)
-          mid_board_body(J, MT, tiles[g].data(), W, raw, &fault, 0, 1, g, groups, [] {}, [&] { hb.wait(); });
-        else
-          mid_board_body(J, MT, tiles[g].data(), ws_flat{ws.data()}, raw, &fault, 0, 1, g, groups, [] {},
-                         [&] { hb.wait(); });
+        mid_board_body(J, MT, tiles[g].data(), ws.data(), raw, &fault, 0, 1, g, groups, [] {}, [&] { hb.wait(); });
       });
     for (auto& t : threads) t.join();
   }

@@ -144,32 +144,11 @@ PG_HD void build_set0(const mid_job_t& J, const mid_tables& MT, const level_t& L
     }
 }
 
-// The workspace as one array (shared memory of one CTA, or global memory).
-struct ws_flat {
-  uint4* p;
-  PG_HD uint4* at(int i) const { return p + i; }
-};
-
-// The workspace split in equal chunks over the shared memories of the CTAs of
-// a cluster: entry i lives in CTA i / chunk (part[] holds each CTA's chunk as
-// seen from this CTA, local or distributed shared memory).
-constexpr int kClusterMax = 4;
-struct ws_split {
-  uint4* part[kClusterMax];
-  int chunk;
-  PG_HD uint4* at(int i) const {
-    const int r = (i >= chunk) + (i >= 2 * chunk) + (i >= 3 * chunk);
-    return part[r] + (i - r * chunk);
-  }
-};
-
-// inner (mid/internal.h:358-408) on workspace entries [in_lo, in_lo + in_size)
-// (input level) and [out_lo, out_lo + out_size) (output level).
+// inner (mid/internal.h:358-408)
 // Returns false (and does nothing) if an index would leave the workspace.
-template<class WS>
 PG_HD bool inner(const mid_job_t& J, const mid_tables& MT, const level_t& L, const set0_info& I0, int s1p,
-                 int aggressive, const WS& ws, int in_lo, int out_lo, int in_ny, int out_ny, int in_size,
-                 int out_size, uint4* results) {
+                 int aggressive, const uint4* in, uint4* out, int in_ny, int out_ny, int in_size, int out_size,
+                 uint4* results) {
   const int n = L.n, spots = L.spots, k0 = L.k0, k1 = L.k1;
   const uint64_t set1p = J.sets1p[J.sets1p_off[n] + s1p];
   const int turn_aggressive = aggressive ^ (n & 1);
@@ -191,7 +170,7 @@ PG_HD bool inner(const mid_job_t& J, const mid_tables& MT, const level_t& L, con
     unmoved &= unmoved - 1;
     const int idx = int(I0.child_s0s[i]) * in_ny + cs[i];
     if (unsigned(idx) >= unsigned(in_size)) return false;
-    us = h_or(us, h_from(*ws.at(in_lo + idx)));
+    us = h_or(us, h_from(in[idx]));
   }
   const uint4* w1 = J.wins1 + 2 * (J.wins1_off[n] + s1);
   const half4 after = h_from(w1[0]), before = h_from(w1[1]);
@@ -202,7 +181,7 @@ PG_HD bool inner(const mid_job_t& J, const mid_tables& MT, const level_t& L, con
   const int o = int(s1) * out_ny + s0p;
   if (unsigned(o) >= unsigned(out_size) || (n <= 1 && n + s1p >= 19)) return false;
   if (n <= 1) results[n + s1p] = h_to(us);
-  *ws.at(out_lo + o) = h_to(h_or(h_rmax(h_not(us)), before));
+  out[o] = h_to(h_or(h_rmax(h_not(us)), before));
   return true;
 }
 
@@ -299,8 +278,8 @@ PG_HD void traverse(const mid_job_t& J, const mid_tables& MT, const uint4* super
 // the next level only after the all-group barrier.  Run with one group of one
 // thread and no-op barriers it is the same computation done sequentially
 // (used by the CPU self-test).  `raw` and `fault` are shared by the groups.
-template<class WS, class Barrier, class GridBarrier>
-PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* tiles, const WS& ws,
+template<class Barrier, class GridBarrier>
+PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* tiles, uint4* ws,
                           uint4 (*raw)[19], int* fault, int tid, int nt, int cta, int ncta, Barrier barrier,
                           GridBarrier gbarrier, uint4* dump = nullptr) {
   const int spots = J.spots;
@@ -341,6 +320,8 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
     for (int n = spots; n >= 0; n--) {
       const level_t L = make_level(J, MT, n);
       const mid_grab gi = J.spaces[n + 1], go = J.spaces[n];
+      const uint4* in = ws + gi.lo;
+      uint4* out = ws + go.lo;
       // This group's items [i0, i1) and the set0 rows they touch
       const int64_t total = int64_t(L.nsets0) * L.nsets1p;
       const int64_t i0 = total * cta / ncta, i1 = total * (cta + 1) / ncta;
@@ -354,8 +335,8 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
         const int64_t b = i1 < int64_t(base + rows) * L.nsets1p ? i1 : int64_t(base + rows) * L.nsets1p;
         for (int64_t it = a + tid; it < b; it += nt) {
           const int row = int(it / L.nsets1p), s1p = int(it - int64_t(row) * L.nsets1p);
-          if (!inner(J, MT, L, tiles[row - base], s1p, aggressive, ws, gi.lo, go.lo, gi.ny, go.ny,
-                     J.ws_size - gi.lo, J.ws_size - go.lo, raw[aggressive]))
+          if (!inner(J, MT, L, tiles[row - base], s1p, aggressive, in, out, gi.ny, go.ny, J.ws_size - gi.lo,
+                     J.ws_size - go.lo, raw[aggressive]))
             *fault = 1;
         }
         barrier();

@@ -95,7 +95,7 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_a
     mid_job_t J = E.job;
     const int gang = E.gang, rank = E.rank, first = E.first;
     if (gang <= 1) {
-      mid_board_body(J, MT, tiles, ws_flat{J.workspace}, raw, &fault, int(threadIdx.x), int(blockDim.x), 0, 1,
+      mid_board_body(J, MT, tiles, J.workspace, raw, &fault, int(threadIdx.x), int(blockDim.x), 0, 1,
                      sync_threads(), sync_threads());
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -107,8 +107,7 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_a
       // gang are consecutive, so earlier requests never wait on later ones.
       gang_aux& X = aux[first];
       const board_barrier gb{&X.count, &X.gen, gang, &X.fault};
-      mid_board_body(J, MT, tiles, ws_flat{J.workspace}, X.raw, &X.fault, int(threadIdx.x), int(blockDim.x), rank,
-                     gang,
+      mid_board_body(J, MT, tiles, J.workspace, X.raw, &X.fault, int(threadIdx.x), int(blockDim.x), rank, gang,
                      sync_threads(), gb);
       __syncthreads();
       if (rank == 0 && threadIdx.x == 0) {
