@@ -396,13 +396,32 @@ def main():
     units_all = out_nodes * 256 * args.steps * world
     value = units_all / (elapsed_ms / 1e3)
 
-    # End-to-end through the public API with host buffers
+    # End-to-end through the public API with host buffers.  The lines go in
+    # chunks of four blocks, each chunk's copy in, compute and copy out on its
+    # own stream, so that the two copy directions and the kernels overlap.
+    chunk = 16
+    chunks = [list(range(c, min(c + chunk, len(ls)))) for c in range(0, len(ls), chunk)]
+    chunk_plans = [end.Plan([ls[i] for i in c]) for c in chunks]
+    streams = [torch.cuda.Stream(device=dev) for _ in range(3)]
+
     def e2e_step():
-        for l, hi in zip(ls, host_in):
-            l.input.copy_(hi, non_blocking=True)
-        plan.run(stream)
-        for l, ho in zip(ls, host_out):
-            ho.copy_(l.output, non_blocking=True)
+        go = torch.cuda.Event()
+        go.record(stream)
+        done = []
+        for k, (c, p) in enumerate(zip(chunks, chunk_plans)):
+            st = streams[k % len(streams)]
+            st.wait_event(go)
+            with torch.cuda.stream(st):
+                for i in c:
+                    ls[i].input.copy_(host_in[i], non_blocking=True)
+                p.run(st)
+                for i in c:
+                    host_out[i].copy_(ls[i].output, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(st)
+            done.append(ev)
+        for ev in done:
+            stream.wait_event(ev)
         stream.synchronize()
 
     for _ in range(max(1, args.warmup)):
