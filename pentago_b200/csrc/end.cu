@@ -458,12 +458,12 @@ struct end_plan {
   parent_rec* recs_dev = nullptr;
 };
 
-template<int DIM> static int set_smem_limit() {
-  static int rc = -1;
-  if (rc < 0)
-    rc = cudaFuncSetAttribute(end_line_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template<int DIM> static int set_smem_attr() {
+  return cudaFuncSetAttribute(end_line_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kSubBytes + kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
-  return rc;
+}
+template<int DIM> static int set_smem_limit() {
+  return per_device_once((const void*)&set_smem_attr<DIM>, set_smem_attr<DIM>);
 }
 
 static int launch_group(const end_plan& P, int dim, cudaStream_t stream, const dev_tables_t& T) {
@@ -831,12 +831,12 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
 static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");
 static_assert(sizeof(family_t) % 16 == 0, "family_t array keeps proto 16-byte aligned");
 
-template<int DIM> static int sweep_smem_limit() {
-  static int rc = -1;
-  if (rc < 0)
-    rc = cudaFuncSetAttribute(sweep_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template<int DIM> static int sweep_smem_attr() {
+  return cudaFuncSetAttribute(sweep_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kSubBytes + kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
-  return rc;
+}
+template<int DIM> static int sweep_smem_limit() {
+  return per_device_once((const void*)&sweep_smem_attr<DIM>, sweep_smem_attr<DIM>);
 }
 
 // Per-section (we-win, we-win-or-tie, total) counts over distinct positions

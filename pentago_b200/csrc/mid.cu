@@ -135,16 +135,17 @@ bool plan_board(uint64_t raw, board_plan& P, std::string& err) {
   return true;
 }
 
+static int mid_kernel_attrs() {
+  return cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) == cudaSuccess &&
+                 cudaFuncSetAttribute(mid_board_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(kMidThreads * sizeof(set0_info))) == cudaSuccess
+             ? 0 : PG_ERR_CUDA;
+}
+
 static int upload_consts() {
   if (int rc = mid_prepare_device()) return rc;
-  static int attr = -1;
-  if (attr < 0)
-    attr = cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) == cudaSuccess &&
-                   cudaFuncSetAttribute(mid_board_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        int(kMidThreads * sizeof(set0_info))) == cudaSuccess
-               ? 0 : PG_ERR_CUDA;
-  return attr;
+  return per_device_once((const void*)&mid_kernel_attrs, mid_kernel_attrs);
 }
 
 static size_t align256(size_t x) { return (x + 255) & ~size_t(255); }

@@ -3,6 +3,7 @@
 #pragma once
 #include "superscore.cuh"
 #include "tables.h"
+#include "runtime.h"
 #include "../../include/pentago_b200.h"
 #include <cstring>
 #include <string>
@@ -419,11 +420,7 @@ size_t scratch_bytes_of(const board_plan& P, bool global_ws = false);
 void carve_scratch(board_plan& P, char* base, bool global_ws = false);
 
 // Upload this translation unit's constant tables (once per device).
-static int mid_prepare_device() {
-  static int uploaded_device = -1;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return PG_ERR_CUDA;
-  if (uploaded_device == dev) return PG_OK;
+static int mid_upload_constants() {
   uint32_t ch[19][11];
   for (int n = 0; n <= 18; n++)
     for (int k = 0; k <= 10; k++) ch[n][k] = uint32_t(hchoose(n, k));
@@ -431,8 +428,8 @@ static int mid_prepare_device() {
   if (cudaMemcpyToSymbol(c_choose, ch, sizeof ch) != cudaSuccess ||
       cudaMemcpyToSymbol(c_winpat, T.winpat, sizeof T.winpat) != cudaSuccess)
     return PG_ERR_CUDA;
-  uploaded_device = dev;
   return PG_OK;
 }
+static int mid_prepare_device() { return per_device_once((const void*)&c_choose, mid_upload_constants); }
 
 }  // namespace pg

@@ -2,6 +2,7 @@
 #include "runtime.h"
 #include "tables.h"
 #include "../../include/pentago_b200.h"
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -14,6 +15,20 @@ int fail(int code, const std::string& msg) { last_error = msg; return code; }
 int cuda_fail(cudaError_t e, const char* what) {
   last_error = std::string(what) + ": " + cudaGetErrorString(e);
   return PG_ERR_CUDA;
+}
+
+static std::mutex once_mutex;
+static std::map<std::pair<int, const void*>, int> once_done;
+
+int per_device_once(const void* key, int (*f)()) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return fail(PG_ERR_CUDA, "no CUDA device");
+  std::lock_guard<std::mutex> lock(once_mutex);
+  auto it = once_done.find({dev, key});
+  if (it != once_done.end()) return it->second;
+  const int rc = f();
+  once_done[{dev, key}] = rc;
+  return rc;
 }
 
 static std::mutex dev_mutex;

@@ -30,6 +30,11 @@ struct dev_tables_t {
 // sets the error on failure.
 const dev_tables_t* device_tables();
 
+// Run f() once per (current device, key) and return its result from then on
+// (thread safe).  For per-device set-up such as kernel attributes and
+// constant-memory uploads.
+int per_device_once(const void* key, int (*f)());
+
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
