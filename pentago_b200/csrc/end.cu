@@ -557,20 +557,20 @@ extern "C" int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream_
   end_plan P;
   if (int rc = plan_lines(lines, n, P)) return rc;
   if (P.recs.empty()) return PG_OK;
+  stream_scratch X(stream);
   parent_rec* recs = nullptr;
-  PG_CUDA(cudaMallocAsync(&recs, sizeof(parent_rec) * P.recs.size(), stream));
+  PG_CUDA(X.alloc(&recs, sizeof(parent_rec) * P.recs.size()));
   PG_CUDA(cudaMemcpyAsync(recs, P.recs.data(), sizeof(parent_rec) * P.recs.size(), cudaMemcpyHostToDevice, stream));
   bind_records(P, recs);
   int rc = PG_OK;
   for (int dim = 0; dim < 4 && !rc; dim++) {
     if (P.host[dim].empty()) continue;
     const size_t bytes = sizeof(line_dev_t) * P.host[dim].size();
-    PG_CUDA(cudaMallocAsync(&P.dev[dim], bytes, stream));
+    PG_CUDA(X.alloc(&P.dev[dim], bytes));
     PG_CUDA(cudaMemcpyAsync(P.dev[dim], P.host[dim].data(), bytes, cudaMemcpyHostToDevice, stream));
     rc = launch_group(P, dim, stream, *T);
-    PG_CUDA(cudaFreeAsync(P.dev[dim], stream));
+    P.dev[dim] = nullptr;  // released with the scratch, not by end_plan
   }
-  PG_CUDA(cudaFreeAsync(recs, stream));
   return rc;
 }
 
@@ -1012,12 +1012,13 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
       recs.insert(recs.end(), tmp.begin(), tmp.end());
     }
     if (fams.empty()) continue;
+    stream_scratch X(stream);
     parent_rec* recs_dev = nullptr;
-    PG_CUDA(cudaMallocAsync(&recs_dev, sizeof(parent_rec) * recs.size(), stream));
+    PG_CUDA(X.alloc(&recs_dev, sizeof(parent_rec) * recs.size()));
     PG_CUDA(cudaMemcpyAsync(recs_dev, recs.data(), sizeof(parent_rec) * recs.size(), cudaMemcpyHostToDevice, stream));
     for (size_t f = 0; f < fams.size(); f++) fams[f].proto.recs = recs_dev + rec_off[f];
     family_t* d = nullptr;
-    PG_CUDA(cudaMallocAsync(&d, sizeof(family_t) * fams.size(), stream));
+    PG_CUDA(X.alloc(&d, sizeof(family_t) * fams.size()));
     PG_CUDA(cudaMemcpyAsync(d, fams.data(), sizeof(family_t) * fams.size(), cudaMemcpyHostToDevice, stream));
     const size_t smem = kSubBytes + size_t(kMicro) * maxchild * 64;
     for (int line0 = 0; line0 < total; line0 += 1 << 30) {
@@ -1033,8 +1034,6 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
       if (rc) return fail(rc, "cudaFuncSetAttribute failed");
       PG_CUDA(cudaGetLastError());
     }
-    PG_CUDA(cudaFreeAsync(d, stream));
-    PG_CUDA(cudaFreeAsync(recs_dev, stream));
   }
   return PG_OK;
 }
@@ -1090,8 +1089,9 @@ extern "C" int pg_section_counts(const uint64_t* sigs, int n, const uint64_t* sl
   }
   if (!n) return PG_OK;
   PG_CUDA(cudaMemsetAsync(counts3, 0, sizeof(uint64_t) * 3 * n, stream));
+  stream_scratch X(stream);
   count_section_t* d = nullptr;
-  PG_CUDA(cudaMallocAsync(&d, sizeof(count_section_t) * n, stream));
+  PG_CUDA(X.alloc(&d, sizeof(count_section_t) * n));
   PG_CUDA(cudaMemcpyAsync(d, secs.data(), sizeof(count_section_t) * n, cudaMemcpyHostToDevice, stream));
   for (int64_t b0 = 0; b0 < blocks; b0 += int64_t(1) << 30) {
     // grid.x covers at most 2^30 blocks per launch; the kernel reads blockIdx.x only,
@@ -1100,7 +1100,6 @@ extern "C" int pg_section_counts(const uint64_t* sigs, int n, const uint64_t* sl
     count_kernel<<<unsigned(blocks), 256, 0, stream>>>(d, n, slice, (unsigned long long*)counts3, T->rmin_flat, stab);
     PG_CUDA(cudaGetLastError());
   }
-  PG_CUDA(cudaFreeAsync(d, stream));
   return PG_OK;
 }
 

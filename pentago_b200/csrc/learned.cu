@@ -776,19 +776,13 @@ extern "C" int pg_rans_learned_encode(const uint8_t* model, const pg_block_ref_t
     alt_off[nstreams + s] = 256 * hb[s].nodes;
     total += (rans_stream_bound(256 * hb[s].nodes) + 15) & ~15;
   }
-  // Scratch for the format-2 streams, released on every path out
-  struct scratch {
-    void* p[3] = {nullptr, nullptr, nullptr};
-    cudaStream_t st;
-    ~scratch() { for (void* q : p) if (q) cudaFreeAsync(q, st); }
-  } X;
-  X.st = st;
-  PG_CUDA(cudaMallocAsync(&X.p[0], std::max<int64_t>(total, 16), st));
-  PG_CUDA(cudaMallocAsync(&X.p[1], sizeof(int64_t) * 2 * nstreams, st));
-  PG_CUDA(cudaMallocAsync(&X.p[2], sizeof(int64_t) * nstreams, st));
-  uint8_t* alt = static_cast<uint8_t*>(X.p[0]);
-  int64_t* alt_off_d = static_cast<int64_t*>(X.p[1]);
-  int64_t* alt_sizes = static_cast<int64_t*>(X.p[2]);
+  // Scratch for the format-2 streams
+  stream_scratch X(st);
+  uint8_t* alt = nullptr;
+  int64_t *alt_off_d = nullptr, *alt_sizes = nullptr;
+  PG_CUDA(X.alloc(&alt, std::max<int64_t>(total, 16)));
+  PG_CUDA(X.alloc(&alt_off_d, sizeof(int64_t) * 2 * nstreams));
+  PG_CUDA(X.alloc(&alt_sizes, sizeof(int64_t) * nstreams));
   PG_CUDA(cudaMemcpyAsync(alt_off_d, alt_off.data(), sizeof(int64_t) * 2 * nstreams, cudaMemcpyHostToDevice, st));
   if (int rc = launch_rans_encode(symbols, offsets, nstreams, alt, alt_off_d, alt_sizes, alt_off_d + nstreams, st))
     return rc;
@@ -859,18 +853,14 @@ extern "C" int pg_learned_grad(const float* params, const pg_block_ref_t* blocks
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int grid = int(std::max<int64_t>(1, std::min<int64_t>((n + kGradThreads - 1) / kGradThreads, sms)));
-  struct scratch {
-    float* p = nullptr;
-    cudaStream_t st;
-    ~scratch() { if (p) cudaFreeAsync(p, st); }
-  } X;
-  X.st = st;
-  PG_CUDA(cudaMallocAsync(&X.p, sizeof(float) * grid * (kLmParams + 1), st));
+  stream_scratch X(st);
+  float* partial = nullptr;
+  PG_CUDA(X.alloc(&partial, sizeof(float) * grid * (kLmParams + 1)));
   if (int rc = lm_smem_opt_in(lm_grad_kernel, sizeof(lm_grad_smem))) return rc;
   lm_grad_kernel<<<grid, kGradThreads, sizeof(lm_grad_smem), st>>>(params, L.blocks, nstreams, symbols, offsets,
-                                                                    samples, n, X.p, *T);
+                                                                    samples, n, partial, *T);
   PG_CUDA(cudaGetLastError());
-  lm_reduce_kernel<<<(kLmParams + 1 + 255) / 256, 256, 0, st>>>(X.p, grid, grad, loss);
+  lm_reduce_kernel<<<(kLmParams + 1 + 255) / 256, 256, 0, st>>>(partial, grid, grad, loss);
   PG_CUDA(cudaGetLastError());
   return PG_OK;
 }

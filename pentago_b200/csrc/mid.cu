@@ -165,9 +165,10 @@ static int launch_grid_boards(const mid_job_t* jobs, int boards, int ncta, size_
                               cudaStream_t stream) {
   // Per board: barrier words, the n <= 1 results of both passes, a fault flag
   const size_t bar_bytes = sizeof(unsigned) * 2 * boards, raw_bytes = sizeof(uint4) * 38 * boards;
+  stream_scratch X(stream);
   char* aux = nullptr;
   const size_t aux_bytes = align256(bar_bytes) + align256(raw_bytes) + align256(sizeof(int) * boards);
-  PG_CUDA(cudaMallocAsync((void**)&aux, aux_bytes, stream));
+  PG_CUDA(X.alloc(&aux, aux_bytes));
   PG_CUDA(cudaMemsetAsync(aux, 0, aux_bytes, stream));
   unsigned* bar = (unsigned*)aux;
   uint4* rawg = (uint4*)(aux + align256(bar_bytes));
@@ -175,7 +176,6 @@ static int launch_grid_boards(const mid_job_t* jobs, int boards, int ncta, size_
   void* args[] = {(void*)&jobs, (void*)&wf, (void*)&ncta, (void*)&bar, (void*)&rawg, (void*)&faults};
   PG_CUDA(cudaLaunchCooperativeKernel((void*)mid_board_grid_kernel, dim3(unsigned(boards * ncta)), dim3(kMidThreads),
                                       args, smem, stream));
-  PG_CUDA(cudaFreeAsync(aux, stream));
   return PG_OK;
 }
 
@@ -232,11 +232,10 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     if (!plan_board(raws[i], plans[i], err)) return fail(PG_ERR_ARG, "board " + std::to_string(i) + ": " + err);
     total += scratch_bytes_of(plans[i]);
   }
+  stream_scratch X(stream);
   char* base = (char*)scratch;
-  bool owned = false;
   if (!base) {
-    PG_CUDA(cudaMallocAsync((void**)&base, std::max<size_t>(total, 256), stream));
-    owned = true;
+    PG_CUDA(X.alloc(&base, std::max<size_t>(total, 256)));
   } else if (size_t(scratch_bytes) < total) {
     return fail(PG_ERR_CAPACITY, "midsolve scratch too small");
   }
@@ -254,7 +253,7 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     auto& jobs = pass ? large : small;
     if (jobs.empty()) continue;
     mid_job_t* d = nullptr;
-    PG_CUDA(cudaMallocAsync(&d, sizeof(mid_job_t) * jobs.size(), stream));
+    PG_CUDA(X.alloc(&d, sizeof(mid_job_t) * jobs.size()));
     PG_CUDA(cudaMemcpyAsync(d, jobs.data(), sizeof(mid_job_t) * jobs.size(), cudaMemcpyHostToDevice, stream));
     const int smem_ws = pass == 0;
     const size_t smem = kMidThreads * sizeof(set0_info) + (smem_ws ? kSmemWorkspaceMax * 16 : 0);
@@ -265,9 +264,7 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     } else {
       if (int rc = launch_grid_boards(d, int(jobs.size()), ncta, smem, T->win_factors, stream)) return rc;
     }
-    PG_CUDA(cudaFreeAsync(d, stream));
   }
-  if (owned) PG_CUDA(cudaFreeAsync(base, stream));
   return PG_OK;
 }
 

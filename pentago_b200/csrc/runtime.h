@@ -35,6 +35,28 @@ const dev_tables_t* device_tables();
 // constant-memory uploads.
 int per_device_once(const void* key, int (*f)());
 
+// Device scratch of one call: allocated with cudaMallocAsync on the call's
+// stream and released with cudaFreeAsync on it when the guard goes out of
+// scope, on every return path.
+struct stream_scratch {
+  cudaStream_t stream;
+  void* ptrs[8] = {};
+  int n = 0;
+  explicit stream_scratch(cudaStream_t s) : stream(s) {}
+  stream_scratch(const stream_scratch&) = delete;
+  stream_scratch& operator=(const stream_scratch&) = delete;
+  template<class T> cudaError_t alloc(T** p, size_t bytes) {
+    *p = nullptr;
+    if (n == 8) return cudaErrorMemoryAllocation;
+    const cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), bytes ? bytes : 16, stream);
+    if (e == cudaSuccess) ptrs[n++] = *p;
+    return e;
+  }
+  ~stream_scratch() {
+    for (int i = 0; i < n; i++) cudaFreeAsync(ptrs[i], stream);
+  }
+};
+
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
