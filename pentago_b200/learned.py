@@ -207,10 +207,39 @@ def freqs(model, refs, symbols, offsets, samples, stream=None):
     return out
 
 
+def static_roundtrip(symbols, offsets, stream=None):
+    """Format-2 coding of the same symbol ranges on the GPU, timed both ways:
+    (sizes, encode ms, decode ms, lossless)."""
+    import torch
+    L = capi.lib()
+    off = offsets.cpu().numpy()
+    n = len(off) - 1
+    caps = np.array([L.pg_rans_bound(int(off[i + 1] - off[i])) for i in range(n)], np.int64)
+    out_off = np.zeros(n + 1, np.int64)
+    out_off[1:] = np.cumsum(caps)
+    out = torch.empty(int(out_off[-1]), dtype=torch.uint8, device="cuda")
+    out_off_d = torch.from_numpy(out_off).cuda()
+    sizes = torch.empty(n, dtype=torch.int64, device="cuda")
+    back = torch.empty_like(symbols)
+    sym_caps = (offsets[1:] - offsets[:-1]).contiguous()
+    status = torch.empty(n, dtype=torch.int64, device="cuda")
+    h = capi.stream_handle(stream)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record()
+    capi.check(L.pg_rans_encode_batch(symbols.data_ptr(), offsets.data_ptr(), n, out.data_ptr(),
+                                      out_off_d.data_ptr(), sizes.data_ptr(), h))
+    e1.record()
+    capi.check(L.pg_rans_decode_batch(out.data_ptr(), out_off_d.data_ptr(), sizes.data_ptr(), n, back.data_ptr(),
+                                      offsets.data_ptr(), sym_caps.data_ptr(), status.data_ptr(), h))
+    e2.record()
+    torch.cuda.synchronize()
+    ok = bool(torch.equal(back, symbols)) and bool(torch.equal(status, sym_caps))
+    return sizes, e0.elapsed_time(e1), e1.elapsed_time(e2), ok
+
+
 def static_sizes(symbols, offsets, stream=None):
     """Format-2 stream sizes of the same symbol ranges."""
     import torch
-    from . import rans
     L = capi.lib()
     off = offsets.cpu().numpy()
     n = len(off) - 1
@@ -260,7 +289,8 @@ def run_config3(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.0
     del tsym, tr
     # Code the blocks spread evenly over the slice, chunk by chunk
     pick = np.unique(np.linspace(0, len(nodes) - 1, nblocks).astype(np.int64))
-    tot = {"learned": 0, "static": 0, "symbols": 0, "enc_ms": 0.0, "dec_ms": 0.0, "static_streams": 0}
+    tot = {"learned": 0, "static": 0, "symbols": 0, "enc_ms": 0.0, "dec_ms": 0.0, "static_streams": 0,
+           "static_enc_ms": 0.0, "static_dec_ms": 0.0}
     lossless = True
     cpu_sample = None
     for c0 in range(0, len(pick), chunk_blocks):
@@ -273,10 +303,13 @@ def run_config3(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.0
         e1.record()
         dec, _, status = decode(model, crefs, data, doff, dsz, nodes[idx])
         e2.record()
-        ssz = static_sizes(sym, off)
         torch.cuda.synchronize()
         tot["enc_ms"] += e0.elapsed_time(e1)
         tot["dec_ms"] += e1.elapsed_time(e2)
+        ssz, s_enc, s_dec, s_ok = static_roundtrip(sym, off)
+        tot["static_enc_ms"] += s_enc
+        tot["static_dec_ms"] += s_dec
+        lossless &= s_ok
         dsz_h = dsz.cpu().numpy()
         if (dsz_h < 0).any():
             raise RuntimeError("encode failed")
@@ -304,6 +337,8 @@ def run_config3(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.0
         "decode_GBps_of_nodes": tot["symbols"] / 4 / (tot["dec_ms"] / 1e3) / 1e9,
         "encode_Msym_per_s": tot["symbols"] / (tot["enc_ms"] / 1e3) / 1e6,
         "decode_Msym_per_s": tot["symbols"] / (tot["dec_ms"] / 1e3) / 1e6,
+        "static_gpu_encode_Msym_per_s": tot["symbols"] / (tot["static_enc_ms"] / 1e3) / 1e6,
+        "static_gpu_decode_Msym_per_s": tot["symbols"] / (tot["static_dec_ms"] / 1e3) / 1e6,
         "train_blocks": int(ntrain), "train_steps": steps, "train_batch": batch, "train_s": t_train,
         "train_loss_bits": hist, "sweep_s": t_sweep}
     if sample_blocks > 0:
