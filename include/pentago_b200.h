@@ -195,8 +195,9 @@ int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* s
 int pg_midsolve_batch_noalloc(const uint64_t* raws, int n, pg_mid_values_t* out, void* stream);
 
 /* ---------------------------------------------------------------------------
- * Midsolve server: continuous batching on a persistent kernel (one worker CTA
- * per SM).  Requests are admitted while others run, as long as the request
+ * Midsolve server: continuous batching on a persistent kernel (two worker
+ * CTAs per SM; boards with many empty spots are solved by a gang of workers).
+ * Requests are admitted while others run, as long as the request
  * ring has a free entry and the device scratch budget has room for the
  * board's tables and workspace; otherwise submit returns PG_ERR_CAPACITY and
  * the caller polls and retries.  Workers leave after ~2 s without work and
@@ -208,6 +209,9 @@ int pg_serve_open(int64_t budget_bytes, pg_server_t* server);
 int64_t pg_serve_submit(pg_server_t server, uint64_t raw);          /* ticket >= 0 */
 int pg_serve_poll(pg_server_t server, int64_t ticket, pg_mid_values_t* result); /* 1 done, 0 pending */
 int pg_serve_close(pg_server_t server);
+/* State of the server's workers: 1 running, 2 left after about 2 s without
+ * requests (the next submit relaunches them), 3 closed, 0 never launched. */
+int pg_serve_state(pg_server_t server);
 
 /* ---------------------------------------------------------------------------
  * Static rANS coder for ternary win/tie/loss symbols, byte-identical to the

@@ -100,6 +100,7 @@ SIGNATURES = {
     "pg_serve_submit": (_I64, [_P, _U64]),
     "pg_serve_poll": (_I, [_P, _I64, _P]),
     "pg_serve_close": (_I, [_P]),
+    "pg_serve_state": (_I, [_P]),
     "pg_rans_bound": (_I64, [_I64]),
     "pg_rans_encode_batch": (_I, [_P, _P, _I, _P, _P, _P, _P]),
     "pg_rans_decode_batch": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P]),

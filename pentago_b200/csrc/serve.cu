@@ -270,6 +270,13 @@ extern "C" int pg_serve_poll(pg_server_t h, int64_t ticket, pg_mid_values_t* res
   return done > 0 ? 1 : fail(PG_ERR_BOUNDS, "midsolve bounds check failed");
 }
 
+extern "C" int pg_serve_state(pg_server_t h) {
+  if (!h) return fail(PG_ERR_ARG, "null server");
+  server& S = *reinterpret_cast<server*>(h);
+  std::lock_guard<std::mutex> lock(S.m);
+  return S.launched ? int(S.ctl->status) : 0;
+}
+
 extern "C" int pg_serve_close(pg_server_t h) {
   if (!h) return PG_OK;
   server* S = reinterpret_cast<server*>(h);

@@ -39,6 +39,10 @@ class Server:
         rec = self._rec
         return [(rec.entries[i].raw, rec.entries[i].value) for i in range(rec.size)]
 
+    def state(self):
+        """1 running, 2 workers left after idling, 3 closed, 0 never launched."""
+        return capi.check(capi.lib().pg_serve_state(self._h))
+
     def close(self):
         if self._h:
             capi.check(capi.lib().pg_serve_close(self._h))

@@ -3,6 +3,8 @@ admission under a small scratch budget, and clean close."""
 import numpy as np
 import pytest
 
+from tests.oracle import P
+
 pytestmark = pytest.mark.gpu
 
 
@@ -56,3 +58,25 @@ def test_server_matches_oracle_small_boards(cuda, O):
         res, _, _ = serve.run_stream(S, raws, np.zeros(len(raws)), timeout=60)
     for r, got in zip(raws, res):
         assert got == oracle_values(O, r)
+
+
+def test_idle_workers_leave_and_come_back(cuda, O):
+    """The workers' wait for requests is bounded: with nothing submitted they
+    leave after about 2 s (the host reads the state), and the next submit
+    relaunches them with correct results."""
+    import time
+    from pentago_b200 import mid, serve
+    raws = mid.random_boards(21, 2, 28)
+    with serve.Server(1 << 30) as S:
+        first, _, _ = serve.run_stream(S, raws[:1], np.zeros(1), timeout=60)
+        assert S.state() == 1
+        t0 = time.perf_counter()
+        while S.state() == 1 and time.perf_counter() - t0 < 30:
+            time.sleep(0.2)
+        assert S.state() == 2, "idle workers should have left"
+        second, _, _ = serve.run_stream(S, raws[1:], np.zeros(1), timeout=60)
+        assert S.state() == 1
+    for raw, got in zip(raws, first + second):
+        r, v = np.zeros(200, np.uint64), np.zeros(200, np.int32)
+        n = O.midsolve(int(raw), P(r), P(v))
+        assert got == list(zip(r[:n].tolist(), v[:n].tolist()))
