@@ -322,6 +322,10 @@ int pg_selftest_midsolve_host(const uint64_t* raws, int n, pg_mid_values_t* out,
 /* The same solve split into `groups` cooperating groups (one host thread
  * each, a shared barrier between levels), as the multi-CTA kernel splits it. */
 int pg_selftest_midsolve_groups_host(const uint64_t* raws, int n, int groups, pg_mid_values_t* out);
+/* A CTA waits at a two-CTA barrier that nobody else reaches, with a limit of
+ * `polls` polls: the wait runs out and *fault_out = 1 (device check of the
+ * bounded barrier the multi-CTA midsolve and the server use). */
+int pg_debug_barrier_timeout(unsigned polls, int* fault_out);
 
 #ifdef __cplusplus
 }

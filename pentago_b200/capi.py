@@ -117,6 +117,7 @@ SIGNATURES = {
     "pg_midsolve_workspace_size": (_I, [_I]),
     "pg_selftest_midsolve_host": (_I, [_P, _I, _P, _P]),
     "pg_selftest_midsolve_groups_host": (_I, [_P, _I, _I, _P]),
+    "pg_debug_barrier_timeout": (_I, [ctypes.c_uint, ctypes.POINTER(_I)]),
     "pg_midsolve_scratch_bytes": (_I, [_P, _I, ctypes.POINTER(_I64)]),
     "pg_midsolve_batch": (_I, [_P, _I, _P, _P, _I64, _P]),
     "pg_midsolve_batch_noalloc": (_I, [_P, _I, _P, _P]),

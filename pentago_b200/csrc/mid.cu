@@ -42,6 +42,16 @@ mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict_
   mid_board_body(J, MT, tiles, ws, raw, &fault, threadIdx.x, blockDim.x, 0, 1, sync_threads(), sync_threads());
 }
 
+// One CTA waiting twice at a barrier of two that the other never reaches:
+// the first wait runs out after `polls` polls and marks the fault, the second
+// returns at once (what a board whose CTAs stopped meeting gets).
+__global__ void barrier_timeout_kernel(unsigned* words, int* fault, unsigned polls) {
+  board_barrier gb{words, words + 1, 2, fault};
+  gb.polls = polls;
+  gb();
+  gb();
+}
+
 // A few large boards: ncta CTAs per board (blockIdx.x / ncta), each taking a
 // contiguous share of every level.  bar: 2 words per board; raw: 38 uint4 per
 // board; faults: one per board; all zero at launch.
@@ -265,6 +275,23 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
       if (int rc = launch_grid_boards(d, int(jobs.size()), ncta, smem, T->win_factors, stream)) return rc;
     }
   }
+  return PG_OK;
+}
+
+extern "C" int pg_debug_barrier_timeout(unsigned polls, int* fault_out) {
+  if (!fault_out) return fail(PG_ERR_ARG, "null argument");
+  cudaStream_t st = nullptr;
+  stream_scratch X(st);
+  unsigned* words = nullptr;
+  int* fault = nullptr;
+  PG_CUDA(X.alloc(&words, 2 * sizeof(unsigned)));
+  PG_CUDA(X.alloc(&fault, sizeof(int)));
+  PG_CUDA(cudaMemsetAsync(words, 0, 2 * sizeof(unsigned), st));
+  PG_CUDA(cudaMemsetAsync(fault, 0, sizeof(int), st));
+  barrier_timeout_kernel<<<1, 32, 0, st>>>(words, fault, polls);
+  PG_CUDA(cudaGetLastError());
+  PG_CUDA(cudaMemcpyAsync(fault_out, fault, sizeof(int), cudaMemcpyDeviceToHost, st));
+  PG_CUDA(cudaStreamSynchronize(st));
   return PG_OK;
 }
 

@@ -377,6 +377,7 @@ struct board_barrier {
   unsigned* gen;    // generation number
   int ncta;
   int* fault;
+  unsigned polls = kBarrierPolls;  // wait limit
   __device__ void operator()() const {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -390,7 +391,7 @@ struct board_barrier {
         atomicAdd(gen, 1u);
       } else {
         for (unsigned i = 0; *vg == g && !*vf; i++) {
-          if (i > kBarrierPolls) { atomicExch(fault, 1); break; }
+          if (i > polls) { atomicExch(fault, 1); break; }
           __nanosleep(64);
         }
       }

@@ -60,3 +60,17 @@ def test_midsolve_workspace_sizes(cuda):
     w = json.load(open(os.path.join(GOLD, "workspace.json")))
     for i, size in enumerate(w["sizes"]):
         assert mid.workspace_size(w["first_slice"] + i) == size
+
+
+def test_group_barrier_wait_runs_out_with_a_status(cuda):
+    """The barrier between the CTAs of a board waits a bounded time: a CTA left
+    alone gives up, marks the fault (which fails the board's record) and the
+    kernel ends."""
+    import ctypes
+    import time
+    from pentago_b200 import capi
+    fault = ctypes.c_int(0)
+    t0 = time.perf_counter()
+    capi.check(capi.lib().pg_debug_barrier_timeout(20000, ctypes.byref(fault)))
+    assert fault.value == 1
+    assert time.perf_counter() - t0 < 10
