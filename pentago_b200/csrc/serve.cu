@@ -11,9 +11,9 @@
 // arrives while others are on the GPU joins them as soon as resources free up.
 //
 // Every wait is bounded: an idle worker polls with nanosleep back-off and
-// leaves after a fixed number of polls (status kIdleExit), so a host that
-// stops talking cannot hold the GPU; the host relaunches workers on the next
-// submit.
+// leaves after 2 s without work, by the GPU's global timer and a cap on polls
+// (status kIdleExit), so a host that stops talking cannot hold the GPU; the
+// host relaunches workers on the next submit.
 #include "mid_body.cuh"
 #include "runtime.h"
 #include "../../include/pentago_b200.h"
@@ -26,7 +26,17 @@
 namespace pg {
 
 constexpr int kRing = 1024;
-constexpr unsigned long long kIdlePolls = 2000000ull;  // ~2 s of 1 us sleeps
+// An idle worker leaves after 2 s without work (GPU global timer), or after a
+// hard cap of polls whatever the timer says; its sleep between polls grows to
+// 20 us, so hundreds of idle workers do not flood the bus with mapped reads.
+constexpr unsigned long long kIdleNs = 2000000000ull;
+constexpr unsigned long long kIdlePollsMax = 1000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 enum : int { kRunning = 1, kIdleExit = 2, kClosed = 3, kFault = 4 };
 
 struct serve_entry {          // host-mapped
@@ -75,6 +85,8 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_a
     if (threadIdx.x == 0) {
       claimed = -1;
       unsigned long long polls = 0;
+      const unsigned long long idle_since = global_ns();
+      unsigned sleep_ns = 256;
       for (;;) {
         const unsigned long long h = atomicAdd(head, 0ull);
         const unsigned long long t = ctl->tail;
@@ -83,8 +95,9 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_a
           continue;
         }
         if (ctl->close) { ctl->status = kClosed; break; }
-        if (++polls > kIdlePolls) { ctl->status = kIdleExit; break; }
-        __nanosleep(1000);
+        if (++polls > kIdlePollsMax || global_ns() - idle_since > kIdleNs) { ctl->status = kIdleExit; break; }
+        __nanosleep(sleep_ns);
+        if (sleep_ns < 20000) sleep_ns *= 2;
       }
       fault = 0;
     }
