@@ -209,8 +209,17 @@ PG_HD uint4 pattern_terms(const line_dev_t& L, const dev_tables_t& T, int side, 
   return ldg(reinterpret_cast<const uint4*>(T.term_sub) + DIM * 512 + mask);
 }
 
-PG_HD super8 super_from(const uint4* p) {
-  const uint4 a = p[0], b = p[1];
+// Per-microline results live in shared memory as separate arrays of 16-byte
+// halves (structure of arrays): lanes reading different entries then spread
+// over the banks instead of colliding on the few positions an array of 32- or
+// 64-byte records leaves them.  Pattern results: half h of entry e at
+// h * 2 kMaxPat + e.  Children: quarter c of child j at c * nchild + j.
+PG_HD void pattern_store(uint4* pat, int e, const super8& w) {
+  pat[e] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
+  pat[2 * kMaxPat + e] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
+}
+PG_HD super8 pattern_from(const uint4* pat, int e) {
+  const uint4 a = pat[e], b = pat[2 * kMaxPat + e];
   return super8{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
 }
 
@@ -232,10 +241,11 @@ PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, in
   super8 qn = s_translate(s_rmax(s_not(cw)), l);
   s_phi_runtime(qw, L.g);
   s_phi_runtime(qn, L.g);
-  q[4 * j + 0] = make_uint4(qw.w[0], qw.w[1], qw.w[2], qw.w[3]);
-  q[4 * j + 1] = make_uint4(qw.w[4], qw.w[5], qw.w[6], qw.w[7]);
-  q[4 * j + 2] = make_uint4(qn.w[0], qn.w[1], qn.w[2], qn.w[3]);
-  q[4 * j + 3] = make_uint4(qn.w[4], qn.w[5], qn.w[6], qn.w[7]);
+  const int nc = L.nchild;
+  q[j] = make_uint4(qw.w[0], qw.w[1], qw.w[2], qw.w[3]);
+  q[j + nc] = make_uint4(qw.w[4], qw.w[5], qw.w[6], qw.w[7]);
+  q[j + 2 * nc] = make_uint4(qn.w[0], qn.w[1], qn.w[2], qn.w[3]);
+  q[j + 3 * nc] = make_uint4(qn.w[4], qn.w[5], qn.w[6], qn.w[7]);
 }
 
 // Parent i of a microline (compute.cc:308-356).
@@ -248,8 +258,8 @@ PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab
   const uint32_t mvw[5] = {h.y, h.z, h.w, mw.x, mw.y};
   const int nmoves = int(h.x >> 16 & 0xff);
   // super_wins of both sides, looked up by stone pattern
-  const super8 wins0 = super_from(pats + 2 * int(h.x & 0xff));
-  const super8 wins1 = super_from(pats + 2 * (kMaxPat + int(h.x >> 8 & 0xff)));
+  const super8 wins0 = pattern_from(pats, int(h.x & 0xff));
+  const super8 wins1 = pattern_from(pats, kMaxPat + int(h.x >> 8 & 0xff));
   // Every move wins immediately where super_wins(side0 | move) does; the
   // union over the empty cells is one table evaluation of the union of the
   // covered terms.
@@ -268,7 +278,8 @@ PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab
       const int ir = int(mvw[k >> 1] >> (16 * (k & 1)) & 0xffff);
       const int j = ir >> 2, r = ir & 3;
       if (j >= L.nchild) { *errors |= 1u; continue; }
-      const uint4 a = qs[4 * j], bq = qs[4 * j + 1], cc = qs[4 * j + 2], d = qs[4 * j + 3];
+      const int nc = L.nchild;
+      const uint4 a = qs[j], bq = qs[j + nc], cc = qs[j + 2 * nc], d = qs[j + 3 * nc];
       const super8 qw = {{a.x, a.y, a.z, a.w, bq.x, bq.y, bq.z, bq.w}};
       const super8 qn = {{cc.x, cc.y, cc.z, cc.w, d.x, d.y, d.z, d.w}};
       wins = s_or(wins, s_translate_axis<DIM>(qw, r));
@@ -347,9 +358,7 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
   for (int x = tid; x < M * pp; x += nt) {
     const int k = x / pp, r = x - k * pp, side = r >= p0, rr = side ? r - p0 : r;
     const super8 w = table_eval<DIM>(S.tab[k][side], psub[side * kMaxPat + rr]);
-    uint4* out = S.pat[k] + 2 * (side * kMaxPat + rr);
-    out[0] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
-    out[1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
+    pattern_store(S.pat[k], side * kMaxPat + rr, w);
   }
   if (!L.slice35 && tid < M * nc) {
     // Each thread's next child is loaded while it transforms the current one.
@@ -430,8 +439,7 @@ template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_table
       for (int e = 0; e < kTab; e++) tab[side][e] = table_entry(fterm, c0, e);
       for (int r = 0; r < L.npat[side]; r++) {
         const super8 w = table_eval<DIM>(tab[side], pattern_terms<DIM>(L, T, side, r));
-        pat[2 * (side * kMaxPat + r)] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
-        pat[2 * (side * kMaxPat + r) + 1] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
+        pattern_store(pat.data(), side * kMaxPat + r, w);
       }
     }
     if (!L.slice35)
