@@ -124,7 +124,11 @@ struct micro_ctx {
 
 constexpr int kMaxPat = 126;  // C(9,4): most stone patterns of one count in a quadrant
 constexpr int kTerms = 17;    // win patterns touching one quadrant
-constexpr int kTab = 160;     // subset tables: terms 0-5 (64), 6-11 (64), 12-16 (32)
+constexpr int kTab = 80;      // subset tables: terms 0-3, 4-7, 8-11 (16 entries each), 12-16 (32)
+
+// Chunk of subset-table entry e (the first three tables fill one 128-byte
+// row of shared-memory banks each, so their lookups never conflict).
+PG_HD int table_chunk(int e) { return e < 48 ? e >> 4 : 3; }
 
 // super_wins with the line quadrant DIM varying and the other three fixed,
 // as subset tables.  Each win pattern touching DIM ("term" t) wins at the
@@ -179,11 +183,11 @@ PG_HD uint64_t miss_fixed(const dev_tables_t& T, int u, uint64_t sd) {
 // Entry e of the subset tables from the 17 f_t; the first table also carries
 // c0, the OR of the patterns that miss DIM, so every evaluation includes it.
 PG_HD uint2 table_entry(const uint2* f, uint64_t c0, int e) {
-  const int c = e < 64 ? 0 : e < 128 ? 1 : 2, s = e - 64 * c;
+  const int c = table_chunk(e), s = e - 16 * c;
   uint32_t lo = c ? 0u : uint32_t(c0), hi = c ? 0u : uint32_t(c0 >> 32);
 #pragma unroll
-  for (int b = 0; b < 6; b++)
-    if (s >> b & 1) { lo |= f[6 * c + b].x; hi |= f[6 * c + b].y; }
+  for (int b = 0; b < 5; b++)
+    if (s >> b & 1) { lo |= f[4 * c + b].x; hi |= f[4 * c + b].y; }
   return make_uint2(lo, hi);
 }
 
@@ -194,9 +198,10 @@ PG_HD super8 table_eval(const uint2* tab, const uint4 sub) {
   const uint32_t S[4] = {sub.x, sub.y, sub.z, sub.w};
 #pragma unroll
   for (int d = 0; d < 4; d++) {
-    const uint2 a = tab[S[d] & 63], b = tab[64 + (S[d] >> 6 & 63)], c = tab[128 + (S[d] >> 12 & 31)];
-    r.w[2 * d] = a.x | b.x | c.x;
-    r.w[2 * d + 1] = a.y | b.y | c.y;
+    const uint2 a = tab[S[d] & 15], b = tab[16 + (S[d] >> 4 & 15)], c = tab[32 + (S[d] >> 8 & 15)],
+                e = tab[48 + (S[d] >> 12 & 31)];
+    r.w[2 * d] = a.x | b.x | c.x | e.x;
+    r.w[2 * d + 1] = a.y | b.y | c.y | e.y;
   }
   if constexpr (DIM != 3) s_swap_axes<DIM, 3>(r);
   return r;
@@ -339,15 +344,15 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
 #pragma unroll
     for (int o = 16; o; o >>= 1) c0 |= __shfl_xor_sync(0xffffffffu, c0, o);
 #pragma unroll
-    for (int j = 0; j < 5; j++) {
-      const int e = lane + 32 * j, c = j < 2 ? 0 : j < 4 ? 1 : 2, sub = e - 64 * c;
+    for (int j = 0; j < (kTab + 31) / 32; j++) {
+      const int e = lane + 32 * j, c = table_chunk(e), sub = e - 16 * c;
       uint64_t v = c ? 0 : c0;
 #pragma unroll
-      for (int b = 0; b < 6; b++) {
-        const uint64_t fb = __shfl_sync(0xffffffffu, f, 6 * c + b);
-        if (sub >> b & 1 && 6 * c + b < kTerms) v |= fb;
+      for (int b = 0; b < 5; b++) {
+        const uint64_t fb = __shfl_sync(0xffffffffu, f, 4 * c + b < kTerms ? 4 * c + b : 0);
+        if (sub >> b & 1) v |= fb;
       }
-      S.tab[k][side][e] = make_uint2(uint32_t(v), uint32_t(v >> 32));
+      if (e < kTab) S.tab[k][side][e] = make_uint2(uint32_t(v), uint32_t(v >> 32));
     }
   }
   for (int x = tid; x < pp; x += nt) {
