@@ -30,6 +30,7 @@ extern "C" {
 #define PG_ERR_TIMEOUT -4  /* a bounded device wait ran out */
 #define PG_ERR_FORMAT -5   /* malformed encoded stream */
 #define PG_ERR_CAPACITY -6 /* output buffer too small / budget exceeded */
+#define PG_ERR_IO -7       /* a file could not be opened, read or written */
 
 const char* pg_last_error(void);
 
@@ -296,6 +297,92 @@ int pg_learned_adam(float* params, float* m, float* v, const float* grad, int64_
                     void* stream);
 /* Serialize host fp32 parameters into a model (host, pg_learned_model_bytes). */
 int pg_learned_export(const float* params, uint8_t* model);
+
+/* ---------------------------------------------------------------------------
+ * Slice files: the reference's .pentago supertensor format
+ * (pentago/data/supertensor.h:1-232, supertensor.cc), single-section files
+ * ("pentago supertensor\n") and multiple-section files ("pentago sections
+ * \n", version 3).  Blocks are compressed independently with zlib (level
+ * 1-9) or xz (level 20 + preset), as compress() does in
+ * pentago/data/compress.cc:34-60; xz needs liblzma.so.5 at run time.  On disk
+ * a node is the pair [black wins, white wins]; filter 1 interleaves the bits
+ * of the two supers (interleave_super, pentago/data/filter.h:76-127).  The
+ * filter and the conversion to and from the end engine's [we win, we win or
+ * tie] nodes (pentago/mpi/io.cc:79-86, 476-481) run on the GPU; compression
+ * runs on host threads.
+ *
+ * `turn` arguments: 0 = black to move (even slices), 1 = white to move, both
+ * converting to/from the end engine's node form; PG_ST_RAW keeps the on-disk
+ * pair.  Blocks are named by (section index in the file, 4 block coordinates);
+ * their nodes are row-major in the block's own shape.
+ * ------------------------------------------------------------------------- */
+
+#define PG_ST_RAW 2
+
+typedef struct {
+  uint32_t version;     /* 2 or 3 */
+  uint32_t valid;       /* 1 once the file was finalized */
+  uint32_t stones;
+  uint32_t block_size;  /* even, 2..26 */
+  uint64_t section;     /* section signature (counts as in pg_line_t.section) */
+  uint16_t shape[4];
+  uint16_t blocks[4];   /* ceil(shape / block_size) */
+  uint32_t filter;      /* 0 none, 1 interleave */
+  uint32_t reserved;
+  uint64_t index[3];    /* compressed block index: uncompressed size, compressed size, offset */
+} pg_supertensor_header_t;
+
+/* The 85-byte packed header (supertensor_header_t::pack / unpack,
+ * pentago/data/supertensor.cc:95-129); unpack checks the magic string. */
+int pg_supertensor_header_pack(const pg_supertensor_header_t* h, uint8_t* out85);
+int pg_supertensor_header_unpack(const uint8_t* in85, pg_supertensor_header_t* h);
+
+/* Filter n nodes (device) into their on-disk bytes (device, 64 per node), and back. */
+int pg_supertensor_filter(const uint64_t* nodes, int64_t n, int turn, int filter, uint8_t* out, void* stream);
+int pg_supertensor_unfilter(const uint8_t* in, int64_t n, int turn, int filter, uint64_t* nodes, void* stream);
+
+/* Reading (supertensor_reader_t, open_supertensors).  pg_supertensor_open
+ * returns the number of sections; every header is checked as the reference's
+ * reader checks it (supertensor.cc:143-192), and the block indices are read. */
+typedef struct pg_supertensor_reader_s* pg_supertensor_reader_t;
+int pg_supertensor_open(const char* path, pg_supertensor_reader_t* reader);
+int pg_supertensor_header(pg_supertensor_reader_t reader, int section, pg_supertensor_header_t* h);
+/* blob3 = uncompressed size, compressed size, file offset of one block */
+int pg_supertensor_block_blob(pg_supertensor_reader_t reader, int section, const uint8_t* block4, uint64_t* blob3);
+/* Block i = (sections[i], blocks[4i .. 4i+3]): read and decompress its
+ * on-disk bytes into host memory at out + out_offsets[i], on `threads` host
+ * threads (0 = every core). */
+int pg_supertensor_read_blocks_host(pg_supertensor_reader_t reader, int n, const int32_t* sections,
+                                    const uint8_t* blocks, uint8_t* out, const int64_t* out_offsets, int threads);
+/* The same blocks into device memory, unfiltered on the GPU: block i's nodes
+ * go to nodes + 8 * node_offsets[i].  Decompression of one batch overlaps the
+ * copy and unfilter of the previous one. */
+int pg_supertensor_read_blocks(pg_supertensor_reader_t reader, int n, const int32_t* sections, const uint8_t* blocks,
+                               uint64_t* nodes, const int64_t* node_offsets, int turn, int threads, void* stream);
+int pg_supertensor_close(pg_supertensor_reader_t reader);
+
+/* Writing (supertensor_writer_t, supertensor_writers).  A file of sections
+ * sections[0..n); multiple = 0 writes a single-section file (n = 1).  Blocks
+ * are placed in the order they are written; each may be written once. */
+typedef struct pg_supertensor_writer_s* pg_supertensor_writer_t;
+int pg_supertensor_create(const char* path, const uint64_t* sections, int n, int multiple, int block_size, int filter,
+                          int level, pg_supertensor_writer_t* writer);
+/* Blocks whose on-disk bytes (already filtered) are in host memory. */
+int pg_supertensor_write_blocks_host(pg_supertensor_writer_t writer, int n, const int32_t* sections,
+                                     const uint8_t* blocks, const uint8_t* data, const int64_t* data_offsets,
+                                     int threads);
+/* Blocks whose nodes are in device memory (block i at nodes + 8 *
+ * node_offsets[i]): filtered on the GPU and compressed on host threads while
+ * the GPU filters and copies the next batch. */
+int pg_supertensor_write_blocks(pg_supertensor_writer_t writer, int n, const int32_t* sections, const uint8_t* blocks,
+                                const uint64_t* nodes, const int64_t* node_offsets, int turn, int threads,
+                                void* stream);
+/* Write the block index and the header of one section (-1: every section);
+ * fails if a block of it was never written. */
+int pg_supertensor_finalize(pg_supertensor_writer_t writer, int section);
+/* Close; a file with an unfinalized section is removed, as the reference's
+ * writer removes it (supertensor.cc:281-289). */
+int pg_supertensor_writer_close(pg_supertensor_writer_t writer);
 
 /* ---------------------------------------------------------------------------
  * Unit-level device operations, used by tests to check the superscore

@@ -1117,3 +1117,72 @@ int64_t or_rans_decode(const u8* data, int64_t size, u8* sym, int64_t cap) {  /*
   }
   return (int64_t)n;
 }
+
+/* ------------------------------------------------------------------------
+ * Slice-file filter (pentago/data/filter.h:76-127, portable forms) and the
+ * conversion between [win, notlost] nodes and the on-disk [black wins,
+ * white wins] pair (pentago/mpi/io.cc:79-86 writing, 476-481 reading).
+ * ------------------------------------------------------------------------ */
+static u64 st_expand(u64 a) { /* low 32 bits to the even bits */
+  a &= 0x00000000ffffffffull;
+  a = (a | a << 16) & 0x0000ffff0000ffffull;
+  a = (a | a << 8) & 0x00ff00ff00ff00ffull;
+  a = (a | a << 4) & 0x0f0f0f0f0f0f0f0full;
+  a = (a | a << 2) & 0x3333333333333333ull;
+  a = (a | a << 1) & 0x5555555555555555ull;
+  return a;
+}
+static u64 st_contract(u64 a) { /* even bits to the low 32 bits */
+  a &= 0x5555555555555555ull;
+  a = (a | a >> 1) & 0x3333333333333333ull;
+  a = (a | a >> 2) & 0x0f0f0f0f0f0f0f0full;
+  a = (a | a >> 4) & 0x00ff00ff00ff00ffull;
+  a = (a | a >> 8) & 0x0000ffff0000ffffull;
+  a = (a | a >> 16) & 0x00000000ffffffffull;
+  return a;
+}
+
+void or_st_filter(const u64* nodes, int64_t n, int turn, int filter, u64* out) {
+  for (int64_t i = 0; i < n; i++) {
+    const u64* x = nodes + 8 * i;
+    u64 s0[4], s1[4], *o = out + 8 * i;
+    for (int k = 0; k < 4; k++) {
+      if (turn == 0) { s0[k] = x[k]; s1[k] = ~x[4 + k]; }
+      else if (turn == 1) { s0[k] = ~x[4 + k]; s1[k] = x[k]; }
+      else { s0[k] = x[k]; s1[k] = x[4 + k]; }
+    }
+    if (!filter) {
+      for (int k = 0; k < 4; k++) { o[k] = s0[k]; o[4 + k] = s1[k]; }
+      continue;
+    }
+    /* super h of the output interleaves words 2h, 2h+1 of both supers:
+       LO(a)|LO(a')<<1, HI(a)|HI(a')<<1, LO(b)|LO(b')<<1, HI(b)|HI(b')<<1 */
+    for (int h = 0; h < 2; h++)
+      for (int j = 0; j < 2; j++) {
+        const u64 a = s0[2 * h + j], b = s1[2 * h + j];
+        o[4 * h + 2 * j] = st_expand(a) | st_expand(b) << 1;
+        o[4 * h + 2 * j + 1] = st_expand(a >> 32) | st_expand(b >> 32) << 1;
+      }
+  }
+}
+
+void or_st_unfilter(const u64* in, int64_t n, int turn, int filter, u64* nodes) {
+  for (int64_t i = 0; i < n; i++) {
+    const u64* x = in + 8 * i;
+    u64 s0[4], s1[4], *o = nodes + 8 * i;
+    for (int m = 0; m < 4; m++) {
+      if (filter) {
+        s0[m] = st_contract(x[2 * m]) | st_contract(x[2 * m + 1]) << 32;
+        s1[m] = st_contract(x[2 * m] >> 1) | st_contract(x[2 * m + 1] >> 1) << 32;
+      } else {
+        s0[m] = x[m];
+        s1[m] = x[4 + m];
+      }
+    }
+    for (int k = 0; k < 4; k++) {
+      if (turn == 0) { o[k] = s0[k]; o[4 + k] = ~s1[k]; }
+      else if (turn == 1) { o[k] = s1[k]; o[4 + k] = ~s0[k]; }
+      else { o[k] = s0[k]; o[4 + k] = s1[k]; }
+    }
+  }
+}

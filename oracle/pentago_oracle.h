@@ -47,6 +47,14 @@ int or_midsolve(uint64_t raw, uint64_t* out_raws, int32_t* out_values);
 void or_midsolve_internal(uint64_t raw, uint64_t* out);
 int or_midsolve_workspace_size(int stones);
 
+/* Slice-file filter: the interleave of pentago/data/filter.h:76-127 (the
+ * portable forms) with the node-form conversion of the slice writer and
+ * reader, pentago/mpi/io.cc:79-86 and 476-481.  turn 0/1 converts from/to
+ * [win, notlost] nodes of the side to move; turn 2 keeps the on-disk
+ * [black wins, white wins] pair.  filter 0 leaves the bits in place. */
+void or_st_filter(const uint64_t* nodes, int64_t n, int turn, int filter, uint64_t* out);
+void or_st_unfilter(const uint64_t* in, int64_t n, int turn, int filter, uint64_t* nodes);
+
 int64_t or_rans_encode(const uint8_t* symbols, int64_t n, uint8_t* out, int64_t cap);
 int64_t or_rans_decode(const uint8_t* data, int64_t size, uint8_t* symbols, int64_t cap);
 

@@ -10,6 +10,9 @@
 //   ref_count_block_wins              end/block_store.cc:330-352
 //   ref_midsolve                      mid/midengine.cc:161-169 (+ midsolve_traverse :127-158)
 //   ref_rans_encode / ref_rans_decode shard/arithmetic.cc:366-452 (+ serialize :456-495)
+//   ref_random_supers                 base/superscore.cc:118-127
+//   ref_st_interleave                 data/filter.cc (interleave / uninterleave)
+//   ref_block_write_order             data/supertensor_test.cc:31-55 (iteration order of its block map)
 
 #include "pentago/base/board.h"
 #include "pentago/base/count.h"
@@ -20,16 +23,19 @@
 #include "pentago/end/blocks.h"
 #include "pentago/end/compute.h"
 #include "pentago/end/sections.h"
+#include "pentago/data/filter.h"
 #include "pentago/high/board.h"
 #include "pentago/mid/halfsuper.h"
 #include "pentago/mid/midengine.h"
 #include "pentago/shard/arithmetic.h"
 #include "pentago/shard/ternary.h"
 #include "pentago/utility/thread.h"
+#include "pentago/utility/vector.h"
 #include <atomic>
 #include <condition_variable>
 #include <cstring>
 #include <mutex>
+#include <unordered_map>
 
 using namespace pentago;
 using namespace pentago::end;
@@ -266,6 +272,42 @@ int64_t ref_rans_decode(const uint8_t* data, int64_t size, uint8_t* symbols, int
   } catch (...) {
     return -2;
   }
+}
+
+// random_supers(key, n) with key = hi << 64 | lo: n supers of 4 words each.
+void ref_random_supers(uint64_t key_hi, uint64_t key_lo, int n, uint64_t* out) {
+  const auto s = random_supers((uint128_t(key_hi) << 64) | key_lo, n);
+  for (int i = 0; i < n; i++) store_super(out + 4 * i, s[i]);
+}
+
+// interleave (inverse = 0) or uninterleave (1) n on-disk pairs in place.
+void ref_st_interleave(uint64_t* data, int64_t n, int inverse) {
+  Array<Vector<super_t,2>> a(static_cast<int>(n));
+  for (int64_t i = 0; i < n; i++)
+    for (int k = 0; k < 2; k++) a[i][k] = load_super(data + 8 * i + 4 * k);
+  if (inverse) uninterleave(a);
+  else interleave(a);
+  for (int64_t i = 0; i < n; i++)
+    for (int k = 0; k < 2; k++) store_super(data + 8 * i + 4 * k, a[i][k]);
+}
+
+// The order in which supertensor_test.cc writes its blocks: it inserts every
+// block of a blocks[0] x .. x blocks[3] grid, in row-major order, into an
+// unordered_map keyed by Vector<uint8_t,4> and writes them in the map's
+// iteration order.  Returns the block count; out gets 4 bytes per block.
+int ref_block_write_order(const int* blocks, uint8_t* out) {
+  std::unordered_map<Vector<uint8_t,4>, int> data;
+  for (int i = 0; i < blocks[0]; i++)
+    for (int j = 0; j < blocks[1]; j++)
+      for (int k = 0; k < blocks[2]; k++)
+        for (int l = 0; l < blocks[3]; l++)
+          data[vec(uint8_t(i), uint8_t(j), uint8_t(k), uint8_t(l))] = 0;
+  int n = 0;
+  for (const auto& e : data) {
+    for (int a = 0; a < 4; a++) out[4 * n + a] = e.first[a];
+    n++;
+  }
+  return n;
 }
 
 }  // extern "C"

@@ -50,7 +50,7 @@ def build(verbose=False, jobs=None):
         raise RuntimeError("nvcc failed")
     if not procs and os.path.exists(LIB):
         return LIB
-    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread"]
+    cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-ldl", "-lpthread", "-lz"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)

@@ -17,6 +17,7 @@ PG_ERR_BOUNDS = -3
 PG_ERR_TIMEOUT = -4
 PG_ERR_FORMAT = -5
 PG_ERR_CAPACITY = -6
+PG_ERR_IO = -7
 
 PG_LINE_STORE = 0
 PG_LINE_OR = 1
@@ -72,6 +73,13 @@ class pg_mid_values_t(ctypes.Structure):
 
 MID_VALUES_BYTES = 8 + 16 * 163
 
+
+class pg_supertensor_header_t(ctypes.Structure):
+    _fields_ = [("version", ctypes.c_uint32), ("valid", ctypes.c_uint32), ("stones", ctypes.c_uint32),
+                ("block_size", ctypes.c_uint32), ("section", ctypes.c_uint64), ("shape", ctypes.c_uint16 * 4),
+                ("blocks", ctypes.c_uint16 * 4), ("filter", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("index", ctypes.c_uint64 * 3)]
+
 # Every exported symbol of include/pentago_b200.h with its ctypes signature.
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -121,6 +129,21 @@ SIGNATURES = {
     "pg_midsolve_scratch_bytes": (_I, [_P, _I, ctypes.POINTER(_I64)]),
     "pg_midsolve_batch": (_I, [_P, _I, _P, _P, _I64, _P]),
     "pg_midsolve_batch_noalloc": (_I, [_P, _I, _P, _P]),
+    "pg_supertensor_header_pack": (_I, [ctypes.POINTER(pg_supertensor_header_t), _P]),
+    "pg_supertensor_header_unpack": (_I, [_P, ctypes.POINTER(pg_supertensor_header_t)]),
+    "pg_supertensor_filter": (_I, [_P, _I64, _I, _I, _P, _P]),
+    "pg_supertensor_unfilter": (_I, [_P, _I64, _I, _I, _P, _P]),
+    "pg_supertensor_open": (_I, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+    "pg_supertensor_header": (_I, [_P, _I, ctypes.POINTER(pg_supertensor_header_t)]),
+    "pg_supertensor_block_blob": (_I, [_P, _I, _P, _P]),
+    "pg_supertensor_read_blocks_host": (_I, [_P, _I, _P, _P, _P, _P, _I]),
+    "pg_supertensor_read_blocks": (_I, [_P, _I, _P, _P, _P, _P, _I, _I, _P]),
+    "pg_supertensor_close": (_I, [_P]),
+    "pg_supertensor_create": (_I, [ctypes.c_char_p, _P, _I, _I, _I, _I, _I, ctypes.POINTER(_P)]),
+    "pg_supertensor_write_blocks_host": (_I, [_P, _I, _P, _P, _P, _P, _I]),
+    "pg_supertensor_write_blocks": (_I, [_P, _I, _P, _P, _P, _P, _I, _I, _P]),
+    "pg_supertensor_finalize": (_I, [_P, _I]),
+    "pg_supertensor_writer_close": (_I, [_P]),
 }
 
 _lib = None

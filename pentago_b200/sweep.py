@@ -8,12 +8,16 @@ returned in the format of data/counts-N.npy (mpi/io.cc:573-581):
 [sig, black wins, white wins, total] over distinct positions.
 
     python -m pentago_b200.sweep --root 4,4,4,5,4,3,3,3 [--min-slice 30]
+        [--checkpoint DIR] [--resume DIR/slice-N.pentago]
 
-runs the sweep and prints one JSON line of timings and HBM throughput.
+runs the sweep and prints one JSON line of timings and HBM throughput.  With
+--checkpoint every solved slice is also written as a .pentago slice file
+(the reference's format), and --resume starts from such a file.
 """
 import argparse
 import ctypes
 import json
+import os
 import time
 
 import numpy as np
@@ -49,8 +53,18 @@ def to_golden(sigs, counts, slice_):
     return out
 
 
-def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None):
+def _slice_of(path):
+    from .supertensor import supertensor_slice
+    return supertensor_slice(path)
+
+
+def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, checkpoint=None, resume=None, level=6):
     """Solve all sections below `root` from slice 35 down to `min_slice`.
+
+    checkpoint: a directory that receives every solved slice as
+    slice-N.pentago (the reference's slice file format).  resume: a slice
+    file (slice N, holding at least the sections the root needs at N) to
+    start from instead of solving slices 35..N again.
 
     Returns {slice: counts-N rows}; with keep_last also the last slice tensor."""
     import torch
@@ -62,7 +76,14 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None):
     child_sigs = np.zeros(0, np.uint64)
     child = None
     results = {}
-    for slice_ in range(35, min_slice - 1, -1):
+    top = 35
+    if resume is not None:
+        from .supertensor import read_slice
+        start = _slice_of(resume)
+        child_sigs = descendent_sections(root, start)
+        _, child_sigs, child = read_slice(resume, child_sigs, stream=stream)
+        top = start - 1
+    for slice_ in range(top, min_slice - 1, -1):
         sigs = descendent_sections(root, slice_)
         torch.cuda.synchronize()
         off = slice_layout(sigs)
@@ -77,6 +98,10 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None):
         capi.check(L.pg_section_counts(capi.ptr(sigs), len(sigs), parent.data_ptr(), counts.data_ptr(), s_handle))
         c = counts.cpu().numpy().view(np.uint64)
         results[slice_] = to_golden(sigs, c, slice_)
+        if checkpoint is not None:
+            from .supertensor import write_slice
+            write_slice(os.path.join(checkpoint, f"slice-{slice_}.pentago"), slice_, sigs, parent, level=level,
+                        stream=stream)
         if timings is not None:
             torch.cuda.synchronize()
             timings[slice_] = {"ms": t0.elapsed_time(t1), "sections": len(sigs), "nodes": int(off[-1]),
@@ -94,6 +119,9 @@ def main():
     ap.add_argument("--root", default="4,4,4,5,4,3,3,3")
     ap.add_argument("--min-slice", type=int, default=None)
     ap.add_argument("--golden", default=None, help="npz of counts_N arrays to compare against")
+    ap.add_argument("--checkpoint", default=None, help="directory for slice-N.pentago files of every solved slice")
+    ap.add_argument("--resume", default=None, help="slice file to start from")
+    ap.add_argument("--level", type=int, default=6, help="compression level of checkpoint files (zlib 1-9, xz 20-29)")
     args = ap.parse_args()
     c = [int(x) for x in args.root.split(",")]
     root = section_sig([[c[0], c[1]], [c[2], c[3]], [c[4], c[5]], [c[6], c[7]]])
@@ -103,7 +131,8 @@ def main():
     torch.cuda.synchronize()
     timings = {}
     t = time.perf_counter()
-    res = sweep(root, args.min_slice, timings=timings)
+    res = sweep(root, args.min_slice, timings=timings, checkpoint=args.checkpoint, resume=args.resume,
+                level=args.level)
     wall = time.perf_counter() - t
     ok = None
     if args.golden:

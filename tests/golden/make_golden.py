@@ -15,6 +15,12 @@ Fixtures written:
                      data/counts-{30..35}.npy
   lines.json         block lines computed by the reference engine itself (oracle/_ref)
                      on seeded inputs: the seed and the SHA-1 of the output
+  supertensor.json   the parameters and expected file SHA-1s of
+                     pentago/data/supertensor_test.cc, with the order in which that
+                     test writes its blocks (its unordered_map's iteration order,
+                     taken from the reference compiled in place)
+  db/slice-N.pentago the reference's solved database for slices 0..5 (data/), and
+  counts_0_5.npz     its per-section counts (data/counts-{0..5}.npy)
 """
 import ctypes
 import json
@@ -109,6 +115,32 @@ def main(ref_root):
                       "seed": seed, "input_nodes": ni.value, "output_nodes": no.value,
                       "output_sha1": hashlib.sha1(res.tobytes()).hexdigest()})
     json.dump(lines, open(os.path.join(HERE, "lines.json"), "w"), indent=1)
+
+    # 7. supertensor_test.cc: parameters, hashes, block write order
+    st = src("pentago/data/supertensor_test.cc")
+    sec = numbers(re.search(r"const section_t section\(\{(.*?)\}\);", st, re.S).group(1))
+    order_blocks = numbers(re.search(r"ASSERT_EQ\(blocks, vec<uint16_t>\((.*?)\)\)", st).group(1))
+    blocks = (ctypes.c_int * 4)(*order_blocks)
+    order = np.zeros(4 * int(np.prod(order_blocks)), np.uint8)
+    n = R.lib.ref_block_write_order(blocks, ctypes.c_void_p(order.ctypes.data))
+    json.dump({"section": [sec[0:2], sec[2:4], sec[4:6], sec[6:8]],
+               "block_size": numbers(re.search(r"const int block_size = (\d+);", st).group(1))[0],
+               "filter": numbers(re.search(r"const int filter = (\d+);", st).group(1))[0],
+               "level": numbers(re.search(r"const int level = (\d+);", st).group(1))[0],
+               "key": numbers(re.search(r"uint128_t key = (\d+);", st).group(1))[0],
+               "blocks": order_blocks,
+               "write_order": order[:4 * n].reshape(-1, 4).tolist(),
+               "sha1": re.findall(r'hash == "([0-9a-f]{40})"', st)},
+              open(os.path.join(HERE, "supertensor.json"), "w"), indent=1)
+
+    # 8. the solved database of slices 0..5 and its counts
+    import shutil
+    os.makedirs(os.path.join(HERE, "db"), exist_ok=True)
+    for s in range(6):
+        shutil.copyfile(os.path.join(ref_root, "data", f"slice-{s}.pentago"),
+                        os.path.join(HERE, "db", f"slice-{s}.pentago"))
+    np.savez_compressed(os.path.join(HERE, "counts_0_5.npz"),
+                        **{f"counts_{s}": np.load(os.path.join(ref_root, "data", f"counts-{s}.npy")) for s in range(6)})
     print("wrote fixtures to", HERE)
 
 

@@ -34,6 +34,8 @@ SIGS = {
     "midsolve": (_i, [_u64, _p, _p]),
     "midsolve_internal": (None, [_u64, _p]),
     "midsolve_workspace_size": (_i, [_i]),
+    "st_filter": (None, [_p, _i64, _i, _i, _p]),
+    "st_unfilter": (None, [_p, _i64, _i, _i, _p]),
     "rans_encode": (_i64, [_p, _i64, _p, _i64]),
     "rans_decode": (_i64, [_p, _i64, _p, _i64]),
     "lm_nodes": (_i64, [_u64, _p]),
