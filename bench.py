@@ -317,6 +317,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-coder measurement")
+    ap.add_argument("--no-slice-files", action="store_true", help="skip the slice-file filter and I/O measurement")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -445,6 +446,7 @@ def main():
     midsolve = None
     learned = None
     sweep2 = None
+    slice_files = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(seconds=12.0)
     if rank == 0 and world == 1:
@@ -464,6 +466,15 @@ def main():
             learned["cpu_static_coder"] = cpu_static_coder_rate(*sample, seconds=5.0)
             sweep2["cpu_baseline"] = cpu_sweep_estimate(CONFIG2_ROOT, timings, seconds_per_slice=1.5)
             sweep2["kernel_speedup_vs_cpu_estimate"] = sweep2["cpu_baseline"]["estimated_s"] / (sweep2["kernel_ms"] / 1e3)
+
+    if rank == 0 and world == 1 and not args.no_slice_files:
+        # The .pentago slice files: filter kernels alone against the HBM
+        # roofline, and a real 2.7 GB slice written and read back end to end
+        torch.cuda.empty_cache()
+        from pentago_b200 import supertensor
+        slice_files = {"filter_kernels": supertensor.bench_filter(), "slice_io": supertensor.bench_slice_io(levels=(1,))}
+        for k in ("filter", "unfilter"):
+            slice_files["filter_kernels"][k]["frac_of_hbm_peak"] = slice_files["filter_kernels"][k]["GBps"] / peak
 
     if rank == 0:
         result = {
@@ -488,6 +499,7 @@ def main():
             "midsolve_config0": midsolve,
             "sweep_config2": sweep2,
             "learned_rans_config3": learned,
+            "slice_files": slice_files,
             "clocks": clocks.summary(),
         }
         print(json.dumps(result))

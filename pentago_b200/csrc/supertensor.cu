@@ -50,36 +50,44 @@ struct seg_t {
   int64_t src, dst, n;  // node offsets into the source and destination, node count
 };
 
-// Bits 0..31 of x to the even bits of a 64-bit word (Morton spreading).
-__device__ __forceinline__ uint64_t spread_even(uint32_t x) {
-  uint64_t a = x;
-  a = (a | a << 16) & 0x0000ffff0000ffffull;
-  a = (a | a << 8) & 0x00ff00ff00ff00ffull;
-  a = (a | a << 4) & 0x0f0f0f0f0f0f0f0full;
-  a = (a | a << 2) & 0x3333333333333333ull;
-  a = (a | a << 1) & 0x5555555555555555ull;
-  return a;
+// Bit interleave of two 16-bit halves: z = [x0 x1 y0 y1] (bytes, from a
+// byte permute) becomes x's bits at the even and y's at the odd positions by
+// three delta swaps (the outer perfect shuffle, Hacker's Delight 7-2, after
+// its first stage, which the byte permute already did).  unshuffle32 undoes
+// the three swaps in reverse order (each swap is its own inverse).
+__device__ __forceinline__ uint32_t delta_swap(uint32_t z, uint32_t m, int k) {
+  const uint32_t t = (z ^ (z >> k)) & m;
+  return z ^ t ^ (t << k);
+}
+__device__ __forceinline__ uint32_t shuffle32(uint32_t z) {
+  z = delta_swap(z, 0x00f000f0u, 4);
+  z = delta_swap(z, 0x0c0c0c0cu, 2);
+  return delta_swap(z, 0x22222222u, 1);
+}
+__device__ __forceinline__ uint32_t unshuffle32(uint32_t z) {
+  z = delta_swap(z, 0x22222222u, 1);
+  z = delta_swap(z, 0x0c0c0c0cu, 2);
+  return delta_swap(z, 0x00f000f0u, 4);
 }
 
-// The even bits of x gathered into 32 bits (inverse of spread_even).
-__device__ __forceinline__ uint32_t gather_even(uint64_t x) {
-  uint64_t a = x & 0x5555555555555555ull;
-  a = (a | a >> 1) & 0x3333333333333333ull;
-  a = (a | a >> 2) & 0x0f0f0f0f0f0f0f0full;
-  a = (a | a >> 4) & 0x00ff00ff00ff00ffull;
-  a = (a | a >> 8) & 0x0000ffff0000ffffull;
-  a = (a | a >> 16) & 0x00000000ffffffffull;
-  return uint32_t(a);
+// One interleaved 64-bit word from 32 bits of each super: bit i of a goes to
+// bit 2i, bit i of b to bit 2i+1 (EXPAND(a) | EXPAND(b) << 1 of filter.h).
+__device__ __forceinline__ uint2 interleave_word(uint32_t a, uint32_t b) {
+  return make_uint2(shuffle32(__byte_perm(a, b, 0x5140)), shuffle32(__byte_perm(a, b, 0x7362)));
+}
+// Its inverse: the even bits of w to a, the odd bits to b.
+__device__ __forceinline__ void deinterleave_word(uint2 w, uint32_t& a, uint32_t& b) {
+  const uint32_t lo = unshuffle32(w.x), hi = unshuffle32(w.y);
+  a = __byte_perm(lo, hi, 0x6420);
+  b = __byte_perm(lo, hi, 0x7531);
 }
 
 __device__ __forceinline__ uint4 u4_not(uint4 a) { return make_uint4(~a.x, ~a.y, ~a.z, ~a.w); }
-__device__ __forceinline__ uint4 u4_of(uint64_t lo, uint64_t hi) {
-  return make_uint4(uint32_t(lo), uint32_t(lo >> 32), uint32_t(hi), uint32_t(hi >> 32));
-}
+__device__ __forceinline__ uint4 u4_of(uint2 lo, uint2 hi) { return make_uint4(lo.x, lo.y, hi.x, hi.y); }
 
 // Nodes -> on-disk bytes.  Node form [we win, we win or tie] becomes [black
 // wins, white wins] (io.cc:79-86); PG_ST_RAW nodes already are that pair.
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 8)
 st_filter_kernel(const uint4* __restrict__ in, uint4* __restrict__ out, const seg_t* __restrict__ segs, int seg0,
                  int turn, int filter) {
   const seg_t s = segs[seg0 + blockIdx.y];
@@ -94,8 +102,8 @@ st_filter_kernel(const uint4* __restrict__ in, uint4* __restrict__ out, const se
     else if (turn == 1) { s0 = u4_not(b); s1 = a; }
     else { s0 = a; s1 = b; }
     if (filter) {
-      q[2 * h] = u4_of(spread_even(s0.x) | spread_even(s1.x) << 1, spread_even(s0.y) | spread_even(s1.y) << 1);
-      q[2 * h + 1] = u4_of(spread_even(s0.z) | spread_even(s1.z) << 1, spread_even(s0.w) | spread_even(s1.w) << 1);
+      q[2 * h] = u4_of(interleave_word(s0.x, s1.x), interleave_word(s0.y, s1.y));
+      q[2 * h + 1] = u4_of(interleave_word(s0.z, s1.z), interleave_word(s0.w, s1.w));
     } else {
       q[h] = s0;
       q[2 + h] = s1;
@@ -104,7 +112,7 @@ st_filter_kernel(const uint4* __restrict__ in, uint4* __restrict__ out, const se
 }
 
 // On-disk bytes -> nodes (uninterleave_super, filter.h:102-127, then io.cc:476-481).
-__global__ void __launch_bounds__(256, 4)
+__global__ void __launch_bounds__(256, 8)
 st_unfilter_kernel(const uint4* __restrict__ in, uint4* __restrict__ out, const seg_t* __restrict__ segs, int seg0,
                    int turn, int filter) {
   const seg_t s = segs[seg0 + blockIdx.y];
@@ -116,10 +124,10 @@ st_unfilter_kernel(const uint4* __restrict__ in, uint4* __restrict__ out, const 
     uint4 s0, s1;
     if (filter) {
       const uint4 u = p[2 * h], v = p[2 * h + 1];  // interleaved super h
-      const uint64_t w0 = uint64_t(u.y) << 32 | u.x, w1 = uint64_t(u.w) << 32 | u.z,
-                     w2 = uint64_t(v.y) << 32 | v.x, w3 = uint64_t(v.w) << 32 | v.z;
-      s0 = make_uint4(gather_even(w0), gather_even(w1), gather_even(w2), gather_even(w3));
-      s1 = make_uint4(gather_even(w0 >> 1), gather_even(w1 >> 1), gather_even(w2 >> 1), gather_even(w3 >> 1));
+      deinterleave_word(make_uint2(u.x, u.y), s0.x, s1.x);
+      deinterleave_word(make_uint2(u.z, u.w), s0.y, s1.y);
+      deinterleave_word(make_uint2(v.x, v.y), s0.z, s1.z);
+      deinterleave_word(make_uint2(v.z, v.w), s0.w, s1.w);
     } else {
       s0 = p[h];
       s1 = p[2 + h];

@@ -315,3 +315,90 @@ def read_slice(path, sigs=None, threads=0, stream=None):
                                                      threads, capi.stream_handle(stream)))
     f.close()
     return slice_, sigs, out
+
+
+# ---------------------------------------------------------------------------
+# Measurement
+
+IO_ROOT = [[4, 4], [5, 4], [4, 5], [4, 3]]   # a 33-stone root: its slice 34 is 2.7 GB of solved nodes
+
+
+def bench_filter(nodes=1 << 24, reps=5):
+    """Filter and unfilter kernels alone: 64 B read + 64 B written per node,
+    inputs and outputs (1 GiB each at the default size) far beyond L2."""
+    import torch
+    L = capi.lib()
+    a = torch.randint(-2**62, 2**62, (nodes, 8), dtype=torch.int64, device="cuda")
+    b = torch.empty_like(a)
+    s = capi.stream_handle()
+    out = {}
+    for name, f, src, dst in (("filter", L.pg_supertensor_filter, a, b), ("unfilter", L.pg_supertensor_unfilter, b, a)):
+        for _ in range(2):
+            capi.check(f(src.data_ptr(), nodes, 0, 1, dst.data_ptr(), s))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            capi.check(f(src.data_ptr(), nodes, 0, 1, dst.data_ptr(), s))
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"ms": ms, "GBps": 128 * nodes / (ms / 1e3) / 1e9}
+    out["nodes"] = nodes
+    out["bytes_per_node"] = 128
+    return out
+
+
+def bench_slice_io(levels=(1, 6), threads=0, directory=None):
+    """Write and read back a real solved slice (slice 34 below IO_ROOT) with
+    the GPU filter and host-thread compression; wall-clock GB/s of node data."""
+    import shutil
+    import tempfile
+    import time
+    import torch
+    from . import sweep as sweep_mod
+    root = section_sig(IO_ROOT)
+    _, nodes, sigs = sweep_mod.sweep(root, min_slice=34, keep_last=True)
+    torch.cuda.synchronize()
+    nbytes = nodes.shape[0] * 64
+    d = tempfile.mkdtemp(dir=directory)
+    res = {"workload": f"slice 34 below the root {IO_ROOT}: {len(sigs)} sections, {nodes.shape[0]} nodes "
+                       f"({nbytes / 1e9:.2f} GB), block size 8, interleave filter",
+           "threads": threads or os.cpu_count(), "levels": {}}
+    try:
+        for level in levels:
+            path = os.path.join(d, f"slice-34-{level}.pentago")
+            t = time.perf_counter()
+            write_slice(path, 34, sigs, nodes, level=level, threads=threads)
+            tw = time.perf_counter() - t
+            size = os.path.getsize(path)
+            t = time.perf_counter()
+            _, _, back = read_slice(path, threads=threads)
+            torch.cuda.synchronize()
+            tr = time.perf_counter() - t
+            ok = bool(torch.equal(back, nodes))
+            del back
+            res["levels"][str(level)] = {"write_s": tw, "read_s": tr, "write_GBps": nbytes / tw / 1e9,
+                                         "read_GBps": nbytes / tr / 1e9, "file_bytes": size,
+                                         "bits_per_position": 8 * size / (nodes.shape[0] * 256), "roundtrip_ok": ok}
+            os.remove(path)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    return res
+
+
+def main():
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="slice-file filter and I/O throughput")
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--levels", default="1,6")
+    args = ap.parse_args()
+    import torch
+    capi.check(capi.lib().pg_init())
+    torch.zeros(1, device="cuda")
+    print(json.dumps({"filter_kernels": bench_filter(),
+                      "slice_io": bench_slice_io(tuple(int(x) for x in args.levels.split(",")), args.threads)}))
+
+
+if __name__ == "__main__":
+    main()
