@@ -385,6 +385,46 @@ int pg_supertensor_finalize(pg_supertensor_writer_t writer, int section);
 int pg_supertensor_writer_close(pg_supertensor_writer_t writer);
 
 /* ---------------------------------------------------------------------------
+ * Shards of solved positions for training (pentago/shard/shard.h, shard.cc,
+ * shard_permute.h), slices 0..18.  Entry (section, position, rotation) of a
+ * slice has linear index offset[section] + 256 position + rotation, with the
+ * sections of pg_shard_sections and positions row-major over the section's
+ * shape; a fixed permutation shuffles it, and shard s of a power-of-two
+ * count N holds the shuffled indices congruent to s mod N, at index >>
+ * log2(N).  An entry's symbol is black wins + 2 white wins, as the reference
+ * stores it (shard.cc:447-449); a shard's symbols of one slice are one
+ * format-2 stream (pg_rans_encode_batch).
+ * ------------------------------------------------------------------------- */
+
+/* Sections of a slice in the mapping's order (all_boards_sections(slice, 8)). */
+int pg_shard_sections(int slice, uint64_t* sigs, int cap);
+/* Entries of a slice (256 x positions), and of one shard of it. */
+int64_t pg_shard_total(int slice);
+int64_t pg_shard_size(int slice, int total_shards, int shard);
+/* The permutation (inverse = 1: its inverse) of n device indices. */
+int pg_shard_permute(int slice, const uint64_t* in, int64_t n, int inverse, uint64_t* out, void* stream);
+/* board_t of n shuffled indices (device arrays; shard_mapping_t::board). */
+int pg_shard_boards(int slice, const uint64_t* shuffled, int64_t n, uint64_t* boards, void* stream);
+
+typedef struct {
+  int32_t section;     /* index into pg_shard_sections(slice) */
+  uint8_t block[4];    /* block coordinates */
+  int32_t block_size;  /* even, 2..26 (8 for the end engine's and the database's blocks) */
+  int32_t reserved;
+  int64_t node_offset; /* first node of the block in `nodes` (row-major in the block's shape) */
+} pg_shard_block_t;
+
+/* scatter_block (shard.cc:405-464) for a batch of blocks (host array): every
+ * entry whose shard lies in [shard_lo, shard_hi) stores its symbol (one byte)
+ * at symbols + shard_offsets[shard - shard_lo] + its position in the shard.
+ * nodes (device) are on-disk pairs (turn = PG_ST_RAW) or end-engine nodes of
+ * the side to move (turn 0 / 1).  shard_offsets is a host array; each shard
+ * needs pg_shard_size bytes. */
+int pg_shard_scatter(int slice, int total_shards, int shard_lo, int shard_hi, const pg_shard_block_t* blocks,
+                     int nblocks, const uint64_t* nodes, int turn, uint8_t* symbols, const int64_t* shard_offsets,
+                     void* stream);
+
+/* ---------------------------------------------------------------------------
  * Unit-level device operations, used by tests to check the superscore
  * library against the reference (pentago/base/superscore.h, symmetry.h).
  *   op 0: out[i] = rmax(in[i])                         in: supers
@@ -413,6 +453,9 @@ int pg_selftest_midsolve_groups_host(const uint64_t* raws, int n, int groups, pg
  * `polls` polls: the wait runs out and *fault_out = 1 (device check of the
  * bounded barrier the multi-CTA midsolve and the server use). */
 int pg_debug_barrier_timeout(unsigned polls, int* fault_out);
+/* The shard permutation (op 0 forward, 1 inverse) and boards (op 2) of n
+ * host indices, with the kernels' own functions. */
+int pg_selftest_shard_host(int op, int slice, const uint64_t* in, int64_t n, uint64_t* out);
 
 #ifdef __cplusplus
 }

@@ -1186,3 +1186,159 @@ void or_st_unfilter(const u64* in, int64_t n, int turn, int filter, u64* nodes) 
     }
   }
 }
+
+/* ------------------------------------------------------------------------
+ * Shards.  The shuffled index of (section, position, rotation) is
+ * permute(offset[section] + 256 position + rotation), positions row-major
+ * over the section's shape (pentago/shard/shard.cc:44-135); a shard of a
+ * power-of-two count takes the indices congruent to it (shard.h:87-115).
+ * ------------------------------------------------------------------------ */
+
+/* Shift amounts of the permutation per slice (pentago/shard/shard_permute.h:40-60;
+ * the entry counts there equal or_shard_total). */
+static const u8 perm_shifts[19][8] = {
+  {3,2,1,5,2,2,3,6}, {6,6,4,1,3,2,6,4}, {4,6,4,8,7,6,6,3}, {14,6,13,12,9,7,10,3},
+  {6,13,8,10,6,15,4,1}, {15,17,6,16,15,13,5,18}, {19,21,17,16,23,16,11,20},
+  {15,26,10,16,13,16,9,22}, {22,23,17,24,16,19,25,21}, {11,24,29,23,16,21,23,1},
+  {24,27,3,24,7,29,25,30}, {27,30,7,27,1,28,9,31}, {29,33,10,34,7,29,1,31},
+  {18,7,4,31,34,26,18,2}, {24,29,14,35,15,22,10,18}, {4,9,23,41,10,37,32,35},
+  {8,35,33,34,14,38,7,5}, {4,42,19,41,5,39,17,37}, {33,40,33,39,5,42,34,37}};
+
+typedef struct {
+  int nsec;
+  u64* sigs;
+  u64* offsets;  /* nsec + 1 */
+} shard_map;
+static shard_map shard_maps[19];
+
+/* all_boards_sections(n, 8) (pentago/base/all_boards.cc:160-203): counts of
+ * quadrants 3, 2, 1 in nested loops, quadrant 0 determined, standardized
+ * sections only, sorted by signature */
+int or_shard_sections(int n, u64* out, int cap) {
+  or_init();
+  const int white = n / 2, black = n - white;
+  int count = 0;
+  enum { MAXSEC = 16384 };
+  u64* sigs = (u64*)malloc(sizeof(u64) * MAXSEC);
+  for (int b3 = 0; b3 <= (black < 9 ? black : 9); b3++)
+    for (int w3 = 0; w3 <= (white < 9 - b3 ? white : 9 - b3); w3++) {
+      const int lb = black - b3, lw = white - w3;
+      for (int b2 = 0; b2 <= (lb < 9 ? lb : 9); b2++) {
+        const int w2lo = lw - (18 - (lb - b2)) > 0 ? lw - (18 - (lb - b2)) : 0, w2hi = lw < 9 - b2 ? lw : 9 - b2;
+        for (int w2 = w2lo; w2 <= w2hi; w2++) {
+          const int lb2 = lb - b2, lw2 = lw - w2;
+          const int b1lo = lb2 - 9 > 0 ? lb2 - 9 : 0, b1hi = lb2 < 9 ? lb2 : 9;
+          for (int b1 = b1lo; b1 <= b1hi; b1++) {
+            const int w1lo = lw2 - (9 - lb2 + b1) > 0 ? lw2 - (9 - lb2 + b1) : 0, w1hi = lw2 < 9 - b1 ? lw2 : 9 - b1;
+            for (int w1 = w1lo; w1 <= w1hi; w1++) {
+              section s;
+              s.c[0][0] = (u8)(lb2 - b1); s.c[0][1] = (u8)(lw2 - w1);
+              s.c[1][0] = (u8)b1; s.c[1][1] = (u8)w1;
+              s.c[2][0] = (u8)b2; s.c[2][1] = (u8)w2;
+              s.c[3][0] = (u8)b3; s.c[3][1] = (u8)w3;
+              if (sec_sig(sec_standardize(s, NULL)) != sec_sig(s)) continue;
+              if (count < MAXSEC) sigs[count] = sec_sig(s);
+              count++;
+            }
+          }
+        }
+      }
+    }
+  if (count <= MAXSEC) {
+    qsort(sigs, (size_t)count, sizeof(u64), cmp_u64);
+    for (int i = 0; i < count && i < cap; i++) out[i] = sigs[i];
+  } else
+    count = -1;
+  free(sigs);
+  return count;
+}
+
+static const shard_map* shard_map_of(int slice) {
+  shard_map* m = &shard_maps[slice];
+  if (m->sigs) return m;
+  const int n = or_shard_sections(slice, NULL, 0);
+  u64* sigs = (u64*)malloc(sizeof(u64) * (n ? n : 1));
+  u64* off = (u64*)malloc(sizeof(u64) * (n + 1));
+  or_shard_sections(slice, sigs, n);
+  off[0] = 0;
+  for (int i = 0; i < n; i++) {
+    int sh[4];
+    sec_shape(sec_from_sig(sigs[i]), sh);
+    off[i + 1] = off[i] + 256ull * sh[0] * sh[1] * sh[2] * sh[3];
+  }
+  m->nsec = n;
+  m->offsets = off;
+  m->sigs = sigs;
+  return m;
+}
+
+uint64_t or_shard_total(int slice) { or_init(); const shard_map* m = shard_map_of(slice); return m->offsets[m->nsec]; }
+
+/* The permutation: two overlapping power-of-two windows L = [0, 2^k) and
+ * H = [n - 2^k, n), with k = floor(log2 n); steps in pairs on L, H, L, H,
+ * each pair x ^= x >> s then x += x << s (mod 2^k) (shard_permute.h:62-170). */
+uint64_t or_shard_permute(int slice, u64 x, int inverse) {
+  const u64 n = or_shard_total(slice);
+  const int k = 63 - __builtin_clzll(n);
+  const u64 pow2k = 1ull << k, mask = pow2k - 1, offset = n - pow2k;
+  const u8* s = perm_shifts[slice];
+  for (int j = 0; j < 4; j++) {
+    const int pair = inverse ? 3 - j : j, i = 2 * pair;
+    const int high = pair & 1;
+    if (high ? x < offset : x >= pow2k) continue;
+    u64 t = high ? x - offset : x;
+    if (!inverse) {
+      t ^= t >> s[i];
+      t = (t + (t << s[i + 1])) & mask;
+    } else {
+      /* (1 + 2^s)^-1 = (1 - 2^s)(1 + 2^2s)(1 + 2^4s)..., (I + R^s)^-1 = (I + R^s)(I + R^2s)... */
+      t = (t - (t << s[i + 1])) & mask;
+      for (int s2 = 2 * s[i + 1]; s2 < k; s2 *= 2) t = (t + (t << s2)) & mask;
+      for (int s2 = s[i]; s2 < k; s2 *= 2) t ^= t >> s2;
+    }
+    x = high ? t + offset : t;
+  }
+  return x;
+}
+
+uint64_t or_shard_board(int slice, u64 shuffled) {
+  const shard_map* m = shard_map_of(slice);
+  const u64 linear = or_shard_permute(slice, shuffled, 1);
+  int si = 0;
+  while (m->offsets[si + 1] <= linear) si++;
+  const u64 within = linear - m->offsets[si];
+  u64 pos = within >> 8;
+  const int rot = (int)(within & 255);
+  const section s = sec_from_sig(m->sigs[si]);
+  int sh[4], idx[4];
+  sec_shape(s, sh);
+  for (int q = 3; q >= 0; q--) { idx[q] = (int)(pos % (u64)sh[q]); pos /= (u64)sh[q]; }
+  u64 board = 0;
+  for (int q = 0; q < 4; q++) {
+    const u16 v = rmin_list(s.c[q][0], s.c[q][1])[idx[q]];
+    const int r = rot >> (2 * q) & 3;
+    const u16 w = (u16)(T_pack[rot_left_n(T_unpack[v][0], r)] + 2 * T_pack[rot_left_n(T_unpack[v][1], r)]);
+    board |= (u64)w << (16 * q);
+  }
+  return board;
+}
+
+uint64_t or_shard_size(int slice, int total_shards, int shard) {
+  const int shift = __builtin_ctz((unsigned)total_shards);
+  return (or_shard_total(slice) + (u64)(total_shards - 1) - (u64)shard) >> shift;
+}
+
+void or_shard_symbols(int slice, int total_shards, int shard, const u64* nodes, const int64_t* section_base, u8* out) {
+  const shard_map* m = shard_map_of(slice);
+  const int shift = __builtin_ctz((unsigned)total_shards);
+  const u64 size = or_shard_size(slice, total_shards, shard);
+  for (u64 i = 0; i < size; i++) {
+    const u64 linear = or_shard_permute(slice, (i << shift) | (u64)shard, 1);
+    int si = 0;
+    while (m->offsets[si + 1] <= linear) si++;
+    const u64 within = linear - m->offsets[si];
+    const u64* node = nodes + 8 * (section_base[si] + (int64_t)(within >> 8));
+    const int r = (int)(within & 255);
+    out[i] = (u8)((node[r >> 6] >> (r & 63) & 1) + 2 * (node[4 + (r >> 6)] >> (r & 63) & 1));
+  }
+}

@@ -55,6 +55,20 @@ int or_midsolve_workspace_size(int stones);
 void or_st_filter(const uint64_t* nodes, int64_t n, int turn, int filter, uint64_t* out);
 void or_st_unfilter(const uint64_t* in, int64_t n, int turn, int filter, uint64_t* nodes);
 
+/* Shards (pentago/shard/shard.h, shard.cc, shard_permute.h): the sections of
+ * a slice in all_boards_sections(slice, 8) order, the slice's entry count
+ * (256 per position), the L/H window permutation, the board of a shuffled
+ * index, a shard's size, and a shard's symbols (black wins + 2 white wins)
+ * gathered from on-disk node pairs stored row-major per section at
+ * nodes + 8 * (section_base[i] + position). */
+int or_shard_sections(int slice, uint64_t* sigs, int cap);
+uint64_t or_shard_total(int slice);
+uint64_t or_shard_permute(int slice, uint64_t x, int inverse);
+uint64_t or_shard_board(int slice, uint64_t shuffled);
+uint64_t or_shard_size(int slice, int total_shards, int shard);
+void or_shard_symbols(int slice, int total_shards, int shard, const uint64_t* nodes, const int64_t* section_base,
+                      uint8_t* out);
+
 int64_t or_rans_encode(const uint8_t* symbols, int64_t n, uint8_t* out, int64_t cap);
 int64_t or_rans_decode(const uint8_t* data, int64_t size, uint8_t* symbols, int64_t cap);
 

@@ -12,6 +12,7 @@
 //   ref_rans_encode / ref_rans_decode shard/arithmetic.cc:366-452 (+ serialize :456-495)
 //   ref_random_supers                 base/superscore.cc:118-127
 //   ref_st_interleave                 data/filter.cc (interleave / uninterleave)
+//   ref_shard_*                       shard/shard.cc (shard_mapping_t, scatter_block), shard/shard_permute.h
 //   ref_block_write_order             data/supertensor_test.cc:31-55 (iteration order of its block map)
 
 #include "pentago/base/board.h"
@@ -24,6 +25,8 @@
 #include "pentago/end/compute.h"
 #include "pentago/end/sections.h"
 #include "pentago/data/filter.h"
+#include "pentago/base/all_boards.h"
+#include "pentago/shard/shard.h"
 #include "pentago/high/board.h"
 #include "pentago/mid/halfsuper.h"
 #include "pentago/mid/midengine.h"
@@ -289,6 +292,50 @@ void ref_st_interleave(uint64_t* data, int64_t n, int inverse) {
   else interleave(a);
   for (int64_t i = 0; i < n; i++)
     for (int k = 0; k < 2; k++) store_super(data + 8 * i + 4 * k, a[i][k]);
+}
+
+// Shards: sections of a slice in the mapping's order, the entry count, the
+// permutation, boards of shuffled indices, and scatter_block of blocks of
+// on-disk pairs (block b: section sigs[b], coordinates blocks[4b..], shape
+// shapes[4b..], nodes at data + 8 * offsets[b]) into one shard's symbols.
+int ref_shard_sections(int slice, uint64_t* sigs, int cap) {
+  const auto s = all_boards_sections(slice, 8);
+  for (int i = 0; i < s.size() && i < cap; i++) {
+    uint64_t sig = 0;
+    for (int q = 0; q < 4; q++)
+      for (int c = 0; c < 2; c++) sig |= uint64_t(s[i].counts[q][c]) << (16 * q + 8 * c);
+    sigs[i] = sig;
+  }
+  return s.size();
+}
+
+uint64_t ref_shard_total(int slice) { return shard_mapping_t(slice).total(); }
+
+void ref_shard_permute(int slice, const uint64_t* in, int64_t n, int inverse, uint64_t* out) {
+  const shard_permute_t p(slice);
+  for (int64_t i = 0; i < n; i++) out[i] = inverse ? p.inverse(in[i]) : p.forward(in[i]);
+}
+
+void ref_shard_board(int slice, const uint64_t* in, int64_t n, uint64_t* out) {
+  const shard_mapping_t m(slice);
+  for (int64_t i = 0; i < n; i++) out[i] = m.board(in[i]);
+}
+
+void ref_shard_scatter(int slice, int total_shards, int shard, int nblocks, const uint64_t* sigs,
+                       const uint8_t* blocks, const int* shapes, const int64_t* offsets, const uint64_t* data,
+                       uint8_t* out) {
+  const shard_mapping_t m(slice);
+  const shard_locator_t loc(total_shards, range(shard, shard + 1));
+  ternaries_t buf(loc.shard_size(m.total(), shard));
+  for (int b = 0; b < nblocks; b++) {
+    const Vector<int,4> shape(shapes[4 * b], shapes[4 * b + 1], shapes[4 * b + 2], shapes[4 * b + 3]);
+    const auto* nodes = reinterpret_cast<const Vector<super_t,2>*>(data + 8 * offsets[b]);
+    const RawArray<const Vector<super_t,2>,4> block_data(shape, nodes);
+    scatter_block(m, total_shards, range(shard, shard + 1), RawArray<ternaries_t>(1, &buf),
+                  section_from_sig(sigs[b]),
+                  Vector<uint8_t,4>(blocks[4 * b], blocks[4 * b + 1], blocks[4 * b + 2], blocks[4 * b + 3]), block_data);
+  }
+  for (uint64_t i = 0; i < buf.size; i++) out[i] = uint8_t(buf[i]);
 }
 
 // The order in which supertensor_test.cc writes its blocks: it inserts every

@@ -74,6 +74,11 @@ class pg_mid_values_t(ctypes.Structure):
 MID_VALUES_BYTES = 8 + 16 * 163
 
 
+class pg_shard_block_t(ctypes.Structure):
+    _fields_ = [("section", ctypes.c_int32), ("block", ctypes.c_uint8 * 4), ("block_size", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("node_offset", ctypes.c_int64)]
+
+
 class pg_supertensor_header_t(ctypes.Structure):
     _fields_ = [("version", ctypes.c_uint32), ("valid", ctypes.c_uint32), ("stones", ctypes.c_uint32),
                 ("block_size", ctypes.c_uint32), ("section", ctypes.c_uint64), ("shape", ctypes.c_uint16 * 4),
@@ -144,6 +149,13 @@ SIGNATURES = {
     "pg_supertensor_write_blocks": (_I, [_P, _I, _P, _P, _P, _P, _I, _I, _P]),
     "pg_supertensor_finalize": (_I, [_P, _I]),
     "pg_supertensor_writer_close": (_I, [_P]),
+    "pg_shard_sections": (_I, [_I, _P, _I]),
+    "pg_shard_total": (_I64, [_I]),
+    "pg_shard_size": (_I64, [_I, _I, _I]),
+    "pg_shard_permute": (_I, [_I, _P, _I64, _I, _P, _P]),
+    "pg_shard_boards": (_I, [_I, _P, _I64, _P, _P]),
+    "pg_shard_scatter": (_I, [_I, _I, _I, _I, _P, _I, _P, _I, _P, _P, _P]),
+    "pg_selftest_shard_host": (_I, [_I, _I, _P, _I64, _P]),
 }
 
 _lib = None

@@ -635,11 +635,7 @@ extern "C" int pg_end_plan_destroy(pg_end_plan_t plan) {
 }
 
 extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
-  const tables_t& H = tables();
-  const dev_tables_t T = {H.rmin_flat, H.rmin_inv, &H.unpack[0][0], &H.win_factors[0][0][0], H.rmin_off,
-                          &H.commute[0][0], H.win_union.data(), H.pack, H.pop_masks, H.rank9,
-                          &H.term_pat[0][0], &H.term_other[0][0][0], &H.term_sub[0][0][0], &H.cov[0][0][0],
-                          &H.miss_pat[0][0], &H.miss_quad[0][0][0]};
+  const dev_tables_t T = host_tables_view();
   std::string err;
   unsigned errors = 0;
   std::vector<parent_rec> recs;

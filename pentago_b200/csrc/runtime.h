@@ -24,11 +24,16 @@ struct dev_tables_t {
   const uint8_t* cov;          // 32 x 4 x 512
   const uint8_t* miss_pat;     // 4 x 15
   const uint8_t* miss_quad;    // 4 x 15 x 3
+  const uint16_t* rot;         // 512 x 2: [left, right] rotation of a quadrant side
 };
 
 // Tables on the current device (uploaded on first use).  Returns nullptr and
 // sets the error on failure.
 const dev_tables_t* device_tables();
+
+// The same tables as host pointers, for the host self-tests that run kernel
+// arithmetic on the CPU.
+dev_tables_t host_tables_view();
 
 // Run f() once per (current device, key) and return its result from then on
 // (thread safe).  For per-device set-up such as kernel attributes and

@@ -21,6 +21,9 @@ Fixtures written:
                      taken from the reference compiled in place)
   db/slice-N.pentago the reference's solved database for slices 0..5 (data/), and
   counts_0_5.npz     its per-section counts (data/counts-{0..5}.npy)
+  shards.json        pentago/shard/sharder_test.cc's server-verified (board, value)
+                     samples of shard 7 of 32 over slices 0..5, and the per-slice
+                     entry counts listed in pentago/shard/shard_permute.h
 """
 import ctypes
 import json
@@ -139,6 +142,16 @@ def main(ref_root):
     for s in range(6):
         shutil.copyfile(os.path.join(ref_root, "data", f"slice-{s}.pentago"),
                         os.path.join(HERE, "db", f"slice-{s}.pentago"))
+    # 9. shard samples and entry counts
+    sh = src("pentago/shard/sharder_test.cc")
+    pairs = re.findall(r"\{(\d+),(-?\d+)\}", re.search(r"server_values = \{(.*?)\};", sh, re.S).group(1))
+    fixture = re.search(r"class shard_iterator_test.*?max_slice = (\d+);.*?total_shards = (\d+);", sh, re.S)
+    shard_id = int(re.search(r"TEST_F\(shard_iterator_test, correctness\) \{\s*const int shard_id = (\d+);", sh).group(1))
+    perm = src("pentago/shard/shard_permute.h")
+    totals = [int(n) for n in re.findall(r"\{(\d+), \{[\d,]+\}\},\s*// slice", perm)]
+    json.dump({"max_slice": int(fixture.group(1)), "total_shards": int(fixture.group(2)), "shard_id": shard_id,
+               "server_values": [[int(b), int(v)] for b, v in pairs], "slice_totals": totals},
+              open(os.path.join(HERE, "shards.json"), "w"))
     np.savez_compressed(os.path.join(HERE, "counts_0_5.npz"),
                         **{f"counts_{s}": np.load(os.path.join(ref_root, "data", f"counts-{s}.npy")) for s in range(6)})
     print("wrote fixtures to", HERE)
