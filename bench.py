@@ -229,6 +229,53 @@ def cpu_static_coder_rate(symbols, offsets, seconds=5.0):
             "sample": f"{len(blocks)} blocks' symbols, format-2 encode repeated for {el:.1f} s"}
 
 
+def cpu_scatter_rate(slice_, total_shards, seconds=8.0):
+    """The reference's scatter_block (oracle/_ref) on the host cores into every
+    shard, on a sample of the slice's blocks sized to about `seconds`."""
+    import ctypes
+    import numpy as np
+    from tests.oracle import reference, P
+    from pentago_b200 import shard as shard_mod
+    from pentago_b200.end import section_shape
+    from pentago_b200.supertensor import section_block_offsets
+    R = reference()
+    if R is None:
+        return None
+    R.lib.ref_shard_scatter_seconds.restype = ctypes.c_double
+    m = shard_mod.shard_mapping_t(slice_)
+    sigs, coords, shapes = [], [], []
+    for sig in m.sections:
+        shape = np.array(section_shape(int(sig)))
+        idx, _ = section_block_offsets(shape)
+        for b in idx:
+            sigs.append(int(sig))
+            coords.append(b)
+            shapes.append(np.minimum(8, shape - 8 * b.astype(np.int64)))
+    order = np.random.default_rng(0).permutation(len(sigs))
+    threads = os.cpu_count() or 1
+
+    def run(k):
+        pick = order[:k]
+        sg = np.array([sigs[i] for i in pick], np.uint64)
+        cd = np.ascontiguousarray(np.array([coords[i] for i in pick], np.uint8))
+        sh = np.ascontiguousarray(np.array([shapes[i] for i in pick], np.int32))
+        n = sh.prod(1).astype(np.int64)
+        off = np.zeros(k, np.int64)
+        off[1:] = np.cumsum(n)[:-1]
+        rng = np.random.default_rng(1)
+        x, y, z = (rng.integers(0, 2**63, size=(int(n.sum()), 4), dtype=np.uint64) for _ in range(3))
+        data = np.ascontiguousarray(np.concatenate([x & y, ~x & z], 1))
+        sec = R.lib.ref_shard_scatter_seconds(slice_, total_shards, k, P(sg), P(cd), P(sh), P(off), P(data), threads)
+        return sec, int(n.sum()) * 256
+    k = min(len(sigs), 4 * threads)
+    sec, entries = run(k)
+    k = min(len(sigs), max(k, int(k * seconds / max(sec, 1e-3))))
+    sec, entries = run(k)
+    return {"entries_per_s": entries / sec, "cores": threads, "kind": "reference",
+            "sample": f"scatter_block of {k} random blocks of slice {slice_} ({entries} entries) into all "
+                      f"{total_shards} shards, {sec:.1f} s; format-2 coding not included"}
+
+
 def sweep_summary(timings, wall_s):
     """Config 2 from the per-slice timings of the sweep (slices 35 -> 30)."""
     ms = sum(v["ms"] for v in timings.values())
@@ -318,6 +365,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-coder measurement")
     ap.add_argument("--no-slice-files", action="store_true", help="skip the slice-file filter and I/O measurement")
+    ap.add_argument("--no-sharder", action="store_true", help="skip the sharder measurement")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -447,6 +495,7 @@ def main():
     learned = None
     sweep2 = None
     slice_files = None
+    sharder = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(seconds=12.0)
     if rank == 0 and world == 1:
@@ -476,6 +525,16 @@ def main():
         for k in ("filter", "unfilter"):
             slice_files["filter_kernels"][k]["frac_of_hbm_peak"] = slice_files["filter_kernels"][k]["GBps"] / peak
 
+    if rank == 0 and world == 1 and not args.no_sharder:
+        # Training shards: slice 10 (16 G entries, synthetic values) scattered
+        # into 1,024 shards and each shard's group coded, resident in HBM
+        torch.cuda.empty_cache()
+        from pentago_b200 import shard as shard_mod
+        sharder = shard_mod.bench_scatter(10, 1024)
+        torch.cuda.empty_cache()
+        if not args.no_cpu_baseline:
+            sharder["cpu_baseline"] = cpu_scatter_rate(10, 1024, seconds=8.0)
+
     if rank == 0:
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -500,6 +559,7 @@ def main():
             "sweep_config2": sweep2,
             "learned_rans_config3": learned,
             "slice_files": slice_files,
+            "sharder": sharder,
             "clocks": clocks.summary(),
         }
         print(json.dumps(result))

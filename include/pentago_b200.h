@@ -418,8 +418,9 @@ typedef struct {
  * entry whose shard lies in [shard_lo, shard_hi) stores its symbol (one byte)
  * at symbols + shard_offsets[shard - shard_lo] + its position in the shard.
  * nodes (device) are on-disk pairs (turn = PG_ST_RAW) or end-engine nodes of
- * the side to move (turn 0 / 1).  shard_offsets is a host array; each shard
- * needs pg_shard_size bytes. */
+ * the side to move (turn 0 / 1).  shard_offsets is a host array (each shard
+ * needs pg_shard_size bytes), or NULL for shards shard_lo .. shard_hi - 1
+ * packed back to back from symbols, which is faster (no table lookups). */
 int pg_shard_scatter(int slice, int total_shards, int shard_lo, int shard_hi, const pg_shard_block_t* blocks,
                      int nblocks, const uint64_t* nodes, int turn, uint8_t* symbols, const int64_t* shard_offsets,
                      void* stream);

@@ -38,6 +38,8 @@
 #include <condition_variable>
 #include <cstring>
 #include <mutex>
+#include <chrono>
+#include <thread>
 #include <unordered_map>
 
 using namespace pentago;
@@ -336,6 +338,34 @@ void ref_shard_scatter(int slice, int total_shards, int shard, int nblocks, cons
                   Vector<uint8_t,4>(blocks[4 * b], blocks[4 * b + 1], blocks[4 * b + 2], blocks[4 * b + 3]), block_data);
   }
   for (uint64_t i = 0; i < buf.size; i++) out[i] = uint8_t(buf[i]);
+}
+
+// Seconds the reference's scatter_block takes for the given blocks into every
+// shard of total_shards (one buffer per shard), on `threads` host threads
+// taking blocks in turn (as sharder.cc's parallel_for does).
+double ref_shard_scatter_seconds(int slice, int total_shards, int nblocks, const uint64_t* sigs,
+                                 const uint8_t* blocks, const int* shapes, const int64_t* offsets,
+                                 const uint64_t* data, int threads) {
+  const shard_mapping_t m(slice);
+  const shard_locator_t loc(total_shards, range(0, total_shards));
+  vector<ternaries_t> buffers;
+  for (int s = 0; s < total_shards; s++) buffers.emplace_back(loc.shard_size(m.total(), s));
+  std::atomic<int> next{0};
+  const auto t0 = std::chrono::steady_clock::now();
+  auto work = [&] {
+    for (int b; (b = next.fetch_add(1)) < nblocks;) {
+      const Vector<int,4> shape(shapes[4 * b], shapes[4 * b + 1], shapes[4 * b + 2], shapes[4 * b + 3]);
+      const auto* nodes = reinterpret_cast<const Vector<super_t,2>*>(data + 8 * offsets[b]);
+      scatter_block(m, total_shards, range(0, total_shards), asarray(buffers), section_from_sig(sigs[b]),
+                    Vector<uint8_t,4>(blocks[4 * b], blocks[4 * b + 1], blocks[4 * b + 2], blocks[4 * b + 3]),
+                    RawArray<const Vector<super_t,2>,4>(shape, nodes));
+    }
+  };
+  vector<std::thread> pool;
+  for (int t = 1; t < threads; t++) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // The order in which supertensor_test.cc writes its blocks: it inserts every

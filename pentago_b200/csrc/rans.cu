@@ -61,7 +61,37 @@ __device__ inline uint32_t get_u32(const uint8_t* p) {
 }
 __device__ inline uint64_t get_u64(const uint8_t* p) { return uint64_t(get_u32(p)) | uint64_t(get_u32(p + 4)) << 32; }
 
+// Encoder constants of one symbol: state / freq by a reciprocal multiply
+// (x < 2^31 after renormalization, where the reciprocal is exact), as in
+// F. Giesen's ryg_rans (RansEncSymbolInit / RansEncPutSymbol, after
+// Alverson, "Integer division using reciprocals", 1991).  The new state is
+// x + bias + q * (total - freq) = (x / freq) * total + x % freq + cum.
+struct rans_enc_sym {
+  uint32_t xmax, rcp, shift, bias, cmpl;
+};
+
+__host__ __device__ inline rans_enc_sym enc_sym(const rans_freq& t, int s) {
+  rans_enc_sym e;
+  const uint32_t f = t.freq[s];
+  e.xmax = t.xmax[s];
+  e.cmpl = kRansTotal - f;
+  if (f < 2) {
+    e.rcp = ~0u;
+    e.shift = 0;
+    e.bias = t.cum[s] + kRansTotal - 1;
+  } else {
+    uint32_t sh = 0;
+    while (f > (1u << sh)) sh++;
+    e.rcp = uint32_t(((uint64_t(1) << (sh + 31)) + f - 1) / f);
+    e.shift = sh - 1;
+    e.bias = t.cum[s];
+  }
+  return e;
+}
+
 // One 8-thread group per stream.  out_offsets[s] has room for stream_bound(n_s).
+// Long streams are latency bound (8 sequential chains per stream), so each
+// lane loads its next 16 symbols while it codes the current 16.
 __global__ void __launch_bounds__(256)
 rans_encode_kernel(const uint8_t* __restrict__ symbols, const int64_t* __restrict__ offsets, int nstreams,
                    uint8_t* __restrict__ out, const int64_t* __restrict__ out_offsets, int64_t* __restrict__ sizes,
@@ -77,33 +107,76 @@ rans_encode_kernel(const uint8_t* __restrict__ symbols, const int64_t* __restric
     return;
   }
   const uint8_t* sym = symbols + begin;
-  // Count symbols
-  uint64_t c[3] = {0, 0, 0};
-  for (int64_t i = lane; i < n; i += kLanes) {
-    const uint8_t s = sym[i];
-    c[0] += s == 0;
-    c[1] += s == 1;
-    c[2] += s == 2;
+  // Count symbols (ones and twos; zeros are the rest) and look for values
+  // above 2: whole aligned words by all lanes, the ragged ends by lane 0
+  uint64_t c1 = 0, c2 = 0;
+  uint32_t badbits = 0;
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(sym), a1 = a0 + uintptr_t(n);
+  uintptr_t w0 = (a0 + 3) & ~uintptr_t(3), w1 = a1 & ~uintptr_t(3);
+  if (w1 < w0) w0 = w1 = a1;
+  const uint32_t* W = reinterpret_cast<const uint32_t*>(w0);
+  const int64_t nw = int64_t(w1 - w0) >> 2;
+#pragma unroll 4
+  for (int64_t k = lane; k < nw; k += kLanes) {
+    const uint32_t w = W[k];
+    c1 += __popc(w & 0x01010101u);
+    c2 += __popc(w & 0x02020202u);
+    badbits |= (w & 0xfcfcfcfcu) | (w & (w >> 1) & 0x01010101u);
   }
-  for (int o = 4; o; o >>= 1)
-    for (int k = 0; k < 3; k++) c[k] += __shfl_xor_sync(gmask, c[k], o, 8);
+  if (lane == 0) {
+    for (uintptr_t a = a0; a < a1; a++) {
+      if (a == w0) a = w1;
+      if (a >= a1) break;
+      const uint32_t v = *reinterpret_cast<const uint8_t*>(a);
+      c1 += v == 1;
+      c2 += v == 2;
+      badbits |= v > 2;
+    }
+  }
+  for (int o = 4; o; o >>= 1) {
+    c1 += __shfl_xor_sync(gmask, c1, o, 8);
+    c2 += __shfl_xor_sync(gmask, c2, o, 8);
+    badbits |= __shfl_xor_sync(gmask, badbits, o, 8);
+  }
+  if (badbits) {
+    if (lane == 0) sizes[group] = PG_ERR_ARG;
+    return;
+  }
+  const uint64_t c[3] = {uint64_t(n) - c1 - c2, c1, c2};
   const rans_freq t = make_freq(c);
-  // Encode this lane backward into its slot
+  const rans_enc_sym e0 = enc_sym(t, 0), e1 = enc_sym(t, 1), e2 = enc_sym(t, 2);
+  // Encode this lane's symbols (i = lane mod 8) backward into its slot
   uint8_t* base = out + out_offsets[group];
   const int64_t cap = lane_capacity(n);
   uint8_t* slot_end = base + kHeader + (lane + 1) * cap;
   uint8_t* cur = slot_end;
   uint32_t state = kRansLower;
-  int bad = 0;
-  for (int64_t i = (n - 1) - (((n - 1) - lane) & 7); i >= lane && i < n; i -= kLanes) {
-    int s = sym[i];
-    if (s > 2) { bad = 1; s = 0; }
-    while (state >= t.xmax[s]) { *--cur = uint8_t(state & 0xff); state >>= 8; }
-    state = ((state / t.freq[s]) << kRansTotalBits) + (state % t.freq[s]) + t.cum[s];
+  const int64_t cnt = n > lane ? (n - 1 - lane) / kLanes + 1 : 0;  // this lane's symbols
+  const uint8_t* last = sym + lane + kLanes * (cnt - 1);          // its last symbol, coded first
+  constexpr int kAhead = 16;
+  uint8_t now[kAhead], next[kAhead];
+#pragma unroll
+  for (int k = 0; k < kAhead; k++) now[k] = k < cnt ? last[-kLanes * int64_t(k)] : 0;
+  for (int64_t j0 = 0; j0 < cnt; j0 += kAhead) {
+#pragma unroll
+    for (int k = 0; k < kAhead; k++) {
+      const int64_t j = j0 + kAhead + k;
+      next[k] = j < cnt ? last[-kLanes * j] : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kAhead; k++) {
+      if (j0 + k >= cnt) break;
+      const int s = now[k];
+      const rans_enc_sym e = s == 0 ? e0 : s == 1 ? e1 : e2;
+      while (state >= e.xmax) { *--cur = uint8_t(state & 0xff); state >>= 8; }
+      const uint32_t q = __umulhi(state, e.rcp) >> e.shift;
+      state += e.bias + q * e.cmpl;
+    }
+#pragma unroll
+    for (int k = 0; k < kAhead; k++) now[k] = next[k];
   }
   for (int j = 0; j < 4; j++) *--cur = uint8_t(state >> (8 * j));
   const uint32_t len = uint32_t(slot_end - cur);
-  bad = __any_sync(gmask, bad);
   // Lengths of all lanes, and this lane's destination behind the header
   uint32_t lens[kLanes];
   for (int l = 0; l < kLanes; l++) lens[l] = __shfl_sync(gmask, len, l, 8);
@@ -123,7 +196,7 @@ rans_encode_kernel(const uint8_t* __restrict__ symbols, const int64_t* __restric
     for (int k = 0; k < 3; k++) put_u64(base + 4 + 8 * k, c[k]);
     int64_t total = kHeader;
     for (int l = 0; l < kLanes; l++) { put_u32(base + 28 + 4 * l, lens[l]); total += lens[l]; }
-    sizes[group] = bad ? PG_ERR_ARG : total;
+    sizes[group] = total;
   }
 }
 

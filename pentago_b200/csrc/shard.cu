@@ -197,6 +197,15 @@ struct block_dev_t {
   int64_t node_offset;
 };
 
+// Where shard s's symbols start.  Packed (shard_off null): shards lo .. hi-1
+// back to back, shard t holding q + (t < r) entries for n = q 2^shift + r,
+// so the offset is arithmetic; otherwise the caller's table.
+PG_HD int64_t shard_start(const int64_t* shard_off, uint64_t n, int shift, int lo, int s) {
+  if (shard_off) return ldg(shard_off + (s - lo));
+  const int64_t q = int64_t(n >> shift), r = int64_t(n & ((uint64_t(1) << shift) - 1));
+  return (s - lo) * q + (std::min<int64_t>(s, r) - std::min<int64_t>(lo, r));
+}
+
 // scatter_block (shard.cc:405-464) for a batch of blocks: thread t of grid
 // row b handles node t >> 3 of block b, rotations 32 (t & 7) .. + 31.
 __global__ void __launch_bounds__(256)
@@ -232,7 +241,8 @@ shard_scatter_kernel(const shard_dev_t D, const block_dev_t* __restrict__ blocks
       const uint64_t y = perm_forward(D.perm, base + bit);
       const int s = int(y & smask);
       if (s < lo || s >= hi) continue;
-      symbols[ldg(shard_off + (s - lo)) + int64_t(y >> shift)] = uint8_t((black >> bit & 1) + 2 * (white >> bit & 1));
+      symbols[shard_start(shard_off, D.perm.n, shift, lo, s) + int64_t(y >> shift)] =
+          uint8_t((black >> bit & 1) + 2 * (white >> bit & 1));
     }
   }
 }
@@ -319,7 +329,7 @@ extern "C" int pg_shard_scatter(int slice, int total_shards, int shard_lo, int s
                                 int nblocks, const uint64_t* nodes, int turn, uint8_t* symbols,
                                 const int64_t* shard_offsets, void* stream_) {
   if (!slice_ok(slice) || !shards_ok(total_shards) || shard_lo < 0 || shard_lo >= shard_hi ||
-      shard_hi > total_shards || nblocks < 0 || turn < 0 || turn > PG_ST_RAW || !shard_offsets ||
+      shard_hi > total_shards || nblocks < 0 || turn < 0 || turn > PG_ST_RAW ||
       (nblocks && (!blocks || !nodes || !symbols)))
     return fail(PG_ERR_ARG, "bad scatter arguments");
   if (reinterpret_cast<uintptr_t>(nodes) & 15) return fail(PG_ERR_ARG, "nodes must be 16-byte aligned");
@@ -355,9 +365,12 @@ extern "C" int pg_shard_scatter(int slice, int total_shards, int shard_lo, int s
   block_dev_t* bdev = nullptr;
   int64_t* off = nullptr;
   PG_CUDA(scratch.alloc(&bdev, sizeof(block_dev_t) * nblocks));
-  PG_CUDA(scratch.alloc(&off, sizeof(int64_t) * (shard_hi - shard_lo)));
   PG_CUDA(cudaMemcpyAsync(bdev, bd.data(), sizeof(block_dev_t) * nblocks, cudaMemcpyHostToDevice, stream));
-  PG_CUDA(cudaMemcpyAsync(off, shard_offsets, sizeof(int64_t) * (shard_hi - shard_lo), cudaMemcpyHostToDevice, stream));
+  if (shard_offsets) {
+    PG_CUDA(scratch.alloc(&off, sizeof(int64_t) * (shard_hi - shard_lo)));
+    PG_CUDA(cudaMemcpyAsync(off, shard_offsets, sizeof(int64_t) * (shard_hi - shard_lo), cudaMemcpyHostToDevice,
+                            stream));
+  }
   const int shift = __builtin_ctz(unsigned(total_shards));
   const int64_t threads = 8 * max_nodes;
   for (int b0 = 0; b0 < nblocks; b0 += 65535) {

@@ -257,9 +257,10 @@ def sharder(input_dir, output_dir, max_slice=18, total_shards=1 << 17, shard_ran
                         blocks[k].block[q] = b[q]
                     blocks[k].block_size = r.header.block_size
                     blocks[k].node_offset = o
+                # the batch's shards are packed back to back: no offset table needed
                 capi.check(capi.lib().pg_shard_scatter(slice_, total_shards, b0, b1, blocks, len(chunk),
                                                        nodes.data_ptr(), supertensor.RAW, symbols.data_ptr(),
-                                                       capi.ptr(offs), capi.stream_handle(stream)))
+                                                       None, capi.stream_handle(stream)))
                 torch.cuda.synchronize()
                 t_read += t1 - t0
                 t_scatter += time.perf_counter() - t1
@@ -278,21 +279,99 @@ def sharder(input_dir, output_dir, max_slice=18, total_shards=1 << 17, shard_ran
     return [shard_filename(total_shards, s) for s in range(lo, hi)]
 
 
+def synthetic_slice(slice_, seed=0):
+    """Every block (block size 8) of every section of a slice, back to back in
+    the end engine's block-major layout, with seeded synthetic on-disk pairs
+    (black and white wins disjoint, each bit set with probability 1/4).
+    Returns (mapping, pg_shard_block_t array, device nodes)."""
+    import torch
+    from .end import section_shape
+    from .supertensor import section_block_offsets
+    m = shard_mapping_t(slice_)
+    parts, base = [], 0
+    for i, sig in enumerate(m.sections):
+        shape = section_shape(int(sig))
+        idx, off = section_block_offsets(shape)
+        parts.append((i, idx, off + base))
+        base += int(np.prod(shape))
+    nb = sum(len(p[1]) for p in parts)
+    blocks = (capi.pg_shard_block_t * nb)()
+    k = 0
+    for i, idx, off in parts:
+        for b, o in zip(idx, off):
+            blocks[k].section = i
+            for q in range(4):
+                blocks[k].block[q] = int(b[q])
+            blocks[k].block_size = 8
+            blocks[k].node_offset = int(o)
+            k += 1
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    r = lambda: torch.randint(-2**63, 2**63 - 1, (base, 4), dtype=torch.int64, device="cuda", generator=g)
+    x, y, z = r(), r(), r()
+    nodes = torch.cat([x & y, ~x & z], 1).contiguous()
+    del x, y, z
+    return m, blocks, nodes
+
+
+def bench_scatter(slice_=10, total_shards=1024, reps=3):
+    """The sharder's GPU work for one slice into every shard of a count:
+    scatter (permutation of every entry) and the format-2 coding of each
+    shard's group, on a synthetic slice resident in HBM."""
+    import torch
+    m, blocks, nodes = synthetic_slice(slice_)
+    loc = shard_locator_t(total_shards)
+    sizes = np.array([loc.shard_size(m.total(), s) for s in range(total_shards)], np.int64)
+    offs = np.zeros(total_shards + 1, np.int64)
+    offs[1:] = np.cumsum(sizes)
+    symbols = torch.empty(int(offs[-1]), dtype=torch.uint8, device="cuda")
+    s = capi.stream_handle()
+    run = lambda: capi.check(capi.lib().pg_shard_scatter(slice_, total_shards, 0, total_shards, blocks, len(blocks),
+                                                         nodes.data_ptr(), 2, symbols.data_ptr(), None, s))
+    run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    scatter_ms = e0.elapsed_time(e1) / reps
+    rans.encode_device(symbols[:1 << 20], np.array([0, 1 << 20], np.int64))  # warm the coder
+    torch.cuda.synchronize()
+    e0.record()
+    out, out_off, sz = rans.encode_device(symbols, offs)
+    e1.record()
+    torch.cuda.synchronize()
+    encode_ms = e0.elapsed_time(e1)
+    n = m.total()
+    return {"workload": f"slice {slice_} (all {len(m.sections)} sections, {n} entries, synthetic values) "
+                        f"into {total_shards} shards", "entries": n, "nodes": int(nodes.shape[0]),
+            "blocks": len(blocks), "scatter_ms": scatter_ms, "scatter_entries_per_s": n / (scatter_ms / 1e3),
+            "encode_ms": encode_ms, "encode_entries_per_s": n / (encode_ms / 1e3),
+            "entries_per_s": n / ((scatter_ms + encode_ms) / 1e3), "coded_bytes": int(sz.sum()),
+            "scatter_algorithmic_GBps": (64 * nodes.shape[0] + n) / (scatter_ms / 1e3) / 1e9}
+
+
 def main():
     import argparse
     import json
     import time
     ap = argparse.ArgumentParser(description="convert .pentago slice files to .pentago.shard files on the GPU")
-    ap.add_argument("input_dir")
-    ap.add_argument("output_dir")
+    ap.add_argument("input_dir", nargs="?")
+    ap.add_argument("output_dir", nargs="?")
+    ap.add_argument("--bench", type=int, default=None, metavar="SLICE",
+                    help="time the scatter and coding of a synthetic slice into all shards instead")
     ap.add_argument("--max-slice", type=int, default=18)
-    ap.add_argument("--shards", type=int, required=True, help="total shard count, a power of two")
+    ap.add_argument("--shards", type=int, default=1024, help="total shard count, a power of two")
     ap.add_argument("--range", default=":")
     ap.add_argument("--threads", type=int, default=0)
     args = ap.parse_args()
     import torch
     capi.check(capi.lib().pg_init())
     torch.zeros(1, device="cuda")
+    if args.bench is not None:
+        print(json.dumps(bench_scatter(args.bench, args.shards)))
+        return
     timings = {}
     t = time.perf_counter()
     files = sharder(args.input_dir, args.output_dir, args.max_slice, args.shards,
