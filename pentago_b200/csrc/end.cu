@@ -217,14 +217,15 @@ PG_HD uint4 pattern_terms(const line_dev_t& L, const dev_tables_t& T, int side, 
 // Per-microline results live in shared memory as separate arrays of 16-byte
 // halves (structure of arrays): lanes reading different entries then spread
 // over the banks instead of colliding on the few positions an array of 32- or
-// 64-byte records leaves them.  Pattern results: half h of entry e at
-// h * 2 kMaxPat + e.  Children: quarter c of child j at c * nchild + j.
-PG_HD void pattern_store(uint4* pat, int e, const super8& w) {
+// 64-byte records leaves them.  Pattern results: entry e (the mover's
+// patterns, then the opponent's: pp in all) has half h at h * pp + e.
+// Children: quarter c of child j at c * nchild + j.
+PG_HD void pattern_store(uint4* pat, int e, int pp, const super8& w) {
   pat[e] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
-  pat[2 * kMaxPat + e] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
+  pat[pp + e] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
 }
-PG_HD super8 pattern_from(const uint4* pat, int e) {
-  const uint4 a = pat[e], b = pat[2 * kMaxPat + e];
+PG_HD super8 pattern_from(const uint4* pat, int e, int pp) {
+  const uint4 a = pat[e], b = pat[pp + e];
   return super8{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
 }
 
@@ -263,8 +264,9 @@ PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab
   const uint32_t mvw[5] = {h.y, h.z, h.w, mw.x, mw.y};
   const int nmoves = int(h.x >> 16 & 0xff);
   // super_wins of both sides, looked up by stone pattern
-  const super8 wins0 = pattern_from(pats, int(h.x & 0xff));
-  const super8 wins1 = pattern_from(pats, kMaxPat + int(h.x >> 8 & 0xff));
+  const int p0 = L.npat[0], pp = p0 + L.npat[1];
+  const super8 wins0 = pattern_from(pats, int(h.x & 0xff), pp);
+  const super8 wins1 = pattern_from(pats, p0 + int(h.x >> 8 & 0xff), pp);
   // Every move wins immediately where super_wins(side0 | move) does; the
   // union over the empty cells is one table evaluation of the union of the
   // covered terms.
@@ -312,13 +314,25 @@ constexpr int kMicro = 4;  // microlines per CTA
 
 __device__ void record_errors(unsigned e);
 
-// Shared memory of a CTA besides the covered-terms list and the children.
+// Static shared memory of a CTA: per microline its geometry and the mover's
+// subset tables (the parents evaluate them once more).
 struct cta_smem {
   micro_ctx ctx[kMicro];
-  uint2 tab[kMicro][2][kTab];                  // subset tables per microline and side
-  uint4 pat[kMicro][2 * kMaxPat * 2];          // super_wins per microline and stone pattern
+  uint2 tab[kMicro][kTab];
 };
-constexpr int kSubBytes = 2 * kMaxPat * 16;    // covered terms of every stone pattern (dynamic smem head)
+
+// Dynamic shared memory: the stone-pattern results of every microline
+// (kMicro x 2 pp uint4), then the children (kMicro x 4 nchild uint4).  Until
+// the children are written their space holds the pattern set-up: the covered
+// terms of every pattern (pp uint4) and the opponent's subset tables
+// (kMicro x kTab uint2).  Sized per launch for its largest line, so that
+// three CTAs fit an SM on the longest lines of 30-stone sections.
+PG_HD size_t pattern_bytes(int pp) { return size_t(kMicro) * pp * 32; }
+PG_HD size_t setup_bytes(int pp) { return size_t(pp) * 16 + size_t(kMicro) * kTab * 8; }
+inline size_t line_smem_bytes(int pp, int nchild) {
+  return pattern_bytes(pp) + std::max(size_t(kMicro) * nchild * 64, setup_bytes(pp));
+}
+const size_t kMaxLineSmem = line_smem_bytes(2 * kMaxPat, kMaxLine);
 
 // A CTA's microlines m0 .. m0 + M - 1.  Set-up: warp 2 k + side builds
 // microline k's geometry and that side's subset tables (lane t < 17: term t;
@@ -331,8 +345,10 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
                                                uint4* dyn, int m0, int M, int tid, int nt) {
   const int nc = L.nchild, np = L.nparent;
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
-  uint4* psub = dyn;
-  uint4* q_smem = dyn + kSubBytes / 16;
+  uint4* pats = dyn;                                   // microline k at 2 pp k
+  uint4* q_smem = dyn + kMicro * 2 * pp;               // microline k at 4 nc k
+  uint4* psub = q_smem;                                // set-up scratch, until the children
+  uint2* tab1 = reinterpret_cast<uint2*>(psub + pp);   // opponent's tables, microline k at kTab k
   const int warp = tid >> 5, lane = tid & 31;
   if (warp < 2 * M) {
     const int k = warp >> 1, side = warp & 1;
@@ -343,6 +359,7 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
     uint64_t c0 = lane < kTerms ? 0 : f;
 #pragma unroll
     for (int o = 16; o; o >>= 1) c0 |= __shfl_xor_sync(0xffffffffu, c0, o);
+    uint2* tab = side ? tab1 + k * kTab : S.tab[k];
 #pragma unroll
     for (int j = 0; j < (kTab + 31) / 32; j++) {
       const int e = lane + 32 * j, c = table_chunk(e), sub = e - 16 * c;
@@ -352,23 +369,26 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
         const uint64_t fb = __shfl_sync(0xffffffffu, f, 4 * c + b < kTerms ? 4 * c + b : 0);
         if (sub >> b & 1) v |= fb;
       }
-      if (e < kTab) S.tab[k][side][e] = make_uint2(uint32_t(v), uint32_t(v >> 32));
+      if (e < kTab) tab[e] = make_uint2(uint32_t(v), uint32_t(v >> 32));
     }
   }
-  for (int x = tid; x < pp; x += nt) {
-    const int side = x >= p0, rr = side ? x - p0 : x;
-    psub[side * kMaxPat + rr] = pattern_terms<DIM>(L, T, side, rr);
-  }
+  for (int x = tid; x < pp; x += nt) psub[x] = pattern_terms<DIM>(L, T, x >= p0, x >= p0 ? x - p0 : x);
   __syncthreads();
-  for (int x = tid; x < M * pp; x += nt) {
-    const int k = x / pp, r = x - k * pp, side = r >= p0, rr = side ? r - p0 : r;
-    const super8 w = table_eval<DIM>(S.tab[k][side], psub[side * kMaxPat + rr]);
-    pattern_store(S.pat[k], side * kMaxPat + rr, w);
+  // Each thread's first child is loaded while the patterns are evaluated.
+  super8 cw, cn;
+  if (!L.slice35 && tid < M * nc) {
+    const uint64_t* a = child_addr(L, S.ctx[tid / nc].G, tid % nc);
+    cw = s_load_ldg(a);
+    cn = s_load_ldg(a + 4);
   }
+  for (int x = tid; x < M * pp; x += nt) {
+    const int k = x / pp, e = x - k * pp;
+    const super8 w = table_eval<DIM>(e >= p0 ? tab1 + k * kTab : S.tab[k], psub[e]);
+    pattern_store(pats + 2 * pp * k, e, pp, w);
+  }
+  __syncthreads();  // the set-up scratch is free from here on
   if (!L.slice35 && tid < M * nc) {
     // Each thread's next child is loaded while it transforms the current one.
-    const uint64_t* a = child_addr(L, S.ctx[tid / nc].G, tid % nc);
-    super8 cw = s_load_ldg(a), cn = s_load_ldg(a + 4);
     for (int x = tid; x < M * nc; x += nt) {
       const int k = x / nc, j = x - k * nc;
       const super8 w = cw, n = cn;
@@ -397,7 +417,7 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
       const int in = (x + nt) % np;
       r0 = ldg(recs + 3 * in); r1 = ldg(recs + 3 * in + 1); r2 = ldg(recs + 3 * in + 2);
     }
-    parent_node<DIM>(L, S.ctx[k], S.tab[k][0], q_smem + 4 * k * nc, S.pat[k], a, b, c, i, &errors);
+    parent_node<DIM>(L, S.ctx[k], S.tab[k], q_smem + 4 * k * nc, pats + 2 * pp * k, a, b, c, i, &errors);
   }
   if (errors) record_errors(errors);
 }
@@ -427,7 +447,8 @@ end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
 // The same microline code run sequentially on the host, for CPU self-tests of
 // the kernel arithmetic.  Never used by the device entry points.
 template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_tables_t& T) {
-  std::vector<uint4> q(4 * std::max(L.nchild, 1)), pat(2 * kMaxPat * 2);
+  const int pp = L.npat[0] + L.npat[1];
+  std::vector<uint4> q(4 * std::max(L.nchild, 1)), pat(2 * std::max(pp, 1));
   unsigned errors = 0;
   micro_ctx c;
   uint2 fterm[kTerms], tab[2][kTab];
@@ -444,7 +465,7 @@ template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_table
       for (int e = 0; e < kTab; e++) tab[side][e] = table_entry(fterm, c0, e);
       for (int r = 0; r < L.npat[side]; r++) {
         const super8 w = table_eval<DIM>(tab[side], pattern_terms<DIM>(L, T, side, r));
-        pattern_store(pat.data(), side * kMaxPat + r, w);
+        pattern_store(pat.data(), side ? L.npat[0] + r : r, pp, w);
       }
     }
     if (!L.slice35)
@@ -465,6 +486,7 @@ struct end_plan {
   std::vector<line_dev_t> host[4];
   line_dev_t* dev[4] = {nullptr, nullptr, nullptr, nullptr};
   int maxchild[4] = {0, 0, 0, 0};
+  int maxpat[4] = {0, 0, 0, 0};         // most stone patterns (both sides) of a line
   // parent records of every (section, dimension) used, back to back
   std::vector<parent_rec> recs;
   std::vector<size_t> rec_off[4];       // per planned line: offset into recs
@@ -473,7 +495,7 @@ struct end_plan {
 
 template<int DIM> static int set_smem_attr() {
   return cudaFuncSetAttribute(end_line_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kSubBytes + kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
+                              kMaxLineSmem) == cudaSuccess ? 0 : PG_ERR_CUDA;
 }
 template<int DIM> static int set_smem_limit() {
   return per_device_once((const void*)&set_smem_attr<DIM>, set_smem_attr<DIM>);
@@ -483,7 +505,7 @@ static int launch_group(const end_plan& P, int dim, cudaStream_t stream, const d
   const int n = int(P.host[dim].size());
   if (!n) return PG_OK;
   const dim3 grid((512 + kMicro - 1) / kMicro, unsigned(n));
-  const size_t smem = kSubBytes + size_t(kMicro) * P.maxchild[dim] * 64;
+  const size_t smem = line_smem_bytes(P.maxpat[dim], P.maxchild[dim]);
   int rc = 0;
   switch (dim) {
     case 0: rc = set_smem_limit<0>(); end_line_kernel<0><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
@@ -549,6 +571,7 @@ static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
       seen.emplace_back(key, off);
     }
     P.maxchild[d.dim] = std::max(P.maxchild[d.dim], d.nchild);
+    P.maxpat[d.dim] = std::max(P.maxpat[d.dim], d.npat[0] + d.npat[1]);
     P.host[d.dim].push_back(d);
     P.rec_off[d.dim].push_back(off);
   }
@@ -842,7 +865,7 @@ static_assert(sizeof(family_t) % 16 == 0, "family_t array keeps proto 16-byte al
 
 template<int DIM> static int sweep_smem_attr() {
   return cudaFuncSetAttribute(sweep_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              kSubBytes + kMicro * kMaxLine * 64) == cudaSuccess ? 0 : PG_ERR_CUDA;
+                              kMaxLineSmem) == cudaSuccess ? 0 : PG_ERR_CUDA;
 }
 template<int DIM> static int sweep_smem_limit() {
   return per_device_once((const void*)&sweep_smem_attr<DIM>, sweep_smem_attr<DIM>);
@@ -1002,7 +1025,7 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
     std::vector<family_t> fams;
     std::vector<parent_rec> recs;
     std::vector<size_t> rec_off;
-    int total = 0, maxchild = 0;
+    int total = 0, maxchild = 0, maxpat = 0;
     for (int i = 0; i < np; i++) {
       const section_t sec = section_t::from_sig(parent_sigs[i]);
       if (sec.c[dim][0] + sec.c[dim][1] >= 9) continue;
@@ -1016,6 +1039,7 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
       F.first_line = total;
       total += F.nlines;
       maxchild = std::max(maxchild, F.proto.nchild);
+      maxpat = std::max(maxpat, F.proto.npat[0] + F.proto.npat[1]);
       parent_records(sec.sig(), dim, tmp);
       rec_off.push_back(recs.size());
       recs.insert(recs.end(), tmp.begin(), tmp.end());
@@ -1029,7 +1053,7 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
     family_t* d = nullptr;
     PG_CUDA(X.alloc(&d, sizeof(family_t) * fams.size()));
     PG_CUDA(cudaMemcpyAsync(d, fams.data(), sizeof(family_t) * fams.size(), cudaMemcpyHostToDevice, stream));
-    const size_t smem = kSubBytes + size_t(kMicro) * maxchild * 64;
+    const size_t smem = line_smem_bytes(maxpat, maxchild);
     for (int line0 = 0; line0 < total; line0 += 1 << 30) {
       const dim3 grid(unsigned(std::min(total - line0, 1 << 30)), (512 + kMicro - 1) / kMicro);
       int rc = 0;
