@@ -426,6 +426,27 @@ int pg_shard_scatter(int slice, int total_shards, int shard_lo, int shard_hi, co
                      void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Board values from solved slice files (block_cache_t::lookup and value(),
+ * pentago/data/block_cache.cc:27-58, pentago/high/check.cc:21-37), batched:
+ * the boards are located on the GPU, missing blocks are read into a block
+ * cache in device memory (least recently used slots are reused), and the
+ * values are read there.  Boards are absolute board_t (black moves first;
+ * the side to move is the stone-count parity, not at a half move); a value
+ * is 1 (the side to move wins), 0 (tie), -1 (loses) or PG_LOOKUP_MISSING
+ * when no open file holds the board's section.
+ * ------------------------------------------------------------------------- */
+
+#define PG_LOOKUP_MISSING -2
+
+typedef struct pg_lookup_s* pg_lookup_t;
+/* Open slice files (block size 8) and a device cache of cache_bytes. */
+int pg_lookup_open(const char* const* paths, int npaths, int64_t cache_bytes, pg_lookup_t* lookup);
+/* boards and values are host arrays; one call may touch at most as many
+ * distinct blocks as the cache has slots (else PG_ERR_CAPACITY). */
+int pg_lookup_values(pg_lookup_t lookup, const uint64_t* boards, int64_t n, int32_t* values, void* stream);
+int pg_lookup_close(pg_lookup_t lookup);
+
+/* ---------------------------------------------------------------------------
  * Unit-level device operations, used by tests to check the superscore
  * library against the reference (pentago/base/superscore.h, symmetry.h).
  *   op 0: out[i] = rmax(in[i])                         in: supers
@@ -457,6 +478,10 @@ int pg_debug_barrier_timeout(unsigned polls, int* fault_out);
 /* The shard permutation (op 0 forward, 1 inverse) and boards (op 2) of n
  * host indices, with the kernels' own functions. */
 int pg_selftest_shard_host(int op, int slice, const uint64_t* in, int64_t n, uint64_t* out);
+/* The lookup's location of n boards on the host (the kernel's own code):
+ * standardized section, rotation-minimal index per quadrant, symmetry, side to move. */
+int pg_selftest_lookup_locate_host(const uint64_t* boards, int64_t n, uint64_t* sections, int32_t* index4,
+                                   uint16_t* syms, int32_t* turns);
 
 #ifdef __cplusplus
 }

@@ -1342,3 +1342,53 @@ void or_shard_symbols(int slice, int total_shards, int shard, const u64* nodes, 
     out[i] = (u8)((node[r >> 6] >> (r & 63) & 1) + 2 * (node[4 + (r >> 6)] >> (r & 63) & 1));
   }
 }
+
+/* ------------------------------------------------------------------------
+ * Board lookup in the solved database (pentago/data/block_cache.cc:27-58,
+ * with transform_board of pentago/base/symmetry.cc:46-78).
+ * ------------------------------------------------------------------------ */
+static u64 or_transform_board_global(int g, u64 board) {
+  static const int rotate_quadrants[4][4] = {{0, 1, 2, 3}, {1, 3, 0, 2}, {3, 2, 1, 0}, {2, 0, 3, 1}};
+  u16 q[4][2], r[4][2];
+  for (int i = 0; i < 4; i++) {
+    const u16 v = quadrant(board, i);
+    q[i][0] = rot_left_n(T_unpack[v][0], g & 3);
+    q[i][1] = rot_left_n(T_unpack[v][1], g & 3);
+  }
+  for (int i = 0; i < 4; i++)
+    for (int k = 0; k < 2; k++) r[i][k] = q[rotate_quadrants[g & 3][i]][k];
+  if (g & 4) {
+    for (int k = 0; k < 2; k++) { const u16 t = r[0][k]; r[0][k] = r[3][k]; r[3][k] = t; }
+    for (int i = 0; i < 4; i++)
+      for (int k = 0; k < 2; k++) r[i][k] = T_refl[r[i][k]];
+  }
+  u64 out = 0;
+  for (int i = 0; i < 4; i++) out |= (u64)(T_pack[r[i][0]] + 2 * T_pack[r[i][1]]) << (16 * i);
+  return out;
+}
+
+void or_lookup_locate(u64 board, u64* section_out, int32_t* index4, u16* sym, int32_t* turn) {
+  or_init();
+  section s;
+  int stones = 0;
+  for (int q = 0; q < 4; q++) {
+    const u16 v = quadrant(board, q);
+    s.c[q][0] = (u8)popc64(T_unpack[v][0]);
+    s.c[q][1] = (u8)popc64(T_unpack[v][1]);
+    stones += s.c[q][0] + s.c[q][1];
+  }
+  int g = 0;
+  const section std = sec_standardize(s, &g);
+  const u64 b1 = or_transform_board_global(g, board);
+  int local = 0;
+  for (int q = 0; q < 4; q++) {
+    const int ir = T_rmin_inv[quadrant(b1, q)];
+    index4[q] = ir >> 2;
+    local |= (ir & 3) << (2 * q);
+  }
+  /* symmetry1.inverse() * local: the inverse of a pure global symmetry is
+     global, and a local factor on the right only sets the local part */
+  *sym = (u16)(invert_global(g) << 8 | local);
+  *section_out = sec_sig(std);
+  *turn = stones & 1;
+}

@@ -69,6 +69,16 @@ uint64_t or_shard_size(int slice, int total_shards, int shard);
 void or_shard_symbols(int slice, int total_shards, int shard, const uint64_t* nodes, const int64_t* section_base,
                       uint8_t* out);
 
+/* Where a board's value lives in the solved database: block_cache_t::lookup
+ * (pentago/data/block_cache.cc:27-58) for an absolute board (black moves
+ * first; the side to move is the stone-count parity).  Outputs the
+ * standardized section, the rotation-minimal index per quadrant, the
+ * symmetry (global << 8 | local) that maps the stored super to the board's,
+ * and the side to move.  The board's value is bit 0 of
+ * transform_super(sym, extract(turn, aggressive, pair)) for aggressive 1
+ * (win) and 0 (win or tie). */
+void or_lookup_locate(uint64_t board, uint64_t* section, int32_t* index4, uint16_t* sym, int32_t* turn);
+
 int64_t or_rans_encode(const uint8_t* symbols, int64_t n, uint8_t* out, int64_t cap);
 int64_t or_rans_decode(const uint8_t* data, int64_t size, uint8_t* symbols, int64_t cap);
 

@@ -18,6 +18,7 @@ PG_ERR_TIMEOUT = -4
 PG_ERR_FORMAT = -5
 PG_ERR_CAPACITY = -6
 PG_ERR_IO = -7
+PG_LOOKUP_MISSING = -2
 
 PG_LINE_STORE = 0
 PG_LINE_OR = 1
@@ -156,6 +157,10 @@ SIGNATURES = {
     "pg_shard_boards": (_I, [_I, _P, _I64, _P, _P]),
     "pg_shard_scatter": (_I, [_I, _I, _I, _I, _P, _I, _P, _I, _P, _P, _P]),
     "pg_selftest_shard_host": (_I, [_I, _I, _P, _I64, _P]),
+    "pg_lookup_open": (_I, [ctypes.POINTER(ctypes.c_char_p), _I, _I64, ctypes.POINTER(_P)]),
+    "pg_lookup_values": (_I, [_P, _P, _I64, _P, _P]),
+    "pg_lookup_close": (_I, [_P]),
+    "pg_selftest_lookup_locate_host": (_I, [_P, _I64, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -34,6 +34,7 @@ SIGS = {
     "midsolve": (_i, [_u64, _p, _p]),
     "midsolve_internal": (None, [_u64, _p]),
     "midsolve_workspace_size": (_i, [_i]),
+    "lookup_locate": (None, [_u64, _p, _p, _p, _p]),
     "st_filter": (None, [_p, _i64, _i, _i, _p]),
     "st_unfilter": (None, [_p, _i64, _i, _i, _p]),
     "rans_encode": (_i64, [_p, _i64, _p, _i64]),
