@@ -428,9 +428,10 @@ int pg_shard_scatter(int slice, int total_shards, int shard_lo, int shard_hi, co
 /* ---------------------------------------------------------------------------
  * Board values from solved slice files (block_cache_t::lookup and value(),
  * pentago/data/block_cache.cc:27-58, pentago/high/check.cc:21-37), batched:
- * the boards are located on the GPU, missing blocks are read into a block
- * cache in device memory (least recently used slots are reused), and the
- * values are read there.  Boards are absolute board_t (black moves first;
+ * the boards are located on the GPU and their blocks found in a block cache
+ * in device memory through a device hash table; only blocks not cached go
+ * through the host, which reads them into free slots or slots no board of
+ * the call uses (in clock order); the values are then read on the GPU.  Boards are absolute board_t (black moves first;
  * the side to move is the stone-count parity, not at a half move); a value
  * is 1 (the side to move wins), 0 (tie), -1 (loses) or PG_LOOKUP_MISSING
  * when no open file holds the board's section.
@@ -445,6 +446,8 @@ int pg_lookup_open(const char* const* paths, int npaths, int64_t cache_bytes, pg
  * distinct blocks as the cache has slots (else PG_ERR_CAPACITY). */
 int pg_lookup_values(pg_lookup_t lookup, const uint64_t* boards, int64_t n, int32_t* values, void* stream);
 int pg_lookup_close(pg_lookup_t lookup);
+/* Boards served without reading a block, blocks read, and cache slots, so far. */
+int pg_lookup_stats(pg_lookup_t lookup, int64_t* stats3);
 
 /* ---------------------------------------------------------------------------
  * Unit-level device operations, used by tests to check the superscore

@@ -160,6 +160,7 @@ SIGNATURES = {
     "pg_lookup_open": (_I, [ctypes.POINTER(ctypes.c_char_p), _I, _I64, ctypes.POINTER(_P)]),
     "pg_lookup_values": (_I, [_P, _P, _I64, _P, _P]),
     "pg_lookup_close": (_I, [_P]),
+    "pg_lookup_stats": (_I, [_P, _P]),
     "pg_selftest_lookup_locate_host": (_I, [_P, _I64, _P, _P, _P, _P]),
 }
 

@@ -10,7 +10,7 @@
 #include "../../include/pentago_b200.h"
 #include "runtime.h"
 #include "superscore.cuh"
-#include <list>
+#include <algorithm>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -157,14 +157,78 @@ __global__ void lookup_value_kernel(const lookup_loc_t* __restrict__ locs, const
   }
 }
 
-struct block_key {
-  uint64_t section;
-  uint32_t block;
-  bool operator==(const block_key& o) const { return section == o.section && block == o.block; }
+// Cache keys: the section's eight counts (4 bits each) and the block's four
+// coordinates (6 bits each) in one word; ~0 marks an empty table entry.
+PG_HD uint64_t block_key(const lookup_loc_t& L) {
+  uint64_t k = 0;
+  for (int i = 0; i < 8; i++) k |= (L.section >> (8 * i) & 15) << (4 * i);
+  for (int q = 0; q < 4; q++) k |= uint64_t(L.block[q] & 63) << (32 + 6 * q);
+  return k;
+}
+constexpr uint64_t kEmpty = ~uint64_t(0);
+
+PG_HD uint64_t key_hash(uint64_t k) {
+  k ^= k >> 29;
+  k *= 0xBF58476D1CE4E5B9ull;
+  k ^= k >> 32;
+  return k;
+}
+
+// The open-addressed (linear probing) map block -> cache slot, mirrored on
+// the device; the host edits it when blocks come and go.
+struct slot_table {
+  uint64_t* keys;   // mask + 1 entries
+  int32_t* slots;
+  uint64_t mask;
 };
-struct block_key_hash {
-  size_t operator()(const block_key& k) const { return std::hash<uint64_t>()(k.section * 0x9E3779B97F4A7C15ull ^ k.block); }
-};
+
+PG_HD int32_t table_find(const slot_table& H, uint64_t key) {
+  for (uint64_t i = key_hash(key) & H.mask;; i = (i + 1) & H.mask) {
+    const uint64_t k = ldg(H.keys + i);
+    if (k == key) return ldg(H.slots + i);
+    if (k == kEmpty) return -1;
+  }
+}
+
+// Sections the open files hold (sorted), for telling missing boards apart.
+PG_HD bool section_known(const uint64_t* secs, int n, uint64_t s) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ldg(secs + mid) < s) lo = mid + 1; else hi = mid;
+  }
+  return lo < n && ldg(secs + lo) == s;
+}
+
+// Locate every board and find its block in the cache: slot >= 0 (and the
+// slot is marked used by this call), PG_LOOKUP_MISSING for boards of no
+// open section, or -1 with the board queued for the host.
+__global__ void lookup_probe_kernel(const dev_tables_t T, const uint64_t* __restrict__ boards, int64_t n,
+                                    const uint64_t* __restrict__ secs, int nsecs, const slot_table H,
+                                    lookup_loc_t* __restrict__ locs, int32_t* __restrict__ slot_of_board,
+                                    uint32_t* __restrict__ used, uint32_t call, unsigned long long* __restrict__ nmiss,
+                                    int64_t* __restrict__ misses) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    const lookup_loc_t L = lookup_locate(T, boards[i]);
+    locs[i] = L;
+    int32_t slot = PG_LOOKUP_MISSING;
+    if (section_known(secs, nsecs, L.section)) {
+      slot = table_find(H, block_key(L));
+      if (slot >= 0) used[slot] = call;
+      else misses[atomicAdd(nmiss, 1ull)] = i;
+    }
+    slot_of_board[i] = slot;
+  }
+}
+
+// The queued boards, once their blocks are in the cache.
+__global__ void lookup_reprobe_kernel(const int64_t* __restrict__ misses, int64_t m, const lookup_loc_t* __restrict__ locs,
+                                      const slot_table H, int32_t* __restrict__ slot_of_board) {
+  for (int64_t j = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < m; j += int64_t(gridDim.x) * blockDim.x) {
+    const int64_t i = misses[j];
+    slot_of_board[i] = table_find(H, block_key(locs[i]));
+  }
+}
 
 unsigned grid_for(int64_t n) { return unsigned(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 32))); }
 
@@ -176,13 +240,54 @@ using namespace pg;
 struct pg_lookup_s {
   std::vector<pg_supertensor_reader_t> readers;
   std::unordered_map<uint64_t, std::pair<int, int>> where;  // section -> (reader, section index)
+  uint64_t* secs_dev = nullptr;                             // the sections, sorted
+  int nsecs = 0;
   uint64_t* cache = nullptr;
   int slots = 0;
-  // least recently used first
-  std::list<block_key> lru;
-  std::unordered_map<block_key, std::pair<int, std::list<block_key>::iterator>, block_key_hash> slot_of;
-  std::vector<int> free_slots;
+  // block -> slot map: host copy and device copy
+  std::vector<uint64_t> keys;
+  std::vector<int32_t> table_slots;
+  slot_table dev = {nullptr, nullptr, 0};
+  std::vector<uint64_t> key_of_slot;  // kEmpty when free
+  uint32_t* used_dev = nullptr;       // per slot: the last call that used it
+  uint32_t call = 0;
+  int hand = 0;                       // next slot the eviction looks at
+  int64_t hits = 0, reads = 0;
 };
+
+namespace {
+
+void table_insert(pg_lookup_s& L, uint64_t key, int32_t slot) {
+  uint64_t i = key_hash(key) & L.dev.mask;
+  while (L.keys[i] != kEmpty) i = (i + 1) & L.dev.mask;
+  L.keys[i] = key;
+  L.table_slots[i] = slot;
+}
+
+// Removal from a linear-probing table: later entries of the run move back
+// into the hole when their home position allows it.
+void table_erase(pg_lookup_s& L, uint64_t key) {
+  const uint64_t m = L.dev.mask;
+  uint64_t i = key_hash(key) & m;
+  while (L.keys[i] != key) {
+    if (L.keys[i] == kEmpty) return;
+    i = (i + 1) & m;
+  }
+  for (uint64_t j = (i + 1) & m;; j = (j + 1) & m) {
+    if (L.keys[j] == kEmpty) break;
+    const uint64_t h = key_hash(L.keys[j]) & m;
+    // entry j may fill hole i if its home h is not cyclically inside (i, j]
+    if (((j - h) & m) >= ((j - i) & m)) {
+      L.keys[i] = L.keys[j];
+      L.table_slots[i] = L.table_slots[j];
+      i = j;
+    }
+  }
+  L.keys[i] = kEmpty;
+  L.table_slots[i] = -1;
+}
+
+}  // namespace
 
 extern "C" int pg_lookup_open(const char* const* paths, int npaths, int64_t cache_bytes, pg_lookup_t* out) {
   if (!out || npaths < 0 || (npaths && !paths) || cache_bytes < 0) return fail(PG_ERR_ARG, "bad lookup arguments");
@@ -195,6 +300,7 @@ extern "C" int pg_lookup_open(const char* const* paths, int npaths, int64_t cach
     pg_lookup_close(L);
     return rc;
   };
+  std::vector<uint64_t> secs;
   for (int f = 0; f < npaths; f++) {
     pg_supertensor_reader_t r = nullptr;
     const int ns = pg_supertensor_open(paths[f], &r);
@@ -204,13 +310,29 @@ extern "C" int pg_lookup_open(const char* const* paths, int npaths, int64_t cach
       pg_supertensor_header_t h;
       pg_supertensor_header(r, s, &h);
       if (h.block_size != 8) return cleanup(fail(PG_ERR_FORMAT, "lookups need files of block size 8"));
-      L->where.emplace(h.section, std::make_pair(f, s));
+      if (L->where.emplace(h.section, std::make_pair(f, s)).second) secs.push_back(h.section);
     }
   }
-  L->slots = int(std::min<int64_t>(cache_bytes / slot_bytes, 1 << 30));
-  if (cudaMalloc(&L->cache, size_t(L->slots) * slot_bytes) != cudaSuccess)
+  std::sort(secs.begin(), secs.end());
+  L->nsecs = int(secs.size());
+  L->slots = int(std::min<int64_t>(cache_bytes / slot_bytes, 1 << 28));
+  uint64_t cap = 2;
+  while (cap < 2 * uint64_t(L->slots)) cap <<= 1;
+  L->keys.assign(cap, kEmpty);
+  L->table_slots.assign(cap, -1);
+  L->key_of_slot.assign(L->slots, kEmpty);
+  L->dev.mask = cap - 1;
+  if (cudaMalloc(&L->cache, size_t(L->slots) * slot_bytes) != cudaSuccess ||
+      cudaMalloc(&L->dev.keys, sizeof(uint64_t) * cap) != cudaSuccess ||
+      cudaMalloc(&L->dev.slots, sizeof(int32_t) * cap) != cudaSuccess ||
+      cudaMalloc(&L->used_dev, sizeof(uint32_t) * L->slots) != cudaSuccess ||
+      cudaMalloc(&L->secs_dev, sizeof(uint64_t) * std::max<size_t>(secs.size(), 1)) != cudaSuccess)
     return cleanup(fail(PG_ERR_CAPACITY, "cannot allocate the block cache"));
-  for (int s = L->slots - 1; s >= 0; s--) L->free_slots.push_back(s);
+  if (cudaMemcpy(L->dev.keys, L->keys.data(), sizeof(uint64_t) * cap, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(L->dev.slots, L->table_slots.data(), sizeof(int32_t) * cap, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemset(L->used_dev, 0, sizeof(uint32_t) * L->slots) != cudaSuccess ||
+      (secs.size() && cudaMemcpy(L->secs_dev, secs.data(), sizeof(uint64_t) * secs.size(), cudaMemcpyHostToDevice) != cudaSuccess))
+    return cleanup(fail(PG_ERR_CUDA, "cannot initialize the block cache"));
   *out = L;
   return PG_OK;
 }
@@ -225,82 +347,89 @@ extern "C" int pg_lookup_values(pg_lookup_t L, const uint64_t* boards, int64_t n
   uint64_t* b_dev = nullptr;
   lookup_loc_t* loc_dev = nullptr;
   int32_t *slot_dev = nullptr, *val_dev = nullptr;
+  int64_t* miss_dev = nullptr;
+  unsigned long long* nmiss_dev = nullptr;
   PG_CUDA(scratch.alloc(&b_dev, sizeof(uint64_t) * n));
   PG_CUDA(scratch.alloc(&loc_dev, sizeof(lookup_loc_t) * n));
   PG_CUDA(scratch.alloc(&slot_dev, sizeof(int32_t) * n));
   PG_CUDA(scratch.alloc(&val_dev, sizeof(int32_t) * n));
+  PG_CUDA(scratch.alloc(&miss_dev, sizeof(int64_t) * n));
+  PG_CUDA(scratch.alloc(&nmiss_dev, sizeof(unsigned long long)));
+  const uint32_t call = ++L->call;
+  PG_CUDA(cudaMemsetAsync(nmiss_dev, 0, sizeof(unsigned long long), stream));
   PG_CUDA(cudaMemcpyAsync(b_dev, boards, sizeof(uint64_t) * n, cudaMemcpyHostToDevice, stream));
-  lookup_locate_kernel<<<grid_for(n), 256, 0, stream>>>(*T, b_dev, n, loc_dev);
+  lookup_probe_kernel<<<grid_for(n), 256, 0, stream>>>(*T, b_dev, n, L->secs_dev, L->nsecs, L->dev, loc_dev, slot_dev,
+                                                       L->used_dev, call, nmiss_dev, miss_dev);
   PG_CUDA(cudaGetLastError());
-  std::vector<lookup_loc_t> locs(n);
-  PG_CUDA(cudaMemcpyAsync(locs.data(), loc_dev, sizeof(lookup_loc_t) * n, cudaMemcpyDeviceToHost, stream));
+  unsigned long long m = 0;
+  PG_CUDA(cudaMemcpyAsync(&m, nmiss_dev, sizeof m, cudaMemcpyDeviceToHost, stream));
   PG_CUDA(cudaStreamSynchronize(stream));
-  // The call's distinct blocks; refused before any change if they outnumber the slots
-  std::vector<block_key> keys(n);
-  std::vector<char> known(n, 0);
-  std::unordered_map<block_key, int, block_key_hash> mine;  // block -> slot
-  for (int64_t i = 0; i < n; i++) {
-    if (!L->where.count(locs[i].section)) continue;
-    keys[i] = {locs[i].section, uint32_t(locs[i].block[0]) | uint32_t(locs[i].block[1]) << 8 |
-                                    uint32_t(locs[i].block[2]) << 16 | uint32_t(locs[i].block[3]) << 24};
-    known[i] = 1;
-    mine.emplace(keys[i], -1);
-  }
-  if (int64_t(mine.size()) > L->slots) return fail(PG_ERR_CAPACITY, "more distinct blocks than cache slots in one call");
-  // Cached blocks move to the back of the LRU list, so that the missing ones,
-  // which take free slots or evict from the front, never evict one of them
-  for (auto& kv : mine) {
-    const auto c = L->slot_of.find(kv.first);
-    if (c == L->slot_of.end()) continue;
-    kv.second = c->second.first;
-    L->lru.erase(c->second.second);
-    L->lru.push_back(kv.first);
-    c->second.second = std::prev(L->lru.end());
-  }
-  std::vector<std::vector<std::pair<block_key, int>>> reads(L->readers.size());
-  for (auto& kv : mine) {
-    if (kv.second >= 0) continue;
-    int slot;
-    if (!L->free_slots.empty()) {
-      slot = L->free_slots.back();
-      L->free_slots.pop_back();
-    } else {
-      const block_key old = L->lru.front();
-      L->lru.pop_front();
-      slot = L->slot_of[old].first;
-      L->slot_of.erase(old);
-    }
-    L->lru.push_back(kv.first);
-    L->slot_of[kv.first] = std::make_pair(slot, std::prev(L->lru.end()));
-    kv.second = slot;
-    reads[L->where[kv.first.section].first].emplace_back(kv.first, slot);
-  }
-  std::vector<int32_t> slots(n, -1);
-  for (int64_t i = 0; i < n; i++)
-    if (known[i]) slots[i] = mine[keys[i]];
-  for (size_t f = 0; f < reads.size(); f++) {
-    if (reads[f].empty()) continue;
-    std::vector<int32_t> secs;
-    std::vector<uint8_t> blks;
-    std::vector<int64_t> offs;
-    for (const auto& kv : reads[f]) {
-      secs.push_back(L->where[kv.first.section].second);
-      for (int q = 0; q < 4; q++) blks.push_back(uint8_t(kv.first.block >> (8 * q)));
-      offs.push_back(int64_t(kv.second) * kBlockNodes);
-    }
-    const int rc = pg_supertensor_read_blocks(L->readers[f], int(secs.size()), secs.data(), blks.data(), L->cache,
-                                              offs.data(), PG_ST_RAW, 0, stream);
-    if (rc) {
-      // the slots of a failed read hold nothing valid
-      for (const auto& kv : reads[f]) {
-        L->lru.erase(L->slot_of[kv.first].second);
-        L->slot_of.erase(kv.first);
-        L->free_slots.push_back(kv.second);
+  L->hits += n - int64_t(m);
+  if (m) {
+    // Which blocks the queued boards need
+    std::vector<int64_t> miss(m);
+    std::vector<lookup_loc_t> locs(n);
+    PG_CUDA(cudaMemcpyAsync(miss.data(), miss_dev, sizeof(int64_t) * m, cudaMemcpyDeviceToHost, stream));
+    PG_CUDA(cudaMemcpyAsync(locs.data(), loc_dev, sizeof(lookup_loc_t) * n, cudaMemcpyDeviceToHost, stream));
+    std::vector<uint32_t> used(L->slots);
+    PG_CUDA(cudaMemcpyAsync(used.data(), L->used_dev, sizeof(uint32_t) * L->slots, cudaMemcpyDeviceToHost, stream));
+    PG_CUDA(cudaStreamSynchronize(stream));
+    std::unordered_map<uint64_t, const lookup_loc_t*> need;
+    for (int64_t i : miss) need.emplace(block_key(locs[i]), &locs[i]);
+    int64_t busy = 0;
+    for (int s = 0; s < L->slots; s++) busy += used[s] == call;
+    if (busy + int64_t(need.size()) > L->slots)
+      return fail(PG_ERR_CAPACITY, "more distinct blocks than cache slots in one call");
+    // Slots not used by this call, free ones first, then round the clock
+    std::vector<std::vector<std::pair<const lookup_loc_t*, int>>> reads(L->readers.size());
+    std::vector<int> taken;
+    for (const auto& kv : need) {
+      int slot = -1;
+      for (int tries = 0; tries < L->slots && slot < 0; tries++) {
+        const int s = L->hand;
+        L->hand = (L->hand + 1) % L->slots;
+        if (used[s] == call) continue;
+        slot = s;
       }
-      return rc;
+      used[slot] = call;
+      if (L->key_of_slot[slot] != kEmpty) table_erase(*L, L->key_of_slot[slot]);
+      L->key_of_slot[slot] = kv.first;
+      table_insert(*L, kv.first, slot);
+      taken.push_back(slot);
+      reads[L->where[kv.second->section].first].emplace_back(kv.second, slot);
     }
+    int rc = PG_OK;
+    for (size_t f = 0; f < reads.size() && rc == PG_OK; f++) {
+      if (reads[f].empty()) continue;
+      std::vector<int32_t> secs;
+      std::vector<uint8_t> blks;
+      std::vector<int64_t> offs;
+      for (const auto& r : reads[f]) {
+        secs.push_back(L->where[r.first->section].second);
+        for (int q = 0; q < 4; q++) blks.push_back(r.first->block[q]);
+        offs.push_back(int64_t(r.second) * kBlockNodes);
+      }
+      rc = pg_supertensor_read_blocks(L->readers[f], int(secs.size()), secs.data(), blks.data(), L->cache,
+                                      offs.data(), PG_ST_RAW, 0, stream);
+      L->reads += int64_t(secs.size());
+    }
+    if (rc != PG_OK) {
+      // the slots of this call's reads hold nothing valid
+      for (int s : taken) {
+        table_erase(*L, L->key_of_slot[s]);
+        L->key_of_slot[s] = kEmpty;
+      }
+    }
+    const uint64_t cap = L->dev.mask + 1;
+    PG_CUDA(cudaMemcpyAsync(L->dev.keys, L->keys.data(), sizeof(uint64_t) * cap, cudaMemcpyHostToDevice, stream));
+    PG_CUDA(cudaMemcpyAsync(L->dev.slots, L->table_slots.data(), sizeof(int32_t) * cap, cudaMemcpyHostToDevice, stream));
+    PG_CUDA(cudaMemcpyAsync(L->used_dev, used.data(), sizeof(uint32_t) * L->slots, cudaMemcpyHostToDevice, stream));
+    // the host copies above are read before they change again
+    PG_CUDA(cudaStreamSynchronize(stream));
+    if (rc != PG_OK) return rc;
+    lookup_reprobe_kernel<<<grid_for(int64_t(m)), 256, 0, stream>>>(miss_dev, int64_t(m), loc_dev, L->dev, slot_dev);
+    PG_CUDA(cudaGetLastError());
   }
-  PG_CUDA(cudaMemcpyAsync(slot_dev, slots.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
   lookup_value_kernel<<<grid_for(n), 256, 0, stream>>>(loc_dev, slot_dev, n, L->cache, val_dev);
   PG_CUDA(cudaGetLastError());
   PG_CUDA(cudaMemcpyAsync(values, val_dev, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, stream));
@@ -311,8 +440,17 @@ extern "C" int pg_lookup_values(pg_lookup_t L, const uint64_t* boards, int64_t n
 extern "C" int pg_lookup_close(pg_lookup_t L) {
   if (!L) return PG_OK;
   for (auto r : L->readers) pg_supertensor_close(r);
-  if (L->cache) cudaFree(L->cache);
+  for (void* p : {(void*)L->cache, (void*)L->dev.keys, (void*)L->dev.slots, (void*)L->used_dev, (void*)L->secs_dev})
+    if (p) cudaFree(p);
   delete L;
+  return PG_OK;
+}
+
+extern "C" int pg_lookup_stats(pg_lookup_t L, int64_t* stats3) {
+  if (!L || !stats3) return fail(PG_ERR_ARG, "bad arguments");
+  stats3[0] = L->hits;
+  stats3[1] = L->reads;
+  stats3[2] = L->slots;
   return PG_OK;
 }
 

@@ -40,6 +40,12 @@ class block_cache_t:
     def value(self, board):
         return int(self.values([board])[0])
 
+    def stats(self):
+        """(boards served without reading a block, blocks read, cache slots)."""
+        out = np.zeros(3, np.int64)
+        capi.check(capi.lib().pg_lookup_stats(self.handle, capi.ptr(out)))
+        return tuple(int(x) for x in out)
+
     def close(self):
         if self.handle:
             capi.lib().pg_lookup_close(self.handle)
@@ -52,3 +58,31 @@ class block_cache_t:
 def reader_block_cache(paths, memory=1 << 30):
     """A block cache over slice files (block_cache.cc:85-140)."""
     return block_cache_t(paths, memory)
+
+
+def bench(paths, nboards=1 << 22, slices=range(6), reps=5, memory=1 << 30):
+    """Lookups per second of random positions of the given slices (through
+    the shard mapping's boards), with every block already cached, host boards
+    in and host values out included."""
+    import time
+    import torch
+    from .shard import shard_mapping_t
+    rng = np.random.default_rng(0)
+    parts = []
+    for s in slices:
+        m = shard_mapping_t(s)
+        parts.append(m.board(rng.integers(0, m.total(), nboards // len(slices), dtype=np.uint64)))
+    boards = np.ascontiguousarray(np.concatenate(parts))
+    cache = reader_block_cache(paths, memory)
+    t = time.perf_counter()
+    cache.values(boards)
+    cold = time.perf_counter() - t
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    for _ in range(reps):
+        cache.values(boards)
+    warm = (time.perf_counter() - t) / reps
+    hits, reads, slots = cache.stats()
+    return {"workload": f"{len(boards)} random positions of slices {list(slices)} per call", "boards": len(boards),
+            "cold_s": cold, "warm_s": warm, "boards_per_s": len(boards) / warm, "blocks_read": reads,
+            "cache_slots": slots}
