@@ -276,6 +276,51 @@ def cpu_scatter_rate(slice_, total_shards, seconds=8.0):
                       f"{total_shards} shards, {sec:.1f} s; format-2 coding not included"}
 
 
+def cpu_lookup_rate(paths, seconds=5.0):
+    """The oracle's restatement of the reference's block-cache lookup and
+    value() (a scalar port, one thread) over the same slice files, held
+    decompressed in host memory (so no reads are timed), on random positions."""
+    import ctypes
+    import numpy as np
+    from tests.oracle import oracle, P
+    from pentago_b200 import supertensor
+    from pentago_b200.sweep import slice_layout
+    O = oracle()
+    for name in ("or_shard_total", "or_shard_board"):
+        getattr(O.lib, name).restype = ctypes.c_uint64
+    O.lib.or_shard_board.argtypes = [ctypes.c_int, ctypes.c_uint64]
+    readers = {}
+    slices = []
+    for path in paths:
+        for r in supertensor.open_supertensors(path):
+            readers[r.header.section] = r
+            slices.append(r.header.stones)
+    secs = np.array(sorted(readers), np.uint64)
+    off = slice_layout(secs)
+    data = np.zeros((int(off[-1]), 8), np.uint64)
+    for i, sig in enumerate(secs):
+        r = readers[int(sig)]
+        idx, boff = supertensor.section_block_offsets(r.header.shape)
+        for b, o in zip(idx, boff):
+            raw = np.frombuffer(r.read_block_filtered(tuple(int(x) for x in b)).tobytes(), np.uint64).reshape(-1, 8)
+            pair = np.zeros_like(raw)
+            O.st_unfilter(P(raw), len(raw), 2, 1, P(pair))
+            data[off[i] + o:off[i] + o + len(pair)] = pair
+    rng = np.random.default_rng(0)
+    boards = np.array([O.lib.or_shard_board(s, int(x)) for s in sorted(set(slices))
+                       for x in rng.integers(0, O.lib.or_shard_total(s), 2000)], np.uint64)
+    base = np.ascontiguousarray(off[:-1])
+    vals = np.zeros(len(boards), np.int32)
+    done = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        O.lookup_values(P(boards), len(boards), P(secs), len(secs), P(base), P(data), P(vals))
+        done += len(boards)
+    el = time.perf_counter() - t0
+    return {"boards_per_s": done / el, "cores": 1, "kind": "port",
+            "sample": f"{len(boards)} random positions, lookups repeated for {el:.1f} s, blocks in host memory"}
+
+
 def sweep_summary(timings, wall_s):
     """Config 2 from the per-slice timings of the sweep (slices 35 -> 30)."""
     ms = sum(v["ms"] for v in timings.values())
@@ -366,6 +411,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-coder measurement")
     ap.add_argument("--no-slice-files", action="store_true", help="skip the slice-file filter and I/O measurement")
     ap.add_argument("--no-sharder", action="store_true", help="skip the sharder measurement")
+    ap.add_argument("--no-lookup", action="store_true", help="skip the board lookup measurement")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -496,6 +542,7 @@ def main():
     sweep2 = None
     slice_files = None
     sharder = None
+    lookups = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(seconds=12.0)
     if rank == 0 and world == 1:
@@ -535,6 +582,16 @@ def main():
         if not args.no_cpu_baseline:
             sharder["cpu_baseline"] = cpu_scatter_rate(10, 1024, seconds=8.0)
 
+    if rank == 0 and world == 1 and not args.no_lookup:
+        # Board values from the reference's solved database (slices 0..5)
+        # through the device block cache, every block already cached
+        import glob
+        from pentago_b200 import lookup as lookup_mod
+        db = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "db", "slice-*.pentago")))
+        lookups = lookup_mod.bench(db)
+        if not args.no_cpu_baseline:
+            lookups["cpu_baseline"] = cpu_lookup_rate(db, seconds=5.0)
+
     if rank == 0:
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -560,6 +617,7 @@ def main():
             "learned_rans_config3": learned,
             "slice_files": slice_files,
             "sharder": sharder,
+            "lookups": lookups,
             "clocks": clocks.summary(),
         }
         print(json.dumps(result))

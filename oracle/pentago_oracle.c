@@ -1392,3 +1392,45 @@ void or_lookup_locate(u64 board, u64* section_out, int32_t* index4, u16* sym, in
   *section_out = sec_sig(std);
   *turn = stones & 1;
 }
+
+void or_lookup_values(const u64* boards, int64_t n, const u64* secs, int nsecs, const int64_t* base, const u64* data,
+                      int32_t* values) {
+  or_init();
+  for (int64_t i = 0; i < n; i++) {
+    u64 sec;
+    int32_t idx[4], turn;
+    u16 sym;
+    or_lookup_locate(boards[i], &sec, idx, &sym, &turn);
+    int lo = 0, hi = nsecs;
+    while (lo < hi) { const int mid = (lo + hi) / 2; if (secs[mid] < sec) lo = mid + 1; else hi = mid; }
+    if (lo == nsecs || secs[lo] != sec) { values[i] = -2; continue; }
+    /* the node's offset in the block-major layout: blocks row-major, each row-major in its shape */
+    int shape[4], b[4], bs[4];
+    sec_shape(sec_from_sig(sec), shape);
+    for (int q = 0; q < 4; q++) { b[q] = idx[q] / 8; bs[q] = shape[q] - 8 * b[q] < 8 ? shape[q] - 8 * b[q] : 8; }
+    int64_t off = 0, before = 1;
+    for (int q = 0; q < 4; q++) {
+      int64_t after = 1;
+      for (int r = q + 1; r < 4; r++) after *= shape[r];
+      off += before * 8 * b[q] * after;
+      before *= bs[q];
+    }
+    const int64_t in = (((int64_t)(idx[0] % 8) * bs[1] + idx[1] % 8) * bs[2] + idx[2] % 8) * bs[3] + idx[3] % 8;
+    const u64* node = data + 8 * (base[lo] + off + in);
+    int v = -1;
+    for (int aggressive = 1; aggressive >= 0; aggressive--) {
+      super s;
+      u64 w[4];
+      for (int k = 0; k < 4; k++) {
+        const u64 black = node[k], white = node[4 + k];
+        w[k] = aggressive ? (turn ? white : black) : ~(turn ? black : white);
+      }
+      memcpy(&s, w, 32);
+      const sym_t t = {sym >> 8, sym & 255};
+      s = transform_super(t, s);
+      memcpy(w, &s, 32);
+      v += (int)(w[0] & 1);
+    }
+    values[i] = v;
+  }
+}

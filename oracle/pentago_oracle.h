@@ -78,6 +78,11 @@ void or_shard_symbols(int slice, int total_shards, int shard, const uint64_t* no
  * transform_super(sym, extract(turn, aggressive, pair)) for aggressive 1
  * (win) and 0 (win or tie). */
 void or_lookup_locate(uint64_t board, uint64_t* section, int32_t* index4, uint16_t* sym, int32_t* turn);
+/* value() of n boards (1, 0, -1 for the side to move; -2 if the section is
+ * absent) from slices held in host memory: sections secs[0..nsecs) sorted,
+ * section i's on-disk pairs in 8^4-block-major order at data + 8 base[i]. */
+void or_lookup_values(const uint64_t* boards, int64_t n, const uint64_t* secs, int nsecs, const int64_t* base,
+                      const uint64_t* data, int32_t* values);
 
 int64_t or_rans_encode(const uint8_t* symbols, int64_t n, uint8_t* out, int64_t cap);
 int64_t or_rans_decode(const uint8_t* data, int64_t size, uint8_t* symbols, int64_t cap);

@@ -35,6 +35,7 @@ SIGS = {
     "midsolve_internal": (None, [_u64, _p]),
     "midsolve_workspace_size": (_i, [_i]),
     "lookup_locate": (None, [_u64, _p, _p, _p, _p]),
+    "lookup_values": (None, [_p, _i64, _p, _i, _p, _p, _p]),
     "st_filter": (None, [_p, _i64, _i, _i, _p]),
     "st_unfilter": (None, [_p, _i64, _i, _i, _p]),
     "rans_encode": (_i64, [_p, _i64, _p, _i64]),
