@@ -118,6 +118,13 @@ int pg_descendent_sections(uint64_t root, int slice, uint64_t* sigs, int cap);
  * slice).  child_slice is the slice above (ignored for slice 35). */
 int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t* parent_slice,
                        const uint64_t* child_sigs, int nc, const uint64_t* child_slice, void* stream);
+/* The lines of a slice that read one child section only, with that
+ * section's nodes (block-major) at child_nodes: every such line ORs into
+ * parent_slice, which must start zeroed.  Calling it for every child section
+ * equals pg_end_sweep_slice, so a sweep can keep the child slice compressed
+ * and decompress one section at a time. */
+int pg_end_sweep_slice_child(const uint64_t* parent_sigs, int np, uint64_t* parent_slice, uint64_t child_section,
+                             const uint64_t* child_nodes, void* stream);
 
 /* Per-section (we-win, we-win-or-tie, total) counts over distinct positions
  * into device counts3[3 n] (count_block_wins, pentago/end/block_store.cc:330-352,
@@ -240,6 +247,13 @@ int pg_rans_decode_batch(const uint8_t* in, const int64_t* in_offsets, const int
  * node): black wins + 2 white wins, the on-disk convention of
  * pentago/shard/shard.cc:448-449.  turn = 1 when white is to move. */
 int pg_node_symbols(const uint64_t* nodes, int64_t n, int turn, uint8_t* symbols, void* stream);
+/* The inverse: n nodes of the side to move from their 256 n symbols (device,
+ * symbols 16-byte aligned). */
+int pg_symbols_nodes(const uint8_t* symbols, int64_t n, int turn, uint64_t* nodes, void* stream);
+/* Copy n coded streams (device bytes at in + in_offsets[s], sizes[s] long;
+ * the three arrays on the device) back to back at out + out_offsets[s]. */
+int pg_pack_streams(const uint8_t* in, const int64_t* in_offsets, const int64_t* sizes, int n, uint8_t* out,
+                    const int64_t* out_offsets, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Learned-model rANS for solved blocks: stream format version 3.  No

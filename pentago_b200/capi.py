@@ -109,6 +109,7 @@ SIGNATURES = {
     "pg_slice_layout": (_I, [_P, _I, _P]),
     "pg_descendent_sections": (_I, [_U64, _I, _P, _I]),
     "pg_end_sweep_slice": (_I, [_P, _I, _P, _P, _I, _P, _P]),
+    "pg_end_sweep_slice_child": (_I, [_P, _I, _P, _U64, _P, _P]),
     "pg_section_counts": (_I, [_P, _I, _P, _P, _P]),
     "pg_serve_open": (_I, [_I64, ctypes.POINTER(_P)]),
     "pg_serve_submit": (_I64, [_P, _U64]),
@@ -119,6 +120,8 @@ SIGNATURES = {
     "pg_rans_encode_batch": (_I, [_P, _P, _I, _P, _P, _P, _P]),
     "pg_rans_decode_batch": (_I, [_P, _P, _P, _I, _P, _P, _P, _P, _P]),
     "pg_node_symbols": (_I, [_P, _I64, _I, _P, _P]),
+    "pg_symbols_nodes": (_I, [_P, _I64, _I, _P, _P]),
+    "pg_pack_streams": (_I, [_P, _P, _P, _I, _P, _P, _P]),
     "pg_learned_model_bytes": (_I64, []),
     "pg_rans_learned_bound": (_I64, [_I64]),
     "pg_rans_learned_encode": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _P]),

@@ -1010,8 +1010,10 @@ extern "C" int pg_slice_layout(const uint64_t* sigs, int n, int64_t* offsets) {
   return PG_OK;
 }
 
-extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t* parent_slice,
-                                  const uint64_t* child_sigs, int nc, const uint64_t* child_slice, void* stream_) {
+// The lines of a slice, or (one_child) only those that read child_sigs[0],
+// every line then ORing into the parent slice.
+static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_slice, const uint64_t* child_sigs, int nc,
+                       const uint64_t* child_slice, bool one_child, void* stream_) {
   if (np < 0 || nc < 0 || (np && (!parent_sigs || !parent_slice))) return fail(PG_ERR_ARG, "bad sweep arguments");
   const dev_tables_t* T = device_tables();
   if (!T) return PG_ERR_CUDA;
@@ -1029,12 +1031,13 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
     for (int i = 0; i < np; i++) {
       const section_t sec = section_t::from_sig(parent_sigs[i]);
       if (sec.c[dim][0] + sec.c[dim][1] >= 9) continue;
+      if (one_child && sec.child(dim).standardize(nullptr).sig() != child_sigs[0]) continue;
       int first = 0;
       while (sec.c[first][0] + sec.c[first][1] >= 9) first++;
       fams.emplace_back();
       family_t& F = fams.back();
       if (!make_family(sec, dim, poff[i], child_sigs, nc, coff.data(), parent_slice, child_slice,
-                       dim == first ? PG_LINE_STORE : PG_LINE_OR, F, err))
+                       dim == first && !one_child ? PG_LINE_STORE : PG_LINE_OR, F, err))
         return fail(PG_ERR_ARG, "section " + std::to_string(i) + ": " + err);
       F.first_line = total;
       total += F.nlines;
@@ -1069,6 +1072,19 @@ extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t*
     }
   }
   return PG_OK;
+}
+
+extern "C" int pg_end_sweep_slice(const uint64_t* parent_sigs, int np, uint64_t* parent_slice,
+                                  const uint64_t* child_sigs, int nc, const uint64_t* child_slice, void* stream) {
+  return sweep_lines(parent_sigs, np, parent_slice, child_sigs, nc, child_slice, false, stream);
+}
+
+extern "C" int pg_end_sweep_slice_child(const uint64_t* parent_sigs, int np, uint64_t* parent_slice,
+                                        uint64_t child_section, const uint64_t* child_nodes, void* stream) {
+  if (!child_nodes) return fail(PG_ERR_ARG, "null child section");
+  const section_t c = section_t::from_sig(child_section);
+  if (!c.valid() || c.standardize(nullptr).sig() != child_section) return fail(PG_ERR_ARG, "child section not standardized");
+  return sweep_lines(parent_sigs, np, parent_slice, &child_section, 1, child_nodes, true, stream);
 }
 
 namespace pg {

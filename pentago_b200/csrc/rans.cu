@@ -284,9 +284,77 @@ __global__ void node_symbols_kernel(const uint64_t* __restrict__ nodes, int64_t 
   for (int b = 0; b < 64; b++) out[b] = uint8_t((black >> b & 1) + 2 * (white >> b & 1));
 }
 
+// The inverse: nodes of the side to move from their symbols (one thread per
+// 64 symbols, read as four 16-byte words).
+__global__ void symbols_nodes_kernel(const uint8_t* __restrict__ symbols, int64_t n, int turn,
+                                     uint64_t* __restrict__ nodes) {
+  const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i >= n * 4) return;
+  const int64_t k = i >> 2;
+  const int w = int(i & 3);
+  const uint4* in = reinterpret_cast<const uint4*>(symbols + 64 * i);
+  uint64_t black = 0, white = 0;
+#pragma unroll
+  for (int v = 0; v < 4; v++) {
+    const uint4 q = in[v];
+    const uint32_t part[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+    for (int p = 0; p < 4; p++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const uint32_t sym = part[p] >> (8 * b) & 0xff;
+        const int bit = 16 * v + 4 * p + b;
+        black |= uint64_t(sym == 1) << bit;
+        white |= uint64_t(sym == 2) << bit;
+      }
+  }
+  nodes[8 * k + w] = turn ? white : black;
+  nodes[8 * k + 4 + w] = ~(turn ? black : white);
+}
+
+// Copy stream s (in + in_offsets[s], sizes[s] bytes) to out + out_offsets[s]:
+// one CTA per stream, 16-byte words where both ends allow it.
+__global__ void pack_streams_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ in_offsets,
+                                    const int64_t* __restrict__ sizes, uint8_t* __restrict__ out,
+                                    const int64_t* __restrict__ out_offsets) {
+  const int s = blockIdx.x;
+  const uint8_t* src = in + in_offsets[s];
+  uint8_t* dst = out + out_offsets[s];
+  const int64_t n = sizes[s];
+  if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+    const int64_t w = n >> 4;
+    for (int64_t i = threadIdx.x; i < w; i += blockDim.x)
+      reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+    for (int64_t i = 16 * w + threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  } else {
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+  }
+}
+
 }  // namespace pg
 
 using namespace pg;
+
+extern "C" int pg_symbols_nodes(const uint8_t* symbols, int64_t n, int turn, uint64_t* nodes, void* stream) {
+  if (n < 0 || (n && (!symbols || !nodes))) return fail(PG_ERR_ARG, "bad node count");
+  if (reinterpret_cast<uintptr_t>(symbols) & 15) return fail(PG_ERR_ARG, "symbols must be 16-byte aligned");
+  if (!n) return PG_OK;
+  const int64_t threads = 4 * n;
+  symbols_nodes_kernel<<<unsigned((threads + 255) / 256), 256, 0, (cudaStream_t)stream>>>(symbols, n, turn & 1, nodes);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}
+
+extern "C" int pg_pack_streams(const uint8_t* in, const int64_t* in_offsets, const int64_t* sizes, int n, uint8_t* out,
+                               const int64_t* out_offsets, void* stream) {
+  if (n < 0 || (n && (!in || !in_offsets || !sizes || !out || !out_offsets))) return fail(PG_ERR_ARG, "bad pack arguments");
+  for (int s0 = 0; s0 < n; s0 += 65535) {
+    const int k = n - s0 < 65535 ? n - s0 : 65535;
+    pack_streams_kernel<<<k, 256, 0, (cudaStream_t)stream>>>(in, in_offsets + s0, sizes + s0, out, out_offsets + s0);
+    PG_CUDA(cudaGetLastError());
+  }
+  return PG_OK;
+}
 
 extern "C" int64_t pg_rans_bound(int64_t n) { return n < 0 ? PG_ERR_ARG : stream_bound(n); }
 

@@ -58,23 +58,28 @@ def _slice_of(path):
     return supertensor_slice(path)
 
 
-def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, checkpoint=None, resume=None, level=6):
+def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, checkpoint=None, resume=None, level=6,
+          compress=False):
     """Solve all sections below `root` from slice 35 down to `min_slice`.
 
     checkpoint: a directory that receives every solved slice as
     slice-N.pentago (the reference's slice file format).  resume: a slice
     file (slice N, holding at least the sections the root needs at N) to
-    start from instead of solving slices 35..N again.
+    start from instead of solving slices 35..N again.  compress: keep each
+    finished slice in HBM as format-2 streams (slice_store.compressed_slice)
+    and decompress one child section at a time while the slice below is
+    built, for roots whose two largest adjacent slices do not fit raw.
 
     Returns {slice: counts-N rows}; with keep_last also the last slice tensor."""
     import torch
+    from .slice_store import compressed_slice
     root = int(root)
     if min_slice is None:
         min_slice = sum(sum(c) for c in [[(root >> (16 * q + 8 * k)) & 255 for k in range(2)] for q in range(4)])
     L = capi.lib()
     s_handle = capi.stream_handle(stream)
     child_sigs = np.zeros(0, np.uint64)
-    child = None
+    child = None   # the slice above: a raw tensor, or compressed
     results = {}
     top = 35
     if resume is not None:
@@ -82,18 +87,33 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
         start = _slice_of(resume)
         child_sigs = descendent_sections(root, start)
         _, child_sigs, child = read_slice(resume, child_sigs, stream=stream)
+        if compress:
+            child = compressed_slice(child, child_sigs, start & 1, stream=stream)
+            torch.cuda.empty_cache()
         top = start - 1
     for slice_ in range(top, min_slice - 1, -1):
         sigs = descendent_sections(root, slice_)
         torch.cuda.synchronize()
         off = slice_layout(sigs)
-        parent = torch.empty((int(off[-1]), 8), dtype=torch.int64, device="cuda")
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
-        t0.record()
-        capi.check(L.pg_end_sweep_slice(capi.ptr(sigs), len(sigs), parent.data_ptr(), capi.ptr(child_sigs),
-                                        len(child_sigs), child.data_ptr() if child is not None else None, s_handle))
-        t1.record()
+        if isinstance(child, compressed_slice):
+            # every line reads one child section: decompress them one by one
+            parent = torch.zeros((int(off[-1]), 8), dtype=torch.int64, device="cuda")
+            t0.record()
+            for ci, csig in enumerate(child.sigs):
+                staging = child.section_nodes(ci, stream)
+                capi.check(L.pg_end_sweep_slice_child(capi.ptr(sigs), len(sigs), parent.data_ptr(),
+                                                      ctypes.c_uint64(int(csig)), staging.data_ptr(), s_handle))
+                del staging
+            t1.record()
+        else:
+            parent = torch.empty((int(off[-1]), 8), dtype=torch.int64, device="cuda")
+            t0.record()
+            capi.check(L.pg_end_sweep_slice(capi.ptr(sigs), len(sigs), parent.data_ptr(), capi.ptr(child_sigs),
+                                            len(child_sigs), child.data_ptr() if child is not None else None,
+                                            s_handle))
+            t1.record()
         counts = torch.zeros((len(sigs), 3), dtype=torch.int64, device="cuda")
         capi.check(L.pg_section_counts(capi.ptr(sigs), len(sigs), parent.data_ptr(), counts.data_ptr(), s_handle))
         c = counts.cpu().numpy().view(np.uint64)
@@ -105,10 +125,22 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
         if timings is not None:
             torch.cuda.synchronize()
             timings[slice_] = {"ms": t0.elapsed_time(t1), "sections": len(sigs), "nodes": int(off[-1]),
-                               "child_nodes": int(child.shape[0]) if child is not None else 0}
+                               "child_nodes": 0 if child is None else
+                               int(child.base[-1]) if isinstance(child, compressed_slice) else int(child.shape[0])}
         del child
         torch.cuda.empty_cache()  # the slice above is gone; its HBM must be reusable at 180 GB scale
-        child, child_sigs = parent, sigs
+        if compress and slice_ > min_slice:
+            e0 = time.perf_counter()
+            child = compressed_slice(parent, sigs, slice_ & 1, stream=stream)
+            del parent
+            torch.cuda.empty_cache()
+            if timings is not None:
+                torch.cuda.synchronize()
+                timings[slice_].update({"compress_s": time.perf_counter() - e0, "compressed_bytes": child.bytes,
+                                        "raw_bytes": child.raw_bytes})
+        else:
+            child = parent
+        child_sigs = sigs
     if keep_last:
         return results, child, child_sigs
     return results
@@ -122,6 +154,7 @@ def main():
     ap.add_argument("--checkpoint", default=None, help="directory for slice-N.pentago files of every solved slice")
     ap.add_argument("--resume", default=None, help="slice file to start from")
     ap.add_argument("--level", type=int, default=6, help="compression level of checkpoint files (zlib 1-9, xz 20-29)")
+    ap.add_argument("--compress", action="store_true", help="keep finished slices compressed in HBM (deeper roots)")
     args = ap.parse_args()
     c = [int(x) for x in args.root.split(",")]
     root = section_sig([[c[0], c[1]], [c[2], c[3]], [c[4], c[5]], [c[6], c[7]]])
@@ -132,7 +165,7 @@ def main():
     timings = {}
     t = time.perf_counter()
     res = sweep(root, args.min_slice, timings=timings, checkpoint=args.checkpoint, resume=args.resume,
-                level=args.level)
+                level=args.level, compress=args.compress)
     wall = time.perf_counter() - t
     ok = None
     if args.golden:
@@ -146,7 +179,8 @@ def main():
     print(json.dumps({"root": args.root, "slices": {str(k): v for k, v in timings.items()}, "kernel_ms": total_ms,
                       "wall_s": wall, "sections": sum(v["sections"] for v in timings.values()),
                       "sections_per_s": sum(v["sections"] for v in timings.values()) / (total_ms / 1e3),
-                      "algorithmic_GBps": nbytes / (total_ms / 1e3) / 1e9, "golden_counts_match": ok}))
+                      "algorithmic_GBps": nbytes / (total_ms / 1e3) / 1e9, "golden_counts_match": ok,
+                      "peak_GB": torch.cuda.max_memory_allocated() / 1e9}))
 
 
 if __name__ == "__main__":

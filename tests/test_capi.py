@@ -85,3 +85,14 @@ def test_line_rejects_bad_input():
         end.line_info(end.Line(end.section_sig([[4, 4], [4, 4], [4, 3], [3, 4]]), 0, (0, 0, 0), length=3))
     with pytest.raises(capi.PentagoError):
         end.line_info(end.Line(end.section_sig([[1, 4], [4, 4], [4, 3], [3, 4]]), 0, (0, 0, 0), length=1))
+
+
+def test_sweep_child_refuses_unstandardized_sections():
+    from pentago_b200 import capi
+    from pentago_b200.end import section_sig
+    L = capi.lib()
+    sig = section_sig([[4, 4], [4, 5], [4, 3], [3, 3]])
+    parents = np.array([sig], np.uint64)
+    bad = section_sig([[3, 3], [4, 3], [4, 5], [4, 4]])   # not standardized
+    dummy = np.zeros(8, np.uint64)
+    assert L.pg_end_sweep_slice_child(P(parents), 1, P(dummy), bad, P(dummy), None) == capi.PG_ERR_ARG
