@@ -256,6 +256,31 @@ int pg_pack_streams(const uint8_t* in, const int64_t* in_offsets, const int64_t*
                     const int64_t* out_offsets, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Store coder for solved blocks kept in device memory (deeper sweeps).  No
+ * reference counterpart and no file format: an internal, lossless coding of
+ * end-engine nodes (the sweep's [win, win or tie] form for side `turn`).
+ * Symbols black wins + 2 white wins per rotation, static rANS over 1024
+ * contexts (the four axis neighbours of the rotation in the node and the
+ * same rotation of the previous node); one table of 1024 x 3 frequencies
+ * (device uint16) per batch.  Block b = count[b] nodes (at most 4096) at
+ * nodes + 8 first[b]; all arrays are device arrays.
+ * ------------------------------------------------------------------------- */
+
+/* Bytes a block of `nodes` nodes may need. */
+int64_t pg_store_bound(int64_t nodes);
+/* The frequency table of a batch of blocks (from its context counts). */
+int pg_store_table(const uint64_t* nodes, const int64_t* first, const int32_t* count, int nblocks, int turn,
+                   uint16_t* table, void* stream);
+/* Block b into out + out_offsets[b] (room for pg_store_bound); sizes[b] = its bytes. */
+int pg_store_encode(const uint64_t* nodes, const int64_t* first, const int32_t* count, int nblocks, int turn,
+                    const uint16_t* table, uint8_t* out, const int64_t* out_offsets, int64_t* sizes, void* stream);
+/* Stream b (in + in_offsets[b], in_sizes[b] bytes, count[b] nodes) back to
+ * nodes + 8 dst[b]; status[b] = nodes decoded or PG_ERR_FORMAT. */
+int pg_store_decode(const uint8_t* in, const int64_t* in_offsets, const int64_t* in_sizes, const int32_t* count,
+                    const int64_t* dst, int nblocks, int turn, const uint16_t* table, uint64_t* nodes, int64_t* status,
+                    void* stream);
+
+/* ---------------------------------------------------------------------------
  * Learned-model rANS for solved blocks: stream format version 3.  No
  * reference counterpart; it replaces the per-block static table of format 2
  * (arithmetic_encode, pentago/shard/arithmetic.cc:366-401) by a 3-layer MLP

@@ -122,6 +122,10 @@ SIGNATURES = {
     "pg_node_symbols": (_I, [_P, _I64, _I, _P, _P]),
     "pg_symbols_nodes": (_I, [_P, _I64, _I, _P, _P]),
     "pg_pack_streams": (_I, [_P, _P, _P, _I, _P, _P, _P]),
+    "pg_store_bound": (_I64, [_I64]),
+    "pg_store_table": (_I, [_P, _P, _P, _I, _I, _P, _P]),
+    "pg_store_encode": (_I, [_P, _P, _P, _I, _I, _P, _P, _P, _P, _P]),
+    "pg_store_decode": (_I, [_P, _P, _P, _P, _P, _I, _I, _P, _P, _P, _P]),
     "pg_learned_model_bytes": (_I64, []),
     "pg_rans_learned_bound": (_I64, [_I64]),
     "pg_rans_learned_encode": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _P]),

@@ -1,0 +1,309 @@
+// Store coder: how the sweep keeps finished slices compressed in HBM.  No
+// reference counterpart (the reference compresses blocks in memory with
+// snappy, pentago/end/fast_compress.cc); this is an internal format that
+// never leaves the device, so only its round trip is specified.
+//
+// A block of solved nodes is coded as the ternary symbols black wins + 2
+// white wins of its 256 rotations per node (the on-disk convention), with
+// static rANS (14-bit frequencies, byte renormalization at 2^23) whose
+// frequencies depend on a context of five already-coded symbols: the same
+// node one step back along each of the four rotation axes (3 where the
+// coordinate is 0) and the same rotation of the previous node of the lane.
+// One frequency table (1024 contexts x 3) serves a whole batch of blocks.
+// A block's 8 lanes each take a contiguous run of its nodes, so every context
+// symbol is on the lane that codes the symbol and the lanes decode in
+// parallel.  Stream layout: 8 lane lengths (u32), then the lanes' bytes.
+#include "../../include/pentago_b200.h"
+#include "runtime.h"
+#include <cstdint>
+
+namespace pg {
+namespace {
+
+constexpr int kCtx = 1024;
+constexpr int kLanesS = 8;
+constexpr uint32_t kTotBits = 14, kTot = 1u << kTotBits, kLow = 1u << 23;
+constexpr int kHead = 4 * kLanesS;
+constexpr int kGroups = 16;  // streams per CTA of the coder kernels
+
+// Nodes per lane of a block of n nodes.
+__host__ __device__ inline int lane_nodes(int n) { return (n + kLanesS - 1) / kLanesS; }
+__host__ __device__ inline int64_t lane_cap(int n) { return int64_t(lane_nodes(n)) * 256 * 2 + 64; }
+__host__ __device__ inline int64_t store_bound(int n) { return kHead + kLanesS * lane_cap(n); }
+
+// Symbols of one node packed 2 bits each (16 per word, rotation r at bits
+// 2 (r & 15) of word r >> 4): black bit + 2 white bit, for the side-to-move
+// form [win, win or tie] of the sweep.
+__device__ __forceinline__ uint32_t spread16(uint32_t x) {
+  x &= 0xffffu;
+  x = (x | x << 8) & 0x00ff00ffu;
+  x = (x | x << 4) & 0x0f0f0f0fu;
+  x = (x | x << 2) & 0x33333333u;
+  return (x | x << 1) & 0x55555555u;
+}
+__device__ __forceinline__ uint32_t gather16(uint32_t x) {
+  x &= 0x55555555u;
+  x = (x | x >> 1) & 0x33333333u;
+  x = (x | x >> 2) & 0x0f0f0f0fu;
+  x = (x | x >> 4) & 0x00ff00ffu;
+  return (x | x >> 8) & 0xffffu;
+}
+__device__ __forceinline__ void pack_node(const uint64_t* node, int turn, uint32_t* sym) {
+#pragma unroll
+  for (int w = 0; w < 4; w++) {
+    const uint64_t win = node[w], nl = node[4 + w];
+    const uint64_t black = turn ? ~nl : win, white = turn ? win : ~nl;
+#pragma unroll
+    for (int h = 0; h < 4; h++)
+      sym[4 * w + h] = spread16(uint32_t(black >> (16 * h))) | spread16(uint32_t(white >> (16 * h))) << 1;
+  }
+}
+__device__ __forceinline__ int sym_at(const uint32_t* sym, int r) { return int(sym[r >> 4] >> (2 * (r & 15)) & 3); }
+
+__device__ __forceinline__ int context(const uint32_t* cur, const uint32_t* prev, int r) {
+  int c = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) c = 4 * c + ((r >> (2 * q) & 3) ? sym_at(cur, r - (1 << (2 * q))) : 3);
+  return 4 * c + (prev ? sym_at(prev, r) : 3);
+}
+
+// Context counts over a batch of blocks: one CTA per block, thread r takes
+// rotation r of every node in lane order.
+__global__ void __launch_bounds__(256)
+store_hist_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restrict__ first,
+                  const int32_t* __restrict__ count, int turn, unsigned* __restrict__ hist) {
+  __shared__ unsigned h[kCtx * 3];
+  __shared__ uint32_t cur[16], prev[16];
+  for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x) h[i] = 0;
+  const int b = blockIdx.x, n = count[b], m = lane_nodes(n), r = threadIdx.x;
+  const uint64_t* base = nodes + 8 * first[b];
+  __syncthreads();
+  for (int k = 0; k < n; k++) {
+    if (r < 16) {
+      const uint64_t* node = base + 8 * int64_t(k);
+      const int w = r >> 2, hq = r & 3;
+      const uint64_t win = node[w], nl = node[4 + w];
+      const uint64_t black = turn ? ~nl : win, white = turn ? win : ~nl;
+      cur[r] = spread16(uint32_t(black >> (16 * hq))) | spread16(uint32_t(white >> (16 * hq))) << 1;
+    }
+    __syncthreads();
+    const int c = context(cur, k % m ? prev : nullptr, r);
+    atomicAdd(&h[3 * c + sym_at(cur, r)], 1u);
+    __syncthreads();
+    if (r < 16) prev[r] = cur[r];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x)
+    if (h[i]) atomicAdd(hist + i, h[i]);
+}
+
+// Frequencies per context from its counts: proportional, at least 1, the
+// rounding left on the largest (uniform when the context never occurs).
+__global__ void store_table_kernel(const unsigned* __restrict__ hist, uint16_t* __restrict__ freq) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= kCtx) return;
+  const uint64_t n[3] = {hist[3 * c], hist[3 * c + 1], hist[3 * c + 2]};
+  const uint64_t sum = n[0] + n[1] + n[2];
+  uint32_t f[3];
+  if (!sum) {
+    f[0] = kTot - 2 * (kTot / 3);
+    f[1] = f[2] = kTot / 3;
+  } else {
+    for (int i = 0; i < 3; i++) {
+      f[i] = uint32_t(n[i] * kTot / sum);
+      if (!f[i]) f[i] = 1;
+    }
+    const int big = f[1] > f[0] ? (f[2] > f[1] ? 2 : 1) : (f[2] > f[0] ? 2 : 0);
+    f[big] = uint32_t(int32_t(f[big]) + int32_t(kTot) - int32_t(f[0] + f[1] + f[2]));
+  }
+  for (int i = 0; i < 3; i++) freq[3 * c + i] = uint16_t(f[i]);
+}
+
+// Encode: one 8-lane group per block; lane l codes its run of nodes backward,
+// each node's rotations from 255 to 0, into its own slot, then the lanes are
+// packed behind the header.
+__global__ void __launch_bounds__(kGroups * kLanesS)
+store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restrict__ first,
+                    const int32_t* __restrict__ count, int nblocks, int turn, const uint16_t* __restrict__ freq,
+                    uint8_t* __restrict__ out, const int64_t* __restrict__ out_offsets, int64_t* __restrict__ sizes) {
+  __shared__ uint16_t F[kCtx * 3];
+  __shared__ uint32_t buf[kGroups * kLanesS][2][16];
+  for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x) F[i] = freq[i];
+  __syncthreads();
+  const int g = threadIdx.x / kLanesS, lane = threadIdx.x % kLanesS;
+  const int b = blockIdx.x * kGroups + g;
+  if (b >= nblocks) return;
+  const unsigned gmask = 0xffu << (threadIdx.x & 24);
+  const int n = count[b], m = lane_nodes(n);
+  const int k0 = lane * m, k1 = min(n, k0 + m);
+  const uint64_t* base = nodes + 8 * first[b];
+  uint8_t* sbase = out + out_offsets[b];
+  const int64_t cap = lane_cap(n);
+  uint8_t* slot_end = sbase + kHead + (lane + 1) * cap;
+  uint8_t* p = slot_end;
+  uint32_t state = kLow;
+  uint32_t* cur = buf[threadIdx.x][0];
+  uint32_t* prev = buf[threadIdx.x][1];
+  if (k1 > k0) pack_node(base + 8 * int64_t(k1 - 1), turn, cur);
+  for (int k = k1 - 1; k >= k0; k--) {
+    const bool has_prev = k > k0;
+    if (has_prev) pack_node(base + 8 * int64_t(k - 1), turn, prev);
+    for (int r = 255; r >= 0; r--) {
+      const int s = sym_at(cur, r);
+      const int c = context(cur, has_prev ? prev : nullptr, r);
+      const uint32_t f = F[3 * c + s];
+      const uint32_t cum = s == 0 ? 0u : s == 1 ? F[3 * c] : uint32_t(F[3 * c]) + F[3 * c + 1];
+      const uint32_t xmax = ((kLow >> kTotBits) << 8) * f;
+      while (state >= xmax) { *--p = uint8_t(state); state >>= 8; }
+      state = ((state / f) << kTotBits) + state % f + cum;
+    }
+    uint32_t* t = cur; cur = prev; prev = t;
+  }
+  for (int j = 0; j < 4; j++) *--p = uint8_t(state >> (8 * j));
+  const uint32_t len = uint32_t(slot_end - p);
+  uint32_t lens[kLanesS];
+  for (int l = 0; l < kLanesS; l++) lens[l] = __shfl_sync(gmask, len, l, kLanesS);
+  int64_t dst = kHead;
+  for (int l = 0; l < lane; l++) dst += lens[l];
+  // lane l's bytes move left, never past a lane not yet moved
+  for (int l = 0; l < kLanesS; l++) {
+    __syncwarp(gmask);
+    if (l == lane)
+      for (uint32_t i = 0; i < len; i++) sbase[dst + i] = p[i];
+  }
+  __syncwarp(gmask);
+  if (lane == 0) {
+    int64_t total = kHead;
+    for (int l = 0; l < kLanesS; l++) {
+      for (int j = 0; j < 4; j++) sbase[4 * l + j] = uint8_t(lens[l] >> (8 * j));
+      total += lens[l];
+    }
+    sizes[b] = total;
+  }
+}
+
+// Decode: lane l decodes its nodes forward into shared memory, one node at a
+// time, and writes each finished node (64 bytes) to its place.  status[b] =
+// nodes decoded, or PG_ERR_FORMAT for a stream that does not end exactly
+// where its lengths say with the initial state.
+__global__ void __launch_bounds__(kGroups * kLanesS)
+store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ in_offsets,
+                    const int64_t* __restrict__ in_sizes, const int32_t* __restrict__ count,
+                    const int64_t* __restrict__ dst, int nblocks, int turn, const uint16_t* __restrict__ freq,
+                    uint64_t* __restrict__ nodes, int64_t* __restrict__ status) {
+  __shared__ uint16_t F[kCtx * 3];
+  __shared__ uint32_t buf[kGroups * kLanesS][2][16];
+  for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x) F[i] = freq[i];
+  __syncthreads();
+  const int g = threadIdx.x / kLanesS, lane = threadIdx.x % kLanesS;
+  const int b = blockIdx.x * kGroups + g;
+  if (b >= nblocks) return;
+  const unsigned gmask = 0xffu << (threadIdx.x & 24);
+  const int n = count[b], m = lane_nodes(n);
+  const int k0 = lane * m, k1 = min(n, k0 + m);
+  const uint8_t* sbase = in + in_offsets[b];
+  const int64_t size = in_sizes[b];
+  int bad = size < kHead;
+  uint64_t start = 0, total = 0;
+  uint32_t mylen = 0;
+  if (!bad) {
+    for (int l = 0; l < kLanesS; l++) {
+      uint32_t v = 0;
+      for (int j = 0; j < 4; j++) v |= uint32_t(sbase[4 * l + j]) << (8 * j);
+      if (l < lane) start += v;
+      if (l == lane) mylen = v;
+      total += v;
+    }
+    bad = total != uint64_t(size - kHead);
+  }
+  const uint8_t* p = sbase + kHead + start;
+  const uint8_t* end = p + (bad ? 0 : mylen);
+  uint32_t state = 0;
+  for (int j = 0; j < 4 && p < end; j++) state = (state << 8) | *p++;
+  uint32_t* cur = buf[threadIdx.x][0];
+  uint32_t* prev = buf[threadIdx.x][1];
+  uint64_t* outp = nodes + 8 * dst[b];
+  for (int k = k0; k < k1 && !bad; k++) {
+    const bool has_prev = k > k0;
+    for (int i = 0; i < 16; i++) cur[i] = 0;
+    for (int r = 0; r < 256; r++) {
+      const int c = context(cur, has_prev ? prev : nullptr, r);
+      const uint32_t f0 = F[3 * c], f1 = F[3 * c + 1];
+      const uint32_t slot = state & (kTot - 1);
+      const int s = slot < f0 ? 0 : slot < f0 + f1 ? 1 : 2;
+      const uint32_t f = s == 0 ? f0 : s == 1 ? f1 : F[3 * c + 2];
+      const uint32_t cum = s == 0 ? 0u : s == 1 ? f0 : f0 + f1;
+      state = f * (state >> kTotBits) + slot - cum;
+      while (state < kLow && p < end) state = (state << 8) | *p++;
+      cur[r >> 4] |= uint32_t(s) << (2 * (r & 15));
+    }
+    uint64_t* o = outp + 8 * int64_t(k);
+    for (int w = 0; w < 4; w++) {
+      uint64_t black = 0, white = 0;
+      for (int h = 0; h < 4; h++) {
+        const uint32_t x = cur[4 * w + h];
+        black |= uint64_t(gather16(x)) << (16 * h);
+        white |= uint64_t(gather16(x >> 1)) << (16 * h);
+      }
+      o[w] = turn ? white : black;
+      o[4 + w] = ~(turn ? black : white);
+    }
+    uint32_t* t = cur; cur = prev; prev = t;
+  }
+  if (!bad) bad = p != end || state != kLow;
+  bad = __any_sync(gmask, bad);
+  if (lane == 0) status[b] = bad ? PG_ERR_FORMAT : n;
+}
+
+int blocks_grid(int nblocks) { return (nblocks + kGroups - 1) / kGroups; }
+
+}  // namespace
+}  // namespace pg
+
+using namespace pg;
+
+extern "C" int64_t pg_store_bound(int64_t nodes) {
+  if (nodes < 0 || nodes > 8 * 8 * 8 * 8 * 64) return fail(PG_ERR_ARG, "bad node count");
+  return store_bound(int(nodes));
+}
+
+extern "C" int pg_store_table(const uint64_t* nodes, const int64_t* first, const int32_t* count, int nblocks, int turn,
+                              uint16_t* table, void* stream_) {
+  if (nblocks < 0 || !table || (nblocks && (!nodes || !first || !count))) return fail(PG_ERR_ARG, "bad store arguments");
+  cudaStream_t stream = (cudaStream_t)stream_;
+  stream_scratch scratch(stream);
+  unsigned* hist = nullptr;
+  PG_CUDA(scratch.alloc(&hist, sizeof(unsigned) * kCtx * 3));
+  PG_CUDA(cudaMemsetAsync(hist, 0, sizeof(unsigned) * kCtx * 3, stream));
+  if (nblocks) {
+    store_hist_kernel<<<nblocks, 256, 0, stream>>>(nodes, first, count, turn & 1, hist);
+    PG_CUDA(cudaGetLastError());
+  }
+  store_table_kernel<<<kCtx / 256, 256, 0, stream>>>(hist, table);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}
+
+extern "C" int pg_store_encode(const uint64_t* nodes, const int64_t* first, const int32_t* count, int nblocks, int turn,
+                               const uint16_t* table, uint8_t* out, const int64_t* out_offsets, int64_t* sizes,
+                               void* stream) {
+  if (nblocks < 0 || (nblocks && (!nodes || !first || !count || !table || !out || !out_offsets || !sizes)))
+    return fail(PG_ERR_ARG, "bad store arguments");
+  if (!nblocks) return PG_OK;
+  store_encode_kernel<<<blocks_grid(nblocks), kGroups * kLanesS, 0, (cudaStream_t)stream>>>(
+      nodes, first, count, nblocks, turn & 1, table, out, out_offsets, sizes);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}
+
+extern "C" int pg_store_decode(const uint8_t* in, const int64_t* in_offsets, const int64_t* in_sizes,
+                               const int32_t* count, const int64_t* dst, int nblocks, int turn, const uint16_t* table,
+                               uint64_t* nodes, int64_t* status, void* stream) {
+  if (nblocks < 0 || (nblocks && (!in || !in_offsets || !in_sizes || !count || !dst || !table || !nodes || !status)))
+    return fail(PG_ERR_ARG, "bad store arguments");
+  if (!nblocks) return PG_OK;
+  store_decode_kernel<<<blocks_grid(nblocks), kGroups * kLanesS, 0, (cudaStream_t)stream>>>(
+      in, in_offsets, in_sizes, count, dst, nblocks, turn & 1, table, nodes, status);
+  PG_CUDA(cudaGetLastError());
+  return PG_OK;
+}

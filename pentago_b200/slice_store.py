@@ -2,15 +2,16 @@
 
 The role of the reference's in-memory block compression
 (pentago/end/fast_compress.cc, compacting_store.cc) for the GPU sweep: every
-8^4 block of a slice becomes one format-2 rANS stream (the reference's own
-coder, byte-identical, on the GPU) of its 256 symbols per node, and a child
+8^4 block of a slice is coded by the library's store coder (pg_store_*: rANS
+with a 1024-context model of each rotation's neighbours, one frequency table
+per chunk of blocks, coded from and decoded to nodes on the GPU), and a child
 section is decompressed into a staging buffer only while the lines that read
 it run (pg_end_sweep_slice_child).  A slice then costs its coded size while
 the slice below it is built.
 """
 import numpy as np
 
-from . import capi, rans
+from . import capi
 from .end import section_shape
 
 
@@ -31,18 +32,29 @@ def slice_blocks(sigs):
     return np.concatenate(sec), np.concatenate(first), np.concatenate(count), np.array(sec_first), base
 
 
+def store_bound(count):
+    """pg_store_bound for an array of block node counts: a 32-byte header and
+    8 lanes of ceil(count / 8) nodes at 2 bytes per symbol, plus 64 each."""
+    count = np.asarray(count, np.int64)
+    return 32 + 8 * ((count + 7) // 8 * 512 + 64)
+
+
 class compressed_slice:
     """A slice tensor (end-engine nodes, sections `sigs` in slice layout) as
-    one format-2 stream per block, coded in chunks of at most chunk_nodes
-    nodes and packed back to back per chunk."""
+    one store-coder stream per block, in chunks of at most chunk_nodes nodes
+    (one frequency table and one packed byte buffer per chunk)."""
 
     def __init__(self, nodes, sigs, turn, chunk_nodes=1 << 24, stream=None):
         import torch
+        L = capi.lib()
+        sh = capi.stream_handle(stream)
         self.sigs = np.ascontiguousarray(sigs, dtype=np.uint64)
         self.turn = turn
         self.sec, self.first, self.count, self.sec_first, self.base = slice_blocks(self.sigs)
         self.raw_bytes = 64 * int(self.base[-1])
-        self.chunks = []   # (first block, last block + 1, device bytes, packed stream offsets, sizes)
+        self.chunks = []   # (first block, last block + 1, table, device bytes, packed offsets, sizes)
+        dev = nodes.device
+        t64 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64)).to(dev)
         nb = len(self.first)
         b0 = 0
         while b0 < nb:
@@ -50,45 +62,52 @@ class compressed_slice:
             while b1 < nb and (b1 == b0 or used + self.count[b1] <= chunk_nodes):
                 used += int(self.count[b1])
                 b1 += 1
-            n0 = int(self.first[b0])
-            sym = rans.node_symbols(nodes[n0:n0 + used], turn, stream)
-            sym_off = np.zeros(b1 - b0 + 1, np.int64)
-            sym_off[1:] = 256 * np.cumsum(self.count[b0:b1])
-            out, out_off, sz = rans.encode_device(sym, sym_off, stream)
-            del sym
+            k = b1 - b0
+            first = t64(self.first[b0:b1])
+            count = torch.from_numpy(self.count[b0:b1].astype(np.int32)).to(dev)
+            table = torch.empty(1024 * 3, dtype=torch.int16, device=dev)
+            capi.check(L.pg_store_table(nodes.data_ptr(), first.data_ptr(), count.data_ptr(), k, turn,
+                                        table.data_ptr(), sh))
+            caps = (store_bound(self.count[b0:b1]) + 15) // 16 * 16
+            out_off = np.zeros(k + 1, np.int64)
+            out_off[1:] = np.cumsum(caps)
+            out = torch.empty(int(out_off[-1]), dtype=torch.uint8, device=dev)
+            d_off = t64(out_off[:-1])
+            sizes = torch.zeros(k, dtype=torch.int64, device=dev)
+            capi.check(L.pg_store_encode(nodes.data_ptr(), first.data_ptr(), count.data_ptr(), k, turn,
+                                         table.data_ptr(), out.data_ptr(), d_off.data_ptr(), sizes.data_ptr(), sh))
+            sz = sizes.cpu().numpy()
             # the coder leaves room for its worst case after every stream: pack them
-            dev = out.device
-            packed = np.zeros(len(sz) + 1, np.int64)
+            packed = np.zeros(k + 1, np.int64)
             packed[1:] = np.cumsum(sz)
             data = torch.empty(max(int(packed[-1]), 1), dtype=torch.uint8, device=dev)
-            t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64)).to(dev)
-            d_in, d_sz, d_out = t(out_off[:-1]), t(sz), t(packed[:-1])
-            capi.check(capi.lib().pg_pack_streams(out.data_ptr(), d_in.data_ptr(), d_sz.data_ptr(), len(sz),
-                                                  data.data_ptr(), d_out.data_ptr(), capi.stream_handle(stream)))
+            d_packed = t64(packed[:-1])
+            capi.check(L.pg_pack_streams(out.data_ptr(), d_off.data_ptr(), sizes.data_ptr(), k, data.data_ptr(),
+                                         d_packed.data_ptr(), sh))
             del out
-            self.chunks.append((b0, b1, data, packed, sz.astype(np.int64)))
+            self.chunks.append((b0, b1, table, data, packed, sz.astype(np.int64)))
             b0 = b1
-        self.bytes = sum(int(c[2].numel()) for c in self.chunks)
+        self.bytes = sum(int(c[3].numel()) + 2 * 1024 * 3 for c in self.chunks)
 
     def section_nodes(self, i, stream=None):
         """Section i's nodes (block-major), decompressed on the GPU."""
         import torch
+        L = capi.lib()
         lo, hi = int(self.sec_first[i]), int(self.sec_first[i + 1])
         n_base = int(self.base[i])
         out = torch.empty((int(self.base[i + 1]) - n_base, 8), dtype=torch.int64, device="cuda")
-        for b0, b1, data, packed, sz in self.chunks:
+        t64 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64)).to(out.device)
+        for b0, b1, table, data, packed, sz in self.chunks:
             a, b = max(lo, b0), min(hi, b1)
             if a >= b:
                 continue
             k0, k1 = a - b0, b - b0
-            sym_off = np.zeros(k1 - k0 + 1, np.int64)
-            sym_off[1:] = 256 * np.cumsum(self.count[a:b])
-            sym, status = rans.decode_device(data, packed[k0:k1 + 1], sz[k0:k1], sym_off, stream)
-            if (status != 256 * self.count[a:b]).any():
+            count = torch.from_numpy(self.count[a:b].astype(np.int32)).to(out.device)
+            status = torch.zeros(k1 - k0, dtype=torch.int64, device=out.device)
+            d_in, d_sz, d_dst = t64(packed[k0:k1]), t64(sz[k0:k1]), t64(self.first[a:b] - n_base)
+            capi.check(L.pg_store_decode(data.data_ptr(), d_in.data_ptr(), d_sz.data_ptr(), count.data_ptr(),
+                                         d_dst.data_ptr(), k1 - k0, self.turn, table.data_ptr(), out.data_ptr(),
+                                         status.data_ptr(), capi.stream_handle(stream)))
+            if (status.cpu().numpy() != self.count[a:b]).any():
                 raise capi.PentagoError(capi.PG_ERR_FORMAT, "a compressed block did not decode")
-            n0 = int(self.first[a]) - n_base
-            n = int(self.count[a:b].sum())
-            capi.check(capi.lib().pg_symbols_nodes(sym.data_ptr(), n, self.turn, out[n0:n0 + n].data_ptr(),
-                                                   capi.stream_handle(stream)))
-            del sym
         return out

@@ -66,7 +66,7 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
     slice-N.pentago (the reference's slice file format).  resume: a slice
     file (slice N, holding at least the sections the root needs at N) to
     start from instead of solving slices 35..N again.  compress: keep each
-    finished slice in HBM as format-2 streams (slice_store.compressed_slice)
+    finished slice in HBM as store-coder streams (slice_store.compressed_slice)
     and decompress one child section at a time while the slice below is
     built, for roots whose two largest adjacent slices do not fit raw.
 

@@ -1,5 +1,7 @@
-"""Slices kept compressed in HBM: symbols back to nodes, a solved slice
-through the per-block format-2 store and back, and a sweep that keeps every
+"""Slices kept compressed in HBM: symbols back to nodes, the store coder's
+round trip on ragged blocks of random nodes and its refusal of damaged
+streams, a solved slice through the per-block store and back, and a sweep
+that keeps every
 finished slice compressed, computing each slice one child section at a time,
 with the same counts and the same last slice as the plain sweep."""
 import numpy as np
@@ -25,6 +27,56 @@ def test_symbols_to_nodes_inverts_node_symbols(cuda):
         assert torch.equal(back, nodes)
 
 
+def test_store_coder_roundtrip_and_damage(cuda):
+    import torch
+    from pentago_b200 import capi
+    from pentago_b200.slice_store import store_bound
+    L = capi.lib()
+    counts = np.array([1, 7, 8, 9, 100, 4096, 4095, 512], np.int32)
+    assert [L.pg_store_bound(int(c)) for c in counts] == store_bound(counts).tolist()
+    first = np.concatenate([[0], np.cumsum(counts)[:-1]]).astype(np.int64)
+    n = int(counts.sum())
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    r = lambda: torch.randint(-2**63, 2**63 - 1, (n, 4), dtype=torch.int64, device="cuda", generator=g)
+    x = r()
+    win = x & r() & r()             # skewed, so the contexts matter
+    nodes = torch.cat([win, win | (x & r())], 1).contiguous()
+    t = lambda a, dt=np.int64: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).cuda()
+    d_first, d_count = t(first), t(counts, np.int32)
+    for turn in (0, 1):
+        table = torch.empty(3072, dtype=torch.int16, device="cuda")
+        capi.check(L.pg_store_table(nodes.data_ptr(), d_first.data_ptr(), d_count.data_ptr(), len(counts), turn,
+                                    table.data_ptr(), None))
+        f = table.cpu().numpy().view(np.uint16).reshape(1024, 3).astype(np.int64)
+        assert (f >= 1).all() and (f.sum(1) == 1 << 14).all()
+        caps = store_bound(counts)
+        off = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+        out = torch.zeros(int(caps.sum()), dtype=torch.uint8, device="cuda")
+        sizes = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
+        d_off = t(off)
+        capi.check(L.pg_store_encode(nodes.data_ptr(), d_first.data_ptr(), d_count.data_ptr(), len(counts), turn,
+                                     table.data_ptr(), out.data_ptr(), d_off.data_ptr(), sizes.data_ptr(), None))
+        sz = sizes.cpu().numpy()
+        assert (sz > 32).all() and (sz <= caps).all()
+
+        def decode(data, sizes_):
+            back = torch.zeros_like(nodes)
+            status = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
+            capi.check(L.pg_store_decode(data.data_ptr(), d_off.data_ptr(), t(sizes_).data_ptr(), d_count.data_ptr(),
+                                         d_first.data_ptr(), len(counts), turn, table.data_ptr(), back.data_ptr(),
+                                         status.data_ptr(), None))
+            return back, status.cpu().numpy()
+        back, status = decode(out, sz)
+        assert status.tolist() == counts.tolist() and torch.equal(back, nodes)
+        bad = out.clone()
+        bad[int(off[5]) + 40 + int(sz[5]) // 2] ^= 0x5A   # the middle of the 4096-node block
+        _, status = decode(bad, sz)
+        assert status[5] == capi.PG_ERR_FORMAT and status[4] == counts[4]
+        _, status = decode(out, sz - 1)                    # every stream one byte short
+        assert (status == capi.PG_ERR_FORMAT).all()
+
+
 def test_compressed_slice_roundtrip(cuda):
     import torch
     from pentago_b200 import sweep
@@ -32,7 +84,7 @@ def test_compressed_slice_roundtrip(cuda):
     from pentago_b200.slice_store import compressed_slice
     _, nodes, sigs = sweep.sweep(section_sig(ROOT), min_slice=34, keep_last=True)
     store = compressed_slice(nodes, sigs, 34 & 1, chunk_nodes=1 << 20)
-    assert len(store.chunks) > 1 and store.bytes < store.raw_bytes / 1.3
+    assert len(store.chunks) > 1 and store.bytes < store.raw_bytes / 2.5
     for i in range(len(sigs)):
         assert torch.equal(store.section_nodes(i), nodes[int(store.base[i]):int(store.base[i + 1])])
 
@@ -49,4 +101,4 @@ def test_compressed_sweep_matches_plain(cuda):
     for s in plain:
         assert np.array_equal(plain[s], packed[s]), s
     assert torch.equal(last, last2)
-    assert all(timings[s]["compressed_bytes"] < timings[s]["raw_bytes"] / 1.3 for s in (35, 34))
+    assert all(timings[s]["compressed_bytes"] < timings[s]["raw_bytes"] / 2.5 for s in (35, 34))
