@@ -12,7 +12,10 @@
 // One frequency table (1024 contexts x 3) serves a whole batch of blocks.
 // A block's 8 lanes each take a contiguous run of its nodes, so every context
 // symbol is on the lane that codes the symbol and the lanes decode in
-// parallel.  Stream layout: 8 lane lengths (u32), then the lanes' bytes.
+// parallel.  Stream layout: 8 lane lengths (u32), then the lanes' bytes; a
+// block that some lane cannot code within its nodes' raw size is stored raw
+// instead (first length ~0, then the 64-byte nodes), so a stream never
+// needs more than its raw size plus 32 + 8 x 64 bytes.
 #include "../../include/pentago_b200.h"
 #include "runtime.h"
 #include <cstdint>
@@ -28,8 +31,9 @@ constexpr int kGroups = 16;  // streams per CTA of the coder kernels
 
 // Nodes per lane of a block of n nodes.
 __host__ __device__ inline int lane_nodes(int n) { return (n + kLanesS - 1) / kLanesS; }
-__host__ __device__ inline int64_t lane_cap(int n) { return int64_t(lane_nodes(n)) * 256 * 2 + 64; }
+__host__ __device__ inline int64_t lane_cap(int n) { return int64_t(lane_nodes(n)) * 64 + 64; }
 __host__ __device__ inline int64_t store_bound(int n) { return kHead + kLanesS * lane_cap(n); }
+constexpr uint32_t kRawBlock = ~0u;
 
 // Symbols of one node packed 2 bits each (16 per word, rotation r at bits
 // 2 (r & 15) of word r >> 4): black bit + 2 white bit, for the side-to-move
@@ -139,13 +143,15 @@ store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restric
   const uint64_t* base = nodes + 8 * first[b];
   uint8_t* sbase = out + out_offsets[b];
   const int64_t cap = lane_cap(n);
-  uint8_t* slot_end = sbase + kHead + (lane + 1) * cap;
+  uint8_t* slot_begin = sbase + kHead + lane * cap;
+  uint8_t* slot_end = slot_begin + cap;
   uint8_t* p = slot_end;
   uint32_t state = kLow;
+  int over = 0;
   uint32_t* cur = buf[threadIdx.x][0];
   uint32_t* prev = buf[threadIdx.x][1];
   if (k1 > k0) pack_node(base + 8 * int64_t(k1 - 1), turn, cur);
-  for (int k = k1 - 1; k >= k0; k--) {
+  for (int k = k1 - 1; k >= k0 && !over; k--) {
     const bool has_prev = k > k0;
     if (has_prev) pack_node(base + 8 * int64_t(k - 1), turn, prev);
     for (int r = 255; r >= 0; r--) {
@@ -154,10 +160,28 @@ store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restric
       const uint32_t f = F[3 * c + s];
       const uint32_t cum = s == 0 ? 0u : s == 1 ? F[3 * c] : uint32_t(F[3 * c]) + F[3 * c + 1];
       const uint32_t xmax = ((kLow >> kTotBits) << 8) * f;
-      while (state >= xmax) { *--p = uint8_t(state); state >>= 8; }
+      while (state >= xmax) {
+        if (p - slot_begin <= 4) { over = 1; break; }   // keep room for the final state
+        *--p = uint8_t(state);
+        state >>= 8;
+      }
+      if (over) break;
       state = ((state / f) << kTotBits) + state % f + cum;
     }
     uint32_t* t = cur; cur = prev; prev = t;
+  }
+  if (__any_sync(gmask, over)) {
+    // some lane would pass its nodes' raw size: store the block raw
+    __syncwarp(gmask);
+    const int64_t words = 8 * int64_t(n);
+    for (int64_t i = lane; i < words; i += kLanesS)
+      reinterpret_cast<uint64_t*>(sbase + kHead)[i] = base[i];
+    if (lane == 0) {
+      for (int j = 0; j < 4; j++) sbase[j] = 0xff;
+      for (int j = 4; j < kHead; j++) sbase[j] = 0;
+      sizes[b] = kHead + 8 * words;
+    }
+    return;
   }
   for (int j = 0; j < 4; j++) *--p = uint8_t(state >> (8 * j));
   const uint32_t len = uint32_t(slot_end - p);
@@ -206,6 +230,24 @@ store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ 
   int bad = size < kHead;
   uint64_t start = 0, total = 0;
   uint32_t mylen = 0;
+  if (!bad && (sbase[0] & sbase[1] & sbase[2] & sbase[3]) == 0xff) {
+    // a block stored raw
+    const int64_t words = 8 * int64_t(n);
+    const int ok = size == kHead + 8 * words;
+    const uint8_t* src = sbase + kHead;
+    uint64_t* o = nodes + 8 * dst[b];
+    if (ok && !(reinterpret_cast<uintptr_t>(src) & 7)) {
+      for (int64_t i = lane; i < words; i += kLanesS) o[i] = reinterpret_cast<const uint64_t*>(src)[i];
+    } else if (ok) {
+      for (int64_t i = lane; i < words; i += kLanesS) {
+        uint64_t v = 0;
+        for (int j = 0; j < 8; j++) v |= uint64_t(src[8 * i + j]) << (8 * j);
+        o[i] = v;
+      }
+    }
+    if (lane == 0) status[b] = ok ? n : PG_ERR_FORMAT;
+    return;
+  }
   if (!bad) {
     for (int l = 0; l < kLanesS; l++) {
       uint32_t v = 0;

@@ -34,9 +34,9 @@ def slice_blocks(sigs):
 
 def store_bound(count):
     """pg_store_bound for an array of block node counts: a 32-byte header and
-    8 lanes of ceil(count / 8) nodes at 2 bytes per symbol, plus 64 each."""
+    8 lanes of the raw size of ceil(count / 8) nodes plus 64 bytes each."""
     count = np.asarray(count, np.int64)
-    return 32 + 8 * ((count + 7) // 8 * 512 + 64)
+    return 32 + 8 * ((count + 7) // 8 * 64 + 64)
 
 
 class compressed_slice:
@@ -44,29 +44,39 @@ class compressed_slice:
     one store-coder stream per block, in chunks of at most chunk_nodes nodes
     (one frequency table and one packed byte buffer per chunk)."""
 
-    def __init__(self, nodes, sigs, turn, chunk_nodes=1 << 24, stream=None):
-        import torch
-        L = capi.lib()
-        sh = capi.stream_handle(stream)
+    def __init__(self, nodes, sigs, turn, chunk_nodes=1 << 26, stream=None):
+        """Code a whole slice tensor (nodes None: start empty and add sections)."""
         self.sigs = np.ascontiguousarray(sigs, dtype=np.uint64)
         self.turn = turn
+        self.chunk_nodes = chunk_nodes
         self.sec, self.first, self.count, self.sec_first, self.base = slice_blocks(self.sigs)
         self.raw_bytes = 64 * int(self.base[-1])
         self.chunks = []   # (first block, last block + 1, table, device bytes, packed offsets, sizes)
+        self.bytes = 0
+        if nodes is not None:
+            for i in range(len(self.sigs)):
+                self.add_section(i, nodes[int(self.base[i]):int(self.base[i + 1])], stream)
+
+    def add_section(self, i, nodes, stream=None):
+        """Code section i from its nodes (block-major, the section alone)."""
+        import torch
+        L = capi.lib()
+        sh = capi.stream_handle(stream)
         dev = nodes.device
         t64 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64)).to(dev)
-        nb = len(self.first)
-        b0 = 0
-        while b0 < nb:
+        lo, hi = int(self.sec_first[i]), int(self.sec_first[i + 1])
+        n_base = int(self.base[i])
+        b0 = lo
+        while b0 < hi:
             b1, used = b0, 0
-            while b1 < nb and (b1 == b0 or used + self.count[b1] <= chunk_nodes):
+            while b1 < hi and (b1 == b0 or used + self.count[b1] <= self.chunk_nodes):
                 used += int(self.count[b1])
                 b1 += 1
             k = b1 - b0
-            first = t64(self.first[b0:b1])
+            first = t64(self.first[b0:b1] - n_base)
             count = torch.from_numpy(self.count[b0:b1].astype(np.int32)).to(dev)
             table = torch.empty(1024 * 3, dtype=torch.int16, device=dev)
-            capi.check(L.pg_store_table(nodes.data_ptr(), first.data_ptr(), count.data_ptr(), k, turn,
+            capi.check(L.pg_store_table(nodes.data_ptr(), first.data_ptr(), count.data_ptr(), k, self.turn,
                                         table.data_ptr(), sh))
             caps = (store_bound(self.count[b0:b1]) + 15) // 16 * 16
             out_off = np.zeros(k + 1, np.int64)
@@ -74,20 +84,21 @@ class compressed_slice:
             out = torch.empty(int(out_off[-1]), dtype=torch.uint8, device=dev)
             d_off = t64(out_off[:-1])
             sizes = torch.zeros(k, dtype=torch.int64, device=dev)
-            capi.check(L.pg_store_encode(nodes.data_ptr(), first.data_ptr(), count.data_ptr(), k, turn,
+            capi.check(L.pg_store_encode(nodes.data_ptr(), first.data_ptr(), count.data_ptr(), k, self.turn,
                                          table.data_ptr(), out.data_ptr(), d_off.data_ptr(), sizes.data_ptr(), sh))
             sz = sizes.cpu().numpy()
-            # the coder leaves room for its worst case after every stream: pack them
+            # the coder leaves room for its worst case after every stream: pack
+            # them, each starting on a 16-byte boundary
             packed = np.zeros(k + 1, np.int64)
-            packed[1:] = np.cumsum(sz)
+            packed[1:] = np.cumsum((sz + 15) // 16 * 16)
             data = torch.empty(max(int(packed[-1]), 1), dtype=torch.uint8, device=dev)
             d_packed = t64(packed[:-1])
             capi.check(L.pg_pack_streams(out.data_ptr(), d_off.data_ptr(), sizes.data_ptr(), k, data.data_ptr(),
                                          d_packed.data_ptr(), sh))
             del out
             self.chunks.append((b0, b1, table, data, packed, sz.astype(np.int64)))
+            self.bytes += int(data.numel()) + 2 * 1024 * 3
             b0 = b1
-        self.bytes = sum(int(c[3].numel()) + 2 * 1024 * 3 for c in self.chunks)
 
     def section_nodes(self, i, stream=None):
         """Section i's nodes (block-major), decompressed on the GPU."""

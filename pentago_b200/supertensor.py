@@ -289,6 +289,30 @@ def write_slice(path, slice_, sigs, nodes, level=6, threads=0, stream=None):
     w.close()
 
 
+class slice_writer:
+    """A slice file written one section at a time (the same file write_slice
+    makes): write_section(i, nodes of section i alone), then finalize()."""
+
+    def __init__(self, path, slice_, sigs, level=6, threads=0):
+        self.sigs = np.ascontiguousarray(sigs, dtype=np.uint64)
+        self.turn = slice_ & 1
+        self.threads = threads
+        self._w = _Writer(path, self.sigs, True, 8, 1, level)
+
+    def write_section(self, i, nodes, stream=None):
+        idx, off = section_block_offsets(section_shape(int(self.sigs[i])))
+        secs = np.full(len(idx), i, np.int32)
+        blocks = np.ascontiguousarray(idx, dtype=np.uint8)
+        offs = np.ascontiguousarray(off, dtype=np.int64)
+        capi.check(capi.lib().pg_supertensor_write_blocks(self._w.handle, len(secs), capi.ptr(secs), capi.ptr(blocks),
+                                                          nodes.data_ptr(), capi.ptr(offs), self.turn, self.threads,
+                                                          capi.stream_handle(stream)))
+
+    def finalize(self):
+        capi.check(capi.lib().pg_supertensor_finalize(self._w.handle, -1))
+        self._w.close()
+
+
 def read_slice(path, sigs=None, threads=0, stream=None):
     """Read sections of a slice file into a slice tensor (end-engine node
     form).  sigs: the sections wanted (default: all in the file), sorted.

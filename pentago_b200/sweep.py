@@ -58,6 +58,94 @@ def _slice_of(path):
     return supertensor_slice(path)
 
 
+def _child_of(sig, dim):
+    """The standardized child section of a section along quadrant dim (the
+    mover places a stone there), or None when that quadrant is full."""
+    c = [[(int(sig) >> (16 * q + 8 * k)) & 255 for k in range(2)] for q in range(4)]
+    if c[dim][0] + c[dim][1] >= 9:
+        return None
+    c[dim][sum(map(sum, c)) & 1] += 1
+    std = ctypes.c_uint64()
+    t = ctypes.c_int32()
+    capi.check(capi.lib().pg_section_standardize(ctypes.c_uint64(section_sig(c)), ctypes.byref(std), ctypes.byref(t)))
+    return int(std.value)
+
+
+def _compressed_slice_step(root, slice_, sigs, off, child, last, checkpoint, level, stream, t0, t1, timings,
+                           cache_fraction=0.0):
+    """One slice of a compressed sweep, one parent section at a time: the
+    section's lines read the (at most four) child sections it needs, decoded
+    from the coded child slice one at a time (cache_fraction of the free
+    memory may keep decoded sections for later parents), then the
+    section is counted, written to the checkpoint, and coded into the new
+    slice before the next one is built.  The last slice stays raw.
+    Returns (counts rows, coded slice or None, raw slice or None)."""
+    import collections
+    import time as _time
+    import torch
+    from .slice_store import compressed_slice
+    L = capi.lib()
+    s_handle = capi.stream_handle(stream)
+    store = None if last else compressed_slice(None, sigs, slice_ & 1)
+    raw = torch.empty((int(off[-1]), 8), dtype=torch.int64, device="cuda") if last else None
+    writer = None
+    if checkpoint is not None:
+        from .supertensor import slice_writer
+        writer = slice_writer(os.path.join(checkpoint, f"slice-{slice_}.pentago"), slice_, sigs, level)
+    counts = np.zeros((len(sigs), 3), np.uint64)
+    cache = collections.OrderedDict()
+    budget = int(torch.cuda.mem_get_info()[0] * cache_fraction)
+    child_index = {int(s): i for i, s in enumerate(child.sigs)} if child is not None else {}
+    decode_s = code_s = 0.0
+    t0.record()
+    for i, psig in enumerate(sigs):
+        n = int(off[i + 1] - off[i])
+        pbuf = raw[int(off[i]):int(off[i + 1])] if last else torch.empty((n, 8), dtype=torch.int64, device="cuda")
+        one = np.array([psig], np.uint64)
+        if child is None:
+            capi.check(L.pg_end_sweep_slice(capi.ptr(one), 1, pbuf.data_ptr(), None, 0, None, s_handle))
+        else:
+            pbuf.zero_()
+            for csig in sorted({c for c in (_child_of(psig, d) for d in range(4)) if c is not None}):
+                if csig not in cache:
+                    ci = child_index[csig]
+                    need = 64 * int(child.base[ci + 1] - child.base[ci])
+                    # room first: decoded sections this section has used are done
+                    while cache and sum(64 * v.shape[0] for v in cache.values()) + need > budget:
+                        cache.popitem(last=False)
+                    e = _time.perf_counter()
+                    cache[csig] = child.section_nodes(ci, stream)
+                    decode_s += _time.perf_counter() - e
+                cache.move_to_end(csig)
+                capi.check(L.pg_end_sweep_slice_child(capi.ptr(one), 1, pbuf.data_ptr(), ctypes.c_uint64(csig),
+                                                      cache[csig].data_ptr(), s_handle))
+            while cache and sum(64 * v.shape[0] for v in cache.values()) > budget:
+                cache.popitem(last=False)
+        cnt = torch.zeros((1, 3), dtype=torch.int64, device="cuda")
+        capi.check(L.pg_section_counts(capi.ptr(one), 1, pbuf.data_ptr(), cnt.data_ptr(), s_handle))
+        counts[i] = cnt.cpu().numpy().view(np.uint64)[0]
+        if writer is not None:
+            writer.write_section(i, pbuf, stream)
+        if store is not None:
+            e = _time.perf_counter()
+            store.add_section(i, pbuf, stream)
+            code_s += _time.perf_counter() - e
+        del pbuf
+    t1.record()
+    if writer is not None:
+        writer.finalize()
+    del cache
+    torch.cuda.empty_cache()
+    if timings is not None:
+        torch.cuda.synchronize()
+        timings[slice_] = {"ms": t0.elapsed_time(t1), "sections": len(sigs), "nodes": int(off[-1]),
+                           "child_nodes": int(child.base[-1]) if child is not None else 0,
+                           "decode_s": decode_s, "code_s": code_s}
+        if store is not None:
+            timings[slice_].update({"compressed_bytes": store.bytes, "raw_bytes": store.raw_bytes})
+    return to_golden(sigs, counts, slice_), store, raw
+
+
 def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, checkpoint=None, resume=None, level=6,
           compress=False):
     """Solve all sections below `root` from slice 35 down to `min_slice`.
@@ -97,23 +185,18 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
         off = slice_layout(sigs)
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
-        if isinstance(child, compressed_slice):
-            # every line reads one child section: decompress them one by one
-            parent = torch.zeros((int(off[-1]), 8), dtype=torch.int64, device="cuda")
-            t0.record()
-            for ci, csig in enumerate(child.sigs):
-                staging = child.section_nodes(ci, stream)
-                capi.check(L.pg_end_sweep_slice_child(capi.ptr(sigs), len(sigs), parent.data_ptr(),
-                                                      ctypes.c_uint64(int(csig)), staging.data_ptr(), s_handle))
-                del staging
-            t1.record()
-        else:
-            parent = torch.empty((int(off[-1]), 8), dtype=torch.int64, device="cuda")
-            t0.record()
-            capi.check(L.pg_end_sweep_slice(capi.ptr(sigs), len(sigs), parent.data_ptr(), capi.ptr(child_sigs),
-                                            len(child_sigs), child.data_ptr() if child is not None else None,
-                                            s_handle))
-            t1.record()
+        if compress:
+            results[slice_], child, parent = _compressed_slice_step(
+                root, slice_, sigs, off, child, slice_ == min_slice, checkpoint, level, stream, t0, t1, timings)
+            child_sigs = sigs
+            if parent is not None:
+                child = parent
+            continue
+        parent = torch.empty((int(off[-1]), 8), dtype=torch.int64, device="cuda")
+        t0.record()
+        capi.check(L.pg_end_sweep_slice(capi.ptr(sigs), len(sigs), parent.data_ptr(), capi.ptr(child_sigs),
+                                        len(child_sigs), child.data_ptr() if child is not None else None, s_handle))
+        t1.record()
         counts = torch.zeros((len(sigs), 3), dtype=torch.int64, device="cuda")
         capi.check(L.pg_section_counts(capi.ptr(sigs), len(sigs), parent.data_ptr(), counts.data_ptr(), s_handle))
         c = counts.cpu().numpy().view(np.uint64)
@@ -125,22 +208,10 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
         if timings is not None:
             torch.cuda.synchronize()
             timings[slice_] = {"ms": t0.elapsed_time(t1), "sections": len(sigs), "nodes": int(off[-1]),
-                               "child_nodes": 0 if child is None else
-                               int(child.base[-1]) if isinstance(child, compressed_slice) else int(child.shape[0])}
+                               "child_nodes": int(child.shape[0]) if child is not None else 0}
         del child
         torch.cuda.empty_cache()  # the slice above is gone; its HBM must be reusable at 180 GB scale
-        if compress and slice_ > min_slice:
-            e0 = time.perf_counter()
-            child = compressed_slice(parent, sigs, slice_ & 1, stream=stream)
-            del parent
-            torch.cuda.empty_cache()
-            if timings is not None:
-                torch.cuda.synchronize()
-                timings[slice_].update({"compress_s": time.perf_counter() - e0, "compressed_bytes": child.bytes,
-                                        "raw_bytes": child.raw_bytes})
-        else:
-            child = parent
-        child_sigs = sigs
+        child, child_sigs = parent, sigs
     if keep_last:
         return results, child, child_sigs
     return results

@@ -69,6 +69,22 @@ def test_store_coder_roundtrip_and_damage(cuda):
             return back, status.cpu().numpy()
         back, status = decode(out, sz)
         assert status.tolist() == counts.tolist() and torch.equal(back, nodes)
+        # blocks that no lane can code within their raw size are stored raw
+        noise = torch.randint(-2**63, 2**63 - 1, (n, 8), dtype=torch.int64, device="cuda", generator=g)
+        noisy = torch.cat([noise[:, :4] & noise[:, 4:], noise[:, :4] | noise[:, 4:]], 1).contiguous()
+        raw_sizes = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
+        raw_out = torch.zeros_like(out)
+        capi.check(L.pg_store_encode(noisy.data_ptr(), d_first.data_ptr(), d_count.data_ptr(), len(counts), turn,
+                                     table.data_ptr(), raw_out.data_ptr(), d_off.data_ptr(), raw_sizes.data_ptr(),
+                                     None))
+        rs = raw_sizes.cpu().numpy()
+        assert (rs <= caps).all() and (rs == 32 + 64 * counts.astype(np.int64)).any()
+        back = torch.zeros_like(noisy)
+        status = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
+        capi.check(L.pg_store_decode(raw_out.data_ptr(), d_off.data_ptr(), t(rs).data_ptr(), d_count.data_ptr(),
+                                     d_first.data_ptr(), len(counts), turn, table.data_ptr(), back.data_ptr(),
+                                     status.data_ptr(), None))
+        assert status.cpu().numpy().tolist() == counts.tolist() and torch.equal(back, noisy)
         bad = out.clone()
         bad[int(off[5]) + 40 + int(sz[5]) // 2] ^= 0x5A   # the middle of the 4096-node block
         _, status = decode(bad, sz)
@@ -89,16 +105,20 @@ def test_compressed_slice_roundtrip(cuda):
         assert torch.equal(store.section_nodes(i), nodes[int(store.base[i]):int(store.base[i + 1])])
 
 
-def test_compressed_sweep_matches_plain(cuda):
+def test_compressed_sweep_matches_plain(cuda, tmp_path):
     import torch
-    from pentago_b200 import sweep
+    from pentago_b200 import supertensor, sweep
     from pentago_b200.end import section_sig
     root = section_sig(ROOT)
     plain, last, _ = sweep.sweep(root, keep_last=True)
     timings = {}
-    packed, last2, _ = sweep.sweep(root, keep_last=True, compress=True, timings=timings)
+    packed, last2, _ = sweep.sweep(root, keep_last=True, compress=True, timings=timings, checkpoint=str(tmp_path),
+                                   level=1)
     assert sorted(plain) == sorted(packed)
     for s in plain:
         assert np.array_equal(plain[s], packed[s]), s
     assert torch.equal(last, last2)
     assert all(timings[s]["compressed_bytes"] < timings[s]["raw_bytes"] / 2.5 for s in (35, 34))
+    # the section-by-section checkpoint holds the same slice
+    _, _, back = supertensor.read_slice(str(tmp_path / "slice-33.pentago"))
+    assert torch.equal(back, last)
