@@ -492,31 +492,37 @@ def main():
     value = units_all / (elapsed_ms / 1e3)
 
     # End-to-end through the public API with host buffers.  The lines go in
-    # chunks of four blocks, each chunk's copy in, compute and copy out on its
-    # own stream, so that the two copy directions and the kernels overlap.
-    chunk = 16
+    # chunks of one block (its four lines) through a three-stage pipeline: one
+    # stream copies every chunk in, one runs the chunks' plans as their inputs
+    # land, one copies every chunk's results out, so that both copy directions
+    # run back to back and the kernels hide between them.
+    chunk = 4
     chunks = [list(range(c, min(c + chunk, len(ls)))) for c in range(0, len(ls), chunk)]
     chunk_plans = [end.Plan([ls[i] for i in c]) for c in chunks]
-    streams = [torch.cuda.Stream(device=dev) for _ in range(3)]
+    h2d, comp, d2h = (torch.cuda.Stream(device=dev) for _ in range(3))
 
     def e2e_step():
         go = torch.cuda.Event()
         go.record(stream)
-        done = []
-        for k, (c, p) in enumerate(zip(chunks, chunk_plans)):
-            st = streams[k % len(streams)]
+        for st in (h2d, comp, d2h):
             st.wait_event(go)
-            with torch.cuda.stream(st):
+        for c, p in zip(chunks, chunk_plans):
+            with torch.cuda.stream(h2d):
                 for i in c:
                     ls[i].input.copy_(host_in[i], non_blocking=True)
-                p.run(st)
+            landed = torch.cuda.Event()
+            landed.record(h2d)
+            comp.wait_event(landed)
+            p.run(comp)
+            solved = torch.cuda.Event()
+            solved.record(comp)
+            d2h.wait_event(solved)
+            with torch.cuda.stream(d2h):
                 for i in c:
                     host_out[i].copy_(ls[i].output, non_blocking=True)
-            ev = torch.cuda.Event()
-            ev.record(st)
-            done.append(ev)
-        for ev in done:
-            stream.wait_event(ev)
+        done = torch.cuda.Event()
+        done.record(d2h)
+        stream.wait_event(done)
         stream.synchronize()
 
     for _ in range(max(1, args.warmup)):

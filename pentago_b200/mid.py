@@ -174,7 +174,8 @@ def positions(raw):
 
 def bench_config0(steps=20, warmup=3):
     """Config 0: 64 seeded 26-stone boards (13 black, 13 white, no five);
-    GPU time per batch from CUDA events.  Returns the result and the boards."""
+    GPU time per batch from CUDA events (median of three trials).  Returns
+    the result and the boards."""
     import torch
     raws = random_boards(0, 64, 26)
     pos = sum(positions(r) for r in raws)
@@ -183,13 +184,17 @@ def bench_config0(steps=20, warmup=3):
     for _ in range(warmup):
         values_device(raws, out=out, scratch=scratch)
     torch.cuda.synchronize()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record()
-    for _ in range(steps):
-        values_device(raws, out=out, scratch=scratch)
-    b.record()
-    torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / steps
+    # three trials of `steps` batches each; the median trial is reported
+    trials = []
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            values_device(raws, out=out, scratch=scratch)
+        b.record()
+        torch.cuda.synchronize()
+        trials.append(a.elapsed_time(b) / steps)
+    ms = sorted(trials)[1]
     result = {"workload": "64 seeded 26-stone boards (13 black, 13 white, no five), full midsolve",
               "positions_per_batch": pos, "ms_per_batch": ms, "value": pos / (ms / 1e3),
               "boards_per_s": len(raws) / (ms / 1e3), "unit": "positions/s"}
