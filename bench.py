@@ -328,6 +328,8 @@ def sweep_summary(timings, wall_s):
     sections = sum(v["sections"] for v in timings.values())
     return {"workload": f"all sections below root {CONFIG2_ROOT}, slices 35 -> 30, in HBM",
             "sections": sections, "nodes": sum(v["nodes"] for v in timings.values()), "kernel_ms": ms,
+            "arena_ms": sum(v.get("arena_ms", 0.0) for v in timings.values()),
+            "arena_GB": max(v.get("arena_GB", 0.0) for v in timings.values()),
             "wall_s": wall_s, "sections_per_s": sections / (ms / 1e3),
             "algorithmic_GBps": nbytes / (ms / 1e3) / 1e9}
 

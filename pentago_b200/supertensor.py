@@ -313,10 +313,11 @@ class slice_writer:
         self._w.close()
 
 
-def read_slice(path, sigs=None, threads=0, stream=None):
+def read_slice(path, sigs=None, threads=0, stream=None, out=None):
     """Read sections of a slice file into a slice tensor (end-engine node
     form).  sigs: the sections wanted (default: all in the file), sorted.
-    Returns (slice, sigs, tensor)."""
+    out: a contiguous (nodes, 8) int64 device tensor to read into (default:
+    a new one).  Returns (slice, sigs, tensor)."""
     import torch
     f = _File(path)
     headers = [supertensor_header_t(f.header(s)) for s in range(f.sections)]
@@ -333,7 +334,11 @@ def read_slice(path, sigs=None, threads=0, stream=None):
     slice_ = stones.pop()
     secs, blocks, offs, total = _slice_blocks(sigs)
     file_secs = np.array([where[int(sigs[i])] for i in secs], np.int32)
-    out = torch.empty((total, 8), dtype=torch.int64, device="cuda")
+    if out is None:
+        out = torch.empty((total, 8), dtype=torch.int64, device="cuda")
+    elif (tuple(out.shape) != (total, 8) or out.dtype != torch.int64 or not out.is_cuda
+          or not out.is_contiguous()):
+        raise ValueError(f"out must be a contiguous ({total}, 8) int64 device tensor")
     capi.check(capi.lib().pg_supertensor_read_blocks(f.handle, len(file_secs), capi.ptr(file_secs),
                                                      capi.ptr(blocks), out.data_ptr(), capi.ptr(offs), slice_ & 1,
                                                      threads, capi.stream_handle(stream)))

@@ -2,8 +2,9 @@
 
 The GPU form of the reference's slice loop (pentago/mpi/toplevel.cc:337-415):
 for each slice from 35 down to the root's, compute every block line of every
-section into one slice tensor (pg_end_sweep_slice), count wins per section
-(pg_section_counts), then free the slice above.  Per-section counts are
+section into one slice tensor (pg_end_sweep_slice) and count wins per section
+(pg_section_counts).  The slices take turns at the two ends of one device
+arena, so only two adjacent slices are ever held.  Per-section counts are
 returned in the format of data/counts-N.npy (mpi/io.cc:573-581):
 [sig, black wins, white wins, total] over distinct positions.
 
@@ -146,6 +147,13 @@ def _compressed_slice_step(root, slice_, sigs, off, child, last, checkpoint, lev
     return to_golden(sigs, counts, slice_), store, raw
 
 
+def _arena_nodes(root, chain):
+    """Nodes of the sweep arena for the slices `chain` (top first): the most
+    that two adjacent slices hold together."""
+    nodes = [int(slice_layout(descendent_sections(root, s))[-1]) for s in chain]
+    return max([a + b for a, b in zip(nodes, nodes[1:])] + nodes + [1])
+
+
 def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, checkpoint=None, resume=None, level=6,
           compress=False):
     """Solve all sections below `root` from slice 35 down to `min_slice`.
@@ -158,9 +166,19 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
     and decompress one child section at a time while the slice below is
     built, for roots whose two largest adjacent slices do not fit raw.
 
-    Returns {slice: counts-N rows}; with keep_last also the last slice tensor."""
+    Without compress every slice lives in one device arena sized for the two
+    largest adjacent slices: slices alternate between its front and its back,
+    so a slice never overlaps the one above it, and nothing is allocated or
+    freed while the slices are solved.  (Fresh device memory is cleared by the
+    driver before its first use; with an allocation per slice that clearing
+    landed inside the kernels of every slice, at up to several times their
+    time.)  The arena is allocated and zeroed once before the first slice;
+    timings of the first slice carry that time as "arena_ms".
+
+    Returns {slice: counts-N rows}; with keep_last also the last slice tensor
+    and its sections (without compress, the tensor is a view of the arena,
+    which stays allocated while the caller holds it)."""
     import torch
-    from .slice_store import compressed_slice
     root = int(root)
     if min_slice is None:
         min_slice = sum(sum(c) for c in [[(root >> (16 * q + 8 * k)) & 255 for k in range(2)] for q in range(4)])
@@ -170,16 +188,43 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
     child = None   # the slice above: a raw tensor, or compressed
     results = {}
     top = 35
+    start = None
+    if resume is not None:
+        start = _slice_of(resume)
+        top = start - 1
+    order = list(range(top, min_slice - 1, -1))
+    arena = None
+    arena_ms = None
+    if not compress:
+        chain = ([start] if start is not None else []) + order
+        nodes = _arena_nodes(root, chain)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        arena = torch.empty((nodes, 8), dtype=torch.int64, device="cuda")
+        arena.zero_()
+        e1.record()
+        torch.cuda.synchronize()
+        arena_ms = e0.elapsed_time(e1)
+    k = 0  # slices placed so far: even ones at the arena's front, odd ones at its back
+
+    def place(n):
+        nonlocal k
+        view = arena[:n] if k % 2 == 0 else arena[arena.shape[0] - n:]
+        k += 1
+        return view
+
     if resume is not None:
         from .supertensor import read_slice
-        start = _slice_of(resume)
         child_sigs = descendent_sections(root, start)
-        _, child_sigs, child = read_slice(resume, child_sigs, stream=stream)
         if compress:
+            from .slice_store import compressed_slice
+            _, child_sigs, child = read_slice(resume, child_sigs, stream=stream)
             child = compressed_slice(child, child_sigs, start & 1, stream=stream)
             torch.cuda.empty_cache()
-        top = start - 1
-    for slice_ in range(top, min_slice - 1, -1):
+        else:
+            out = place(int(slice_layout(child_sigs)[-1]))
+            _, child_sigs, child = read_slice(resume, child_sigs, stream=stream, out=out)
+    for slice_ in order:
         sigs = descendent_sections(root, slice_)
         torch.cuda.synchronize()
         off = slice_layout(sigs)
@@ -192,7 +237,7 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
             if parent is not None:
                 child = parent
             continue
-        parent = torch.empty((int(off[-1]), 8), dtype=torch.int64, device="cuda")
+        parent = place(int(off[-1]))
         t0.record()
         capi.check(L.pg_end_sweep_slice(capi.ptr(sigs), len(sigs), parent.data_ptr(), capi.ptr(child_sigs),
                                         len(child_sigs), child.data_ptr() if child is not None else None, s_handle))
@@ -209,9 +254,11 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
             torch.cuda.synchronize()
             timings[slice_] = {"ms": t0.elapsed_time(t1), "sections": len(sigs), "nodes": int(off[-1]),
                                "child_nodes": int(child.shape[0]) if child is not None else 0}
-        del child
-        torch.cuda.empty_cache()  # the slice above is gone; its HBM must be reusable at 180 GB scale
+            if arena_ms is not None and slice_ == order[0]:
+                timings[slice_]["arena_ms"] = arena_ms
+                timings[slice_]["arena_GB"] = 64 * arena.shape[0] / 1e9
         child, child_sigs = parent, sigs
+    del arena
     if keep_last:
         return results, child, child_sigs
     return results
@@ -248,6 +295,7 @@ def main():
     total_ms = sum(v["ms"] for v in timings.values())
     nbytes = sum(64 * (v["nodes"] + v["child_nodes"]) for v in timings.values())
     print(json.dumps({"root": args.root, "slices": {str(k): v for k, v in timings.items()}, "kernel_ms": total_ms,
+                      "arena_ms": sum(v.get("arena_ms", 0.0) for v in timings.values()),
                       "wall_s": wall, "sections": sum(v["sections"] for v in timings.values()),
                       "sections_per_s": sum(v["sections"] for v in timings.values()) / (total_ms / 1e3),
                       "algorithmic_GBps": nbytes / (total_ms / 1e3) / 1e9, "golden_counts_match": ok,
