@@ -3,7 +3,7 @@
 The GPU form of the reference's slice loop (pentago/mpi/toplevel.cc:337-415):
 for each slice from 35 down to the root's, compute every block line of every
 section into one slice tensor (pg_end_sweep_slice) and count wins per section
-(pg_section_counts).  The slices take turns at the two ends of one device
+(pg_section_counts).  The slices take turns in the two halves of one device
 arena, so only two adjacent slices are ever held.  Per-section counts are
 returned in the format of data/counts-N.npy (mpi/io.cc:573-581):
 [sig, black wins, white wins, total] over distinct positions.
@@ -148,10 +148,11 @@ def _compressed_slice_step(root, slice_, sigs, off, child, last, checkpoint, lev
 
 
 def _arena_nodes(root, chain):
-    """Nodes of the sweep arena for the slices `chain` (top first): the most
-    that two adjacent slices hold together."""
+    """Nodes of the two halves of the sweep arena for the slices `chain`
+    (top first): slices take turns between the halves, so each half holds
+    the largest slice of its turns."""
     nodes = [int(slice_layout(descendent_sections(root, s))[-1]) for s in chain]
-    return max([a + b for a, b in zip(nodes, nodes[1:])] + nodes + [1])
+    return max(nodes[0::2] + [1]), max(nodes[1::2] + [1])
 
 
 def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, checkpoint=None, resume=None, level=6,
@@ -166,18 +167,20 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
     and decompress one child section at a time while the slice below is
     built, for roots whose two largest adjacent slices do not fit raw.
 
-    Without compress every slice lives in one device arena sized for the two
-    largest adjacent slices: slices alternate between its front and its back,
-    so a slice never overlaps the one above it, and nothing is allocated or
-    freed while the slices are solved.  (Fresh device memory is cleared by the
-    driver before its first use; with an allocation per slice that clearing
-    landed inside the kernels of every slice, at up to several times their
-    time.)  The arena is allocated and zeroed once before the first slice;
-    timings of the first slice carry that time as "arena_ms".
+    Without compress the slices live in a device arena of two halves that
+    they take turns in, so a slice never overlaps the one above it and
+    nothing is allocated or freed while the slices are solved.  (Fresh device
+    memory is cleared by the driver before its first use; with an allocation
+    per slice that clearing landed inside the kernels of every slice, at up
+    to several times their time.)  Slice sizes rise and then fall along a
+    sweep, so the halves together hold what the two largest adjacent slices
+    need.  The arena is allocated and zeroed once before the first slice
+    (timings of the first slice carry that time as "arena_ms"); at the end the
+    half without the last slice is released.
 
     Returns {slice: counts-N rows}; with keep_last also the last slice tensor
-    and its sections (without compress, the tensor is a view of the arena,
-    which stays allocated while the caller holds it)."""
+    and its sections (without compress, the tensor is a view of its arena
+    half, which stays allocated while the caller holds it)."""
     import torch
     root = int(root)
     if min_slice is None:
@@ -193,23 +196,23 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
         start = _slice_of(resume)
         top = start - 1
     order = list(range(top, min_slice - 1, -1))
-    arena = None
+    halves = None
     arena_ms = None
     if not compress:
         chain = ([start] if start is not None else []) + order
-        nodes = _arena_nodes(root, chain)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        arena = torch.empty((nodes, 8), dtype=torch.int64, device="cuda")
-        arena.zero_()
+        halves = [torch.empty((n, 8), dtype=torch.int64, device="cuda") for n in _arena_nodes(root, chain)]
+        for h in halves:
+            h.zero_()
         e1.record()
         torch.cuda.synchronize()
         arena_ms = e0.elapsed_time(e1)
-    k = 0  # slices placed so far: even ones at the arena's front, odd ones at its back
+    k = 0  # slices placed so far: even ones in the first half, odd ones in the second
 
     def place(n):
         nonlocal k
-        view = arena[:n] if k % 2 == 0 else arena[arena.shape[0] - n:]
+        view = halves[k % 2][:n]
         k += 1
         return view
 
@@ -222,8 +225,8 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
             child = compressed_slice(child, child_sigs, start & 1, stream=stream)
             torch.cuda.empty_cache()
         else:
-            out = place(int(slice_layout(child_sigs)[-1]))
-            _, child_sigs, child = read_slice(resume, child_sigs, stream=stream, out=out)
+            _, child_sigs, child = read_slice(resume, child_sigs, stream=stream,
+                                              out=place(int(slice_layout(child_sigs)[-1])))
     for slice_ in order:
         sigs = descendent_sections(root, slice_)
         torch.cuda.synchronize()
@@ -256,9 +259,11 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
                                "child_nodes": int(child.shape[0]) if child is not None else 0}
             if arena_ms is not None and slice_ == order[0]:
                 timings[slice_]["arena_ms"] = arena_ms
-                timings[slice_]["arena_GB"] = 64 * arena.shape[0] / 1e9
+                timings[slice_]["arena_GB"] = 64 * sum(h.shape[0] for h in halves) / 1e9
         child, child_sigs = parent, sigs
-    del arena
+    if halves is not None:
+        halves = None
+        torch.cuda.empty_cache()   # the half without the last slice
     if keep_last:
         return results, child, child_sigs
     return results
