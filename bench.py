@@ -436,23 +436,34 @@ def main():
     capi.check(capi.lib().pg_init())
     stream = torch.cuda.current_stream()
 
-    # Buffers: pinned host copies (for the end-to-end leg) and device copies
+    # Buffers: the four lines of one block share one pinned host buffer and
+    # one device buffer per direction (the end-to-end leg moves a block with
+    # one copy in and one copy out); each line reads and writes its own part.
     lines = plan_lines(args.blocks, rank)
-    host_in, host_out, dev_lines = [], [], []
+    chunk = 4
+    blocks = []   # (host in, device in, host out, device out) per block
     in_bytes = out_bytes = 0
     out_nodes = 0
     alg_bytes = 0
-    for line, info, seed in lines:
-        hi = torch.from_numpy(random_nodes(seed, info.input_nodes).view(np.int64)).pin_memory()
-        ho = torch.empty((info.output_nodes, 8), dtype=torch.int64).pin_memory()
-        line.input = hi.to(dev, non_blocking=True)
-        line.output = torch.empty((info.output_nodes, 8), dtype=torch.int64, device=dev)
-        host_in.append(hi)
-        host_out.append(ho)
+    for c in range(0, len(lines), chunk):
+        part = lines[c:c + chunk]
+        hi = torch.from_numpy(np.concatenate([random_nodes(seed, info.input_nodes) for _, info, seed in part])
+                              .view(np.int64)).pin_memory()
+        n_out = sum(info.output_nodes for _, info, _ in part)
+        ho = torch.empty((n_out, 8), dtype=torch.int64).pin_memory()
+        di = hi.to(dev, non_blocking=True)
+        do = torch.empty((n_out, 8), dtype=torch.int64, device=dev)
+        a = b = 0
+        for line, info, _ in part:
+            line.input = di[a:a + info.input_nodes]
+            line.output = do[b:b + info.output_nodes]
+            a += info.input_nodes
+            b += info.output_nodes
+            out_nodes += info.output_nodes
+            alg_bytes += 64 * (info.input_nodes + info.output_nodes)
+        blocks.append((hi, di, ho, do))
         in_bytes += hi.numel() * 8
         out_bytes += ho.numel() * 8
-        out_nodes += info.output_nodes
-        alg_bytes += 64 * (info.input_nodes + info.output_nodes)
     ls = [l for l, _, _ in lines]
     torch.cuda.synchronize()
     plan = end.Plan(ls)
@@ -493,14 +504,12 @@ def main():
     units_all = out_nodes * 256 * args.steps * world
     value = units_all / (elapsed_ms / 1e3)
 
-    # End-to-end through the public API with host buffers.  The lines go in
-    # chunks of one block (its four lines) through a three-stage pipeline: one
-    # stream copies every chunk in, one runs the chunks' plans as their inputs
-    # land, one copies every chunk's results out, so that both copy directions
-    # run back to back and the kernels hide between them.
-    chunk = 4
-    chunks = [list(range(c, min(c + chunk, len(ls)))) for c in range(0, len(ls), chunk)]
-    chunk_plans = [end.Plan([ls[i] for i in c]) for c in chunks]
+    # End-to-end through the public API with host buffers.  The blocks go
+    # through a three-stage pipeline: one stream copies every block in, one
+    # runs each block's plan (its four lines) as its inputs land, one copies
+    # every block's results out, so that both copy directions run back to
+    # back and the kernels hide between them.
+    chunk_plans = [end.Plan(ls[c:c + chunk]) for c in range(0, len(ls), chunk)]
     h2d, comp, d2h = (torch.cuda.Stream(device=dev) for _ in range(3))
 
     def e2e_step():
@@ -508,10 +517,9 @@ def main():
         go.record(stream)
         for st in (h2d, comp, d2h):
             st.wait_event(go)
-        for c, p in zip(chunks, chunk_plans):
+        for (hi, di, ho, do), p in zip(blocks, chunk_plans):
             with torch.cuda.stream(h2d):
-                for i in c:
-                    ls[i].input.copy_(host_in[i], non_blocking=True)
+                di.copy_(hi, non_blocking=True)
             landed = torch.cuda.Event()
             landed.record(h2d)
             comp.wait_event(landed)
@@ -520,8 +528,7 @@ def main():
             solved.record(comp)
             d2h.wait_event(solved)
             with torch.cuda.stream(d2h):
-                for i in c:
-                    host_out[i].copy_(ls[i].output, non_blocking=True)
+                ho.copy_(do, non_blocking=True)
         done = torch.cuda.Event()
         done.record(d2h)
         stream.wait_event(done)
