@@ -90,10 +90,17 @@ int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream);
 
 /* Prepared lines: plan once on the host (line_details_t's work,
  * compute.cc:55-123), run many times.  The plan keeps the lines' buffer
- * pointers; the buffers must outlive it. */
+ * pointers; the buffers must outlive it.  A run launches one kernel per
+ * dimension present.  When no line has PG_LINE_OR and no line's output can
+ * touch a buffer range of a line of another dimension, those launches run on
+ * streams of the plan's own, forked from and joined back into `stream`
+ * (their last waves then overlap); otherwise one after another on `stream`.
+ * A plan is run by one host thread at a time.  pg_end_plan_streams returns
+ * how many streams a run uses (1 when the launches are serial). */
 typedef struct pg_end_plan_s* pg_end_plan_t;
 int pg_end_plan_create(const pg_line_t* lines, int n, pg_end_plan_t* plan);
 int pg_end_plan_run(pg_end_plan_t plan, void* stream);
+int pg_end_plan_streams(pg_end_plan_t plan);
 int pg_end_plan_destroy(pg_end_plan_t plan);
 
 /* Synchronize `stream` and report device-side bounds violations recorded by

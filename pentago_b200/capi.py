@@ -99,6 +99,7 @@ SIGNATURES = {
     "pg_end_check": (_I, [_P]),
     "pg_end_plan_create": (_I, [ctypes.POINTER(pg_line_t), _I, ctypes.POINTER(_P)]),
     "pg_end_plan_run": (_I, [_P, _P]),
+    "pg_end_plan_streams": (_I, [_P]),
     "pg_end_plan_destroy": (_I, [_P]),
     "pg_section_shape": (_I, [_U64, ctypes.POINTER(ctypes.c_int32)]),
     "pg_section_standardize": (_I, [_U64, ctypes.POINTER(_U64), ctypes.POINTER(ctypes.c_int32)]),

@@ -491,6 +491,12 @@ struct end_plan {
   std::vector<parent_rec> recs;
   std::vector<size_t> rec_off[4];       // per planned line: offset into recs
   parent_rec* recs_dev = nullptr;
+  // When the dimensions' lines are independent (dims_independent), the
+  // launches of all but the first dimension run on side streams, forked from
+  // and joined back into the caller's stream.
+  bool concurrent = false;
+  cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
 };
 
 template<int DIM> static int set_smem_attr() {
@@ -579,6 +585,58 @@ static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
 }
 
 // Point every planned line at its records, given their device copy.
+// Byte range [lo, hi) that a line's blocks can touch in one of its buffers:
+// block b at node offset off[b] holds the cross-section's nodes times 8 along
+// the line (fewer in the last block, `last` nodes along the line).
+static void line_span(const void* base, const int64_t* off, int nblocks, int64_t cross, int last,
+                      uintptr_t& lo, uintptr_t& hi) {
+  int64_t a = off[0], b = 0;
+  for (int i = 0; i < nblocks; i++) {
+    a = std::min(a, off[i]);
+    b = std::max(b, off[i] + cross * (i == nblocks - 1 ? last : 8));
+  }
+  lo = reinterpret_cast<uintptr_t>(base) + uintptr_t(a) * 64;
+  hi = reinterpret_cast<uintptr_t>(base) + uintptr_t(b) * 64;
+}
+
+// Whether the launches of different dimensions may run at the same time: no
+// line ORs into its output, and no line's output range meets a range (input
+// or output) of a line of another dimension.  Plans of more than 4096 lines
+// are not checked and run one dimension after another.
+static bool dims_independent(const end_plan& P) {
+  struct span_t { uintptr_t lo, hi; int dim; bool out; };
+  std::vector<span_t> v;
+  for (int d = 0; d < 4; d++)
+    for (const line_dev_t& L : P.host[d]) {
+      if (L.flags & PG_LINE_OR) return false;
+      const int64_t cross = int64_t(L.cross[0]) * L.cross[1] * L.cross[2];
+      span_t s{0, 0, d, true};
+      line_span(L.output, L.out_off, L.length, cross, (L.nparent & 7) ? (L.nparent & 7) : 8, s.lo, s.hi);
+      v.push_back(s);
+      if (!L.slice35) {
+        span_t t{0, 0, d, false};
+        line_span(L.input, L.in_off, L.input_blocks, cross, (L.nchild & 7) ? (L.nchild & 7) : 8, t.lo, t.hi);
+        v.push_back(t);
+      }
+    }
+  if (v.size() > 8192) return false;
+  for (const span_t& a : v) {
+    if (!a.out) continue;
+    for (const span_t& b : v)
+      if (b.dim != a.dim && a.lo < b.hi && b.lo < a.hi) return false;
+  }
+  return true;
+}
+
+static void release_plan(end_plan* P) {
+  for (auto* d : P->dev) if (d) cudaFree(d);
+  if (P->recs_dev) cudaFree(P->recs_dev);
+  for (auto s : P->side) if (s) cudaStreamDestroy(s);
+  for (auto e : P->join) if (e) cudaEventDestroy(e);
+  if (P->fork) cudaEventDestroy(P->fork);
+  delete P;
+}
+
 static void bind_records(end_plan& P, parent_rec* recs_dev) {
   P.recs_dev = recs_dev;
   for (int dim = 0; dim < 4; dim++)
@@ -622,38 +680,76 @@ extern "C" int pg_end_plan_create(const pg_line_t* lines, int n, pg_end_plan_t* 
     if (e != cudaSuccess) { if (recs) cudaFree(recs); delete P; return cuda_fail(e, "pg_end_plan_create"); }
     bind_records(*P, recs);
   }
+  int ndims = 0;
   for (int dim = 0; dim < 4; dim++) {
     if (P->host[dim].empty()) continue;
+    ndims++;
     const size_t bytes = sizeof(line_dev_t) * P->host[dim].size();
     cudaError_t e = cudaMalloc(&P->dev[dim], bytes);
     if (e == cudaSuccess) e = cudaMemcpy(P->dev[dim], P->host[dim].data(), bytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
-      for (auto* d : P->dev) if (d) cudaFree(d);
-      if (P->recs_dev) cudaFree(P->recs_dev);
-      delete P;
+      release_plan(P);
       return cuda_fail(e, "pg_end_plan_create");
     }
+  }
+  if (ndims > 1 && dims_independent(*P)) {
+    cudaError_t e = cudaEventCreateWithFlags(&P->fork, cudaEventDisableTiming);
+    for (int k = 0; k < ndims - 1 && e == cudaSuccess; k++) {
+      e = cudaStreamCreateWithFlags(&P->side[k], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&P->join[k], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+      release_plan(P);
+      return cuda_fail(e, "pg_end_plan_create");
+    }
+    P->concurrent = true;
   }
   *plan = reinterpret_cast<pg_end_plan_t>(P);
   return PG_OK;
 }
 
-extern "C" int pg_end_plan_run(pg_end_plan_t plan, void* stream) {
+extern "C" int pg_end_plan_run(pg_end_plan_t plan, void* stream_) {
   if (!plan) return fail(PG_ERR_ARG, "null plan");
   const dev_tables_t* T = device_tables();
   if (!T) return PG_ERR_CUDA;
   const end_plan& P = *reinterpret_cast<end_plan*>(plan);
-  for (int dim = 0; dim < 4; dim++)
-    if (int rc = launch_group(P, dim, (cudaStream_t)stream, *T)) return rc;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  if (!P.concurrent) {
+    for (int dim = 0; dim < 4; dim++)
+      if (int rc = launch_group(P, dim, stream, *T)) return rc;
+    return PG_OK;
+  }
+  // One launch per dimension, each on its own stream, so that the tail of
+  // one launch's last wave overlaps the next launch instead of idling SMs.
+  PG_CUDA(cudaEventRecord(P.fork, stream));
+  int k = -1;
+  for (int dim = 0; dim < 4; dim++) {
+    if (P.host[dim].empty()) continue;
+    if (k < 0) {
+      if (int rc = launch_group(P, dim, stream, *T)) return rc;
+    } else {
+      PG_CUDA(cudaStreamWaitEvent(P.side[k], P.fork, 0));
+      if (int rc = launch_group(P, dim, P.side[k], *T)) return rc;
+      PG_CUDA(cudaEventRecord(P.join[k], P.side[k]));
+      PG_CUDA(cudaStreamWaitEvent(stream, P.join[k], 0));
+    }
+    k++;
+  }
   return PG_OK;
+}
+
+extern "C" int pg_end_plan_streams(pg_end_plan_t plan) {
+  if (!plan) return fail(PG_ERR_ARG, "null plan");
+  const end_plan& P = *reinterpret_cast<end_plan*>(plan);
+  if (!P.concurrent) return 1;
+  int n = 0;
+  for (int dim = 0; dim < 4; dim++) n += !P.host[dim].empty();
+  return n;
 }
 
 extern "C" int pg_end_plan_destroy(pg_end_plan_t plan) {
   if (!plan) return PG_OK;
-  auto* P = reinterpret_cast<end_plan*>(plan);
-  for (auto* d : P->dev) if (d) cudaFree(d);
-  if (P->recs_dev) cudaFree(P->recs_dev);
-  delete P;
+  release_plan(reinterpret_cast<end_plan*>(plan));
   return PG_OK;
 }
 

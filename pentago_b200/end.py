@@ -140,6 +140,12 @@ class Plan:
     def run(self, stream=None):
         capi.check(capi.lib().pg_end_plan_run(self._h, capi.stream_handle(stream)))
 
+    @property
+    def streams(self):
+        """Streams a run uses: one per dimension when the dimensions' lines
+        are independent, else 1."""
+        return capi.check(capi.lib().pg_end_plan_streams(self._h))
+
     def close(self):
         if self._h:
             capi.lib().pg_end_plan_destroy(self._h)

@@ -134,6 +134,7 @@ def test_prepared_plan_runs_repeatedly(cuda):
         lines.append(line)
         want.append(case["output_sha1"])
     plan = end.Plan(lines)
+    assert plan.streams == 4   # four dimensions, every line its own output
     for _ in range(2):
         for l in lines:
             l.output.zero_()
@@ -141,3 +142,52 @@ def test_prepared_plan_runs_repeatedly(cuda):
         end.check_errors()
         assert [sha1(to_host(l.output)) for l in lines] == want
     plan.close()
+
+
+def test_plan_streams_follow_line_independence(cuda):
+    """The four lines through one block of a 30-stone section, writing
+    disjoint parts of one buffer, run on four streams and give what one call
+    per line gives; lines that OR into their outputs, or whose outputs
+    overlap, run on one stream."""
+    import torch
+    from pentago_b200 import capi, end
+    from pentago_b200.synthetic import random_nodes
+    sig = end.section_sig([[4, 4], [4, 4], [4, 3], [3, 4]])
+    lines, infos = [], []
+    for dim in range(4):
+        line = end.Line(sig, dim, (0, 0, 0))
+        info = end.line_info(line)
+        line.input = to_dev(random_nodes(10 + dim, info.input_nodes))
+        lines.append(line)
+        infos.append(info)
+    total = sum(i.output_nodes for i in infos)
+    shared = torch.full((total, 8), -1, dtype=torch.int64, device=cuda)
+    o = 0
+    for line, info in zip(lines, infos):
+        line.output = shared[o:o + info.output_nodes]
+        o += info.output_nodes
+    plan = end.Plan(lines)
+    assert plan.streams == 4
+    plan.run()
+    end.check_errors()
+    got = shared.clone()
+    o = 0
+    for line, info in zip(lines, infos):
+        alone = torch.zeros((info.output_nodes, 8), dtype=torch.int64, device=cuda)
+        single = end.Line(sig, line.dimension, line.block_base)
+        single.input, single.output = line.input, alone
+        end.compute_lines([single])
+        assert torch.equal(got[o:o + info.output_nodes], alone), line.dimension
+        o += info.output_nodes
+    plan.close()
+    # OR into the outputs: one stream
+    for line in lines:
+        line.flags = capi.PG_LINE_OR
+    assert end.Plan(lines).streams == 1
+    # outputs of two dimensions that overlap: one stream
+    for line in lines:
+        line.flags = capi.PG_LINE_STORE
+    lines[1].output = shared[8:8 + infos[1].output_nodes]
+    assert end.Plan(lines).streams == 1
+    # one dimension only: one stream
+    assert end.Plan(lines[:1]).streams == 1
