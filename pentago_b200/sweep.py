@@ -200,9 +200,15 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
     arena_ms = None
     if not compress:
         chain = ([start] if start is not None else []) + order
+        sizes = _arena_nodes(root, chain)
+        need = 64 * sum(sizes)
+        free = torch.cuda.mem_get_info()[0] + torch.cuda.memory_reserved() - torch.cuda.memory_allocated()
+        if need > free:
+            raise capi.PentagoError(capi.PG_ERR_CAPACITY, f"the sweep holds two adjacent slices raw, {need / 1e9:.1f} GB, "
+                                    f"and the device has {free / 1e9:.1f} GB free; sweep with compress=True")
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        halves = [torch.empty((n, 8), dtype=torch.int64, device="cuda") for n in _arena_nodes(root, chain)]
+        halves = [torch.empty((n, 8), dtype=torch.int64, device="cuda") for n in sizes]
         for h in halves:
             h.zero_()
         e1.record()
@@ -273,7 +279,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--root", default="4,4,4,5,4,3,3,3")
     ap.add_argument("--min-slice", type=int, default=None)
-    ap.add_argument("--golden", default=None, help="npz of counts_N arrays to compare against")
+    ap.add_argument("--golden", nargs="+", default=None, help="npz files of counts_N arrays to compare against")
     ap.add_argument("--checkpoint", default=None, help="directory for slice-N.pentago files of every solved slice")
     ap.add_argument("--resume", default=None, help="slice file to start from")
     ap.add_argument("--level", type=int, default=6, help="compression level of checkpoint files (zlib 1-9, xz 20-29)")
@@ -292,7 +298,9 @@ def main():
     wall = time.perf_counter() - t
     ok = None
     if args.golden:
-        g = np.load(args.golden)
+        g = {}
+        for path in args.golden:
+            g.update(dict(np.load(path)))
         ok = True
         for s, rows in res.items():
             gold = {int(r[0]): r for r in g[f"counts_{s}"]}

@@ -24,6 +24,9 @@ Fixtures written:
   shards.json        pentago/shard/sharder_test.cc's server-verified (board, value)
                      samples of shard 7 of 32 over slices 0..5, and the per-slice
                      entry counts listed in pentago/shard/shard_permute.h
+  counts_28_29.npz   the rows of data/counts-{28,29}.npy for the sections of the
+                     28-stone root DEEP_ROOT at slices 28 and 29 (with
+                     counts_30_35.npz, every section of its sweep)
 """
 import ctypes
 import json
@@ -49,6 +52,24 @@ LINE_CASES = [([[4, 4], [4, 5], [4, 3], [4, 4]], 2, (1, 0, 1)),
               ([[5, 4], [4, 5], [5, 4], [4, 4]], 3, (0, 0, 0)),
               ([[4, 4], [4, 4], [4, 3], [3, 4]], 0, (1, 1, 1)),
               ([[4, 4], [4, 4], [4, 3], [3, 4]], 3, (1, 1, 1))]
+
+
+# A 28-stone root whose two largest adjacent slices (31 and 30: 105.4 + 99.5 GB)
+# do not fit a B200's HBM raw; its sweep needs slices kept compressed.
+DEEP_ROOT = [[4, 4], [4, 5], [4, 3], [2, 2]]
+
+
+def deep_root_counts(ref_root):
+    from pentago_b200.end import section_sig
+    from pentago_b200.sweep import descendent_sections
+    out = {}
+    for s in (28, 29):
+        want = {int(x) for x in descendent_sections(section_sig(DEEP_ROOT), s)}
+        rows = np.load(os.path.join(ref_root, "data", f"counts-{s}.npy"))
+        rows = rows[[int(r[0]) in want for r in rows]]
+        assert len(rows) == len(want)
+        out[f"counts_{s}"] = rows
+    np.savez_compressed(os.path.join(HERE, "counts_28_29.npz"), **out)
 
 
 def numbers(text):
@@ -154,6 +175,8 @@ def main(ref_root):
               open(os.path.join(HERE, "shards.json"), "w"))
     np.savez_compressed(os.path.join(HERE, "counts_0_5.npz"),
                         **{f"counts_{s}": np.load(os.path.join(ref_root, "data", f"counts-{s}.npy")) for s in range(6)})
+    # 10. counts of the deep root's sections at slices 28 and 29
+    deep_root_counts(ref_root)
     print("wrote fixtures to", HERE)
 
 

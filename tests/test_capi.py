@@ -96,3 +96,18 @@ def test_sweep_child_refuses_unstandardized_sections():
     bad = section_sig([[3, 3], [4, 3], [4, 5], [4, 4]])   # not standardized
     dummy = np.zeros(8, np.uint64)
     assert L.pg_end_sweep_slice_child(P(parents), 1, P(dummy), bad, P(dummy), None) == capi.PG_ERR_ARG
+
+
+def test_deep_root_slices_and_golden_rows():
+    """The 28-stone root of the compressed-sweep test: its two largest
+    adjacent slices need more than a B200 holds raw, and the committed golden
+    rows cover exactly its sections at slices 28 and 29."""
+    from pentago_b200 import sweep
+    from pentago_b200.end import section_sig
+    from tests.test_slice_store_gpu import DEEP_ROOT
+    root = section_sig(DEEP_ROOT)
+    nodes = {s: int(sweep.slice_layout(sweep.descendent_sections(root, s))[-1]) for s in range(28, 36)}
+    assert 64 * max(nodes[s] + nodes[s + 1] for s in range(28, 35)) > 192e9
+    gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "counts_28_29.npz"))
+    for s in (28, 29):
+        assert sorted(int(r[0]) for r in gold[f"counts_{s}"]) == [int(x) for x in sweep.descendent_sections(root, s)]

@@ -3,7 +3,9 @@ round trip on ragged blocks of random nodes and its refusal of damaged
 streams, a solved slice through the per-block store and back, and a sweep
 that keeps every
 finished slice compressed, computing each slice one child section at a time,
-with the same counts and the same last slice as the plain sweep."""
+with the same counts and the same last slice as the plain sweep; and a root
+too deep to sweep raw in one device's memory, solved compressed and checked
+against the reference's counts."""
 import numpy as np
 import pytest
 
@@ -122,3 +124,37 @@ def test_compressed_sweep_matches_plain(cuda, tmp_path):
     # the section-by-section checkpoint holds the same slice
     _, _, back = supertensor.read_slice(str(tmp_path / "slice-33.pentago"))
     assert torch.equal(back, last)
+
+
+# A 28-stone root whose slices 31 and 30 (105.4 + 99.5 GB) do not fit a B200's
+# HBM side by side raw (tests/golden/make_golden.py: DEEP_ROOT).
+DEEP_ROOT = [[4, 4], [4, 5], [4, 3], [2, 2]]
+
+
+def test_deep_root_needs_compression_and_matches_golden(cuda):
+    """The plain sweep of the 28-stone root is refused before it allocates
+    anything; the compressed sweep solves slices 35 down to 28 well inside the
+    device's memory, and every one of the 75 sections' counts equals the row
+    of data/counts-N.npy from the original solve (about two minutes)."""
+    import os
+    import torch
+    from pentago_b200 import capi, sweep
+    from pentago_b200.end import section_sig
+    here = os.path.join(os.path.dirname(__file__), "golden")
+    gold = dict(np.load(os.path.join(here, "counts_30_35.npz")))
+    gold.update(dict(np.load(os.path.join(here, "counts_28_29.npz"))))
+    root = section_sig(DEEP_ROOT)
+    with pytest.raises(capi.PentagoError) as refused:
+        sweep.sweep(root)
+    assert refused.value.code == capi.PG_ERR_CAPACITY
+    torch.cuda.empty_cache()
+    torch.cuda.reset_peak_memory_stats()
+    res = sweep.sweep(root, compress=True)
+    assert sorted(res) == list(range(28, 36))
+    assert sum(len(rows) for rows in res.values()) == 75
+    for s, rows in res.items():
+        want = {int(r[0]): r for r in gold[f"counts_{s}"]}
+        for r in rows:
+            assert np.array_equal(want[int(r[0])], r), f"slice {s} section {int(r[0]):#x}"
+    total = torch.cuda.get_device_properties(0).total_memory
+    assert torch.cuda.max_memory_allocated() < 0.75 * total
