@@ -28,12 +28,12 @@ constexpr int kLanesS = 8;
 constexpr uint32_t kTotBits = 14, kTot = 1u << kTotBits, kLow = 1u << 23;
 constexpr int kHead = 4 * kLanesS;
 constexpr int kGroups = 16;  // streams per CTA of the coder kernels
+constexpr int kThreads = kGroups * kLanesS;
 
 // Nodes per lane of a block of n nodes.
 __host__ __device__ inline int lane_nodes(int n) { return (n + kLanesS - 1) / kLanesS; }
 __host__ __device__ inline int64_t lane_cap(int n) { return int64_t(lane_nodes(n)) * 64 + 64; }
 __host__ __device__ inline int64_t store_bound(int n) { return kHead + kLanesS * lane_cap(n); }
-constexpr uint32_t kRawBlock = ~0u;
 
 // Symbols of one node packed 2 bits each (16 per word, rotation r at bits
 // 2 (r & 15) of word r >> 4): black bit + 2 white bit, for the side-to-move
@@ -52,6 +52,10 @@ __device__ __forceinline__ uint32_t gather16(uint32_t x) {
   x = (x | x >> 4) & 0x00ff00ffu;
   return (x | x >> 8) & 0xffffu;
 }
+// A node's 16 symbol words live S words apart in shared memory: the coder
+// threads keep theirs in columns (S = threads per CTA), so that a warp whose
+// threads read the same word index reads 32 different banks.
+template<int S>
 __device__ __forceinline__ void pack_node(const uint64_t* node, int turn, uint32_t* sym) {
 #pragma unroll
   for (int w = 0; w < 4; w++) {
@@ -59,16 +63,18 @@ __device__ __forceinline__ void pack_node(const uint64_t* node, int turn, uint32
     const uint64_t black = turn ? ~nl : win, white = turn ? win : ~nl;
 #pragma unroll
     for (int h = 0; h < 4; h++)
-      sym[4 * w + h] = spread16(uint32_t(black >> (16 * h))) | spread16(uint32_t(white >> (16 * h))) << 1;
+      sym[S * (4 * w + h)] = spread16(uint32_t(black >> (16 * h))) | spread16(uint32_t(white >> (16 * h))) << 1;
   }
 }
-__device__ __forceinline__ int sym_at(const uint32_t* sym, int r) { return int(sym[r >> 4] >> (2 * (r & 15)) & 3); }
+template<int S>
+__device__ __forceinline__ int sym_at(const uint32_t* sym, int r) { return int(sym[S * (r >> 4)] >> (2 * (r & 15)) & 3); }
 
+template<int S>
 __device__ __forceinline__ int context(const uint32_t* cur, const uint32_t* prev, int r) {
   int c = 0;
 #pragma unroll
-  for (int q = 0; q < 4; q++) c = 4 * c + ((r >> (2 * q) & 3) ? sym_at(cur, r - (1 << (2 * q))) : 3);
-  return 4 * c + (prev ? sym_at(prev, r) : 3);
+  for (int q = 0; q < 4; q++) c = 4 * c + ((r >> (2 * q) & 3) ? sym_at<S>(cur, r - (1 << (2 * q))) : 3);
+  return 4 * c + (prev ? sym_at<S>(prev, r) : 3);
 }
 
 // Context counts over a batch of blocks: one CTA per block, thread r takes
@@ -91,8 +97,8 @@ store_hist_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restrict_
       cur[r] = spread16(uint32_t(black >> (16 * hq))) | spread16(uint32_t(white >> (16 * hq))) << 1;
     }
     __syncthreads();
-    const int c = context(cur, k % m ? prev : nullptr, r);
-    atomicAdd(&h[3 * c + sym_at(cur, r)], 1u);
+    const int c = context<1>(cur, k % m ? prev : nullptr, r);
+    atomicAdd(&h[3 * c + sym_at<1>(cur, r)], 1u);
     __syncthreads();
     if (r < 16) prev[r] = cur[r];
   }
@@ -131,7 +137,7 @@ store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restric
                     const int32_t* __restrict__ count, int nblocks, int turn, const uint16_t* __restrict__ freq,
                     uint8_t* __restrict__ out, const int64_t* __restrict__ out_offsets, int64_t* __restrict__ sizes) {
   __shared__ uint16_t F[kCtx * 3];
-  __shared__ uint32_t buf[kGroups * kLanesS][2][16];
+  __shared__ uint32_t buf[2 * 16][kThreads];
   for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x) F[i] = freq[i];
   __syncthreads();
   const int g = threadIdx.x / kLanesS, lane = threadIdx.x % kLanesS;
@@ -148,15 +154,15 @@ store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restric
   uint8_t* p = slot_end;
   uint32_t state = kLow;
   int over = 0;
-  uint32_t* cur = buf[threadIdx.x][0];
-  uint32_t* prev = buf[threadIdx.x][1];
-  if (k1 > k0) pack_node(base + 8 * int64_t(k1 - 1), turn, cur);
+  uint32_t* cur = &buf[0][threadIdx.x];
+  uint32_t* prev = &buf[16][threadIdx.x];
+  if (k1 > k0) pack_node<kThreads>(base + 8 * int64_t(k1 - 1), turn, cur);
   for (int k = k1 - 1; k >= k0 && !over; k--) {
     const bool has_prev = k > k0;
-    if (has_prev) pack_node(base + 8 * int64_t(k - 1), turn, prev);
+    if (has_prev) pack_node<kThreads>(base + 8 * int64_t(k - 1), turn, prev);
     for (int r = 255; r >= 0; r--) {
-      const int s = sym_at(cur, r);
-      const int c = context(cur, has_prev ? prev : nullptr, r);
+      const int s = sym_at<kThreads>(cur, r);
+      const int c = context<kThreads>(cur, has_prev ? prev : nullptr, r);
       const uint32_t f = F[3 * c + s];
       const uint32_t cum = s == 0 ? 0u : s == 1 ? F[3 * c] : uint32_t(F[3 * c]) + F[3 * c + 1];
       const uint32_t xmax = ((kLow >> kTotBits) << 8) * f;
@@ -216,7 +222,7 @@ store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ 
                     const int64_t* __restrict__ dst, int nblocks, int turn, const uint16_t* __restrict__ freq,
                     uint64_t* __restrict__ nodes, int64_t* __restrict__ status) {
   __shared__ uint16_t F[kCtx * 3];
-  __shared__ uint32_t buf[kGroups * kLanesS][2][16];
+  __shared__ uint32_t buf[2 * 16][kThreads];
   for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x) F[i] = freq[i];
   __syncthreads();
   const int g = threadIdx.x / kLanesS, lane = threadIdx.x % kLanesS;
@@ -262,14 +268,14 @@ store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ 
   const uint8_t* end = p + (bad ? 0 : mylen);
   uint32_t state = 0;
   for (int j = 0; j < 4 && p < end; j++) state = (state << 8) | *p++;
-  uint32_t* cur = buf[threadIdx.x][0];
-  uint32_t* prev = buf[threadIdx.x][1];
+  uint32_t* cur = &buf[0][threadIdx.x];
+  uint32_t* prev = &buf[16][threadIdx.x];
   uint64_t* outp = nodes + 8 * dst[b];
   for (int k = k0; k < k1 && !bad; k++) {
     const bool has_prev = k > k0;
-    for (int i = 0; i < 16; i++) cur[i] = 0;
+    for (int i = 0; i < 16; i++) cur[kThreads * i] = 0;
     for (int r = 0; r < 256; r++) {
-      const int c = context(cur, has_prev ? prev : nullptr, r);
+      const int c = context<kThreads>(cur, has_prev ? prev : nullptr, r);
       const uint32_t f0 = F[3 * c], f1 = F[3 * c + 1];
       const uint32_t slot = state & (kTot - 1);
       const int s = slot < f0 ? 0 : slot < f0 + f1 ? 1 : 2;
@@ -277,13 +283,13 @@ store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ 
       const uint32_t cum = s == 0 ? 0u : s == 1 ? f0 : f0 + f1;
       state = f * (state >> kTotBits) + slot - cum;
       while (state < kLow && p < end) state = (state << 8) | *p++;
-      cur[r >> 4] |= uint32_t(s) << (2 * (r & 15));
+      cur[kThreads * (r >> 4)] |= uint32_t(s) << (2 * (r & 15));
     }
     uint64_t* o = outp + 8 * int64_t(k);
     for (int w = 0; w < 4; w++) {
       uint64_t black = 0, white = 0;
       for (int h = 0; h < 4; h++) {
-        const uint32_t x = cur[4 * w + h];
+        const uint32_t x = cur[kThreads * (4 * w + h)];
         black |= uint64_t(gather16(x)) << (16 * h);
         white |= uint64_t(gather16(x >> 1)) << (16 * h);
       }
