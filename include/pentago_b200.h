@@ -275,7 +275,8 @@ int pg_pack_streams(const uint8_t* in, const int64_t* in_offsets, const int64_t*
 
 /* Bytes a block of `nodes` nodes may need. */
 int64_t pg_store_bound(int64_t nodes);
-/* The frequency table of a batch of blocks (from its context counts). */
+/* The frequency table of a batch of blocks, from the context counts of at
+ * most 2048 of its blocks spread evenly over it. */
 int pg_store_table(const uint64_t* nodes, const int64_t* first, const int32_t* count, int nblocks, int turn,
                    uint16_t* table, void* stream);
 /* Block b into out + out_offsets[b] (room for pg_store_bound); sizes[b] = its bytes. */

@@ -129,12 +129,6 @@ PG_HD lookup_loc_t lookup_locate(const dev_tables_t& T, uint64_t board, int* ind
   return L;
 }
 
-__global__ void lookup_locate_kernel(const dev_tables_t T, const uint64_t* __restrict__ boards, int64_t n,
-                                     lookup_loc_t* __restrict__ locs) {
-  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
-    locs[i] = lookup_locate(T, boards[i]);
-}
-
 // value(): win (1), tie (0) or loss (-1) for the side to move, from the
 // node's [black wins, white wins] pair: extract (block_cache.cc:114-117) the
 // mover's wins and win-or-tie, move them to the board's rotation, bit 0.

@@ -29,6 +29,9 @@ constexpr uint32_t kTotBits = 14, kTot = 1u << kTotBits, kLow = 1u << 23;
 constexpr int kHead = 4 * kLanesS;
 constexpr int kGroups = 16;  // streams per CTA of the coder kernels
 constexpr int kThreads = kGroups * kLanesS;
+// A batch's frequency table counts the contexts of at most this many of its
+// blocks, spread evenly over it (about 2 G symbols for full blocks).
+constexpr int kTableBlocks = 2048;
 
 // Nodes per lane of a block of n nodes.
 __host__ __device__ inline int lane_nodes(int n) { return (n + kLanesS - 1) / kLanesS; }
@@ -77,15 +80,55 @@ __device__ __forceinline__ int context(const uint32_t* cur, const uint32_t* prev
   return 4 * c + (prev ? sym_at<S>(prev, r) : 3);
 }
 
-// Context counts over a batch of blocks: one CTA per block, thread r takes
-// rotation r of every node in lane order.
+// The coder kernels take a node's symbols a word (16 rotations r = 16 w + i)
+// at a time: the context fields of all 16 come from five words.  Axis 0's
+// neighbour r - 1 and axis 1's r - 4 are symbols i - 1 and i - 4 of the same
+// word (none where i % 4 == 0, resp. i < 4); axis 2's r - 16 and axis 3's
+// r - 64 are words w - 1 and w - 4 (none where w % 4 == 0, resp. w < 4); the
+// previous node's symbol is its word w.  A missing neighbour reads as 3.
+constexpr uint32_t kNoAxis0 = 0x03030303u, kNoAxis1 = 0x000000ffu;
+__device__ __forceinline__ int word_context(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t ap,
+                                            int i) {
+  return int((a0 >> (2 * i) & 3) << 8 | (a1 >> (2 * i) & 3) << 6 | (a2 >> (2 * i) & 3) << 4 |
+             (a3 >> (2 * i) & 3) << 2 | (ap >> (2 * i) & 3));
+}
+
+// Frequencies of a context in one 8-byte shared-memory word: f0 | f1 << 16, f2.
+__device__ __forceinline__ void load_freqs(const uint16_t* __restrict__ freq, uint2* F) {
+  for (int c = threadIdx.x; c < kCtx; c += blockDim.x)
+    F[c] = make_uint2(uint32_t(freq[3 * c]) | uint32_t(freq[3 * c + 1]) << 16, freq[3 * c + 2]);
+}
+
+// The encoder divides the state by a symbol's frequency f with a reciprocal
+// multiply, as in F. Giesen's ryg_rans (after Alverson, "Integer division
+// using reciprocals", 1991): with 2^(sh-1) < f <= 2^sh, rcp = ceil(2^(sh+31)
+// / f) gives state / f = umulhi(state, rcp) >> (sh - 1) for every state below
+// 2^31 (renormalization keeps it below 2^17 f <= 2^31).  f = 1 takes rcp =
+// 2^32 - 1, shift 0 and a bias of 2^14 - 1, which yields the same new state.
+// Per context: three reciprocals, and the three shifts in bits 16.. of F.y.
+__device__ __forceinline__ void encoder_freqs(const uint16_t* __restrict__ freq, uint2* F, uint32_t* rcp) {
+  for (int c = threadIdx.x; c < kCtx; c += blockDim.x) {
+    uint32_t shifts = 0;
+    for (int s = 0; s < 3; s++) {
+      const uint32_t f = freq[3 * c + s];
+      uint32_t sh = 0;
+      while (f > (1u << sh)) sh++;
+      rcp[3 * c + s] = f < 2 ? ~0u : uint32_t(((uint64_t(1) << (sh + 31)) + f - 1) / f);
+      shifts |= (f < 2 ? 0u : sh - 1) << (4 * s);
+    }
+    F[c] = make_uint2(uint32_t(freq[3 * c]) | uint32_t(freq[3 * c + 1]) << 16, freq[3 * c + 2] | shifts << 16);
+  }
+}
+
+// Context counts over every stride-th block of a batch: one CTA per block,
+// thread r takes rotation r of every node in lane order.
 __global__ void __launch_bounds__(256)
 store_hist_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restrict__ first,
-                  const int32_t* __restrict__ count, int turn, unsigned* __restrict__ hist) {
+                  const int32_t* __restrict__ count, int stride, int turn, unsigned* __restrict__ hist) {
   __shared__ unsigned h[kCtx * 3];
   __shared__ uint32_t cur[16], prev[16];
   for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x) h[i] = 0;
-  const int b = blockIdx.x, n = count[b], m = lane_nodes(n), r = threadIdx.x;
+  const int b = blockIdx.x * stride, n = count[b], m = lane_nodes(n), r = threadIdx.x;
   const uint64_t* base = nodes + 8 * first[b];
   __syncthreads();
   for (int k = 0; k < n; k++) {
@@ -136,9 +179,10 @@ __global__ void __launch_bounds__(kGroups * kLanesS)
 store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restrict__ first,
                     const int32_t* __restrict__ count, int nblocks, int turn, const uint16_t* __restrict__ freq,
                     uint8_t* __restrict__ out, const int64_t* __restrict__ out_offsets, int64_t* __restrict__ sizes) {
-  __shared__ uint16_t F[kCtx * 3];
+  __shared__ uint2 F[kCtx];
+  __shared__ uint32_t RCP[kCtx * 3];
   __shared__ uint32_t buf[2 * 16][kThreads];
-  for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x) F[i] = freq[i];
+  encoder_freqs(freq, F, RCP);
   __syncthreads();
   const int g = threadIdx.x / kLanesS, lane = threadIdx.x % kLanesS;
   const int b = blockIdx.x * kGroups + g;
@@ -160,19 +204,31 @@ store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restric
   for (int k = k1 - 1; k >= k0 && !over; k--) {
     const bool has_prev = k > k0;
     if (has_prev) pack_node<kThreads>(base + 8 * int64_t(k - 1), turn, prev);
-    for (int r = 255; r >= 0; r--) {
-      const int s = sym_at<kThreads>(cur, r);
-      const int c = context<kThreads>(cur, has_prev ? prev : nullptr, r);
-      const uint32_t f = F[3 * c + s];
-      const uint32_t cum = s == 0 ? 0u : s == 1 ? F[3 * c] : uint32_t(F[3 * c]) + F[3 * c + 1];
-      const uint32_t xmax = ((kLow >> kTotBits) << 8) * f;
-      while (state >= xmax) {
-        if (p - slot_begin <= 4) { over = 1; break; }   // keep room for the final state
-        *--p = uint8_t(state);
-        state >>= 8;
+    for (int w = 15; w >= 0 && !over; w--) {
+      const uint32_t x = cur[kThreads * w];
+      const uint32_t a0 = x << 2 | kNoAxis0, a1 = x << 8 | kNoAxis1;
+      const uint32_t a2 = (w & 3) ? cur[kThreads * (w - 1)] : ~0u;
+      const uint32_t a3 = w >= 4 ? cur[kThreads * (w - 4)] : ~0u;
+      const uint32_t ap = has_prev ? prev[kThreads * w] : ~0u;
+#pragma unroll
+      for (int i = 15; i >= 0; i--) {
+        const uint32_t sym = x >> (2 * i) & 3;
+        const int c = word_context(a0, a1, a2, a3, ap, i);
+        const uint2 fc = F[c];
+        const uint32_t rcp = RCP[3 * c + sym];
+        const uint32_t f0 = fc.x & 0xffffu, f1 = fc.x >> 16;
+        const uint32_t f = sym == 0 ? f0 : sym == 1 ? f1 : fc.y & 0xffffu;
+        const uint32_t cum = sym == 0 ? 0u : sym == 1 ? f0 : f0 + f1;
+        const uint32_t xmax = ((kLow >> kTotBits) << 8) * f;
+        while (state >= xmax) {
+          if (p - slot_begin <= 4) { over = 1; break; }   // keep room for the final state
+          *--p = uint8_t(state);
+          state >>= 8;
+        }
+        if (over) break;
+        const uint32_t q = __umulhi(state, rcp) >> (fc.y >> (16 + 4 * sym) & 15);
+        state += cum + (f < 2 ? kTot - 1 : 0u) + q * (kTot - f);
       }
-      if (over) break;
-      state = ((state / f) << kTotBits) + state % f + cum;
     }
     uint32_t* t = cur; cur = prev; prev = t;
   }
@@ -221,9 +277,9 @@ store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ 
                     const int64_t* __restrict__ in_sizes, const int32_t* __restrict__ count,
                     const int64_t* __restrict__ dst, int nblocks, int turn, const uint16_t* __restrict__ freq,
                     uint64_t* __restrict__ nodes, int64_t* __restrict__ status) {
-  __shared__ uint16_t F[kCtx * 3];
+  __shared__ uint2 F[kCtx];
   __shared__ uint32_t buf[2 * 16][kThreads];
-  for (int i = threadIdx.x; i < kCtx * 3; i += blockDim.x) F[i] = freq[i];
+  load_freqs(freq, F);
   __syncthreads();
   const int g = threadIdx.x / kLanesS, lane = threadIdx.x % kLanesS;
   const int b = blockIdx.x * kGroups + g;
@@ -273,17 +329,25 @@ store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ 
   uint64_t* outp = nodes + 8 * dst[b];
   for (int k = k0; k < k1 && !bad; k++) {
     const bool has_prev = k > k0;
-    for (int i = 0; i < 16; i++) cur[kThreads * i] = 0;
-    for (int r = 0; r < 256; r++) {
-      const int c = context<kThreads>(cur, has_prev ? prev : nullptr, r);
-      const uint32_t f0 = F[3 * c], f1 = F[3 * c + 1];
-      const uint32_t slot = state & (kTot - 1);
-      const int s = slot < f0 ? 0 : slot < f0 + f1 ? 1 : 2;
-      const uint32_t f = s == 0 ? f0 : s == 1 ? f1 : F[3 * c + 2];
-      const uint32_t cum = s == 0 ? 0u : s == 1 ? f0 : f0 + f1;
-      state = f * (state >> kTotBits) + slot - cum;
-      while (state < kLow && p < end) state = (state << 8) | *p++;
-      cur[kThreads * (r >> 4)] |= uint32_t(s) << (2 * (r & 15));
+    for (int w = 0; w < 16; w++) {
+      const uint32_t a2 = (w & 3) ? cur[kThreads * (w - 1)] : ~0u;
+      const uint32_t a3 = w >= 4 ? cur[kThreads * (w - 4)] : ~0u;
+      const uint32_t ap = has_prev ? prev[kThreads * w] : ~0u;
+      uint32_t x = 0;   // the word's symbols decoded so far
+#pragma unroll
+      for (int i = 0; i < 16; i++) {
+        const uint32_t a0 = x << 2 | kNoAxis0, a1 = x << 8 | kNoAxis1;
+        const uint2 fc = F[word_context(a0, a1, a2, a3, ap, i)];
+        const uint32_t f0 = fc.x & 0xffffu, f1 = fc.x >> 16;
+        const uint32_t slot = state & (kTot - 1);
+        const uint32_t sym = slot < f0 ? 0 : slot < f0 + f1 ? 1 : 2;
+        const uint32_t f = sym == 0 ? f0 : sym == 1 ? f1 : fc.y;
+        const uint32_t cum = sym == 0 ? 0u : sym == 1 ? f0 : f0 + f1;
+        state = f * (state >> kTotBits) + slot - cum;
+        while (state < kLow && p < end) state = (state << 8) | *p++;
+        x |= sym << (2 * i);
+      }
+      cur[kThreads * w] = x;
     }
     uint64_t* o = outp + 8 * int64_t(k);
     for (int w = 0; w < 4; w++) {
@@ -324,7 +388,9 @@ extern "C" int pg_store_table(const uint64_t* nodes, const int64_t* first, const
   PG_CUDA(scratch.alloc(&hist, sizeof(unsigned) * kCtx * 3));
   PG_CUDA(cudaMemsetAsync(hist, 0, sizeof(unsigned) * kCtx * 3, stream));
   if (nblocks) {
-    store_hist_kernel<<<nblocks, 256, 0, stream>>>(nodes, first, count, turn & 1, hist);
+    const int stride = (nblocks + kTableBlocks - 1) / kTableBlocks;
+    store_hist_kernel<<<(nblocks + stride - 1) / stride, 256, 0, stream>>>(nodes, first, count, stride, turn & 1,
+                                                                            hist);
     PG_CUDA(cudaGetLastError());
   }
   store_table_kernel<<<kCtx / 256, 256, 0, stream>>>(hist, table);
