@@ -10,12 +10,12 @@
 // node one step back along each of the four rotation axes (3 where the
 // coordinate is 0) and the same rotation of the previous node of the lane.
 // One frequency table (1024 contexts x 3) serves a whole batch of blocks.
-// A block's 8 lanes each take a contiguous run of its nodes, so every context
-// symbol is on the lane that codes the symbol and the lanes decode in
-// parallel.  Stream layout: 8 lane lengths (u32), then the lanes' bytes; a
-// block that some lane cannot code within its nodes' raw size is stored raw
-// instead (first length ~0, then the 64-byte nodes), so a stream never
-// needs more than its raw size plus 32 + 8 x 64 bytes.
+// A block's 32 lanes (one warp) each take a contiguous run of its nodes, so
+// every context symbol is on the lane that codes the symbol and the lanes
+// decode in parallel.  Stream layout: 32 lane lengths (u32), then the lanes'
+// bytes; a block that some lane cannot code within its nodes' raw size is
+// stored raw instead (first length ~0, then the 64-byte nodes), so a stream
+// never needs more than its raw size plus 128 + 32 x 64 bytes.
 #include "../../include/pentago_b200.h"
 #include "runtime.h"
 #include <cstdint>
@@ -24,10 +24,10 @@ namespace pg {
 namespace {
 
 constexpr int kCtx = 1024;
-constexpr int kLanesS = 8;
+constexpr int kLanesS = 32;   // lanes per block: one warp
 constexpr uint32_t kTotBits = 14, kTot = 1u << kTotBits, kLow = 1u << 23;
 constexpr int kHead = 4 * kLanesS;
-constexpr int kGroups = 16;  // streams per CTA of the coder kernels
+constexpr int kGroups = 4;   // streams per CTA of the coder kernels
 constexpr int kThreads = kGroups * kLanesS;
 // A batch's frequency table counts the contexts of at most this many of its
 // blocks, spread evenly over it (about 2 G symbols for full blocks).
@@ -187,7 +187,7 @@ store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restric
   const int g = threadIdx.x / kLanesS, lane = threadIdx.x % kLanesS;
   const int b = blockIdx.x * kGroups + g;
   if (b >= nblocks) return;
-  const unsigned gmask = 0xffu << (threadIdx.x & 24);
+  constexpr unsigned gmask = 0xffffffffu;   // a block's lanes are one warp
   const int n = count[b], m = lane_nodes(n);
   const int k0 = lane * m, k1 = min(n, k0 + m);
   const uint64_t* base = nodes + 8 * first[b];
@@ -247,25 +247,35 @@ store_encode_kernel(const uint64_t* __restrict__ nodes, const int64_t* __restric
   }
   for (int j = 0; j < 4; j++) *--p = uint8_t(state >> (8 * j));
   const uint32_t len = uint32_t(slot_end - p);
-  uint32_t lens[kLanesS];
-  for (int l = 0; l < kLanesS; l++) lens[l] = __shfl_sync(gmask, len, l, kLanesS);
-  int64_t dst = kHead;
-  for (int l = 0; l < lane; l++) dst += lens[l];
-  // lane l's bytes move left, never past a lane not yet moved
+  // Destination of this lane's bytes behind the header: the lengths of the
+  // lanes before it (an exclusive warp scan), and the stream's total.
+  uint32_t before = len;
+#pragma unroll
+  for (int o = 1; o < kLanesS; o <<= 1) {
+    const uint32_t v = __shfl_up_sync(gmask, before, o);
+    if (lane >= o) before += v;
+  }
+  const uint32_t total = __shfl_sync(gmask, before, kLanesS - 1);
+  before -= len;
+  // The lanes' bytes move left, one lane after another, the whole warp
+  // copying 32 bytes a round; a round reads all its bytes before writing any.
+  // A lane's destination never passes its own source (it moves left) nor a
+  // later lane's source (each lane's bytes fit its slot).
   for (int l = 0; l < kLanesS; l++) {
-    __syncwarp(gmask);
-    if (l == lane)
-      for (uint32_t i = 0; i < len; i++) sbase[dst + i] = p[i];
-  }
-  __syncwarp(gmask);
-  if (lane == 0) {
-    int64_t total = kHead;
-    for (int l = 0; l < kLanesS; l++) {
-      for (int j = 0; j < 4; j++) sbase[4 * l + j] = uint8_t(lens[l] >> (8 * j));
-      total += lens[l];
+    const uint32_t n_l = __shfl_sync(gmask, len, l);
+    const int64_t dst_l = kHead + int64_t(__shfl_sync(gmask, before, l));
+    const uint8_t* src_l = reinterpret_cast<const uint8_t*>(
+        __shfl_sync(gmask, reinterpret_cast<unsigned long long>(p), l));
+    for (uint32_t i0 = 0; i0 < n_l; i0 += kLanesS) {
+      const uint32_t i = i0 + lane;
+      const uint8_t v = i < n_l ? src_l[i] : 0;
+      __syncwarp(gmask);
+      if (i < n_l) sbase[dst_l + i] = v;
+      __syncwarp(gmask);
     }
-    sizes[b] = total;
   }
+  for (int j = 0; j < 4; j++) sbase[4 * lane + j] = uint8_t(len >> (8 * j));
+  if (lane == 0) sizes[b] = kHead + int64_t(total);
 }
 
 // Decode: lane l decodes its nodes forward into shared memory, one node at a
@@ -284,7 +294,7 @@ store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ 
   const int g = threadIdx.x / kLanesS, lane = threadIdx.x % kLanesS;
   const int b = blockIdx.x * kGroups + g;
   if (b >= nblocks) return;
-  const unsigned gmask = 0xffu << (threadIdx.x & 24);
+  constexpr unsigned gmask = 0xffffffffu;   // a block's lanes are one warp
   const int n = count[b], m = lane_nodes(n);
   const int k0 = lane * m, k1 = min(n, k0 + m);
   const uint8_t* sbase = in + in_offsets[b];
@@ -310,15 +320,21 @@ store_decode_kernel(const uint8_t* __restrict__ in, const int64_t* __restrict__ 
     if (lane == 0) status[b] = ok ? n : PG_ERR_FORMAT;
     return;
   }
-  if (!bad) {
-    for (int l = 0; l < kLanesS; l++) {
-      uint32_t v = 0;
-      for (int j = 0; j < 4; j++) v |= uint32_t(sbase[4 * l + j]) << (8 * j);
-      if (l < lane) start += v;
-      if (l == lane) mylen = v;
-      total += v;
+  {
+    // this lane's length, the lengths before it (exclusive scan) and the sum
+    uint32_t v = 0;
+    if (!bad)
+      for (int j = 0; j < 4; j++) v |= uint32_t(sbase[4 * lane + j]) << (8 * j);
+    uint64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < kLanesS; o <<= 1) {
+      const uint64_t u = __shfl_up_sync(gmask, incl, o);
+      if (lane >= o) incl += u;
     }
-    bad = total != uint64_t(size - kHead);
+    mylen = v;
+    start = incl - v;
+    total = __shfl_sync(gmask, incl, kLanesS - 1);
+    if (!bad) bad = total != uint64_t(size - kHead);
   }
   const uint8_t* p = sbase + kHead + start;
   const uint8_t* end = p + (bad ? 0 : mylen);

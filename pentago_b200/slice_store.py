@@ -32,11 +32,16 @@ def slice_blocks(sigs):
     return np.concatenate(sec), np.concatenate(first), np.concatenate(count), np.array(sec_first), base
 
 
+# The store coder's streams: LANES lanes per block, a header of their lengths.
+LANES = 32
+HEAD = 4 * LANES
+
+
 def store_bound(count):
-    """pg_store_bound for an array of block node counts: a 32-byte header and
-    8 lanes of the raw size of ceil(count / 8) nodes plus 64 bytes each."""
+    """pg_store_bound for an array of block node counts: the header and LANES
+    lanes of the raw size of ceil(count / LANES) nodes plus 64 bytes each."""
     count = np.asarray(count, np.int64)
-    return 32 + 8 * ((count + 7) // 8 * 64 + 64)
+    return HEAD + LANES * ((count + LANES - 1) // LANES * 64 + 64)
 
 
 class compressed_slice:

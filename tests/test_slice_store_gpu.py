@@ -32,7 +32,7 @@ def test_symbols_to_nodes_inverts_node_symbols(cuda):
 def test_store_coder_roundtrip_and_damage(cuda):
     import torch
     from pentago_b200 import capi
-    from pentago_b200.slice_store import store_bound
+    from pentago_b200.slice_store import HEAD, store_bound
     L = capi.lib()
     counts = np.array([1, 7, 8, 9, 100, 4096, 4095, 512], np.int32)
     assert [L.pg_store_bound(int(c)) for c in counts] == store_bound(counts).tolist()
@@ -60,7 +60,7 @@ def test_store_coder_roundtrip_and_damage(cuda):
         capi.check(L.pg_store_encode(nodes.data_ptr(), d_first.data_ptr(), d_count.data_ptr(), len(counts), turn,
                                      table.data_ptr(), out.data_ptr(), d_off.data_ptr(), sizes.data_ptr(), None))
         sz = sizes.cpu().numpy()
-        assert (sz > 32).all() and (sz <= caps).all()
+        assert (sz > HEAD).all() and (sz <= caps).all()
 
         def decode(data, sizes_):
             back = torch.zeros_like(nodes)
@@ -80,7 +80,7 @@ def test_store_coder_roundtrip_and_damage(cuda):
                                      table.data_ptr(), raw_out.data_ptr(), d_off.data_ptr(), raw_sizes.data_ptr(),
                                      None))
         rs = raw_sizes.cpu().numpy()
-        assert (rs <= caps).all() and (rs == 32 + 64 * counts.astype(np.int64)).any()
+        assert (rs <= caps).all() and (rs == HEAD + 64 * counts.astype(np.int64)).any()
         back = torch.zeros_like(noisy)
         status = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
         capi.check(L.pg_store_decode(raw_out.data_ptr(), d_off.data_ptr(), t(rs).data_ptr(), d_count.data_ptr(),
