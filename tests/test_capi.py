@@ -111,3 +111,30 @@ def test_deep_root_slices_and_golden_rows():
     gold = np.load(os.path.join(os.path.dirname(__file__), "golden", "counts_28_29.npz"))
     for s in (28, 29):
         assert sorted(int(r[0]) for r in gold[f"counts_{s}"]) == [int(x) for x in sweep.descendent_sections(root, s)]
+
+
+def test_store_bound_matches_the_library():
+    """slice_store.store_bound (what compressed_slice reserves per block) is
+    the library's pg_store_bound for every block size up to a full block."""
+    from pentago_b200 import capi
+    from pentago_b200.slice_store import store_bound
+    L = capi.lib()
+    counts = np.arange(0, 4097)
+    assert store_bound(counts).tolist() == [L.pg_store_bound(int(c)) for c in counts]
+    assert L.pg_store_bound(-1) == capi.PG_ERR_ARG
+
+
+def test_sweep_arena_halves_hold_every_adjacent_pair():
+    """The raw sweep's two arena halves (slices alternate between them) add
+    up to the largest pair of adjacent slices for the config-2 root, whose
+    slice sizes rise and then fall: 63.5 + 78.2 = 141.7 GB."""
+    from pentago_b200 import sweep
+    from pentago_b200.end import section_sig
+    root = section_sig([[4, 4], [4, 5], [4, 3], [3, 3]])
+    chain = list(range(35, 29, -1))
+    halves = sweep._arena_nodes(root, chain)
+    nodes = [int(sweep.slice_layout(sweep.descendent_sections(root, s))[-1]) for s in chain]
+    assert sum(halves) == max(a + b for a, b in zip(nodes, nodes[1:]))
+    assert round(64 * sum(halves) / 1e9, 1) == 141.7
+    # every slice fits the half it is placed in
+    assert all(n <= halves[k % 2] for k, n in enumerate(nodes))
