@@ -1,6 +1,6 @@
 """Benchmark: end-engine block compute on one section, pentago's endgame hot path.
 
-Workload ("config 1", batched): the 30-stone section [[4,4],[4,4],[4,3],[3,4]]
+Workload (batched): the 30-stone section [[4,4],[4,4],[4,3],[3,4]]
 (shape 160x160x318x318, black to move).  One step computes, for B full 8^4
 blocks of that section, the four block lines through each block (one per
 quadrant dimension, each the full line, exactly the reference's unit of work
@@ -176,7 +176,7 @@ def cpu_reference_rate(seconds=12.0, threads=0, passes=None, warmup=0):
                       f"({nodes} parent nodes), reference engine oracle/_ref on {nthreads} threads"}
 
 
-CONFIG2_ROOT = [[4, 4], [4, 5], [4, 3], [3, 3]]
+SWEEP_ROOT = [[4, 4], [4, 5], [4, 3], [3, 3]]
 
 
 def cpu_midsolve_rate(raws, positions, seconds=8.0):
@@ -322,11 +322,11 @@ def cpu_lookup_rate(paths, seconds=5.0):
 
 
 def sweep_summary(timings, wall_s):
-    """Config 2 from the per-slice timings of the sweep (slices 35 -> 30)."""
+    """The full sweep of SWEEP_ROOT (slices 35 -> 30) from its per-slice timings."""
     ms = sum(v["ms"] for v in timings.values())
     nbytes = sum(64 * (v["nodes"] + v["child_nodes"]) for v in timings.values())
     sections = sum(v["sections"] for v in timings.values())
-    return {"workload": f"all sections below root {CONFIG2_ROOT}, slices 35 -> 30, in HBM",
+    return {"workload": f"all sections below root {SWEEP_ROOT}, slices 35 -> 30, in HBM",
             "sections": sections, "nodes": sum(v["nodes"] for v in timings.values()), "kernel_ms": ms,
             "arena_ms": sum(v.get("arena_ms", 0.0) for v in timings.values()),
             "arena_GB": max(v.get("arena_GB", 0.0) for v in timings.values()),
@@ -562,20 +562,20 @@ def main():
         cpu = cpu_reference_rate(seconds=12.0)
     if rank == 0 and world == 1:
         from pentago_b200 import mid
-        midsolve, raws0 = mid.bench_config0()
+        midsolve, raws0 = mid.bench_boards_26()
         if not args.no_cpu_baseline:
             midsolve["cpu_baseline"] = cpu_midsolve_rate(raws0, midsolve["positions_per_batch"], seconds=8.0)
     if rank == 0 and world == 1 and not args.no_learned:
-        # Config 2 (the full sweep of the root) and config 3 on a sample of
-        # 4096 of the root slice's blocks, after training
+        # The full sweep of SWEEP_ROOT, then the learned coder trained on its
+        # 30-stone slice and run on a sample of 4096 of that slice's blocks
         torch.cuda.empty_cache()
         from pentago_b200 import learned as learned_mod
         timings = {}
-        learned, sample = learned_mod.run_config3(max_blocks=4096, sample_blocks=64, sweep_timings=timings)
+        learned, sample = learned_mod.run_slice_coding(max_blocks=4096, sample_blocks=64, sweep_timings=timings)
         sweep2 = sweep_summary(timings, learned["sweep_s"])
         if not args.no_cpu_baseline:
             learned["cpu_static_coder"] = cpu_static_coder_rate(*sample, seconds=5.0)
-            sweep2["cpu_baseline"] = cpu_sweep_estimate(CONFIG2_ROOT, timings, seconds_per_slice=1.5)
+            sweep2["cpu_baseline"] = cpu_sweep_estimate(SWEEP_ROOT, timings, seconds_per_slice=1.5)
             sweep2["kernel_speedup_vs_cpu_estimate"] = sweep2["cpu_baseline"]["estimated_s"] / (sweep2["kernel_ms"] / 1e3)
 
     if rank == 0 and world == 1 and not args.no_slice_files:
@@ -627,9 +627,9 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes},
             "gpu_launches": 4 * args.steps,
-            "midsolve_config0": midsolve,
-            "sweep_config2": sweep2,
-            "learned_rans_config3": learned,
+            "midsolve_64_boards_26_stones": midsolve,
+            "sweep_root_30_stones": sweep2,
+            "learned_rans_slice_30": learned,
             "slice_files": slice_files,
             "sharder": sharder,
             "lookups": lookups,

@@ -254,9 +254,9 @@ def static_sizes(symbols, offsets, stream=None):
     return sizes
 
 
-def run_config3(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.01, steps=1500, batch=32768,
+def run_slice_coding(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.01, steps=1500, batch=32768,
                 chunk_blocks=4096, max_blocks=0, seed=1, sample_blocks=0, sweep_timings=None):
-    """Config 3: solve the root's sections down to its own slice, train on a
+    """Solve the root's sections down to its own slice, train on a
     seeded fraction of the root slice's blocks, code max_blocks blocks (0:
     all) both ways and check the round trip.  With sample_blocks > 0 the
     symbols of that many coded blocks are also returned on the host (for a
@@ -358,7 +358,7 @@ def main():
     args = ap.parse_args()
     c = [int(x) for x in args.root.split(",")]
     capi.check(capi.lib().pg_init())
-    res = run_config3(((c[0], c[1]), (c[2], c[3]), (c[4], c[5]), (c[6], c[7])), args.train_fraction, args.steps,
+    res = run_slice_coding(((c[0], c[1]), (c[2], c[3]), (c[4], c[5]), (c[6], c[7])), args.train_fraction, args.steps,
                       args.batch, args.chunk_blocks, args.max_blocks, args.seed)
     res["root"] = args.root
     print(json.dumps(res))

@@ -172,8 +172,8 @@ def positions(raw):
     return 2 * 128 * items
 
 
-def bench_config0(steps=20, warmup=3):
-    """Config 0: 64 seeded 26-stone boards (13 black, 13 white, no five);
+def bench_boards_26(steps=20, warmup=3):
+    """64 seeded 26-stone boards (13 black, 13 white, no five);
     GPU time per batch from CUDA events (median of three trials).  Returns
     the result and the boards."""
     import torch

@@ -126,7 +126,7 @@ def test_store_bound_matches_the_library():
 
 def test_sweep_arena_halves_hold_every_adjacent_pair():
     """The raw sweep's two arena halves (slices alternate between them) add
-    up to the largest pair of adjacent slices for the config-2 root, whose
+    up to the largest pair of adjacent slices for the root [[4,4],[4,5],[4,3],[3,3]], whose
     slice sizes rise and then fall: 63.5 + 78.2 = 141.7 GB."""
     from pentago_b200 import sweep
     from pentago_b200.end import section_sig

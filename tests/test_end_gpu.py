@@ -83,7 +83,7 @@ def test_line_kernel_reference_padded_layout_and_or_mode(cuda, case):
     assert np.array_equal(got, base | prior)
 
 
-def test_single_block_config1_matches_oracle(cuda, O):
+def test_single_block_30_stone_section_matches_oracle(cuda, O):
     """One 8^4 block of the 30-stone section [[4,4],[4,4],[4,3],[3,4]]: the OR
     of the four block lines through block (1,1,1,1), on seeded children."""
     import torch

@@ -26,7 +26,7 @@ def test_midsolve_kernel_code_on_host_matches_oracle(O, stones):
         assert np.array_equal(sup[k][:4 * n], ref[:4 * n])
 
 
-def test_random_boards_config0():
+def test_random_boards_26_stones():
     from pentago_b200 import mid
     raws = mid.random_boards(0, 64, 26)
     assert len(set(raws.tolist())) == 64

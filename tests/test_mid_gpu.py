@@ -27,7 +27,7 @@ def test_midsolve_matches_oracle(cuda, O, stones):
         assert g == oracle_values(O, raw), f"board {int(raw)}"
 
 
-def test_midsolve_config0_64_boards(cuda, O):
+def test_midsolve_64_boards_26_stones(cuda, O):
     """64 seeded 26-stone boards (13 black, 13 white, no existing five)."""
     from pentago_b200 import mid
     raws = mid.random_boards(0, 64, 26)
