@@ -6,8 +6,10 @@ blocks of that section, the four block lines through each block (one per
 quadrant dimension, each the full line, exactly the reference's unit of work
 schedule_compute_line), on seeded synthetic child superinfo (win subset of
 notlost, ~31% of notlost bits set; pentago_b200/synthetic.py).  Every line
-has its own child input and output buffer, as in the reference.  Inputs and
-outputs together exceed the 126 MB L2, so no flush is needed between steps.
+has its own child input and output region, as in the reference (the four
+lines of a block lie side by side in one device buffer per direction, so the
+end-to-end leg moves a block with one copy each way).  Inputs and outputs
+together exceed the 126 MB L2, so no flush is needed between steps.
 
 Metric: positions/s = parent nodes computed x 256 rotations / second.
 
