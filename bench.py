@@ -123,16 +123,32 @@ def measured_hbm_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes (read + write) per parent node of the line kernel, measured by
-    ncu on this workload at full size and committed in the profile summary."""
+def profiled(key):
+    """A figure of the line kernel's committed profile summary (a line
+    `key: value`), measured by ncu; None if absent."""
     try:
         for line in open(PROFILE):
-            if line.startswith("dram_bytes_per_parent_node:"):
+            if line.startswith(key + ":"):
                 return float(line.split(":")[1])
     except OSError:
         pass
     return None
+
+
+def profiled_traffic():
+    """DRAM bytes (read + write) per parent node of the line kernel, measured by
+    ncu on this workload at full size."""
+    return profiled("dram_bytes_per_parent_node")
+
+
+def profiled_limiter():
+    """What bounds the line kernel instead of HBM: its issue and integer-ALU
+    pipe activity in the ncu capture of the profile summary."""
+    issue, alu = profiled("issue_active_pct"), profiled("alu_pipe_active_pct")
+    if issue is None or alu is None:
+        return None
+    return {"kind": "integer ALU issue and latency", "issue_active_pct": issue, "alu_pipe_active_pct": alu,
+            "source": "ncu --set full of end_line_kernel (profiles/end_line_kernel.md)"}
 
 
 def cpu_reference_rate(seconds=12.0, threads=0, passes=None, warmup=0):
@@ -625,7 +641,7 @@ def main():
                          "traffic": (traffic_per_node * out_nodes / 4) if traffic_per_node else None,
                          "traffic_note": "dram read + write per launch (mean of the 4 dims), ncu at full size",
                          "algorithmic_bytes_per_step": alg_bytes, "kernel": "end_line_kernel",
-                         "launches_per_step": 4},
+                         "launches_per_step": 4, "limiter": profiled_limiter()},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes},
             "gpu_launches": 4 * args.steps,
