@@ -99,6 +99,15 @@ int64_t or_lm_decode(const uint8_t* model, uint64_t section, const int* block, c
 double or_lm_grad(const float* params, uint64_t section, const int* block, const uint8_t* symbols,
                   const int64_t* samples, int64_t n, double* grad);
 
+/* The library's store coder for slices kept in device memory (store_oracle.c):
+ * the table of a batch of blocks, and one block's stream each way. */
+int64_t or_store_bound(int64_t n);
+void or_store_table(const uint64_t* nodes, const int64_t* first, const int32_t* count, int nblocks, int turn,
+                    uint16_t* table);
+int64_t or_store_encode_block(const uint64_t* nodes, int n, int turn, const uint16_t* table, uint8_t* out);
+int64_t or_store_decode_block(const uint8_t* in, int64_t size, int n, int turn, const uint16_t* table,
+                              uint64_t* nodes);
+
 #ifdef __cplusplus
 }
 #endif

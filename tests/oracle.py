@@ -45,6 +45,10 @@ SIGS = {
     "lm_encode": (_i64, [_p, _u64, _p, _p, _p, _i64]),
     "lm_decode": (_i64, [_p, _u64, _p, _p, _i64, _p, _i64]),
     "lm_grad": (ctypes.c_double, [_p, _u64, _p, _p, _p, _i64, _p]),
+    "store_bound": (_i64, [_i64]),
+    "store_table": (None, [_p, _p, _p, _i, _i, _p]),
+    "store_encode_block": (_i64, [_p, _i, _i, _p, _p]),
+    "store_decode_block": (_i64, [_p, _i64, _i, _i, _p, _p]),
 }
 
 

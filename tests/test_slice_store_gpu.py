@@ -158,3 +158,56 @@ def test_deep_root_needs_compression_and_matches_golden(cuda):
             assert np.array_equal(want[int(r[0])], r), f"slice {s} section {int(r[0]):#x}"
     total = torch.cuda.get_device_properties(0).total_memory
     assert torch.cuda.max_memory_allocated() < 0.75 * total
+
+
+def test_store_coder_matches_oracle_bytes(cuda, O):
+    """The GPU's frequency table and every stream byte equal the CPU
+    restatement's (oracle/store_oracle.c): skewed random blocks of ragged
+    sizes in both turns, a batch of 2,100 small blocks (the table then counts
+    every second block), and full blocks of a solved slice."""
+    import torch
+    from pentago_b200 import capi, sweep
+    from pentago_b200.end import section_sig
+    from pentago_b200.slice_store import slice_blocks, store_bound
+    from tests.oracle import P
+    from tests.test_store_cpu import COUNTS, batch
+    L = capi.lib()
+    t = lambda a, dt=np.int64: torch.from_numpy(np.ascontiguousarray(a, dtype=dt)).cuda()
+
+    def check(nodes_np, first, counts, turn, blocks):
+        dev = torch.from_numpy(nodes_np.view(np.int64)).cuda()
+        d_first, d_count = t(first), t(counts, np.int32)
+        table = torch.empty(3072, dtype=torch.int16, device="cuda")
+        capi.check(L.pg_store_table(dev.data_ptr(), d_first.data_ptr(), d_count.data_ptr(), len(counts), turn,
+                                    table.data_ptr(), None))
+        want_table = np.zeros(3072, np.uint16)
+        O.store_table(P(nodes_np), P(first), P(counts), len(counts), turn, P(want_table))
+        assert np.array_equal(table.cpu().numpy().view(np.uint16), want_table)
+        caps = store_bound(counts)
+        off = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+        out = torch.zeros(int(caps.sum()), dtype=torch.uint8, device="cuda")
+        sizes = torch.zeros(len(counts), dtype=torch.int64, device="cuda")
+        d_off = t(off)
+        capi.check(L.pg_store_encode(dev.data_ptr(), d_first.data_ptr(), d_count.data_ptr(), len(counts), turn,
+                                     table.data_ptr(), out.data_ptr(), d_off.data_ptr(), sizes.data_ptr(), None))
+        host, sz = out.cpu().numpy(), sizes.cpu().numpy()
+        for b in blocks:
+            n = int(counts[b])
+            block = np.ascontiguousarray(nodes_np[first[b]:first[b] + n])
+            want = np.zeros(int(O.store_bound(n)), np.uint8)
+            size = O.store_encode_block(P(block), n, turn, P(want_table), P(want))
+            assert sz[b] == size, (b, n, turn)
+            assert np.array_equal(host[off[b]:off[b] + size], want[:size]), (b, n, turn)
+
+    for turn in (0, 1):
+        nodes, first, counts = batch(COUNTS, 21 + turn)
+        check(nodes, first, counts, turn, range(len(counts)))
+    rng = np.random.default_rng(4)
+    nodes, first, counts = batch(rng.integers(1, 9, 2100).tolist(), 8)
+    check(nodes, first, counts, 1, rng.choice(2100, 40, replace=False))
+    _, slice_t, sigs = sweep.sweep(section_sig(ROOT), min_slice=34, keep_last=True)
+    _, bfirst, bcount, _, _ = slice_blocks(sigs)
+    full = np.nonzero(bcount == 4096)[0][:16]
+    lo, hi = int(bfirst[full[0]]), int(bfirst[full[-1]]) + 4096
+    nodes = np.ascontiguousarray(slice_t[lo:hi].cpu().numpy().view(np.uint64))
+    check(nodes, (bfirst[full] - lo).astype(np.int64), bcount[full].astype(np.int32), 0, range(len(full)))
