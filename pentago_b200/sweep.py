@@ -271,8 +271,12 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
                 timings[slice_]["arena_GB"] = 64 * sum(h.shape[0] for h in halves) / 1e9
         child, child_sigs = parent, sigs
     if halves is not None:
-        halves = None
-        torch.cuda.empty_cache()   # the half without the last slice
+        # back to the device: the half without the last slice, or both halves
+        # when the caller does not keep the last slice
+        halves = parent = None
+        if not keep_last:
+            child = None
+        torch.cuda.empty_cache()
     if keep_last:
         return results, child, child_sigs
     return results
