@@ -27,6 +27,8 @@ Fixtures written:
   counts_28_29.npz   the rows of data/counts-{28,29}.npy for the sections of the
                      28-stone root DEEP_ROOT at slices 28 and 29 (with
                      counts_30_35.npz, every section of its sweep)
+  end_totals.json    the node, block and line totals of every 24-stone section
+                     in pentago/end/end_test.cc (TEST(end, simple_partition))
 """
 import ctypes
 import json
@@ -177,6 +179,12 @@ def main(ref_root):
                         **{f"counts_{s}": np.load(os.path.join(ref_root, "data", f"counts-{s}.npy")) for s in range(6)})
     # 10. counts of the deep root's sections at slices 28 and 29
     deep_root_counts(ref_root)
+    # 11. slice totals of end_test.cc
+    et = src("pentago/end/end_test.cc")
+    m = re.search(r"TEST\(end, simple_partition\) \{.*?stones = (\d+);\s*const uint64_t total = (\d+),\s*"
+                  r"total_blocks = (\d+);.*?total_lines = (\d+);", et, re.S)
+    json.dump({"slice": int(m.group(1)), "nodes": int(m.group(2)), "blocks": int(m.group(3)),
+               "lines": int(m.group(4))}, open(os.path.join(HERE, "end_totals.json"), "w"))
     print("wrote fixtures to", HERE)
 
 

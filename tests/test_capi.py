@@ -138,3 +138,46 @@ def test_sweep_arena_halves_hold_every_adjacent_pair():
     assert round(64 * sum(halves) / 1e9, 1) == 141.7
     # every slice fits the half it is placed in
     assert all(n <= halves[k % 2] for k, n in enumerate(nodes))
+
+
+def all_sections(slice_):
+    """Every standardized section of a slice (all_boards_sections(slice, 8),
+    pentago/base/all_boards.cc): each split of the stones over the quadrants,
+    through pg_section_standardize, without duplicates."""
+    from pentago_b200 import capi
+    from pentago_b200.end import section_sig
+    L = capi.lib()
+    std, tr = ctypes.c_uint64(), ctypes.c_int32()
+    pairs = [(b, w) for b in range(10) for w in range(10) if b + w <= 9]
+    seen = set()
+
+    def rec(cs, black, white):
+        if len(cs) == 3:
+            if black + white <= 9:
+                capi.check(L.pg_section_standardize(ctypes.c_uint64(section_sig(cs + [[black, white]])),
+                                                    ctypes.byref(std), ctypes.byref(tr)))
+                seen.add(int(std.value))
+            return
+        for b, w in pairs:
+            if b <= black and w <= white:
+                rec(cs + [[b, w]], black - b, white - w)
+    rec([], (slice_ + 1) // 2, slice_ // 2)
+    return np.array(sorted(seen), np.uint64)
+
+
+def test_slice_totals_match_end_test():
+    """The nodes, 8^4 blocks and block lines (dimensions whose quadrant is
+    not full) of every 24-stone section, from the library's section algebra
+    and shapes, equal the totals in pentago/end/end_test.cc."""
+    from pentago_b200 import sweep
+    from pentago_b200.end import section_shape
+    gold = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "end_totals.json")))
+    sigs = all_sections(gold["slice"])
+    blocks = lines = 0
+    for s in sigs:
+        nb = (np.array(section_shape(int(s))) + 7) // 8
+        blocks += int(np.prod(nb))
+        counts = [[(int(s) >> (16 * q + 8 * k)) & 255 for k in range(2)] for q in range(4)]
+        lines += sum(int(np.prod(np.delete(nb, d))) for d in range(4) if sum(counts[d]) < 9)
+    assert int(sweep.slice_layout(sigs)[-1]) == gold["nodes"]
+    assert blocks == gold["blocks"] and lines == gold["lines"]
