@@ -181,3 +181,22 @@ def test_slice_totals_match_end_test():
         lines += sum(int(np.prod(np.delete(nb, d))) for d in range(4) if sum(counts[d]) < 9)
     assert int(sweep.slice_layout(sigs)[-1]) == gold["nodes"]
     assert blocks == gold["blocks"] and lines == gold["lines"]
+
+
+def test_block_enumerations_agree_and_tile_the_slice():
+    """The three host enumerations of a slice's 8^4 blocks (slice files,
+    compressed slices, the learned coder) give the same node offsets and
+    counts, and the blocks tile the slice tensor exactly, on a slice with
+    ragged sections."""
+    from pentago_b200 import learned, slice_store, supertensor, sweep
+    from pentago_b200.end import section_sig
+    sigs = sweep.descendent_sections(section_sig([[4, 4], [4, 5], [4, 3], [3, 3]]), 33)
+    layout = sweep.slice_layout(sigs)
+    _, first, count, _, _ = slice_store.slice_blocks(sigs)
+    _, _, offs, total = supertensor._slice_blocks(sigs)
+    _, loffs, lcount = learned.slice_blocks(sigs, layout)
+    assert np.array_equal(first, offs) and np.array_equal(first, loffs)
+    assert np.array_equal(count, lcount)
+    assert total == int(layout[-1]) == int(count.sum())
+    assert first[0] == 0 and np.array_equal(first[1:], first[:-1] + count[:-1])
+    assert (count < 4096).any() and (count == 4096).any()
