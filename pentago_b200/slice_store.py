@@ -127,3 +127,103 @@ class compressed_slice:
             if (status.cpu().numpy() != self.count[a:b]).any():
                 raise capi.PentagoError(capi.PG_ERR_FORMAT, "a compressed block did not decode")
         return out
+
+
+# ---------------------------------------------------------------------------
+# Measurement
+
+TIMING_ROOT = [[4, 4], [4, 5], [4, 3], [3, 3]]   # its slice 33: 35.4 GB in 10 sections
+SMALL_ROOT = [[4, 4], [5, 4], [4, 5], [4, 3]]    # its slice 34: 2.7 GB in 2 sections
+
+
+def _coder_case(root, slice_, max_nodes, largest_section, reps):
+    """Solve root's slices down to slice_, take a batch of at most max_nodes
+    nodes of consecutive blocks (from the largest section, or from the slice's
+    start), and time the table, encode and decode kernels on it with CUDA
+    events (each run once untimed, then reps times); check the round trip."""
+    import torch
+    from . import sweep
+    from .end import section_sig
+    L = capi.lib()
+    capi.check(L.pg_init())
+    _, nodes, sigs = sweep.sweep(section_sig(root), min_slice=slice_, keep_last=True)
+    _, first, count, sec_first, base = slice_blocks(sigs)
+    dev = nodes.device
+    i = int(np.argmax(np.diff(base))) if largest_section else 0
+    lo, hi = (int(sec_first[i]), int(sec_first[i + 1])) if largest_section else (0, len(count))
+    b1, used = lo, 0
+    while b1 < hi and used + count[b1] <= max_nodes:
+        used += int(count[b1])
+        b1 += 1
+    k = b1 - lo
+    turn = slice_ & 1
+    t64 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64)).to(dev)
+    d_first, d_count = t64(first[lo:b1]), torch.from_numpy(count[lo:b1].astype(np.int32)).to(dev)
+    table = torch.empty(3 * 1024, dtype=torch.int16, device=dev)
+    caps = (store_bound(count[lo:b1]) + 15) // 16 * 16
+    off = np.zeros(k + 1, np.int64)
+    off[1:] = np.cumsum(caps)
+    out = torch.empty(int(off[-1]), dtype=torch.uint8, device=dev)
+    d_off = t64(off[:-1])
+    sizes = torch.zeros(k, dtype=torch.int64, device=dev)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fn()
+        torch.cuda.synchronize()
+        if not reps:
+            return None
+        a.record()
+        for _ in range(reps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    ms_table = timed(lambda: capi.check(L.pg_store_table(nodes.data_ptr(), d_first.data_ptr(), d_count.data_ptr(),
+                                                         k, turn, table.data_ptr(), None)))
+    ms_encode = timed(lambda: capi.check(L.pg_store_encode(nodes.data_ptr(), d_first.data_ptr(), d_count.data_ptr(),
+                                                           k, turn, table.data_ptr(), out.data_ptr(), d_off.data_ptr(),
+                                                           sizes.data_ptr(), None)))
+    sz = sizes.cpu().numpy()
+    dst = torch.empty((used, 8), dtype=torch.int64, device=dev)
+    status = torch.zeros(k, dtype=torch.int64, device=dev)
+    d_sz, d_dst = t64(sz), t64(first[lo:b1] - first[lo])
+    ms_decode = timed(lambda: capi.check(L.pg_store_decode(out.data_ptr(), d_off.data_ptr(), d_sz.data_ptr(),
+                                                           d_count.data_ptr(), d_dst.data_ptr(), k, turn,
+                                                           table.data_ptr(), dst.data_ptr(), status.data_ptr(), None)))
+    ok = bool(torch.equal(dst, nodes[int(first[lo]):int(first[lo]) + used]))
+    symbols = used * 256
+    rate = lambda ms: symbols / (ms / 1e3) / 1e9 if ms else None
+    return {"root": root, "slice": slice_, "blocks": k, "nodes": used, "symbols": symbols,
+            "ratio": 64 * used / float(sz.sum()), "ms": {"table": ms_table, "encode": ms_encode, "decode": ms_decode},
+            "G_symbols_per_s": {"table": rate(ms_table), "encode": rate(ms_encode), "decode": rate(ms_decode)},
+            "roundtrip": ok}
+
+
+def main():
+    """Store-coder kernels on one batch of a solved slice.
+
+        python -m pentago_b200.slice_store           # 2^26 nodes of the largest
+                                                     # section of slice 33 of
+                                                     # [[4,4],[4,5],[4,3],[3,3]]
+        python -m pentago_b200.slice_store --small   # 2^24 nodes of slice 34 of
+                                                     # [[4,4],[5,4],[4,5],[4,3]],
+                                                     # each kernel once (profiling)
+    """
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description="store-coder kernels on one batch of a solved slice")
+    ap.add_argument("--small", action="store_true", help="the small case: few GB on the device, one run per kernel")
+    args = ap.parse_args()
+    if args.small:
+        res = _coder_case(SMALL_ROOT, 34, 1 << 24, largest_section=False, reps=0)
+    else:
+        res = _coder_case(TIMING_ROOT, 33, 1 << 26, largest_section=True, reps=3)
+    print(json.dumps(res))
+    if not res["roundtrip"]:
+        raise SystemExit("store coder round trip failed")
+
+
+if __name__ == "__main__":
+    main()
