@@ -15,6 +15,7 @@ engine's [we win, we win or tie] with turn = 0 / 1 (side to move).
 """
 import ctypes
 import os
+import struct
 
 import numpy as np
 
@@ -344,6 +345,95 @@ def read_slice(path, sigs=None, threads=0, stream=None, out=None):
                                                      threads, capi.stream_handle(stream)))
     f.close()
     return slice_, sigs, out
+
+
+# ---------------------------------------------------------------------------
+# Slice index files (.pentago.index, pentago/high/index.h, index.cc)
+#
+# A 20-byte magic, the slice (u32), then for every section of the slice in
+# descendent_sections(empty board, slice) order and every block of it in
+# row-major order a 12-byte blob: the block's file offset (u64, as two u32
+# words, low first) and compressed size (u32), all little endian.  A reader
+# with random access to the .pentago file fetches a block's blob at a
+# computable offset, then the block's bytes.
+
+INDEX_MAGIC = b"pentago index      \n"
+INDEX_HEAD = 24
+INDEX_BLOB = 12
+
+
+def index_sections(slice_):
+    """Every section of a slice in the index order (all sections reachable
+    from the empty board, sorted as descendent_sections sorts them)."""
+    from .sweep import descendent_sections
+    return descendent_sections(0, slice_)
+
+
+def _section_block_counts(sigs):
+    return [int(np.prod((np.asarray(section_shape(int(s)), np.int64) + 7) // 8)) for s in sigs]
+
+
+def write_index(path, slice_paths):
+    """Write the .pentago.index of a complete slice held in the given slice
+    files (write_supertensor_index, pentago/high/index.cc:82-118): every
+    section of the slice must be in some file, with block size 8 and the
+    interleave filter.  Returns the index bytes."""
+    if isinstance(slice_paths, (str, bytes, os.PathLike)):
+        slice_paths = [slice_paths]
+    readers = {}
+    slice_ = None
+    for p in slice_paths:
+        for r in open_supertensors(p):
+            if r.header.filter != 1 or r.header.block_size != 8:
+                raise ValueError("an index covers interleave-filtered files of block size 8")
+            if slice_ is None:
+                slice_ = r.header.stones
+            elif r.header.stones != slice_:
+                raise ValueError("the files hold more than one slice")
+            readers[int(r.header.section)] = r
+    if slice_ is None:
+        raise ValueError("no sections")
+    sigs = index_sections(slice_)
+    missing = [int(s) for s in sigs if int(s) not in readers]
+    if missing:
+        raise KeyError(f"the slice's sections {missing} are in none of the files")
+    parts = [INDEX_MAGIC, struct.pack("<I", slice_)]
+    for sig in sigs:
+        r = readers[int(sig)]
+        for b in r.header.all_blocks():
+            _, size, offset = r.blob(b)
+            parts.append(struct.pack("<III", offset & 0xffffffff, offset >> 32, size))
+    data = b"".join(parts)
+    assert len(data) == INDEX_HEAD + INDEX_BLOB * sum(_section_block_counts(sigs))
+    with open(path, "wb") as f:
+        f.write(data)
+    return data
+
+
+def index_blob_location(slice_, section, block):
+    """(offset, size) of a block's blob in the slice's index file
+    (supertensor_index_t::blob_location, index.cc:48-59)."""
+    sigs = index_sections(slice_)
+    where = {int(s): i for i, s in enumerate(sigs)}
+    if int(section) not in where:
+        raise KeyError(f"section {section:#x} is not in slice {slice_}")
+    i = where[int(section)]
+    B = (np.asarray(section_shape(int(section)), np.int64) + 7) // 8
+    if any(not 0 <= int(block[k]) < int(B[k]) for k in range(4)):
+        raise IndexError(f"block {tuple(block)} outside {tuple(B)}")
+    flat = int(np.ravel_multi_index(tuple(int(x) for x in block), tuple(int(x) for x in B)))
+    base = INDEX_HEAD + INDEX_BLOB * sum(_section_block_counts(sigs[:i]))
+    return base + INDEX_BLOB * flat, INDEX_BLOB
+
+
+def index_block_location(blob):
+    """(offset, compressed size) of a block in the .pentago file from its
+    12-byte blob (supertensor_index_t::block_location, index.cc:61-67)."""
+    blob = bytes(blob)
+    if len(blob) != INDEX_BLOB:
+        raise ValueError(f"expected {INDEX_BLOB} bytes, got {len(blob)}")
+    lo, hi, size = struct.unpack("<III", blob)
+    return lo | hi << 32, size
 
 
 # ---------------------------------------------------------------------------

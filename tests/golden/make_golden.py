@@ -19,7 +19,9 @@ Fixtures written:
                      pentago/data/supertensor_test.cc, with the order in which that
                      test writes its blocks (its unordered_map's iteration order,
                      taken from the reference compiled in place)
-  db/slice-N.pentago the reference's solved database for slices 0..5 (data/), and
+  db/slice-N.pentago the reference's solved database for slices 0..5 (data/), its
+                     index files (slice-N.pentago.index), the sizes of the index
+                     files of slices 6..8 (index_sizes.json), and
   counts_0_5.npz     its per-section counts (data/counts-{0..5}.npy)
   shards.json        pentago/shard/sharder_test.cc's server-verified (board, value)
                      samples of shard 7 of 32 over slices 0..5, and the per-slice
@@ -165,6 +167,12 @@ def main(ref_root):
     for s in range(6):
         shutil.copyfile(os.path.join(ref_root, "data", f"slice-{s}.pentago"),
                         os.path.join(HERE, "db", f"slice-{s}.pentago"))
+        shutil.copyfile(os.path.join(ref_root, "data", f"slice-{s}.pentago.index"),
+                        os.path.join(HERE, "db", f"slice-{s}.pentago.index"))
+    # sizes of the index files whose slices are not copied (slice 6) or not
+    # shipped with the reference (slices 7 and 8)
+    json.dump({str(s): os.path.getsize(os.path.join(ref_root, "data", f"slice-{s}.pentago.index"))
+               for s in (6, 7, 8)}, open(os.path.join(HERE, "index_sizes.json"), "w"))
     # 9. shard samples and entry counts
     sh = src("pentago/shard/sharder_test.cc")
     pairs = re.findall(r"\{(\d+),(-?\d+)\}", re.search(r"server_values = \{(.*?)\};", sh, re.S).group(1))

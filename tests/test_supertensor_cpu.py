@@ -290,3 +290,35 @@ def test_writer_errors(O, tmp_path):
     assert os.path.exists(path)
     w.close()
     assert not os.path.exists(path)   # an unfinished file is removed
+
+
+def test_slice_index_files_match_the_reference():
+    """The .pentago.index of each solved slice 0..5 written from the slice
+    file equals the reference's index file byte for byte
+    (pentago/high/index.cc write_supertensor_index); every block's blob,
+    located through the index, gives the offset and compressed size that the
+    reader reports; the index layout predicts the size of the reference's
+    index files of slices 6..8."""
+    import json
+    import tempfile
+    from pentago_b200 import supertensor as S
+    rng = np.random.default_rng(6)
+    for s in range(6):
+        path = os.path.join(GOLDEN, "db", f"slice-{s}.pentago")
+        want = open(path + ".index", "rb").read()
+        with tempfile.TemporaryDirectory() as d:
+            data = S.write_index(os.path.join(d, "slice.index"), path)
+        assert data == want, s
+        readers = S.open_supertensors(path)
+        for r in [readers[i] for i in rng.choice(len(readers), min(4, len(readers)), replace=False)]:
+            for b in r.header.all_blocks():
+                off, size = S.index_blob_location(s, r.header.section, b)
+                assert size == S.INDEX_BLOB
+                _, compressed, offset = r.blob(b)
+                assert S.index_block_location(data[off:off + size]) == (offset, compressed)
+    sizes = json.load(open(os.path.join(GOLDEN, "index_sizes.json")))
+    for s, n in sizes.items():
+        sigs = S.index_sections(int(s))
+        assert S.INDEX_HEAD + S.INDEX_BLOB * sum(S._section_block_counts(sigs)) == n, s
+    with pytest.raises(IndexError):
+        S.index_blob_location(5, int(S.index_sections(5)[0]), (60, 0, 0, 0))
