@@ -436,6 +436,28 @@ def index_block_location(blob):
     return lo | hi << 32, size
 
 
+def index_read_block_filtered(pentago_path, index_data, slice_, section, block, expected_size=None):
+    """A block's decompressed on-disk bytes (filtered as stored), fetched the
+    way a byte-range reader does: its blob from the index, then its bytes
+    from the .pentago file (supertensor_index_t::unpack_block's decompress,
+    index.cc:69-74; xz streams are told from zlib ones by the xz magic, as
+    pentago/data/compress.cc:37-40 does).  The GPU unfilter
+    (pg_supertensor_unfilter) turns them into nodes."""
+    import lzma
+    import zlib
+    off, size = index_blob_location(slice_, section, block)
+    offset, csize = index_block_location(bytes(index_data[off:off + size]))
+    with open(pentago_path, "rb") as f:
+        f.seek(offset)
+        raw = f.read(csize)
+    if len(raw) != csize:
+        raise IOError(f"{pentago_path}: block {tuple(block)} of section {section:#x} is truncated")
+    data = lzma.decompress(raw) if raw[:6] == b"\xfd7zXZ\x00" else zlib.decompress(raw)
+    if expected_size is not None and len(data) != expected_size:
+        raise ValueError(f"block {tuple(block)}: {len(data)} bytes, expected {expected_size}")
+    return np.frombuffer(data, np.uint8)
+
+
 # ---------------------------------------------------------------------------
 # Measurement
 

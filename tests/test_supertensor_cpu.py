@@ -314,8 +314,10 @@ def test_slice_index_files_match_the_reference():
             for b in r.header.all_blocks():
                 off, size = S.index_blob_location(s, r.header.section, b)
                 assert size == S.INDEX_BLOB
-                _, compressed, offset = r.blob(b)
+                uncompressed, compressed, offset = r.blob(b)
                 assert S.index_block_location(data[off:off + size]) == (offset, compressed)
+                got = S.index_read_block_filtered(path, data, s, r.header.section, b, uncompressed)
+                assert np.array_equal(got, r.read_block_filtered(b))
     sizes = json.load(open(os.path.join(GOLDEN, "index_sizes.json")))
     for s, n in sizes.items():
         sigs = S.index_sections(int(s))
