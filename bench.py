@@ -57,17 +57,59 @@ def max_over_ranks(x, world, device):
     return float(t.item())
 
 
+def section_sig(counts):
+    """section_t::sig() (pentago/base/section.h:35-42) of [[b0,w0],...,[b3,w3]]."""
+    return sum(int(counts[q][k]) << (16 * q + 8 * k) for q in range(4) for k in range(2))
+
+
+def synthetic():
+    """The seeded child generator (pentago_b200/synthetic.py), loaded by file
+    path so that the reference arm imports nothing of the package."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_bench_synthetic", os.path.join(ROOT, "pentago_b200", "synthetic.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def line_seed(t, dim):
+    """Seed of the children of the line along `dim` through benchmark block t."""
+    return 1000003 * t + dim
+
+
 def plan_lines(blocks, rank):
     """Line descriptors (without buffers) for this rank's blocks."""
     from pentago_b200 import end
-    sig = end.section_sig(SECTION)
+    sig = section_sig(SECTION)
     lines = []
     for t, b in enumerate(rank_blocks(blocks, rank)):
         for dim in range(4):
             bb = tuple(b[i] for i in range(4) if i != dim)
             line = end.Line(sig, dim, bb)
-            lines.append((line, end.line_info(line), 1000003 * (rank * blocks + t) + dim))
+            lines.append((line, end.line_info(line), line_seed(rank * blocks + t, dim)))
     return lines
+
+
+def reference_lines(R, blocks, rank):
+    """The same lines as plan_lines, for the reference engine (oracle/_ref):
+    (dim, length, block_base, children, output) with line sizes from the
+    reference's own line_data_t."""
+    import ctypes
+    import numpy as np
+    syn = synthetic()
+    sig = section_sig(SECTION)
+    shape = (ctypes.c_int32 * 4)()
+    R.lib.ref_section_shape(ctypes.c_uint64(sig), shape)
+    work = []
+    for t, b in enumerate(rank_blocks(blocks, rank)):
+        for dim in range(4):
+            bb = (ctypes.c_uint8 * 3)(*[b[i] for i in range(4) if i != dim])
+            length = (shape[dim] + 7) // 8
+            nin, nout = ctypes.c_int64(), ctypes.c_int64()
+            R.line_sizes(sig, dim, length, bb, ctypes.byref(nin), ctypes.byref(nout))
+            work.append((dim, length, bb, syn.random_nodes(line_seed(rank * blocks + t, dim), nin.value),
+                         np.zeros((nout.value, 8), np.uint64)))
+    return work
 
 
 class ClockSampler:
@@ -115,63 +157,61 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def measured_hbm_peak():
+def measured_peaks():
     try:
-        p = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def measured_hbm_peak():
+    p = measured_peaks()
+    if "hbm_gbs" in p:
         return float(p["hbm_gbs"]), "measured"
-    except (OSError, KeyError, ValueError):
-        return 6650.0, "fallback"
+    return 6650.0, "fallback"
 
 
-def profiled(key):
-    """A figure of the line kernel's committed profile summary (a line
-    `key: value`), measured by ncu; None if absent."""
+def profiled(key, cast=float):
+    """A figure of the line kernel's committed ncu summary (a line
+    `key: value`); None if absent.  These come from an earlier capture, not
+    from this run, and the bench line says so."""
     try:
         for line in open(PROFILE):
             if line.startswith(key + ":"):
-                return float(line.split(":")[1])
-    except OSError:
+                return cast(line.split(":", 1)[1].strip())
+    except (OSError, ValueError):
         pass
     return None
 
 
-def profiled_traffic():
-    """DRAM bytes (read + write) per parent node of the line kernel, measured by
-    ncu on this workload at full size."""
-    return profiled("dram_bytes_per_parent_node")
+def profile_source():
+    return {"source": "profile", "kernel_version": profiled("kernel_version", str),
+            "captured": profiled("captured", str)}
 
 
 def profiled_limiter():
     """What bounds the line kernel instead of HBM: its issue and integer-ALU
-    pipe activity in the ncu capture of the profile summary."""
+    pipe activity in the committed ncu capture of the kernel."""
     issue, alu = profiled("issue_active_pct"), profiled("alu_pipe_active_pct")
     if issue is None or alu is None:
         return None
-    return {"kind": "integer ALU issue and latency", "issue_active_pct": issue, "alu_pipe_active_pct": alu,
-            "source": "ncu --set full of end_line_kernel (profiles/end_line_kernel.md)"}
+    return dict({"kind": "integer ALU issue and latency", "issue_active_pct": issue, "alu_pipe_active_pct": alu,
+                 "capture": "ncu --set full of one end_line_kernel launch, small case"}, **profile_source())
 
 
-def cpu_reference_rate(seconds=12.0, threads=0, passes=None, warmup=0):
-    """The reference's own CPU engine (oracle/_ref) on the four lines through
-    block (1,1,1,1) of the section, repeated for about `seconds` (or exactly
+def cpu_reference_rate(seconds=12.0, threads=0, passes=None, warmup=0, blocks=16, rank=0):
+    """The reference's own CPU engine (oracle/_ref) on the same block lines
+    as the GPU arm (the four lines through each of `blocks` benchmark
+    blocks, same children), repeated for about `seconds` (or exactly
     `passes` times after `warmup` untimed passes)."""
-    import ctypes
-    import numpy as np
     from tests.oracle import reference, P
-    from pentago_b200.synthetic import random_nodes
-    from pentago_b200 import end
     R = reference()
     if R is None:
         return None
     nthreads = R.lib.ref_threads(threads)
-    sig = end.section_sig(SECTION)
-    work = []
-    for dim in range(4):
-        bb = tuple(1 for i in range(4) if i != dim)
-        line = end.Line(sig, dim, bb)
-        info = end.line_info(line)
-        work.append((dim, line.length, (ctypes.c_uint8 * 3)(*bb), random_nodes(dim + 1, info.input_nodes),
-                     np.zeros((info.output_nodes, 8), np.uint64)))
+    sig = section_sig(SECTION)
+    work = reference_lines(R, blocks, rank)
+
     def one_pass():
         n = 0
         for dim, length, bb, inp, out in work:
@@ -190,8 +230,41 @@ def cpu_reference_rate(seconds=12.0, threads=0, passes=None, warmup=0):
             break
     return {"value": nodes * 256 / el, "unit": UNIT, "cores": nthreads, "kind": "reference", "passes": done,
             "ms_per_pass": 1e3 * el / done,
-            "sample": f"4 block lines through block (1,1,1,1) of section {SECTION}, {done} passes in {el:.1f} s "
-                      f"({nodes} parent nodes), reference engine oracle/_ref on {nthreads} threads"}
+            "sample": f"the {len(work)} block lines of the GPU step (4 through each of {blocks} blocks of section "
+                      f"{SECTION}, same children), {done} passes in {el:.1f} s ({nodes} parent nodes), "
+                      f"reference engine oracle/_ref on {nthreads} threads"}
+
+
+def check_against_reference(lines, blocks, rank, per_dim=None):
+    """Bit-exact check of the GPU's outputs for the bench lines (the last
+    timed step's) against the reference engine on the same children: every
+    line, or the first `per_dim` lines of each dimension."""
+    import ctypes
+    import hashlib
+    import numpy as np
+    from tests.oracle import reference, oracle, P
+    R = reference()
+    checker, C = ("reference", R) if R is not None else ("oracle", oracle())
+    sig = section_sig(SECTION)
+    syn = synthetic()
+    seen = [0, 0, 0, 0]
+    bad = []
+    checked = 0
+    for (line, info, seed) in lines:
+        d = line.dimension
+        if per_dim is not None and seen[d] >= per_dim:
+            continue
+        seen[d] += 1
+        inp = syn.random_nodes(seed, info.input_nodes)
+        want = np.zeros((info.output_nodes, 8), np.uint64)
+        C.compute_line(sig, d, line.length, (ctypes.c_uint8 * 3)(*line.block_base), P(inp), P(want), 0)
+        got = line.output.cpu().numpy().view(np.uint64)
+        checked += 1
+        if not np.array_equal(got, want):
+            bad.append({"dim": d, "block_base": list(line.block_base),
+                        "got_sha1": hashlib.sha1(got.tobytes()).hexdigest()[:16],
+                        "want_sha1": hashlib.sha1(want.tobytes()).hexdigest()[:16]})
+    return {"ok": not bad, "lines_checked": checked, "checker": checker, "mismatches": bad[:4]}
 
 
 SWEEP_ROOT = [[4, 4], [4, 5], [4, 3], [3, 3]]
@@ -401,9 +474,9 @@ def cpu_sweep_estimate(root_counts, timings, seconds_per_slice=1.5):
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return
-    # One step = one pass of the reference engine over the four lines through
-    # one block of the section (about 12 ms on 16 cores), so K steps stay short.
-    r = cpu_reference_rate(passes=max(1, args.steps), warmup=args.warmup)
+    # One step = one pass of the reference engine over the same block lines
+    # as one GPU step (4 lines through each of --blocks blocks).
+    r = cpu_reference_rate(passes=max(1, args.steps), warmup=args.warmup, blocks=args.blocks)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
         return
@@ -411,13 +484,24 @@ def run_reference_arm(args, rank, world):
             "warmup": args.warmup, "ms_per_step": r["ms_per_pass"], "higher_is_better": True,
             "impl": "reference", "dtype": "u64 bitsets",
             "data": "synthetic",
-            "config": {"workload": f"end-engine block compute: 4 full block lines through each of {args.blocks} "
-                                   f"8^4 blocks of the 30-stone section {SECTION} per GPU",
-                       "reference_step": "the 4 lines through one block per step (the rate is per position)",
-                       "host_cpu": True},
+            "config": workload_config(args.blocks, world, reference=True),
             "cpu_baseline": r, "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                        "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def workload_config(blocks, world, reference=False):
+    """The config object both arms print: the workload is the same lines."""
+    c = {"workload": f"end-engine block compute: 4 full block lines through each of {blocks} "
+                     f"8^4 blocks of the 30-stone section {SECTION} per GPU",
+         "blocks_per_gpu": blocks, "lines_per_gpu": 4 * blocks,
+         "positions": "parent nodes written by each line x 256 rotations: a parent node lies on the lines of "
+                      "its quadrant dimensions and is counted once per line, as the reference computes it "
+                      "(schedule_compute_line per line, OR-accumulated)",
+         "l2": "inputs+outputs exceed L2; no flush between steps", "parallelism": f"lines sharded, dp{world}"}
+    if reference:
+        c["host_cpu"] = True
+    return c
 
 
 def main():
@@ -432,6 +516,8 @@ def main():
     ap.add_argument("--no-slice-files", action="store_true", help="skip the slice-file filter and I/O measurement")
     ap.add_argument("--no-sharder", action="store_true", help="skip the sharder measurement")
     ap.add_argument("--no-lookup", action="store_true", help="skip the board lookup measurement")
+    ap.add_argument("--no-parity", action="store_true", help="skip the check of the timed outputs")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -521,6 +607,10 @@ def main():
     kernel_ms = sum(a.elapsed_time(b) for a, b in zip(starts, stops)) / args.steps
     units_all = out_nodes * 256 * args.steps * world
     value = units_all / (elapsed_ms / 1e3)
+    # What the timed steps wrote, checked bit for bit against the reference
+    # engine on the same children (outside the timed region)
+    parity = None if args.no_parity else check_against_reference(lines, args.blocks, rank,
+                                                                   per_dim=None if world == 1 else 1)
 
     # End-to-end through the public API with host buffers.  The blocks go
     # through a three-stage pipeline: one stream copies every block in, one
@@ -552,23 +642,48 @@ def main():
         stream.wait_event(done)
         stream.synchronize()
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    barrier()
-    e_start = torch.cuda.Event(enable_timing=True)
-    e_stop = torch.cuda.Event(enable_timing=True)
+    def copy_step():
+        """The e2e step's copies alone, on the same streams and buffers: the
+        PCIe bound of the end-to-end figure."""
+        go = torch.cuda.Event()
+        go.record(stream)
+        for st in (h2d, d2h):
+            st.wait_event(go)
+        for (hi, di, ho, do) in blocks:
+            with torch.cuda.stream(h2d):
+                di.copy_(hi, non_blocking=True)
+            with torch.cuda.stream(d2h):
+                ho.copy_(do, non_blocking=True)
+        for st in (h2d, d2h):
+            done = torch.cuda.Event()
+            done.record(st)
+            stream.wait_event(done)
+        stream.synchronize()
+
+    def timed(fn, n):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        barrier()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        barrier()
+        return slowest(a.elapsed_time(b)) / n
+
     e2e_steps = max(2, min(20, args.steps // 2))
-    e_start.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
-    e_stop.record(stream)
-    barrier()
-    e2e_ms = slowest(e_start.elapsed_time(e_stop))
-    e2e_value = out_nodes * 256 * e2e_steps * world / (e2e_ms / 1e3)
+    e2e_ms = timed(e2e_step, e2e_steps)
+    e2e_value = out_nodes * 256 * world / (e2e_ms / 1e3)
+    copy_ms = timed(copy_step, e2e_steps)
+    copy_only = {"ms_per_step": copy_ms, "h2d_bytes": in_bytes, "d2h_bytes": out_bytes,
+                 "GBps_both_directions": (in_bytes + out_bytes) / (copy_ms / 1e3) / 1e9,
+                 "e2e_frac_of_copy_bound": copy_ms / e2e_ms}
 
     peak, peak_kind = measured_hbm_peak()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
-    traffic_per_node = profiled_traffic()
+    traffic_per_node = profiled("dram_bytes_per_parent_node")
     cpu = None
     midsolve = None
     learned = None
@@ -580,9 +695,16 @@ def main():
         cpu = cpu_reference_rate(seconds=12.0)
     if rank == 0 and world == 1:
         from pentago_b200 import mid
-        midsolve, raws0 = mid.bench_boards_26()
+        midsolve, raws0 = mid.bench_boards_26(sm_max_mhz=measured_peaks().get("sm_max_mhz", 1965.0))
         if not args.no_cpu_baseline:
             midsolve["cpu_baseline"] = cpu_midsolve_rate(raws0, midsolve["positions_per_batch"], seconds=8.0)
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        # Config 4: the continuous-batching server on a Poisson stream of
+        # 18..30-stone requests, against the same boards one at a time
+        from pentago_b200 import serve
+        serving = serve.bench()
+
     if rank == 0 and world == 1 and not args.no_learned:
         # The full sweep of SWEEP_ROOT, then the learned coder trained on its
         # 30-stone slice and run on a sample of 4096 of that slice's blocks
@@ -625,27 +747,35 @@ def main():
         if not args.no_cpu_baseline:
             lookups["cpu_baseline"] = cpu_lookup_rate(db, seconds=5.0)
 
+    parity_all = parity
+    if world > 1 and parity is not None:
+        ok = torch.tensor([1 if parity["ok"] else 0], dtype=torch.int32, device=dev)
+        dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+        parity_all = dict(parity, ok=bool(ok.item()), scope="rank 0's counts; ok is the AND over ranks")
     if rank == 0:
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64 bitsets", "data": "synthetic",
-            "config": {"workload": f"end-engine block compute: 4 full block lines through each of {args.blocks} "
-                                   f"8^4 blocks of the 30-stone section {SECTION} per GPU",
-                       "blocks_per_gpu": args.blocks, "lines_per_gpu": len(ls),
-                       "parent_nodes_per_step_per_gpu": out_nodes,
-                       "bytes_resident_per_gpu": in_bytes + out_bytes,
-                       "l2": "inputs+outputs exceed L2; no flush between steps", "parallelism": f"lines sharded, dp{world}"},
+            "config": dict(workload_config(args.blocks, world),
+                           parent_nodes_per_step_per_gpu=out_nodes, bytes_resident_per_gpu=in_bytes + out_bytes),
+            "parity": parity_all,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (traffic_per_node * out_nodes / 4) if traffic_per_node else None,
-                         "traffic_note": "dram read + write per launch (mean of the 4 dims), ncu at full size",
-                         "algorithmic_bytes_per_step": alg_bytes, "kernel": "end_line_kernel",
-                         "launches_per_step": 4, "limiter": profiled_limiter()},
+                         "traffic_note": "dram read + write per launch (mean of the 4 dims) from an earlier ncu "
+                                         "capture at full size, scaled by parent nodes",
+                         "traffic_source": profile_source(),
+                         "algorithmic_bytes_per_step": alg_bytes,
+                         "algorithmic_bytes": "64 B per child node read + 64 B per parent node written, per line",
+                         "kernel": "end_line_kernel", "launches_per_step": 4,
+                         "kernel_ms_per_step": kernel_ms, "limiter": profiled_limiter()},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": out_bytes,
+                    "ms_per_step": e2e_ms, "copy_only": copy_only},
             "gpu_launches": 4 * args.steps,
             "midsolve_64_boards_26_stones": midsolve,
+            "serving": serving,
             "sweep_root_30_stones": sweep2,
             "learned_rans_slice_30": learned,
             "slice_files": slice_files,

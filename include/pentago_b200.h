@@ -185,10 +185,10 @@ int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* s
 /* Midsolve that allocates nothing (no counterpart in the reference).
  *
  * For callers that cannot allocate device memory when they need a solve: code
- * running while a stream is captured into a CUDA graph, code whose framework
- * owns the device's memory pool, latency-critical loops that must not wait for
- * or fail in an allocation.  It gives the same results as pg_midsolve_batch
- * but uses only fixed device arrays that are part of the library image:
+ * whose framework owns the device's memory pool, and latency-critical loops
+ * that must not wait for or fail in an allocation.  It gives the same results
+ * as pg_midsolve_batch but uses only fixed device arrays that are part of the
+ * library image:
  * PG_NOALLOC_SCRATCH_BYTES of scratch (held on every GPU that loads the
  * library until the process exits) plus a fixed copy of the win-pattern
  * table.  The caller passes the inputs (host array of raw_t) and the outputs
@@ -199,9 +199,14 @@ int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* s
  *     than 10 empty spots) workspaces must fit in PG_NOALLOC_SCRATCH_BYTES
  *     together; otherwise the call returns PG_ERR_CAPACITY and does nothing.
  *     About 64 boards of 26+ stones, or one board of 22 stones, fit;
+ *   - every board is solved by one CTA; pg_midsolve_batch spreads boards
+ *     with more than 10 empty spots (25 stones or fewer) over many CTAs, so
+ *     such boards take far longer here;
+ *   - each call copies its boards' job descriptors from host memory to the
+ *     fixed array with cudaMemcpyAsync on the given stream;
  *   - the first call on a device sets that device up (it resolves the arrays'
- *     device addresses and fills the pattern table; no allocation).  Make that
- *     first call, with the device current, before any stream capture;
+ *     device addresses and fills the pattern table; no allocation), once, with
+ *     a lock, so threads may race to make it;
  *   - all calls share the one scratch array, which keeps the last call's
  *     contents; nothing in it needs to start at zero (every entry is written
  *     before it is read).  Calls whose kernels overlap on the GPU (for example

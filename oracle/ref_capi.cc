@@ -6,6 +6,7 @@
 // Every function mirrors one reference interface:
 //   ref_rmax / ref_super_wins        base/superscore.h:264-306, base/superscore.cc:38-96
 //   ref_transform_super               base/symmetry.cc:146-307
+//   ref_section_shape / ref_line_sizes base/section.h:73, end/compute.cc:24-46 (line_data_t)
 //   ref_compute_line                  end/compute.cc:55-123 (line_details_t) + :394-404
 //   ref_count_block_wins              end/block_store.cc:330-352
 //   ref_midsolve                      mid/midengine.cc:161-169 (+ midsolve_traverse :127-158)
@@ -131,6 +132,13 @@ void ref_halfsuper_rmax(const uint64_t* in, uint64_t* out, int n) {
     for (int r = 0; r < 128; r++)
       if (h[uint8_t(r)]) out[2 * i + (r >> 6)] |= uint64_t(1) << (r & 63);
   }
+}
+
+// section_t::shape (base/section.h:73): rotation-minimal quadrant counts.
+int ref_section_shape(uint64_t section_sig, int32_t* shape) {
+  const auto s = section_from_sig(section_sig).shape();
+  for (int i = 0; i < 4; i++) shape[i] = s[i];
+  return 0;
 }
 
 // Shapes for a line: fills input_nodes/output_nodes (node counts of the packed

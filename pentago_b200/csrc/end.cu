@@ -191,8 +191,10 @@ PG_HD uint2 table_entry(const uint2* f, uint64_t c0, int e) {
   return make_uint2(lo, hi);
 }
 
-// super_wins from the tables and the covered terms per rotation of DIM.
-template<int DIM>
+// super_wins from the tables and the covered terms per rotation of DIM, in
+// the line frame: axes DIM and 3 exchanged, so that rotation p of the line
+// quadrant is word pair p (words 2p, 2p + 1) and a translation along the
+// line's axis is a choice of pairs, not arithmetic.
 PG_HD super8 table_eval(const uint2* tab, const uint4 sub) {
   super8 r;
   const uint32_t S[4] = {sub.x, sub.y, sub.z, sub.w};
@@ -203,30 +205,73 @@ PG_HD super8 table_eval(const uint2* tab, const uint4 sub) {
     r.w[2 * d] = a.x | b.x | c.x | e.x;
     r.w[2 * d + 1] = a.y | b.y | c.y | e.y;
   }
-  if constexpr (DIM != 3) s_swap_axes<DIM, 3>(r);
   return r;
 }
 
-// Covered terms of stone pattern r of a side of the line quadrant.
+// Standard frame <-> line frame (exchanging axes DIM and 3 is its own
+// inverse).  For DIM 2 the exchange of index bits 4 and 6 moves 16-bit
+// halves between words (byte permutes) and that of bits 5 and 7 renames words.
+template<int DIM> PG_HD void s_line_frame(super8& s) {
+  if constexpr (DIM == 2) {
+#ifdef __CUDA_ARCH__
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const int w = (k & 1) | (k & 2) << 1;  // 0, 1, 4, 5
+      const uint32_t lo = s.w[w], hi = s.w[w | 2];
+      s.w[w] = __byte_perm(lo, hi, 0x5410);
+      s.w[w | 2] = __byte_perm(lo, hi, 0x7632);
+    }
+    uint32_t t = s.w[1]; s.w[1] = s.w[4]; s.w[4] = t;
+    t = s.w[3]; s.w[3] = s.w[6]; s.w[6] = t;
+#else
+    s_swap_axes<2, 3>(s);
+#endif
+  } else if constexpr (DIM < 2) {
+    s_swap_axes<DIM, 3>(s);
+  }
+}
+
+// Covered terms of the representative of rotation class r of a side's stone
+// patterns in the line quadrant.
 template<int DIM>
 PG_HD uint4 pattern_terms(const line_dev_t& L, const dev_tables_t& T, int side, int r) {
-  const int mask = ldg(T.pop_masks + L.pat_off[side] + r);
+  const int mask = ldg(T.cls_masks + L.pat_off[side] + r);
   return ldg(reinterpret_cast<const uint4*>(T.term_sub) + DIM * 512 + mask);
 }
 
-// Per-microline results live in shared memory as separate arrays of 16-byte
-// halves (structure of arrays): lanes reading different entries then spread
-// over the banks instead of colliding on the few positions an array of 32- or
-// 64-byte records leaves them.  Pattern results: entry e (the mover's
-// patterns, then the opponent's: pp in all) has half h at h * pp + e.
-// Children: quarter c of child j at c * nchild + j.
-PG_HD void pattern_store(uint4* pat, int e, int pp, const super8& w) {
-  pat[e] = make_uint4(w.w[0], w.w[1], w.w[2], w.w[3]);
-  pat[pp + e] = make_uint4(w.w[4], w.w[5], w.w[6], w.w[7]);
+// x = k n + i with 0 <= i < n, for 0 <= x < 2^20 and m = floor((2^32 - 1) / n):
+// the high product gives k exactly or one short.
+PG_HD void split(int x, int n, uint32_t m, int& k, int& i) {
+#ifdef __CUDA_ARCH__
+  k = int(__umulhi(uint32_t(x), m));
+#else
+  k = int((uint64_t(uint32_t(x)) * m) >> 32);
+#endif
+  i = x - k * n;
+  if (i >= n) { i -= n; k++; }
 }
-PG_HD super8 pattern_from(const uint4* pat, int e, int pp) {
-  const uint4 a = pat[e], b = pat[pp + e];
-  return super8{{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w}};
+
+// Per-microline results live in shared memory as structures of arrays, word
+// pair by word pair (lanes reading different entries then spread over the
+// banks).  Pattern results: rotation class e (the mover's classes, then the
+// opponent's: pp in all) has pair p at p * pp + e.  Children: pair p of Q_j
+// with its not-lost pair, one uint4, at p * nchild + j.
+PG_HD void pattern_store(uint2* pat, int e, int pp, const super8& w) {
+#pragma unroll
+  for (int p = 0; p < 4; p++) pat[p * pp + e] = make_uint2(w.w[2 * p], w.w[2 * p + 1]);
+}
+// super_wins of class e's representative rotated left rho times: rotating the
+// line quadrant shifts the rotation sets along its axis, so pair p of the
+// result is pair p + rho of the representative's.
+PG_HD super8 pattern_rotated(const uint2* pat, int e, int pp, int rho) {
+  super8 r;
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const uint2 a = pat[((p + rho) & 3) * pp + e];
+    r.w[2 * p] = a.x;
+    r.w[2 * p + 1] = a.y;
+  }
+  return r;
 }
 
 // Address of child j of a microline in the line's input.
@@ -238,67 +283,77 @@ PG_HD const uint64_t* child_addr(const line_dev_t& L, const microline_geom& G, i
   return L.input + 8 * idx;
 }
 
-// Child j (its node: cw = win, cn = not lost) -> Q_j, 4 uint4: win half then
-// not-lost half, both already moved into the parent's frame.
-PG_HD void child_node(const line_dev_t& L, const microline_geom& G, uint4* q, int j, const super8& cw,
-                      const super8& cn) {
+// Child j (its node: cw = win, cn = not lost) -> Q_j in the line frame, both
+// halves already moved into the parent's frame.  The win half also carries
+// W_j = super_wins of the mover's stones once the move is made (csub: the
+// terms they cover per rotation): a move that makes the child wins at once,
+// and super_wins of the moved quadrant is W_j translated by the move's
+// rotation exactly as the child's value is, so a parent ORs one translated
+// Q_j for both.
+template<int DIM>
+PG_HD void child_node(const line_dev_t& L, const microline_geom& G, const uint2* tab0, uint4* q, int j,
+                      const super8& cw, const super8& cn, const uint4 csub) {
   const int l = ladd(G.base_l, L.csym[j]);
   super8 qw = s_translate(s_rmax(s_not(cn)), l);
   super8 qn = s_translate(s_rmax(s_not(cw)), l);
   s_phi_runtime(qw, L.g);
   s_phi_runtime(qn, L.g);
+  s_line_frame<DIM>(qw);
+  s_line_frame<DIM>(qn);
+  qw = s_or(qw, table_eval(tab0, csub));
   const int nc = L.nchild;
-  q[j] = make_uint4(qw.w[0], qw.w[1], qw.w[2], qw.w[3]);
-  q[j + nc] = make_uint4(qw.w[4], qw.w[5], qw.w[6], qw.w[7]);
-  q[j + 2 * nc] = make_uint4(qn.w[0], qn.w[1], qn.w[2], qn.w[3]);
-  q[j + 3 * nc] = make_uint4(qn.w[4], qn.w[5], qn.w[6], qn.w[7]);
+#pragma unroll
+  for (int p = 0; p < 4; p++) q[p * nc + j] = make_uint4(qw.w[2 * p], qw.w[2 * p + 1], qn.w[2 * p], qn.w[2 * p + 1]);
 }
 
-// Parent i of a microline (compute.cc:308-356).
+// Parent i of a microline (compute.cc:308-356), in the line frame until its
+// store.  h is the first 16 bytes of its record, rec the record.
 template<int DIM>
-PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab0, const uint4* qs,
-                       const uint4* pats, const uint4 usub, const uint4 h, const uint4 mw, int i, unsigned* errors) {
-  // The parent's 48-byte record (parent_records): the terms covered after
-  // some move (usub), pattern ranks, and the child index and rotation (4 j +
-  // r) of every move.
-  const uint32_t mvw[5] = {h.y, h.z, h.w, mw.x, mw.y};
-  const int nmoves = int(h.x >> 16 & 0xff);
-  // super_wins of both sides, looked up by stone pattern
+PG_HD void parent_node(const line_dev_t& L, const microline_geom& G, const uint2* tab0, const uint4* qs,
+                       const uint2* pats, const uint4 h, const uint4* rec, int i, unsigned* errors) {
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
-  const super8 wins0 = pattern_from(pats, int(h.x & 0xff), pp);
-  const super8 wins1 = pattern_from(pats, p0 + int(h.x >> 8 & 0xff), pp);
-  // Every move wins immediately where super_wins(side0 | move) does; the
-  // union over the empty cells is one table evaluation of the union of the
-  // covered terms.
-  const super8 moved = table_eval<DIM>(tab0, usub);
-  super8 wins = moved, not_loss;
+  // super_wins of both sides, from their rotation classes
+  const super8 wins0 = pattern_rotated(pats, int(h.x & 0xff), pp, int(h.x >> 16 & 3));
+  const super8 wins1 = pattern_rotated(pats, p0 + int(h.x >> 8 & 0xff), pp, int(h.x >> 18 & 3));
+  super8 wins, not_loss;
   if (L.slice35) {
     // The board is full after the move: the child's value is immediate
-    // (compute.cc:329-333); rmax is OR-linear, so the union over moves works.
-    wins = s_or(wins, s_rmax(s_andnot(moved, wins1)));
+    // (compute.cc:329-333); the union over the empty cells of super_wins
+    // after the move is one table evaluation of the union of the covered
+    // terms, and rmax is OR-linear, so the union over moves works.
+    const super8 moved = table_eval(tab0, ldg(rec + 2));
+    wins = s_or(moved, s_rmax(s_andnot(moved, wins1)));
     not_loss = s_rmax(s_or(moved, s_not(wins1)));
   } else {
-    not_loss = s_zero();
+    wins = not_loss = s_zero();
+    const int nmoves = int(h.x >> 24);
+    const uint4 h2 = nmoves > 6 ? ldg(rec + 1) : make_uint4(0, 0, 0, 0);
+    const uint32_t mvw[5] = {h.y, h.z, h.w, h2.x, h2.y};
+    const int nc = L.nchild;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       if (k >= nmoves) break;
       const int ir = int(mvw[k >> 1] >> (16 * (k & 1)) & 0xffff);
       const int j = ir >> 2, r = ir & 3;
-      if (j >= L.nchild) { *errors |= 1u; continue; }
-      const int nc = L.nchild;
-      const uint4 a = qs[j], bq = qs[j + nc], cc = qs[j + 2 * nc], d = qs[j + 3 * nc];
-      const super8 qw = {{a.x, a.y, a.z, a.w, bq.x, bq.y, bq.z, bq.w}};
-      const super8 qn = {{cc.x, cc.y, cc.z, cc.w, d.x, d.y, d.z, d.w}};
-      wins = s_or(wins, s_translate_axis<DIM>(qw, r));
-      not_loss = s_or(not_loss, s_translate_axis<DIM>(qn, r));
+      if (j >= nc) { *errors |= 1u; continue; }
+#pragma unroll
+      for (int p = 0; p < 4; p++) {
+        const uint4 a = qs[((p + r) & 3) * nc + j];
+        wins.w[2 * p] |= a.x;
+        wins.w[2 * p + 1] |= a.y;
+        not_loss.w[2 * p] |= a.z;
+        not_loss.w[2 * p + 1] |= a.w;
+      }
     }
   }
   const super8 immediate = s_or(wins0, wins1);
-  const super8 r0 = s_or(s_andnot(wins, immediate), s_andnot(wins0, wins1));
-  const super8 r1 = s_or(s_andnot(not_loss, immediate), wins0);
+  super8 r0 = s_or(s_andnot(wins, immediate), s_andnot(wins0, wins1));
+  super8 r1 = s_or(s_andnot(not_loss, immediate), wins0);
+  s_line_frame<DIM>(r0);
+  s_line_frame<DIM>(r1);
   const int blk = i >> 3;
-  const int64_t oidx = L.out_off[blk] + (blk == L.length - 1 ? c.G.last_output_base : c.G.output_base) +
-                       int64_t(c.G.output_stride) * (i & 7);
+  const int64_t oidx = L.out_off[blk] + (blk == L.length - 1 ? G.last_output_base : G.output_base) +
+                       int64_t(G.output_stride) * (i & 7);
   uint64_t* out = L.output + 8 * oidx;
   if (L.flags & PG_LINE_OR) {
     s_store(out, s_or(s_load(out), r0));
@@ -309,24 +364,45 @@ PG_HD void parent_node(const line_dev_t& L, const micro_ctx& c, const uint2* tab
   }
 }
 
+// The subset tables of one side of a microline (sd: that side's stones in
+// the fixed quadrants), built by one warp: lane t < 17 computes term t,
+// lanes 17-31 the patterns that miss the line quadrant (ORed into c0).
+template<int DIM>
+__device__ __forceinline__ void warp_tables(const dev_tables_t& T, uint64_t sd, uint2* tab, int lane) {
+  const uint64_t f = lane < kTerms ? term_fixed<DIM>(T, lane, sd) : miss_fixed<DIM>(T, lane - kTerms, sd);
+  uint64_t c0 = lane < kTerms ? 0 : f;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) c0 |= __shfl_xor_sync(0xffffffffu, c0, o);
+#pragma unroll
+  for (int j = 0; j < (kTab + 31) / 32; j++) {
+    const int e = lane + 32 * j, c = table_chunk(e), sub = e - 16 * c;
+    uint64_t v = c ? 0 : c0;
+#pragma unroll
+    for (int b = 0; b < 5; b++) {
+      const uint64_t fb = __shfl_sync(0xffffffffu, f, 4 * c + b < kTerms ? 4 * c + b : 0);
+      if (sub >> b & 1) v |= fb;
+    }
+    if (e < kTab) tab[e] = make_uint2(uint32_t(v), uint32_t(v >> 32));
+  }
+}
+
 constexpr int kLineThreads = 256;
 constexpr int kMicro = 4;  // microlines per CTA
 
 __device__ void record_errors(unsigned e);
 
 // Static shared memory of a CTA: per microline its geometry and the mover's
-// subset tables (the parents evaluate them once more).
+// subset tables (the children and the 35-stone parents evaluate them again).
 struct cta_smem {
   micro_ctx ctx[kMicro];
   uint2 tab[kMicro][kTab];
 };
 
 // Dynamic shared memory: the stone-pattern results of every microline
-// (kMicro x 2 pp uint4), then the children (kMicro x 4 nchild uint4).  Until
+// (kMicro x 4 pp uint2), then the children (kMicro x 4 nchild uint4).  Until
 // the children are written their space holds the pattern set-up: the covered
-// terms of every pattern (pp uint4) and the opponent's subset tables
-// (kMicro x kTab uint2).  Sized per launch for its largest line, so that
-// three CTAs fit an SM on the longest lines of 30-stone sections.
+// terms of every pattern class (pp uint4) and the opponent's subset tables
+// (kMicro x kTab uint2).  Sized per launch for its largest line.
 PG_HD size_t pattern_bytes(int pp) { return size_t(kMicro) * pp * 32; }
 PG_HD size_t setup_bytes(int pp) { return size_t(pp) * 16 + size_t(kMicro) * kTab * 8; }
 inline size_t line_smem_bytes(int pp, int nchild) {
@@ -334,90 +410,88 @@ inline size_t line_smem_bytes(int pp, int nchild) {
 }
 const size_t kMaxLineSmem = line_smem_bytes(2 * kMaxPat, kMaxLine);
 
-// A CTA's microlines m0 .. m0 + M - 1.  Set-up: warp 2 k + side builds
-// microline k's geometry and that side's subset tables (lane t < 17: term t;
-// lanes 17-31: the patterns that miss the line quadrant, ORed into c0) while
-// the other threads stage the covered terms of every stone pattern; barrier;
-// super_wins of every stone pattern and all children into shared memory;
-// barrier; all parents.
+// A CTA's microlines m0 .. m0 + M - 1.  Set-up: lane k of warp 0 computes
+// microline k's geometry while the other threads stage the covered terms of
+// every pattern class; barrier; warp 2 k + side builds microline k's subset
+// tables for that side; barrier; super_wins of every pattern class (the
+// first children are loaded meanwhile); barrier; all children into shared
+// memory; barrier; all parents.
 template<int DIM>
 __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_tables_t& T, cta_smem& S,
                                                uint4* dyn, int m0, int M, int tid, int nt) {
   const int nc = L.nchild, np = L.nparent;
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
-  uint4* pats = dyn;                                   // microline k at 2 pp k
+  uint2* pats = reinterpret_cast<uint2*>(dyn);         // microline k at 4 pp k
   uint4* q_smem = dyn + kMicro * 2 * pp;               // microline k at 4 nc k
   uint4* psub = q_smem;                                // set-up scratch, until the children
   uint2* tab1 = reinterpret_cast<uint2*>(psub + pp);   // opponent's tables, microline k at kTab k
   const int warp = tid >> 5, lane = tid & 31;
+  if (tid < M) S.ctx[tid].G = microline_setup<DIM>(L, T, m0 + tid);
+  for (int x = tid; x < pp; x += nt) psub[x] = pattern_terms<DIM>(L, T, x >= p0, x >= p0 ? x - p0 : x);
+  __syncthreads();
   if (warp < 2 * M) {
     const int k = warp >> 1, side = warp & 1;
-    const microline_geom G = microline_setup<DIM>(L, T, m0 + k);
-    const uint64_t sd = side ? G.base_side1 : G.base_side0;
-    if (!side && !lane) S.ctx[k].G = G;
-    const uint64_t f = lane < kTerms ? term_fixed<DIM>(T, lane, sd) : miss_fixed<DIM>(T, lane - kTerms, sd);
-    uint64_t c0 = lane < kTerms ? 0 : f;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) c0 |= __shfl_xor_sync(0xffffffffu, c0, o);
-    uint2* tab = side ? tab1 + k * kTab : S.tab[k];
-#pragma unroll
-    for (int j = 0; j < (kTab + 31) / 32; j++) {
-      const int e = lane + 32 * j, c = table_chunk(e), sub = e - 16 * c;
-      uint64_t v = c ? 0 : c0;
-#pragma unroll
-      for (int b = 0; b < 5; b++) {
-        const uint64_t fb = __shfl_sync(0xffffffffu, f, 4 * c + b < kTerms ? 4 * c + b : 0);
-        if (sub >> b & 1) v |= fb;
-      }
-      if (e < kTab) tab[e] = make_uint2(uint32_t(v), uint32_t(v >> 32));
-    }
+    const microline_geom& G = S.ctx[k].G;
+    warp_tables<DIM>(T, side ? G.base_side1 : G.base_side0, side ? tab1 + k * kTab : S.tab[k], lane);
   }
-  for (int x = tid; x < pp; x += nt) psub[x] = pattern_terms<DIM>(L, T, x >= p0, x >= p0 ? x - p0 : x);
   __syncthreads();
   // Each thread's first child is loaded while the patterns are evaluated.
   super8 cw, cn;
-  if (!L.slice35 && tid < M * nc) {
-    const uint64_t* a = child_addr(L, S.ctx[tid / nc].G, tid % nc);
+  uint4 cs = make_uint4(0, 0, 0, 0);
+  const bool children = !L.slice35 && tid < M * nc;
+  if (children) {
+    int k, j;
+    split(tid, nc, L.split_m[1], k, j);
+    const uint64_t* a = child_addr(L, S.ctx[k].G, j);
     cw = s_load_ldg(a);
     cn = s_load_ldg(a + 4);
+    cs = ldg(reinterpret_cast<const uint4*>(L.crecs) + j);
   }
   for (int x = tid; x < M * pp; x += nt) {
-    const int k = x / pp, e = x - k * pp;
-    const super8 w = table_eval<DIM>(e >= p0 ? tab1 + k * kTab : S.tab[k], psub[e]);
-    pattern_store(pats + 2 * pp * k, e, pp, w);
+    int k, e;
+    split(x, pp, L.split_m[2], k, e);
+    const super8 w = table_eval(e >= p0 ? tab1 + k * kTab : S.tab[k], psub[e]);
+    pattern_store(pats + 4 * pp * k, e, pp, w);
   }
   __syncthreads();  // the set-up scratch is free from here on
-  if (!L.slice35 && tid < M * nc) {
+  if (children) {
     // Each thread's next child is loaded while it transforms the current one.
     for (int x = tid; x < M * nc; x += nt) {
-      const int k = x / nc, j = x - k * nc;
+      int k, j;
+      split(x, nc, L.split_m[1], k, j);
       const super8 w = cw, n = cn;
+      const uint4 s = cs;
       if (x + nt < M * nc) {
-        const int xn = x + nt;
-        const uint64_t* b = child_addr(L, S.ctx[xn / nc].G, xn % nc);
+        int kn, jn;
+        split(x + nt, nc, L.split_m[1], kn, jn);
+        const uint64_t* b = child_addr(L, S.ctx[kn].G, jn);
         cw = s_load_ldg(b);
         cn = s_load_ldg(b + 4);
+        cs = ldg(reinterpret_cast<const uint4*>(L.crecs) + jn);
       }
-      child_node(L, S.ctx[k].G, q_smem + 4 * k * nc, j, w, n);
+      child_node<DIM>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, j, w, n, s);
     }
   }
   __syncthreads();
   unsigned errors = 0;
-  // Each thread's next record is loaded while it computes the current parent.
+  // Each thread's next record header is loaded while it computes the current parent.
   const uint4* recs = reinterpret_cast<const uint4*>(L.recs);
-  uint4 r0 = make_uint4(0, 0, 0, 0), r1 = r0, r2 = r0;
+  uint4 h = make_uint4(0, 0, 0, 0);
   if (tid < M * np) {
-    const int i = tid % np;
-    r0 = ldg(recs + 3 * i); r1 = ldg(recs + 3 * i + 1); r2 = ldg(recs + 3 * i + 2);
+    int k, i;
+    split(tid, np, L.split_m[0], k, i);
+    h = ldg(recs + 3 * i);
   }
   for (int x = tid; x < M * np; x += nt) {
-    const int k = x / np, i = x - k * np;
-    const uint4 a = r0, b = r1, c = r2;
+    int k, i;
+    split(x, np, L.split_m[0], k, i);
+    const uint4 a = h;
     if (x + nt < M * np) {
-      const int in = (x + nt) % np;
-      r0 = ldg(recs + 3 * in); r1 = ldg(recs + 3 * in + 1); r2 = ldg(recs + 3 * in + 2);
+      int kn, in;
+      split(x + nt, np, L.split_m[0], kn, in);
+      h = ldg(recs + 3 * in);
     }
-    parent_node<DIM>(L, S.ctx[k], S.tab[k], q_smem + 4 * k * nc, pats + 2 * pp * k, a, b, c, i, &errors);
+    parent_node<DIM>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, pats + 4 * pp * k, a, recs + 3 * i, i, &errors);
   }
   if (errors) record_errors(errors);
 }
@@ -448,14 +522,14 @@ end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
 // the kernel arithmetic.  Never used by the device entry points.
 template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_tables_t& T) {
   const int pp = L.npat[0] + L.npat[1];
-  std::vector<uint4> q(4 * std::max(L.nchild, 1)), pat(2 * std::max(pp, 1));
+  std::vector<uint4> q(4 * std::max(L.nchild, 1));
+  std::vector<uint2> pat(4 * std::max(pp, 1));
   unsigned errors = 0;
-  micro_ctx c;
   uint2 fterm[kTerms], tab[2][kTab];
   for (int m = 0; m < L.cross[0] * L.cross[1] * L.cross[2]; m++) {
-    c.G = microline_setup<DIM>(L, T, m);
+    const microline_geom G = microline_setup<DIM>(L, T, m);
     for (int side = 0; side < 2; side++) {
-      const uint64_t sd = side ? c.G.base_side1 : c.G.base_side0;
+      const uint64_t sd = side ? G.base_side1 : G.base_side0;
       uint64_t c0 = 0;
       for (int u = 0; u < 15; u++) c0 |= miss_fixed<DIM>(T, u, sd);
       for (int t = 0; t < kTerms; t++) {
@@ -464,21 +538,50 @@ template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_table
       }
       for (int e = 0; e < kTab; e++) tab[side][e] = table_entry(fterm, c0, e);
       for (int r = 0; r < L.npat[side]; r++) {
-        const super8 w = table_eval<DIM>(tab[side], pattern_terms<DIM>(L, T, side, r));
+        const super8 w = table_eval(tab[side], pattern_terms<DIM>(L, T, side, r));
         pattern_store(pat.data(), side ? L.npat[0] + r : r, pp, w);
       }
     }
     if (!L.slice35)
       for (int j = 0; j < L.nchild; j++) {
-        const uint64_t* a = child_addr(L, c.G, j);
-        child_node(L, c.G, q.data(), j, s_load_ldg(a), s_load_ldg(a + 4));
+        const uint64_t* a = child_addr(L, G, j);
+        child_node<DIM>(L, G, tab[0], q.data(), j, s_load_ldg(a), s_load_ldg(a + 4),
+                        reinterpret_cast<const uint4*>(L.crecs)[j]);
       }
     for (int i = 0; i < L.nparent; i++) {
       const uint4* rp = reinterpret_cast<const uint4*>(L.recs + i);
-      parent_node<DIM>(L, c, tab[0], q.data(), pat.data(), rp[0], rp[1], rp[2], i, &errors);
+      parent_node<DIM>(L, G, tab[0], q.data(), pat.data(), rp[0], rp, i, &errors);
     }
   }
   return errors;
+}
+
+// The records of the (section, dimension) pairs of a set of lines, back to
+// back in one buffer of 16-byte words (each pair once).
+struct record_set {
+  std::vector<uint4> words;
+  std::vector<std::pair<uint64_t, std::pair<size_t, size_t>>> seen;
+  // Word offsets of the parent and the child records of (section, dim).
+  std::pair<size_t, size_t> add(uint64_t section, int dim) {
+    const uint64_t key = section << 2 | uint64_t(dim);
+    for (const auto& kv : seen) if (kv.first == key) return kv.second;
+    std::vector<parent_rec> recs;
+    std::vector<child_rec> crecs;
+    line_records(section, dim, recs, crecs);
+    std::pair<size_t, size_t> off(words.size(), 0);
+    const uint4* pw = reinterpret_cast<const uint4*>(recs.data());
+    words.insert(words.end(), pw, pw + 3 * recs.size());
+    off.second = words.size();
+    const uint4* cw = reinterpret_cast<const uint4*>(crecs.data());
+    words.insert(words.end(), cw, cw + crecs.size());
+    seen.emplace_back(key, off);
+    return off;
+  }
+};
+
+static void bind_line_records(line_dev_t& L, const uint4* base, std::pair<size_t, size_t> off) {
+  L.recs = reinterpret_cast<const parent_rec*>(base + off.first);
+  L.crecs = reinterpret_cast<const child_rec*>(base + off.second);
 }
 
 // A set of planned lines, grouped by dimension, with their descriptors on the device.
@@ -486,11 +589,11 @@ struct end_plan {
   std::vector<line_dev_t> host[4];
   line_dev_t* dev[4] = {nullptr, nullptr, nullptr, nullptr};
   int maxchild[4] = {0, 0, 0, 0};
-  int maxpat[4] = {0, 0, 0, 0};         // most stone patterns (both sides) of a line
-  // parent records of every (section, dimension) used, back to back
-  std::vector<parent_rec> recs;
-  std::vector<size_t> rec_off[4];       // per planned line: offset into recs
-  parent_rec* recs_dev = nullptr;
+  int maxpat[4] = {0, 0, 0, 0};         // most stone-pattern classes (both sides) of a line
+  // records of every (section, dimension) used
+  record_set recs;
+  std::vector<std::pair<size_t, size_t>> rec_off[4];  // per planned line: its records' word offsets
+  uint4* recs_dev = nullptr;
   // When the dimensions' lines are independent (dims_independent), the
   // launches of all but the first dimension run on side streams, forked from
   // and joined back into the caller's stream.
@@ -561,21 +664,11 @@ extern "C" int pg_line_info(const pg_line_t* line, pg_line_info_t* info) {
 
 static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
   std::string err;
-  std::vector<std::pair<uint64_t, size_t>> seen;  // (section << 2 | dim) -> offset into P.recs
-  std::vector<parent_rec> tmp;
   for (int i = 0; i < n; i++) {
     line_dev_t d;
     if (!plan_line(to_in(lines[i]), d, err)) return fail(PG_ERR_ARG, "line " + std::to_string(i) + ": " + err);
     if (!d.output || (!d.slice35 && !d.input)) return fail(PG_ERR_ARG, "null line buffer");
-    const uint64_t key = lines[i].section << 2 | lines[i].dimension;
-    size_t off = SIZE_MAX;
-    for (const auto& kv : seen) if (kv.first == key) off = kv.second;
-    if (off == SIZE_MAX) {
-      parent_records(lines[i].section, lines[i].dimension, tmp);
-      off = P.recs.size();
-      P.recs.insert(P.recs.end(), tmp.begin(), tmp.end());
-      seen.emplace_back(key, off);
-    }
+    const auto off = P.recs.add(lines[i].section, lines[i].dimension);
     P.maxchild[d.dim] = std::max(P.maxchild[d.dim], d.nchild);
     P.maxpat[d.dim] = std::max(P.maxpat[d.dim], d.npat[0] + d.npat[1]);
     P.host[d.dim].push_back(d);
@@ -637,10 +730,10 @@ static void release_plan(end_plan* P) {
   delete P;
 }
 
-static void bind_records(end_plan& P, parent_rec* recs_dev) {
+static void bind_records(end_plan& P, uint4* recs_dev) {
   P.recs_dev = recs_dev;
   for (int dim = 0; dim < 4; dim++)
-    for (size_t k = 0; k < P.host[dim].size(); k++) P.host[dim][k].recs = recs_dev + P.rec_off[dim][k];
+    for (size_t k = 0; k < P.host[dim].size(); k++) bind_line_records(P.host[dim][k], recs_dev, P.rec_off[dim][k]);
 }
 
 extern "C" int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream_) {
@@ -650,11 +743,12 @@ extern "C" int pg_end_compute_lines(const pg_line_t* lines, int n, void* stream_
   cudaStream_t stream = (cudaStream_t)stream_;
   end_plan P;
   if (int rc = plan_lines(lines, n, P)) return rc;
-  if (P.recs.empty()) return PG_OK;
+  if (P.recs.words.empty()) return PG_OK;
   stream_scratch X(stream);
-  parent_rec* recs = nullptr;
-  PG_CUDA(X.alloc(&recs, sizeof(parent_rec) * P.recs.size()));
-  PG_CUDA(cudaMemcpyAsync(recs, P.recs.data(), sizeof(parent_rec) * P.recs.size(), cudaMemcpyHostToDevice, stream));
+  const size_t rbytes = sizeof(uint4) * P.recs.words.size();
+  uint4* recs = nullptr;
+  PG_CUDA(X.alloc(&recs, rbytes));
+  PG_CUDA(cudaMemcpyAsync(recs, P.recs.words.data(), rbytes, cudaMemcpyHostToDevice, stream));
   bind_records(P, recs);
   int rc = PG_OK;
   for (int dim = 0; dim < 4 && !rc; dim++) {
@@ -673,10 +767,11 @@ extern "C" int pg_end_plan_create(const pg_line_t* lines, int n, pg_end_plan_t* 
   if (!device_tables()) return PG_ERR_CUDA;
   auto* P = new end_plan;
   if (int rc = plan_lines(lines, n, *P)) { delete P; return rc; }
-  if (!P->recs.empty()) {
-    parent_rec* recs = nullptr;
-    cudaError_t e = cudaMalloc(&recs, sizeof(parent_rec) * P->recs.size());
-    if (e == cudaSuccess) e = cudaMemcpy(recs, P->recs.data(), sizeof(parent_rec) * P->recs.size(), cudaMemcpyHostToDevice);
+  if (!P->recs.words.empty()) {
+    const size_t rbytes = sizeof(uint4) * P->recs.words.size();
+    uint4* recs = nullptr;
+    cudaError_t e = cudaMalloc(&recs, rbytes);
+    if (e == cudaSuccess) e = cudaMemcpy(recs, P->recs.words.data(), rbytes, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) { if (recs) cudaFree(recs); delete P; return cuda_fail(e, "pg_end_plan_create"); }
     bind_records(*P, recs);
   }
@@ -758,11 +853,13 @@ extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
   std::string err;
   unsigned errors = 0;
   std::vector<parent_rec> recs;
+  std::vector<child_rec> crecs;
   for (int i = 0; i < n; i++) {
     line_dev_t d;
     if (!plan_line(to_in(lines[i]), d, err)) return fail(PG_ERR_ARG, err);
-    parent_records(lines[i].section, lines[i].dimension, recs);
+    line_records(lines[i].section, lines[i].dimension, recs, crecs);
     d.recs = recs.data();
+    d.crecs = crecs.data();
     switch (d.dim) {
       case 0: errors |= host_line<0>(d, T); break;
       case 1: errors |= host_line<1>(d, T); break;
@@ -1118,11 +1215,10 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
   if (int rc = pg_slice_layout(parent_sigs, np, poff.data())) return rc;
   if (int rc = pg_slice_layout(child_sigs, nc, coff.data())) return rc;
   std::string err;
-  std::vector<parent_rec> tmp;
   for (int dim = 0; dim < 4; dim++) {
     std::vector<family_t> fams;
-    std::vector<parent_rec> recs;
-    std::vector<size_t> rec_off;
+    record_set recs;
+    std::vector<std::pair<size_t, size_t>> rec_off;
     int total = 0, maxchild = 0, maxpat = 0;
     for (int i = 0; i < np; i++) {
       const section_t sec = section_t::from_sig(parent_sigs[i]);
@@ -1139,16 +1235,15 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
       total += F.nlines;
       maxchild = std::max(maxchild, F.proto.nchild);
       maxpat = std::max(maxpat, F.proto.npat[0] + F.proto.npat[1]);
-      parent_records(sec.sig(), dim, tmp);
-      rec_off.push_back(recs.size());
-      recs.insert(recs.end(), tmp.begin(), tmp.end());
+      rec_off.push_back(recs.add(sec.sig(), dim));
     }
     if (fams.empty()) continue;
     stream_scratch X(stream);
-    parent_rec* recs_dev = nullptr;
-    PG_CUDA(X.alloc(&recs_dev, sizeof(parent_rec) * recs.size()));
-    PG_CUDA(cudaMemcpyAsync(recs_dev, recs.data(), sizeof(parent_rec) * recs.size(), cudaMemcpyHostToDevice, stream));
-    for (size_t f = 0; f < fams.size(); f++) fams[f].proto.recs = recs_dev + rec_off[f];
+    const size_t rbytes = sizeof(uint4) * recs.words.size();
+    uint4* recs_dev = nullptr;
+    PG_CUDA(X.alloc(&recs_dev, rbytes));
+    PG_CUDA(cudaMemcpyAsync(recs_dev, recs.words.data(), rbytes, cudaMemcpyHostToDevice, stream));
+    for (size_t f = 0; f < fams.size(); f++) bind_line_records(fams[f].proto, recs_dev, rec_off[f]);
     family_t* d = nullptr;
     PG_CUDA(X.alloc(&d, sizeof(family_t) * fams.size()));
     PG_CUDA(cudaMemcpyAsync(d, fams.data(), sizeof(family_t) * fams.size(), cudaMemcpyHostToDevice, stream));

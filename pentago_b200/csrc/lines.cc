@@ -161,9 +161,11 @@ bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error) {
   d.line_moves = d.refl_moves[d.child_dim];
   for (int side = 0; side < 2; side++) {  // stones of mover (side 0) and opponent in the line quadrant
     const int k = sec.c[dim][side ? 1 - d.turn : d.turn];
-    d.pat_off[side] = T.pop_off[k];
-    d.npat[side] = T.pop_off[k + 1] - T.pop_off[k];
+    d.pat_off[side] = T.cls_off[k];
+    d.npat[side] = T.cls_off[k + 1] - T.cls_off[k];
   }
+  const int counts[3] = {d.nparent, d.nchild, d.npat[0] + d.npat[1]};
+  for (int i = 0; i < 3; i++) d.split_m[i] = counts[i] > 0 ? 0xffffffffu / uint32_t(counts[i]) : 0u;
   d.input = in.input;
   d.output = in.output;
   if (s.input_blocks > kMaxBlocks || in.length > kMaxBlocks || d.nchild > kMaxLine) {
@@ -177,7 +179,7 @@ bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error) {
   return true;
 }
 
-void parent_records(uint64_t section, int dim, std::vector<parent_rec>& recs) {
+void line_records(uint64_t section, int dim, std::vector<parent_rec>& recs, std::vector<child_rec>& crecs) {
   const auto& T = tables();
   const section_t sec = section_t::from_sig(section);
   const int turn = sec.sum() & 1;
@@ -188,8 +190,9 @@ void parent_records(uint64_t section, int dim, std::vector<parent_rec>& recs) {
     const uint16_t q = T.rmin_flat[T.rmin_off[k] + i];
     const uint16_t s0 = T.unpack[q][turn], s1 = T.unpack[q][1 - turn];
     parent_rec& r = recs[i];
-    r.r0 = T.rank9[s0];
-    r.r1 = T.rank9[s1];
+    r.c0 = T.cls_rank[s0];
+    r.c1 = T.cls_rank[s1];
+    r.rot = uint8_t(T.cls_rot[s0] | T.cls_rot[s1] << 2);
     int m = 0;
     for (int b = 0, p3 = 1; b < 9; b++, p3 *= 3)
       if (!((s0 | s1) >> b & 1)) {
@@ -197,6 +200,17 @@ void parent_records(uint64_t section, int dim, std::vector<parent_rec>& recs) {
         for (int k = 0; k < 4; k++) r.usub[k] |= T.term_sub[dim][s0 | 1 << b][k];
       }
     r.nmoves = uint8_t(m);
+  }
+  crecs.clear();
+  if (sec.sum() < 35) {
+    const section_t child = sec.child(dim);
+    const int kc = rmin_bucket(child.c[dim][0], child.c[dim][1]);
+    const int nc = T.rmin_off[kc + 1] - T.rmin_off[kc];
+    crecs.assign(nc, child_rec{});
+    for (int j = 0; j < nc; j++) {
+      const uint16_t mover = T.unpack[T.rmin_flat[T.rmin_off[kc] + j]][turn];
+      for (int r = 0; r < 4; r++) crecs[j].csub[r] = T.term_sub[dim][mover][r];
+    }
   }
 }
 

@@ -32,15 +32,25 @@ constexpr int kMaxLine = 424;    // nodes along a quadrant axis, rounded up
 
 // Per-parent facts that depend only on the parent's quadrant along the line
 // (the same for every microline of every line of one section and
-// dimension), so the kernel reads them in three coalesced 16-byte loads.
+// dimension).  The kernel reads the first 16 bytes for every parent, the
+// second only when the line quadrant has more than 6 empty cells, the third
+// only on 35-stone sections.
 struct alignas(16) parent_rec {
-  uint32_t usub[4];    // win terms (term_sub) the mover covers after a stone on some empty cell, per rotation
-  uint8_t r0, r1;      // ranks of the mover's / opponent's stone patterns (rank9)
-  uint8_t nmoves, pad;
+  uint8_t c0, c1;      // rotation classes (cls_rank) of the mover's / opponent's stone patterns
+  uint8_t rot;         // bits 0-1 (2-3): the mover's (opponent's) pattern is its class rotated left this often
+  uint8_t nmoves;
   uint16_t mv[14];     // per empty cell, increasing: rotation_minimal_quadrants_inverse of the child quadrant
-                       // (4 j + r); at most 9 used
+                       // (4 j + r); at most 9 used, mv[0..5] in the first 16 bytes
+  uint32_t usub[4];    // win terms (term_sub) the mover covers after a stone on some empty cell, per rotation
 };
 static_assert(sizeof(parent_rec) == 48, "parent_rec layout");
+
+// Per child quadrant state j (index j of the rotation-minimal list of the
+// line quadrant after the move): the win terms the mover's stones cover, per
+// rotation of the quadrant.
+struct alignas(16) child_rec {
+  uint32_t csub[4];
+};
 
 // Everything a CTA needs to compute one microline of a line.  Plain data,
 // copied to the device as is.
@@ -52,11 +62,13 @@ struct alignas(16) line_dev_t {
   int32_t perm[4], refl_moves[4], block0[4], first_child_block[4];
   int32_t out_shape[4];
   int32_t rmin_off[4];              // offsets of the parent quadrant lists in rmin_flat
-  int32_t pat_off[2], npat[2];      // stone patterns of the line quadrant: mover, opponent
+  int32_t pat_off[2], npat[2];      // rotation classes of the line quadrant's stone patterns: mover, opponent
+  uint32_t split_m[3];              // floor((2^32 - 1) / n) for n = nparent, nchild, npat[0] + npat[1]
+  int32_t pad;
   const uint64_t* input;
   uint64_t* output;
   const parent_rec* recs;           // nparent records for this (section, dimension)
-  const void* pad_ptr;
+  const child_rec* crecs;           // nchild records for this (section, dimension)
   int64_t in_off[kMaxBlocks], out_off[kMaxBlocks];
   uint8_t csym[kMaxLine];           // reflection locals along the child dimension
   uint8_t xsym[4][8];               // reflection locals of the cross dimensions
@@ -82,10 +94,11 @@ struct line_shapes_t {
 
 // Validate and compute shapes; returns false with a message on bad input.
 bool line_shapes(const line_in_t& in, line_shapes_t& out, std::string& error);
-// Fill the device descriptor (recs is left null; see parent_records).
+// Fill the device descriptor (recs and crecs are left null; see line_records).
 bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error);
 
-// The parent records of a (section, dimension): nparent entries.
-void parent_records(uint64_t section, int dim, std::vector<parent_rec>& recs);
+// The records of a (section, dimension): nparent parent records and (below
+// 35 stones) nchild child records.
+void line_records(uint64_t section, int dim, std::vector<parent_rec>& recs, std::vector<child_rec>& crecs);
 
 }  // namespace pg

@@ -20,6 +20,7 @@
 // mid_values_t records.
 #include "mid_body.cuh"
 #include "runtime.h"
+#include <atomic>
 #include <algorithm>
 #include <condition_variable>
 #include <mutex>
@@ -386,14 +387,14 @@ extern "C" int pg_selftest_midsolve_groups_host(const uint64_t* raws, int n, int
 // Midsolve without allocation.
 //
 // Some callers cannot allocate device memory at the moment they want a
-// solve: code running while a CUDA stream is being captured into a graph
-// (where cudaMalloc is not allowed), code inside a framework whose memory pool
-// owns the whole device, or a real-time loop that must not pay for, or fail
-// in, an allocation.  pg_midsolve_batch_noalloc serves them with the same
-// kernel as pg_midsolve_batch, but every byte of device scratch it uses (the
-// boards' job descriptors, their per-level tables and, for boards with more
-// than 10 empty spots, their workspace) lives in one fixed array that is part
-// of the library image, plus a fixed copy of the win-pattern table.
+// solve: code inside a framework whose memory pool owns the whole device, or
+// a real-time loop that must not pay for, or fail in, an allocation.
+// pg_midsolve_batch_noalloc serves them with the board kernel of
+// pg_midsolve_batch (one CTA per board), but every byte of device scratch it
+// uses (the boards' job descriptors, their per-level tables and, for boards
+// with more than 10 empty spots, their workspace) lives in one fixed array
+// that is part of the library image, plus a fixed copy of the win-pattern
+// table.
 // ===========================================================================
 
 namespace pg {
@@ -408,16 +409,21 @@ static __device__ __align__(256) uint32_t noalloc_win_factors[4 * 512 * 16];
 struct noalloc_device {
   unsigned char* scratch = nullptr;   // device address of noalloc_scratch
   uint32_t* win_factors = nullptr;    // device address of noalloc_win_factors
+  std::atomic<bool> ready{false};     // set last, once both are valid
 };
 static noalloc_device noalloc_state[64];  // per device ordinal
+static std::mutex noalloc_mutex;
 
 // Per-device set-up on the first call with that device current: resolve the
 // device addresses of the two arrays (in host code their names are only
 // host-side stand-ins) and fill the win-pattern table.  Nothing here
-// allocates device memory.
+// allocates device memory.  Threads that race to make the first call wait on
+// the lock; the ready flag is published after the addresses.
 static int noalloc_setup(int dev) {
   noalloc_device& D = noalloc_state[dev];
-  if (D.scratch) return PG_OK;
+  if (D.ready.load(std::memory_order_acquire)) return PG_OK;
+  std::lock_guard<std::mutex> lock(noalloc_mutex);
+  if (D.ready.load(std::memory_order_relaxed)) return PG_OK;
   void* s = nullptr;
   void* w = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&s, noalloc_scratch);
@@ -430,6 +436,7 @@ static int noalloc_setup(int dev) {
   if (int rc = upload_consts()) return fail(rc, "midsolve constant upload failed");
   D.win_factors = static_cast<uint32_t*>(w);
   D.scratch = static_cast<unsigned char*>(s);
+  D.ready.store(true, std::memory_order_release);
   return PG_OK;
 }
 

@@ -67,9 +67,10 @@ const dev_tables_t* device_tables() {
   t->miss_quad = upload(&T.miss_quad[0][0][0], 4 * 15 * 3);
   t->rot = upload(&T.rot[0][0], 512 * 2);
   t->refl = upload(T.refl, 512);
+  t->cls_masks = upload(T.cls_masks, 512);
   if (!t->rmin_flat || !t->rmin_inv || !t->unpack || !t->win_factors || !t->rmin_off || !t->commute ||
       !t->win_union || !t->pack || !t->pop_masks || !t->rank9 || !t->term_pat || !t->term_other || !t->term_sub ||
-      !t->cov || !t->miss_pat || !t->miss_quad || !t->rot || !t->refl) {
+      !t->cov || !t->miss_pat || !t->miss_quad || !t->rot || !t->refl || !t->cls_masks) {
     set_error("table upload failed");
     delete t;
     return nullptr;
@@ -83,7 +84,7 @@ dev_tables_t host_tables_view() {
   return dev_tables_t{H.rmin_flat, H.rmin_inv, &H.unpack[0][0], &H.win_factors[0][0][0], H.rmin_off,
                       &H.commute[0][0], H.win_union.data(), H.pack, H.pop_masks, H.rank9,
                       &H.term_pat[0][0], &H.term_other[0][0][0], &H.term_sub[0][0][0], &H.cov[0][0][0],
-                      &H.miss_pat[0][0], &H.miss_quad[0][0][0], &H.rot[0][0], H.refl};
+                      &H.miss_pat[0][0], &H.miss_quad[0][0][0], &H.rot[0][0], H.refl, H.cls_masks};
 }
 
 }  // namespace pg

@@ -26,6 +26,7 @@ struct dev_tables_t {
   const uint8_t* miss_quad;    // 4 x 15 x 3
   const uint16_t* rot;         // 512 x 2: [left, right] rotation of a quadrant side
   const uint16_t* refl;        // 512: reflection of a quadrant side about x = y
+  const uint16_t* cls_masks;   // 512: rotation-class representatives, grouped by stone count
 };
 
 // Tables on the current device (uploaded on first use).  Returns nullptr and

@@ -262,6 +262,27 @@ void build_pop(tables_t& T) {
       if (__builtin_popcount(m) == k) { T.pop_masks[next++] = uint16_t(m); T.rank9[m] = uint8_t(r++); }
   }
   T.pop_off[10] = uint16_t(next);
+  // Rotation classes: each represented by its smallest mask
+  auto rep_of = [&](int m) {
+    int rep = m, v = m;
+    for (int i = 1; i < 4; i++) { v = T.rot[v][0]; rep = std::min(rep, v); }
+    return rep;
+  };
+  next = 0;
+  for (int k = 0; k <= 9; k++) {
+    T.cls_off[k] = uint16_t(next);
+    int r = 0;
+    for (int m = 0; m < 512; m++)
+      if (__builtin_popcount(m) == k && rep_of(m) == m) { T.cls_masks[next++] = uint16_t(m); T.cls_rank[m] = uint8_t(r++); }
+  }
+  T.cls_off[10] = uint16_t(next);
+  for (int m = 0; m < 512; m++) {
+    const int rep = rep_of(m);
+    int v = rep, rho = 0;
+    while (v != m) { v = T.rot[v][0]; rho++; }
+    T.cls_rank[m] = T.cls_rank[rep];
+    T.cls_rot[m] = uint8_t(rho);
+  }
 }
 
 void build_union(tables_t& T) {

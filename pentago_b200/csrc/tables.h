@@ -49,6 +49,14 @@ struct tables_t {
   uint16_t pop_off[11];
   uint16_t pop_masks[512];
   uint8_t rank9[512];
+  // Rotation classes of 9-bit quadrant sides, grouped by stone count:
+  // cls_masks[cls_off[k] + c] is the smallest mask of the c-th class with k
+  // stones, and mask v = rotl^cls_rot[v](cls_masks[cls_off[k] + cls_rank[v]])
+  // (rotl = rot[.][0], the least such count).
+  uint16_t cls_off[11];
+  uint16_t cls_masks[512];
+  uint8_t cls_rank[512];
+  uint8_t cls_rot[512];
 };
 
 // Built once on first use; thread safe.

@@ -254,6 +254,31 @@ def static_sizes(symbols, offsets, stream=None):
     return sizes
 
 
+def store_sizes(slice_t, node_off, nodes, turn, stream=None):
+    """The store coder on the same blocks (pg_store_*: rANS over a counted
+    1024-context table of each rotation's neighbouring rotations and the
+    previous node, no network): (stream bytes of each block, table bytes)."""
+    import torch
+    from .slice_store import store_bound
+    L = capi.lib()
+    sh = capi.stream_handle(stream)
+    dev = slice_t.device
+    k = len(node_off)
+    t64 = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.int64)).to(dev)
+    first = t64(node_off)
+    count = torch.from_numpy(np.ascontiguousarray(nodes, dtype=np.int32)).to(dev)
+    table = torch.empty(1024 * 3, dtype=torch.int16, device=dev)
+    capi.check(L.pg_store_table(slice_t.data_ptr(), first.data_ptr(), count.data_ptr(), k, turn, table.data_ptr(), sh))
+    caps = (store_bound(nodes) + 15) // 16 * 16
+    out_off = np.zeros(k + 1, np.int64)
+    out_off[1:] = np.cumsum(caps)
+    out = torch.empty(int(out_off[-1]), dtype=torch.uint8, device=dev)
+    sizes = torch.zeros(k, dtype=torch.int64, device=dev)
+    capi.check(L.pg_store_encode(slice_t.data_ptr(), first.data_ptr(), count.data_ptr(), k, turn, table.data_ptr(),
+                                 out.data_ptr(), t64(out_off[:-1]).data_ptr(), sizes.data_ptr(), sh))
+    return sizes.cpu().numpy(), 2 * 1024 * 3
+
+
 def run_slice_coding(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.01, steps=1500, batch=32768,
                 chunk_blocks=4096, max_blocks=0, seed=1, sample_blocks=0, sweep_timings=None):
     """Solve the root's sections down to its own slice, train on a
@@ -289,7 +314,7 @@ def run_slice_coding(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fractio
     del tsym, tr
     # Code the blocks spread evenly over the slice, chunk by chunk
     pick = np.unique(np.linspace(0, len(nodes) - 1, nblocks).astype(np.int64))
-    tot = {"learned": 0, "static": 0, "symbols": 0, "enc_ms": 0.0, "dec_ms": 0.0, "static_streams": 0,
+    tot = {"learned": 0, "static": 0, "store": 0, "symbols": 0, "enc_ms": 0.0, "dec_ms": 0.0, "static_streams": 0,
            "static_enc_ms": 0.0, "static_dec_ms": 0.0}
     lossless = True
     cpu_sample = None
@@ -315,6 +340,8 @@ def run_slice_coding(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fractio
             raise RuntimeError("encode failed")
         tot["learned"] += int(dsz_h.sum())
         tot["static"] += int(ssz.sum().item())
+        st_sz, st_table = store_sizes(slice_t, node_off[idx], nodes[idx], turn)
+        tot["store"] += int(st_sz.sum()) + st_table
         tot["symbols"] += int(sym.numel())
         tot["static_streams"] += int((dsz_h == ssz.cpu().numpy()).sum())
         lossless &= bool(torch.equal(dec, sym)) and bool((status.cpu().numpy() == nodes[idx] * 256).all())
@@ -331,7 +358,15 @@ def run_slice_coding(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fractio
                     f"({'all' if len(pick) == len(nodes) else len(pick)} of {len(nodes)} blocks coded)",
         "blocks": int(len(pick)), "positions": tot["symbols"],
         "static_bits_per_position": bits(tot["static"]), "learned_bits_per_position": bits(tot["learned"]),
-        "learned_over_static": tot["learned"] / tot["static"], "model_bytes": len(model),
+        "context_table_bits_per_position": bits(tot["store"]),
+        "learned_over_static": tot["learned"] / tot["static"],
+        "learned_over_context_table": tot["learned"] / tot["store"],
+        "coders": {"static": "format 2: one order-0 table per block (the reference's coder)",
+                   "context_table": "store coder: counted 1024-context table per chunk of blocks (the neighbouring "
+                                    "rotations and the previous node's), table bytes included, no network",
+                   "learned": "format 3: the MLP over the board, the rotation and the coded neighbouring rotations, "
+                              "model shared by the slice (not counted per block)"},
+        "model_bytes": len(model),
         "blocks_kept_static": tot["static_streams"], "lossless": lossless,
         "encode_GBps_of_nodes": tot["symbols"] / 4 / (tot["enc_ms"] / 1e3) / 1e9,
         "decode_GBps_of_nodes": tot["symbols"] / 4 / (tot["dec_ms"] / 1e3) / 1e9,

@@ -172,30 +172,70 @@ def positions(raw):
     return 2 * 128 * items
 
 
-def bench_boards_26(steps=20, warmup=3):
+def algorithmic_bytes(raw):
+    """Bytes a midsolve of this board moves through its workspace: both
+    passes, at every level n the (s0, s1p) items (N_n of them) each read
+    spots - n child halfsupers and write one, 16 bytes each
+    (mid/internal.h:358-408 over the info_t levels, mid/internal.h:37-69)."""
+    from math import comb
+    b = int(raw) & ((1 << 63) - 1)
+    spots = 36 - bin(side_of(b, 1) | side_of(b, 2)).count("1")
+    total = 0
+    for n in range(spots + 1):
+        items = comb(spots, n >> 1) * comb(spots - (n >> 1), n - (n >> 1))
+        total += items * (16 * (spots - n) + 16)
+    return 2 * total
+
+
+def bench_boards_26(steps=20, warmup=3, sm_max_mhz=1965.0):
     """64 seeded 26-stone boards (13 black, 13 white, no five);
-    GPU time per batch from CUDA events (median of three trials).  Returns
-    the result and the boards."""
+    GPU time per batch from CUDA events (median of three trials), and the
+    same batch end to end: boards in from the host through the C ABI and the
+    64 result records (mid_values_t) copied back to pinned host memory every
+    batch.  Returns the result and the boards."""
     import torch
     raws = random_boards(0, 64, 26)
     pos = sum(positions(r) for r in raws)
+    alg = sum(algorithmic_bytes(r) for r in raws)
     out = torch.zeros((len(raws), RECORD_BYTES), dtype=torch.uint8, device="cuda")
+    host = torch.empty((len(raws), RECORD_BYTES), dtype=torch.uint8).pin_memory()
     scratch = torch.empty(scratch_bytes(raws), dtype=torch.uint8, device="cuda")
-    for _ in range(warmup):
+    stream = torch.cuda.current_stream()
+
+    def device_batch():
         values_device(raws, out=out, scratch=scratch)
-    torch.cuda.synchronize()
-    # three trials of `steps` batches each; the median trial is reported
-    trials = []
-    for _ in range(3):
+
+    def e2e_batch():
+        values_device(raws, out=out, scratch=scratch)
+        host.copy_(out, non_blocking=True)
+        stream.synchronize()
+
+    def trial(fn):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         for _ in range(steps):
-            values_device(raws, out=out, scratch=scratch)
+            fn()
         b.record()
         torch.cuda.synchronize()
-        trials.append(a.elapsed_time(b) / steps)
-    ms = sorted(trials)[1]
+        return a.elapsed_time(b) / steps
+    for _ in range(warmup):
+        device_batch()
+        e2e_batch()
+    torch.cuda.synchronize()
+    # three trials of `steps` batches each; the median trial is reported
+    ms = sorted(trial(device_batch) for _ in range(3))[1]
+    e2e_ms = sorted(trial(e2e_batch) for _ in range(3))[1]
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    peak = 128 * sms * sm_max_mhz * 1e6 / 1e9
     result = {"workload": "64 seeded 26-stone boards (13 black, 13 white, no five), full midsolve",
               "positions_per_batch": pos, "ms_per_batch": ms, "value": pos / (ms / 1e3),
-              "boards_per_s": len(raws) / (ms / 1e3), "unit": "positions/s"}
+              "boards_per_s": len(raws) / (ms / 1e3), "unit": "positions/s",
+              "roofline": {"bound": "shared memory (each board's workspace lives in its CTA's shared memory)",
+                           "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                           "frac": alg / (ms / 1e3) / 1e9 / peak,
+                           "peak_kind": f"nominal: 128 B per clock per SM x {sms} SMs x {sm_max_mhz:.0f} MHz",
+                           "algorithmic_bytes_per_batch": alg,
+                           "note": "one CTA per board: 64 boards occupy 64 SMs"},
+              "e2e": {"value": pos / (e2e_ms / 1e3), "unit": "positions/s", "ms_per_batch": e2e_ms,
+                      "h2d_bytes_per_step": 8 * len(raws), "d2h_bytes_per_step": RECORD_BYTES * len(raws)}}
     return result, raws

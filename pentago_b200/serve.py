@@ -112,6 +112,65 @@ def one_at_a_time(raws):
     return res, lat, time.perf_counter() - t0
 
 
+def queued_latency(arrivals, service):
+    """Latencies of a FIFO single server with the given service times under
+    the given arrivals (the one-at-a-time baseline under the same stream)."""
+    finish, out = 0.0, np.zeros(len(service))
+    for i in range(len(service)):
+        finish = max(arrivals[i], finish) + service[i]
+        out[i] = finish - arrivals[i]
+    return out
+
+
+def bench(requests=400, rate=200.0, trials=3, budget_gb=40.0, seed=4):
+    """Config 4: seeded requests with stones uniform in 18..30.  Per trial
+    (its own seeded Poisson arrivals): the server under the stream (p50/p99
+    latency, arrival to result), the server under overload (every request at
+    once: its capacity in boards/s), and the same boards one request at a
+    time through pg_midsolve_batch (boards/s, and its latencies under the
+    same arrivals as a FIFO queue).  Every result of the stream must equal the
+    same board solved alone."""
+    import torch
+    capi.check(capi.lib().pg_init())
+    raws, stones = request_boards(seed, requests)
+    budget = int(budget_gb * (1 << 30))
+    with Server(budget) as S:  # warm-up
+        run_stream(S, raws[:16], np.zeros(16))
+    one_at_a_time(raws[:16])
+    out = []
+    identical = True
+    for k in range(trials):
+        arrivals = np.cumsum(np.random.default_rng(seed + k).exponential(1.0 / rate, requests))
+        with Server(budget) as S:
+            res, lat, wall = run_stream(S, raws, arrivals)
+        with Server(budget) as S:
+            cap_res, _, cap_wall = run_stream(S, raws, np.zeros(requests))
+        base_res, base_lat, base_wall = one_at_a_time(raws)
+        done = np.array([r is not None for r in res])
+        identical &= all(a == b for a, b in zip(res, base_res)) and all(a == b for a, b in zip(cap_res, base_res))
+        q = queued_latency(arrivals, base_lat)
+        out.append({"p50_ms": float(np.percentile(lat[done], 50) * 1e3),
+                    "p99_ms": float(np.percentile(lat[done], 99) * 1e3),
+                    "completed": int(done.sum()), "stream_wall_s": wall,
+                    "capacity_boards_per_s": requests / cap_wall,
+                    "baseline_boards_per_s": requests / base_wall,
+                    "baseline_p50_ms_same_arrivals": float(np.percentile(q, 50) * 1e3),
+                    "baseline_p99_ms_same_arrivals": float(np.percentile(q, 99) * 1e3)})
+    torch.cuda.synchronize()
+    med = lambda key: float(np.median([t[key] for t in out]))
+    base = [t["baseline_boards_per_s"] for t in out]
+    return {"workload": f"{requests} seeded midsolve requests, stones uniform 18..30, Poisson arrivals at "
+                        f"{rate:.0f}/s, scratch budget {budget_gb:.0f} GiB; {trials} trials",
+            "p50_ms": med("p50_ms"), "p99_ms": med("p99_ms"),
+            "capacity_boards_per_s": med("capacity_boards_per_s"),
+            "baseline_one_at_a_time_boards_per_s": {"median": float(np.median(base)), "min": min(base),
+                                                    "max": max(base)},
+            "capacity_over_baseline_max": med("capacity_boards_per_s") / max(base),
+            "baseline_p50_ms_same_arrivals": med("baseline_p50_ms_same_arrivals"),
+            "baseline_p99_ms_same_arrivals": med("baseline_p99_ms_same_arrivals"),
+            "results_identical_alone_and_in_mix": bool(identical), "trials": out}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=600)

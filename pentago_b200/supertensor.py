@@ -14,6 +14,7 @@ turn=RAW (the on-disk pair, what the reference's reader returns), or the end
 engine's [we win, we win or tie] with turn = 0 / 1 (side to move).
 """
 import ctypes
+import functools
 import os
 import struct
 
@@ -410,11 +411,20 @@ def write_index(path, slice_paths):
     return data
 
 
+@functools.lru_cache(maxsize=64)
+def _index_layout(slice_):
+    """Per section of a slice (in index order): its position and the number
+    of blocks before it (the reference's section_offset, index.cc:22-33)."""
+    sigs = index_sections(slice_)
+    before = np.zeros(len(sigs) + 1, np.int64)
+    before[1:] = np.cumsum(_section_block_counts(sigs))
+    return {int(s): i for i, s in enumerate(sigs)}, before
+
+
 def index_blob_location(slice_, section, block):
     """(offset, size) of a block's blob in the slice's index file
     (supertensor_index_t::blob_location, index.cc:48-59)."""
-    sigs = index_sections(slice_)
-    where = {int(s): i for i, s in enumerate(sigs)}
+    where, before = _index_layout(int(slice_))
     if int(section) not in where:
         raise KeyError(f"section {section:#x} is not in slice {slice_}")
     i = where[int(section)]
@@ -422,8 +432,7 @@ def index_blob_location(slice_, section, block):
     if any(not 0 <= int(block[k]) < int(B[k]) for k in range(4)):
         raise IndexError(f"block {tuple(block)} outside {tuple(B)}")
     flat = int(np.ravel_multi_index(tuple(int(x) for x in block), tuple(int(x) for x in B)))
-    base = INDEX_HEAD + INDEX_BLOB * sum(_section_block_counts(sigs[:i]))
-    return base + INDEX_BLOB * flat, INDEX_BLOB
+    return INDEX_HEAD + INDEX_BLOB * (int(before[i]) + flat), INDEX_BLOB
 
 
 def index_block_location(blob):

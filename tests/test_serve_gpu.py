@@ -9,15 +9,39 @@ pytestmark = pytest.mark.gpu
 
 
 def test_results_same_alone_and_in_mix(cuda):
+    """Stone counts 18-30: boards with 12 or more empty spots run as gangs of
+    workers sharing the bounded group barrier, beside single-worker boards;
+    every result equals the same board solved alone."""
     from pentago_b200 import mid, serve
-    raws, stones = serve.request_boards(11, 40, lo=22, hi=30)
+    raws, stones = serve.request_boards(11, 40, lo=18, hi=30)
+    assert (stones <= 21).sum() >= 4, "the mix should hold several gang boards"
     alone = [mid.midsolve(np.array([r], np.uint64))[0] for r in raws]
     arrivals = np.linspace(0, 0.05, len(raws))
-    with serve.Server(2 << 30) as S:
+    with serve.Server(8 << 30) as S:
         res, lat, wall = serve.run_stream(S, raws, arrivals, timeout=120)
     assert all(r is not None for r in res)
     for a, b in zip(alone, res):
         assert a == b
+
+
+def test_server_golden_18_stone_board(cuda):
+    """The reference's 18-stone benchmark board (pentago/mid/benchmark_test.cc:42-58)
+    through the server, alone and among 26-stone boards arriving with it: its
+    163 (raw, value) pairs equal the golden ones both times."""
+    import json
+    import os
+    from pentago_b200 import mid, serve
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "midsolve_18.json")))
+    want = {(b | m << 63): v for b, m, v in g["results"]}
+    others = mid.random_boards(3, 12, 26)
+    with serve.Server(8 << 30) as S:
+        alone, _, _ = serve.run_stream(S, np.array([g["root"]], np.uint64), np.zeros(1), timeout=120)
+        raws = np.concatenate([others[:6], np.array([g["root"]], np.uint64), others[6:]])
+        mix, _, _ = serve.run_stream(S, raws, np.linspace(0, 0.01, len(raws)), timeout=120)
+    assert len(alone[0]) == 163 and dict(alone[0]) == want
+    assert dict(mix[6]) == want
+    for r, got in zip(others, mix[:6] + mix[7:]):
+        assert got == mid.midsolve(np.array([r], np.uint64))[0]
 
 
 def test_admission_respects_budget(cuda):

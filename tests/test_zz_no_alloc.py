@@ -1,8 +1,8 @@
 """pg_midsolve_batch_noalloc: the midsolve entry point for callers that cannot
-allocate device memory when they need a solve (for example while a stream is
-being captured into a CUDA graph, or inside a framework that owns the whole
-device memory pool).  It must give exactly what pg_midsolve_batch gives, call
-after call, although every call reuses the same fixed scratch array.
+allocate device memory when they need a solve (for example inside a framework
+that owns the whole device memory pool, or a loop that must not wait for an
+allocation).  It must give exactly what pg_midsolve_batch gives, call after
+call, although every call reuses the same fixed scratch array.
 
 This file is named to be collected last, so a run that stops at its first
 failure has already run every other test."""
