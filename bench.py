@@ -412,17 +412,28 @@ def cpu_lookup_rate(paths, seconds=5.0):
             "sample": f"{len(boards)} random positions, lookups repeated for {el:.1f} s, blocks in host memory"}
 
 
-def sweep_summary(timings, wall_s):
+def sweep_summary(timings, wall_s, peak):
     """The full sweep of SWEEP_ROOT (slices 35 -> 30) from its per-slice timings."""
     ms = sum(v["ms"] for v in timings.values())
-    nbytes = sum(64 * (v["nodes"] + v["child_nodes"]) for v in timings.values())
+    slice_bytes = sum(64 * (v["nodes"] + v["child_nodes"]) for v in timings.values())
+    line_bytes = sum(v.get("line_bytes", 0) for v in timings.values())
     sections = sum(v["sections"] for v in timings.values())
+    per_slice = {str(k): {"kernel_ms": v["ms"], "sections": v["sections"], "lines_per_dim": v.get("lines"),
+                          "ctas_per_dim": v.get("ctas"),
+                          "line_GBps": v.get("line_bytes", 0) / (v["ms"] / 1e3) / 1e9}
+                 for k, v in sorted(timings.items())}
     return {"workload": f"all sections below root {SWEEP_ROOT}, slices 35 -> 30, in HBM",
             "sections": sections, "nodes": sum(v["nodes"] for v in timings.values()), "kernel_ms": ms,
             "arena_ms": sum(v.get("arena_ms", 0.0) for v in timings.values()),
             "arena_GB": max(v.get("arena_GB", 0.0) for v in timings.values()),
             "wall_s": wall_s, "sections_per_s": sections / (ms / 1e3),
-            "algorithmic_GBps": nbytes / (ms / 1e3) / 1e9}
+            "algorithmic_GBps": line_bytes / (ms / 1e3) / 1e9,
+            "algorithmic_bytes": "per block line: 64 B per child node read + 64 B per parent node written "
+                                 "(the bench kernel's measure), summed over every line of the sweep",
+            "frac_of_hbm_peak": line_bytes / (ms / 1e3) / 1e9 / peak,
+            "slice_GBps": slice_bytes / (ms / 1e3) / 1e9,
+            "slice_bytes_note": "every node of every slice read once as a child and written once as a parent",
+            "per_slice": per_slice}
 
 
 def cpu_sweep_estimate(root_counts, timings, seconds_per_slice=1.5):
@@ -518,6 +529,7 @@ def main():
     ap.add_argument("--no-lookup", action="store_true", help="skip the board lookup measurement")
     ap.add_argument("--no-parity", action="store_true", help="skip the check of the timed outputs")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--no-midsolve", action="store_true", help="skip the midsolve measurement")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", 0))
@@ -693,7 +705,7 @@ def main():
     lookups = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(seconds=12.0)
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_midsolve:
         from pentago_b200 import mid
         midsolve, raws0 = mid.bench_boards_26(sm_max_mhz=measured_peaks().get("sm_max_mhz", 1965.0))
         if not args.no_cpu_baseline:
@@ -707,12 +719,12 @@ def main():
 
     if rank == 0 and world == 1 and not args.no_learned:
         # The full sweep of SWEEP_ROOT, then the learned coder trained on its
-        # 30-stone slice and run on a sample of 4096 of that slice's blocks
+        # 30-stone slice and run on 16384 of that slice's blocks, spread evenly over it
         torch.cuda.empty_cache()
         from pentago_b200 import learned as learned_mod
         timings = {}
-        learned, sample = learned_mod.run_slice_coding(max_blocks=4096, sample_blocks=64, sweep_timings=timings)
-        sweep2 = sweep_summary(timings, learned["sweep_s"])
+        learned, sample = learned_mod.run_slice_coding(max_blocks=16384, sample_blocks=64, sweep_timings=timings)
+        sweep2 = sweep_summary(timings, learned["sweep_s"], measured_hbm_peak()[0])
         if not args.no_cpu_baseline:
             learned["cpu_static_coder"] = cpu_static_coder_rate(*sample, seconds=5.0)
             sweep2["cpu_baseline"] = cpu_sweep_estimate(SWEEP_ROOT, timings, seconds_per_slice=1.5)

@@ -283,27 +283,172 @@ PG_HD const uint64_t* child_addr(const line_dev_t& L, const microline_geom& G, i
   return L.input + 8 * idx;
 }
 
+// ---------------------------------------------------------------------------
+// The children's transform, line frame first.  A child's contribution is
+// Q = swap_DIM3(phi_g(T_l(y))) with y = rmax(~child).  Writing phi_g as
+// s * sigma (sigma an axis permutation, s = -1 when g holds the reflection),
+// Q[u] = Z[s u + sigma(l)] with Z = swap_DIM3(sigma(y)): a fixed axis
+// permutation, then on each line-frame axis a rotation (s = 1) or a
+// reflection (s = -1) by the matching component of sigma(l).  Axis 3 of the
+// line frame is the child's own line axis: its map is applied by the
+// addresses the word pairs are stored at.
+
+// Cost in word operations of exchanging axes a < b (delta swaps within
+// words, between words, or renaming words).
+constexpr int swap_cost(int a, int b) {
+  return (a == 2 && b == 3) ? 20 : b == 3 ? 40 : (a == 0 && b == 1) ? 64 : 52;
+}
+// The cheapest sequence of at most four axis exchanges giving p.
+struct swap_seq { int n, a[4], b[4]; };
+constexpr swap_seq cheapest_swaps(axis_perm target) {
+  const int pa[6] = {0, 0, 0, 1, 1, 2}, pb[6] = {1, 2, 3, 2, 3, 3};
+  swap_seq best{-1, {0, 0, 0, 0}, {0, 0, 0, 0}};
+  int best_cost = 1 << 30;
+  for (int n = 0; n <= 4; n++) {
+    int total = 1;
+    for (int i = 0; i < n; i++) total *= 6;
+    for (int code = 0; code < total; code++) {
+      axis_perm p = perm_id();
+      int cost = 0, c = code;
+      swap_seq s{n, {0, 0, 0, 0}, {0, 0, 0, 0}};
+      for (int i = 0; i < n; i++, c /= 6) {
+        s.a[i] = pa[c % 6];
+        s.b[i] = pb[c % 6];
+        p = perm_swap(p, s.a[i], s.b[i]);
+        cost += swap_cost(s.a[i], s.b[i]);
+      }
+      bool same = true;
+      for (int q = 0; q < 4; q++) same = same && p.to[q] == target.to[q];
+      if (same && cost < best_cost) { best = s; best_cost = cost; }
+    }
+  }
+  return best;
+}
+template<int DIM, int G> PG_HD void line_permute(super8& s) {
+  constexpr swap_seq q = cheapest_swaps(line_sigma(DIM, G));
+  static_assert(q.n >= 0, "every axis permutation is a product of at most four exchanges");
+  if constexpr (q.n > 0) s_swap_axes<q.a[0], q.b[0]>(s);
+  if constexpr (q.n > 1) s_swap_axes<q.a[1], q.b[1]>(s);
+  if constexpr (q.n > 2) s_swap_axes<q.a[2], q.b[2]>(s);
+  if constexpr (q.n > 3) s_swap_axes<q.a[3], q.b[3]>(s);
+}
+
+PG_HD uint32_t byte_perm(uint32_t x, uint32_t y, uint32_t s) {
+#ifdef __CUDA_ARCH__
+  return __byte_perm(x, y, s);
+#else
+  const uint64_t v = uint64_t(y) << 32 | x;
+  uint32_t r = 0;
+  for (int i = 0; i < 4; i++) r |= uint32_t(v >> (8 * (s >> (4 * i) & 7)) & 0xff) << (8 * i);
+  return r;
+#endif
+}
+
+// Maps of line-frame axes 0-2 with amounts c0, c1, c2: out[u] = in[u + c]
+// (rotations) or out[u] = in[c - u] (reflections), per axis.
+template<bool REFL> PG_HD void axis_maps(super8& s, int c0, int c1, int c2) {
+  if constexpr (REFL) {
+    // axis 0 (bits of a nibble): c - u is u ^ c for odd c
+    if (c0 & 1) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) s.w[i] = ((s.w[i] >> 1) & 0x55555555u) | ((s.w[i] << 1) & 0xaaaaaaaau);
+      if (c0 & 2)
+#pragma unroll
+        for (int i = 0; i < 8; i++) s.w[i] = ((s.w[i] >> 2) & 0x33333333u) | ((s.w[i] << 2) & 0xccccccccu);
+    } else {
+      const uint32_t m = c0 ? 0x11111111u : 0x22222222u;   // positions 0, 2 or 1, 3 exchanged
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const uint32_t t = ((s.w[i] >> 2) ^ s.w[i]) & m;
+        s.w[i] ^= t ^ (t << 2);
+      }
+    }
+    // axis 1 (nibbles of a 16-bit half)
+    if (c1 & 1) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) s.w[i] = ((s.w[i] >> 4) & 0x0f0f0f0fu) | ((s.w[i] << 4) & 0xf0f0f0f0u);
+      if (c1 & 2)
+#pragma unroll
+        for (int i = 0; i < 8; i++) s.w[i] = byte_perm(s.w[i], 0, 0x2301);
+    } else {
+      const uint32_t m = c1 ? 0x000f000fu : 0x00f000f0u;
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        const uint32_t t = ((s.w[i] >> 8) ^ s.w[i]) & m;
+        s.w[i] ^= t ^ (t << 8);
+      }
+    }
+  } else {
+    const uint32_t m0 = (0xfu >> c0) * 0x11111111u, m1 = (0xffffu >> (4 * c1)) * 0x10001u;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      uint32_t x = s.w[i];
+      x = ((x >> c0) & m0) | ((x << (4 - c0)) & ~m0);
+      x = ((x >> (4 * c1)) & m1) | ((x << (16 - 4 * c1)) & ~m1);
+      s.w[i] = x;
+    }
+  }
+  // axis 2 (half of a word, then word of a pair): byte permutes per pair,
+  // selectors for c = 0..3 packed 16 bits each
+  const uint64_t klo = REFL ? 0x5476325410327610ull : 0x1076765454323210ull;
+  const uint64_t khi = REFL ? 0x1032761054763254ull : 0x5432321010767654ull;
+  const uint32_t slo = uint32_t(klo >> (16 * c2)) & 0xffff, shi = uint32_t(khi >> (16 * c2)) & 0xffff;
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    const uint32_t lo = s.w[2 * p], hi = s.w[2 * p + 1];
+    s.w[2 * p] = byte_perm(lo, hi, slo);
+    s.w[2 * p + 1] = byte_perm(lo, hi, shi);
+  }
+}
+
+template<int DIM, int G> PG_HD void child_maps(super8& a, super8& b, int c) {
+  line_permute<DIM, G>(a);
+  line_permute<DIM, G>(b);
+  axis_maps<(G >= 4)>(a, c & 3, c >> 2 & 3, c >> 4 & 3);
+  axis_maps<(G >= 4)>(b, c & 3, c >> 2 & 3, c >> 4 & 3);
+}
+
+PG_HD uint32_t select4(const uint4 v, int i) {
+  return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+
 // Child j (its node: cw = win, cn = not lost) -> Q_j in the line frame, both
-// halves already moved into the parent's frame.  The win half also carries
-// W_j = super_wins of the mover's stones once the move is made (csub: the
-// terms they cover per rotation): a move that makes the child wins at once,
-// and super_wins of the moved quadrant is W_j translated by the move's
-// rotation exactly as the child's value is, so a parent ORs one translated
-// Q_j for both.
+// halves already moved into the parent's frame: Q_j = swap(phi_g(rmax(~child)
+// - l_j)), done as a fixed axis permutation of rmax(~child) and a rotation or
+// reflection of each line-frame axis (see axis_maps); the map of axis 3, the
+// child's own line axis, is applied by the addresses of the stored word
+// pairs.  The win half also carries W_j = super_wins of the mover's stones
+// once the move is made (csub: the terms they cover per rotation): a move
+// that makes the child wins at once, and super_wins of the moved quadrant is
+// W_j translated by the move's rotation exactly as the child's value is, so a
+// parent ORs one translated Q_j for both.
 template<int DIM>
 PG_HD void child_node(const line_dev_t& L, const microline_geom& G, const uint2* tab0, uint4* q, int j,
                       const super8& cw, const super8& cn, const uint4 csub) {
-  const int l = ladd(G.base_l, L.csym[j]);
-  super8 qw = s_translate(s_rmax(s_not(cn)), l);
-  super8 qn = s_translate(s_rmax(s_not(cw)), l);
-  s_phi_runtime(qw, L.g);
-  s_phi_runtime(qn, L.g);
-  s_line_frame<DIM>(qw);
-  s_line_frame<DIM>(qn);
-  qw = s_or(qw, table_eval(tab0, csub));
+  super8 zw = s_rmax(s_not(cn)), zn = s_rmax(s_not(cw));
+  const int c = ladd(G.base_l, int(L.csym[j]) << 6);   // the translation, axes moved to the line frame
+  switch (L.g) {
+    case 0: child_maps<DIM, 0>(zw, zn, c); break;
+    case 1: child_maps<DIM, 1>(zw, zn, c); break;
+    case 2: child_maps<DIM, 2>(zw, zn, c); break;
+    case 3: child_maps<DIM, 3>(zw, zn, c); break;
+    case 4: child_maps<DIM, 4>(zw, zn, c); break;
+    case 5: child_maps<DIM, 5>(zw, zn, c); break;
+    case 6: child_maps<DIM, 6>(zw, zn, c); break;
+    default: child_maps<DIM, 7>(zw, zn, c); break;
+  }
+  // Pair k goes to pair p(k) = k - c3 (rotation) or c3 - k (reflection), and
+  // W_j's pair p(k) is evaluated beside it.
+  const int c3 = c >> 6 & 3, sgn = L.g >= 4 ? -1 : 1;
+  int pk[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) pk[k] = (sgn * (k - c3)) & 3;
+  const super8 w = table_eval(tab0, make_uint4(select4(csub, pk[0]), select4(csub, pk[1]), select4(csub, pk[2]),
+                                                select4(csub, pk[3])));
   const int nc = L.nchild;
 #pragma unroll
-  for (int p = 0; p < 4; p++) q[p * nc + j] = make_uint4(qw.w[2 * p], qw.w[2 * p + 1], qn.w[2 * p], qn.w[2 * p + 1]);
+  for (int k = 0; k < 4; k++)
+    q[pk[k] * nc + j] = make_uint4(zw.w[2 * k] | w.w[2 * k], zw.w[2 * k + 1] | w.w[2 * k + 1], zn.w[2 * k], zn.w[2 * k + 1]);
 }
 
 // Parent i of a microline (compute.cc:308-356), in the line frame until its
@@ -1180,7 +1325,7 @@ static bool make_family(const section_t& sec, int dim, int64_t parent_base, cons
       for (int j = 0; j < n && j < kMaxLine; j++) {
         const uint16_t q = T.rmin_flat[T.rmin_off[k] + j];
         const int rq = T.pack[T.refl[T.unpack[q][0]]] + 2 * T.pack[T.refl[T.unpack[q][1]]];
-        F.xsym_full[i][j] = uint8_t((T.rmin_inv[rq] & 3) << (2 * i));
+        F.xsym_full[i][j] = uint8_t(sigma_apply(line_sigma(dim, F.proto.g), (T.rmin_inv[rq] & 3) << (2 * i)));
       }
     }
   }

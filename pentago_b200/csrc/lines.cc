@@ -140,8 +140,10 @@ bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error) {
     const int st = s.st;
     const int ag = (4 - (st & 3)) & 3, al = 0x55 * (st & 3), bg = st & 4;
     d.g = T.gprod[ag][bg];
-    d.inv_l = T.commute[bg][al];
+    d.inv_l = sigma_apply(line_sigma(dim, d.g), T.commute[bg][al]);
   }
+  const axis_perm sg = line_sigma(dim, d.g);
+  if (sg.to[s.child_dim] != 3) { error = "child dimension does not map to the line axis"; return false; }
   // Reflection bookkeeping (compute.cc:96-122)
   if (s.st & 4) {
     for (int i = 0; i < 4; i++) {
@@ -152,9 +154,9 @@ bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error) {
       for (int j = 0; j < n; j++) {
         const uint16_t q = crmin[8 * d.first_child_block[i] + j];
         const int rq = T.pack[T.refl[T.unpack[q][0]]] + 2 * T.pack[T.refl[T.unpack[q][1]]];
-        const uint8_t local = uint8_t((T.rmin_inv[rq] & 3) << (2 * i));
-        if (i == s.child_dim) { if (j < kMaxLine) d.csym[j] = local; }
-        else if (j < 8) d.xsym[i][j] = local;
+        const int rot = T.rmin_inv[rq] & 3;
+        if (i == s.child_dim) { if (j < kMaxLine) d.csym[j] = uint8_t(rot); }
+        else if (j < 8) d.xsym[i][j] = uint8_t(sigma_apply(sg, rot << (2 * i)));
       }
     }
   }

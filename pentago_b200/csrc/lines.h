@@ -27,6 +27,37 @@ struct section_t {
 void quadrant_permutation(int global, int* p);
 inline int invert_global(int g) { return g ^ ((~g >> 2 & (g & 1)) << 1); }
 
+// An axis permutation of the rotation index space Z_4^4, as where the
+// content of axis q goes.
+struct axis_perm { int to[4]; };
+constexpr axis_perm perm_id() { return axis_perm{{0, 1, 2, 3}}; }
+// p, then the contents of axes a and b exchanged.
+constexpr axis_perm perm_swap(axis_perm p, int a, int b) {
+  for (int q = 0; q < 4; q++) p.to[q] = p.to[q] == a ? b : p.to[q] == b ? a : p.to[q];
+  return p;
+}
+// The axis permutation of a line's children's transform: that of phi_g (the
+// conjugation by global symmetry g, without its negation of every axis when
+// g reflects), then the exchange of the line's axis DIM with axis 3.
+constexpr axis_perm line_sigma(int dim, int g) {
+  axis_perm p = perm_id();
+  if (g == 1) { p = perm_swap(p, 1, 3); p = perm_swap(p, 0, 3); p = perm_swap(p, 2, 3); }
+  if (g == 2) { p = perm_swap(p, 0, 3); p = perm_swap(p, 1, 2); }
+  if (g == 3) { p = perm_swap(p, 2, 3); p = perm_swap(p, 0, 3); p = perm_swap(p, 1, 3); }
+  if (g == 4) { p = perm_swap(p, 0, 3); }
+  if (g == 5) { p = perm_swap(p, 1, 3); p = perm_swap(p, 0, 2); }
+  if (g == 6) { p = perm_swap(p, 1, 2); }
+  if (g == 7) { p = perm_swap(p, 2, 3); p = perm_swap(p, 0, 1); }
+  if (dim != 3) p = perm_swap(p, dim, 3);
+  return p;
+}
+// A translation l (2 bits per axis) with its axes moved by p.
+inline int sigma_apply(const axis_perm& p, int l) {
+  int r = 0;
+  for (int q = 0; q < 4; q++) r |= (l >> (2 * q) & 3) << (2 * p.to[q]);
+  return r;
+}
+
 constexpr int kMaxBlocks = 64;   // 420 nodes / 8 per block < 64
 constexpr int kMaxLine = 424;    // nodes along a quadrant axis, rounded up
 
@@ -56,7 +87,8 @@ struct alignas(16) child_rec {
 // copied to the device as is.
 struct alignas(16) line_dev_t {
   int32_t dim, child_dim, turn, slice35, flags;
-  int32_t g, inv_l;                 // base transform = (g, inv_l + reflection locals)
+  int32_t g, inv_l;                 // base transform = (g, inv_l + reflection locals); inv_l and the
+                                    // reflection locals below with their axes moved by line_sigma(dim, g)
   int32_t nparent, nchild, length, input_blocks, line_moves;
   int32_t odims[3], cross[3];       // the three cross dimensions and their extents
   int32_t perm[4], refl_moves[4], block0[4], first_child_block[4];
@@ -70,8 +102,8 @@ struct alignas(16) line_dev_t {
   const parent_rec* recs;           // nparent records for this (section, dimension)
   const child_rec* crecs;           // nchild records for this (section, dimension)
   int64_t in_off[kMaxBlocks], out_off[kMaxBlocks];
-  uint8_t csym[kMaxLine];           // reflection locals along the child dimension
-  uint8_t xsym[4][8];               // reflection locals of the cross dimensions
+  uint8_t csym[kMaxLine];           // reflection rotations along the child dimension (0..3)
+  uint8_t xsym[4][8];               // reflection locals of the cross dimensions (axes moved)
 };
 
 struct line_in_t {

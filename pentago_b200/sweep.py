@@ -150,6 +150,35 @@ def _compressed_slice_step(root, slice_, sigs, off, child, last, checkpoint, lev
     return to_golden(sigs, counts, slice_), store, raw
 
 
+def line_work(sigs, child_sigs):
+    """The block lines of a slice: per quadrant dimension, the number of lines
+    and of their microline CTAs (4 microlines each), and the slice's
+    algorithmic bytes counted per line (every line reads its child line and
+    writes its parent line once, 64 bytes per node: over a slice, each
+    (section, non-full dimension) pair reads its whole child section and
+    writes the whole section)."""
+    child_nodes = {}
+    if len(child_sigs):
+        off = slice_layout(child_sigs)
+        child_nodes = {int(c): int(off[i + 1] - off[i]) for i, c in enumerate(child_sigs)}
+    lines, ctas, nbytes = [0] * 4, [0] * 4, 0
+    for sig in sigs:
+        shape = section_shape(int(sig))
+        n = int(np.prod(shape))
+        for d in range(4):
+            c = _child_of(sig, d)
+            if c is None:
+                continue
+            blocks = [(shape[i] + 7) // 8 for i in range(4)]
+            nl = int(np.prod([blocks[i] for i in range(4) if i != d]))
+            lines[d] += nl
+            # microlines of a line: its cross-section (8^3 unless a cross block is short)
+            per_dim = [[min(8, shape[i] - 8 * b) for b in range(blocks[i])] for i in range(4) if i != d]
+            ctas[d] += sum((a * b * cc + 3) // 4 for a in per_dim[0] for b in per_dim[1] for cc in per_dim[2])
+            nbytes += 64 * (n + child_nodes.get(c, 0))
+    return {"lines": lines, "ctas": ctas, "line_bytes": nbytes}
+
+
 def _arena_nodes(root, chain):
     """Nodes of the two halves of the sweep arena for the slices `chain`
     (top first): slices take turns between the halves, so each half holds
@@ -266,6 +295,7 @@ def sweep(root, min_slice=None, stream=None, keep_last=False, timings=None, chec
             torch.cuda.synchronize()
             timings[slice_] = {"ms": t0.elapsed_time(t1), "sections": len(sigs), "nodes": int(off[-1]),
                                "child_nodes": int(child.shape[0]) if child is not None else 0}
+            timings[slice_].update(line_work(sigs, child_sigs))
             if arena_ms is not None and slice_ == order[0]:
                 timings[slice_]["arena_ms"] = arena_ms
                 timings[slice_]["arena_GB"] = 64 * sum(h.shape[0] for h in halves) / 1e9

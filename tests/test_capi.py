@@ -76,6 +76,54 @@ def test_kernel_line_code_on_host_matches_reference_golden(case):
     assert sha1(line.output) == case["output_sha1"]
 
 
+def random_section(rng, stones):
+    """A valid section with `stones` stones (black has the extra one when odd)."""
+    c = [[0, 0] for _ in range(4)]
+    for color, cnt in ((0, (stones + 1) // 2), (1, stones // 2)):
+        for _ in range(cnt):
+            free = [q for q in range(4) if sum(c[q]) < 9]
+            c[free[int(rng.integers(len(free)))]][color] += 1
+    return c
+
+
+def test_kernel_line_code_on_host_matches_oracle_for_every_symmetry(O):
+    """Random block lines of 33- to 35-stone sections, run through the
+    kernel's own microline code on the host, equal the oracle's line compute;
+    between them the lines' children are standardized by each of the 8 global
+    symmetries (the per-line axis maps of the children's transform)."""
+    import collections
+    from pentago_b200 import end
+    from pentago_b200.synthetic import random_nodes
+    rng = np.random.default_rng(123)
+    seen = collections.Counter()
+    n = 0
+    while n < 60:
+        stones = int(rng.integers(33, 36))
+        c = random_section(rng, stones)
+        dims = [d for d in range(4) if sum(c[d]) < 9]
+        if not dims:
+            continue
+        dim = dims[int(rng.integers(len(dims)))]
+        sig = end.section_sig(c)
+        shape = end.section_shape(sig)
+        bb = tuple(int(rng.integers((shape[i] + 7) // 8)) for i in range(4) if i != dim)
+        line = end.Line(sig, dim, bb)
+        info = end.line_info(line)
+        if info.output_nodes > 40000:
+            continue
+        inp = random_nodes(n + 7, max(info.input_nodes, 1))
+        got = np.zeros((info.output_nodes, 8), np.uint64)
+        want = np.zeros_like(got)
+        line.input, line.output = inp, got
+        end.selftest_lines_host([line])
+        O.compute_line(sig, dim, line.length, (ctypes.c_uint8 * 3)(*bb), P(inp), P(want), 8)
+        assert np.array_equal(got, want), (c, dim, bb)
+        child = [[c[q][k] + (q == dim and k == stones % 2) for k in range(2)] for q in range(4)]
+        seen[end.section_standardize(end.section_sig(child))[1]] += 1
+        n += 1
+    assert sorted(seen) == list(range(8)), seen
+
+
 def test_line_rejects_bad_input():
     from pentago_b200 import capi, end
     full = end.section_sig([[5, 4], [4, 5], [4, 4], [4, 3]])

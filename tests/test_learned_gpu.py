@@ -156,6 +156,36 @@ def test_trained_model_beats_static_and_roundtrips(cuda):
     assert torch.equal(back, sym)
 
 
+def test_network_gain_on_held_out_blocks(cuda):
+    """The same 64 held-out blocks coded three ways: format 2 (one order-0
+    table per block), the store coder's counted context table (the same kind
+    of context as the network's neighbour features, counted from the blocks
+    themselves, no network) and the trained network.  Prints the three
+    figures in bits per position; the network must be at least 10% smaller
+    than format 2 and round-trip (the store coder's own round trips are
+    tested with the compressed sweeps)."""
+    import torch
+    from pentago_b200 import learned
+    model, _, train_blocks = trained()
+    refs_all, off_all, nodes_all, slice_t = solved()
+    rng = np.random.default_rng(6)
+    held_out = sorted([i for i in rng.choice(len(nodes_all), 96, replace=False) if i not in train_blocks][:64])
+    refs, sym, offsets, n = pick(held_out)
+    data, doff, dsz = learned.encode(model, refs, sym, offsets, n)
+    back, _, status = learned.decode(model, refs, data, doff, dsz, n)
+    assert torch.equal(back, sym)
+    static, _, _, ok = learned.static_roundtrip(sym, offsets)
+    assert ok
+    ctx_sizes, table_bytes = learned.store_sizes(slice_t, off_all[held_out], nodes_all[held_out], 33 & 1)
+    positions = int(sym.numel())
+    bits = {"static": 8.0 * int(static.sum().item()) / positions,
+            "context_table": 8.0 * (int(ctx_sizes.sum()) + table_bytes) / positions,
+            "learned": 8.0 * int(dsz.sum().item()) / positions}
+    print("bits per position on held-out blocks:", bits)
+    assert bits["learned"] <= 0.9 * bits["static"], bits
+    assert bits["context_table"] < bits["static"], bits
+
+
 def test_untrained_model_falls_back_to_static(cuda):
     import torch
     from pentago_b200 import learned
