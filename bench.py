@@ -46,6 +46,18 @@ def rank_blocks(blocks, rank):
     return [block_of(rank * blocks + t) for t in range(blocks)]
 
 
+def combine_parity(parity, world, device):
+    """Every rank's parity check folded into rank 0's record: ok only when
+    every rank's lines matched (all ranks take part)."""
+    if world == 1:
+        return parity
+    import torch
+    import torch.distributed as dist
+    ok = torch.tensor([1 if parity["ok"] else 0], dtype=torch.int32, device=device)
+    dist.all_reduce(ok, op=dist.ReduceOp.MIN)
+    return dict(parity, ok=bool(ok.item()), scope="rank 0's counts; ok is the AND over ranks")
+
+
 def max_over_ranks(x, world, device):
     """The slowest rank's time (all ranks take part)."""
     if world == 1:
@@ -759,11 +771,7 @@ def main():
         if not args.no_cpu_baseline:
             lookups["cpu_baseline"] = cpu_lookup_rate(db, seconds=5.0)
 
-    parity_all = parity
-    if world > 1 and parity is not None:
-        ok = torch.tensor([1 if parity["ok"] else 0], dtype=torch.int32, device=dev)
-        dist.all_reduce(ok, op=dist.ReduceOp.MIN)
-        parity_all = dict(parity, ok=bool(ok.item()), scope="rank 0's counts; ok is the AND over ranks")
+    parity_all = parity if parity is None else combine_parity(parity, world, dev)
     if rank == 0:
         result = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

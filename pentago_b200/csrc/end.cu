@@ -474,16 +474,18 @@ PG_HD void parent_node(const line_dev_t& L, const microline_geom& G, const uint2
     const int nmoves = int(h.x >> 24);
     const uint4 h2 = nmoves > 6 ? ldg(rec + 1) : make_uint4(0, 0, 0, 0);
     const uint32_t mvw[5] = {h.y, h.z, h.w, h2.x, h2.y};
-    const int nc = L.nchild;
+    // A move's entry is the slot r nc + j of the child's pair r; pair p + r
+    // follows nc p slots later, wrapping around the 4 nc slots.
+    const int nc = L.nchild, all = 4 * nc;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
       if (k >= nmoves) break;
-      const int ir = int(mvw[k >> 1] >> (16 * (k & 1)) & 0xffff);
-      const int j = ir >> 2, r = ir & 3;
-      if (j >= nc) { *errors |= 1u; continue; }
+      const int a0 = int(mvw[k >> 1] >> (16 * (k & 1)) & 0xffff);
+      if (a0 >= all) { *errors |= 1u; continue; }
 #pragma unroll
       for (int p = 0; p < 4; p++) {
-        const uint4 a = qs[((p + r) & 3) * nc + j];
+        const int ap = a0 + p * nc;
+        const uint4 a = qs[ap >= all ? ap - all : ap];
         wins.w[2 * p] |= a.x;
         wins.w[2 * p + 1] |= a.y;
         not_loss.w[2 * p] |= a.z;
@@ -1121,17 +1123,28 @@ PG_HD int64_t block_offset(const int32_t* S, const int* b) {
   return off;
 }
 
+// Block coordinates of line t of a family (row-major over the other three
+// block counts; 0 along the line); returns the line's microline count.
+PG_HD int family_blocks(const family_t& F, int t, int* b) {
+  const int dim = F.proto.dim;
+  int od[3], k = 0;
+  for (int i = 0; i < 4; i++) if (i != dim) od[k++] = i;
+  b[od[2]] = t % F.bcount[od[2]];
+  b[od[1]] = t / F.bcount[od[2]] % F.bcount[od[1]];
+  b[od[0]] = t / (F.bcount[od[2]] * F.bcount[od[1]]);
+  b[dim] = 0;
+  int n = 1;
+  for (int j = 0; j < 3; j++) n *= std::min(8, F.pshape[od[j]] - 8 * b[od[j]]);
+  return n;
+}
+
 // Fill the per-line fields of a family member (line t of the family).
 PG_HD void family_line(const family_t& F, int t, line_dev_t& L) {
   const int dim = F.proto.dim;
   int od[3], k = 0;
   for (int i = 0; i < 4; i++) if (i != dim) od[k++] = i;
-  // block_base in row-major order over the other three block counts
   int b[4];
-  b[od[2]] = t % F.bcount[od[2]];
-  b[od[1]] = t / F.bcount[od[2]] % F.bcount[od[1]];
-  b[od[0]] = t / (F.bcount[od[2]] * F.bcount[od[1]]);
-  b[dim] = 0;
+  family_blocks(F, t, b);
   for (int i = 0; i < 4; i++) {
     L.block0[i] = b[i];
     L.out_shape[i] = i == dim ? F.pshape[i] : std::min(8, F.pshape[i] - 8 * b[i]);
@@ -1166,7 +1179,7 @@ __global__ void __launch_bounds__(kLineThreads, 3)
 sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_tables_t T) {
   __shared__ __align__(16) line_dev_t L;
   __shared__ cta_smem S;
-  __shared__ int s_fam;
+  __shared__ int s_fam, s_nmicro;
   extern __shared__ uint4 dyn_smem[];
   const int tid = threadIdx.x, nt = blockDim.x;
   const int line = line0 + blockIdx.x;
@@ -1177,8 +1190,12 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
       if (fams[mid].first_line <= line) lo = mid; else hi = mid - 1;
     }
     s_fam = lo;
+    int b[4];
+    s_nmicro = family_blocks(fams[lo], line - fams[lo].first_line, b);
   }
   __syncthreads();
+  // CTAs past a short line's last microline leave before any set-up
+  if (int(blockIdx.y) * kMicro >= s_nmicro) return;
   const family_t& F = fams[s_fam];
   // copy the prototype (as 16-byte words) and fill in this line
   {
@@ -1350,6 +1367,14 @@ extern "C" int pg_slice_layout(const uint64_t* sigs, int n, int64_t* offsets) {
 
 // The lines of a slice, or (one_child) only those that read child_sigs[0],
 // every line then ORing into the parent slice.
+// CTAs of the sweep kernel an SM holds at this dynamic shared memory (three
+// at most, by registers): 228 KB per SM, each CTA also holding its static
+// shared memory and 1 KB the hardware reserves.
+static int sweep_ctas_per_sm(size_t dyn) {
+  const size_t per = dyn + sizeof(line_dev_t) + sizeof(cta_smem) + 64 + 1024;
+  return int(std::max<size_t>(1, std::min<size_t>(3, (size_t(228) << 10) / per)));
+}
+
 static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_slice, const uint64_t* child_sigs, int nc,
                        const uint64_t* child_slice, bool one_child, void* stream_) {
   if (np < 0 || nc < 0 || (np && (!parent_sigs || !parent_slice))) return fail(PG_ERR_ARG, "bad sweep arguments");
@@ -1364,7 +1389,6 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
     std::vector<family_t> fams;
     record_set recs;
     std::vector<std::pair<size_t, size_t>> rec_off;
-    int total = 0, maxchild = 0, maxpat = 0;
     for (int i = 0; i < np; i++) {
       const section_t sec = section_t::from_sig(parent_sigs[i]);
       if (sec.c[dim][0] + sec.c[dim][1] >= 9) continue;
@@ -1376,10 +1400,6 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
       if (!make_family(sec, dim, poff[i], child_sigs, nc, coff.data(), parent_slice, child_slice,
                        dim == first && !one_child ? PG_LINE_STORE : PG_LINE_OR, F, err))
         return fail(PG_ERR_ARG, "section " + std::to_string(i) + ": " + err);
-      F.first_line = total;
-      total += F.nlines;
-      maxchild = std::max(maxchild, F.proto.nchild);
-      maxpat = std::max(maxpat, F.proto.npat[0] + F.proto.npat[1]);
       rec_off.push_back(recs.add(sec.sig(), dim));
     }
     if (fams.empty()) continue;
@@ -1389,22 +1409,39 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
     PG_CUDA(X.alloc(&recs_dev, rbytes));
     PG_CUDA(cudaMemcpyAsync(recs_dev, recs.words.data(), rbytes, cudaMemcpyHostToDevice, stream));
     for (size_t f = 0; f < fams.size(); f++) bind_line_records(fams[f].proto, recs_dev, rec_off[f]);
-    family_t* d = nullptr;
-    PG_CUDA(X.alloc(&d, sizeof(family_t) * fams.size()));
-    PG_CUDA(cudaMemcpyAsync(d, fams.data(), sizeof(family_t) * fams.size(), cudaMemcpyHostToDevice, stream));
-    const size_t smem = line_smem_bytes(maxpat, maxchild);
-    for (int line0 = 0; line0 < total; line0 += 1 << 30) {
-      const dim3 grid(unsigned(std::min(total - line0, 1 << 30)), (512 + kMicro - 1) / kMicro);
-      int rc = 0;
-      switch (dim) {
+    // One launch per occupancy class: a launch's shared memory is sized for
+    // its largest line, so families whose lines fit three CTAs on an SM do not
+    // run at the occupancy of the longest lines of the dimension.
+    std::vector<family_t> group[3];
+    int gtotal[3] = {0, 0, 0}, gchild[3] = {0, 0, 0}, gpat[3] = {0, 0, 0};
+    for (const family_t& F : fams) {
+      const int pp = F.proto.npat[0] + F.proto.npat[1];
+      const int k = 3 - sweep_ctas_per_sm(line_smem_bytes(pp, F.proto.nchild));
+      group[k].push_back(F);
+      group[k].back().first_line = gtotal[k];
+      gtotal[k] += F.nlines;
+      gchild[k] = std::max(gchild[k], F.proto.nchild);
+      gpat[k] = std::max(gpat[k], pp);
+    }
+    for (int k = 0; k < 3; k++) {
+      if (group[k].empty()) continue;
+      family_t* d = nullptr;
+      PG_CUDA(X.alloc(&d, sizeof(family_t) * group[k].size()));
+      PG_CUDA(cudaMemcpyAsync(d, group[k].data(), sizeof(family_t) * group[k].size(), cudaMemcpyHostToDevice, stream));
+      const size_t smem = line_smem_bytes(gpat[k], gchild[k]);
+      for (int line0 = 0; line0 < gtotal[k]; line0 += 1 << 30) {
+        const dim3 grid(unsigned(std::min(gtotal[k] - line0, 1 << 30)), (512 + kMicro - 1) / kMicro);
+        int rc = 0;
+        switch (dim) {
 #define PG_SWEEP(D) case D: \
-        rc = sweep_smem_limit<D>(); \
-        sweep_kernel<D><<<grid, kLineThreads, smem, stream>>>(d, int(fams.size()), line0, *T); break;
-        PG_SWEEP(0) PG_SWEEP(1) PG_SWEEP(2) PG_SWEEP(3)
+          rc = sweep_smem_limit<D>(); \
+          sweep_kernel<D><<<grid, kLineThreads, smem, stream>>>(d, int(group[k].size()), line0, *T); break;
+          PG_SWEEP(0) PG_SWEEP(1) PG_SWEEP(2) PG_SWEEP(3)
 #undef PG_SWEEP
+        }
+        if (rc) return fail(rc, "cudaFuncSetAttribute failed");
+        PG_CUDA(cudaGetLastError());
       }
-      if (rc) return fail(rc, "cudaFuncSetAttribute failed");
-      PG_CUDA(cudaGetLastError());
     }
   }
   return PG_OK;

@@ -187,6 +187,12 @@ void line_records(uint64_t section, int dim, std::vector<parent_rec>& recs, std:
   const int turn = sec.sum() & 1;
   const int k = rmin_bucket(sec.c[dim][0], sec.c[dim][1]);
   const int n = T.rmin_off[k + 1] - T.rmin_off[k];
+  int nchild = 0;
+  if (sec.sum() < 35) {
+    const section_t child = sec.child(dim);
+    const int kc = rmin_bucket(child.c[dim][0], child.c[dim][1]);
+    nchild = T.rmin_off[kc + 1] - T.rmin_off[kc];
+  }
   recs.assign(n, parent_rec{});
   for (int i = 0; i < n; i++) {
     const uint16_t q = T.rmin_flat[T.rmin_off[k] + i];
@@ -198,7 +204,8 @@ void line_records(uint64_t section, int dim, std::vector<parent_rec>& recs, std:
     int m = 0;
     for (int b = 0, p3 = 1; b < 9; b++, p3 *= 3)
       if (!((s0 | s1) >> b & 1)) {
-        r.mv[m++] = T.rmin_inv[q + (1 + turn) * p3];
+        const int ir = T.rmin_inv[q + (1 + turn) * p3];
+        r.mv[m++] = uint16_t((ir & 3) * nchild + (ir >> 2));
         for (int k = 0; k < 4; k++) r.usub[k] |= T.term_sub[dim][s0 | 1 << b][k];
       }
     r.nmoves = uint8_t(m);

@@ -70,8 +70,10 @@ struct alignas(16) parent_rec {
   uint8_t c0, c1;      // rotation classes (cls_rank) of the mover's / opponent's stone patterns
   uint8_t rot;         // bits 0-1 (2-3): the mover's (opponent's) pattern is its class rotated left this often
   uint8_t nmoves;
-  uint16_t mv[14];     // per empty cell, increasing: rotation_minimal_quadrants_inverse of the child quadrant
-                       // (4 j + r); at most 9 used, mv[0..5] in the first 16 bytes
+  uint16_t mv[14];     // per empty cell, increasing: the child quadrant as rotation r of rotation-minimal
+                       // child j (rotation_minimal_quadrants_inverse = 4 j + r), stored as r * nchild + j
+                       // (pair 0's slot of the child in the line kernel's shared memory, nchild the
+                       // number of child quadrant states); at most 9 used, mv[0..5] in the first 16 bytes
   uint32_t usub[4];    // win terms (term_sub) the mover covers after a stone on some empty cell, per rotation
 };
 static_assert(sizeof(parent_rec) == 48, "parent_rec layout");

@@ -1,6 +1,7 @@
 """The multi-GPU path of bench.py, run on the CPU: two gloo ranks take
-disjoint sets of full blocks (weak scaling, no data exchange) and agree on
-the slowest rank's time, as `bench.py --gpus N` does over NCCL."""
+disjoint sets of full blocks (weak scaling, no data exchange), agree on the
+slowest rank's time and on the parity of every rank's lines, as
+`bench.py --gpus N` does over NCCL."""
 import socket
 from datetime import timedelta
 
@@ -24,7 +25,10 @@ def _rank(rank, world, port, q):
         slowest = bench.max_over_ranks(10.0 * (rank + 1), world, torch.device("cpu"))
         gathered = [None] * world
         dist.all_gather_object(gathered, blocks)
-        q.put((rank, slowest, gathered))
+        # parity: both ranks match, then rank 1 alone reports a mismatch
+        both = bench.combine_parity({"ok": True, "lines_checked": 4}, world, torch.device("cpu"))
+        one_bad = bench.combine_parity({"ok": rank != 1, "lines_checked": 4}, world, torch.device("cpu"))
+        q.put((rank, slowest, gathered, both["ok"], one_bad["ok"]))
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -45,8 +49,9 @@ def test_two_gloo_ranks_shard_blocks_and_take_the_slowest_time():
         p.join(timeout=60)
         assert p.exitcode == 0
     shape = section_shape(section_sig(bench.SECTION))
-    for rank, slowest, gathered in results:
+    for rank, slowest, gathered, both_ok, one_bad_ok in results:
         assert slowest == 20.0
+        assert both_ok and not one_bad_ok
         a, b = (set(map(tuple, g)) for g in gathered)
         assert len(a) == len(b) == 16 and not (a & b)
         for blk in a | b:
