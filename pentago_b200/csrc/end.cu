@@ -274,13 +274,23 @@ PG_HD super8 pattern_rotated(const uint2* pat, int e, int pp, int rho) {
   return r;
 }
 
+// What the children of a line need from its descriptor, read once per thread.
+struct child_src {
+  const uint64_t* input;
+  const int64_t* in_off;
+  int line_moves, last_block;
+};
+PG_HD child_src child_source(const line_dev_t& L) {
+  return child_src{L.input, L.in_off, L.line_moves, L.input_blocks - 1};
+}
+
 // Address of child j of a microline in the line's input.
-PG_HD const uint64_t* child_addr(const line_dev_t& L, const microline_geom& G, int j) {
-  const int jj = j ^ int(j < L.line_moves);
+PG_HD const uint64_t* child_addr(const child_src& C, const microline_geom& G, int j) {
+  const int jj = j ^ int(j < C.line_moves);
   const int blk = j >> 3;
-  const int64_t idx = L.in_off[blk] + (blk == L.input_blocks - 1 ? G.last_input_base : G.input_base) +
+  const int64_t idx = C.in_off[blk] + (blk == C.last_block ? G.last_input_base : G.input_base) +
                       int64_t(G.input_stride) * (jj & 7);
-  return L.input + 8 * idx;
+  return C.input + 8 * idx;
 }
 
 // ---------------------------------------------------------------------------
@@ -422,30 +432,20 @@ PG_HD uint32_t select4(const uint4 v, int i) {
 // that makes the child wins at once, and super_wins of the moved quadrant is
 // W_j translated by the move's rotation exactly as the child's value is, so a
 // parent ORs one translated Q_j for both.
-template<int DIM>
-PG_HD void child_node(const line_dev_t& L, const microline_geom& G, const uint2* tab0, uint4* q, int j,
+template<int DIM, int G>
+PG_HD void child_node(const line_dev_t& L, const microline_geom& geom, const uint2* tab0, uint4* q, int j, int nc,
                       const super8& cw, const super8& cn, const uint4 csub) {
   super8 zw = s_rmax(s_not(cn)), zn = s_rmax(s_not(cw));
-  const int c = ladd(G.base_l, int(L.csym[j]) << 6);   // the translation, axes moved to the line frame
-  switch (L.g) {
-    case 0: child_maps<DIM, 0>(zw, zn, c); break;
-    case 1: child_maps<DIM, 1>(zw, zn, c); break;
-    case 2: child_maps<DIM, 2>(zw, zn, c); break;
-    case 3: child_maps<DIM, 3>(zw, zn, c); break;
-    case 4: child_maps<DIM, 4>(zw, zn, c); break;
-    case 5: child_maps<DIM, 5>(zw, zn, c); break;
-    case 6: child_maps<DIM, 6>(zw, zn, c); break;
-    default: child_maps<DIM, 7>(zw, zn, c); break;
-  }
+  const int c = ladd(geom.base_l, int(L.csym[j]) << 6);   // the translation, axes moved to the line frame
+  child_maps<DIM, G>(zw, zn, c);
   // Pair k goes to pair p(k) = k - c3 (rotation) or c3 - k (reflection), and
   // W_j's pair p(k) is evaluated beside it.
-  const int c3 = c >> 6 & 3, sgn = L.g >= 4 ? -1 : 1;
+  const int c3 = c >> 6 & 3, sgn = G >= 4 ? -1 : 1;
   int pk[4];
 #pragma unroll
   for (int k = 0; k < 4; k++) pk[k] = (sgn * (k - c3)) & 3;
   const super8 w = table_eval(tab0, make_uint4(select4(csub, pk[0]), select4(csub, pk[1]), select4(csub, pk[2]),
                                                 select4(csub, pk[3])));
-  const int nc = L.nchild;
 #pragma unroll
   for (int k = 0; k < 4; k++)
     q[pk[k] * nc + j] = make_uint4(zw.w[2 * k] | w.w[2 * k], zw.w[2 * k + 1] | w.w[2 * k + 1], zn.w[2 * k], zn.w[2 * k + 1]);
@@ -563,7 +563,7 @@ const size_t kMaxLineSmem = line_smem_bytes(2 * kMaxPat, kMaxLine);
 // tables for that side; barrier; super_wins of every pattern class (the
 // first children are loaded meanwhile); barrier; all children into shared
 // memory; barrier; all parents.
-template<int DIM>
+template<int DIM, int G>
 __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_tables_t& T, cta_smem& S,
                                                uint4* dyn, int m0, int M, int tid, int nt) {
   const int nc = L.nchild, np = L.nparent;
@@ -578,21 +578,24 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
   __syncthreads();
   if (warp < 2 * M) {
     const int k = warp >> 1, side = warp & 1;
-    const microline_geom& G = S.ctx[k].G;
-    warp_tables<DIM>(T, side ? G.base_side1 : G.base_side0, side ? tab1 + k * kTab : S.tab[k], lane);
+    const microline_geom& geom = S.ctx[k].G;
+    warp_tables<DIM>(T, side ? geom.base_side1 : geom.base_side0, side ? tab1 + k * kTab : S.tab[k], lane);
   }
   __syncthreads();
   // Each thread's first child is loaded while the patterns are evaluated.
   super8 cw, cn;
   uint4 cs = make_uint4(0, 0, 0, 0);
   const bool children = !L.slice35 && tid < M * nc;
+  const child_src C = child_source(L);
+  const uint4* crecs = reinterpret_cast<const uint4*>(L.crecs);
+  const uint32_t mc = L.split_m[1];
   if (children) {
     int k, j;
-    split(tid, nc, L.split_m[1], k, j);
-    const uint64_t* a = child_addr(L, S.ctx[k].G, j);
+    split(tid, nc, mc, k, j);
+    const uint64_t* a = child_addr(C, S.ctx[k].G, j);
     cw = s_load_ldg(a);
     cn = s_load_ldg(a + 4);
-    cs = ldg(reinterpret_cast<const uint4*>(L.crecs) + j);
+    cs = ldg(crecs + j);
   }
   for (int x = tid; x < M * pp; x += nt) {
     int k, e;
@@ -605,18 +608,18 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
     // Each thread's next child is loaded while it transforms the current one.
     for (int x = tid; x < M * nc; x += nt) {
       int k, j;
-      split(x, nc, L.split_m[1], k, j);
+      split(x, nc, mc, k, j);
       const super8 w = cw, n = cn;
       const uint4 s = cs;
       if (x + nt < M * nc) {
         int kn, jn;
-        split(x + nt, nc, L.split_m[1], kn, jn);
-        const uint64_t* b = child_addr(L, S.ctx[kn].G, jn);
+        split(x + nt, nc, mc, kn, jn);
+        const uint64_t* b = child_addr(C, S.ctx[kn].G, jn);
         cw = s_load_ldg(b);
         cn = s_load_ldg(b + 4);
-        cs = ldg(reinterpret_cast<const uint4*>(L.crecs) + jn);
+        cs = ldg(crecs + jn);
       }
-      child_node<DIM>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, j, w, n, s);
+      child_node<DIM, G>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, j, nc, w, n, s);
     }
   }
   __syncthreads();
@@ -643,12 +646,13 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
   if (errors) record_errors(errors);
 }
 
-// One CTA computes kMicro microlines of one line.
-template<int DIM>
+// One CTA computes kMicro microlines of one line.  All lines of a launch
+// have line axis DIM and children standardized by global symmetry G.
+template<int DIM, int G>
 __global__ void __launch_bounds__(kLineThreads, 3)
 end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
-  const line_dev_t& G = lines[blockIdx.y];
-  const int nmicro = G.cross[0] * G.cross[1] * G.cross[2];
+  const line_dev_t& D = lines[blockIdx.y];
+  const int nmicro = D.cross[0] * D.cross[1] * D.cross[2];
   const int m0 = blockIdx.x * kMicro;
   if (m0 >= nmicro) return;
   const int M = min(kMicro, nmicro - m0);
@@ -657,26 +661,26 @@ end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
   __shared__ cta_smem S;
   extern __shared__ uint4 dyn_smem[];
   {
-    const uint4* src = reinterpret_cast<const uint4*>(&G);
+    const uint4* src = reinterpret_cast<const uint4*>(&D);
     uint4* dst = reinterpret_cast<uint4*>(&L);
     for (int i = threadIdx.x; i < int(sizeof(line_dev_t) / 16); i += blockDim.x) dst[i] = src[i];
   }
   __syncthreads();
-  cta_microlines<DIM>(L, T, S, dyn_smem, m0, M, threadIdx.x, blockDim.x);
+  cta_microlines<DIM, G>(L, T, S, dyn_smem, m0, M, threadIdx.x, blockDim.x);
 }
 
 // The same microline code run sequentially on the host, for CPU self-tests of
 // the kernel arithmetic.  Never used by the device entry points.
-template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_tables_t& T) {
+template<int DIM, int G> static unsigned host_line(const line_dev_t& L, const dev_tables_t& T) {
   const int pp = L.npat[0] + L.npat[1];
   std::vector<uint4> q(4 * std::max(L.nchild, 1));
   std::vector<uint2> pat(4 * std::max(pp, 1));
   unsigned errors = 0;
   uint2 fterm[kTerms], tab[2][kTab];
   for (int m = 0; m < L.cross[0] * L.cross[1] * L.cross[2]; m++) {
-    const microline_geom G = microline_setup<DIM>(L, T, m);
+    const microline_geom geom = microline_setup<DIM>(L, T, m);
     for (int side = 0; side < 2; side++) {
-      const uint64_t sd = side ? G.base_side1 : G.base_side0;
+      const uint64_t sd = side ? geom.base_side1 : geom.base_side0;
       uint64_t c0 = 0;
       for (int u = 0; u < 15; u++) c0 |= miss_fixed<DIM>(T, u, sd);
       for (int t = 0; t < kTerms; t++) {
@@ -691,13 +695,13 @@ template<int DIM> static unsigned host_line(const line_dev_t& L, const dev_table
     }
     if (!L.slice35)
       for (int j = 0; j < L.nchild; j++) {
-        const uint64_t* a = child_addr(L, G, j);
-        child_node<DIM>(L, G, tab[0], q.data(), j, s_load_ldg(a), s_load_ldg(a + 4),
-                        reinterpret_cast<const uint4*>(L.crecs)[j]);
+        const uint64_t* a = child_addr(child_source(L), geom, j);
+        child_node<DIM, G>(L, geom, tab[0], q.data(), j, L.nchild, s_load_ldg(a), s_load_ldg(a + 4),
+                           reinterpret_cast<const uint4*>(L.crecs)[j]);
       }
     for (int i = 0; i < L.nparent; i++) {
       const uint4* rp = reinterpret_cast<const uint4*>(L.recs + i);
-      parent_node<DIM>(L, G, tab[0], q.data(), pat.data(), rp[0], rp, i, &errors);
+      parent_node<DIM>(L, geom, tab[0], q.data(), pat.data(), rp[0], rp, i, &errors);
     }
   }
   return errors;
@@ -749,28 +753,43 @@ struct end_plan {
   cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
 };
 
-template<int DIM> static int set_smem_attr() {
-  return cudaFuncSetAttribute(end_line_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+// Every (line axis, child symmetry) pair the kernels are instantiated for.
+#define PG_FOR_DIM_G(X) \
+  X(0, 0) X(0, 1) X(0, 2) X(0, 3) X(0, 4) X(0, 5) X(0, 6) X(0, 7) \
+  X(1, 0) X(1, 1) X(1, 2) X(1, 3) X(1, 4) X(1, 5) X(1, 6) X(1, 7) \
+  X(2, 0) X(2, 1) X(2, 2) X(2, 3) X(2, 4) X(2, 5) X(2, 6) X(2, 7) \
+  X(3, 0) X(3, 1) X(3, 2) X(3, 3) X(3, 4) X(3, 5) X(3, 6) X(3, 7)
+
+template<int DIM, int G> static int set_smem_attr() {
+  return cudaFuncSetAttribute(end_line_kernel<DIM, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kMaxLineSmem) == cudaSuccess ? 0 : PG_ERR_CUDA;
 }
-template<int DIM> static int set_smem_limit() {
-  return per_device_once((const void*)&set_smem_attr<DIM>, set_smem_attr<DIM>);
+template<int DIM, int G> static int set_smem_limit() {
+  return per_device_once((const void*)&set_smem_attr<DIM, G>, set_smem_attr<DIM, G>);
 }
 
+// The planned lines of one dimension, sorted by child symmetry: one launch
+// per symmetry, so each kernel holds only its own children's transform.
 static int launch_group(const end_plan& P, int dim, cudaStream_t stream, const dev_tables_t& T) {
   const int n = int(P.host[dim].size());
-  if (!n) return PG_OK;
-  const dim3 grid((512 + kMicro - 1) / kMicro, unsigned(n));
   const size_t smem = line_smem_bytes(P.maxpat[dim], P.maxchild[dim]);
-  int rc = 0;
-  switch (dim) {
-    case 0: rc = set_smem_limit<0>(); end_line_kernel<0><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
-    case 1: rc = set_smem_limit<1>(); end_line_kernel<1><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
-    case 2: rc = set_smem_limit<2>(); end_line_kernel<2><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
-    default: rc = set_smem_limit<3>(); end_line_kernel<3><<<grid, kLineThreads, smem, stream>>>(P.dev[dim], T); break;
+  for (int a = 0, b = 0; a < n; a = b) {
+    const int g = P.host[dim][a].g;
+    while (b < n && P.host[dim][b].g == g) b++;
+    const dim3 grid((512 + kMicro - 1) / kMicro, unsigned(b - a));
+    const line_dev_t* lines = P.dev[dim] + a;
+    int rc = PG_ERR_ARG;
+    switch (dim * 8 + g) {
+#define PG_CASE(D, G) case D * 8 + G: \
+      rc = set_smem_limit<D, G>(); \
+      if (!rc) end_line_kernel<D, G><<<grid, kLineThreads, smem, stream>>>(lines, T); \
+      break;
+      PG_FOR_DIM_G(PG_CASE)
+#undef PG_CASE
+    }
+    if (rc) return fail(rc, "cudaFuncSetAttribute failed");
+    PG_CUDA(cudaGetLastError());
   }
-  if (rc) return fail(rc, "cudaFuncSetAttribute failed");
-  PG_CUDA(cudaGetLastError());
   return PG_OK;
 }
 
@@ -820,6 +839,17 @@ static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
     P.maxpat[d.dim] = std::max(P.maxpat[d.dim], d.npat[0] + d.npat[1]);
     P.host[d.dim].push_back(d);
     P.rec_off[d.dim].push_back(off);
+  }
+  for (int dim = 0; dim < 4; dim++) {
+    std::vector<size_t> order(P.host[dim].size());
+    for (size_t i = 0; i < order.size(); i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t b) { return P.host[dim][a].g < P.host[dim][b].g; });
+    std::vector<line_dev_t> h;
+    std::vector<std::pair<size_t, size_t>> r;
+    for (size_t i : order) { h.push_back(P.host[dim][i]); r.push_back(P.rec_off[dim][i]); }
+    P.host[dim].swap(h);
+    P.rec_off[dim].swap(r);
   }
   return PG_OK;
 }
@@ -1007,11 +1037,10 @@ extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
     line_records(lines[i].section, lines[i].dimension, recs, crecs);
     d.recs = recs.data();
     d.crecs = crecs.data();
-    switch (d.dim) {
-      case 0: errors |= host_line<0>(d, T); break;
-      case 1: errors |= host_line<1>(d, T); break;
-      case 2: errors |= host_line<2>(d, T); break;
-      default: errors |= host_line<3>(d, T); break;
+    switch (d.dim * 8 + d.g) {
+#define PG_CASE(D, G) case D * 8 + G: errors |= host_line<D, G>(d, T); break;
+      PG_FOR_DIM_G(PG_CASE)
+#undef PG_CASE
     }
   }
   return errors ? fail(PG_ERR_BOUNDS, "bounds check failed") : PG_OK;
@@ -1174,7 +1203,7 @@ PG_HD void family_offsets(const family_t& F, line_dev_t& L, int start, int step)
   }
 }
 
-template<int DIM>
+template<int DIM, int G>
 __global__ void __launch_bounds__(kLineThreads, 3)
 sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_tables_t T) {
   __shared__ __align__(16) line_dev_t L;
@@ -1212,18 +1241,18 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   const int m0 = blockIdx.y * kMicro;
   if (m0 >= nmicro) return;
   const int M = min(kMicro, nmicro - m0);
-  cta_microlines<DIM>(L, T, S, dyn_smem, m0, M, tid, nt);
+  cta_microlines<DIM, G>(L, T, S, dyn_smem, m0, M, tid, nt);
 }
 
 static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");
 static_assert(sizeof(family_t) % 16 == 0, "family_t array keeps proto 16-byte aligned");
 
-template<int DIM> static int sweep_smem_attr() {
-  return cudaFuncSetAttribute(sweep_kernel<DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template<int DIM, int G> static int sweep_smem_attr() {
+  return cudaFuncSetAttribute(sweep_kernel<DIM, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kMaxLineSmem) == cudaSuccess ? 0 : PG_ERR_CUDA;
 }
-template<int DIM> static int sweep_smem_limit() {
-  return per_device_once((const void*)&sweep_smem_attr<DIM>, sweep_smem_attr<DIM>);
+template<int DIM, int G> static int sweep_smem_limit() {
+  return per_device_once((const void*)&sweep_smem_attr<DIM, G>, sweep_smem_attr<DIM, G>);
 }
 
 // Per-section (we-win, we-win-or-tie, total) counts over distinct positions
@@ -1409,35 +1438,50 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
     PG_CUDA(X.alloc(&recs_dev, rbytes));
     PG_CUDA(cudaMemcpyAsync(recs_dev, recs.words.data(), rbytes, cudaMemcpyHostToDevice, stream));
     for (size_t f = 0; f < fams.size(); f++) bind_line_records(fams[f].proto, recs_dev, rec_off[f]);
-    // One launch per occupancy class: a launch's shared memory is sized for
-    // its largest line, so families whose lines fit three CTAs on an SM do not
-    // run at the occupancy of the longest lines of the dimension.
-    std::vector<family_t> group[3];
-    int gtotal[3] = {0, 0, 0}, gchild[3] = {0, 0, 0}, gpat[3] = {0, 0, 0};
-    for (const family_t& F : fams) {
-      const int pp = F.proto.npat[0] + F.proto.npat[1];
-      const int k = 3 - sweep_ctas_per_sm(line_smem_bytes(pp, F.proto.nchild));
-      group[k].push_back(F);
-      group[k].back().first_line = gtotal[k];
-      gtotal[k] += F.nlines;
-      gchild[k] = std::max(gchild[k], F.proto.nchild);
-      gpat[k] = std::max(gpat[k], pp);
+    // One launch per (occupancy class, child symmetry): a launch's shared
+    // memory is sized for its largest line, so families whose lines fit three
+    // CTAs on an SM do not run at the occupancy of the longest lines of the
+    // dimension, and each kernel holds only its own children's transform.
+    struct group_t { int k, g; size_t first, count; int lines, maxchild, maxpat; };
+    std::vector<size_t> order(fams.size());
+    std::vector<int> klass(fams.size());
+    for (size_t f = 0; f < fams.size(); f++) {
+      order[f] = f;
+      klass[f] = 3 - sweep_ctas_per_sm(line_smem_bytes(fams[f].proto.npat[0] + fams[f].proto.npat[1],
+                                                       fams[f].proto.nchild));
     }
-    for (int k = 0; k < 3; k++) {
-      if (group[k].empty()) continue;
-      family_t* d = nullptr;
-      PG_CUDA(X.alloc(&d, sizeof(family_t) * group[k].size()));
-      PG_CUDA(cudaMemcpyAsync(d, group[k].data(), sizeof(family_t) * group[k].size(), cudaMemcpyHostToDevice, stream));
-      const size_t smem = line_smem_bytes(gpat[k], gchild[k]);
-      for (int line0 = 0; line0 < gtotal[k]; line0 += 1 << 30) {
-        const dim3 grid(unsigned(std::min(gtotal[k] - line0, 1 << 30)), (512 + kMicro - 1) / kMicro);
-        int rc = 0;
-        switch (dim) {
-#define PG_SWEEP(D) case D: \
-          rc = sweep_smem_limit<D>(); \
-          sweep_kernel<D><<<grid, kLineThreads, smem, stream>>>(d, int(group[k].size()), line0, *T); break;
-          PG_SWEEP(0) PG_SWEEP(1) PG_SWEEP(2) PG_SWEEP(3)
-#undef PG_SWEEP
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      return klass[a] != klass[b] ? klass[a] < klass[b] : fams[a].proto.g < fams[b].proto.g;
+    });
+    std::vector<family_t> sorted;
+    std::vector<group_t> groups;
+    for (size_t f : order) {
+      const family_t& F = fams[f];
+      if (groups.empty() || groups.back().k != klass[f] || groups.back().g != F.proto.g)
+        groups.push_back(group_t{klass[f], F.proto.g, sorted.size(), 0, 0, 0, 0});
+      group_t& G = groups.back();
+      sorted.push_back(F);
+      sorted.back().first_line = G.lines;
+      G.count++;
+      G.lines += F.nlines;
+      G.maxchild = std::max(G.maxchild, F.proto.nchild);
+      G.maxpat = std::max(G.maxpat, F.proto.npat[0] + F.proto.npat[1]);
+    }
+    family_t* d = nullptr;
+    PG_CUDA(X.alloc(&d, sizeof(family_t) * sorted.size()));
+    PG_CUDA(cudaMemcpyAsync(d, sorted.data(), sizeof(family_t) * sorted.size(), cudaMemcpyHostToDevice, stream));
+    for (const group_t& G : groups) {
+      const size_t smem = line_smem_bytes(G.maxpat, G.maxchild);
+      for (int line0 = 0; line0 < G.lines; line0 += 1 << 30) {
+        const dim3 grid(unsigned(std::min(G.lines - line0, 1 << 30)), (512 + kMicro - 1) / kMicro);
+        int rc = PG_ERR_ARG;
+        switch (dim * 8 + G.g) {
+#define PG_CASE(D, GG) case D * 8 + GG: \
+          rc = sweep_smem_limit<D, GG>(); \
+          if (!rc) sweep_kernel<D, GG><<<grid, kLineThreads, smem, stream>>>(d + G.first, int(G.count), line0, *T); \
+          break;
+          PG_FOR_DIM_G(PG_CASE)
+#undef PG_CASE
         }
         if (rc) return fail(rc, "cudaFuncSetAttribute failed");
         PG_CUDA(cudaGetLastError());
