@@ -57,6 +57,22 @@ PG_HD void row_strides(const int* shape, int* st) {
   st[0] = shape[3] * shape[2] * shape[1];
 }
 
+// Both sides' stones in the three fixed (cross) quadrants of microline m.
+template<int DIM>
+PG_HD void microline_sides(const line_dev_t& L, const dev_tables_t& T, int m, uint64_t& s0, uint64_t& s1) {
+  const int c1 = L.cross[1], c2 = L.cross[2];
+  s0 = s1 = 0;
+#pragma unroll
+  for (int q = 0, k = 0; q < 4; q++) {
+    if (q == DIM) continue;
+    const int f = k == 0 ? m / (c1 * c2) : k == 1 ? m / c2 % c1 : m % c2;
+    k++;
+    const int qv = ldg(T.rmin_flat + L.rmin_off[q] + 8 * L.block0[q] + f);
+    s0 |= uint64_t(ldg(T.unpack + 2 * qv + L.turn)) << (16 * q);
+    s1 |= uint64_t(ldg(T.unpack + 2 * qv + 1 - L.turn)) << (16 * q);
+  }
+}
+
 // Index bookkeeping of compute_microline (compute.cc:224-281).
 template<int DIM>
 PG_HD microline_geom microline_setup(const line_dev_t& L, const dev_tables_t& T, int m) {
@@ -546,41 +562,43 @@ struct cta_smem {
 };
 
 // Dynamic shared memory: the stone-pattern results of every microline
-// (kMicro x 4 pp uint2), then the children (kMicro x 4 nchild uint4).  Until
-// the children are written their space holds the pattern set-up: the covered
-// terms of every pattern class (pp uint4) and the opponent's subset tables
-// (kMicro x kTab uint2).  Sized per launch for its largest line.
+// (kMicro x 4 pp uint2), the pattern set-up (the covered terms of every
+// pattern class, pp uint4, and the opponent's subset tables, kMicro x kTab
+// uint2), then the children (kMicro x 4 nchild uint4).  The set-up has its
+// own space, so patterns and children are computed in one phase.  Sized per
+// launch for its largest line.
 PG_HD size_t pattern_bytes(int pp) { return size_t(kMicro) * pp * 32; }
 PG_HD size_t setup_bytes(int pp) { return size_t(pp) * 16 + size_t(kMicro) * kTab * 8; }
 inline size_t line_smem_bytes(int pp, int nchild) {
-  return pattern_bytes(pp) + std::max(size_t(kMicro) * nchild * 64, setup_bytes(pp));
+  return pattern_bytes(pp) + setup_bytes(pp) + size_t(kMicro) * nchild * 64;
 }
 const size_t kMaxLineSmem = line_smem_bytes(2 * kMaxPat, kMaxLine);
 
-// A CTA's microlines m0 .. m0 + M - 1.  Set-up: lane k of warp 0 computes
-// microline k's geometry while the other threads stage the covered terms of
-// every pattern class; barrier; warp 2 k + side builds microline k's subset
-// tables for that side; barrier; super_wins of every pattern class (the
-// first children are loaded meanwhile); barrier; all children into shared
-// memory; barrier; all parents.
+// A CTA's microlines m0 .. m0 + M - 1.  Set-up: warp k builds microline
+// k's subset tables for both sides while lane k of warp M computes microline
+// k's geometry and the other threads stage the covered terms of every
+// pattern class; barrier; super_wins of every pattern class, then all
+// children into shared memory (each thread's first child loaded before the
+// patterns); barrier; all parents.
 template<int DIM, int G>
 __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_tables_t& T, cta_smem& S,
                                                uint4* dyn, int m0, int M, int tid, int nt) {
   const int nc = L.nchild, np = L.nparent;
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
   uint2* pats = reinterpret_cast<uint2*>(dyn);         // microline k at 4 pp k
-  uint4* q_smem = dyn + kMicro * 2 * pp;               // microline k at 4 nc k
-  uint4* psub = q_smem;                                // set-up scratch, until the children
+  uint4* psub = dyn + kMicro * 2 * pp;                 // pattern set-up
   uint2* tab1 = reinterpret_cast<uint2*>(psub + pp);   // opponent's tables, microline k at kTab k
+  uint4* q_smem = psub + pp + kMicro * kTab / 2;       // microline k at 4 nc k
   const int warp = tid >> 5, lane = tid & 31;
-  if (tid < M) S.ctx[tid].G = microline_setup<DIM>(L, T, m0 + tid);
-  for (int x = tid; x < pp; x += nt) psub[x] = pattern_terms<DIM>(L, T, x >= p0, x >= p0 ? x - p0 : x);
-  __syncthreads();
-  if (warp < 2 * M) {
-    const int k = warp >> 1, side = warp & 1;
-    const microline_geom& geom = S.ctx[k].G;
-    warp_tables<DIM>(T, side ? geom.base_side1 : geom.base_side0, side ? tab1 + k * kTab : S.tab[k], lane);
+  if (warp < M) {
+    uint64_t s0, s1;
+    microline_sides<DIM>(L, T, m0 + warp, s0, s1);
+    warp_tables<DIM>(T, s0, S.tab[warp], lane);
+    warp_tables<DIM>(T, s1, tab1 + warp * kTab, lane);
+  } else if (warp == M && lane < M) {
+    S.ctx[lane].G = microline_setup<DIM>(L, T, m0 + lane);
   }
+  for (int x = tid; x < pp; x += nt) psub[x] = pattern_terms<DIM>(L, T, x >= p0, x >= p0 ? x - p0 : x);
   __syncthreads();
   // Each thread's first child is loaded while the patterns are evaluated.
   super8 cw, cn;
@@ -603,7 +621,6 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
     const super8 w = table_eval(e >= p0 ? tab1 + k * kTab : S.tab[k], psub[e]);
     pattern_store(pats + 4 * pp * k, e, pp, w);
   }
-  __syncthreads();  // the set-up scratch is free from here on
   if (children) {
     // Each thread's next child is loaded while it transforms the current one.
     for (int x = tid; x < M * nc; x += nt) {
