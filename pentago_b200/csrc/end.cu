@@ -46,7 +46,6 @@ __device__ void record_errors(unsigned e) { atomicOr(&d_end_errors, e); }
 struct microline_geom {
   int64_t input_base, last_input_base, output_base, last_output_base;
   int input_stride, output_stride;
-  uint64_t base_side0, base_side1;
   int base_l;
 };
 
@@ -57,25 +56,11 @@ PG_HD void row_strides(const int* shape, int* st) {
   st[0] = shape[3] * shape[2] * shape[1];
 }
 
-// Both sides' stones in the three fixed (cross) quadrants of microline m.
+// Index bookkeeping of compute_microline (compute.cc:224-281): addressing
+// and the base translation (no global loads; the cross quadrants' stones
+// come from the line's cross records).
 template<int DIM>
-PG_HD void microline_sides(const line_dev_t& L, const dev_tables_t& T, int m, uint64_t& s0, uint64_t& s1) {
-  const int c1 = L.cross[1], c2 = L.cross[2];
-  s0 = s1 = 0;
-#pragma unroll
-  for (int q = 0, k = 0; q < 4; q++) {
-    if (q == DIM) continue;
-    const int f = k == 0 ? m / (c1 * c2) : k == 1 ? m / c2 % c1 : m % c2;
-    k++;
-    const int qv = ldg(T.rmin_flat + L.rmin_off[q] + 8 * L.block0[q] + f);
-    s0 |= uint64_t(ldg(T.unpack + 2 * qv + L.turn)) << (16 * q);
-    s1 |= uint64_t(ldg(T.unpack + 2 * qv + 1 - L.turn)) << (16 * q);
-  }
-}
-
-// Index bookkeeping of compute_microline (compute.cc:224-281).
-template<int DIM>
-PG_HD microline_geom microline_setup(const line_dev_t& L, const dev_tables_t& T, int m) {
+PG_HD microline_geom microline_addressing(const line_dev_t& L, int m) {
   microline_geom G;
   int fb[4];
   const int c1 = L.cross[1], c2 = L.cross[2];
@@ -86,17 +71,6 @@ PG_HD microline_geom microline_setup(const line_dev_t& L, const dev_tables_t& T,
     fb[i] = k == 0 ? m / (c1 * c2) : k == 1 ? m / c2 % c1 : m % c2;
     k++;
   }
-  // Parent quadrants of the cross-section
-  uint64_t s0 = 0, s1 = 0;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    if (q == DIM) continue;
-    const int qv = ldg(T.rmin_flat + L.rmin_off[q] + 8 * L.block0[q] + fb[q]);
-    s0 |= uint64_t(ldg(T.unpack + 2 * qv + L.turn)) << (16 * q);
-    s1 |= uint64_t(ldg(T.unpack + 2 * qv + 1 - L.turn)) << (16 * q);
-  }
-  G.base_side0 = s0;
-  G.base_side1 = s1;
   // Output addressing
   int obs[4], ost[4];
 #pragma unroll
@@ -165,33 +139,40 @@ PG_HD uint64_t axis_broadcast(int a, uint32_t c) {
   return f;
 }
 
-// f_t for term t of quadrant DIM and one side's fixed quadrants sd.
+// The cross quadrants' state indices (in their sections' rotation-minimal
+// lists) of microline m.
 template<int DIM>
-PG_HD uint64_t term_fixed(const dev_tables_t& T, int t, uint64_t sd) {
-  const int p = ldg(T.term_pat + kTerms * DIM + t);
-  uint64_t f = ~uint64_t(0);
+PG_HD void cross_index(const line_dev_t& L, int m, int* xq) {
+  const int c1 = L.cross[1], c2 = L.cross[2];
 #pragma unroll
-  for (int k = 0; k < 2; k++) {
-    const int q = ldg(T.term_other + 2 * (kTerms * DIM + t) + k);
-    if (q > 3) break;
-    const uint32_t c = ldg(T.cov + (4 * p + q) * 512 + int(sd >> (16 * q) & 511));
-    f &= axis_broadcast(q == 3 ? DIM : q, c);
+  for (int q = 0, k = 0; q < 4; q++) {
+    if (q == DIM) { xq[q] = 0; continue; }
+    const int f = k == 0 ? m / (c1 * c2) : k == 1 ? m / c2 % c1 : m % c2;
+    k++;
+    xq[q] = 8 * L.block0[q] + f;
   }
-  return f;
 }
 
-// Product factor of win pattern u among the 15 that miss quadrant DIM (it
-// wins at every rotation of DIM), in the same frame.
+// The factor of lane t of a table warp for one side of a microline (its
+// cross states xq): for t < 17 term t's f_t, else the product of missed
+// pattern t - 17, in the line frame, from the cross records (one load per
+// quadrant the pattern touches, all independent).
 template<int DIM>
-PG_HD uint64_t miss_fixed(const dev_tables_t& T, int u, uint64_t sd) {
-  const int p = ldg(T.miss_pat + 15 * DIM + u);
+PG_HD uint64_t lane_factor(const line_dev_t& L, const int* xq, int side, int t) {
+  const bool term = t < kTerms;
+  const int u = term ? t : t - kTerms;
+  const int p = term ? L.term_pat[u] : L.miss_pat[u];
+  const int nq = term ? 2 : 3;
+  const uint4* xr = reinterpret_cast<const uint4*>(L.xrecs);
   uint64_t f = ~uint64_t(0);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    const int q = ldg(T.miss_quad + 3 * (15 * DIM + u) + k);
+    if (k >= nq) break;
+    const int q = term ? L.term_q[u][k] : L.miss_q[u][k];
     if (q > 3) break;
-    const uint32_t c = ldg(T.cov + (4 * p + q) * 512 + int(sd >> (16 * q) & 511));
-    f &= axis_broadcast(q == 3 ? DIM : q, c);
+    const uint4 e = ldg(xr + L.xoff[q] + 2 * xq[q] + side);
+    const uint32_t w = (p >> 3) == 0 ? e.x : (p >> 3) == 1 ? e.y : (p >> 3) == 2 ? e.z : e.w;
+    f &= axis_broadcast(q == 3 ? DIM : q, w >> (4 * (p & 7)) & 15);
   }
   return f;
 }
@@ -245,14 +226,6 @@ template<int DIM> PG_HD void s_line_frame(super8& s) {
   } else if constexpr (DIM < 2) {
     s_swap_axes<DIM, 3>(s);
   }
-}
-
-// Covered terms of the representative of rotation class r of a side's stone
-// patterns in the line quadrant.
-template<int DIM>
-PG_HD uint4 pattern_terms(const line_dev_t& L, const dev_tables_t& T, int side, int r) {
-  const int mask = ldg(T.cls_masks + L.pat_off[side] + r);
-  return ldg(reinterpret_cast<const uint4*>(T.term_sub) + DIM * 512 + mask);
 }
 
 // x = k n + i with 0 <= i < n, for 0 <= x < 2^20 and m = floor((2^32 - 1) / n):
@@ -531,8 +504,8 @@ PG_HD void parent_node(const line_dev_t& L, const microline_geom& G, const uint2
 // the fixed quadrants), built by one warp: lane t < 17 computes term t,
 // lanes 17-31 the patterns that miss the line quadrant (ORed into c0).
 template<int DIM>
-__device__ __forceinline__ void warp_tables(const dev_tables_t& T, uint64_t sd, uint2* tab, int lane) {
-  const uint64_t f = lane < kTerms ? term_fixed<DIM>(T, lane, sd) : miss_fixed<DIM>(T, lane - kTerms, sd);
+__device__ __forceinline__ void warp_tables(const line_dev_t& L, const int* xq, int side, uint2* tab, int lane) {
+  const uint64_t f = lane_factor<DIM>(L, xq, side, lane);
   uint64_t c0 = lane < kTerms ? 0 : f;
 #pragma unroll
   for (int o = 16; o; o >>= 1) c0 |= __shfl_xor_sync(0xffffffffu, c0, o);
@@ -574,11 +547,12 @@ inline size_t line_smem_bytes(int pp, int nchild) {
 }
 const size_t kMaxLineSmem = line_smem_bytes(2 * kMaxPat, kMaxLine);
 
-// A CTA's microlines m0 .. m0 + M - 1.  Set-up: warp k builds microline
-// k's subset tables for both sides while lane k of warp M computes microline
-// k's geometry and the other threads stage the covered terms of every
-// pattern class; barrier; super_wins of every pattern class, then all
-// children into shared memory (each thread's first child loaded before the
+// A CTA's microlines m0 .. m0 + M - 1.  Set-up: warp 2 k + side builds
+// microline k's subset tables for that side from the cross records (one
+// level of loads), the side-1 warp's lane 0 also the microline's addressing
+// (no loads), and every thread stages the covered terms of the pattern
+// classes; barrier; super_wins of every pattern class, then all children
+// into shared memory (each thread's first child loaded before the
 // patterns); barrier; all parents.
 template<int DIM, int G>
 __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_tables_t& T, cta_smem& S,
@@ -590,15 +564,14 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
   uint2* tab1 = reinterpret_cast<uint2*>(psub + pp);   // opponent's tables, microline k at kTab k
   uint4* q_smem = psub + pp + kMicro * kTab / 2;       // microline k at 4 nc k
   const int warp = tid >> 5, lane = tid & 31;
-  if (warp < M) {
-    uint64_t s0, s1;
-    microline_sides<DIM>(L, T, m0 + warp, s0, s1);
-    warp_tables<DIM>(T, s0, S.tab[warp], lane);
-    warp_tables<DIM>(T, s1, tab1 + warp * kTab, lane);
-  } else if (warp == M && lane < M) {
-    S.ctx[lane].G = microline_setup<DIM>(L, T, m0 + lane);
+  if (warp < 2 * M) {
+    const int k = warp >> 1, side = warp & 1;
+    if (side && lane == 0) S.ctx[k].G = microline_addressing<DIM>(L, m0 + k);
+    int xq[4];
+    cross_index<DIM>(L, m0 + k, xq);
+    warp_tables<DIM>(L, xq, side, side ? tab1 + k * kTab : S.tab[k], lane);
   }
-  for (int x = tid; x < pp; x += nt) psub[x] = pattern_terms<DIM>(L, T, x >= p0, x >= p0 ? x - p0 : x);
+  for (int x = tid; x < pp; x += nt) psub[x] = ldg(reinterpret_cast<const uint4*>(L.precs) + x);
   __syncthreads();
   // Each thread's first child is loaded while the patterns are evaluated.
   super8 cw, cn;
@@ -695,19 +668,21 @@ template<int DIM, int G> static unsigned host_line(const line_dev_t& L, const de
   unsigned errors = 0;
   uint2 fterm[kTerms], tab[2][kTab];
   for (int m = 0; m < L.cross[0] * L.cross[1] * L.cross[2]; m++) {
-    const microline_geom geom = microline_setup<DIM>(L, T, m);
+    const microline_geom geom = microline_addressing<DIM>(L, m);
+    int xq[4];
+    cross_index<DIM>(L, m, xq);
     for (int side = 0; side < 2; side++) {
-      const uint64_t sd = side ? geom.base_side1 : geom.base_side0;
       uint64_t c0 = 0;
-      for (int u = 0; u < 15; u++) c0 |= miss_fixed<DIM>(T, u, sd);
+      for (int u = 0; u < 15; u++) c0 |= lane_factor<DIM>(L, xq, side, kTerms + u);
       for (int t = 0; t < kTerms; t++) {
-        const uint64_t f = term_fixed<DIM>(T, t, sd);
+        const uint64_t f = lane_factor<DIM>(L, xq, side, t);
         fterm[t] = make_uint2(uint32_t(f), uint32_t(f >> 32));
       }
       for (int e = 0; e < kTab; e++) tab[side][e] = table_entry(fterm, c0, e);
       for (int r = 0; r < L.npat[side]; r++) {
-        const super8 w = table_eval(tab[side], pattern_terms<DIM>(L, T, side, r));
-        pattern_store(pat.data(), side ? L.npat[0] + r : r, pp, w);
+        const int e = side ? L.npat[0] + r : r;
+        const super8 w = table_eval(tab[side], reinterpret_cast<const uint4*>(L.precs)[e]);
+        pattern_store(pat.data(), e, pp, w);
       }
     }
     if (!L.slice35)
@@ -726,30 +701,43 @@ template<int DIM, int G> static unsigned host_line(const line_dev_t& L, const de
 
 // The records of the (section, dimension) pairs of a set of lines, back to
 // back in one buffer of 16-byte words (each pair once).
+// Where the records of one (section, dimension) start, in 16-byte words.
+struct rec_loc {
+  size_t parent, child, cross, cls;
+  int32_t xoff[4];
+};
+
 struct record_set {
   std::vector<uint4> words;
-  std::vector<std::pair<uint64_t, std::pair<size_t, size_t>>> seen;
-  // Word offsets of the parent and the child records of (section, dim).
-  std::pair<size_t, size_t> add(uint64_t section, int dim) {
+  std::vector<std::pair<uint64_t, rec_loc>> seen;
+  rec_loc add(uint64_t section, int dim) {
     const uint64_t key = section << 2 | uint64_t(dim);
     for (const auto& kv : seen) if (kv.first == key) return kv.second;
-    std::vector<parent_rec> recs;
-    std::vector<child_rec> crecs;
-    line_records(section, dim, recs, crecs);
-    std::pair<size_t, size_t> off(words.size(), 0);
-    const uint4* pw = reinterpret_cast<const uint4*>(recs.data());
-    words.insert(words.end(), pw, pw + 3 * recs.size());
-    off.second = words.size();
-    const uint4* cw = reinterpret_cast<const uint4*>(crecs.data());
-    words.insert(words.end(), cw, cw + crecs.size());
-    seen.emplace_back(key, off);
-    return off;
+    line_rec_set R;
+    line_records(section, dim, R);
+    rec_loc at;
+    auto put = [&](const void* p, size_t n16) {
+      const size_t o = words.size();
+      const uint4* w = static_cast<const uint4*>(p);
+      words.insert(words.end(), w, w + n16);
+      return o;
+    };
+    at.parent = put(R.recs.data(), 3 * R.recs.size());
+    at.child = put(R.crecs.data(), R.crecs.size());
+    at.cross = put(R.xrecs.data(), R.xrecs.size());
+    at.cls = put(R.precs.data(), R.precs.size());
+    for (int q = 0; q < 4; q++) at.xoff[q] = R.xoff[q];
+    seen.emplace_back(key, at);
+    return at;
   }
 };
 
-static void bind_line_records(line_dev_t& L, const uint4* base, std::pair<size_t, size_t> off) {
-  L.recs = reinterpret_cast<const parent_rec*>(base + off.first);
-  L.crecs = reinterpret_cast<const child_rec*>(base + off.second);
+static void bind_line_records(line_dev_t& L, const uint4* base, const rec_loc& at) {
+  L.recs = reinterpret_cast<const parent_rec*>(base + at.parent);
+  L.crecs = reinterpret_cast<const child_rec*>(base + at.child);
+  L.xrecs = reinterpret_cast<const cross_rec*>(base + at.cross);
+  L.precs = reinterpret_cast<const class_rec*>(base + at.cls);
+  for (int q = 0; q < 4; q++) L.xoff[q] = at.xoff[q];
 }
 
 // A set of planned lines, grouped by dimension, with their descriptors on the device.
@@ -760,7 +748,7 @@ struct end_plan {
   int maxpat[4] = {0, 0, 0, 0};         // most stone-pattern classes (both sides) of a line
   // records of every (section, dimension) used
   record_set recs;
-  std::vector<std::pair<size_t, size_t>> rec_off[4];  // per planned line: its records' word offsets
+  std::vector<rec_loc> rec_off[4];       // per planned line: where its records start
   uint4* recs_dev = nullptr;
   // When the dimensions' lines are independent (dims_independent), the
   // launches of all but the first dimension run on side streams, forked from
@@ -863,7 +851,7 @@ static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
     std::stable_sort(order.begin(), order.end(),
                      [&](size_t a, size_t b) { return P.host[dim][a].g < P.host[dim][b].g; });
     std::vector<line_dev_t> h;
-    std::vector<std::pair<size_t, size_t>> r;
+    std::vector<rec_loc> r;
     for (size_t i : order) { h.push_back(P.host[dim][i]); r.push_back(P.rec_off[dim][i]); }
     P.host[dim].swap(h);
     P.rec_off[dim].swap(r);
@@ -1046,14 +1034,12 @@ extern "C" int pg_selftest_end_lines_host(const pg_line_t* lines, int n) {
   const dev_tables_t T = host_tables_view();
   std::string err;
   unsigned errors = 0;
-  std::vector<parent_rec> recs;
-  std::vector<child_rec> crecs;
   for (int i = 0; i < n; i++) {
     line_dev_t d;
     if (!plan_line(to_in(lines[i]), d, err)) return fail(PG_ERR_ARG, err);
-    line_records(lines[i].section, lines[i].dimension, recs, crecs);
-    d.recs = recs.data();
-    d.crecs = crecs.data();
+    record_set rs;
+    const rec_loc at = rs.add(lines[i].section, lines[i].dimension);
+    bind_line_records(d, rs.words.data(), at);
     switch (d.dim * 8 + d.g) {
 #define PG_CASE(D, G) case D * 8 + G: errors |= host_line<D, G>(d, T); break;
       PG_FOR_DIM_G(PG_CASE)
@@ -1434,7 +1420,7 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
   for (int dim = 0; dim < 4; dim++) {
     std::vector<family_t> fams;
     record_set recs;
-    std::vector<std::pair<size_t, size_t>> rec_off;
+    std::vector<rec_loc> rec_off;
     for (int i = 0; i < np; i++) {
       const section_t sec = section_t::from_sig(parent_sigs[i]);
       if (sec.c[dim][0] + sec.c[dim][1] >= 9) continue;

@@ -166,6 +166,14 @@ bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error) {
     d.pat_off[side] = T.cls_off[k];
     d.npat[side] = T.cls_off[k + 1] - T.cls_off[k];
   }
+  for (int t = 0; t < 17; t++) {
+    d.term_pat[t] = T.term_pat[dim][t];
+    for (int k = 0; k < 2; k++) d.term_q[t][k] = T.term_other[dim][t][k];
+  }
+  for (int u = 0; u < 15; u++) {
+    d.miss_pat[u] = T.miss_pat[dim][u];
+    for (int k = 0; k < 3; k++) d.miss_q[u][k] = T.miss_quad[dim][u][k];
+  }
   const int counts[3] = {d.nparent, d.nchild, d.npat[0] + d.npat[1]};
   for (int i = 0; i < 3; i++) d.split_m[i] = counts[i] > 0 ? 0xffffffffu / uint32_t(counts[i]) : 0u;
   d.input = in.input;
@@ -181,7 +189,9 @@ bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error) {
   return true;
 }
 
-void line_records(uint64_t section, int dim, std::vector<parent_rec>& recs, std::vector<child_rec>& crecs) {
+void line_records(uint64_t section, int dim, line_rec_set& out) {
+  std::vector<parent_rec>& recs = out.recs;
+  std::vector<child_rec>& crecs = out.crecs;
   const auto& T = tables();
   const section_t sec = section_t::from_sig(section);
   const int turn = sec.sum() & 1;
@@ -219,6 +229,30 @@ void line_records(uint64_t section, int dim, std::vector<parent_rec>& recs, std:
     for (int j = 0; j < nc; j++) {
       const uint16_t mover = T.unpack[T.rmin_flat[T.rmin_off[kc] + j]][turn];
       for (int r = 0; r < 4; r++) crecs[j].csub[r] = T.term_sub[dim][mover][r];
+    }
+  }
+  // Cross quadrants: the coverage of every win pattern by each side's stones
+  out.xrecs.clear();
+  for (int q = 0; q < 4; q++) {
+    out.xoff[q] = int32_t(out.xrecs.size());
+    if (q == dim) continue;
+    const int kq = rmin_bucket(sec.c[q][0], sec.c[q][1]);
+    for (int f = T.rmin_off[kq]; f < T.rmin_off[kq + 1]; f++)
+      for (int side = 0; side < 2; side++) {
+        const uint16_t stones = T.unpack[T.rmin_flat[f]][side ? 1 - turn : turn];
+        cross_rec e{};
+        for (int p = 0; p < 32; p++) e.cov[p >> 3] |= uint32_t(T.cov[p][q][stones]) << (4 * (p & 7));
+        out.xrecs.push_back(e);
+      }
+  }
+  // Stone-pattern classes of the line quadrant: the terms they cover
+  out.precs.clear();
+  for (int side = 0; side < 2; side++) {
+    const int kc = sec.c[dim][side ? 1 - turn : turn];
+    for (int r = T.cls_off[kc]; r < T.cls_off[kc + 1]; r++) {
+      class_rec e{};
+      for (int k = 0; k < 4; k++) e.sub[k] = T.term_sub[dim][T.cls_masks[r]][k];
+      out.precs.push_back(e);
     }
   }
 }

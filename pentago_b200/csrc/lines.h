@@ -85,6 +85,22 @@ struct alignas(16) child_rec {
   uint32_t csub[4];
 };
 
+// Per state of a cross quadrant (a quadrant other than the line's) and per
+// side (the mover's, then the opponent's stones): the coverage of all 32 win
+// patterns, 4 bits each (bit r: the side's stones, rotated left r times,
+// cover the pattern's cells in that quadrant), pattern p at bits 4 (p % 8)
+// of word p / 8.
+struct alignas(16) cross_rec {
+  uint32_t cov[4];
+};
+
+// Per rotation class of the line quadrant's stone patterns (the mover's
+// classes, then the opponent's): the win terms its representative covers, per
+// rotation.
+struct alignas(16) class_rec {
+  uint32_t sub[4];
+};
+
 // Everything a CTA needs to compute one microline of a line.  Plain data,
 // copied to the device as is.
 struct alignas(16) line_dev_t {
@@ -103,6 +119,14 @@ struct alignas(16) line_dev_t {
   uint64_t* output;
   const parent_rec* recs;           // nparent records for this (section, dimension)
   const child_rec* crecs;           // nchild records for this (section, dimension)
+  const cross_rec* xrecs;           // cross quadrant q's records start at xrecs + xoff[q], 2 per state
+  const class_rec* precs;           // npat[0] + npat[1] records
+  int32_t xoff[4];
+  // The win patterns touching the line quadrant ("terms") with the one or two
+  // other quadrants each touches, and the 15 that miss it with theirs (0xff: none).
+  uint8_t term_pat[17], term_q[17][2];
+  uint8_t miss_pat[15], miss_q[15][3];
+  uint8_t pad2;
   int64_t in_off[kMaxBlocks], out_off[kMaxBlocks];
   uint8_t csym[kMaxLine];           // reflection rotations along the child dimension (0..3)
   uint8_t xsym[4][8];               // reflection locals of the cross dimensions (axes moved)
@@ -128,11 +152,19 @@ struct line_shapes_t {
 
 // Validate and compute shapes; returns false with a message on bad input.
 bool line_shapes(const line_in_t& in, line_shapes_t& out, std::string& error);
-// Fill the device descriptor (recs and crecs are left null; see line_records).
+// Fill the device descriptor (its record pointers are left null; see line_records).
 bool plan_line(const line_in_t& in, line_dev_t& d, std::string& error);
 
-// The records of a (section, dimension): nparent parent records and (below
-// 35 stones) nchild child records.
-void line_records(uint64_t section, int dim, std::vector<parent_rec>& recs, std::vector<child_rec>& crecs);
+// The records of a (section, dimension): nparent parent records, (below 35
+// stones) nchild child records, the cross quadrants' records (quadrant q's at
+// xoff[q]) and the pattern-class records.
+struct line_rec_set {
+  std::vector<parent_rec> recs;
+  std::vector<child_rec> crecs;
+  std::vector<cross_rec> xrecs;
+  std::vector<class_rec> precs;
+  int32_t xoff[4];
+};
+void line_records(uint64_t section, int dim, line_rec_set& out);
 
 }  // namespace pg
