@@ -153,28 +153,35 @@ PG_HD void cross_index(const line_dev_t& L, int m, int* xq) {
   }
 }
 
-// The factor of lane t of a table warp for one side of a microline (its
-// cross states xq): for t < 17 term t's f_t, else the product of missed
-// pattern t - 17, in the line frame, from the cross records (one load per
-// quadrant the pattern touches, all independent).
+// The factor of lane t of a table warp for one side of a microline: for
+// t < 17 term t's f_t, else the product of missed pattern t - 17, in the
+// line frame, from the side's cross records of the microline's cross
+// quadrant states (xe[c]: the c-th quadrant other than DIM).
 template<int DIM>
-PG_HD uint64_t lane_factor(const line_dev_t& L, const int* xq, int side, int t) {
+PG_HD uint64_t lane_factor(const line_dev_t& L, const uint4* xe, int t) {
   const bool term = t < kTerms;
   const int u = term ? t : t - kTerms;
   const int p = term ? L.term_pat[u] : L.miss_pat[u];
   const int nq = term ? 2 : 3;
-  const uint4* xr = reinterpret_cast<const uint4*>(L.xrecs);
   uint64_t f = ~uint64_t(0);
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     if (k >= nq) break;
     const int q = term ? L.term_q[u][k] : L.miss_q[u][k];
     if (q > 3) break;
-    const uint4 e = ldg(xr + L.xoff[q] + 2 * xq[q] + side);
+    const uint4 e = xe[q - (q > DIM)];
     const uint32_t w = (p >> 3) == 0 ? e.x : (p >> 3) == 1 ? e.y : (p >> 3) == 2 ? e.z : e.w;
     f &= axis_broadcast(q == 3 ? DIM : q, w >> (4 * (p & 7)) & 15);
   }
   return f;
+}
+
+// Where the cross record of one side of a microline's c-th cross quadrant
+// state lies.
+template<int DIM>
+PG_HD const uint4* cross_entry(const line_dev_t& L, const int* xq, int side, int c) {
+  const int q = c + (c >= DIM);
+  return reinterpret_cast<const uint4*>(L.xrecs) + L.xoff[q] + 2 * xq[q] + side;
 }
 
 // Entry e of the subset tables from the 17 f_t; the first table also carries
@@ -504,8 +511,8 @@ PG_HD void parent_node(const line_dev_t& L, const microline_geom& G, const uint2
 // the fixed quadrants), built by one warp: lane t < 17 computes term t,
 // lanes 17-31 the patterns that miss the line quadrant (ORed into c0).
 template<int DIM>
-__device__ __forceinline__ void warp_tables(const line_dev_t& L, const int* xq, int side, uint2* tab, int lane) {
-  const uint64_t f = lane_factor<DIM>(L, xq, side, lane);
+__device__ __forceinline__ void warp_tables(const line_dev_t& L, const uint4* xe, uint2* tab, int lane) {
+  const uint64_t f = lane_factor<DIM>(L, xe, lane);
   uint64_t c0 = lane < kTerms ? 0 : f;
 #pragma unroll
   for (int o = 16; o; o >>= 1) c0 |= __shfl_xor_sync(0xffffffffu, c0, o);
@@ -523,16 +530,43 @@ __device__ __forceinline__ void warp_tables(const line_dev_t& L, const int* xq, 
 }
 
 constexpr int kLineThreads = 256;
-constexpr int kMicro = 4;  // microlines per CTA
+constexpr int kMicro = 4;  // microlines per unit
+constexpr int kUnits = 4;  // units a CTA computes one after another (consecutive, one line)
+// CTAs per line: a line has at most 8^3 microlines.
+constexpr int kUnitGroups = (512 / kMicro + kUnits - 1) / kUnits;
+
+// 16-byte asynchronous copies from global to shared memory (no registers
+// held while they fly); a thread waits only for its own.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned a = unsigned(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 __device__ void record_errors(unsigned e);
 
 // Static shared memory of a CTA: per microline its geometry and the mover's
-// subset tables (the children and the 35-stone parents evaluate them again).
+// subset tables (the children and the 35-stone parents evaluate them again),
+// and the cross records of the unit's microlines ([microline][side][cross
+// quadrant], staged while the previous unit's parents run).
 struct cta_smem {
   micro_ctx ctx[kMicro];
   uint2 tab[kMicro][kTab];
+  uint4 xs[kMicro][2][3];
 };
+
+// Stage the cross records of microlines m0 .. m0 + M - 1 (6 per microline).
+template<int DIM>
+__device__ __forceinline__ void stage_cross(const line_dev_t& L, cta_smem& S, int m0, int M, int tid) {
+  if (tid < 6 * M) {
+    const int k = tid / 6, r = tid - 6 * k, side = r / 3, c = r - 3 * side;
+    int xq[4];
+    cross_index<DIM>(L, m0 + k, xq);
+    cp_async16(&S.xs[k][side][c], cross_entry<DIM>(L, xq, side, c));
+  }
+  cp_async_commit();
+}
 
 // Dynamic shared memory: the stone-pattern results of every microline
 // (kMicro x 4 pp uint2), the pattern set-up (the covered terms of every
@@ -547,16 +581,17 @@ inline size_t line_smem_bytes(int pp, int nchild) {
 }
 const size_t kMaxLineSmem = line_smem_bytes(2 * kMaxPat, kMaxLine);
 
-// A CTA's microlines m0 .. m0 + M - 1.  Set-up: warp 2 k + side builds
-// microline k's subset tables for that side from the cross records (one
-// level of loads), the side-1 warp's lane 0 also the microline's addressing
-// (no loads), and every thread stages the covered terms of the pattern
-// classes; barrier; super_wins of every pattern class, then all children
+// A CTA's units unit0 .. unit0 + nunits - 1 of a line (nmicro microlines),
+// kMicro microlines each.  Once: the covered terms of the pattern classes
+// and the first unit's cross records.  Per unit: barrier; warp 2 k + side
+// builds microline k's subset tables for that side from the staged cross
+// records, the side-1 warp's lane 0 also the microline's addressing (no
+// loads); barrier; super_wins of every pattern class, then all children
 // into shared memory (each thread's first child loaded before the
-// patterns); barrier; all parents.
+// patterns); barrier; the next unit's cross records staged, all parents.
 template<int DIM, int G>
-__device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_tables_t& T, cta_smem& S,
-                                               uint4* dyn, int m0, int M, int tid, int nt) {
+__device__ __forceinline__ void cta_units(const line_dev_t& L, cta_smem& S, uint4* dyn, int unit0, int nunits,
+                                          int nmicro, int tid, int nt) {
   const int nc = L.nchild, np = L.nparent;
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
   uint2* pats = reinterpret_cast<uint2*>(dyn);         // microline k at 4 pp k
@@ -564,88 +599,101 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, const dev_ta
   uint2* tab1 = reinterpret_cast<uint2*>(psub + pp);   // opponent's tables, microline k at kTab k
   uint4* q_smem = psub + pp + kMicro * kTab / 2;       // microline k at 4 nc k
   const int warp = tid >> 5, lane = tid & 31;
-  if (warp < 2 * M) {
-    const int k = warp >> 1, side = warp & 1;
-    if (side && lane == 0) S.ctx[k].G = microline_addressing<DIM>(L, m0 + k);
-    int xq[4];
-    cross_index<DIM>(L, m0 + k, xq);
-    warp_tables<DIM>(L, xq, side, side ? tab1 + k * kTab : S.tab[k], lane);
-  }
-  for (int x = tid; x < pp; x += nt) psub[x] = ldg(reinterpret_cast<const uint4*>(L.precs) + x);
-  __syncthreads();
-  // Each thread's first child is loaded while the patterns are evaluated.
-  super8 cw, cn;
-  uint4 cs = make_uint4(0, 0, 0, 0);
-  const bool children = !L.slice35 && tid < M * nc;
   const child_src C = child_source(L);
   const uint4* crecs = reinterpret_cast<const uint4*>(L.crecs);
-  const uint32_t mc = L.split_m[1];
-  if (children) {
-    int k, j;
-    split(tid, nc, mc, k, j);
-    const uint64_t* a = child_addr(C, S.ctx[k].G, j);
-    cw = s_load_ldg(a);
-    cn = s_load_ldg(a + 4);
-    cs = ldg(crecs + j);
-  }
-  for (int x = tid; x < M * pp; x += nt) {
-    int k, e;
-    split(x, pp, L.split_m[2], k, e);
-    const super8 w = table_eval(e >= p0 ? tab1 + k * kTab : S.tab[k], psub[e]);
-    pattern_store(pats + 4 * pp * k, e, pp, w);
-  }
-  if (children) {
-    // Each thread's next child is loaded while it transforms the current one.
-    for (int x = tid; x < M * nc; x += nt) {
-      int k, j;
-      split(x, nc, mc, k, j);
-      const super8 w = cw, n = cn;
-      const uint4 s = cs;
-      if (x + nt < M * nc) {
-        int kn, jn;
-        split(x + nt, nc, mc, kn, jn);
-        const uint64_t* b = child_addr(C, S.ctx[kn].G, jn);
-        cw = s_load_ldg(b);
-        cn = s_load_ldg(b + 4);
-        cs = ldg(crecs + jn);
-      }
-      child_node<DIM, G>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, j, nc, w, n, s);
-    }
-  }
-  __syncthreads();
-  unsigned errors = 0;
-  // Each thread's next record header is loaded while it computes the current parent.
   const uint4* recs = reinterpret_cast<const uint4*>(L.recs);
-  uint4 h = make_uint4(0, 0, 0, 0);
-  if (tid < M * np) {
-    int k, i;
-    split(tid, np, L.split_m[0], k, i);
-    h = ldg(recs + 3 * i);
-  }
-  for (int x = tid; x < M * np; x += nt) {
-    int k, i;
-    split(x, np, L.split_m[0], k, i);
-    const uint4 a = h;
-    if (x + nt < M * np) {
-      int kn, in;
-      split(x + nt, np, L.split_m[0], kn, in);
-      h = ldg(recs + 3 * in);
+  const uint32_t mc = L.split_m[1];
+  for (int x = tid; x < pp; x += nt) psub[x] = ldg(reinterpret_cast<const uint4*>(L.precs) + x);
+  int m0 = unit0 * kMicro, M = min(kMicro, nmicro - m0);
+  stage_cross<DIM>(L, S, m0, M, tid);
+  cp_async_wait_all();
+  unsigned errors = 0;
+  for (int u = 0;; u++) {
+    __syncthreads();
+    if (warp < 2 * M) {
+      const int k = warp >> 1, side = warp & 1;
+      if (side && lane == 0) S.ctx[k].G = microline_addressing<DIM>(L, m0 + k);
+      warp_tables<DIM>(L, S.xs[k][side], side ? tab1 + k * kTab : S.tab[k], lane);
     }
-    parent_node<DIM>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, pats + 4 * pp * k, a, recs + 3 * i, i, &errors);
+    __syncthreads();
+    // Each thread's first child is loaded while the patterns are evaluated.
+    super8 cw, cn;
+    uint4 cs = make_uint4(0, 0, 0, 0);
+    const bool children = !L.slice35 && tid < M * nc;
+    if (children) {
+      int k, j;
+      split(tid, nc, mc, k, j);
+      const uint64_t* a = child_addr(C, S.ctx[k].G, j);
+      cw = s_load_ldg(a);
+      cn = s_load_ldg(a + 4);
+      cs = ldg(crecs + j);
+    }
+    for (int x = tid; x < M * pp; x += nt) {
+      int k, e;
+      split(x, pp, L.split_m[2], k, e);
+      const super8 w = table_eval(e >= p0 ? tab1 + k * kTab : S.tab[k], psub[e]);
+      pattern_store(pats + 4 * pp * k, e, pp, w);
+    }
+    if (children) {
+      // Each thread's next child is loaded while it transforms the current one.
+      for (int x = tid; x < M * nc; x += nt) {
+        int k, j;
+        split(x, nc, mc, k, j);
+        const super8 w = cw, n = cn;
+        const uint4 s = cs;
+        if (x + nt < M * nc) {
+          int kn, jn;
+          split(x + nt, nc, mc, kn, jn);
+          const uint64_t* b = child_addr(C, S.ctx[kn].G, jn);
+          cw = s_load_ldg(b);
+          cn = s_load_ldg(b + 4);
+          cs = ldg(crecs + jn);
+        }
+        child_node<DIM, G>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, j, nc, w, n, s);
+      }
+    }
+    __syncthreads();
+    // The next unit's cross records fly while the parents are computed.
+    const int m0n = m0 + kMicro;
+    const bool more = u + 1 < nunits && m0n < nmicro;
+    const int Mn = more ? min(kMicro, nmicro - m0n) : 0;
+    if (more) stage_cross<DIM>(L, S, m0n, Mn, tid);
+    // Each thread's next record header is loaded while it computes the current parent.
+    uint4 h = make_uint4(0, 0, 0, 0);
+    if (tid < M * np) {
+      int k, i;
+      split(tid, np, L.split_m[0], k, i);
+      h = ldg(recs + 3 * i);
+    }
+    for (int x = tid; x < M * np; x += nt) {
+      int k, i;
+      split(x, np, L.split_m[0], k, i);
+      const uint4 a = h;
+      if (x + nt < M * np) {
+        int kn, in;
+        split(x + nt, np, L.split_m[0], kn, in);
+        h = ldg(recs + 3 * in);
+      }
+      parent_node<DIM>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, pats + 4 * pp * k, a, recs + 3 * i, i, &errors);
+    }
+    if (!more) break;
+    cp_async_wait_all();
+    m0 = m0n;
+    M = Mn;
   }
   if (errors) record_errors(errors);
 }
 
-// One CTA computes kMicro microlines of one line.  All lines of a launch
-// have line axis DIM and children standardized by global symmetry G.
+// One CTA computes kUnits units of kMicro microlines of one line.  All
+// lines of a launch have line axis DIM and children standardized by global
+// symmetry G.
 template<int DIM, int G>
 __global__ void __launch_bounds__(kLineThreads, 3)
 end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
   const line_dev_t& D = lines[blockIdx.y];
   const int nmicro = D.cross[0] * D.cross[1] * D.cross[2];
-  const int m0 = blockIdx.x * kMicro;
-  if (m0 >= nmicro) return;
-  const int M = min(kMicro, nmicro - m0);
+  const int unit0 = blockIdx.x * kUnits;
+  if (unit0 * kMicro >= nmicro) return;
   // The descriptor is read throughout; shared memory keeps those reads short.
   __shared__ __align__(16) line_dev_t L;
   __shared__ cta_smem S;
@@ -656,7 +704,7 @@ end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
     for (int i = threadIdx.x; i < int(sizeof(line_dev_t) / 16); i += blockDim.x) dst[i] = src[i];
   }
   __syncthreads();
-  cta_microlines<DIM, G>(L, T, S, dyn_smem, m0, M, threadIdx.x, blockDim.x);
+  cta_units<DIM, G>(L, S, dyn_smem, unit0, kUnits, nmicro, threadIdx.x, blockDim.x);
 }
 
 // The same microline code run sequentially on the host, for CPU self-tests of
@@ -672,10 +720,12 @@ template<int DIM, int G> static unsigned host_line(const line_dev_t& L, const de
     int xq[4];
     cross_index<DIM>(L, m, xq);
     for (int side = 0; side < 2; side++) {
+      uint4 xe[3];
+      for (int c = 0; c < 3; c++) xe[c] = *cross_entry<DIM>(L, xq, side, c);
       uint64_t c0 = 0;
-      for (int u = 0; u < 15; u++) c0 |= lane_factor<DIM>(L, xq, side, kTerms + u);
+      for (int u = 0; u < 15; u++) c0 |= lane_factor<DIM>(L, xe, kTerms + u);
       for (int t = 0; t < kTerms; t++) {
-        const uint64_t f = lane_factor<DIM>(L, xq, side, t);
+        const uint64_t f = lane_factor<DIM>(L, xe, t);
         fterm[t] = make_uint2(uint32_t(f), uint32_t(f >> 32));
       }
       for (int e = 0; e < kTab; e++) tab[side][e] = table_entry(fterm, c0, e);
@@ -781,7 +831,7 @@ static int launch_group(const end_plan& P, int dim, cudaStream_t stream, const d
   for (int a = 0, b = 0; a < n; a = b) {
     const int g = P.host[dim][a].g;
     while (b < n && P.host[dim][b].g == g) b++;
-    const dim3 grid((512 + kMicro - 1) / kMicro, unsigned(b - a));
+    const dim3 grid(kUnitGroups, unsigned(b - a));
     const line_dev_t* lines = P.dev[dim] + a;
     int rc = PG_ERR_ARG;
     switch (dim * 8 + g) {
@@ -1227,7 +1277,7 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   }
   __syncthreads();
   // CTAs past a short line's last microline leave before any set-up
-  if (int(blockIdx.y) * kMicro >= s_nmicro) return;
+  if (int(blockIdx.y) * kUnits * kMicro >= s_nmicro) return;
   const family_t& F = fams[s_fam];
   // copy the prototype (as 16-byte words) and fill in this line
   {
@@ -1241,10 +1291,7 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   family_offsets(F, L, tid, nt);
   __syncthreads();
   const int nmicro = L.cross[0] * L.cross[1] * L.cross[2];
-  const int m0 = blockIdx.y * kMicro;
-  if (m0 >= nmicro) return;
-  const int M = min(kMicro, nmicro - m0);
-  cta_microlines<DIM, G>(L, T, S, dyn_smem, m0, M, tid, nt);
+  cta_units<DIM, G>(L, S, dyn_smem, int(blockIdx.y) * kUnits, kUnits, nmicro, tid, nt);
 }
 
 static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");
@@ -1476,7 +1523,7 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
     for (const group_t& G : groups) {
       const size_t smem = line_smem_bytes(G.maxpat, G.maxchild);
       for (int line0 = 0; line0 < G.lines; line0 += 1 << 30) {
-        const dim3 grid(unsigned(std::min(G.lines - line0, 1 << 30)), (512 + kMicro - 1) / kMicro);
+        const dim3 grid(unsigned(std::min(G.lines - line0, 1 << 30)), kUnitGroups);
         int rc = PG_ERR_ARG;
         switch (dim * 8 + G.g) {
 #define PG_CASE(D, GG) case D * 8 + GG: \
