@@ -407,44 +407,47 @@ template<bool REFL> PG_HD void axis_maps(super8& s, int c0, int c1, int c2) {
   }
 }
 
-template<int DIM, int G> PG_HD void child_maps(super8& a, super8& b, int c) {
+template<int DIM, int G> PG_HD void child_map(super8& a, int c) {
   line_permute<DIM, G>(a);
-  line_permute<DIM, G>(b);
   axis_maps<(G >= 4)>(a, c & 3, c >> 2 & 3, c >> 4 & 3);
-  axis_maps<(G >= 4)>(b, c & 3, c >> 2 & 3, c >> 4 & 3);
 }
 
 PG_HD uint32_t select4(const uint4 v, int i) {
   return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
 }
 
-// Child j (its node: cw = win, cn = not lost) -> Q_j in the line frame, both
-// halves already moved into the parent's frame: Q_j = swap(phi_g(rmax(~child)
-// - l_j)), done as a fixed axis permutation of rmax(~child) and a rotation or
-// reflection of each line-frame axis (see axis_maps); the map of axis 3, the
-// child's own line axis, is applied by the addresses of the stored word
-// pairs.  The win half also carries W_j = super_wins of the mover's stones
-// once the move is made (csub: the terms they cover per rotation): a move
-// that makes the child wins at once, and super_wins of the moved quadrant is
-// W_j translated by the move's rotation exactly as the child's value is, so a
-// parent ORs one translated Q_j for both.
+// Child j -> Q_j in the line frame, both halves already moved into the
+// parent's frame: Q_j = swap(phi_g(rmax(~child) - l_j)), done as a fixed
+// axis permutation of rmax(~child) and a rotation or reflection of each
+// line-frame axis (see axis_maps); the map of axis 3, the child's own line
+// axis, is applied by the addresses of the stored word pairs.  The win half
+// also carries W_j = super_wins of the mover's stones once the move is made
+// (csub: the terms they cover per rotation): a move that makes the child
+// wins at once, and super_wins of the moved quadrant is W_j translated by the
+// move's rotation exactly as the child's value is, so a parent ORs one
+// translated Q_j for both.
+//
+// The two halves are independent and computed by adjacent threads: half 0
+// is the win half (x = the child's not-lost super, with W_j), half 1 the
+// not-lost half (x = its win super).  q2 holds pair p of Q_j as the uint2
+// halves 2 (p nc + j) + half.
 template<int DIM, int G>
-PG_HD void child_node(const line_dev_t& L, const microline_geom& geom, const uint2* tab0, uint4* q, int j, int nc,
-                      const super8& cw, const super8& cn, const uint4 csub) {
-  super8 zw = s_rmax(s_not(cn)), zn = s_rmax(s_not(cw));
+PG_HD void child_half(const line_dev_t& L, const microline_geom& geom, const uint2* tab0, uint2* q2, int j, int nc,
+                      int half, const super8& x, const uint4 csub) {
+  super8 z = s_rmax(s_not(x));
   const int c = ladd(geom.base_l, int(L.csym[j]) << 6);   // the translation, axes moved to the line frame
-  child_maps<DIM, G>(zw, zn, c);
+  child_map<DIM, G>(z, c);
   // Pair k goes to pair p(k) = k - c3 (rotation) or c3 - k (reflection), and
   // W_j's pair p(k) is evaluated beside it.
   const int c3 = c >> 6 & 3, sgn = G >= 4 ? -1 : 1;
   int pk[4];
 #pragma unroll
   for (int k = 0; k < 4; k++) pk[k] = (sgn * (k - c3)) & 3;
-  const super8 w = table_eval(tab0, make_uint4(select4(csub, pk[0]), select4(csub, pk[1]), select4(csub, pk[2]),
-                                                select4(csub, pk[3])));
+  if (half == 0)
+    z = s_or(z, table_eval(tab0, make_uint4(select4(csub, pk[0]), select4(csub, pk[1]), select4(csub, pk[2]),
+                                            select4(csub, pk[3]))));
 #pragma unroll
-  for (int k = 0; k < 4; k++)
-    q[pk[k] * nc + j] = make_uint4(zw.w[2 * k] | w.w[2 * k], zw.w[2 * k + 1] | w.w[2 * k + 1], zn.w[2 * k], zn.w[2 * k + 1]);
+  for (int k = 0; k < 4; k++) q2[2 * (pk[k] * nc + j) + half] = make_uint2(z.w[2 * k], z.w[2 * k + 1]);
 }
 
 // Parent i of a microline (compute.cc:308-356), in the line frame until its
@@ -530,11 +533,9 @@ __device__ __forceinline__ void warp_tables(const line_dev_t& L, const uint4* xe
 }
 
 constexpr int kLineThreads = 256;
-constexpr int kMicro = 4;  // microlines per unit
-constexpr int kUnits = 4;  // units a CTA computes one after another (consecutive, one line)
-// CTAs per line: a line has at most 8^3 microlines.
-constexpr int kUnitGroups = (512 / kMicro + kUnits - 1) / kUnits;
-
+// CTAs per SM the line kernels are compiled for (64 registers a thread): a
+// CTA's set-up and phase changes are latency chains, which other CTAs cover.
+constexpr int kLineCtasPerSm = 4;
 // 16-byte asynchronous copies from global to shared memory (no registers
 // held while they fly); a thread waits only for its own.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -546,19 +547,19 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 __device__ void record_errors(unsigned e);
 
-// Static shared memory of a CTA: per microline its geometry and the mover's
-// subset tables (the children and the 35-stone parents evaluate them again),
-// and the cross records of the unit's microlines ([microline][side][cross
-// quadrant], staged while the previous unit's parents run).
-struct cta_smem {
-  micro_ctx ctx[kMicro];
-  uint2 tab[kMicro][kTab];
-  uint4 xs[kMicro][2][3];
+// Static shared memory of a CTA of MICRO microlines: per microline its
+// geometry, the mover's subset tables (the children and the 35-stone parents
+// evaluate them again) and its cross records ([microline][side][cross
+// quadrant]).
+template<int MICRO> struct cta_smem {
+  micro_ctx ctx[MICRO];
+  uint2 tab[MICRO][kTab];
+  uint4 xs[MICRO][2][3];
 };
 
 // Stage the cross records of microlines m0 .. m0 + M - 1 (6 per microline).
-template<int DIM>
-__device__ __forceinline__ void stage_cross(const line_dev_t& L, cta_smem& S, int m0, int M, int tid) {
+template<int DIM, int MICRO>
+__device__ __forceinline__ void stage_cross(const line_dev_t& L, cta_smem<MICRO>& S, int m0, int M, int tid) {
   if (tid < 6 * M) {
     const int k = tid / 6, r = tid - 6 * k, side = r / 3, c = r - 3 * side;
     int xq[4];
@@ -568,135 +569,134 @@ __device__ __forceinline__ void stage_cross(const line_dev_t& L, cta_smem& S, in
   cp_async_commit();
 }
 
-// Dynamic shared memory: the stone-pattern results of every microline
-// (kMicro x 4 pp uint2), the pattern set-up (the covered terms of every
-// pattern class, pp uint4, and the opponent's subset tables, kMicro x kTab
-// uint2), then the children (kMicro x 4 nchild uint4).  The set-up has its
-// own space, so patterns and children are computed in one phase.  Sized per
-// launch for its largest line.
-PG_HD size_t pattern_bytes(int pp) { return size_t(kMicro) * pp * 32; }
-PG_HD size_t setup_bytes(int pp) { return size_t(pp) * 16 + size_t(kMicro) * kTab * 8; }
-inline size_t line_smem_bytes(int pp, int nchild) {
-  return pattern_bytes(pp) + setup_bytes(pp) + size_t(kMicro) * nchild * 64;
+// Dynamic shared memory of a CTA of `micro` microlines: the stone-pattern
+// results of every microline (micro x 4 pp uint2), the pattern set-up (the
+// covered terms of every pattern class, pp uint4, and the opponent's subset
+// tables, micro x kTab uint2), then the children (micro x 4 nchild uint4).
+// The set-up has its own space, so patterns and children are computed in one
+// phase.  Sized per launch for its largest line.
+PG_HD size_t pattern_bytes(int pp, int micro) { return size_t(micro) * pp * 32; }
+PG_HD size_t setup_bytes(int pp, int micro) { return size_t(pp) * 16 + size_t(micro) * kTab * 8; }
+inline size_t line_smem_bytes(int pp, int nchild, int micro) {
+  return pattern_bytes(pp, micro) + setup_bytes(pp, micro) + size_t(micro) * nchild * 64;
 }
-const size_t kMaxLineSmem = line_smem_bytes(2 * kMaxPat, kMaxLine);
+const size_t kMaxLineSmem = line_smem_bytes(2 * kMaxPat, kMaxLine, 4);
 
-// A CTA's units unit0 .. unit0 + nunits - 1 of a line (nmicro microlines),
-// kMicro microlines each.  Once: the covered terms of the pattern classes
-// and the first unit's cross records.  Per unit: barrier; warp 2 k + side
-// builds microline k's subset tables for that side from the staged cross
-// records, the side-1 warp's lane 0 also the microline's addressing (no
-// loads); barrier; super_wins of every pattern class, then all children
-// into shared memory (each thread's first child loaded before the
-// patterns); barrier; the next unit's cross records staged, all parents.
-template<int DIM, int G>
-__device__ __forceinline__ void cta_units(const line_dev_t& L, cta_smem& S, uint4* dyn, int unit0, int nunits,
-                                          int nmicro, int tid, int nt) {
+// Microlines per CTA for a launch whose lines have at most np parents, pp
+// pattern classes and nc children per microline: 8 when a microline is short
+// (so a CTA's threads have about as many parents as on long lines, and its
+// set-up is spread over as much work) and 8 still fit 4 CTAs to an SM, else 4.
+inline int line_micro(int np, int pp, int nc) {
+  return np <= 192 && line_smem_bytes(pp, nc, 8) <= (size_t(48) << 10) ? 8 : 4;
+}
+
+// Microlines m0 .. m0 + M - 1 (M <= MICRO) of a line.  Set-up: the covered
+// terms of the pattern classes and the microlines' cross records are staged,
+// and the microlines' addressing worked out (no loads); barrier; each
+// thread's first child requested, and warp w builds the subset tables of
+// side w & 1 of microline w >> 1 (and w + 8 and so on) from the staged
+// records; barrier; super_wins of every pattern class, then all children
+// into shared memory; each thread's first parent record requested; barrier;
+// all parents.
+template<int DIM, int G, int MICRO>
+__device__ __forceinline__ void cta_microlines(const line_dev_t& L, cta_smem<MICRO>& S, uint4* dyn, int m0, int M,
+                                               int tid, int nt) {
   const int nc = L.nchild, np = L.nparent;
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
   uint2* pats = reinterpret_cast<uint2*>(dyn);         // microline k at 4 pp k
-  uint4* psub = dyn + kMicro * 2 * pp;                 // pattern set-up
+  uint4* psub = dyn + MICRO * 2 * pp;                  // pattern set-up
   uint2* tab1 = reinterpret_cast<uint2*>(psub + pp);   // opponent's tables, microline k at kTab k
-  uint4* q_smem = psub + pp + kMicro * kTab / 2;       // microline k at 4 nc k
+  uint4* q_smem = psub + pp + MICRO * kTab / 2;        // microline k at 4 nc k
   const int warp = tid >> 5, lane = tid & 31;
   const child_src C = child_source(L);
   const uint4* crecs = reinterpret_cast<const uint4*>(L.crecs);
   const uint4* recs = reinterpret_cast<const uint4*>(L.recs);
   const uint32_t mc = L.split_m[1];
-  for (int x = tid; x < pp; x += nt) psub[x] = ldg(reinterpret_cast<const uint4*>(L.precs) + x);
-  int m0 = unit0 * kMicro, M = min(kMicro, nmicro - m0);
   stage_cross<DIM>(L, S, m0, M, tid);
+  for (int x = tid; x < pp; x += nt) psub[x] = ldg(reinterpret_cast<const uint4*>(L.precs) + x);
+  // The last warp's first M lanes work out the microlines' addressing while
+  // the records fly.
+  if (tid >= nt - 32 && lane < M) S.ctx[lane].G = microline_addressing<DIM>(L, m0 + lane);
   cp_async_wait_all();
-  unsigned errors = 0;
-  for (int u = 0;; u++) {
-    __syncthreads();
-    if (warp < 2 * M) {
-      const int k = warp >> 1, side = warp & 1;
-      if (side && lane == 0) S.ctx[k].G = microline_addressing<DIM>(L, m0 + k);
-      warp_tables<DIM>(L, S.xs[k][side], side ? tab1 + k * kTab : S.tab[k], lane);
-    }
-    __syncthreads();
-    // Each thread's first child is loaded while the patterns are evaluated.
-    super8 cw, cn;
-    uint4 cs = make_uint4(0, 0, 0, 0);
-    const bool children = !L.slice35 && tid < M * nc;
-    if (children) {
+  __syncthreads();
+  // Each thread's first child half is requested before the tables are built
+  // and the patterns evaluated; adjacent threads take the two halves of a
+  // child.
+  const int half = tid & 1;
+  super8 cx;
+  uint4 cs = make_uint4(0, 0, 0, 0);
+  const bool children = !L.slice35 && tid < 2 * M * nc;
+  if (children) {
+    int k, j;
+    split(tid >> 1, nc, mc, k, j);
+    cx = s_load_ldg(child_addr(C, S.ctx[k].G, j) + 4 * (1 - half));
+    if (!half) cs = ldg(crecs + j);
+  }
+  for (int w = warp; w < 2 * M; w += nt >> 5) {
+    const int k = w >> 1;
+    warp_tables<DIM>(L, S.xs[k][w & 1], w & 1 ? tab1 + k * kTab : S.tab[k], lane);
+  }
+  __syncthreads();
+  for (int x = tid; x < M * pp; x += nt) {
+    int k, e;
+    split(x, pp, L.split_m[2], k, e);
+    const super8 w = table_eval(e >= p0 ? tab1 + k * kTab : S.tab[k], psub[e]);
+    pattern_store(pats + 4 * pp * k, e, pp, w);
+  }
+  if (children) {
+    // Each thread's next child half is loaded while it transforms the
+    // current one (nt is even, so a thread keeps its half).
+    for (int x = tid; x < 2 * M * nc; x += nt) {
       int k, j;
-      split(tid, nc, mc, k, j);
-      const uint64_t* a = child_addr(C, S.ctx[k].G, j);
-      cw = s_load_ldg(a);
-      cn = s_load_ldg(a + 4);
-      cs = ldg(crecs + j);
-    }
-    for (int x = tid; x < M * pp; x += nt) {
-      int k, e;
-      split(x, pp, L.split_m[2], k, e);
-      const super8 w = table_eval(e >= p0 ? tab1 + k * kTab : S.tab[k], psub[e]);
-      pattern_store(pats + 4 * pp * k, e, pp, w);
-    }
-    if (children) {
-      // Each thread's next child is loaded while it transforms the current one.
-      for (int x = tid; x < M * nc; x += nt) {
-        int k, j;
-        split(x, nc, mc, k, j);
-        const super8 w = cw, n = cn;
-        const uint4 s = cs;
-        if (x + nt < M * nc) {
-          int kn, jn;
-          split(x + nt, nc, mc, kn, jn);
-          const uint64_t* b = child_addr(C, S.ctx[kn].G, jn);
-          cw = s_load_ldg(b);
-          cn = s_load_ldg(b + 4);
-          cs = ldg(crecs + jn);
-        }
-        child_node<DIM, G>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, j, nc, w, n, s);
+      split(x >> 1, nc, mc, k, j);
+      const super8 v = cx;
+      const uint4 s = cs;
+      if (x + nt < 2 * M * nc) {
+        int kn, jn;
+        split((x + nt) >> 1, nc, mc, kn, jn);
+        cx = s_load_ldg(child_addr(C, S.ctx[kn].G, jn) + 4 * (1 - half));
+        if (!half) cs = ldg(crecs + jn);
       }
+      child_half<DIM, G>(L, S.ctx[k].G, S.tab[k], reinterpret_cast<uint2*>(q_smem + 4 * k * nc), j, nc, half, v, s);
     }
-    __syncthreads();
-    // The next unit's cross records fly while the parents are computed.
-    const int m0n = m0 + kMicro;
-    const bool more = u + 1 < nunits && m0n < nmicro;
-    const int Mn = more ? min(kMicro, nmicro - m0n) : 0;
-    if (more) stage_cross<DIM>(L, S, m0n, Mn, tid);
-    // Each thread's next record header is loaded while it computes the current parent.
-    uint4 h = make_uint4(0, 0, 0, 0);
-    if (tid < M * np) {
-      int k, i;
-      split(tid, np, L.split_m[0], k, i);
-      h = ldg(recs + 3 * i);
+  }
+  // Each thread's first record header is requested before the barrier, the
+  // next one while it computes the current parent.
+  uint4 h = make_uint4(0, 0, 0, 0);
+  if (tid < M * np) {
+    int k, i;
+    split(tid, np, L.split_m[0], k, i);
+    h = ldg(recs + 3 * i);
+  }
+  __syncthreads();
+  unsigned errors = 0;
+  for (int x = tid; x < M * np; x += nt) {
+    int k, i;
+    split(x, np, L.split_m[0], k, i);
+    const uint4 a = h;
+    if (x + nt < M * np) {
+      int kn, in;
+      split(x + nt, np, L.split_m[0], kn, in);
+      h = ldg(recs + 3 * in);
     }
-    for (int x = tid; x < M * np; x += nt) {
-      int k, i;
-      split(x, np, L.split_m[0], k, i);
-      const uint4 a = h;
-      if (x + nt < M * np) {
-        int kn, in;
-        split(x + nt, np, L.split_m[0], kn, in);
-        h = ldg(recs + 3 * in);
-      }
-      parent_node<DIM>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, pats + 4 * pp * k, a, recs + 3 * i, i, &errors);
-    }
-    if (!more) break;
-    cp_async_wait_all();
-    m0 = m0n;
-    M = Mn;
+    parent_node<DIM>(L, S.ctx[k].G, S.tab[k], q_smem + 4 * k * nc, pats + 4 * pp * k, a, recs + 3 * i, i, &errors);
   }
   if (errors) record_errors(errors);
 }
 
-// One CTA computes kUnits units of kMicro microlines of one line.  All
-// lines of a launch have line axis DIM and children standardized by global
-// symmetry G.
-template<int DIM, int G>
-__global__ void __launch_bounds__(kLineThreads, 3)
+// One CTA computes MICRO consecutive microlines of one line (fewer at the
+// line's end).  All lines of a launch have line axis DIM and children
+// standardized by global symmetry G.
+template<int DIM, int G, int MICRO>
+__global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm)
 end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
   const line_dev_t& D = lines[blockIdx.y];
   const int nmicro = D.cross[0] * D.cross[1] * D.cross[2];
-  const int unit0 = blockIdx.x * kUnits;
-  if (unit0 * kMicro >= nmicro) return;
+  const int m0 = blockIdx.x * MICRO;
+  if (m0 >= nmicro) return;
   // The descriptor is read throughout; shared memory keeps those reads short.
   __shared__ __align__(16) line_dev_t L;
-  __shared__ cta_smem S;
+  __shared__ cta_smem<MICRO> S;
   extern __shared__ uint4 dyn_smem[];
   {
     const uint4* src = reinterpret_cast<const uint4*>(&D);
@@ -704,7 +704,7 @@ end_line_kernel(const line_dev_t* __restrict__ lines, const dev_tables_t T) {
     for (int i = threadIdx.x; i < int(sizeof(line_dev_t) / 16); i += blockDim.x) dst[i] = src[i];
   }
   __syncthreads();
-  cta_units<DIM, G>(L, S, dyn_smem, unit0, kUnits, nmicro, threadIdx.x, blockDim.x);
+  cta_microlines<DIM, G, MICRO>(L, S, dyn_smem, m0, min(MICRO, nmicro - m0), threadIdx.x, blockDim.x);
 }
 
 // The same microline code run sequentially on the host, for CPU self-tests of
@@ -738,8 +738,9 @@ template<int DIM, int G> static unsigned host_line(const line_dev_t& L, const de
     if (!L.slice35)
       for (int j = 0; j < L.nchild; j++) {
         const uint64_t* a = child_addr(child_source(L), geom, j);
-        child_node<DIM, G>(L, geom, tab[0], q.data(), j, L.nchild, s_load_ldg(a), s_load_ldg(a + 4),
-                           reinterpret_cast<const uint4*>(L.crecs)[j]);
+        for (int half = 0; half < 2; half++)
+          child_half<DIM, G>(L, geom, tab[0], reinterpret_cast<uint2*>(q.data()), j, L.nchild, half,
+                             s_load_ldg(a + 4 * (1 - half)), reinterpret_cast<const uint4*>(L.crecs)[j]);
       }
     for (int i = 0; i < L.nparent; i++) {
       const uint4* rp = reinterpret_cast<const uint4*>(L.recs + i);
@@ -796,6 +797,8 @@ struct end_plan {
   line_dev_t* dev[4] = {nullptr, nullptr, nullptr, nullptr};
   int maxchild[4] = {0, 0, 0, 0};
   int maxpat[4] = {0, 0, 0, 0};         // most stone-pattern classes (both sides) of a line
+  int maxparent[4] = {0, 0, 0, 0};      // most parents of a microline
+  int order[4] = {3, 2, 1, 0};          // launch order: longest CTAs (most parents per microline) first
   // records of every (section, dimension) used
   record_set recs;
   std::vector<rec_loc> rec_off[4];       // per planned line: where its records start
@@ -815,29 +818,36 @@ struct end_plan {
   X(2, 0) X(2, 1) X(2, 2) X(2, 3) X(2, 4) X(2, 5) X(2, 6) X(2, 7) \
   X(3, 0) X(3, 1) X(3, 2) X(3, 3) X(3, 4) X(3, 5) X(3, 6) X(3, 7)
 
-template<int DIM, int G> static int set_smem_attr() {
-  return cudaFuncSetAttribute(end_line_kernel<DIM, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template<int DIM, int G, int MICRO> static int set_smem_attr() {
+  return cudaFuncSetAttribute(end_line_kernel<DIM, G, MICRO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kMaxLineSmem) == cudaSuccess ? 0 : PG_ERR_CUDA;
 }
-template<int DIM, int G> static int set_smem_limit() {
-  return per_device_once((const void*)&set_smem_attr<DIM, G>, set_smem_attr<DIM, G>);
+template<int DIM, int G, int MICRO> static int set_smem_limit() {
+  return per_device_once((const void*)&set_smem_attr<DIM, G, MICRO>, set_smem_attr<DIM, G, MICRO>);
+}
+// A launch of end_line_kernel<DIM, G, MICRO>.
+template<int DIM, int G, int MICRO>
+static int launch_lines(const line_dev_t* lines, int n, size_t smem, cudaStream_t stream, const dev_tables_t& T) {
+  if (int rc = set_smem_limit<DIM, G, MICRO>()) return rc;
+  end_line_kernel<DIM, G, MICRO><<<dim3(512 / MICRO, unsigned(n)), kLineThreads, smem, stream>>>(lines, T);
+  return 0;
 }
 
 // The planned lines of one dimension, sorted by child symmetry: one launch
 // per symmetry, so each kernel holds only its own children's transform.
 static int launch_group(const end_plan& P, int dim, cudaStream_t stream, const dev_tables_t& T) {
   const int n = int(P.host[dim].size());
-  const size_t smem = line_smem_bytes(P.maxpat[dim], P.maxchild[dim]);
+  const int micro = line_micro(P.maxparent[dim], P.maxpat[dim], P.maxchild[dim]);
+  const size_t smem = line_smem_bytes(P.maxpat[dim], P.maxchild[dim], micro);
   for (int a = 0, b = 0; a < n; a = b) {
     const int g = P.host[dim][a].g;
     while (b < n && P.host[dim][b].g == g) b++;
-    const dim3 grid(kUnitGroups, unsigned(b - a));
     const line_dev_t* lines = P.dev[dim] + a;
     int rc = PG_ERR_ARG;
     switch (dim * 8 + g) {
 #define PG_CASE(D, G) case D * 8 + G: \
-      rc = set_smem_limit<D, G>(); \
-      if (!rc) end_line_kernel<D, G><<<grid, kLineThreads, smem, stream>>>(lines, T); \
+      rc = micro == 8 ? launch_lines<D, G, 8>(lines, b - a, smem, stream, T) \
+                      : launch_lines<D, G, 4>(lines, b - a, smem, stream, T); \
       break;
       PG_FOR_DIM_G(PG_CASE)
 #undef PG_CASE
@@ -892,6 +902,7 @@ static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
     const auto off = P.recs.add(lines[i].section, lines[i].dimension);
     P.maxchild[d.dim] = std::max(P.maxchild[d.dim], d.nchild);
     P.maxpat[d.dim] = std::max(P.maxpat[d.dim], d.npat[0] + d.npat[1]);
+    P.maxparent[d.dim] = std::max(P.maxparent[d.dim], d.nparent);
     P.host[d.dim].push_back(d);
     P.rec_off[d.dim].push_back(off);
   }
@@ -906,6 +917,7 @@ static int plan_lines(const pg_line_t* lines, int n, end_plan& P) {
     P.host[dim].swap(h);
     P.rec_off[dim].swap(r);
   }
+  std::stable_sort(P.order, P.order + 4, [&](int a, int b) { return P.maxparent[a] > P.maxparent[b]; });
   return PG_OK;
 }
 
@@ -1048,9 +1060,12 @@ extern "C" int pg_end_plan_run(pg_end_plan_t plan, void* stream_) {
   }
   // One launch per dimension, each on its own stream, so that the tail of
   // one launch's last wave overlaps the next launch instead of idling SMs.
+  // The dimensions with the longest CTAs go first, so that a step ends on
+  // short CTAs.
   PG_CUDA(cudaEventRecord(P.fork, stream));
   int k = -1;
-  for (int dim = 0; dim < 4; dim++) {
+  for (int d = 0; d < 4; d++) {
+    const int dim = P.order[d];
     if (P.host[dim].empty()) continue;
     if (k < 0) {
       if (int rc = launch_group(P, dim, stream, *T)) return rc;
@@ -1256,11 +1271,14 @@ PG_HD void family_offsets(const family_t& F, line_dev_t& L, int start, int step)
   }
 }
 
+// Microlines per sweep CTA (a launch mixes sections of every size).
+constexpr int kSweepMicro = 4;
+
 template<int DIM, int G>
-__global__ void __launch_bounds__(kLineThreads, 3)
+__global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm)
 sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_tables_t T) {
   __shared__ __align__(16) line_dev_t L;
-  __shared__ cta_smem S;
+  __shared__ cta_smem<kSweepMicro> S;
   __shared__ int s_fam, s_nmicro;
   extern __shared__ uint4 dyn_smem[];
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -1277,7 +1295,7 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   }
   __syncthreads();
   // CTAs past a short line's last microline leave before any set-up
-  if (int(blockIdx.y) * kUnits * kMicro >= s_nmicro) return;
+  if (int(blockIdx.y) * kSweepMicro >= s_nmicro) return;
   const family_t& F = fams[s_fam];
   // copy the prototype (as 16-byte words) and fill in this line
   {
@@ -1291,7 +1309,8 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   family_offsets(F, L, tid, nt);
   __syncthreads();
   const int nmicro = L.cross[0] * L.cross[1] * L.cross[2];
-  cta_units<DIM, G>(L, S, dyn_smem, int(blockIdx.y) * kUnits, kUnits, nmicro, tid, nt);
+  const int m0 = int(blockIdx.y) * kSweepMicro;
+  cta_microlines<DIM, G, kSweepMicro>(L, S, dyn_smem, m0, min(kSweepMicro, nmicro - m0), tid, nt);
 }
 
 static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");
@@ -1450,8 +1469,8 @@ extern "C" int pg_slice_layout(const uint64_t* sigs, int n, int64_t* offsets) {
 // at most, by registers): 228 KB per SM, each CTA also holding its static
 // shared memory and 1 KB the hardware reserves.
 static int sweep_ctas_per_sm(size_t dyn) {
-  const size_t per = dyn + sizeof(line_dev_t) + sizeof(cta_smem) + 64 + 1024;
-  return int(std::max<size_t>(1, std::min<size_t>(3, (size_t(228) << 10) / per)));
+  const size_t per = dyn + sizeof(line_dev_t) + sizeof(cta_smem<kSweepMicro>) + 64 + 1024;
+  return int(std::max<size_t>(1, std::min<size_t>(kLineCtasPerSm, (size_t(228) << 10) / per)));
 }
 
 static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_slice, const uint64_t* child_sigs, int nc,
@@ -1497,8 +1516,9 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
     std::vector<int> klass(fams.size());
     for (size_t f = 0; f < fams.size(); f++) {
       order[f] = f;
-      klass[f] = 3 - sweep_ctas_per_sm(line_smem_bytes(fams[f].proto.npat[0] + fams[f].proto.npat[1],
-                                                       fams[f].proto.nchild));
+      klass[f] = kLineCtasPerSm - sweep_ctas_per_sm(
+                                      line_smem_bytes(fams[f].proto.npat[0] + fams[f].proto.npat[1], fams[f].proto.nchild,
+                                                      kSweepMicro));
     }
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
       return klass[a] != klass[b] ? klass[a] < klass[b] : fams[a].proto.g < fams[b].proto.g;
@@ -1521,9 +1541,9 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
     PG_CUDA(X.alloc(&d, sizeof(family_t) * sorted.size()));
     PG_CUDA(cudaMemcpyAsync(d, sorted.data(), sizeof(family_t) * sorted.size(), cudaMemcpyHostToDevice, stream));
     for (const group_t& G : groups) {
-      const size_t smem = line_smem_bytes(G.maxpat, G.maxchild);
+      const size_t smem = line_smem_bytes(G.maxpat, G.maxchild, kSweepMicro);
       for (int line0 = 0; line0 < G.lines; line0 += 1 << 30) {
-        const dim3 grid(unsigned(std::min(G.lines - line0, 1 << 30)), kUnitGroups);
+        const dim3 grid(unsigned(std::min(G.lines - line0, 1 << 30)), 512 / kSweepMicro);
         int rc = PG_ERR_ARG;
         switch (dim * 8 + G.g) {
 #define PG_CASE(D, GG) case D * 8 + GG: \
