@@ -735,7 +735,7 @@ def main():
         torch.cuda.empty_cache()
         from pentago_b200 import learned as learned_mod
         timings = {}
-        learned, sample = learned_mod.run_slice_coding(max_blocks=16384, sample_blocks=64, sweep_timings=timings)
+        learned, sample = learned_mod.run_slice_coding(max_blocks=0, sample_blocks=64, sweep_timings=timings)
         sweep2 = sweep_summary(timings, learned["sweep_s"], measured_hbm_peak()[0])
         if not args.no_cpu_baseline:
             learned["cpu_static_coder"] = cpu_static_coder_rate(*sample, seconds=5.0)

@@ -297,7 +297,7 @@ int pg_store_decode(const uint8_t* in, const int64_t* in_offsets, const int64_t*
  * Learned-model rANS for solved blocks: stream format version 3.  No
  * reference counterpart; it replaces the per-block static table of format 2
  * (arithmetic_encode, pentago/shard/arithmetic.cc:366-401) by a 3-layer MLP
- * (hidden 64, bf16 weights, fp32 arithmetic) that predicts each symbol from
+ * (hidden 64, bf16 weights, fp32 accumulation) that predicts each symbol from
  * the node's board, the rotation and the already coded neighbouring
  * rotations.  Streams are blocks of a section; symbols are pg_node_symbols'
  * (256 per node, nodes in the block's C order).  The encoder keeps whichever
@@ -309,7 +309,12 @@ typedef struct pg_block_ref_t {
   int32_t block[4];   /* block coordinates, 8 positions per block per quadrant */
 } pg_block_ref_t;
 
-/* Bytes of a serialized model: "PGLM", version 1, parameter count, bf16 parameters. */
+/* Bytes of a serialized model: "PGLM", version 2, parameter count, bf16
+ * parameters.  In a version-2 model every column of W1's rotation and
+ * neighbour rows (72..119) and of W2 lies on a grid (integers of magnitude at
+ * most 127 times a power of two), which makes the coder's tensor-core sums
+ * exact; pg_learned_export puts them there, and the coder refuses a model
+ * whose weights are not. */
 int64_t pg_learned_model_bytes(void);
 
 /* Bytes a stream of a block with `nodes` nodes may need (either format). */

@@ -11,11 +11,15 @@
  *     72 + 4 q + i_q         rotation r = i0 + 4 i1 + 16 i2 + 64 i3
  *     88 + 4 n + v           neighbour n = 2 q + e (quadrant q turned +1 for e = 0,
  *                            +3 for e = 1): its symbol if its step is earlier, else v = 3
- *   network: W1 (120 x 64), b1, W2 (64 x 64), b2, W3 (64 x 3), b3 as bf16;
- *     a1 = (node + (RA + RB)) + ((P0 + P1) + (P2 + P3)) with node = b1 + stone rows
- *     ascending, RA = row(72 + i0) + row(76 + i1), RB = row(80 + i2) + row(84 + i3),
- *     Pq = row(88 + 8 q + v_{2q}) + row(92 + 8 q + v_{2q+1}); a2 and z by fma chains
- *     over the input index ascending from the bias; relu(a) = a > 0 ? a : 0
+ *   network: W1 (120 x 64), b1, W2 (64 x 64), b2, W3 (64 x 3), b3 as bf16 (model
+ *     version 2: every column of W1 rows 72..119 and of W2 is integers of magnitude
+ *     at most 127 times 2^-e, e = 7 - x for the column's largest magnitude f 2^x,
+ *     f in [0.5, 1)); a1 = node + S1 with node = b1 + stone rows ascending and S1 the
+ *     exact sum of the rows of the 4 rotation and 8 neighbour features;
+ *     hq = rint(min(max(a1 * 16, 0), 255)); a2 = fma(C, 1/16, b2) with C = the exact
+ *     sum over k of W2[k][j] hq[k]; relu(a) = a > 0 ? a : 0; z = b3 + ((P_0 + P_1) +
+ *     (P_2 + P_3)) where P_t is the fma chain from 0 over the columns j with
+ *     (j >> 1) & 3 = t ascending of W3[j][c] relu(a2[j])
  *   frequencies (15 bits): e_c = 2^((z_c - max) * 1.44269504f) by floor/Taylor
  *     degree 7, f_c = 1 + trunc(e_c / (e0 + e1 + e2) * 32765), remainder to the
  *     first largest
@@ -111,34 +115,78 @@ static int context(const uint8_t* sym, int r, int nb) {
 
 typedef struct { float p[NP]; } model;
 
+/* The grid of a column of n weights w[0], w[stride], ...: each to the nearest
+ * multiple of 2^-e (ties to even), clamped to +-127 2^-e, e = 7 - x for the
+ * largest magnitude f 2^x. */
+static void grid_column(float* w, int n, int stride) {
+  float mx = 0.f;
+  for (int k = 0; k < n; k++) mx = fmaxf(mx, fabsf(w[stride * k]));
+  if (!(mx > 0.f)) {
+    for (int k = 0; k < n; k++) w[stride * k] = 0.f;
+    return;
+  }
+  int x;
+  frexpf(mx, &x);
+  const int e = 7 - x;
+  for (int k = 0; k < n; k++) {
+    float q = nearbyintf(ldexpf(w[stride * k], e));
+    q = q > 127.f ? 127.f : q < -127.f ? -127.f : q;
+    w[stride * k] = ldexpf(q, -e);
+  }
+}
+/* Every grid column: W1 rows 72..119 per hidden unit, W2 per output. */
+static void grid_params(float* p) {
+  for (int k = 0; k < NH; k++) grid_column(p + OFF_W1 + 72 * NH + k, NIN - 72, NH);
+  for (int j = 0; j < NH; j++) grid_column(p + OFF_W2 + j, NH, NH);
+}
+
 static int load_model(const uint8_t* bytes, model* m) {
   uint32_t h[3];
   memcpy(h, bytes, 12);
-  if (h[0] != 0x4d4c4750u || h[1] != 1 || h[2] != NP) return -1;
+  if (h[0] != 0x4d4c4750u || h[1] != 2 || h[2] != NP) return -1;
   for (int i = 0; i < NP; i++) m->p[i] = bf16((uint16_t)(bytes[12 + 2 * i] | bytes[13 + 2 * i] << 8));
-  return 0;
+  float* q = malloc(sizeof(float) * NP);
+  memcpy(q, m->p, sizeof(float) * NP);
+  grid_params(q);
+  const int same = !memcmp(q, m->p, sizeof(float) * NP);
+  free(q);
+  return same ? 0 : -1;
 }
 
 #define W1(f, k) m->p[OFF_W1 + (f) * NH + (k)]
 
+static float act_q(float a) {
+  float v = a * 16.f;
+  v = v > 0.f ? v : 0.f;
+  v = v < 255.f ? v : 255.f;
+  return (v + 8388608.f) - 8388608.f;
+}
+
+/* The 12 rotation and neighbour features of symbol r (rows of W1). */
+static void ctx_features(int r, const uint8_t* sym, int* f) {
+  for (int q = 0; q < 4; q++) f[q] = 72 + 4 * q + ((r >> (2 * q)) & 3);
+  for (int nb = 0; nb < 8; nb++) f[4 + nb] = 88 + 4 * nb + context(sym, r, nb);
+}
+
 static void logits(const model* m, const float* node, int r, const uint8_t* sym, float* z) {
-  float a2[NH];
-  int v[8];
-  for (int nb = 0; nb < 8; nb++) v[nb] = context(sym, r, nb);
-  const int i0 = r & 3, i1 = (r >> 2) & 3, i2 = (r >> 4) & 3, i3 = r >> 6;
-  for (int j = 0; j < NH; j++) a2[j] = m->p[OFF_B2 + j];
+  float hq[NH], part[4][3];
+  int f[12];
+  ctx_features(r, sym, f);
   for (int k = 0; k < NH; k++) {
-    const float ra = W1(72 + i0, k) + W1(76 + i1, k), rb = W1(80 + i2, k) + W1(84 + i3, k);
-    float pq[4];
-    for (int q = 0; q < 4; q++) pq[q] = W1(88 + 8 * q + v[2 * q], k) + W1(92 + 8 * q + v[2 * q + 1], k);
-    const float h = relu((node[k] + (ra + rb)) + ((pq[0] + pq[1]) + (pq[2] + pq[3])));
-    for (int j = 0; j < NH; j++) a2[j] = fmaf(m->p[OFF_W2 + k * NH + j], h, a2[j]);
+    double s1 = 0;   /* exact: at most 12 x 127 units of 2^-e_k */
+    for (int i = 0; i < 12; i++) s1 += W1(f[i], k);
+    hq[k] = act_q(node[k] + (float)s1);
   }
-  for (int c = 0; c < 3; c++) z[c] = m->p[OFF_B3 + c];
+  memset(part, 0, sizeof part);
   for (int j = 0; j < NH; j++) {
-    const float h = relu(a2[j]);
-    for (int c = 0; c < 3; c++) z[c] = fmaf(m->p[OFF_W3 + 3 * j + c], h, z[c]);
+    double c = 0;   /* exact: at most 64 x 127 x 255 units of 2^-e_j */
+    for (int k = 0; k < NH; k++) c += (double)m->p[OFF_W2 + k * NH + j] * hq[k];
+    const float h = relu(fmaf((float)c, 0.0625f, m->p[OFF_B2 + j]));
+    const int t = (j >> 1) & 3;
+    for (int cc = 0; cc < 3; cc++) part[t][cc] = fmaf(m->p[OFF_W3 + 3 * j + cc], h, part[t][cc]);
   }
+  for (int cc = 0; cc < 3; cc++)
+    z[cc] = m->p[OFF_B3 + cc] + ((part[0][cc] + part[1][cc]) + (part[2][cc] + part[3][cc]));
 }
 
 static float exp2_spec(float d) {
@@ -319,6 +367,14 @@ double or_lm_grad(const float* params, uint64_t section, const int* block, const
   if (block_geom(section, block, &g)) return -1;
   model* m = malloc(sizeof(model));
   for (int i = 0; i < NP; i++) m->p[i] = round_bf16(params[i]);
+  {   /* the grid columns from the fp32 parameters */
+    float* q = malloc(sizeof(float) * NP);
+    memcpy(q, params, sizeof(float) * NP);
+    grid_params(q);
+    for (int i = OFF_W1 + 72 * NH; i < OFF_B1; i++) m->p[i] = q[i];
+    for (int i = OFF_W2; i < OFF_B2; i++) m->p[i] = q[i];
+    free(q);
+  }
   memset(grad, 0, sizeof(double) * NP);
   double loss = 0;
   for (int64_t t = 0; t < n; t++) {
@@ -332,14 +388,18 @@ double or_lm_grad(const float* params, uint64_t section, const int* block, const
     for (int q = 0; q < 4; q++) f[nf++] = 72 + 4 * q + ((r >> (2 * q)) & 3);
     for (int nb = 0; nb < 8; nb++) f[nf++] = 88 + 4 * nb + context(sym, r, nb);
     float h1[NH], a2[NH], h2[NH], z[3];
-    for (int k = 0; k < NH; k++) {
+    for (int k = 0; k < NH; k++) {   /* h1 = hq / 16; the last 12 rows summed exactly */
       float a = m->p[OFF_B1 + k];
-      for (int q = 0; q < nf; q++) a = a + W1(f[q], k);
-      h1[k] = relu(a);
+      double s1 = 0;
+      for (int q = 0; q < nf - 12; q++) a = a + W1(f[q], k);
+      for (int q = nf - 12; q < nf; q++) s1 += W1(f[q], k);
+      h1[k] = act_q(a + (float)s1) * 0.0625f;
     }
-    for (int j = 0; j < NH; j++) a2[j] = m->p[OFF_B2 + j];
-    for (int k = 0; k < NH; k++)
-      for (int j = 0; j < NH; j++) a2[j] = fmaf(m->p[OFF_W2 + k * NH + j], h1[k], a2[j]);
+    for (int j = 0; j < NH; j++) {
+      double c = 0;
+      for (int k = 0; k < NH; k++) c += (double)m->p[OFF_W2 + k * NH + j] * h1[k];
+      a2[j] = m->p[OFF_B2 + j] + (float)c;
+    }
     for (int c = 0; c < 3; c++) z[c] = m->p[OFF_B3 + c];
     for (int j = 0; j < NH; j++) {
       h2[j] = relu(a2[j]);
@@ -358,9 +418,9 @@ double or_lm_grad(const float* params, uint64_t section, const int* block, const
       for (int c = 0; c < 3; c++) grad[OFF_W3 + 3 * j + c] += h2[j] * dz[c];
     }
     for (int c = 0; c < 3; c++) grad[OFF_B3 + c] += dz[c];
-    for (int k = 0; k < NH; k++) {
+    for (int k = 0; k < NH; k++) {   /* straight through the quantizer below the clamp */
       d1[k] = 0;
-      if (h1[k] > 0)
+      if (h1[k] > 0 && h1[k] < 255.f * 0.0625f)
         for (int j = 0; j < NH; j++) d1[k] += m->p[OFF_W2 + k * NH + j] * d2[j];
       for (int j = 0; j < NH; j++) grad[OFF_W2 + k * NH + j] += h1[k] * d2[j];
     }

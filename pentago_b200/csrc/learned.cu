@@ -36,31 +36,47 @@ int launch_rans_decode(const uint8_t* in, const int64_t* in_offsets, const int64
 
 constexpr int kLmWarps = 4;
 constexpr int kLmThreads = 32 * kLmWarps;
-constexpr int kW1Pad = 65;  // stone rows padded so lanes reading different rows use different banks
+constexpr int kW1Words = 33;  // a stone row of W1: 64 bf16 as 32 words, padded so lanes reading different rows
+                              // use different banks
+constexpr int kLmCtxRows = kLmIn - kLmRot;   // W1 rows 72..119: the rotation and neighbour features
 
-// Coding tables in shared memory.
+// Coding tables in shared memory.  The tensor cores' B operands are stored
+// transposed, one row of 64 bf16 (8 chunks of 16 bytes) per output unit:
+// w1t row k holds W1[72 + 8 c .. 72 + 8 c + 7][k] in chunk c (c < 6), w2t
+// row j holds W2[8 c .. 8 c + 7][j], chunk c at c ^ (row & 7) so that the
+// eight rows an ldmatrix phase reads fall in different banks.
 struct lm_tables {
-  float w1s[72 * kW1Pad];
-  float ra[kLmHidden][16], rb[kLmHidden][16];  // [k][i0 + 4 i1], [k][i2 + 4 i3]
-  float pt[4][kLmHidden][16];                  // [q][k][va + 4 vb]
-  float w2[kLmHidden][kLmHidden];              // [k][j]
+  uint32_t w1s[72 * kW1Words];   // stone rows of W1, bf16 pairs (k, k + 1)
+  uint4 w1t[kLmHidden][8];
+  uint4 w2t[kLmHidden][8];
   float b1[kLmHidden], b2[kLmHidden];
-  float w3[kLmHidden][4];                      // [j][c]
+  float w3[kLmHidden][4];        // [j][c]
   float b3[4];
 };
 
+__device__ __forceinline__ int swz(int row, int chunk) { return chunk ^ (row & 7); }
+
 __device__ void lm_build_tables(lm_tables& S, const uint16_t* __restrict__ P, int tid, int nt) {
   auto w = [&](int i) { return bf16_value(P[i]); };
-  for (int i = tid; i < 72 * kLmHidden; i += nt) S.w1s[(i / kLmHidden) * kW1Pad + i % kLmHidden] = w(kLmW1 + i);
-  for (int i = tid; i < kLmHidden * 16; i += nt) {
-    const int k = i / 16, u = i % 16, a = u & 3, b = u >> 2;
-    S.ra[k][u] = f_add(w(kLmW1 + (kLmRot + a) * kLmHidden + k), w(kLmW1 + (kLmRot + 4 + b) * kLmHidden + k));
-    S.rb[k][u] = f_add(w(kLmW1 + (kLmRot + 8 + a) * kLmHidden + k), w(kLmW1 + (kLmRot + 12 + b) * kLmHidden + k));
-    for (int q = 0; q < 4; q++)
-      S.pt[q][k][u] = f_add(w(kLmW1 + (kLmCtx + 8 * q + a) * kLmHidden + k),
-                            w(kLmW1 + (kLmCtx + 8 * q + 4 + b) * kLmHidden + k));
+  for (int i = tid; i < 72 * 32; i += nt) {
+    const int f = i >> 5, k2 = i & 31;
+    S.w1s[f * kW1Words + k2] = uint32_t(P[kLmW1 + f * kLmHidden + 2 * k2]) |
+                               uint32_t(P[kLmW1 + f * kLmHidden + 2 * k2 + 1]) << 16;
   }
-  for (int i = tid; i < kLmHidden * kLmHidden; i += nt) S.w2[i / kLmHidden][i % kLmHidden] = w(kLmW2 + i);
+  for (int i = tid; i < kLmHidden * 8; i += nt) {
+    const int j = i >> 3, c = i & 7;
+    uint32_t v[4], u[4];
+    for (int e = 0; e < 4; e++) {
+      const int f = 8 * c + 2 * e;   // feature rows 72 + f, 72 + f + 1 (zero past the 48)
+      u[e] = f < kLmCtxRows ? uint32_t(P[kLmW1 + (kLmRot + f) * kLmHidden + j]) |
+                                  uint32_t(P[kLmW1 + (kLmRot + f + 1) * kLmHidden + j]) << 16
+                            : 0u;
+      v[e] = uint32_t(P[kLmW2 + (8 * c + 2 * e) * kLmHidden + j]) |
+             uint32_t(P[kLmW2 + (8 * c + 2 * e + 1) * kLmHidden + j]) << 16;
+    }
+    S.w1t[j][swz(j, c)] = make_uint4(u[0], u[1], u[2], u[3]);
+    S.w2t[j][swz(j, c)] = make_uint4(v[0], v[1], v[2], v[3]);
+  }
   for (int i = tid; i < kLmHidden; i += nt) {
     S.b1[i] = w(kLmB1 + i);
     S.b2[i] = w(kLmB2 + i);
@@ -71,128 +87,265 @@ __device__ void lm_build_tables(lm_tables& S, const uint16_t* __restrict__ P, in
   if (tid == 3) S.b3[3] = 0.f;
 }
 
-// node[k] = b1[k] + stone rows, ascending.
+// Element k of row t of a transposed table (bf16 -> float).
+__device__ __forceinline__ float lm_tab(const uint4 (*tab)[8], int row, int k) {
+  const uint4 ch = tab[row][swz(row, k >> 3)];
+  const uint32_t pr = (k & 7) < 2 ? ch.x : (k & 7) < 4 ? ch.y : (k & 7) < 6 ? ch.z : ch.w;
+  return f_bits(k & 1 ? pr & 0xffff0000u : pr << 16);
+}
+
+// node[k] = b1[k] + stone rows, ascending (registers of one thread).
 __device__ __forceinline__ void lm_node_sum(const lm_tables& S, const uint8_t* feats, int nf, float* node) {
 #pragma unroll
   for (int k = 0; k < kLmHidden; k++) node[k] = S.b1[k];
   for (int i = 0; i < nf; i++) {
-    const float* row = S.w1s + feats[i] * kW1Pad;
+    const uint32_t* row = S.w1s + feats[i] * kW1Words;
 #pragma unroll
-    for (int k = 0; k < kLmHidden; k++) node[k] = f_add(node[k], row[k]);
+    for (int k2 = 0; k2 < 32; k2++) {
+      const uint32_t v = row[k2];
+      node[2 * k2] = f_add(node[2 * k2], f_bits(v << 16));
+      node[2 * k2 + 1] = f_add(node[2 * k2 + 1], f_bits(v & 0xffff0000u));
+    }
   }
 }
 
-// Logits of one symbol (the order of learned.cuh).
+// The 4 rotation and 8 neighbour features of symbol r (indices into W1 rows
+// 72..119): 4 q + i_q, then 16 + 4 n + v_n with u[q] = v_2q + 4 v_2q+1.
+__device__ __forceinline__ void lm_ctx_features(int r, const int* u, int* f) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    f[q] = 4 * q + ((r >> (2 * q)) & 3);
+    f[4 + 2 * q] = 16 + 8 * q + (u[q] & 3);
+    f[5 + 2 * q] = 20 + 8 * q + (u[q] >> 2);
+  }
+}
+
+// Logits of one symbol, one thread (the frequency check kernel): S1 and C by
+// fp32 chains, exact on a version-2 model, and layer 3 in the order of
+// learned.cuh.
 __device__ __forceinline__ void lm_logits(const lm_tables& S, const float* node, int r, const int* u, float* z) {
-  const int ua = r & 15, ub = r >> 4;
-  float a2[kLmHidden];
-#pragma unroll
-  for (int j = 0; j < kLmHidden; j++) a2[j] = S.b2[j];
-#pragma unroll
+  int f[12];
+  lm_ctx_features(r, u, f);
+  float hq[kLmHidden];
   for (int k = 0; k < kLmHidden; k++) {
-    const float rot = f_add(S.ra[k][ua], S.rb[k][ub]);
-    const float ctx = f_add(f_add(S.pt[0][k][u[0]], S.pt[1][k][u[1]]), f_add(S.pt[2][k][u[2]], S.pt[3][k][u[3]]));
-    const float h = relu(f_add(f_add(node[k], rot), ctx));
-    const float4* w = reinterpret_cast<const float4*>(S.w2[k]);
-#pragma unroll
-    for (int j4 = 0; j4 < kLmHidden / 4; j4++) {
-      const float4 v = w[j4];
-      a2[4 * j4 + 0] = f_fma(v.x, h, a2[4 * j4 + 0]);
-      a2[4 * j4 + 1] = f_fma(v.y, h, a2[4 * j4 + 1]);
-      a2[4 * j4 + 2] = f_fma(v.z, h, a2[4 * j4 + 2]);
-      a2[4 * j4 + 3] = f_fma(v.w, h, a2[4 * j4 + 3]);
-    }
+    float s1 = 0.f;
+    for (int i = 0; i < 12; i++) s1 = f_add(s1, lm_tab(S.w1t, k, f[i]));
+    hq[k] = lm_act_q(f_add(node[k], s1));
   }
-  z[0] = S.b3[0];
-  z[1] = S.b3[1];
-  z[2] = S.b3[2];
+  float part[4][3];
 #pragma unroll
+  for (int t = 0; t < 4; t++) part[t][0] = part[t][1] = part[t][2] = 0.f;
   for (int j = 0; j < kLmHidden; j++) {
-    const float h = relu(a2[j]);
-    const float4 v = *reinterpret_cast<const float4*>(S.w3[j]);
-    z[0] = f_fma(v.x, h, z[0]);
-    z[1] = f_fma(v.y, h, z[1]);
-    z[2] = f_fma(v.z, h, z[2]);
+    float c = 0.f;
+    for (int k = 0; k < kLmHidden; k++) c = f_fma(lm_tab(S.w2t, j, k), hq[k], c);
+    const float h = relu(f_fma(c, kLmActInv, S.b2[j]));
+    const int t = (j >> 1) & 3;
+    for (int cc = 0; cc < 3; cc++) part[t][cc] = f_fma(S.w3[j][cc], h, part[t][cc]);
+  }
+  for (int cc = 0; cc < 3; cc++)
+    z[cc] = f_add(S.b3[cc], f_add(f_add(part[0][cc], part[1][cc]), f_add(part[2][cc], part[3][cc])));
+}
+
+// Tensor-core pieces (mma.sync m16n8k16, bf16 inputs, fp32 accumulation).
+__device__ __forceinline__ void ldsm_x4(uint32_t* r, const void* p) {
+  const unsigned a = unsigned(__cvta_generic_to_shared(p));
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(a));
+}
+__device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
+  asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+               "{%8, %9}, {%0, %1, %2, %3};\n"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// out[n] += A x B for the eight n-tiles of a transposed table, k-tile kt.
+__device__ __forceinline__ void mma_row(float (*acc)[4], const uint32_t* a, const uint4 (*tab)[8], int kt, int lane) {
+#pragma unroll
+  for (int np = 0; np < 4; np++) {
+    const int row = 16 * np + 8 * (lane >> 4) + (lane & 7), chunk = 2 * kt + ((lane >> 3) & 1);
+    uint32_t b[4];
+    ldsm_x4(b, &tab[row][swz(row, chunk)]);
+    mma_bf16(acc[2 * np], a, b[0], b[1]);
+    mma_bf16(acc[2 * np + 1], a, b[2], b[3]);
   }
 }
 
-// Logits of the two symbols of step s (rotations s and s + 128) of one node,
-// whose node sums are node[k * 32] (the lane's column of its warp's block).
-// Each logit follows the order of learned.cuh exactly; the pair shares the
-// node sums, the RA lookup and the W2 rows.
-__device__ __forceinline__ void lm_logits2(const lm_tables& S, const float* node, int s, const int* uA,
-                                           const int* uB, float* zA, float* zB) {
-  const int ua = s & 15, ubA = s >> 4, ubB = ubA + 8;
-  float a2A[kLmHidden], a2B[kLmHidden];
+// bf16 1.0 at the element of value v among the pair (base, base + 1).
+__device__ __forceinline__ uint32_t onehot2(int v, int base) {
+  return v == base ? 0x00003f80u : v == base + 1 ? 0x3f800000u : 0u;
+}
+
+// The warp's 64 rows per step: row lane is symbol s of the lane's node, row
+// 32 + lane symbol s + 128; tile m holds rows 16 m .. 16 m + 15, and lane
+// (g, t) = (lane / 4, lane % 4) holds rows 16 m + g and 16 m + g + 8 of each
+// tile, that is the nodes of lanes 16 (m & 1) + 8 h + g (h = 0, 1), and
+// columns 8 n + 2 t + e (e = 0, 1) of each n-tile.  lm_nodefrag is the node
+// sums at those places (constant over a node's 128 steps).
+struct lm_nodefrag {
+  float v[2][2][8][2];   // [m & 1][h][n][e]
+};
+
+// Chunk kc (hidden units 16 kc .. 16 kc + 15) of the lane's own node sums,
+// own[i] for unit 16 kc + i, spread to the warp's fragment places.
+__device__ __forceinline__ void lm_node_frag(const float* own, int kc, int lane, lm_nodefrag& F) {
+  const int g = lane >> 2, t = lane & 3;
 #pragma unroll
-  for (int j = 0; j < kLmHidden; j++) { a2A[j] = S.b2[j]; a2B[j] = S.b2[j]; }
-#pragma unroll 4
-  for (int k = 0; k < kLmHidden; k++) {
-    const float nk = node[32 * k], ra = S.ra[k][ua];
-    const float ctxA = f_add(f_add(S.pt[0][k][uA[0]], S.pt[1][k][uA[1]]), f_add(S.pt[2][k][uA[2]], S.pt[3][k][uA[3]]));
-    const float ctxB = f_add(f_add(S.pt[0][k][uB[0]], S.pt[1][k][uB[1]]), f_add(S.pt[2][k][uB[2]], S.pt[3][k][uB[3]]));
-    const float hA = relu(f_add(f_add(nk, f_add(ra, S.rb[k][ubA])), ctxA));
-    const float hB = relu(f_add(f_add(nk, f_add(ra, S.rb[k][ubB])), ctxB));
-    const float4* w = reinterpret_cast<const float4*>(S.w2[k]);
+  for (int i = 0; i < 16; i++) {
+    const int k = 16 * kc + i;
 #pragma unroll
-    for (int j4 = 0; j4 < kLmHidden / 4; j4++) {
-      const float4 v = w[j4];
-      a2A[4 * j4 + 0] = f_fma(v.x, hA, a2A[4 * j4 + 0]);
-      a2A[4 * j4 + 1] = f_fma(v.y, hA, a2A[4 * j4 + 1]);
-      a2A[4 * j4 + 2] = f_fma(v.z, hA, a2A[4 * j4 + 2]);
-      a2A[4 * j4 + 3] = f_fma(v.w, hA, a2A[4 * j4 + 3]);
-      a2B[4 * j4 + 0] = f_fma(v.x, hB, a2B[4 * j4 + 0]);
-      a2B[4 * j4 + 1] = f_fma(v.y, hB, a2B[4 * j4 + 1]);
-      a2B[4 * j4 + 2] = f_fma(v.z, hB, a2B[4 * j4 + 2]);
-      a2B[4 * j4 + 3] = f_fma(v.w, hB, a2B[4 * j4 + 3]);
+    for (int mm = 0; mm < 2; mm++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const float x = __shfl_sync(0xffffffffu, own[i], 16 * mm + 8 * h + g);
+        if (((k >> 1) & 3) == t) F.v[mm][h][k >> 3][k & 1] = x;
+      }
+  }
+}
+
+// Logits of the two symbols of step s (rotations s and s + 128) of every
+// lane's node.  ctx is the lane's neighbour context (symbol s in bits 0-15,
+// s + 128 in bits 16-31; 4 bits u_q = v_2q + 4 v_2q+1 per quadrant q).
+// Layer 1's rotation and neighbour rows and layer 2 run on the tensor cores;
+// layer 1's results stay in registers as layer 2's A operand.
+__device__ __forceinline__ void lm_step_logits(const lm_tables& S, const lm_nodefrag& N, int lane, int s, uint32_t ctx,
+                                               float* zA, float* zB) {
+  const int g = lane >> 2, t = lane & 3;
+  uint32_t cx[2][2];
+#pragma unroll
+  for (int mm = 0; mm < 2; mm++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) cx[mm][h] = __shfl_sync(0xffffffffu, ctx, 16 * mm + 8 * h + g);
+  // Row lane is in tile lane / 16 (symbol s) and tile 2 + lane / 16 (s + 128),
+  // half (lane / 8) & 1 of quad lane & 7.
+  const int src = 4 * (lane & 7), mine = lane >> 4, half = (lane >> 3) & 1;
+  // Tile m = 2 sb + mm: one tile at a time (the loop over sb is not unrolled,
+  // so the tiles' registers are not live together)
+#pragma unroll
+  for (int mm = 0; mm < 2; mm++) {
+#pragma unroll 1
+    for (int sb = 0; sb < 2; sb++) {
+      const int r = s + 128 * sb;
+      // Layer 1 A operand: one-hot features.  k-tile 0 is the rotation
+      // (feature 4 q + i_q; the lane's columns 2 t, 2 t + 1 and 8 + 2 t,
+      // 9 + 2 t are quadrants t / 2 and 2 + t / 2), the same for every node;
+      // k-tiles 1 and 2 are neighbours n = 4 (kt - 1) + t / 2 and n + 2.
+      const int base = 2 * (t & 1);
+      uint32_t a1[3][4];
+      a1[0][0] = a1[0][1] = onehot2((r >> (2 * (t >> 1))) & 3, base);
+      a1[0][2] = a1[0][3] = onehot2((r >> (2 * (2 + (t >> 1)))) & 3, base);
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const uint32_t u = cx[mm][h] >> (16 * sb);
+#pragma unroll
+        for (int kt = 1; kt < 3; kt++) {
+          const int n0 = 4 * (kt - 1) + (t >> 1);
+          a1[kt][h] = onehot2(int(u >> (2 * n0)) & 3, base);
+          a1[kt][2 + h] = onehot2(int(u >> (2 * (n0 + 2))) & 3, base);
+        }
+      }
+      float acc[8][4];
+#pragma unroll
+      for (int n = 0; n < 8; n++) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+#pragma unroll
+      for (int kt = 0; kt < 3; kt++) mma_row(acc, a1[kt], S.w1t, kt, lane);
+      // a1 = node + S1, quantized: n-tiles 2 k and 2 k + 1 of layer 1 are the
+      // k-tile k of layer 2's A operand
+      uint32_t a2[4][4];
+#pragma unroll
+      for (int n = 0; n < 8; n++) {
+        const float q00 = lm_act_q(f_add(N.v[mm][0][n][0], acc[n][0]));
+        const float q01 = lm_act_q(f_add(N.v[mm][0][n][1], acc[n][1]));
+        const float q10 = lm_act_q(f_add(N.v[mm][1][n][0], acc[n][2]));
+        const float q11 = lm_act_q(f_add(N.v[mm][1][n][1], acc[n][3]));
+        a2[n >> 1][2 * (n & 1)] = __byte_perm(f_raw(q00), f_raw(q01), 0x7632);
+        a2[n >> 1][2 * (n & 1) + 1] = __byte_perm(f_raw(q10), f_raw(q11), 0x7632);
+      }
+#pragma unroll
+      for (int n = 0; n < 8; n++) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) mma_row(acc, a2[kt], S.w2t, kt, lane);
+      // Layer 3 on the accumulators: the lane's columns make its P_t
+      float p0[3] = {0.f, 0.f, 0.f}, p1[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+      for (int n = 0; n < 8; n++)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+          const int j = 8 * n + 2 * t + e;
+          const float4 w3 = *reinterpret_cast<const float4*>(S.w3[j]);
+          const float b2 = S.b2[j];
+          const float h0 = relu(f_fma(acc[n][e], kLmActInv, b2)), h1 = relu(f_fma(acc[n][2 + e], kLmActInv, b2));
+          p0[0] = f_fma(w3.x, h0, p0[0]);
+          p0[1] = f_fma(w3.y, h0, p0[1]);
+          p0[2] = f_fma(w3.z, h0, p0[2]);
+          p1[0] = f_fma(w3.x, h1, p1[0]);
+          p1[1] = f_fma(w3.y, h1, p1[1]);
+          p1[2] = f_fma(w3.z, h1, p1[2]);
+        }
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        // (P0 + P1) + (P2 + P3); addition commutes, so every lane of the
+        // quad ends with the same bits; then to the row's own lane
+        float q0 = f_add(p0[c], __shfl_xor_sync(0xffffffffu, p0[c], 1));
+        float q1 = f_add(p1[c], __shfl_xor_sync(0xffffffffu, p1[c], 1));
+        q0 = f_add(S.b3[c], f_add(q0, __shfl_xor_sync(0xffffffffu, q0, 2)));
+        q1 = f_add(S.b3[c], f_add(q1, __shfl_xor_sync(0xffffffffu, q1, 2)));
+        const float v0 = __shfl_sync(0xffffffffu, q0, src), v1 = __shfl_sync(0xffffffffu, q1, src);
+        if (mm == mine) {
+          const float v = half ? v1 : v0;
+          if (sb) zB[c] = v;
+          else zA[c] = v;
+        }
+      }
     }
   }
-  zA[0] = zB[0] = S.b3[0];
-  zA[1] = zB[1] = S.b3[1];
-  zA[2] = zB[2] = S.b3[2];
-#pragma unroll
-  for (int j = 0; j < kLmHidden; j++) {
-    const float4 v = *reinterpret_cast<const float4*>(S.w3[j]);
-    const float hA = relu(a2A[j]), hB = relu(a2B[j]);
-    zA[0] = f_fma(v.x, hA, zA[0]);
-    zA[1] = f_fma(v.y, hA, zA[1]);
-    zA[2] = f_fma(v.z, hA, zA[2]);
-    zB[0] = f_fma(v.x, hB, zB[0]);
-    zB[1] = f_fma(v.y, hB, zB[1]);
-    zB[2] = f_fma(v.z, hB, zB[2]);
-  }
 }
 
-// node[k * 32] = b1[k] + stone rows ascending, for this lane's node.
-__device__ __forceinline__ void lm_node_store(const lm_tables& S, const uint8_t* feats, int nf, float* node) {
-#pragma unroll
-  for (int kc = 0; kc < kLmHidden; kc += 16) {
-    float acc[16];
-#pragma unroll
-    for (int i = 0; i < 16; i++) acc[i] = S.b1[kc + i];
-    for (int f = 0; f < nf; f++) {
-      const float* row = S.w1s + feats[f] * kW1Pad + kc;
-#pragma unroll
-      for (int i = 0; i < 16; i++) acc[i] = f_add(acc[i], row[i]);
-    }
-#pragma unroll
-    for (int i = 0; i < 16; i++) node[32 * (kc + i)] = acc[i];
-  }
-}
-
-__device__ __forceinline__ void lm_context_clamped(const uint8_t* sym, int r, int* u) {
+// Neighbour context of symbol r from the node's symbols (those of earlier
+// steps; later ones read as 3), packed as 4 bits per quadrant.
+__device__ __forceinline__ uint32_t lm_context_packed(const uint8_t* sym, int r) {
+  uint32_t p = 0;
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int a = lm_neighbour(r, 2 * q), b = lm_neighbour(r, 2 * q + 1);
     const int va = lm_before(a, r) ? (sym[a] & 3) : 3, vb = lm_before(b, r) ? (sym[b] & 3) : 3;
-    u[q] = va + 4 * vb;
+    p |= uint32_t(va + 4 * vb) << (4 * q);
   }
+  return p;
+}
+__device__ __forceinline__ void lm_context_clamped(const uint8_t* sym, int r, int* u) {
+  const uint32_t p = lm_context_packed(sym, r);
+#pragma unroll
+  for (int q = 0; q < 4; q++) u[q] = int(p >> (4 * q)) & 15;
 }
 
 __device__ __forceinline__ int lm_load_node(const lm_block_t& B, int64_t i, const dev_tables_t& T, uint8_t* feats) {
   uint16_t qid[4];
   lm_node_quadrants(B, i, T.rmin_flat, qid);
   return lm_node_features(qid, T.unpack, feats);
+}
+
+// The lane's node: its node sums (b1 + stone rows ascending), 16 units at a
+// time, spread to the warp's fragment places.
+__device__ __forceinline__ void lm_round_nodes(const lm_tables& S, const lm_block_t& B, int64_t i, bool active,
+                                               const dev_tables_t& T, int lane, lm_nodefrag& N) {
+  uint8_t feats[36];
+  const int nf = active ? lm_load_node(B, i, T, feats) : 0;
+#pragma unroll
+  for (int kc = 0; kc < 4; kc++) {
+    float own[16];
+#pragma unroll
+    for (int u = 0; u < 16; u++) own[u] = S.b1[16 * kc + u];
+    for (int f = 0; f < nf; f++) {
+      const uint32_t* row = S.w1s + feats[f] * kW1Words + 8 * kc;
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        const uint32_t v = row[u];
+        own[2 * u] = f_add(own[2 * u], f_bits(v << 16));
+        own[2 * u + 1] = f_add(own[2 * u + 1], f_bits(v & 0xffff0000u));
+      }
+    }
+    lm_node_frag(own, kc, lane, N);
+  }
 }
 
 __device__ __forceinline__ void put16(uint8_t* p, uint16_t v) { p[0] = uint8_t(v); p[1] = uint8_t(v >> 8); }
@@ -202,10 +355,41 @@ __device__ __forceinline__ uint32_t get32(const uint8_t* p) {
   return uint32_t(p[0]) | uint32_t(p[1]) << 8 | uint32_t(p[2]) << 16 | uint32_t(p[3]) << 24;
 }
 
-// Dynamic shared memory of the coding kernels: the tables, then each warp's
-// node sums (64 x 32 floats, one column per lane).
-constexpr size_t kLmNodeFloats = kLmHidden * 32;
-constexpr size_t kLmCodeSmem = sizeof(lm_tables) + sizeof(float) * kLmNodeFloats * kLmWarps;
+// Dynamic shared memory of the coding kernels: the tables, then per warp its
+// lanes' nodes' symbols (one row of 256 bytes a lane, rows 260 bytes apart
+// so that lanes reading the same rotation use different banks) and, for the
+// decoder, a window of the stream's next words.
+constexpr int kLmSymRow = 260;
+constexpr int kLmWordWin = 1024;   // the decoder's window of upcoming stream words, per warp
+constexpr size_t kLmWarpSmem = size_t(32) * kLmSymRow + 2 * kLmWordWin;
+constexpr size_t kLmCodeSmem = sizeof(lm_tables) + kLmWarpSmem * kLmWarps;
+static_assert(sizeof(lm_tables) % 16 == 0 && kLmWarpSmem % 16 == 0, "coding rows stay 16-byte aligned");
+
+// A node's 256 symbols between global memory and its shared-memory row.
+__device__ __forceinline__ int lm_row_in(uint8_t* row, const uint8_t* g) {
+  int bad = 0;
+  if ((reinterpret_cast<uintptr_t>(g) & 3) == 0) {
+    for (int w = 0; w < 64; w++) {
+      const uint32_t v = reinterpret_cast<const uint32_t*>(g)[w];
+      bad |= (v & 0xfcfcfcfcu) != 0 || (v & v >> 1 & 0x01010101u) != 0;   // a byte above 2
+      reinterpret_cast<uint32_t*>(row)[w] = v;
+    }
+  } else {
+    for (int k = 0; k < 256; k++) {
+      const uint8_t v = g[k];
+      bad |= v > 2;
+      row[k] = v;
+    }
+  }
+  return bad;
+}
+__device__ __forceinline__ void lm_row_out(const uint8_t* row, uint8_t* g) {
+  if ((reinterpret_cast<uintptr_t>(g) & 3) == 0) {
+    for (int w = 0; w < 64; w++) reinterpret_cast<uint32_t*>(g)[w] = reinterpret_cast<const uint32_t*>(row)[w];
+  } else {
+    for (int k = 0; k < 256; k++) g[k] = row[k];
+  }
+}
 
 // Append one 16-bit word per renormalizing lane, in lane order (encoder).
 __device__ __forceinline__ void lm_put_state(uint32_t& x, const lm_freq_t& F, int v, bool active, uint8_t* words,
@@ -221,8 +405,10 @@ __device__ __forceinline__ void lm_put_state(uint32_t& x, const lm_freq_t& F, in
 }
 
 // Decode one symbol per active lane and take this step's words (decoder).
+// Words [wlo, wlo + kLmWordWin) are also in win.
 __device__ __forceinline__ int lm_get_symbol(uint32_t& x, const lm_freq_t& F, bool active, const uint8_t* words,
-                                             int64_t& ptr, unsigned above, int& bad) {
+                                             const uint16_t* win, int64_t wlo, int64_t& ptr, unsigned above,
+                                             int& bad) {
   int v = 0;
   if (active) {
     const uint32_t slot = x & (kLmProbTotal - 1);
@@ -233,27 +419,41 @@ __device__ __forceinline__ int lm_get_symbol(uint32_t& x, const lm_freq_t& F, bo
   const unsigned mask = __ballot_sync(0xffffffffu, need);
   const int64_t at = ptr - 1 - __popc(mask & above);
   if (need) {
-    if (at >= 0) x = (x << 16) | get16(words + 2 * at);
+    if (at >= wlo) x = (x << 16) | win[at - wlo];
+    else if (at >= 0) x = (x << 16) | get16(words + 2 * at);
     else bad = 1;
   }
   ptr -= __popc(mask);
   return v;
 }
 
+// The next stream of a launch, largest first: streams are handed to warps
+// one at a time through a counter, in the order the host sorted them.
+__device__ __forceinline__ int lm_next_stream(int* next, const int32_t* order, int nstreams, int lane) {
+  int k = 0;
+  if (lane == 0) k = atomicAdd(next, 1);
+  k = __shfl_sync(0xffffffffu, k, 0);
+  return k < nstreams ? order[k] : -1;
+}
+
 // One warp per stream (grid-stride over streams).  sizes[s] = stream bytes, or
 // PG_ERR_ARG for a symbol above 2 or a symbol count that does not match.
-__global__ void __launch_bounds__(kLmThreads)
+// Coding kernels are compiled for three CTAs (12 warps) per SM.
+constexpr int kLmCodeCtas = 3;
+
+__global__ void __launch_bounds__(kLmThreads, kLmCodeCtas)
 lm_encode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t* __restrict__ blocks, int nstreams,
-                 const uint8_t* __restrict__ symbols, const int64_t* __restrict__ offsets, uint8_t* __restrict__ out,
+                 const int32_t* __restrict__ order, int* __restrict__ next, const uint8_t* __restrict__ symbols,
+                 const int64_t* __restrict__ offsets, uint8_t* __restrict__ out,
                  const int64_t* __restrict__ out_offsets, int64_t* __restrict__ sizes, const dev_tables_t T) {
   extern __shared__ __align__(16) unsigned char lm_smem_raw[];
   lm_tables& S = *reinterpret_cast<lm_tables*>(lm_smem_raw);
   lm_build_tables(S, P, threadIdx.x, blockDim.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* node = reinterpret_cast<float*>(lm_smem_raw + sizeof(lm_tables)) + kLmNodeFloats * warp + lane;
+  uint8_t* row = lm_smem_raw + sizeof(lm_tables) + kLmWarpSmem * warp + kLmSymRow * lane;
   const unsigned below = (1u << lane) - 1;
-  for (int s = blockIdx.x * kLmWarps + warp; s < nstreams; s += gridDim.x * kLmWarps) {
+  for (int s; (s = lm_next_stream(next, order, nstreams, lane)) >= 0;) {
     const lm_block_t B = blocks[s];
     const int64_t n = B.nodes;
     uint8_t* base = out + out_offsets[s];
@@ -270,25 +470,22 @@ lm_encode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
     for (int64_t round = rounds - 1; round >= 0; round--) {
       const int64_t i = 32 * round + lane;
       const bool active = i < n;
-      uint8_t feats[36];
-      const int nf = active ? lm_load_node(B, i, T, feats) : 0;
-      lm_node_store(S, feats, nf, node);
-      const uint8_t* sym = sym0 + 256 * (active ? i : 0);
+      lm_nodefrag N;
+      lm_round_nodes(S, B, i, active, T, lane, N);
+      if (active) bad |= lm_row_in(row, sym0 + 256 * i);
       for (int st = 127; st >= 0; st--) {
+        const uint32_t ctx = active ? lm_context_packed(row, st) | lm_context_packed(row, st + 128) << 16 : 0u;
+        float zA[3], zB[3];
+        lm_step_logits(S, N, lane, st, ctx, zA, zB);
         lm_freq_t FA = {}, FB = {};
         int vA = 0, vB = 0;
         if (active) {
-          int uA[4], uB[4];
-          lm_context_clamped(sym, st, uA);
-          lm_context_clamped(sym, st + 128, uB);
-          float zA[3], zB[3];
-          lm_logits2(S, node, st, uA, uB, zA, zB);
           FA = lm_freqs(zA);
           FB = lm_freqs(zB);
-          vA = sym[st];
-          vB = sym[st + 128];
-          if (vA > 2) { bad = 1; vA = 0; }
-          if (vB > 2) { bad = 1; vB = 0; }
+          vA = row[st] & 3;
+          vB = row[st + 128] & 3;
+          if (vA > 2) vA = 0;   // (flagged when the row was read)
+          if (vB > 2) vB = 0;
         }
         // the decoder takes s then s + 128, so the encoder puts s + 128 first
         lm_put_state(x, FB, vB, active, words, len, below);
@@ -311,9 +508,10 @@ lm_encode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
 // status[s] = symbols decoded, or PG_ERR_FORMAT / PG_ERR_CAPACITY.  Version-2
 // streams are left to the format-2 decoder (and streams too short to carry a
 // version, which it rejects).
-__global__ void __launch_bounds__(kLmThreads)
+__global__ void __launch_bounds__(kLmThreads, kLmCodeCtas)
 lm_decode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t* __restrict__ blocks, int nstreams,
-                 const uint8_t* __restrict__ in, const int64_t* __restrict__ in_offsets,
+                 const int32_t* __restrict__ order, int* __restrict__ next, const uint8_t* __restrict__ in,
+                 const int64_t* __restrict__ in_offsets,
                  const int64_t* __restrict__ in_sizes, uint8_t* __restrict__ symbols,
                  const int64_t* __restrict__ sym_offsets, const int64_t* __restrict__ sym_caps,
                  int64_t* __restrict__ status, const dev_tables_t T) {
@@ -322,9 +520,11 @@ lm_decode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
   lm_build_tables(S, P, threadIdx.x, blockDim.x);
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* node = reinterpret_cast<float*>(lm_smem_raw + sizeof(lm_tables)) + kLmNodeFloats * warp + lane;
+  uint8_t* row = lm_smem_raw + sizeof(lm_tables) + kLmWarpSmem * warp + kLmSymRow * lane;
+  uint16_t* win = reinterpret_cast<uint16_t*>(lm_smem_raw + sizeof(lm_tables) + kLmWarpSmem * warp +
+                                              32 * kLmSymRow);
   const unsigned above = lane == 31 ? 0u : ~0u << (lane + 1);
-  for (int s = blockIdx.x * kLmWarps + warp; s < nstreams; s += gridDim.x * kLmWarps) {
+  for (int s; (s = lm_next_stream(next, order, nstreams, lane)) >= 0;) {
     const lm_block_t B = blocks[s];
     const int64_t n = B.nodes;
     const uint8_t* base = in + in_offsets[s];
@@ -352,28 +552,29 @@ lm_decode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
     for (int64_t round = 0; round < rounds; round++) {
       const int64_t i = 32 * round + lane;
       const bool active = i < n;
-      uint8_t feats[36];
-      const int nf = active ? lm_load_node(B, i, T, feats) : 0;
-      lm_node_store(S, feats, nf, node);
-      uint8_t* sym = out0 + 256 * (active ? i : 0);
+      lm_nodefrag N;
+      lm_round_nodes(S, B, i, active, T, lane, N);
+      for (int w = 0; w < 64; w++) reinterpret_cast<uint32_t*>(row)[w] = 0u;
+      // the round's words are the last unread ones: stage up to kLmWordWin of them
+      const int64_t wlo = ptr > kLmWordWin ? ptr - kLmWordWin : 0;
+      __syncwarp();
+      for (int64_t w = wlo + lane; w < ptr; w += 32) win[w - wlo] = get16(words + 2 * w);
+      __syncwarp();
       for (int st = 0; st < 128; st++) {
+        const uint32_t ctx = active ? lm_context_packed(row, st) | lm_context_packed(row, st + 128) << 16 : 0u;
+        float zA[3], zB[3];
+        lm_step_logits(S, N, lane, st, ctx, zA, zB);
         lm_freq_t FA = {}, FB = {};
         if (active) {
-          int uA[4], uB[4];
-          lm_context_clamped(sym, st, uA);
-          lm_context_clamped(sym, st + 128, uB);
-          float zA[3], zB[3];
-          lm_logits2(S, node, st, uA, uB, zA, zB);
           FA = lm_freqs(zA);
           FB = lm_freqs(zB);
         }
-        const int vA = lm_get_symbol(x, FA, active, words, ptr, above, bad);
-        const int vB = lm_get_symbol(x, FB, active, words, ptr, above, bad);
-        if (active) {
-          sym[st] = uint8_t(vA);
-          sym[st + 128] = uint8_t(vB);
-        }
+        const int vA = lm_get_symbol(x, FA, active, words, win, wlo, ptr, above, bad);
+        const int vB = lm_get_symbol(x, FB, active, words, win, wlo, ptr, above, bad);
+        row[st] = uint8_t(vA);
+        row[st + 128] = uint8_t(vB);
       }
+      if (active) lm_row_out(row, out0 + 256 * i);
     }
     // A well-formed stream ends with every word read and every lane back at
     // the encoder's initial state.
@@ -431,6 +632,7 @@ __global__ void lm_choose_kernel(int nstreams, uint8_t* __restrict__ out, const 
 // Training
 
 constexpr int kGradThreads = 128;
+constexpr int kW1Pad = 65;  // rows of 64 floats padded so lanes reading different rows use different banks
 constexpr int kMaxFeats = 48;  // 36 stones + 4 rotation + 8 neighbours
 
 struct lm_grad_smem {
@@ -461,7 +663,18 @@ lm_grad_kernel(const float* __restrict__ params, const lm_block_t* __restrict__ 
     G.w1[(i / kLmHidden) * kW1Pad + i % kLmHidden] = bf16_of(params, kLmW1 + i);
     G.gw1[i / kLmHidden][i % kLmHidden] = 0.f;
   }
-  for (int i = tid; i < kLmHidden * kLmHidden; i += kGradThreads) G.w2[i / kLmHidden][i % kLmHidden] = bf16_of(params, kLmW2 + i);
+  __syncthreads();
+  // W1's rotation and neighbour rows and W2 on their column grids, as the
+  // exported model holds them (lm_grid_params)
+  if (tid < kLmHidden) {
+    float col[kLmHidden];
+    for (int f = 0; f < kLmCtxRows; f++) col[f] = params[kLmW1 + (kLmRot + f) * kLmHidden + tid];
+    lm_grid_column(col, kLmCtxRows, 1);
+    for (int f = 0; f < kLmCtxRows; f++) G.w1[(kLmRot + f) * kW1Pad + tid] = col[f];
+    for (int k = 0; k < kLmHidden; k++) col[k] = params[kLmW2 + k * kLmHidden + tid];
+    lm_grid_column(col, kLmHidden, 1);
+    for (int k = 0; k < kLmHidden; k++) G.w2[k][tid] = col[k];
+  }
   if (tid < kLmHidden) {
     G.b1[tid] = bf16_of(params, kLmB1 + tid);
     G.b2[tid] = bf16_of(params, kLmB2 + tid);
@@ -502,18 +715,26 @@ lm_grad_kernel(const float* __restrict__ params, const lm_block_t* __restrict__ 
     float a2[kLmHidden];
     float z[3] = {0.f, 0.f, 0.f};
     if (y >= 0) {
+      // h1 holds the quantized activations hq / 16 (learned.cuh): the stone
+      // rows summed in order, the last 12 (rotation and neighbour rows, on
+      // their grids) summed exactly, then added
+      const int ns = nf - 12;
       for (int k = 0; k < kLmHidden; k++) {
-        float a = G.b1[k];
-        for (int f = 0; f < nf; f++) a += G.w1[G.feats[tid][f] * kW1Pad + k];
-        G.h1[tid][k] = relu(a);
+        float a = G.b1[k], s1 = 0.f;
+        for (int f = 0; f < ns; f++) a += G.w1[G.feats[tid][f] * kW1Pad + k];
+        for (int f = ns; f < nf; f++) s1 += G.w1[G.feats[tid][f] * kW1Pad + k];
+        G.h1[tid][k] = f_mul(lm_act_q(f_add(a, s1)), kLmActInv);
       }
+      // the layer-2 sums are exact on the grid, so a2 = b2 + sum rounds once
 #pragma unroll
-      for (int j = 0; j < kLmHidden; j++) a2[j] = G.b2[j];
+      for (int j = 0; j < kLmHidden; j++) a2[j] = 0.f;
       for (int k = 0; k < kLmHidden; k++) {
         const float h = G.h1[tid][k];
 #pragma unroll
         for (int j = 0; j < kLmHidden; j++) a2[j] = fmaf(G.w2[k][j], h, a2[j]);
       }
+#pragma unroll
+      for (int j = 0; j < kLmHidden; j++) a2[j] = f_add(G.b2[j], a2[j]);
       z[0] = G.b3[0];
       z[1] = G.b3[1];
       z[2] = G.b3[2];
@@ -557,11 +778,13 @@ lm_grad_kernel(const float* __restrict__ params, const lm_block_t* __restrict__ 
       for (int q = 0; q < kGradThreads; q++) gloss += G.loss[q];
     }
     __syncthreads();
-    // dL/da1 into x
+    // dL/da1 into x: the quantizer passes the gradient straight through
+    // where the activation is neither cut by relu nor clamped at the top
     if (y >= 0) {
       for (int k = 0; k < kLmHidden; k++) {
         float d = 0.f;
-        if (G.h1[tid][k] > 0.f)
+        const float h = G.h1[tid][k];
+        if (h > 0.f && h < kLmActMax * kLmActInv)
           for (int j = 0; j < kLmHidden; j++) d = fmaf(G.w2[k][j], G.d2[tid][j], d);
         G.x[tid][k] = d;
       }
@@ -661,7 +884,22 @@ static bool check_model(const uint8_t* model, std::string& err) {
   if (!model) { err = "null model"; return false; }
   uint32_t h[3];
   memcpy(h, model, 12);
-  if (h[0] != kLmMagic || h[1] != 1 || h[2] != uint32_t(kLmParams)) { err = "not a version-1 PGLM model"; return false; }
+  if (h[0] != kLmMagic || h[1] != kLmModelVersion || h[2] != uint32_t(kLmParams)) {
+    err = "not a version-2 PGLM model";
+    return false;
+  }
+  // W1's rotation and neighbour rows and W2 must lie on their column grids,
+  // or the tensor cores' sums would not be exact
+  std::vector<float> w(kLmParams), q;
+  for (int i = 0; i < kLmParams; i++) {
+    const int b = kLmModelHeader + 2 * i;
+    w[i] = bf16_value(uint16_t(model[b] | model[b + 1] << 8));
+    if (!std::isfinite(w[i])) { err = "non-finite parameter " + std::to_string(i); return false; }
+  }
+  q = w;
+  lm_grid_params(q.data());
+  for (int i = 0; i < kLmParams; i++)
+    if (q[i] != w[i]) { err = "parameter " + std::to_string(i) + " is not on its grid"; return false; }
   return true;
 }
 
@@ -689,6 +927,8 @@ static bool resolve_blocks(const pg_block_ref_t* refs, int n, std::vector<lm_blo
 struct lm_launch {
   uint16_t* params = nullptr;
   lm_block_t* blocks = nullptr;
+  int32_t* order = nullptr;   // streams by node count, largest first (after the blocks)
+  int* next = nullptr;        // the coding kernels' stream counter, zeroed (after the order)
   uint64_t hash = 0;
   cudaStream_t stream = nullptr;
   ~lm_launch() {
@@ -709,8 +949,19 @@ static int lm_prepare(const uint8_t* model, const pg_block_ref_t* refs, int n, c
   }
   std::vector<lm_block_t> B;
   if (!resolve_blocks(refs, n, B, err)) return fail(PG_ERR_ARG, err);
-  PG_CUDA(cudaMallocAsync(&L.blocks, sizeof(lm_block_t) * std::max(n, 1), stream));
+  // One buffer: the blocks, the processing order and the counter
+  std::vector<int32_t> order(n);
+  for (int s = 0; s < n; s++) order[s] = s;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return B[a].nodes > B[b].nodes; });
+  const size_t bb = sizeof(lm_block_t) * std::max(n, 1), ob = (sizeof(int32_t) * std::max(n, 1) + 15) & ~size_t(15);
+  char* buf = nullptr;
+  PG_CUDA(cudaMallocAsync(&buf, bb + ob + 16, stream));
+  L.blocks = reinterpret_cast<lm_block_t*>(buf);
+  L.order = reinterpret_cast<int32_t*>(buf + bb);
+  L.next = reinterpret_cast<int*>(buf + bb + ob);
   PG_CUDA(cudaMemcpyAsync(L.blocks, B.data(), sizeof(lm_block_t) * n, cudaMemcpyHostToDevice, stream));
+  PG_CUDA(cudaMemcpyAsync(L.order, order.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
+  PG_CUDA(cudaMemsetAsync(L.next, 0, sizeof(int), stream));
   if (host_blocks) *host_blocks = std::move(B);
   return PG_OK;
 }
@@ -720,11 +971,15 @@ template<class K> static int lm_smem_opt_in(K kernel, size_t bytes) {
   return PG_OK;
 }
 
-static int lm_grid(int nstreams) {
-  int dev = 0, sms = 148;
+// The coding kernels: as many CTAs as are resident at once (the streams are
+// handed out dynamically), no more than there are streams for.
+template<class K> static int lm_code_grid(K kernel, int nstreams) {
+  int dev = 0, sms = 148, per = 1;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return std::max(1, std::min((nstreams + kLmWarps - 1) / kLmWarps, 4 * sms));
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kLmThreads, kLmCodeSmem) != cudaSuccess || per < 1)
+    per = 1;
+  return std::max(1, std::min((nstreams + kLmWarps - 1) / kLmWarps, per * sms));
 }
 
 }  // namespace pg
@@ -740,11 +995,14 @@ extern "C" int64_t pg_rans_learned_bound(int64_t nodes) {
 
 extern "C" int pg_learned_export(const float* params, uint8_t* model) {
   if (!params || !model) return fail(PG_ERR_ARG, "null argument");
-  const uint32_t h[3] = {kLmMagic, 1u, uint32_t(kLmParams)};
+  const uint32_t h[3] = {kLmMagic, kLmModelVersion, uint32_t(kLmParams)};
   memcpy(model, h, 12);
+  std::vector<float> p(params, params + kLmParams);
+  for (int i = 0; i < kLmParams; i++)
+    if (!std::isfinite(p[i])) return fail(PG_ERR_ARG, "non-finite parameter " + std::to_string(i));
+  lm_grid_params(p.data());
   for (int i = 0; i < kLmParams; i++) {
-    if (!std::isfinite(params[i])) return fail(PG_ERR_ARG, "non-finite parameter " + std::to_string(i));
-    const uint16_t b = bf16_round(params[i]);
+    const uint16_t b = bf16_round(p[i]);
     model[kLmModelHeader + 2 * i] = uint8_t(b);
     model[kLmModelHeader + 2 * i + 1] = uint8_t(b >> 8);
   }
@@ -763,9 +1021,8 @@ extern "C" int pg_rans_learned_encode(const uint8_t* model, const pg_block_ref_t
   std::vector<lm_block_t> hb;
   if (int rc = lm_prepare(model, blocks, nstreams, st, L, &hb)) return rc;
   if (int rc = lm_smem_opt_in(lm_encode_kernel, kLmCodeSmem)) return rc;
-  lm_encode_kernel<<<lm_grid(nstreams), kLmThreads, kLmCodeSmem, st>>>(L.params, L.hash, L.blocks, nstreams,
-                                                                              symbols, offsets, out, out_offsets,
-                                                                              sizes, *T);
+  lm_encode_kernel<<<lm_code_grid(lm_encode_kernel, nstreams), kLmThreads, kLmCodeSmem, st>>>(
+      L.params, L.hash, L.blocks, nstreams, L.order, L.next, symbols, offsets, out, out_offsets, sizes, *T);
   PG_CUDA(cudaGetLastError());
   // Format-2 streams of the same symbols; the smaller one is kept
   // alt_off[s] = slot of stream s; alt_off[nstreams + s] = its symbol count
@@ -805,9 +1062,9 @@ extern "C" int pg_rans_learned_decode(const uint8_t* model, const pg_block_ref_t
   if (int rc = launch_rans_decode(in, in_offsets, in_sizes, nstreams, symbols, sym_offsets, sym_caps, status, 1, st))
     return rc;
   if (int rc = lm_smem_opt_in(lm_decode_kernel, kLmCodeSmem)) return rc;
-  lm_decode_kernel<<<lm_grid(nstreams), kLmThreads, kLmCodeSmem, st>>>(L.params, L.hash, L.blocks, nstreams, in,
-                                                                              in_offsets, in_sizes, symbols,
-                                                                              sym_offsets, sym_caps, status, *T);
+  lm_decode_kernel<<<lm_code_grid(lm_decode_kernel, nstreams), kLmThreads, kLmCodeSmem, st>>>(
+      L.params, L.hash, L.blocks, nstreams, L.order, L.next, in, in_offsets, in_sizes, symbols, sym_offsets, sym_caps,
+      status, *T);
   PG_CUDA(cudaGetLastError());
   return PG_OK;
 }

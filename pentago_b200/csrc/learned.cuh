@@ -6,7 +6,7 @@
 // r = i0 + 4 i1 + 16 i2 + 64 i3 (shard/shard.cc:448-449).  A node's symbols are
 // coded in 128 steps; step s codes rotations s and s + 128 (i3 two apart, so
 // never neighbours).  The probability of symbol r comes from a 3-layer MLP
-// (hidden 64, bf16 weights, fp32 arithmetic) over 120 binary features:
+// (hidden 64, bf16 weights, fp32 accumulation) over 120 binary features:
 //
 //   0..71    stones of the node's board: 18 q + 2 c + colour (colour 0 black,
 //            1 white) for cell c of quadrant q;
@@ -16,20 +16,27 @@
 //            symbol if it was coded in an earlier step, else 3.
 //
 // Encoder and decoder must derive identical integer frequencies, so every
-// float operation on the coding path is a separately rounded IEEE operation
-// in the fixed order below (no contraction, explicit fma), which also makes
-// the coder reproducible on the CPU:
+// float operation on the coding path is either a separately rounded IEEE
+// operation in the fixed order below (no contraction, explicit fma) or exact,
+// which also makes the coder reproducible on the CPU:
 //
 //   node[k] = b1[k], then + W1[f][k] for each stone feature f ascending
-//   RA[i0 + 4 i1][k] = W1[72 + i0][k] + W1[76 + i1][k]   (RB likewise, q = 2, 3)
-//   Pq[va + 4 vb][k] = W1[88 + 8 q + va][k] + W1[92 + 8 q + vb][k]
-//   a1 = (node + (RA + RB)) + ((P0 + P1) + (P2 + P3)),  h1 = a1 > 0 ? a1 : 0
-//   a2[j] = b2[j], then a2[j] = fma(W2[k][j], h1[k], a2[j]) for k = 0..63
-//   z[c] = b3[c], then z[c] = fma(W3[j][c], relu(a2[j]), z[c]) for j = 0..63
+//   S1[k]   = sum of W1[f][k] over the 4 rotation and 8 neighbour features, exact
+//   a1 = node + S1,  hq[k] = rint(min(max(a1 * 16, 0), 255))   (an integer 0..255)
+//   a2[j] = fma(C[j], 1/16, b2[j]),  C[j] = sum over k of W2[k][j] hq[k], exact
+//   z[c] = b3[c] + ((P_0 + P_1) + (P_2 + P_3)), P_t = fma chain from 0 over
+//          the columns j with (j >> 1) & 3 = t ascending of W3[j][c] relu(a2[j])
 //
 // then lm_freqs turns the logits into 15-bit frequencies (each at least 1,
-// summing to 2^15).  Training may run the same network in any order; only the
-// coder needs this one.
+// summing to 2^15).  S1 and C are exact because a model's rotation and
+// neighbour rows of W1 and its W2 lie on grids: every column (hidden unit k of
+// W1 rows 72..119, output j of W2) is integers of magnitude at most 127 times
+// 2^-e (lm_grid_exp), so each term and partial sum is a multiple of 2^-e below
+// 2^21 2^-e and an fp32 sum in any order is exact.  The coder forms both sums
+// on the tensor cores (bf16 inputs: one-hot features and integer activations,
+// fp32 accumulation); version-2 models are checked for the grids when loaded.
+// Training may run the same network in any order; only the coder needs this
+// one.
 #pragma once
 #include "superscore.cuh"
 #include <cmath>
@@ -48,8 +55,11 @@ constexpr int kLmB2 = kLmW2 + kLmHidden * kLmHidden;
 constexpr int kLmW3 = kLmB2 + kLmHidden;
 constexpr int kLmB3 = kLmW3 + kLmHidden * kLmOut;
 constexpr int kLmParams = kLmB3 + kLmOut;  // 12099
-// Serialized model: magic "PGLM", version 1, parameter count, bf16 parameters
+// Serialized model: magic "PGLM", version 2, parameter count, bf16 parameters
 constexpr uint32_t kLmMagic = 0x4d4c4750u;
+constexpr uint32_t kLmModelVersion = 2;
+// Activations entering layer 2: integers 0..kLmActMax, a1 scaled by kLmActScale
+constexpr float kLmActScale = 16.f, kLmActInv = 0.0625f, kLmActMax = 255.f;
 constexpr int kLmModelHeader = 12;
 constexpr int64_t kLmModelBytes = kLmModelHeader + 2 * int64_t(kLmParams);
 // Coder: 32-bit states, 16-bit words, 15-bit probabilities, 32 lanes
@@ -115,6 +125,69 @@ PG_HD uint16_t bf16_round(float f) {
   return uint16_t((u + 0x7fffu + ((u >> 16) & 1u)) >> 16);
 }
 PG_HD float relu(float a) { return a > 0.f ? a : 0.f; }
+
+// rint(v) for 0 <= v <= 2^22: adding 2^23 rounds to an integer (ties to even).
+PG_HD float f_rint_small(float v) { return f_add(f_add(v, 8388608.f), -8388608.f); }
+
+// The quantized activation hq of a1: rint(min(max(a1 * 16, 0), 255)), an
+// integer 0..255 as a float.
+PG_HD float lm_act_q(float a) {
+  float v = f_mul(a, kLmActScale);
+  v = v > 0.f ? v : 0.f;
+  return f_rint_small(v < kLmActMax ? v : kLmActMax);
+}
+
+// Round to nearest, ties to even (v finite, |v| < 2^31).
+PG_HD float f_rint(float v) {
+#ifdef __CUDA_ARCH__
+  return __int2float_rn(__float2int_rn(v));
+#else
+  return std::nearbyint(v);
+#endif
+}
+
+// 2^e as a float, for -126 <= e <= 127.
+PG_HD float f_pow2(int e) { return f_bits(uint32_t(127 + e) << 23); }
+
+// The grid of a column whose largest magnitude is m > 0 (finite): its
+// weights are integers of magnitude at most 127 times 2^-e, with
+// e = 7 - x for m = f 2^x, f in [0.5, 1).  Returns e.
+PG_HD int lm_grid_exp(float m) {
+  int s = 0;
+  if (m < f_pow2(-126)) {   // subnormal: scale into the normal range first (exact)
+    m = f_mul(m, f_pow2(64));
+    s = 64;
+  }
+  const int x = int(f_raw(m) >> 23 & 0xff) - 126;   // m = f 2^x with f in [0.5, 1)
+  return 7 - (x - s);
+}
+// w on grid e: the nearest multiple of 2^-e (ties to even), clamped to
+// +-127 2^-e.  Computed as w 2^e in two power-of-two steps (exact) so e may
+// exceed 127.
+PG_HD float lm_grid_quantize(float w, int e) {
+  const int e1 = e / 2, e2 = e - e1;
+  float q = f_rint(f_mul(f_mul(w, f_pow2(e1)), f_pow2(e2)));
+  q = q > 127.f ? 127.f : q < -127.f ? -127.f : q;
+  return f_mul(f_mul(q, f_pow2(-e1)), f_pow2(-e2));
+}
+// A column of n finite weights w[0], w[stride], ... moved onto its grid, in
+// place.  A column on its grid is left unchanged (its largest magnitude
+// keeps the grid).
+PG_HD void lm_grid_column(float* w, int n, int stride) {
+  float m = 0.f;
+  for (int k = 0; k < n; k++) m = fmaxf(m, fabsf(w[k * stride]));
+  if (!(m > 0.f)) {
+    for (int k = 0; k < n; k++) w[k * stride] = 0.f;
+    return;
+  }
+  const int e = lm_grid_exp(m);
+  for (int k = 0; k < n; k++) w[k * stride] = lm_grid_quantize(w[k * stride], e);
+}
+// Every grid column of a parameter vector (fp32 layout of kLmParams), in place.
+PG_HD void lm_grid_params(float* p) {
+  for (int k = 0; k < kLmHidden; k++) lm_grid_column(p + kLmW1 + kLmRot * kLmHidden + k, kLmIn - kLmRot, kLmHidden);
+  for (int j = 0; j < kLmHidden; j++) lm_grid_column(p + kLmW2 + j, kLmHidden, kLmHidden);
+}
 
 // 2^d for d <= 0, 0 below -24: d = n + t with n = floor(d), t in [0, 1); 2^t
 // from its Taylor series (coefficients ln(2)^i / i!, degree 7, Horner), then
