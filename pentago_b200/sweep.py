@@ -173,8 +173,9 @@ def line_work(sigs, child_sigs):
             nl = int(np.prod([blocks[i] for i in range(4) if i != d]))
             lines[d] += nl
             # microlines of a line: its cross-section (8^3 unless a cross block is short)
-            per_dim = [[min(8, shape[i] - 8 * b) for b in range(blocks[i])] for i in range(4) if i != d]
-            ctas[d] += sum((a * b * cc + 3) // 4 for a in per_dim[0] for b in per_dim[1] for cc in per_dim[2])
+            per_dim = [np.minimum(8, shape[i] - 8 * np.arange(blocks[i])) for i in range(4) if i != d]
+            micro = np.multiply.outer(np.multiply.outer(per_dim[0], per_dim[1]), per_dim[2])
+            ctas[d] += int(((micro + 3) // 4).sum())
             nbytes += 64 * (n + child_nodes.get(c, 0))
     return {"lines": lines, "ctas": ctas, "line_bytes": nbytes}
 
