@@ -271,6 +271,90 @@ PG_HD void traverse(const mid_job_t& J, const mid_tables& MT, const uint4* super
   append(out, board_of(side[0], side[1]) | uint64_t(ply & 1) << 63, value);
 }
 
+#ifdef __CUDA_ARCH__
+// traverse on one warp: the root's children (one per lane) at once, their
+// records placed by a prefix sum over the lanes in the order traverse
+// writes them.
+__device__ void put_record(pg_mid_values_t* out, int k, uint64_t raw, int v) {
+  if (k < 163) { out->entries[k].raw = raw; out->entries[k].value = v; out->entries[k].pad = 0; }
+}
+// The 8 rotation children of sd (8 records at out[at..]); returns their best value for the mover.
+__device__ int middle_children_at(const uint64_t* sd, uint32_t p, const uint4* r, pg_mid_values_t* out, int at) {
+  int best = -1;
+  for (int s = 0; s < 8; s++) {
+    const int q = s >> 1, d = (s & 1) ? -1 : 1;
+    const int idx = ((d & 3) << (2 * q)) >> 1;
+    const int v = hbit(r[0], idx) + hbit(r[1], idx) - 1;
+    uint64_t rs[2] = {sd[0], sd[1]};
+    rotate_sides(rs, q, d);
+    put_record(out, at + s, board_of(rs[0], rs[1]) | uint64_t((p + 1) & 1) << 63, v);
+    best = best > -v ? best : -v;
+  }
+  return best;
+}
+__device__ void traverse_warp(const mid_job_t& J, const mid_tables& MT, const uint4* supers, pg_mid_values_t* out,
+                              int lane) {
+  const unsigned full = 0xffffffffu;
+  const uint64_t side[2] = {J.side[0], J.side[1]};
+  const uint32_t ply = J.ply;
+  int value = 0, total = 0;
+  if (done_value(MT, side, ply, &value)) {
+  } else if (!(ply & 1)) {
+    // lane s: the s-th empty cell (at most 18)
+    const uint64_t empty = 0x01ff01ff01ff01ffull ^ side[0] ^ side[1];
+    const int nempty = __popcll(empty);
+    int cnt = 0, cv = -1;
+    uint64_t cs[2] = {side[0], side[1]};
+    if (lane < nempty) {
+      uint64_t e = empty;
+      for (int i = 0; i < lane; i++) e &= e - 1;
+      cs[(ply >> 1) & 1] |= e & (~e + 1);
+      cnt = done_value(MT, cs, ply + 1, &cv) ? 1 : 9;
+    }
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(full, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int base = incl - cnt;
+    total = __shfl_sync(full, incl, 31);
+    if (lane < nempty) {
+      if (cnt == 9) cv = middle_children_at(cs, ply + 1, supers + 2 * (lane + 1), out, base);
+      put_record(out, base + cnt - 1, board_of(cs[0], cs[1]) | uint64_t(1) << 63, cv);
+    }
+    int v = cv;
+    for (int o = 16; o; o >>= 1) {
+      const int w = __shfl_xor_sync(full, v, o);
+      v = v > w ? v : w;
+    }
+    value = v;
+  } else {
+    // lanes 0..7: the root's 8 rotation children
+    int best = -1;
+    if (lane < 8) {
+      const int q = lane >> 1, d = (lane & 1) ? -1 : 1;
+      const int idx = ((d & 3) << (2 * q)) >> 1;
+      const int v = hbit(supers[0], idx) + hbit(supers[1], idx) - 1;
+      uint64_t rs[2] = {side[0], side[1]};
+      rotate_sides(rs, q, d);
+      put_record(out, lane, board_of(rs[0], rs[1]) | uint64_t((ply + 1) & 1) << 63, v);
+      best = -v;
+    }
+    for (int o = 16; o; o >>= 1) {
+      const int w = __shfl_xor_sync(full, best, o);
+      best = best > w ? best : w;
+    }
+    value = best;
+    total = 8;
+  }
+  if (lane == 0) {
+    put_record(out, total, board_of(side[0], side[1]) | uint64_t(ply & 1) << 63, value);
+    out->size = total + 1;
+    out->pad = 0;
+  }
+}
+#endif
+
 // The whole solve of one board by ncta groups of nt cooperating threads
 // (thread tid of group cta).  `barrier` synchronizes one group, `gbarrier`
 // all groups (with one group it is the same barrier).  Inside a level the
@@ -349,6 +433,17 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
   // Interleave (midengine.cc:119-124) and traverse; a failed bounds check
   // marks the record with size -1 instead.
   if (gtid == 0 && *fault) { J.out->size = -1; J.out->pad = 0; }
+#ifdef __CUDA_ARCH__
+  // the first warp traverses (nt >= 32 on the device)
+  if (gtid < 32 && !*fault) {
+    uint4 supers[2 * 19];
+    for (int i = 0; i < 19; i++)
+      for (int j = 0; j < 2; j++) supers[2 * i + j] = raw[j ^ (i == 0)][i];
+    if (dump && gtid == 0)
+      for (int i = 0; i < 38; i++) dump[i] = supers[i];
+    traverse_warp(J, MT, supers, J.out, gtid);
+  }
+#else
   if (gtid == 0 && !*fault) {
     uint4 supers[2 * 19];
     for (int i = 0; i < 19; i++)
@@ -357,6 +452,7 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
       for (int i = 0; i < 38; i++) dump[i] = supers[i];
     traverse(J, MT, supers, J.out);
   }
+#endif
 }
 
 

@@ -187,9 +187,9 @@ def algorithmic_bytes(raw):
     return 2 * total
 
 
-def bench_boards_26(steps=20, warmup=3, sm_max_mhz=1965.0):
+def bench_boards_26(steps=50, warmup=3, sm_max_mhz=1965.0, trials=5):
     """64 seeded 26-stone boards (13 black, 13 white, no five);
-    GPU time per batch from CUDA events (median of three trials), and the
+    GPU time per batch from CUDA events (median of `trials` trials), and the
     same batch end to end: boards in from the host through the C ABI and the
     64 result records (mid_values_t) copied back to pinned host memory every
     batch.  Returns the result and the boards."""
@@ -222,9 +222,9 @@ def bench_boards_26(steps=20, warmup=3, sm_max_mhz=1965.0):
         device_batch()
         e2e_batch()
     torch.cuda.synchronize()
-    # three trials of `steps` batches each; the median trial is reported
-    ms = sorted(trial(device_batch) for _ in range(3))[1]
-    e2e_ms = sorted(trial(e2e_batch) for _ in range(3))[1]
+    # `trials` trials of `steps` batches each; the median trial is reported
+    ms = sorted(trial(device_batch) for _ in range(trials))[trials // 2]
+    e2e_ms = sorted(trial(e2e_batch) for _ in range(trials))[trials // 2]
     sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     peak = 128 * sms * sm_max_mhz * 1e6 / 1e9
     result = {"workload": "64 seeded 26-stone boards (13 black, 13 white, no five), full midsolve",
