@@ -298,9 +298,9 @@ int pg_store_decode(const uint8_t* in, const int64_t* in_offsets, const int64_t*
  * reference counterpart; it replaces the per-block static table of format 2
  * (arithmetic_encode, pentago/shard/arithmetic.cc:366-401) by a 3-layer MLP
  * (hidden 64, bf16 weights, fp32 accumulation) that predicts each symbol from
- * the node's board, the rotation and the already coded neighbouring
- * rotations.  Streams are blocks of a section; symbols are pg_node_symbols'
- * (256 per node, nodes in the block's C order).  The encoder keeps whichever
+ * the node's board, the rotation, the already coded neighbouring rotations
+ * and the previous node's symbol.  Streams are blocks of a section; symbols
+ * are pg_node_symbols' (256 per node, nodes in the block's C order).  The encoder keeps whichever
  * of format 3 and format 2 is smaller, and the decoder reads both.
  * ------------------------------------------------------------------------- */
 
@@ -309,9 +309,9 @@ typedef struct pg_block_ref_t {
   int32_t block[4];   /* block coordinates, 8 positions per block per quadrant */
 } pg_block_ref_t;
 
-/* Bytes of a serialized model: "PGLM", version 2, parameter count, bf16
- * parameters.  In a version-2 model every column of W1's rotation and
- * neighbour rows (72..119) and of W2 lies on a grid (integers of magnitude at
+/* Bytes of a serialized model: "PGLM", version 3, parameter count, bf16
+ * parameters.  In a version-3 model every column of W1's rotation, neighbour
+ * and previous-node rows (72..123) and of W2 lies on a grid (integers of magnitude at
  * most 127 times a power of two), which makes the coder's tensor-core sums
  * exact; pg_learned_export puts them there, and the coder refuses a model
  * whose weights are not. */

@@ -6,16 +6,18 @@
  * written on the GPU decodes here and the bytes written here equal the GPU's:
  *
  *   coding order of a node: 128 steps, step s codes rotation s then s + 128;
- *   features of symbol r of node i of a block (120 binary inputs):
+ *   features of symbol r of node i of a block (124 binary inputs):
  *     18 q + 2 c + colour    stone of colour (0 black, 1 white) on cell c of quadrant q
  *     72 + 4 q + i_q         rotation r = i0 + 4 i1 + 16 i2 + 64 i3
  *     88 + 4 n + v           neighbour n = 2 q + e (quadrant q turned +1 for e = 0,
  *                            +3 for e = 1): its symbol if its step is earlier, else v = 3
- *   network: W1 (120 x 64), b1, W2 (64 x 64), b2, W3 (64 x 3), b3 as bf16 (model
- *     version 2: every column of W1 rows 72..119 and of W2 is integers of magnitude
+ *     120 + v                the previous node of the lane's run: its symbol r, 3 for
+ *                            a run's first node
+ *   network: W1 (124 x 64), b1, W2 (64 x 64), b2, W3 (64 x 3), b3 as bf16 (model
+ *     version 3: every column of W1 rows 72..123 and of W2 is integers of magnitude
  *     at most 127 times 2^-e, e = 7 - x for the column's largest magnitude f 2^x,
  *     f in [0.5, 1)); a1 = node + S1 with node = b1 + stone rows ascending and S1 the
- *     exact sum of the rows of the 4 rotation and 8 neighbour features;
+ *     exact sum of the rows of the 4 rotation, 8 neighbour and 1 previous-node features;
  *     hq = rint(min(max(a1 * 16, 0), 255)); a2 = fma(C, 1/16, b2) with C = the exact
  *     sum over k of W2[k][j] hq[k]; relu(a) = a > 0 ? a : 0; z = b3 + ((P_0 + P_1) +
  *     (P_2 + P_3)) where P_t is the fma chain from 0 over the columns j with
@@ -24,9 +26,10 @@
  *     degree 7, f_c = 1 + trunc(e_c / (e0 + e1 + e2) * 32765), remainder to the
  *     first largest
  *   stream: version 3 | FNV-1a-64 of the model | nodes | words | 32 lane states |
- *     16-bit words; node i on lane i % 32; the encoder runs the decoder's
- *     sequence (round, step, rotation s then s + 128) backward, and
- *     renormalizing lanes append x & 0xffff in lane order when x >= f << 17.
+ *     16-bit words; lane l codes the run of nodes l R .. l R + R - 1 (R = ceil(n / 32)),
+ *     node l R + k in round k; the encoder runs the decoder's sequence (round,
+ *     step, rotation s then s + 128) backward, and renormalizing lanes append
+ *     x & 0xffff in lane order when x >= f << 17.
  */
 #include <math.h>
 #include <stdint.h>
@@ -35,7 +38,7 @@
 
 #include "pentago_oracle.h"
 
-#define NIN 120
+#define NIN 124
 #define NH 64
 #define NP (NIN * NH + NH + NH * NH + NH + NH * 3 + 3)
 #define OFF_W1 0
@@ -143,7 +146,7 @@ static void grid_params(float* p) {
 static int load_model(const uint8_t* bytes, model* m) {
   uint32_t h[3];
   memcpy(h, bytes, 12);
-  if (h[0] != 0x4d4c4750u || h[1] != 2 || h[2] != NP) return -1;
+  if (h[0] != 0x4d4c4750u || h[1] != 3 || h[2] != NP) return -1;
   for (int i = 0; i < NP; i++) m->p[i] = bf16((uint16_t)(bytes[12 + 2 * i] | bytes[13 + 2 * i] << 8));
   float* q = malloc(sizeof(float) * NP);
   memcpy(q, m->p, sizeof(float) * NP);
@@ -162,19 +165,28 @@ static float act_q(float a) {
   return (v + 8388608.f) - 8388608.f;
 }
 
-/* The 12 rotation and neighbour features of symbol r (rows of W1). */
-static void ctx_features(int r, const uint8_t* sym, int* f) {
+/* The 13 rotation, neighbour and previous-node features of symbol r (rows of
+ * W1); prev is the previous node's symbols, or null for a run's first node. */
+static void ctx_features(int r, const uint8_t* sym, const uint8_t* prev, int* f) {
   for (int q = 0; q < 4; q++) f[q] = 72 + 4 * q + ((r >> (2 * q)) & 3);
   for (int nb = 0; nb < 8; nb++) f[4 + nb] = 88 + 4 * nb + context(sym, r, nb);
+  f[12] = 120 + (prev ? (prev[r] & 3) : 3);
 }
 
-static void logits(const model* m, const float* node, int r, const uint8_t* sym, float* z) {
+/* The run length of a block of n nodes (lane l codes nodes l R .. l R + R - 1),
+ * and node i's previous node's symbols (null for a run's first node). */
+static int64_t run_length(int64_t n) { return (n + 31) / 32; }
+static const uint8_t* prev_of(const uint8_t* symbols, int64_t n, int64_t i) {
+  return i % run_length(n) ? symbols + 256 * (i - 1) : NULL;
+}
+
+static void logits(const model* m, const float* node, int r, const uint8_t* sym, const uint8_t* prev, float* z) {
   float hq[NH], part[4][3];
-  int f[12];
-  ctx_features(r, sym, f);
+  int f[13];
+  ctx_features(r, sym, prev, f);
   for (int k = 0; k < NH; k++) {
-    double s1 = 0;   /* exact: at most 12 x 127 units of 2^-e_k */
-    for (int i = 0; i < 12; i++) s1 += W1(f[i], k);
+    double s1 = 0;   /* exact: at most 13 x 127 units of 2^-e_k */
+    for (int i = 0; i < 13; i++) s1 += W1(f[i], k);
     hq[k] = act_q(node[k] + (float)s1);
   }
   memset(part, 0, sizeof part);
@@ -236,7 +248,7 @@ int or_lm_freqs(const uint8_t* model_bytes, uint64_t section, const int* block, 
     const int r = (int)(samples[t] & 255);
     float node[NH], z[3];
     node_sum(m, &g, i, node);
-    logits(m, node, r, symbols + 256 * i, z);
+    logits(m, node, r, symbols + 256 * i, prev_of(symbols, g.nodes, i), z);
     freqs(z, out + 3 * t);
   }
   free(m);
@@ -260,7 +272,7 @@ int64_t or_lm_encode(const uint8_t* model_bytes, uint64_t section, const int* bl
   geom g;
   model* m = malloc(sizeof(model));
   if (block_geom(section, block, &g) || load_model(model_bytes, m)) { free(m); return -1; }
-  const int64_t n = g.nodes, rounds = (n + 31) / 32;
+  const int64_t n = g.nodes, rounds = run_length(n);
   if (cap < HEADER + 2 * 256 * n) { free(m); return -1; }
   uint32_t x[32];
   for (int l = 0; l < 32; l++) x[l] = 1u << 16;
@@ -268,17 +280,17 @@ int64_t or_lm_encode(const uint8_t* model_bytes, uint64_t section, const int* bl
   float (*node)[NH] = malloc(sizeof(float) * NH * 32);
   for (int64_t round = rounds - 1; round >= 0; round--) {
     for (int l = 0; l < 32; l++)
-      if (32 * round + l < n) node_sum(m, &g, 32 * round + l, node[l]);
+      if (rounds * l + round < n) node_sum(m, &g, rounds * l + round, node[l]);
     for (int t = 255; t >= 0; t--)
       for (int l = 0; l < 32; l++) {
         const int r = (t >> 1) + 128 * (t & 1);  /* decoder sequence t: step t / 2, half t % 2 */
-        const int64_t i = 32 * round + l;
+        const int64_t i = rounds * l + round;
         if (i >= n) continue;
         const uint8_t* sym = symbols + 256 * i;
         if (sym[r] > 2) { free(node); free(m); return -1; }
         float z[3];
         uint32_t f[3];
-        logits(m, node[l], r, sym, z);
+        logits(m, node[l], r, sym, prev_of(symbols, n, i), z);
         freqs(z, f);
         const int v = sym[r];
         const uint32_t cum = v == 0 ? 0 : v == 1 ? f[0] : f[0] + f[1];
@@ -309,7 +321,7 @@ int64_t or_lm_decode(const uint8_t* model_bytes, uint64_t section, const int* bl
   geom g;
   model* m = malloc(sizeof(model));
   if (block_geom(section, block, &g) || load_model(model_bytes, m)) { free(m); return -1; }
-  const int64_t n = g.nodes, rounds = (n + 31) / 32;
+  const int64_t n = g.nodes, rounds = run_length(n);
   const uint64_t h = fnv1a(model_bytes, MODEL_BYTES);
   if (size < HEADER || get32(in) != 3 || get32(in + 4) != (uint32_t)h || get32(in + 8) != (uint32_t)(h >> 32) ||
       get32(in + 12) != (uint32_t)n || HEADER + 2 * (int64_t)get32(in + 16) != size || cap < 256 * n) {
@@ -323,18 +335,18 @@ int64_t or_lm_decode(const uint8_t* model_bytes, uint64_t section, const int* bl
   int bad = 0;
   for (int64_t round = 0; round < rounds; round++) {
     for (int l = 0; l < 32; l++)
-      if (32 * round + l < n) node_sum(m, &g, 32 * round + l, node[l]);
+      if (rounds * l + round < n) node_sum(m, &g, rounds * l + round, node[l]);
     for (int t = 0; t < 256; t++) {
       const int r = (t >> 1) + 128 * (t & 1);
       int need[32], k = 0;
       for (int l = 0; l < 32; l++) {
-        const int64_t i = 32 * round + l;
+        const int64_t i = rounds * l + round;
         need[l] = 0;
         if (i >= n) continue;
         uint8_t* sym = symbols + 256 * i;
         float z[3];
         uint32_t f[3];
-        logits(m, node[l], r, sym, z);
+        logits(m, node[l], r, sym, prev_of(symbols, n, i), z);
         freqs(z, f);
         const uint32_t slot = x[l] & 32767u;
         const int v = slot < f[0] ? 0 : slot < f[0] + f[1] ? 1 : 2;
@@ -383,16 +395,18 @@ double or_lm_grad(const float* params, uint64_t section, const int* block, const
     const uint8_t* sym = symbols + 256 * i;
     if (i >= g.nodes || sym[r] > 2) continue;
     const int y = sym[r];
-    int f[48];
+    int f[49];
     int nf = stones(&g, i, f);
     for (int q = 0; q < 4; q++) f[nf++] = 72 + 4 * q + ((r >> (2 * q)) & 3);
     for (int nb = 0; nb < 8; nb++) f[nf++] = 88 + 4 * nb + context(sym, r, nb);
+    const uint8_t* prev = prev_of(symbols, g.nodes, i);
+    f[nf++] = 120 + (prev ? (prev[r] & 3) : 3);
     float h1[NH], a2[NH], h2[NH], z[3];
-    for (int k = 0; k < NH; k++) {   /* h1 = hq / 16; the last 12 rows summed exactly */
+    for (int k = 0; k < NH; k++) {   /* h1 = hq / 16; the last 13 rows summed exactly */
       float a = m->p[OFF_B1 + k];
       double s1 = 0;
-      for (int q = 0; q < nf - 12; q++) a = a + W1(f[q], k);
-      for (int q = nf - 12; q < nf; q++) s1 += W1(f[q], k);
+      for (int q = 0; q < nf - 13; q++) a = a + W1(f[q], k);
+      for (int q = nf - 13; q < nf; q++) s1 += W1(f[q], k);
       h1[k] = act_q(a + (float)s1) * 0.0625f;
     }
     for (int j = 0; j < NH; j++) {

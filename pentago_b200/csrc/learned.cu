@@ -2,14 +2,12 @@
 // kernels that train its network.  The model and the exact arithmetic of the
 // coding path are specified in learned.cuh.
 //
-// Coder layout: one warp per stream; node i of the block is coded by lane
-// i % 32, whose own rANS state walks the steps (round i / 32, rotation r) in
-// order.  The encoder runs the steps backward; at each step the lanes that
-// renormalize append one 16-bit word each, in lane order, to the stream's
-// shared word array, so the decoder (running forward) finds the words of its
-// step as the last unread ones.  The network runs once per symbol on every
-// lane, from tables staged in shared memory (stone rows of W1, pair sums of
-// the rotation and neighbour rows, W2, W3).
+// Coder layout: one warp per stream; lane l codes the run of nodes l R ..
+// l R + R - 1 (R = ceil(n / 32)), node l R + k in round k, its own rANS
+// state walking the steps (round, rotation) in order.  The encoder runs the
+// steps backward; at each step the lanes that renormalize append one 16-bit
+// word each, in lane order, to the stream's shared word array, so the decoder
+// (running forward) finds the words of its step as the last unread ones.
 //
 // Training: one thread per sample (stream, node, rotation) computes the
 // forward pass and the backward pass of the softmax cross entropy with the
@@ -36,9 +34,7 @@ int launch_rans_decode(const uint8_t* in, const int64_t* in_offsets, const int64
 
 constexpr int kLmWarps = 4;
 constexpr int kLmThreads = 32 * kLmWarps;
-constexpr int kW1Words = 33;  // a stone row of W1: 64 bf16 as 32 words, padded so lanes reading different rows
-                              // use different banks
-constexpr int kLmCtxRows = kLmIn - kLmRot;   // W1 rows 72..119: the rotation and neighbour features
+constexpr int kLmCtxRows = kLmIn - kLmRot;   // W1 rows 72..123: the rotation, neighbour and previous-node features
 
 // Coding tables in shared memory.  The tensor cores' B operands are stored
 // transposed, one row of 64 bf16 (8 chunks of 16 bytes) per output unit:
@@ -46,7 +42,6 @@ constexpr int kLmCtxRows = kLmIn - kLmRot;   // W1 rows 72..119: the rotation an
 // row j holds W2[8 c .. 8 c + 7][j], chunk c at c ^ (row & 7) so that the
 // eight rows an ldmatrix phase reads fall in different banks.
 struct lm_tables {
-  uint32_t w1s[72 * kW1Words];   // stone rows of W1, bf16 pairs (k, k + 1)
   uint4 w1t[kLmHidden][8];
   uint4 w2t[kLmHidden][8];
   float b1[kLmHidden], b2[kLmHidden];
@@ -58,11 +53,6 @@ __device__ __forceinline__ int swz(int row, int chunk) { return chunk ^ (row & 7
 
 __device__ void lm_build_tables(lm_tables& S, const uint16_t* __restrict__ P, int tid, int nt) {
   auto w = [&](int i) { return bf16_value(P[i]); };
-  for (int i = tid; i < 72 * 32; i += nt) {
-    const int f = i >> 5, k2 = i & 31;
-    S.w1s[f * kW1Words + k2] = uint32_t(P[kLmW1 + f * kLmHidden + 2 * k2]) |
-                               uint32_t(P[kLmW1 + f * kLmHidden + 2 * k2 + 1]) << 16;
-  }
   for (int i = tid; i < kLmHidden * 8; i += nt) {
     const int j = i >> 3, c = i & 7;
     uint32_t v[4], u[4];
@@ -94,42 +84,52 @@ __device__ __forceinline__ float lm_tab(const uint4 (*tab)[8], int row, int k) {
   return f_bits(k & 1 ? pr & 0xffff0000u : pr << 16);
 }
 
-// node[k] = b1[k] + stone rows, ascending (registers of one thread).
-__device__ __forceinline__ void lm_node_sum(const lm_tables& S, const uint8_t* feats, int nf, float* node) {
+// node[k] = b1[k] + stone rows, ascending (registers of one thread); the
+// stone rows are read from the model (bf16, global memory: a lane reads them
+// once per node).
+__device__ __forceinline__ void lm_node_sum(const lm_tables& S, const uint16_t* __restrict__ P, const uint8_t* feats,
+                                            int nf, float* node) {
 #pragma unroll
   for (int k = 0; k < kLmHidden; k++) node[k] = S.b1[k];
   for (int i = 0; i < nf; i++) {
-    const uint32_t* row = S.w1s + feats[i] * kW1Words;
+    const uint4* row = reinterpret_cast<const uint4*>(P + kLmW1 + feats[i] * kLmHidden);
 #pragma unroll
-    for (int k2 = 0; k2 < 32; k2++) {
-      const uint32_t v = row[k2];
-      node[2 * k2] = f_add(node[2 * k2], f_bits(v << 16));
-      node[2 * k2 + 1] = f_add(node[2 * k2 + 1], f_bits(v & 0xffff0000u));
+    for (int c = 0; c < 8; c++) {
+      const uint4 v = ldg(row + c);
+      const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        node[8 * c + 2 * e] = f_add(node[8 * c + 2 * e], f_bits(w[e] << 16));
+        node[8 * c + 2 * e + 1] = f_add(node[8 * c + 2 * e + 1], f_bits(w[e] & 0xffff0000u));
+      }
     }
   }
 }
 
-// The 4 rotation and 8 neighbour features of symbol r (indices into W1 rows
-// 72..119): 4 q + i_q, then 16 + 4 n + v_n with u[q] = v_2q + 4 v_2q+1.
-__device__ __forceinline__ void lm_ctx_features(int r, const int* u, int* f) {
+// The 4 rotation, 8 neighbour and 1 previous-node features of symbol r
+// (indices into W1 rows 72..123): 4 q + i_q, then 16 + 4 n + v_n with
+// u[q] = v_2q + 4 v_2q+1, then 48 + the previous node's symbol (3: none).
+__device__ __forceinline__ void lm_ctx_features(int r, const int* u, int prev, int* f) {
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     f[q] = 4 * q + ((r >> (2 * q)) & 3);
     f[4 + 2 * q] = 16 + 8 * q + (u[q] & 3);
     f[5 + 2 * q] = 20 + 8 * q + (u[q] >> 2);
   }
+  f[12] = kLmPrev - kLmRot + prev;
 }
 
 // Logits of one symbol, one thread (the frequency check kernel): S1 and C by
-// fp32 chains, exact on a version-2 model, and layer 3 in the order of
+// fp32 chains, exact on a model whose grid columns are on their grids, and layer 3 in the order of
 // learned.cuh.
-__device__ __forceinline__ void lm_logits(const lm_tables& S, const float* node, int r, const int* u, float* z) {
-  int f[12];
-  lm_ctx_features(r, u, f);
+__device__ __forceinline__ void lm_logits(const lm_tables& S, const float* node, int r, const int* u, int prev,
+                                          float* z) {
+  int f[13];
+  lm_ctx_features(r, u, prev, f);
   float hq[kLmHidden];
   for (int k = 0; k < kLmHidden; k++) {
     float s1 = 0.f;
-    for (int i = 0; i < 12; i++) s1 = f_add(s1, lm_tab(S.w1t, k, f[i]));
+    for (int i = 0; i < 13; i++) s1 = f_add(s1, lm_tab(S.w1t, k, f[i]));
     hq[k] = lm_act_q(f_add(node[k], s1));
   }
   float part[4][3];
@@ -203,18 +203,21 @@ __device__ __forceinline__ void lm_node_frag(const float* own, int kc, int lane,
 }
 
 // Logits of the two symbols of step s (rotations s and s + 128) of every
-// lane's node.  ctx is the lane's neighbour context (symbol s in bits 0-15,
-// s + 128 in bits 16-31; 4 bits u_q = v_2q + 4 v_2q+1 per quadrant q).
-// Layer 1's rotation and neighbour rows and layer 2 run on the tensor cores;
-// layer 1's results stay in registers as layer 2's A operand.
-__device__ __forceinline__ void lm_step_logits(const lm_tables& S, const lm_nodefrag& N, int lane, int s, uint32_t ctx,
-                                               float* zA, float* zB) {
+// lane's node.  ctx[0], ctx[1] are the lane's contexts of the two symbols:
+// 4 bits u_q = v_2q + 4 v_2q+1 per quadrant q (bits 0-15), the previous
+// node's symbol (bits 16-17).  Layer 1's rotation, neighbour and
+// previous-node rows and layer 2 run on the tensor cores; layer 1's results
+// stay in registers as layer 2's A operand.
+__device__ __forceinline__ void lm_step_logits(const lm_tables& S, const lm_nodefrag& N, int lane, int s,
+                                               const uint32_t* ctx, float* zA, float* zB) {
   const int g = lane >> 2, t = lane & 3;
-  uint32_t cx[2][2];
+  uint32_t cx[2][2][2];   // [m & 1][h][symbol]
 #pragma unroll
   for (int mm = 0; mm < 2; mm++)
 #pragma unroll
-    for (int h = 0; h < 2; h++) cx[mm][h] = __shfl_sync(0xffffffffu, ctx, 16 * mm + 8 * h + g);
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+      for (int sb = 0; sb < 2; sb++) cx[mm][h][sb] = __shfl_sync(0xffffffffu, ctx[sb], 16 * mm + 8 * h + g);
   // Row lane is in tile lane / 16 (symbol s) and tile 2 + lane / 16 (s + 128),
   // half (lane / 8) & 1 of quad lane & 7.
   const int src = 4 * (lane & 7), mine = lane >> 4, half = (lane >> 3) & 1;
@@ -228,26 +231,29 @@ __device__ __forceinline__ void lm_step_logits(const lm_tables& S, const lm_node
       // Layer 1 A operand: one-hot features.  k-tile 0 is the rotation
       // (feature 4 q + i_q; the lane's columns 2 t, 2 t + 1 and 8 + 2 t,
       // 9 + 2 t are quadrants t / 2 and 2 + t / 2), the same for every node;
-      // k-tiles 1 and 2 are neighbours n = 4 (kt - 1) + t / 2 and n + 2.
+      // k-tiles 1 and 2 are neighbours n = 4 (kt - 1) + t / 2 and n + 2;
+      // k-tile 3 is the previous node's symbol (columns 0-3: lanes t < 2).
       const int base = 2 * (t & 1);
-      uint32_t a1[3][4];
+      uint32_t a1[4][4];
       a1[0][0] = a1[0][1] = onehot2((r >> (2 * (t >> 1))) & 3, base);
       a1[0][2] = a1[0][3] = onehot2((r >> (2 * (2 + (t >> 1)))) & 3, base);
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const uint32_t u = cx[mm][h] >> (16 * sb);
+        const uint32_t u = sb ? cx[mm][h][1] : cx[mm][h][0];
 #pragma unroll
         for (int kt = 1; kt < 3; kt++) {
           const int n0 = 4 * (kt - 1) + (t >> 1);
           a1[kt][h] = onehot2(int(u >> (2 * n0)) & 3, base);
           a1[kt][2 + h] = onehot2(int(u >> (2 * (n0 + 2))) & 3, base);
         }
+        a1[3][h] = t < 2 ? onehot2(int(u >> 16) & 3, 2 * t) : 0u;
+        a1[3][2 + h] = 0u;
       }
       float acc[8][4];
 #pragma unroll
       for (int n = 0; n < 8; n++) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
 #pragma unroll
-      for (int kt = 0; kt < 3; kt++) mma_row(acc, a1[kt], S.w1t, kt, lane);
+      for (int kt = 0; kt < 4; kt++) mma_row(acc, a1[kt], S.w1t, kt, lane);
       // a1 = node + S1, quantized: n-tiles 2 k and 2 k + 1 of layer 1 are the
       // k-tile k of layer 2's A operand
       uint32_t a2[4][4];
@@ -326,8 +332,9 @@ __device__ __forceinline__ int lm_load_node(const lm_block_t& B, int64_t i, cons
 
 // The lane's node: its node sums (b1 + stone rows ascending), 16 units at a
 // time, spread to the warp's fragment places.
-__device__ __forceinline__ void lm_round_nodes(const lm_tables& S, const lm_block_t& B, int64_t i, bool active,
-                                               const dev_tables_t& T, int lane, lm_nodefrag& N) {
+__device__ __forceinline__ void lm_round_nodes(const lm_tables& S, const uint16_t* __restrict__ P,
+                                               const lm_block_t& B, int64_t i, bool active, const dev_tables_t& T,
+                                               int lane, lm_nodefrag& N) {
   uint8_t feats[36];
   const int nf = active ? lm_load_node(B, i, T, feats) : 0;
 #pragma unroll
@@ -336,15 +343,35 @@ __device__ __forceinline__ void lm_round_nodes(const lm_tables& S, const lm_bloc
 #pragma unroll
     for (int u = 0; u < 16; u++) own[u] = S.b1[16 * kc + u];
     for (int f = 0; f < nf; f++) {
-      const uint32_t* row = S.w1s + feats[f] * kW1Words + 8 * kc;
+      const uint4* row = reinterpret_cast<const uint4*>(P + kLmW1 + feats[f] * kLmHidden + 16 * kc);
 #pragma unroll
-      for (int u = 0; u < 8; u++) {
-        const uint32_t v = row[u];
-        own[2 * u] = f_add(own[2 * u], f_bits(v << 16));
-        own[2 * u + 1] = f_add(own[2 * u + 1], f_bits(v & 0xffff0000u));
+      for (int c = 0; c < 2; c++) {
+        const uint4 v = ldg(row + c);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          own[8 * c + 2 * e] = f_add(own[8 * c + 2 * e], f_bits(w[e] << 16));
+          own[8 * c + 2 * e + 1] = f_add(own[8 * c + 2 * e + 1], f_bits(w[e] & 0xffff0000u));
+        }
       }
     }
     lm_node_frag(own, kc, lane, N);
+  }
+}
+
+// A run's previous node (its symbols, 2 bits each, 17 words a lane so that
+// lanes reading the same rotation use different banks); 3 for every
+// rotation before a run's first node.
+constexpr int kLmPrevWords = 17;
+__device__ __forceinline__ int lm_prev_sym(const uint32_t* prev, int r) { return int(prev[r >> 4] >> (2 * (r & 15))) & 3; }
+__device__ __forceinline__ void lm_prev_none(uint32_t* prev) {
+  for (int w = 0; w < 16; w++) prev[w] = 0xffffffffu;
+}
+__device__ __forceinline__ void lm_prev_from(uint32_t* prev, const uint8_t* sym) {
+  for (int w = 0; w < 16; w++) {
+    uint32_t v = 0;
+    for (int k = 0; k < 16; k++) v |= uint32_t(sym[16 * w + k] & 3) << (2 * k);
+    prev[w] = v;
   }
 }
 
@@ -357,11 +384,12 @@ __device__ __forceinline__ uint32_t get32(const uint8_t* p) {
 
 // Dynamic shared memory of the coding kernels: the tables, then per warp its
 // lanes' nodes' symbols (one row of 256 bytes a lane, rows 260 bytes apart
-// so that lanes reading the same rotation use different banks) and, for the
-// decoder, a window of the stream's next words.
+// so that lanes reading the same rotation use different banks), their
+// previous nodes' symbols (packed) and, for the decoder, a window of the
+// stream's next words.
 constexpr int kLmSymRow = 260;
 constexpr int kLmWordWin = 1024;   // the decoder's window of upcoming stream words, per warp
-constexpr size_t kLmWarpSmem = size_t(32) * kLmSymRow + 2 * kLmWordWin;
+constexpr size_t kLmWarpSmem = size_t(32) * kLmSymRow + size_t(32) * 4 * kLmPrevWords + 2 * kLmWordWin;
 constexpr size_t kLmCodeSmem = sizeof(lm_tables) + kLmWarpSmem * kLmWarps;
 static_assert(sizeof(lm_tables) % 16 == 0 && kLmWarpSmem % 16 == 0, "coding rows stay 16-byte aligned");
 
@@ -452,6 +480,8 @@ lm_encode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint8_t* row = lm_smem_raw + sizeof(lm_tables) + kLmWarpSmem * warp + kLmSymRow * lane;
+  uint32_t* prev = reinterpret_cast<uint32_t*>(lm_smem_raw + sizeof(lm_tables) + kLmWarpSmem * warp +
+                                               32 * kLmSymRow) + kLmPrevWords * lane;
   const unsigned below = (1u << lane) - 1;
   for (int s; (s = lm_next_stream(next, order, nstreams, lane)) >= 0;) {
     const lm_block_t B = blocks[s];
@@ -466,15 +496,21 @@ lm_encode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
     uint32_t x = kLmLower;
     uint32_t len = 0;
     int bad = 0;
-    const int64_t rounds = (n + 31) / 32;
-    for (int64_t round = rounds - 1; round >= 0; round--) {
-      const int64_t i = 32 * round + lane;
+    const int64_t R = (n + 31) / 32;   // the run of nodes of each lane
+    for (int64_t round = R - 1; round >= 0; round--) {
+      const int64_t i = R * lane + round;
       const bool active = i < n;
       lm_nodefrag N;
-      lm_round_nodes(S, B, i, active, T, lane, N);
+      lm_round_nodes(S, P, B, i, active, T, lane, N);
       if (active) bad |= lm_row_in(row, sym0 + 256 * i);
+      if (active && round > 0) lm_prev_from(prev, sym0 + 256 * (i - 1));
+      else lm_prev_none(prev);
       for (int st = 127; st >= 0; st--) {
-        const uint32_t ctx = active ? lm_context_packed(row, st) | lm_context_packed(row, st + 128) << 16 : 0u;
+        uint32_t ctx[2] = {0u, 0u};
+        if (active) {
+          ctx[0] = lm_context_packed(row, st) | uint32_t(lm_prev_sym(prev, st)) << 16;
+          ctx[1] = lm_context_packed(row, st + 128) | uint32_t(lm_prev_sym(prev, st + 128)) << 16;
+        }
         float zA[3], zB[3];
         lm_step_logits(S, N, lane, st, ctx, zA, zB);
         lm_freq_t FA = {}, FB = {};
@@ -521,8 +557,10 @@ lm_decode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint8_t* row = lm_smem_raw + sizeof(lm_tables) + kLmWarpSmem * warp + kLmSymRow * lane;
+  uint32_t* prev = reinterpret_cast<uint32_t*>(lm_smem_raw + sizeof(lm_tables) + kLmWarpSmem * warp +
+                                               32 * kLmSymRow) + kLmPrevWords * lane;
   uint16_t* win = reinterpret_cast<uint16_t*>(lm_smem_raw + sizeof(lm_tables) + kLmWarpSmem * warp +
-                                              32 * kLmSymRow);
+                                              32 * kLmSymRow + 32 * 4 * kLmPrevWords);
   const unsigned above = lane == 31 ? 0u : ~0u << (lane + 1);
   for (int s; (s = lm_next_stream(next, order, nstreams, lane)) >= 0;) {
     const lm_block_t B = blocks[s];
@@ -548,12 +586,15 @@ lm_decode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
     uint32_t x = get32(base + 20 + 4 * lane);
     int64_t ptr = len;  // words [0, ptr) are unread
     int bad = 0;
-    const int64_t rounds = (n + 31) / 32;
-    for (int64_t round = 0; round < rounds; round++) {
-      const int64_t i = 32 * round + lane;
+    const int64_t R = (n + 31) / 32;   // the run of nodes of each lane
+    for (int64_t round = 0; round < R; round++) {
+      const int64_t i = R * lane + round;
       const bool active = i < n;
       lm_nodefrag N;
-      lm_round_nodes(S, B, i, active, T, lane, N);
+      lm_round_nodes(S, P, B, i, active, T, lane, N);
+      // the previous node of the run is the row of the last round
+      if (round > 0) lm_prev_from(prev, row);
+      else lm_prev_none(prev);
       for (int w = 0; w < 64; w++) reinterpret_cast<uint32_t*>(row)[w] = 0u;
       // the round's words are the last unread ones: stage up to kLmWordWin of them
       const int64_t wlo = ptr > kLmWordWin ? ptr - kLmWordWin : 0;
@@ -561,7 +602,11 @@ lm_decode_kernel(const uint16_t* __restrict__ P, uint64_t hash, const lm_block_t
       for (int64_t w = wlo + lane; w < ptr; w += 32) win[w - wlo] = get16(words + 2 * w);
       __syncwarp();
       for (int st = 0; st < 128; st++) {
-        const uint32_t ctx = active ? lm_context_packed(row, st) | lm_context_packed(row, st + 128) << 16 : 0u;
+        uint32_t ctx[2] = {0u, 0u};
+        if (active) {
+          ctx[0] = lm_context_packed(row, st) | uint32_t(lm_prev_sym(prev, st)) << 16;
+          ctx[1] = lm_context_packed(row, st + 128) | uint32_t(lm_prev_sym(prev, st + 128)) << 16;
+        }
         float zA[3], zB[3];
         lm_step_logits(S, N, lane, st, ctx, zA, zB);
         lm_freq_t FA = {}, FB = {};
@@ -602,11 +647,14 @@ lm_freqs_kernel(const uint16_t* __restrict__ P, const lm_block_t* __restrict__ b
     uint8_t feats[36];
     const int nf = lm_load_node(blocks[s], i, T, feats);
     float node[kLmHidden];
-    lm_node_sum(S, feats, nf, node);
+    lm_node_sum(S, P, feats, nf, node);
     int u[4];
-    lm_context_clamped(symbols + offsets[s] + 256 * i, r, u);
+    const uint8_t* sym = symbols + offsets[s] + 256 * i;
+    lm_context_clamped(sym, r, u);
+    const int64_t R = (blocks[s].nodes + 31) / 32;   // lanes' runs: the previous node is i - 1 inside a run
+    const int prev = i % R ? (sym[r - 256] & 3) : 3;
     float z[3];
-    lm_logits(S, node, r, u, z);
+    lm_logits(S, node, r, u, prev, z);
     const lm_freq_t F = lm_freqs(z);
     f[0] = F.f[0];
     f[1] = F.f[1];
@@ -633,7 +681,7 @@ __global__ void lm_choose_kernel(int nstreams, uint8_t* __restrict__ out, const 
 
 constexpr int kGradThreads = 128;
 constexpr int kW1Pad = 65;  // rows of 64 floats padded so lanes reading different rows use different banks
-constexpr int kMaxFeats = 48;  // 36 stones + 4 rotation + 8 neighbours
+constexpr int kMaxFeats = 49;  // 36 stones + 4 rotation + 8 neighbours + the previous node
 
 struct lm_grad_smem {
   float w1[kLmIn * kW1Pad];
@@ -708,6 +756,8 @@ lm_grad_kernel(const float* __restrict__ params, const lm_block_t* __restrict__ 
             const int a = lm_neighbour(r, nb);
             G.feats[tid][nf++] = uint8_t(kLmCtx + 4 * nb + (lm_before(a, r) ? (sym[a] & 3) : 3));
           }
+          const int64_t R = (blocks[s].nodes + 31) / 32;   // the coder's runs of nodes
+          G.feats[tid][nf++] = uint8_t(kLmPrev + (i % R ? (sym[r - 256] & 3) : 3));
         }
       }
     }
@@ -716,9 +766,9 @@ lm_grad_kernel(const float* __restrict__ params, const lm_block_t* __restrict__ 
     float z[3] = {0.f, 0.f, 0.f};
     if (y >= 0) {
       // h1 holds the quantized activations hq / 16 (learned.cuh): the stone
-      // rows summed in order, the last 12 (rotation and neighbour rows, on
-      // their grids) summed exactly, then added
-      const int ns = nf - 12;
+      // rows summed in order, the last 13 (rotation, neighbour and
+      // previous-node rows, on their grids) summed exactly, then added
+      const int ns = nf - 13;
       for (int k = 0; k < kLmHidden; k++) {
         float a = G.b1[k], s1 = 0.f;
         for (int f = 0; f < ns; f++) a += G.w1[G.feats[tid][f] * kW1Pad + k];
@@ -885,7 +935,7 @@ static bool check_model(const uint8_t* model, std::string& err) {
   uint32_t h[3];
   memcpy(h, model, 12);
   if (h[0] != kLmMagic || h[1] != kLmModelVersion || h[2] != uint32_t(kLmParams)) {
-    err = "not a version-2 PGLM model";
+    err = "not a version-3 PGLM model";
     return false;
   }
   // W1's rotation and neighbour rows and W2 must lie on their column grids,

@@ -5,15 +5,20 @@
 // Symbols are the on-disk ternaries of a block, 256 per node in rotation order
 // r = i0 + 4 i1 + 16 i2 + 64 i3 (shard/shard.cc:448-449).  A node's symbols are
 // coded in 128 steps; step s codes rotations s and s + 128 (i3 two apart, so
-// never neighbours).  The probability of symbol r comes from a 3-layer MLP
-// (hidden 64, bf16 weights, fp32 accumulation) over 120 binary features:
+// never neighbours).  The block's n nodes are coded by 32 lanes, lane l taking
+// the run of nodes l R .. l R + R - 1 (R = ceil(n / 32)) one after another, so
+// a node's previous node in its run is coded before it.  The probability of
+// symbol r comes from a 3-layer MLP (hidden 64, bf16 weights, fp32
+// accumulation) over 124 binary features:
 //
 //   0..71    stones of the node's board: 18 q + 2 c + colour (colour 0 black,
 //            1 white) for cell c of quadrant q;
 //   72..87   rotation: 72 + 4 q + i_q;
 //   88..119  the 8 neighbouring rotations (i_q + 1 and i_q + 3 in quadrant q,
 //            neighbour n = 2 q + (0 | 1)): 88 + 4 n + v, v = that rotation's
-//            symbol if it was coded in an earlier step, else 3.
+//            symbol if it was coded in an earlier step, else 3;
+//   120..123 the previous node of the run: 120 + v, v = its symbol of the
+//            same rotation, 3 for the first node of a run.
 //
 // Encoder and decoder must derive identical integer frequencies, so every
 // float operation on the coding path is either a separately rounded IEEE
@@ -21,22 +26,22 @@
 // which also makes the coder reproducible on the CPU:
 //
 //   node[k] = b1[k], then + W1[f][k] for each stone feature f ascending
-//   S1[k]   = sum of W1[f][k] over the 4 rotation and 8 neighbour features, exact
+//   S1[k]   = sum of W1[f][k] over the 13 rotation, neighbour and previous-node
+//             features, exact
 //   a1 = node + S1,  hq[k] = rint(min(max(a1 * 16, 0), 255))   (an integer 0..255)
 //   a2[j] = fma(C[j], 1/16, b2[j]),  C[j] = sum over k of W2[k][j] hq[k], exact
 //   z[c] = b3[c] + ((P_0 + P_1) + (P_2 + P_3)), P_t = fma chain from 0 over
 //          the columns j with (j >> 1) & 3 = t ascending of W3[j][c] relu(a2[j])
 //
 // then lm_freqs turns the logits into 15-bit frequencies (each at least 1,
-// summing to 2^15).  S1 and C are exact because a model's rotation and
-// neighbour rows of W1 and its W2 lie on grids: every column (hidden unit k of
-// W1 rows 72..119, output j of W2) is integers of magnitude at most 127 times
-// 2^-e (lm_grid_exp), so each term and partial sum is a multiple of 2^-e below
-// 2^21 2^-e and an fp32 sum in any order is exact.  The coder forms both sums
-// on the tensor cores (bf16 inputs: one-hot features and integer activations,
-// fp32 accumulation); version-2 models are checked for the grids when loaded.
-// Training may run the same network in any order; only the coder needs this
-// one.
+// summing to 2^15).  S1 and C are exact because a model's W1 rows 72..123 and
+// its W2 lie on grids: every column (hidden unit k of W1 rows 72..123, output
+// j of W2) is integers of magnitude at most 127 times 2^-e (lm_grid_exp), so
+// each term and partial sum is a multiple of 2^-e below 2^21 2^-e and an fp32
+// sum in any order is exact.  The coder forms both sums on the tensor cores
+// (bf16 inputs: one-hot features and integer activations, fp32
+// accumulation); models are checked for the grids when loaded.  Training may
+// run the same network in any order; only the coder needs this one.
 #pragma once
 #include "superscore.cuh"
 #include <cmath>
@@ -45,8 +50,8 @@
 
 namespace pg {
 
-constexpr int kLmIn = 120, kLmHidden = 64, kLmOut = 3;
-constexpr int kLmRot = 72, kLmCtx = 88;
+constexpr int kLmIn = 124, kLmHidden = 64, kLmOut = 3;
+constexpr int kLmRot = 72, kLmCtx = 88, kLmPrev = 120;
 // Parameter layout (fp32 master copy and bf16 model alike)
 constexpr int kLmW1 = 0;
 constexpr int kLmB1 = kLmW1 + kLmIn * kLmHidden;
@@ -54,10 +59,10 @@ constexpr int kLmW2 = kLmB1 + kLmHidden;
 constexpr int kLmB2 = kLmW2 + kLmHidden * kLmHidden;
 constexpr int kLmW3 = kLmB2 + kLmHidden;
 constexpr int kLmB3 = kLmW3 + kLmHidden * kLmOut;
-constexpr int kLmParams = kLmB3 + kLmOut;  // 12099
-// Serialized model: magic "PGLM", version 2, parameter count, bf16 parameters
+constexpr int kLmParams = kLmB3 + kLmOut;  // 12355
+// Serialized model: magic "PGLM", version 3, parameter count, bf16 parameters
 constexpr uint32_t kLmMagic = 0x4d4c4750u;
-constexpr uint32_t kLmModelVersion = 2;
+constexpr uint32_t kLmModelVersion = 3;
 // Activations entering layer 2: integers 0..kLmActMax, a1 scaled by kLmActScale
 constexpr float kLmActScale = 16.f, kLmActInv = 0.0625f, kLmActMax = 255.f;
 constexpr int kLmModelHeader = 12;
@@ -68,8 +73,8 @@ constexpr uint32_t kLmLower = 1u << 16;
 constexpr int kLmLanes = 32;
 constexpr uint32_t kLmVersion = 3;
 // Stream: version u32 | model hash u64 | nodes u32 | words u32 | 32 lane states u32 | words u16.
-// Node i is coded by lane i % 32; a lane codes its nodes in order, each node
-// step by step (rotation s, then s + 128).
+// Lane l codes its run of nodes l R .. l R + R - 1 in order, each node step by
+// step (rotation s, then s + 128).
 constexpr int kLmStreamHeader = 20 + 4 * kLmLanes;
 
 PG_HD float f_add(float a, float b) {

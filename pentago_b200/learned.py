@@ -26,8 +26,8 @@ import numpy as np
 
 from . import capi
 
-N_PARAMS = 12099  # W1 120x64, b1, W2 64x64, b2, W3 64x3, b3
-P_W1, P_B1, P_W2, P_B2, P_W3, P_B3 = 0, 7680, 7744, 11840, 11904, 12096
+N_PARAMS = 12355  # W1 124x64, b1, W2 64x64, b2, W3 64x3, b3
+P_W1, P_B1, P_W2, P_B2, P_W3, P_B3 = 0, 7936, 8000, 12096, 12160, 12352
 
 
 def model_bytes():
@@ -364,8 +364,8 @@ def run_slice_coding(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fractio
         "coders": {"static": "format 2: one order-0 table per block (the reference's coder)",
                    "context_table": "store coder: counted 1024-context table per chunk of blocks (the neighbouring "
                                     "rotations and the previous node's), table bytes included, no network",
-                   "learned": "format 3: the MLP over the board, the rotation and the coded neighbouring rotations, "
-                              "model shared by the slice (not counted per block)"},
+                   "learned": "format 3: the MLP over the board, the rotation, the coded neighbouring rotations and "
+                              "the previous node's symbol, model shared by the slice (not counted per block)"},
         "model_bytes": len(model),
         "blocks_kept_static": tot["static_streams"], "lossless": lossless,
         "encode_GBps_of_nodes": tot["symbols"] / 4 / (tot["enc_ms"] / 1e3) / 1e9,

@@ -85,7 +85,7 @@ def test_export_format(O):
     assert learned.model_bytes() == 12 + 2 * learned.N_PARAMS
     capi.check(capi.lib().pg_learned_export(P(params), P(model)))
     assert model[:4].tobytes() == b"PGLM"
-    assert np.frombuffer(model[4:12].tobytes(), np.uint32).tolist() == [2, learned.N_PARAMS]
+    assert np.frombuffer(model[4:12].tobytes(), np.uint32).tolist() == [3, learned.N_PARAMS]
     h = np.frombuffer(model[12:].tobytes(), np.uint16)
     # 1.00390625 = 1 + 2^-8 is a tie and rounds to even (1.0); 1 + 3 * 2^-8 rounds up
     assert h[:4].tolist() == [0x3F80, 0xC020, 0x3F80, 0x3F82]

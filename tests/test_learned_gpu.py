@@ -159,11 +159,12 @@ def test_trained_model_beats_static_and_roundtrips(cuda):
 def test_network_gain_on_held_out_blocks(cuda):
     """The same 64 held-out blocks coded three ways: format 2 (one order-0
     table per block), the store coder's counted context table (the same kind
-    of context as the network's neighbour features, counted from the blocks
-    themselves, no network) and the trained network.  Prints the three
-    figures in bits per position; the network must be at least 10% smaller
-    than format 2 and round-trip (the store coder's own round trips are
-    tested with the compressed sweeps)."""
+    of context as the network's neighbour and previous-node features, counted
+    from the blocks themselves, no network) and the trained network.  Prints
+    the three figures in bits per position; the network must be at least 10%
+    smaller than format 2, smaller than the counted table, and round-trip
+    (the store coder's own round trips are tested with the compressed
+    sweeps)."""
     import torch
     from pentago_b200 import learned
     model, _, train_blocks = trained()
@@ -184,6 +185,7 @@ def test_network_gain_on_held_out_blocks(cuda):
     print("bits per position on held-out blocks:", bits)
     assert bits["learned"] <= 0.9 * bits["static"], bits
     assert bits["context_table"] < bits["static"], bits
+    assert bits["learned"] < bits["context_table"], bits
 
 
 def test_untrained_model_falls_back_to_static(cuda):
