@@ -431,7 +431,7 @@ def sweep_summary(timings, wall_s, peak):
     line_bytes = sum(v.get("line_bytes", 0) for v in timings.values())
     sections = sum(v["sections"] for v in timings.values())
     per_slice = {str(k): {"kernel_ms": v["ms"], "sections": v["sections"], "lines_per_dim": v.get("lines"),
-                          "ctas_per_dim": v.get("ctas"),
+                          "microlines_per_dim": v.get("microlines"),
                           "line_GBps": v.get("line_bytes", 0) / (v["ms"] / 1e3) / 1e9}
                  for k, v in sorted(timings.items())}
     return {"workload": f"all sections below root {SWEEP_ROOT}, slices 35 -> 30, in HBM",

@@ -1271,14 +1271,13 @@ PG_HD void family_offsets(const family_t& F, line_dev_t& L, int start, int step)
   }
 }
 
-// Microlines per sweep CTA (a launch mixes sections of every size).
-constexpr int kSweepMicro = 4;
-
-template<int DIM, int G>
+// One CTA computes MICRO microlines of one line of a family (a launch holds
+// families whose lines take the same MICRO, line_micro).
+template<int DIM, int G, int MICRO>
 __global__ void __launch_bounds__(kLineThreads, kLineCtasPerSm)
 sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_tables_t T) {
   __shared__ __align__(16) line_dev_t L;
-  __shared__ cta_smem<kSweepMicro> S;
+  __shared__ cta_smem<MICRO> S;
   __shared__ int s_fam, s_nmicro;
   extern __shared__ uint4 dyn_smem[];
   const int tid = threadIdx.x, nt = blockDim.x;
@@ -1295,7 +1294,7 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   }
   __syncthreads();
   // CTAs past a short line's last microline leave before any set-up
-  if (int(blockIdx.y) * kSweepMicro >= s_nmicro) return;
+  if (int(blockIdx.y) * MICRO >= s_nmicro) return;
   const family_t& F = fams[s_fam];
   // copy the prototype (as 16-byte words) and fill in this line
   {
@@ -1309,19 +1308,27 @@ sweep_kernel(const family_t* __restrict__ fams, int nfams, int line0, const dev_
   family_offsets(F, L, tid, nt);
   __syncthreads();
   const int nmicro = L.cross[0] * L.cross[1] * L.cross[2];
-  const int m0 = int(blockIdx.y) * kSweepMicro;
-  cta_microlines<DIM, G, kSweepMicro>(L, S, dyn_smem, m0, min(kSweepMicro, nmicro - m0), tid, nt);
+  const int m0 = int(blockIdx.y) * MICRO;
+  cta_microlines<DIM, G, MICRO>(L, S, dyn_smem, m0, min(MICRO, nmicro - m0), tid, nt);
 }
 
 static_assert(sizeof(line_dev_t) % 16 == 0 && alignof(line_dev_t) == 16, "line_dev_t copies as uint4");
 static_assert(sizeof(family_t) % 16 == 0, "family_t array keeps proto 16-byte aligned");
 
-template<int DIM, int G> static int sweep_smem_attr() {
-  return cudaFuncSetAttribute(sweep_kernel<DIM, G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template<int DIM, int G, int MICRO> static int sweep_smem_attr() {
+  return cudaFuncSetAttribute(sweep_kernel<DIM, G, MICRO>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                               kMaxLineSmem) == cudaSuccess ? 0 : PG_ERR_CUDA;
 }
-template<int DIM, int G> static int sweep_smem_limit() {
-  return per_device_once((const void*)&sweep_smem_attr<DIM, G>, sweep_smem_attr<DIM, G>);
+template<int DIM, int G, int MICRO> static int sweep_smem_limit() {
+  return per_device_once((const void*)&sweep_smem_attr<DIM, G, MICRO>, sweep_smem_attr<DIM, G, MICRO>);
+}
+template<int DIM, int G, int MICRO>
+static int launch_sweep(const family_t* fams, int nfams, int lines, int line0, size_t smem, cudaStream_t stream,
+                        const dev_tables_t& T) {
+  if (int rc = sweep_smem_limit<DIM, G, MICRO>()) return rc;
+  sweep_kernel<DIM, G, MICRO><<<dim3(unsigned(lines), 512 / MICRO), kLineThreads, smem, stream>>>(fams, nfams, line0,
+                                                                                                   T);
+  return 0;
 }
 
 // Per-section (we-win, we-win-or-tie, total) counts over distinct positions
@@ -1465,11 +1472,12 @@ extern "C" int pg_slice_layout(const uint64_t* sigs, int n, int64_t* offsets) {
 
 // The lines of a slice, or (one_child) only those that read child_sigs[0],
 // every line then ORing into the parent slice.
-// CTAs of the sweep kernel an SM holds at this dynamic shared memory (three
-// at most, by registers): 228 KB per SM, each CTA also holding its static
-// shared memory and 1 KB the hardware reserves.
-static int sweep_ctas_per_sm(size_t dyn) {
-  const size_t per = dyn + sizeof(line_dev_t) + sizeof(cta_smem<kSweepMicro>) + 64 + 1024;
+// CTAs of the sweep kernel an SM holds at this dynamic shared memory (four at
+// most, by registers): 228 KB per SM, each CTA also holding its static shared
+// memory and 1 KB the hardware reserves.
+static int sweep_ctas_per_sm(size_t dyn, int micro) {
+  const size_t stat = micro == 8 ? sizeof(cta_smem<8>) : sizeof(cta_smem<4>);
+  const size_t per = dyn + sizeof(line_dev_t) + stat + 64 + 1024;
   return int(std::max<size_t>(1, std::min<size_t>(kLineCtasPerSm, (size_t(228) << 10) / per)));
 }
 
@@ -1507,28 +1515,32 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
     PG_CUDA(X.alloc(&recs_dev, rbytes));
     PG_CUDA(cudaMemcpyAsync(recs_dev, recs.words.data(), rbytes, cudaMemcpyHostToDevice, stream));
     for (size_t f = 0; f < fams.size(); f++) bind_line_records(fams[f].proto, recs_dev, rec_off[f]);
-    // One launch per (occupancy class, child symmetry): a launch's shared
-    // memory is sized for its largest line, so families whose lines fit three
+    // One launch per (microlines per CTA, occupancy class, child symmetry):
+    // short lines go 8 microlines to a CTA (line_micro); a launch's shared
+    // memory is sized for its largest line, so families whose lines fit more
     // CTAs on an SM do not run at the occupancy of the longest lines of the
-    // dimension, and each kernel holds only its own children's transform.
-    struct group_t { int k, g; size_t first, count; int lines, maxchild, maxpat; };
+    // dimension; and each kernel holds only its own children's transform.
+    struct group_t { int micro, k, g; size_t first, count; int lines, maxchild, maxpat; };
     std::vector<size_t> order(fams.size());
-    std::vector<int> klass(fams.size());
+    std::vector<int> klass(fams.size()), micro(fams.size());
     for (size_t f = 0; f < fams.size(); f++) {
       order[f] = f;
-      klass[f] = kLineCtasPerSm - sweep_ctas_per_sm(
-                                      line_smem_bytes(fams[f].proto.npat[0] + fams[f].proto.npat[1], fams[f].proto.nchild,
-                                                      kSweepMicro));
+      const line_dev_t& D = fams[f].proto;
+      const int pp = D.npat[0] + D.npat[1];
+      micro[f] = line_micro(D.nparent, pp, D.nchild);
+      klass[f] = kLineCtasPerSm - sweep_ctas_per_sm(line_smem_bytes(pp, D.nchild, micro[f]), micro[f]);
     }
     std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      if (micro[a] != micro[b]) return micro[a] > micro[b];
       return klass[a] != klass[b] ? klass[a] < klass[b] : fams[a].proto.g < fams[b].proto.g;
     });
     std::vector<family_t> sorted;
     std::vector<group_t> groups;
     for (size_t f : order) {
       const family_t& F = fams[f];
-      if (groups.empty() || groups.back().k != klass[f] || groups.back().g != F.proto.g)
-        groups.push_back(group_t{klass[f], F.proto.g, sorted.size(), 0, 0, 0, 0});
+      if (groups.empty() || groups.back().micro != micro[f] || groups.back().k != klass[f] ||
+          groups.back().g != F.proto.g)
+        groups.push_back(group_t{micro[f], klass[f], F.proto.g, sorted.size(), 0, 0, 0, 0});
       group_t& G = groups.back();
       sorted.push_back(F);
       sorted.back().first_line = G.lines;
@@ -1541,14 +1553,14 @@ static int sweep_lines(const uint64_t* parent_sigs, int np, uint64_t* parent_sli
     PG_CUDA(X.alloc(&d, sizeof(family_t) * sorted.size()));
     PG_CUDA(cudaMemcpyAsync(d, sorted.data(), sizeof(family_t) * sorted.size(), cudaMemcpyHostToDevice, stream));
     for (const group_t& G : groups) {
-      const size_t smem = line_smem_bytes(G.maxpat, G.maxchild, kSweepMicro);
+      const size_t smem = line_smem_bytes(G.maxpat, G.maxchild, G.micro);
       for (int line0 = 0; line0 < G.lines; line0 += 1 << 30) {
-        const dim3 grid(unsigned(std::min(G.lines - line0, 1 << 30)), 512 / kSweepMicro);
+        const int lines = std::min(G.lines - line0, 1 << 30);
         int rc = PG_ERR_ARG;
         switch (dim * 8 + G.g) {
 #define PG_CASE(D, GG) case D * 8 + GG: \
-          rc = sweep_smem_limit<D, GG>(); \
-          if (!rc) sweep_kernel<D, GG><<<grid, kLineThreads, smem, stream>>>(d + G.first, int(G.count), line0, *T); \
+          rc = G.micro == 8 ? launch_sweep<D, GG, 8>(d + G.first, int(G.count), lines, line0, smem, stream, *T) \
+                            : launch_sweep<D, GG, 4>(d + G.first, int(G.count), lines, line0, smem, stream, *T); \
           break;
           PG_FOR_DIM_G(PG_CASE)
 #undef PG_CASE

@@ -152,7 +152,8 @@ def _compressed_slice_step(root, slice_, sigs, off, child, last, checkpoint, lev
 
 def line_work(sigs, child_sigs):
     """The block lines of a slice: per quadrant dimension, the number of lines
-    and of their microline CTAs (4 microlines each), and the slice's
+    and of their microlines (1-D runs of nodes along the line; the sweep
+    kernel's CTAs take 4 or 8 of them), and the slice's
     algorithmic bytes counted per line (every line reads its child line and
     writes its parent line once, 64 bytes per node: over a slice, each
     (section, non-full dimension) pair reads its whole child section and
@@ -161,7 +162,7 @@ def line_work(sigs, child_sigs):
     if len(child_sigs):
         off = slice_layout(child_sigs)
         child_nodes = {int(c): int(off[i + 1] - off[i]) for i, c in enumerate(child_sigs)}
-    lines, ctas, nbytes = [0] * 4, [0] * 4, 0
+    lines, micro, nbytes = [0] * 4, [0] * 4, 0
     for sig in sigs:
         shape = section_shape(int(sig))
         n = int(np.prod(shape))
@@ -174,10 +175,9 @@ def line_work(sigs, child_sigs):
             lines[d] += nl
             # microlines of a line: its cross-section (8^3 unless a cross block is short)
             per_dim = [np.minimum(8, shape[i] - 8 * np.arange(blocks[i])) for i in range(4) if i != d]
-            micro = np.multiply.outer(np.multiply.outer(per_dim[0], per_dim[1]), per_dim[2])
-            ctas[d] += int(((micro + 3) // 4).sum())
+            micro[d] += int(np.multiply.outer(np.multiply.outer(per_dim[0], per_dim[1]), per_dim[2]).sum())
             nbytes += 64 * (n + child_nodes.get(c, 0))
-    return {"lines": lines, "ctas": ctas, "line_bytes": nbytes}
+    return {"lines": lines, "microlines": micro, "line_bytes": nbytes}
 
 
 def _arena_nodes(root, chain):
