@@ -29,7 +29,11 @@
 
 namespace pg {
 
-__global__ void __launch_bounds__(kMidThreads)
+// Threads of a CTA that solves one board alone (its tiles stay kMidThreads
+// set0 rows: the extra warps share the rows' items).
+constexpr int kMidBoardThreads = 512;
+
+__global__ void __launch_bounds__(kMidBoardThreads)
 mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict__ wf, int smem_workspace) {
   const mid_job_t& J = jobs[blockIdx.x];
   extern __shared__ uint4 smem[];
@@ -270,7 +274,7 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     const size_t smem = kMidThreads * sizeof(set0_info) + (smem_ws ? kSmemWorkspaceMax * 16 : 0);
     const int ncta = smem_ws ? 1 : grid_ctas_per_board(int(jobs.size()), smem);
     if (ncta <= 1) {
-      mid_board_kernel<<<unsigned(jobs.size()), kMidThreads, smem, stream>>>(d, T->win_factors, smem_ws);
+      mid_board_kernel<<<unsigned(jobs.size()), kMidBoardThreads, smem, stream>>>(d, T->win_factors, smem_ws);
       PG_CUDA(cudaGetLastError());
     } else {
       if (int rc = launch_grid_boards(d, int(jobs.size()), ncta, smem, T->win_factors, stream)) return rc;
@@ -488,7 +492,7 @@ extern "C" int pg_midsolve_batch_noalloc(const uint64_t* raws, int n, pg_mid_val
     PG_CUDA(cudaMemcpyAsync(d, jobs.data(), sizeof(mid_job_t) * jobs.size(), cudaMemcpyHostToDevice, stream));
     const int smem_ws = pass == 0;
     const size_t smem = kMidThreads * sizeof(set0_info) + (smem_ws ? kSmemWorkspaceMax * 16 : 0);
-    mid_board_kernel<<<unsigned(jobs.size()), kMidThreads, smem, stream>>>(d, D.win_factors, smem_ws);
+    mid_board_kernel<<<unsigned(jobs.size()), kMidBoardThreads, smem, stream>>>(d, D.win_factors, smem_ws);
     PG_CUDA(cudaGetLastError());
   }
   return PG_OK;
