@@ -1,4 +1,5 @@
-// The drop-ins of INTEGRATION.md sections 1 and 2, compiled against the
+// The drop-ins a reference maintainer would add for the end engine's lines and
+// for midsolve, compiled against the
 // reference's own headers and run beside the reference's functions on the
 // same buffers.  Test infrastructure: built by `make -C oracle dropin` from
 // this file, the reference objects oracle/Makefile already compiles, and the
@@ -30,7 +31,7 @@
 using namespace pentago;
 using namespace pentago::end;
 
-// the line's own buffers, on the device.
+// schedule_compute_line's drop-in: the line's own buffers, on the device.
 static int gpu_schedule_compute_line(line_details_t& line, const void* input_dev, void* output_dev,
                                      cudaStream_t stream) {
   pg_line_t l;
@@ -47,7 +48,7 @@ static int gpu_schedule_compute_line(line_details_t& line, const void* input_dev
   return pg_end_compute_lines(&l, 1, stream);
 }
 
-// mid_values_t from the GPU midsolve.
+// midsolve's drop-in: mid_values_t from the GPU midsolve.
 static mid_values_t gpu_midsolve(const high_board_t board) {
   static pg_mid_values_t* out = nullptr;
   if (!out && cudaMallocManaged(&out, sizeof(pg_mid_values_t)) != cudaSuccess) throw std::runtime_error("alloc");
