@@ -240,6 +240,7 @@ def cpu_reference_rate(seconds=12.0, threads=0, passes=None, warmup=0, blocks=16
         el = time.perf_counter() - t0
         if (passes is not None and done >= passes) or (passes is None and el >= seconds):
             break
+    R.release_threads()   # its idle workers spin; nothing after this timing should share the host with them
     return {"value": nodes * 256 / el, "unit": UNIT, "cores": nthreads, "kind": "reference", "passes": done,
             "ms_per_pass": 1e3 * el / done,
             "sample": f"the {len(work)} block lines of the GPU step (4 through each of {blocks} blocks of section "
@@ -276,6 +277,7 @@ def check_against_reference(lines, blocks, rank, per_dim=None):
             bad.append({"dim": d, "block_base": list(line.block_base),
                         "got_sha1": hashlib.sha1(got.tobytes()).hexdigest()[:16],
                         "want_sha1": hashlib.sha1(want.tobytes()).hexdigest()[:16]})
+    C.release_threads()
     return {"ok": not bad, "lines_checked": checked, "checker": checker, "mismatches": bad[:4]}
 
 
@@ -489,6 +491,7 @@ def cpu_sweep_estimate(root_counts, timings, seconds_per_slice=1.5):
         rate = nodes / (time.perf_counter() - t0)
         per_slice[str(slice_)] = {"line_nodes": work, "nodes_per_s": rate}
         total_s += work / rate
+    R.release_threads()
     return {"estimated_s": total_s, "cores": nthreads, "kind": "reference", "per_slice": per_slice,
             "sample": "per slice, the block lines through the first block of its largest section on "
                       f"{nthreads} threads, {seconds_per_slice} s each, charged for every line of the sweep"}

@@ -64,14 +64,18 @@ void store_super(uint64_t* p, const super_t s) {
     if (s(uint8_t(r))) p[r >> 6] |= uint64_t(1) << (r & 63);
 }
 
-std::once_flag threads_once;
+// The reference's thread pool (init_threads) runs its idle workers in a busy
+// wait, so it is started when a call needs it and released by the caller when
+// it has finished timing, before anything else runs on the host.
+std::mutex threads_mutex;
 int pool_threads = 0;
 
 void ensure_threads(int n) {
-  std::call_once(threads_once, [n]() {
+  std::lock_guard<std::mutex> lock(threads_mutex);
+  if (!pool_threads) {
     pool_threads = n > 0 ? n : default_threads();
     init_threads(pool_threads, 0);
-  });
+  }
 }
 
 }  // namespace
@@ -81,6 +85,17 @@ extern "C" {
 int ref_threads(int n) {
   ensure_threads(n);
   return pool_threads;
+}
+
+// Stop the thread pool (its workers spin while idle); a later call that
+// needs it starts it again.
+int ref_release_threads(void) {
+  std::lock_guard<std::mutex> lock(threads_mutex);
+  if (pool_threads) {
+    shutdown_threads();
+    pool_threads = 0;
+  }
+  return 0;
 }
 
 const void* ref_table(const char* name, int* bytes) {

@@ -67,8 +67,16 @@ class Checker:
         if prefix == "or_":
             self.lib.or_init()
         else:
+            # the reference's thread pool starts when a call needs it; its idle
+            # workers spin, so callers release it when they are done
             self.lib.ref_threads.restype = _i
-            self.lib.ref_threads(0)
+            self.lib.ref_release_threads.restype = _i
+
+    def release_threads(self):
+        """Stop the reference's thread pool (no-op for the C restatement)."""
+        f = getattr(self.lib, "ref_release_threads", None)
+        if f is not None:
+            f()
 
     def get_table(self, name, dtype):
         import numpy as np
