@@ -201,7 +201,8 @@ int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* s
  *     About 64 boards of 26+ stones, or one board of 22 stones, fit;
  *   - every board is solved by one CTA; pg_midsolve_batch spreads boards
  *     with more than 10 empty spots (25 stones or fewer) over many CTAs, so
- *     such boards take far longer here;
+ *     such boards take far longer here, and runs the two passes of a smaller
+ *     board on two CTAs;
  *   - each call copies its boards' job descriptors from host memory to the
  *     fixed array with cudaMemcpyAsync on the given stream;
  *   - the first call on a device sets that device up (it resolves the arrays'

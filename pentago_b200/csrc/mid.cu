@@ -8,16 +8,16 @@
 // ping-pongs between the two ends of one buffer (mid/internal.h:29-69,
 // :358-408).
 //
-// Here one CTA owns one board.  It precomputes the per-level tables
-// (midengine.cc:57-76), then runs both passes with a CTA barrier between
-// levels.  Inside a level the (s0, s1p) items are split over the CTA's
-// threads in tiles of s0 rows whose per-row data (make_set0_info,
+// Here a CTA runs whole passes of one board.  It precomputes the per-level
+// tables (midengine.cc:57-76), then runs its passes with a CTA barrier
+// between levels.  Inside a level the (s0, s1p) items are split over the
+// CTA's threads in tiles of s0 rows whose per-row data (make_set0_info,
 // internal.h:174-259) is built cooperatively in shared memory.  Boards with
 // up to 10 empty spots (26 or more stones) keep their whole workspace in
-// shared memory (bottleneck(10) = 8400 halfsupers = 134 KB); larger boards
-// use a global-memory workspace.  The last step, midsolve_traverse
-// (midengine.cc:127-158), also runs on the device and writes the reference's
-// mid_values_t records.
+// shared memory (bottleneck(10) = 8400 halfsupers = 134 KB): in a batch, one
+// CTA per pass (mid_pass_kernel); larger boards use a global-memory
+// workspace.  The last step, midsolve_traverse (midengine.cc:127-158), also
+// runs on the device and writes the reference's mid_values_t records.
 #include "mid_body.cuh"
 #include "runtime.h"
 #include <atomic>
@@ -45,6 +45,58 @@ mid_board_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict_
   __syncthreads();
   const mid_tables MT = {c_choose, c_winpat, wf};
   mid_board_body(J, MT, tiles, ws, raw, &fault, threadIdx.x, blockDim.x, 0, 1, sync_threads(), sync_threads());
+}
+
+// Where the two pass CTAs of one board meet: each publishes the n <= 1
+// results of its pass (raw[pass][0..spots]) and its bounds-check fault, then
+// counts itself done; zero at launch.
+struct pass_meet {
+  uint4 raw[2][19];
+  unsigned done;
+  int fault;
+  int pad[2];
+};
+
+// The boards of pg_midsolve_batch whose workspace fits shared memory: two
+// CTAs per board, CTA 2b + p running pass p (aggressive = p) of board b over
+// its own copy of the per-level tables (jobs[2b + p]).  The passes share no
+// workspace, so neither CTA waits for the other: the one that finishes second
+// (an atomic count, no spinning) gathers both passes' results and runs the
+// traversal.  A 64-board batch thus spreads over 128 SMs instead of 64.
+__global__ void __launch_bounds__(kMidBoardThreads)
+mid_pass_kernel(const mid_job_t* __restrict__ jobs, const uint32_t* __restrict__ wf, pass_meet* meet) {
+  const int board = blockIdx.x >> 1, pass = blockIdx.x & 1;
+  const mid_job_t& J = jobs[blockIdx.x];
+  extern __shared__ uint4 smem[];
+  set0_info* tiles = reinterpret_cast<set0_info*>(smem);  // kMidThreads entries
+  uint4* ws = smem + kMidThreads * sizeof(set0_info) / sizeof(uint4);
+  __shared__ uint4 raw[2][19];
+  __shared__ int fault, last;
+  if (threadIdx.x == 0) fault = 0;
+  __syncthreads();
+  const mid_tables MT = {c_choose, c_winpat, wf};
+  mid_board_body(J, MT, tiles, ws, raw, &fault, threadIdx.x, blockDim.x, 0, 1, sync_threads(), sync_threads(),
+                 nullptr, pass, pass + 1, false);
+  pass_meet& M = meet[board];
+  if (threadIdx.x < 19) M.raw[pass][threadIdx.x] = raw[pass][threadIdx.x];
+  if (threadIdx.x == 0 && fault) atomicExch(&M.fault, 1);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&M.done, 1u) == 1u;
+  __syncthreads();
+  if (!last || threadIdx.x >= 32) return;
+  __threadfence();
+  if (atomicAdd(&M.fault, 0)) {
+    if (threadIdx.x == 0) { J.out->size = -1; J.out->pad = 0; }
+    return;
+  }
+  // Interleave (midengine.cc:119-124) and traverse on the first warp
+  uint4 supers[2 * 19];
+  for (int i = 0; i < 19; i++)
+    for (int j = 0; j < 2; j++) supers[2 * i + j] = __ldcg(&M.raw[j ^ (i == 0)][i]);
+#ifdef __CUDA_ARCH__
+  traverse_warp(J, MT, supers, J.out, int(threadIdx.x));
+#endif
 }
 
 // One CTA waiting twice at a barrier of two that the other never reaches:
@@ -151,8 +203,11 @@ bool plan_board(uint64_t raw, board_plan& P, std::string& err) {
 }
 
 static int mid_kernel_attrs() {
-  return cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16)) == cudaSuccess &&
+  const int smem_ws = int(kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16);
+  return cudaFuncSetAttribute(mid_board_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_ws) ==
+                     cudaSuccess &&
+                 cudaFuncSetAttribute(mid_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_ws) ==
+                     cudaSuccess &&
                  cudaFuncSetAttribute(mid_board_grid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(kMidThreads * sizeof(set0_info))) == cudaSuccess
              ? 0 : PG_ERR_CUDA;
@@ -208,6 +263,13 @@ void carve_scratch(board_plan& P, char* base, bool global_ws) {
   J.workspace = global_ws || P.workspace > size_t(kSmemWorkspaceMax) ? (uint4*)(base + off) : nullptr;
 }
 
+// pg_midsolve_batch's scratch: the pass_meet records of the shared-memory
+// boards, then per board its tables (twice for a shared-memory board: one
+// copy per pass CTA) and, for a larger board, its global workspace.
+static bool smem_board(const board_plan& P) { return P.workspace <= size_t(kSmemWorkspaceMax); }
+static size_t batch_bytes_of(const board_plan& P) { return (smem_board(P) ? 2 : 1) * scratch_bytes_of(P); }
+static size_t meet_bytes(int nsmall) { return align256(sizeof(pass_meet) * size_t(nsmall)); }
+
 }  // namespace pg
 
 using namespace pg;
@@ -220,12 +282,14 @@ extern "C" int pg_midsolve_workspace_size(int stones) {
 extern "C" int pg_midsolve_scratch_bytes(const uint64_t* raws, int n, int64_t* bytes) {
   std::string err;
   size_t total = 0;
+  int nsmall = 0;
   for (int i = 0; i < n; i++) {
     board_plan P;
     if (!plan_board(raws[i], P, err)) return fail(PG_ERR_ARG, err);
-    total += scratch_bytes_of(P);
+    total += batch_bytes_of(P);
+    nsmall += smem_board(P);
   }
-  *bytes = int64_t(total);
+  *bytes = int64_t(total + meet_bytes(nsmall));
   return PG_OK;
 }
 
@@ -243,10 +307,13 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
   std::string err;
   std::vector<board_plan> plans(n);
   size_t total = 0;
+  int nsmall = 0;
   for (int i = 0; i < n; i++) {
     if (!plan_board(raws[i], plans[i], err)) return fail(PG_ERR_ARG, "board " + std::to_string(i) + ": " + err);
-    total += scratch_bytes_of(plans[i]);
+    total += batch_bytes_of(plans[i]);
+    nsmall += smem_board(plans[i]);
   }
+  total += meet_bytes(nsmall);
   stream_scratch X(stream);
   char* base = (char*)scratch;
   if (!base) {
@@ -254,27 +321,36 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
   } else if (size_t(scratch_bytes) < total) {
     return fail(PG_ERR_CAPACITY, "midsolve scratch too small");
   }
-  size_t off = 0;
-  std::vector<mid_job_t> small, large;
+  pass_meet* meets = reinterpret_cast<pass_meet*>(base);
+  size_t off = meet_bytes(nsmall);
+  std::vector<mid_job_t> small, large;  // small: two jobs per board, one per pass
   for (int i = 0; i < n; i++) {
     auto& P = plans[i];
-    carve_scratch(P, base + off);
-    off += scratch_bytes_of(P);
-    mid_job_t& J = P.job;
-    J.out = out + i;
-    (P.workspace > size_t(kSmemWorkspaceMax) ? large : small).push_back(J);
+    P.job.out = out + i;
+    const size_t bytes = scratch_bytes_of(P);
+    for (int copy = 0; copy < (smem_board(P) ? 2 : 1); copy++) {
+      carve_scratch(P, base + off);
+      off += bytes;
+      (smem_board(P) ? small : large).push_back(P.job);
+    }
   }
+  if (nsmall) PG_CUDA(cudaMemsetAsync(meets, 0, sizeof(pass_meet) * size_t(nsmall), stream));
   for (int pass = 0; pass < 2; pass++) {
     auto& jobs = pass ? large : small;
     if (jobs.empty()) continue;
     mid_job_t* d = nullptr;
     PG_CUDA(X.alloc(&d, sizeof(mid_job_t) * jobs.size()));
     PG_CUDA(cudaMemcpyAsync(d, jobs.data(), sizeof(mid_job_t) * jobs.size(), cudaMemcpyHostToDevice, stream));
-    const int smem_ws = pass == 0;
-    const size_t smem = kMidThreads * sizeof(set0_info) + (smem_ws ? kSmemWorkspaceMax * 16 : 0);
-    const int ncta = smem_ws ? 1 : grid_ctas_per_board(int(jobs.size()), smem);
+    if (pass == 0) {
+      const size_t smem = kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16;
+      mid_pass_kernel<<<unsigned(jobs.size()), kMidBoardThreads, smem, stream>>>(d, T->win_factors, meets);
+      PG_CUDA(cudaGetLastError());
+      continue;
+    }
+    const size_t smem = kMidThreads * sizeof(set0_info);
+    const int ncta = grid_ctas_per_board(int(jobs.size()), smem);
     if (ncta <= 1) {
-      mid_board_kernel<<<unsigned(jobs.size()), kMidBoardThreads, smem, stream>>>(d, T->win_factors, smem_ws);
+      mid_board_kernel<<<unsigned(jobs.size()), kMidBoardThreads, smem, stream>>>(d, T->win_factors, 0);
       PG_CUDA(cudaGetLastError());
     } else {
       if (int rc = launch_grid_boards(d, int(jobs.size()), ncta, smem, T->win_factors, stream)) return rc;
@@ -393,8 +469,8 @@ extern "C" int pg_selftest_midsolve_groups_host(const uint64_t* raws, int n, int
 // Some callers cannot allocate device memory at the moment they want a
 // solve: code inside a framework whose memory pool owns the whole device, or
 // a real-time loop that must not pay for, or fail in, an allocation.
-// pg_midsolve_batch_noalloc serves them with the board kernel of
-// pg_midsolve_batch (one CTA per board), but every byte of device scratch it
+// pg_midsolve_batch_noalloc serves them with the one-CTA-per-board kernel
+// (mid_board_kernel, both passes in one CTA), and every byte of device scratch it
 // uses (the boards' job descriptors, their per-level tables and, for boards
 // with more than 10 empty spots, their workspace) lives in one fixed array
 // that is part of the library image, plus a fixed copy of the win-pattern

@@ -363,10 +363,14 @@ __device__ void traverse_warp(const mid_job_t& J, const mid_tables& MT, const ui
 // the next level only after the all-group barrier.  Run with one group of one
 // thread and no-op barriers it is the same computation done sequentially
 // (used by the CPU self-test).  `raw` and `fault` are shared by the groups.
+// Passes [pass0, pass1) are run (the two passes share nothing but the
+// per-level tables); `finish` = false stops after them, leaving the records
+// to a caller that gathers both passes' raw results.
 template<class Barrier, class GridBarrier>
 PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* tiles, uint4* ws,
                           uint4 (*raw)[19], int* fault, int tid, int nt, int cta, int ncta, Barrier barrier,
-                          GridBarrier gbarrier, uint4* dump = nullptr) {
+                          GridBarrier gbarrier, uint4* dump = nullptr, int pass0 = 0, int pass1 = 2,
+                          bool finish = true) {
   const int spots = J.spots;
   const int gtid = cta * nt + tid, gnt = ncta * nt;
   // Per-level tables, the same for both passes (midengine.cc:57-76, :101-107)
@@ -401,7 +405,7 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
   }
   gbarrier();
 
-  for (int aggressive = 0; aggressive < 2; aggressive++) {
+  for (int aggressive = pass0; aggressive < pass1; aggressive++) {
     for (int n = spots; n >= 0; n--) {
       const level_t L = make_level(J, MT, n);
       const mid_grab gi = J.spaces[n + 1], go = J.spaces[n];
@@ -430,6 +434,7 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
     }
   }
 
+  if (!finish) return;
   // Interleave (midengine.cc:119-124) and traverse; a failed bounds check
   // marks the record with size -1 instead.
   if (gtid == 0 && *fault) { J.out->size = -1; J.out->pad = 0; }

@@ -235,7 +235,7 @@ def bench_boards_26(steps=50, warmup=3, sm_max_mhz=1965.0, trials=5):
                            "frac": alg / (ms / 1e3) / 1e9 / peak,
                            "peak_kind": f"nominal: 128 B per clock per SM x {sms} SMs x {sm_max_mhz:.0f} MHz",
                            "algorithmic_bytes_per_batch": alg,
-                           "note": "one CTA per board: 64 boards occupy 64 SMs"},
+                           "note": "one CTA per pass of a board: 64 boards occupy 128 SMs"},
               "e2e": {"value": pos / (e2e_ms / 1e3), "unit": "positions/s", "ms_per_batch": e2e_ms,
                       "h2d_bytes_per_step": 8 * len(raws), "d2h_bytes_per_step": RECORD_BYTES * len(raws)}}
     return result, raws
