@@ -42,6 +42,8 @@ struct mid_job_t {
   int32_t pad2;
 };
 
+static_assert(sizeof(mid_job_t) % 16 == 0, "mid_job_t is copied in 16-byte words");
+
 struct set0_info {  // make_set0_info (mid/internal.h:174-259); 256 bytes
   uint4 wins0;
   uint16_t child_s0s[18];

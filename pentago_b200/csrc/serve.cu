@@ -10,6 +10,13 @@
 // arena has room for the board's scratch (its HBM budget), so work that
 // arrives while others are on the GPU joins them as soon as resources free up.
 //
+// Idle workers poll a mirror of the ring's tail in device memory; one idle
+// worker at a time (a device lock) refreshes the mirror from host memory, so
+// at most one read crosses the bus while the pool waits.  (With every idle
+// worker reading the host's tail itself, hundreds of reads in flight over
+// the bus slowed every memory fence and host-memory load on the device by
+// two orders of magnitude: a gang barrier took about 0.6 ms.)
+//
 // Every wait is bounded: an idle worker polls with nanosleep back-off and
 // leaves after 2 s without work, by the GPU's global timer and a cap on polls
 // (status kIdleExit), so a host that stops talking cannot hold the GPU; the
@@ -56,13 +63,24 @@ struct gang_aux {
   uint4 raw[2][19];
 };
 
-// Workers per request: boards with many empty spots are split over several
-// workers so that they finish in tens of milliseconds instead of seconds
-// (shares of the worker pool: 18 empty spots get 3/8 of it, each spot fewer
-// halves that, down to one worker).
-static int gang_size(int spots, int workers) {
-  if (spots < 12) return 1;
-  const int g = int((int64_t(workers) * 3 / 8) >> (18 - std::min(spots, 18)));
+// Workers per request.  The floor is the share a request gets under
+// overload: boards with many empty spots are split over several workers so
+// that they finish in tens of milliseconds instead of seconds (18 empty spots
+// get 3/8 of the pool, each spot fewer halves that, down to one worker).
+// When workers are idle at admission a request takes up to half of them, so
+// that at moderate load a board finishes in a fraction of the time, but no
+// more than keeps every member busy: a pass has about 17,300 (s0, s1p) items
+// at 10 empty spots and 2.9x as many per spot more, and a member gets at
+// least half of that.  Any gang of at most half the pool makes progress: the
+// gang's entries are consecutive in the ring and claimed in order, so a
+// member only waits for workers that are finishing earlier requests.
+static int gang_size(int spots, int workers, int idle) {
+  int g = spots < 12 ? 1 : int((int64_t(workers) * 3 / 8) >> (18 - std::min(spots, 18)));
+  double items = 17303;
+  for (int s = 10; s < spots; s++) items *= 2.87;
+  for (int s = 10; s > spots; s--) items /= 2.87;
+  const int useful = std::max(1, int(items / (17303 / 2)));
+  g = std::max(g, std::min(useful, idle / 2));
   return std::max(1, std::min(g, workers / 2));
 }
 
@@ -72,14 +90,23 @@ struct serve_ctl {            // host-mapped
   volatile int32_t status;            // kRunning / kIdleExit / kClosed
 };
 
+struct serve_dev {            // device memory
+  unsigned long long head;    // entries claimed by workers
+  unsigned long long tail;    // mirror of serve_ctl::tail (never ahead of it)
+  int close;                  // mirror of serve_ctl::close; zeroed at each launch
+  int lock;                   // held by the idle worker refreshing the mirror
+};
+
 __global__ void __launch_bounds__(kMidThreads, 2)
-serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_aux* aux,
+serve_kernel(serve_entry* ring, serve_ctl* ctl, serve_dev* dev, gang_aux* aux,
              const uint32_t* __restrict__ wf) {
   extern __shared__ uint4 smem[];
   set0_info* tiles = reinterpret_cast<set0_info*>(smem);
   __shared__ uint4 raw[2][19];
   __shared__ int fault;
   __shared__ long long claimed;
+  __shared__ mid_job_t job;
+  __shared__ int gang_s, rank_s, first_s;
   const mid_tables MT = {c_choose, c_winpat, wf};
   for (;;) {
     if (threadIdx.x == 0) {
@@ -88,13 +115,21 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_a
       const unsigned long long idle_since = global_ns();
       unsigned sleep_ns = 256;
       for (;;) {
-        const unsigned long long h = atomicAdd(head, 0ull);
-        const unsigned long long t = ctl->tail;
+        const unsigned long long h = atomicAdd(&dev->head, 0ull);
+        const unsigned long long t = atomicAdd(&dev->tail, 0ull);
         if (h < t) {
-          if (atomicCAS(head, h, h + 1) == h) { claimed = (long long)h; __threadfence_system(); break; }
+          if (atomicCAS(&dev->head, h, h + 1) == h) { claimed = (long long)h; __threadfence_system(); break; }
           continue;
         }
-        if (ctl->close) { ctl->status = kClosed; break; }
+        if (atomicAdd(&dev->close, 0)) { ctl->status = kClosed; break; }
+        if (atomicCAS(&dev->lock, 0, 1) == 0) {
+          const unsigned long long ht = ctl->tail;
+          const int hc = ctl->close;
+          atomicMax(&dev->tail, ht);
+          if (hc) atomicExch(&dev->close, 1);
+          atomicExch(&dev->lock, 0);
+          if (ht > t || hc) continue;
+        }
         if (++polls > kIdlePollsMax || global_ns() - idle_since > kIdleNs) { ctl->status = kIdleExit; break; }
         __nanosleep(sleep_ns);
         if (sleep_ns < 20000) sleep_ns *= 2;
@@ -105,8 +140,18 @@ serve_kernel(serve_entry* ring, serve_ctl* ctl, unsigned long long* head, gang_a
     if (claimed < 0) return;
     serve_entry& E = ring[claimed % kRing];
     __threadfence_system();
-    mid_job_t J = E.job;
-    const int gang = E.gang, rank = E.rank, first = E.first;
+    // The entry is in host memory: its descriptor crosses the bus once, into
+    // shared memory, and every thread reads it there (uncached loads, since
+    // ring entries are reused).
+    {
+      const uint4* src = reinterpret_cast<const uint4*>(&E.job);
+      uint4* dst = reinterpret_cast<uint4*>(&job);
+      for (int i = int(threadIdx.x); i < int(sizeof(mid_job_t) / 16); i += int(blockDim.x)) dst[i] = __ldcv(src + i);
+      if (threadIdx.x == 0) { gang_s = __ldcv(&E.gang); rank_s = __ldcv(&E.rank); first_s = __ldcv(&E.first); }
+    }
+    __syncthreads();
+    const mid_job_t& J = job;
+    const int gang = gang_s, rank = rank_s, first = first_s;
     if (gang <= 1) {
       mid_board_body(J, MT, tiles, J.workspace, raw, &fault, int(threadIdx.x), int(blockDim.x), 0, 1,
                      sync_threads(), sync_threads());
@@ -170,10 +215,11 @@ struct server {
   serve_entry* ring = nullptr;        // mapped
   serve_ctl* ctl = nullptr;           // mapped
   pg_mid_values_t* results = nullptr; // mapped, one per ring entry
-  unsigned long long* head = nullptr; // device claim counter
+  serve_dev* dev = nullptr;           // device claim counter and tail mirror
   gang_aux* aux = nullptr;            // device, one per ring slot
   arena A;
   unsigned long long next = 0;        // next ticket (ring entry)
+  int busy = 0;                       // workers in the gangs of unpolled requests
   struct inflight { size_t off, bytes; int gang; bool live; };
   std::vector<inflight> slots;        // per ring entry
   bool launched = false;
@@ -186,7 +232,8 @@ static int launch_workers(server& S) {
   S.ctl->close = 0;
   S.ctl->status = kRunning;
   const size_t smem = kMidThreads * sizeof(set0_info);
-  serve_kernel<<<S.workers, kMidThreads, smem, S.stream>>>(S.ring, S.ctl, S.head, S.aux, T->win_factors);
+  PG_CUDA(cudaMemsetAsync(&S.dev->close, 0, sizeof(int), S.stream));
+  serve_kernel<<<S.workers, kMidThreads, smem, S.stream>>>(S.ring, S.ctl, S.dev, S.aux, T->win_factors);
   PG_CUDA(cudaGetLastError());
   S.launched = true;
   return PG_OK;
@@ -220,8 +267,8 @@ extern "C" int pg_serve_open(int64_t budget_bytes, pg_server_t* out) {
   PG_CUDA(cudaMalloc(&base, size_t(budget_bytes)));
   S->A.init(base, size_t(budget_bytes));
   S->slots.assign(kRing, server::inflight{0, 0, 1, false});
-  PG_CUDA(cudaMalloc(&S->head, sizeof(unsigned long long)));
-  PG_CUDA(cudaMemset(S->head, 0, sizeof(unsigned long long)));
+  PG_CUDA(cudaMalloc(&S->dev, sizeof(serve_dev)));
+  PG_CUDA(cudaMemset(S->dev, 0, sizeof(serve_dev)));
   PG_CUDA(cudaMalloc(&S->aux, sizeof(gang_aux) * kRing));
   PG_CUDA(cudaMemset(S->aux, 0, sizeof(gang_aux) * kRing));
   *out = reinterpret_cast<pg_server_t>(S);
@@ -239,7 +286,7 @@ extern "C" int64_t pg_serve_submit(pg_server_t h, uint64_t raw) {
   if (!plan_board(raw, P, err)) return fail(PG_ERR_ARG, err);
   const unsigned long long ticket = S.next;
   const int slot = int(ticket % kRing);
-  const int gang = gang_size(P.job.spots, S.workers);
+  const int gang = gang_size(P.job.spots, S.workers, std::max(0, S.workers - S.busy));
   for (int g = 0; g < gang; g++)
     if (S.slots[(slot + g) % kRing].live) return fail(PG_ERR_CAPACITY, "request ring full");
   const size_t bytes = scratch_bytes_of(P, true);
@@ -256,6 +303,7 @@ extern "C" int64_t pg_serve_submit(pg_server_t h, uint64_t raw) {
     E.first = slot;
     S.slots[(slot + g) % kRing] = server::inflight{off, bytes, gang, true};
   }
+  S.busy += gang;
   std::atomic_thread_fence(std::memory_order_seq_cst);
   S.next = ticket + gang;
   S.ctl->tail = ticket + gang;
@@ -280,6 +328,7 @@ extern "C" int pg_serve_poll(pg_server_t h, int64_t ticket, pg_mid_values_t* res
   S.A.release(S.slots[slot].off, S.slots[slot].bytes);
   const int gang = S.slots[slot].gang;
   for (int g = 0; g < gang; g++) S.slots[(slot + g) % kRing].live = false;
+  S.busy -= gang;
   return done > 0 ? 1 : fail(PG_ERR_BOUNDS, "midsolve bounds check failed");
 }
 
@@ -297,7 +346,7 @@ extern "C" int pg_serve_close(pg_server_t h) {
   std::atomic_thread_fence(std::memory_order_seq_cst);
   cudaError_t e = cudaStreamSynchronize(S->stream);
   cudaFree(S->A.base);
-  cudaFree(S->head);
+  cudaFree(S->dev);
   cudaFree(S->aux);
   cudaFreeHost((void*)S->ring);
   cudaFreeHost((void*)S->ctl);
