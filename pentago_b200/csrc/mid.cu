@@ -264,11 +264,17 @@ void carve_scratch(board_plan& P, char* base, bool global_ws) {
 }
 
 // pg_midsolve_batch's scratch: the pass_meet records of the shared-memory
-// boards, then per board its tables (twice for a shared-memory board: one
-// copy per pass CTA) and, for a larger board, its global workspace.
+// boards, the job descriptors (two per shared-memory board, one per pass
+// CTA, then one per larger board), then per board its tables (twice for a
+// shared-memory board: one copy per pass CTA) and, for a larger board, its
+// global workspace.  With the caller's scratch, nothing is allocated.
 static bool smem_board(const board_plan& P) { return P.workspace <= size_t(kSmemWorkspaceMax); }
 static size_t batch_bytes_of(const board_plan& P) { return (smem_board(P) ? 2 : 1) * scratch_bytes_of(P); }
 static size_t meet_bytes(int nsmall) { return align256(sizeof(pass_meet) * size_t(nsmall)); }
+static size_t small_jobs_bytes(int nsmall) { return align256(sizeof(mid_job_t) * 2 * size_t(nsmall)); }
+static size_t jobs_bytes(int nsmall, int nlarge) {
+  return small_jobs_bytes(nsmall) + align256(sizeof(mid_job_t) * size_t(nlarge));
+}
 
 }  // namespace pg
 
@@ -289,7 +295,7 @@ extern "C" int pg_midsolve_scratch_bytes(const uint64_t* raws, int n, int64_t* b
     total += batch_bytes_of(P);
     nsmall += smem_board(P);
   }
-  *bytes = int64_t(total + meet_bytes(nsmall));
+  *bytes = int64_t(total + meet_bytes(nsmall) + jobs_bytes(nsmall, n - nsmall));
   return PG_OK;
 }
 
@@ -313,7 +319,9 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     total += batch_bytes_of(plans[i]);
     nsmall += smem_board(plans[i]);
   }
-  total += meet_bytes(nsmall);
+  const int nlarge = n - nsmall;
+  const size_t head = meet_bytes(nsmall), jbytes = jobs_bytes(nsmall, nlarge);
+  total += head + jbytes;
   stream_scratch X(stream);
   char* base = (char*)scratch;
   if (!base) {
@@ -322,38 +330,41 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
     return fail(PG_ERR_CAPACITY, "midsolve scratch too small");
   }
   pass_meet* meets = reinterpret_cast<pass_meet*>(base);
-  size_t off = meet_bytes(nsmall);
-  std::vector<mid_job_t> small, large;  // small: two jobs per board, one per pass
-  for (int i = 0; i < n; i++) {
+  // The job descriptors in the layout they take on the device, copied in one
+  // piece: small boards' pass jobs (board b at 2b, 2b + 1), then large boards.
+  std::vector<char> host_jobs(jbytes);
+  mid_job_t* small = reinterpret_cast<mid_job_t*>(host_jobs.data());
+  mid_job_t* large = reinterpret_cast<mid_job_t*>(host_jobs.data() + small_jobs_bytes(nsmall));
+  size_t off = head + jbytes;
+  for (int i = 0, ns = 0, nl = 0; i < n; i++) {
     auto& P = plans[i];
     P.job.out = out + i;
     const size_t bytes = scratch_bytes_of(P);
     for (int copy = 0; copy < (smem_board(P) ? 2 : 1); copy++) {
       carve_scratch(P, base + off);
       off += bytes;
-      (smem_board(P) ? small : large).push_back(P.job);
+      if (smem_board(P)) small[ns++] = P.job;
+      else large[nl++] = P.job;
     }
   }
-  if (nsmall) PG_CUDA(cudaMemsetAsync(meets, 0, sizeof(pass_meet) * size_t(nsmall), stream));
-  for (int pass = 0; pass < 2; pass++) {
-    auto& jobs = pass ? large : small;
-    if (jobs.empty()) continue;
-    mid_job_t* d = nullptr;
-    PG_CUDA(X.alloc(&d, sizeof(mid_job_t) * jobs.size()));
-    PG_CUDA(cudaMemcpyAsync(d, jobs.data(), sizeof(mid_job_t) * jobs.size(), cudaMemcpyHostToDevice, stream));
-    if (pass == 0) {
-      const size_t smem = kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16;
-      mid_pass_kernel<<<unsigned(jobs.size()), kMidBoardThreads, smem, stream>>>(d, T->win_factors, meets);
-      PG_CUDA(cudaGetLastError());
-      continue;
-    }
+  char* djobs = base + head;
+  PG_CUDA(cudaMemcpyAsync(djobs, host_jobs.data(), jbytes, cudaMemcpyHostToDevice, stream));
+  if (nsmall) {
+    PG_CUDA(cudaMemsetAsync(meets, 0, sizeof(pass_meet) * size_t(nsmall), stream));
+    const size_t smem = kMidThreads * sizeof(set0_info) + kSmemWorkspaceMax * 16;
+    mid_pass_kernel<<<unsigned(2 * nsmall), kMidBoardThreads, smem, stream>>>(
+        reinterpret_cast<const mid_job_t*>(djobs), T->win_factors, meets);
+    PG_CUDA(cudaGetLastError());
+  }
+  if (nlarge) {
+    const mid_job_t* d = reinterpret_cast<const mid_job_t*>(djobs + small_jobs_bytes(nsmall));
     const size_t smem = kMidThreads * sizeof(set0_info);
-    const int ncta = grid_ctas_per_board(int(jobs.size()), smem);
+    const int ncta = grid_ctas_per_board(nlarge, smem);
     if (ncta <= 1) {
-      mid_board_kernel<<<unsigned(jobs.size()), kMidBoardThreads, smem, stream>>>(d, T->win_factors, 0);
+      mid_board_kernel<<<unsigned(nlarge), kMidBoardThreads, smem, stream>>>(d, T->win_factors, 0);
       PG_CUDA(cudaGetLastError());
     } else {
-      if (int rc = launch_grid_boards(d, int(jobs.size()), ncta, smem, T->win_factors, stream)) return rc;
+      if (int rc = launch_grid_boards(d, nlarge, ncta, smem, T->win_factors, stream)) return rc;
     }
   }
   return PG_OK;
