@@ -216,7 +216,7 @@ int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* out, void* s
 int pg_midsolve_batch_noalloc(const uint64_t* raws, int n, pg_mid_values_t* out, void* stream);
 
 /* ---------------------------------------------------------------------------
- * Midsolve server: continuous batching on a persistent kernel (two worker
+ * Midsolve server: continuous batching on a persistent kernel (three worker
  * CTAs per SM; boards with many empty spots are solved by a gang of workers).
  * Requests are admitted while others run, as long as the request
  * ring has a free entry and the device scratch budget has room for the

@@ -231,18 +231,21 @@ static int grid_ctas_per_board(int boards, size_t smem) {
   return std::max(1, sms * per_sm / std::max(boards, 1));
 }
 
+// Per board of the grid kernel: barrier words, the n <= 1 results of both
+// passes, a fault flag; all zero at launch.
+static size_t grid_aux_bytes(int boards) {
+  return align256(sizeof(unsigned) * 2 * size_t(boards)) + align256(sizeof(uint4) * 38 * size_t(boards)) +
+         align256(sizeof(int) * size_t(boards));
+}
+
+// aux: device buffer of grid_aux_bytes(boards).
 static int launch_grid_boards(const mid_job_t* jobs, int boards, int ncta, size_t smem, const uint32_t* wf,
-                              cudaStream_t stream) {
-  // Per board: barrier words, the n <= 1 results of both passes, a fault flag
-  const size_t bar_bytes = sizeof(unsigned) * 2 * boards, raw_bytes = sizeof(uint4) * 38 * boards;
-  stream_scratch X(stream);
-  char* aux = nullptr;
-  const size_t aux_bytes = align256(bar_bytes) + align256(raw_bytes) + align256(sizeof(int) * boards);
-  PG_CUDA(X.alloc(&aux, aux_bytes));
-  PG_CUDA(cudaMemsetAsync(aux, 0, aux_bytes, stream));
+                              char* aux, cudaStream_t stream) {
+  PG_CUDA(cudaMemsetAsync(aux, 0, grid_aux_bytes(boards), stream));
   unsigned* bar = (unsigned*)aux;
-  uint4* rawg = (uint4*)(aux + align256(bar_bytes));
-  int* faults = (int*)(aux + align256(bar_bytes) + align256(raw_bytes));
+  uint4* rawg = (uint4*)(aux + align256(sizeof(unsigned) * 2 * size_t(boards)));
+  int* faults = (int*)(aux + align256(sizeof(unsigned) * 2 * size_t(boards)) +
+                       align256(sizeof(uint4) * 38 * size_t(boards)));
   void* args[] = {(void*)&jobs, (void*)&wf, (void*)&ncta, (void*)&bar, (void*)&rawg, (void*)&faults};
   PG_CUDA(cudaLaunchCooperativeKernel((void*)mid_board_grid_kernel, dim3(unsigned(boards * ncta)), dim3(kMidThreads),
                                       args, smem, stream));
@@ -265,7 +268,8 @@ void carve_scratch(board_plan& P, char* base, bool global_ws) {
 
 // pg_midsolve_batch's scratch: the pass_meet records of the shared-memory
 // boards, the job descriptors (two per shared-memory board, one per pass
-// CTA, then one per larger board), then per board its tables (twice for a
+// CTA, then one per larger board), the grid kernel's per-board words, then
+// per board its tables (twice for a
 // shared-memory board: one copy per pass CTA) and, for a larger board, its
 // global workspace.  With the caller's scratch, nothing is allocated.
 static bool smem_board(const board_plan& P) { return P.workspace <= size_t(kSmemWorkspaceMax); }
@@ -274,6 +278,11 @@ static size_t meet_bytes(int nsmall) { return align256(sizeof(pass_meet) * size_
 static size_t small_jobs_bytes(int nsmall) { return align256(sizeof(mid_job_t) * 2 * size_t(nsmall)); }
 static size_t jobs_bytes(int nsmall, int nlarge) {
   return small_jobs_bytes(nsmall) + align256(sizeof(mid_job_t) * size_t(nlarge));
+}
+// Everything before the boards' tables: pass_meet records, job descriptors
+// and the grid kernel's per-board words.
+static size_t head_bytes(int nsmall, int nlarge) {
+  return meet_bytes(nsmall) + jobs_bytes(nsmall, nlarge) + (nlarge ? grid_aux_bytes(nlarge) : 0);
 }
 
 }  // namespace pg
@@ -295,7 +304,7 @@ extern "C" int pg_midsolve_scratch_bytes(const uint64_t* raws, int n, int64_t* b
     total += batch_bytes_of(P);
     nsmall += smem_board(P);
   }
-  *bytes = int64_t(total + meet_bytes(nsmall) + jobs_bytes(nsmall, n - nsmall));
+  *bytes = int64_t(total + head_bytes(nsmall, n - nsmall));
   return PG_OK;
 }
 
@@ -321,7 +330,7 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
   }
   const int nlarge = n - nsmall;
   const size_t head = meet_bytes(nsmall), jbytes = jobs_bytes(nsmall, nlarge);
-  total += head + jbytes;
+  total += head_bytes(nsmall, nlarge);
   stream_scratch X(stream);
   char* base = (char*)scratch;
   if (!base) {
@@ -335,7 +344,8 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
   std::vector<char> host_jobs(jbytes);
   mid_job_t* small = reinterpret_cast<mid_job_t*>(host_jobs.data());
   mid_job_t* large = reinterpret_cast<mid_job_t*>(host_jobs.data() + small_jobs_bytes(nsmall));
-  size_t off = head + jbytes;
+  char* grid_aux = base + head + jbytes;
+  size_t off = head_bytes(nsmall, nlarge);
   for (int i = 0, ns = 0, nl = 0; i < n; i++) {
     auto& P = plans[i];
     P.job.out = out + i;
@@ -364,7 +374,7 @@ extern "C" int pg_midsolve_batch(const uint64_t* raws, int n, pg_mid_values_t* o
       mid_board_kernel<<<unsigned(nlarge), kMidBoardThreads, smem, stream>>>(d, T->win_factors, 0);
       PG_CUDA(cudaGetLastError());
     } else {
-      if (int rc = launch_grid_boards(d, nlarge, ncta, smem, T->win_factors, stream)) return rc;
+      if (int rc = launch_grid_boards(d, nlarge, ncta, smem, T->win_factors, grid_aux, stream)) return rc;
     }
   }
   return PG_OK;

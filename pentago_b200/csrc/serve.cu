@@ -1,6 +1,6 @@
 // Continuous-batching midsolve server.
 //
-// A persistent kernel keeps one worker CTA per SM.  Requests live in a ring in
+// A persistent kernel keeps three worker CTAs per SM.  Requests live in a ring in
 // host-mapped memory: the host writes a planned board (mid_job_t with its
 // scratch carved out of a device arena) and then publishes it by raising the
 // ring's tail.  Workers claim ring entries with an atomic on a device counter,
@@ -97,7 +97,11 @@ struct serve_dev {            // device memory
   int lock;                   // held by the idle worker refreshing the mirror
 };
 
-__global__ void __launch_bounds__(kMidThreads, 2)
+// Three workers per SM (80 registers, 65 KB of shared memory each): with two,
+// a worker's gathers from its global workspace were less covered, and the
+// server's capacity fell below one-request-at-a-time solving (496 against
+// 511 boards/s on the serving benchmark; three give 602).
+__global__ void __launch_bounds__(kMidThreads, 3)
 serve_kernel(serve_entry* ring, serve_ctl* ctl, serve_dev* dev, gang_aux* aux,
              const uint32_t* __restrict__ wf) {
   extern __shared__ uint4 smem[];

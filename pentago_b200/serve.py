@@ -97,16 +97,20 @@ def run_stream(server, raws, arrivals, timeout=600.0):
 
 
 def one_at_a_time(raws):
-    """Baseline: each board alone through pg_midsolve_batch, in sequence."""
+    """Baseline: each board alone through pg_midsolve_batch, in sequence, with
+    device scratch allocated once up front for the largest board (so no call
+    allocates)."""
     import torch
     out = torch.zeros((1, mid.RECORD_BYTES), dtype=torch.uint8, device="cuda")
+    need = max(mid.scratch_bytes(np.array([r], np.uint64)) for r in raws)
+    scratch = torch.empty(need, dtype=torch.uint8, device="cuda")
     lat = np.zeros(len(raws))
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     res = []
     for i, r in enumerate(raws):
         t = time.perf_counter()
-        mid.values_device(np.array([r], np.uint64), out=out)
+        mid.values_device(np.array([r], np.uint64), out=out, scratch=scratch)
         res.append(mid.decode(out.cpu().numpy())[0])
         lat[i] = time.perf_counter() - t
     return res, lat, time.perf_counter() - t0
