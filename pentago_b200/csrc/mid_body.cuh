@@ -121,30 +121,39 @@ PG_HD level_t make_level(const mid_job_t& J, const mid_tables& MT, int n) {
   return L;
 }
 
-// make_set0_info (mid/internal.h:174-259)
-PG_HD void build_set0(const mid_job_t& J, const mid_tables& MT, const level_t& L, int s0, set0_info& I0) {
+// make_set0_info (mid/internal.h:174-259), in two parts that two threads
+// may build side by side: part 1 the wins and child indices (and the free
+// spots), part 2 the offsets (which recount the free spots for themselves);
+// parts = 3 builds both.
+PG_HD void build_set0(const mid_job_t& J, const mid_tables& MT, const level_t& L, int s0, set0_info& I0,
+                      int parts = 3) {
   const uint64_t set0 = unrank(MT.choose, J.spots, L.k0, s0);
   const uint64_t side0 = L.root0 | set_side(J.empty, L.k0, set0);
-  I0.wins0 = h_to(h_wins(MT.wf, side0, L.parity));
   const uint64_t free_ = 0x01ff01ff01ff01ffull & ~side0;
+  uint8_t empty1[18];
   int next = 0;
   for (int i = 0; i < J.spots; i++)
-    if (free_ >> J.empty[i] & 1) I0.empty1[next++] = uint8_t(i);
-  for (int i = 0; i < J.spots - L.k0; i++) {
-    const int j = I0.empty1[i] - i;
-    int v = choose_t(MT.choose, I0.empty1[i], j + 1);
-    for (int a = 0; a < L.k0; a++) v += choose_t(MT.choose, int(set0 >> (5 * a) & 0x1f), a + (a >= j) + 1);
-    I0.child_s0s[i] = uint16_t(v);
-  }
-  for (int a = 0; a < L.k1; a++)
-    for (int q = 0; q < J.spots - L.k0; q++) {
-      int offset = a ? 0 : s0;
-      for (int i = I0.empty1[q] - q; i < L.k0; i++) {
-        const int v = int(set0 >> (5 * i) & 0x1f);
-        if (v > a) offset -= choose_t(MT.choose, v - a - 1, i);
-      }
-      I0.offset0[a * (J.spots - L.k0) + q] = uint16_t(offset);
+    if (free_ >> J.empty[i] & 1) empty1[next++] = uint8_t(i);
+  if (parts & 1) {
+    I0.wins0 = h_to(h_wins(MT.wf, side0, L.parity));
+    for (int i = 0; i < next; i++) I0.empty1[i] = empty1[i];
+    for (int i = 0; i < J.spots - L.k0; i++) {
+      const int j = empty1[i] - i;
+      int v = choose_t(MT.choose, empty1[i], j + 1);
+      for (int a = 0; a < L.k0; a++) v += choose_t(MT.choose, int(set0 >> (5 * a) & 0x1f), a + (a >= j) + 1);
+      I0.child_s0s[i] = uint16_t(v);
     }
+  }
+  if (parts & 2)
+    for (int a = 0; a < L.k1; a++)
+      for (int q = 0; q < J.spots - L.k0; q++) {
+        int offset = a ? 0 : s0;
+        for (int i = empty1[q] - q; i < L.k0; i++) {
+          const int v = int(set0 >> (5 * i) & 0x1f);
+          if (v > a) offset -= choose_t(MT.choose, v - a - 1, i);
+        }
+        I0.offset0[a * (J.spots - L.k0) + q] = uint16_t(offset);
+      }
 }
 
 // inner (mid/internal.h:358-408)
@@ -420,7 +429,11 @@ PG_HD void mid_board_body(const mid_job_t& J, const mid_tables& MT, set0_info* t
       const int r1 = L.nsets1p && i1 > i0 ? int((i1 - 1) / L.nsets1p) + 1 : r0;
       for (int base = r0; base < r1; base += kMidThreads) {
         const int rows = r1 - base < kMidThreads ? r1 - base : kMidThreads;
-        for (int r = tid; r < rows; r += nt) build_set0(J, MT, L, base + r, tiles[r]);
+        if (nt >= 2 * rows) {  // spare threads: two per row, one part each
+          if (tid < 2 * rows) build_set0(J, MT, L, base + (tid >> 1), tiles[tid >> 1], 1 + (tid & 1));
+        } else {
+          for (int r = tid; r < rows; r += nt) build_set0(J, MT, L, base + r, tiles[r]);
+        }
         barrier();
         const int64_t a = i0 > int64_t(base) * L.nsets1p ? i0 : int64_t(base) * L.nsets1p;
         const int64_t b = i1 < int64_t(base + rows) * L.nsets1p ? i1 : int64_t(base + rows) * L.nsets1p;
