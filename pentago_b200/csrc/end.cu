@@ -275,10 +275,14 @@ struct child_src {
   const uint64_t* input;
   const int64_t* in_off;
   int line_moves, last_block;
+  bool wide;  // 32-byte aligned input: 256-bit loads
 };
 PG_HD child_src child_source(const line_dev_t& L) {
-  return child_src{L.input, L.in_off, L.line_moves, L.input_blocks - 1};
+  return child_src{L.input, L.in_off, L.line_moves, L.input_blocks - 1,
+                   (reinterpret_cast<uintptr_t>(L.input) & 31) == 0};
 }
+// One half of a child node (32 bytes at p, 32-byte aligned when C.wide).
+PG_HD super8 child_load(const child_src& C, const uint64_t* p) { return C.wide ? s_load_nc32(p) : s_load_ldg(p); }
 
 // Address of child j of a microline in the line's input.
 PG_HD const uint64_t* child_addr(const child_src& C, const microline_geom& G, int j) {
@@ -501,9 +505,20 @@ PG_HD void parent_node(const line_dev_t& L, const microline_geom& G, const uint2
   const int64_t oidx = L.out_off[blk] + (blk == L.length - 1 ? G.last_output_base : G.output_base) +
                        int64_t(G.output_stride) * (i & 7);
   uint64_t* out = L.output + 8 * oidx;
+  // Node offsets are multiples of 64 bytes, so a 32-byte aligned output base
+  // allows one 256-bit access per super.
+  const bool wide = (reinterpret_cast<uintptr_t>(L.output) & 31) == 0;
   if (L.flags & PG_LINE_OR) {
-    s_store(out, s_or(s_load(out), r0));
-    s_store(out + 4, s_or(s_load(out + 4), r1));
+    if (wide) {
+      s_store32(out, s_or(s_load32(out), r0));
+      s_store32(out + 4, s_or(s_load32(out + 4), r1));
+    } else {
+      s_store(out, s_or(s_load(out), r0));
+      s_store(out + 4, s_or(s_load(out + 4), r1));
+    }
+  } else if (wide) {
+    s_store32(out, r0);
+    s_store32(out + 4, r1);
   } else {
     s_store(out, r0);
     s_store(out + 4, r1);
@@ -629,7 +644,7 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, cta_smem<MIC
   if (children) {
     int k, j;
     split(tid >> 1, nc, mc, k, j);
-    cx = s_load_ldg(child_addr(C, S.ctx[k].G, j) + 4 * (1 - half));
+    cx = child_load(C, child_addr(C, S.ctx[k].G, j) + 4 * (1 - half));
     if (!half) cs = ldg(crecs + j);
   }
   for (int w = warp; w < 2 * M; w += nt >> 5) {
@@ -654,7 +669,7 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, cta_smem<MIC
       if (x + nt < 2 * M * nc) {
         int kn, jn;
         split((x + nt) >> 1, nc, mc, kn, jn);
-        cx = s_load_ldg(child_addr(C, S.ctx[kn].G, jn) + 4 * (1 - half));
+        cx = child_load(C, child_addr(C, S.ctx[kn].G, jn) + 4 * (1 - half));
         if (!half) cs = ldg(crecs + jn);
       }
       child_half<DIM, G>(L, S.ctx[k].G, S.tab[k], reinterpret_cast<uint2*>(q_smem + 4 * k * nc), j, nc, half, v, s);

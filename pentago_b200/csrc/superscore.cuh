@@ -68,6 +68,44 @@ PG_HD void s_store(uint64_t* p, const super8& s) {
   q[1] = make_uint4(s.w[4], s.w[5], s.w[6], s.w[7]);
 }
 
+// A super in one 256-bit global access (sm_100): p must be 32-byte aligned,
+// which callers check before choosing these over the 128-bit forms above.
+// Each writes or reads a whole 32-byte sector in one instruction.
+PG_HD super8 s_load_nc32(const uint64_t* p) {
+#ifdef __CUDA_ARCH__
+  super8 s;
+  asm("ld.global.nc.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(s.w[0]), "=r"(s.w[1]), "=r"(s.w[2]), "=r"(s.w[3]), "=r"(s.w[4]), "=r"(s.w[5]), "=r"(s.w[6]),
+        "=r"(s.w[7])
+      : "l"(p));
+  return s;
+#else
+  return s_load(p);
+#endif
+}
+PG_HD super8 s_load32(const uint64_t* p) {
+#ifdef __CUDA_ARCH__
+  super8 s;
+  asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(s.w[0]), "=r"(s.w[1]), "=r"(s.w[2]), "=r"(s.w[3]), "=r"(s.w[4]), "=r"(s.w[5]), "=r"(s.w[6]),
+                 "=r"(s.w[7])
+               : "l"(p)
+               : "memory");
+  return s;
+#else
+  return s_load(p);
+#endif
+}
+PG_HD void s_store32(uint64_t* p, const super8& s) {
+#ifdef __CUDA_ARCH__
+  asm volatile("st.global.v8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "r"(s.w[0]), "r"(s.w[1]), "r"(s.w[2]),
+               "r"(s.w[3]), "r"(s.w[4]), "r"(s.w[5]), "r"(s.w[6]), "r"(s.w[7])
+               : "memory");
+#else
+  s_store(p, s);
+#endif
+}
+
 // rmax(f)(a) = max over the 8 single rotations b of f(a + b)
 // (pentago/base/superscore.h:10-16): the OR of f shifted by +-1 along each axis.
 PG_HD super8 s_rmax(const super8& f) {
