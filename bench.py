@@ -733,13 +733,23 @@ def main():
         serving = serve.bench()
 
     if rank == 0 and world == 1 and not args.no_learned:
-        # The full sweep of SWEEP_ROOT, then the learned coder trained on its
-        # 30-stone slice and run on 16384 of that slice's blocks, spread evenly over it
+        # The full sweep of SWEEP_ROOT, its section counts checked against the
+        # original solve's (data/counts-30..35.npy), then the learned coder
+        # trained on its 30-stone slice and run on every block of that slice
         torch.cuda.empty_cache()
         from pentago_b200 import learned as learned_mod
-        timings = {}
-        learned, sample = learned_mod.run_slice_coding(max_blocks=0, sample_blocks=64, sweep_timings=timings)
+        timings, counts = {}, {}
+        learned, sample = learned_mod.run_slice_coding(max_blocks=0, sample_blocks=64, sweep_timings=timings,
+                                                       sweep_counts=counts)
         sweep2 = sweep_summary(timings, learned["sweep_s"], measured_hbm_peak()[0])
+        gold = np.load(os.path.join(ROOT, "tests", "golden", "counts_30_35.npz"))
+        ok = bool(counts)
+        for s, rows in counts.items():
+            by_sig = {int(r[0]): r for r in gold[f"counts_{s}"]}
+            ok &= all(int(r[0]) in by_sig and np.array_equal(by_sig[int(r[0])], r) for r in rows)
+        sweep2["golden_counts_match"] = bool(ok)
+        sweep2["golden_sections_checked"] = sum(len(rows) for rows in counts.values())
+        sweep2["golden_counts_source"] = "tests/golden/counts_30_35.npz (data/counts-30..35.npy of the original solve)"
         if not args.no_cpu_baseline:
             learned["cpu_static_coder"] = cpu_static_coder_rate(*sample, seconds=5.0)
             sweep2["cpu_baseline"] = cpu_sweep_estimate(SWEEP_ROOT, timings, seconds_per_slice=1.5)

@@ -280,19 +280,22 @@ def store_sizes(slice_t, node_off, nodes, turn, stream=None):
 
 
 def run_slice_coding(root_counts=((4, 4), (4, 5), (4, 3), (3, 3)), train_fraction=0.01, steps=1500, batch=32768,
-                chunk_blocks=4096, max_blocks=0, seed=1, sample_blocks=0, sweep_timings=None):
+                chunk_blocks=4096, max_blocks=0, seed=1, sample_blocks=0, sweep_timings=None, sweep_counts=None):
     """Solve the root's sections down to its own slice, train on a
     seeded fraction of the root slice's blocks, code max_blocks blocks (0:
     all) both ways and check the round trip.  With sample_blocks > 0 the
     symbols of that many coded blocks are also returned on the host (for a
-    CPU comparison); sweep_timings receives the sweep's per-slice timings."""
+    CPU comparison); sweep_timings receives the sweep's per-slice timings and
+    sweep_counts its per-slice section counts (as sweep.sweep returns them)."""
     import torch
     from . import sweep
     from .end import section_sig
     root = section_sig([list(c) for c in root_counts])
     slice_ = sum(sum(c) for c in root_counts)
     t0 = time.perf_counter()
-    _, slice_t, sigs = sweep.sweep(root, keep_last=True, timings=sweep_timings)
+    counts, slice_t, sigs = sweep.sweep(root, keep_last=True, timings=sweep_timings)
+    if sweep_counts is not None:
+        sweep_counts.update(counts)
     torch.cuda.synchronize()
     t_sweep = time.perf_counter() - t0
     layout = sweep.slice_layout(sigs)
