@@ -460,6 +460,19 @@ template<int DIM>
 PG_HD void parent_node(const line_dev_t& L, const microline_geom& G, const uint2* tab0, const uint4* qs,
                        const uint2* pats, const uint4 h, const uint4* rec, int i, unsigned* errors) {
   const int p0 = L.npat[0], pp = p0 + L.npat[1];
+  // Where the result goes.  Node offsets are multiples of 64 bytes, so a
+  // 32-byte aligned output base allows one 256-bit access per super.  When
+  // accumulating, the node is prefetched into L1 first, so the read of its
+  // previous value at the end does not wait on memory.
+  const int blk = i >> 3;
+  const int64_t oidx = L.out_off[blk] + (blk == L.length - 1 ? G.last_output_base : G.output_base) +
+                       int64_t(G.output_stride) * (i & 7);
+  uint64_t* out = L.output + 8 * oidx;
+  const bool wide = (reinterpret_cast<uintptr_t>(L.output) & 31) == 0;
+  const bool accumulate = L.flags & PG_LINE_OR;
+#ifdef __CUDA_ARCH__
+  if (accumulate) asm volatile("prefetch.global.L1 [%0];" ::"l"(out));
+#endif
   // super_wins of both sides, from their rotation classes
   const super8 wins0 = pattern_rotated(pats, int(h.x & 0xff), pp, int(h.x >> 16 & 3));
   const super8 wins1 = pattern_rotated(pats, p0 + int(h.x >> 8 & 0xff), pp, int(h.x >> 18 & 3));
@@ -501,22 +514,11 @@ PG_HD void parent_node(const line_dev_t& L, const microline_geom& G, const uint2
   super8 r1 = s_or(s_andnot(not_loss, immediate), wins0);
   s_line_frame<DIM>(r0);
   s_line_frame<DIM>(r1);
-  const int blk = i >> 3;
-  const int64_t oidx = L.out_off[blk] + (blk == L.length - 1 ? G.last_output_base : G.output_base) +
-                       int64_t(G.output_stride) * (i & 7);
-  uint64_t* out = L.output + 8 * oidx;
-  // Node offsets are multiples of 64 bytes, so a 32-byte aligned output base
-  // allows one 256-bit access per super.
-  const bool wide = (reinterpret_cast<uintptr_t>(L.output) & 31) == 0;
-  if (L.flags & PG_LINE_OR) {
-    if (wide) {
-      s_store32(out, s_or(s_load32(out), r0));
-      s_store32(out + 4, s_or(s_load32(out + 4), r1));
-    } else {
-      s_store(out, s_or(s_load(out), r0));
-      s_store(out + 4, s_or(s_load(out + 4), r1));
-    }
-  } else if (wide) {
+  if (accumulate) {
+    r0 = s_or(wide ? s_load32(out) : s_load(out), r0);
+    r1 = s_or(wide ? s_load32(out + 4) : s_load(out + 4), r1);
+  }
+  if (wide) {
     s_store32(out, r0);
     s_store32(out + 4, r1);
   } else {

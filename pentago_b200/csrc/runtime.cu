@@ -75,6 +75,17 @@ const dev_tables_t* device_tables() {
     delete t;
     return nullptr;
   }
+  // The entry points take their small per-call scratch (line records,
+  // descriptors) from the device's default stream-ordered pool.  By default
+  // that pool returns freed memory to the device at every synchronization,
+  // so a caller that synchronizes between calls (a sweep, slice by slice)
+  // paid to map it again on each call; the pool now keeps up to 256 MB for
+  // reuse.  This is an attribute of this process's pool, gone at exit.
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    uint64_t keep = uint64_t(256) << 20;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   per_device[dev] = t;
   return t;
 }

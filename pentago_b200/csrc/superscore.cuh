@@ -83,14 +83,15 @@ PG_HD super8 s_load_nc32(const uint64_t* p) {
   return s_load(p);
 #endif
 }
+// (Not ordered against other memory operations by the compiler: callers
+// read memory that no other access of theirs writes before this load.)
 PG_HD super8 s_load32(const uint64_t* p) {
 #ifdef __CUDA_ARCH__
   super8 s;
-  asm volatile("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(s.w[0]), "=r"(s.w[1]), "=r"(s.w[2]), "=r"(s.w[3]), "=r"(s.w[4]), "=r"(s.w[5]), "=r"(s.w[6]),
-                 "=r"(s.w[7])
-               : "l"(p)
-               : "memory");
+  asm("ld.global.v8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=r"(s.w[0]), "=r"(s.w[1]), "=r"(s.w[2]), "=r"(s.w[3]), "=r"(s.w[4]), "=r"(s.w[5]), "=r"(s.w[6]),
+        "=r"(s.w[7])
+      : "l"(p));
   return s;
 #else
   return s_load(p);
