@@ -447,9 +447,38 @@ PG_HD void child_half(const line_dev_t& L, const microline_geom& geom, const uin
   int pk[4];
 #pragma unroll
   for (int k = 0; k < 4; k++) pk[k] = (sgn * (k - c3)) & 3;
+#ifdef __CUDA_ARCH__
+  // On the device the two threads of a child each evaluate two of W_j's four
+  // word pairs (the not-lost half's pairs 2 and 3 reach the win half by
+  // shuffles), so neither idles while the other does the lookups.  Both
+  // threads of a child are always active together.
+  {
+    uint32_t w[4];
+#pragma unroll
+    for (int kk = 0; kk < 2; kk++) {
+      const uint32_t S = select4(csub, (sgn * (2 * half + kk - c3)) & 3);
+      const uint2 a = tab0[S & 15], b = tab0[16 + (S >> 4 & 15)], d = tab0[32 + (S >> 8 & 15)],
+                  e = tab0[48 + (S >> 12 & 31)];
+      w[2 * kk] = a.x | b.x | d.x | e.x;
+      w[2 * kk + 1] = a.y | b.y | d.y | e.y;
+    }
+    const unsigned mask = __activemask();
+    uint32_t o[4];
+#pragma unroll
+    for (int t = 0; t < 4; t++) o[t] = __shfl_xor_sync(mask, w[t], 1);
+    if (half == 0) {
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        z.w[t] |= w[t];
+        z.w[4 + t] |= o[t];
+      }
+    }
+  }
+#else
   if (half == 0)
     z = s_or(z, table_eval(tab0, make_uint4(select4(csub, pk[0]), select4(csub, pk[1]), select4(csub, pk[2]),
                                             select4(csub, pk[3]))));
+#endif
 #pragma unroll
   for (int k = 0; k < 4; k++) q2[2 * (pk[k] * nc + j) + half] = make_uint2(z.w[2 * k], z.w[2 * k + 1]);
 }
@@ -647,7 +676,7 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, cta_smem<MIC
     int k, j;
     split(tid >> 1, nc, mc, k, j);
     cx = child_load(C, child_addr(C, S.ctx[k].G, j) + 4 * (1 - half));
-    if (!half) cs = ldg(crecs + j);
+    cs = ldg(crecs + j);
   }
   for (int w = warp; w < 2 * M; w += nt >> 5) {
     const int k = w >> 1;
@@ -672,7 +701,7 @@ __device__ __forceinline__ void cta_microlines(const line_dev_t& L, cta_smem<MIC
         int kn, jn;
         split((x + nt) >> 1, nc, mc, kn, jn);
         cx = child_load(C, child_addr(C, S.ctx[kn].G, jn) + 4 * (1 - half));
-        if (!half) cs = ldg(crecs + jn);
+        cs = ldg(crecs + jn);
       }
       child_half<DIM, G>(L, S.ctx[k].G, S.tab[k], reinterpret_cast<uint2*>(q_smem + 4 * k * nc), j, nc, half, v, s);
     }
